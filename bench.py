@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the progressive integrator (one JSON line on rank 0).
+
+A step renders the ring workload (1920x1080, 256 spp: a ringed giant with a
+512-bin optical-depth table, a binary star and a moon eclipse) from a fresh
+accumulation: four 64-sample dispatches of the reference's encode contract.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is whole-job Msamples/s with the scene resident on the device
+(CUDA events around each dispatch, L2 flushed between steps). `e2e` is the
+same metric through the public API with the frame handed over from host
+memory and the 33 MB accumulation read back to the host every step.
+`--impl reference` times the CPU restatement of the reference integrator
+(the oracle; the reference's own Rust/WGSL cannot run here) on the host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Msamples/s at 1080p to 1% RMSE vs oracle; adjoint/forward time ratio"
+UNIT = "Msamples/s"
+BATCH = 64
+
+# Algorithmic work model: source-level FP32/INT operations per counted event
+# of the integrator (add, mul, div, sqrt, compare, transcendental = 1 each),
+# counted from the kernel source (stargaze_b200/csrc/sg_device.cuh,
+# sg_kernels.cu). The kernel counts the events themselves.
+OPS_PER_EVENT = {
+    "vertices": 24,        # loop bookkeeping, closest-hit/ring selection, branch
+    "sphere_tests": 40,    # relative_center, a, b, cross, |cross|^2, discriminant
+    "sphere_hits": 17,     # sqrt, q, c, two divisions, root selection
+    "ring_tests": 70,      # plane denominator, double cross, along, point, annulus
+    "light_samples": 86,   # axis, cone width, stratum, sincos, basis, pdf
+    "shadow_rays": 12,     # loop overhead of light_visibility
+    "ring_events": 120,    # optics, transmission, slab BSDF, MIS, null/scatter
+    "surface_events": 110, # normal, outgoing, albedo, cosine bounce, roulette
+    "rng_draws": 10,       # LCG step + permutation + float conversion
+}
+EVENT_ORDER = ["vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples", "shadow_rays",
+               "ring_events", "surface_events", "rng_draws"]
+# DRAM traffic of one trace launch on this workload from an ncu capture
+# (profiles/trace_kernel_rings_1080p.md); None until measured.
+TRAFFIC_BYTES_PER_LAUNCH = None
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default="rings_1080p")
+    p.add_argument("--spp", type=int, default=256)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread is not None:
+                self.thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(wl, seconds: float, threads: int = 0) -> dict:
+    """The oracle (CPU restatement of the reference integrator) on all host
+    cores, over a bounded sample of the workload: whole frames of
+    8-sample dispatches until `seconds` have elapsed."""
+    from oracle.binding import OracleTracer
+    from stargaze_b200.workloads import render_options as bench_options
+
+    t = OracleTracer((wl.width, wl.height), bench_options(wl, spp=8), threads=threads)
+    for slot, tau in wl.ring_tables.items():
+        t.upload_ring_profile(slot, tau)
+    rows_per_chunk = max(1, wl.height // 27)
+    samples = 0
+    start = time.perf_counter()
+    y = 0
+    frame = wl.frame
+    while True:
+        y1 = min(y + rows_per_chunk, wl.height)
+        t.samples_ = 0
+        t.key = None
+        t.encode(frame, rows=(y, y1))
+        samples += (y1 - y) * wl.width * 8
+        y = 0 if y1 >= wl.height else y1
+        if time.perf_counter() - start >= seconds:
+            break
+    elapsed = time.perf_counter() - start
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return {"value": samples / elapsed / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{samples} samples ({wl.width}x{wl.height} frame, 8-sample dispatches, row bands) "
+                      f"in {elapsed:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from stargaze_b200.workloads import WORKLOADS
+
+    wl = WORKLOADS[args.workload](spp=args.spp)
+    per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        cpu_baseline(wl, min(per_step, 2.0))
+    values = [cpu_baseline(wl, per_step) for _ in range(args.steps)]
+    value = statistics.median(v["value"] for v in values)
+    base = values[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wl.width * wl.height * args.spp / (value * 1e6),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": args.spp,
+                   "max_bounces": wl.max_bounces, "cpu_sample": base["sample"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": base["kind"],
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from stargaze_b200 import PathTracer, abi
+    from stargaze_b200._lib import load
+    from stargaze_b200.workloads import WORKLOADS
+    from stargaze_b200.workloads import render_options as bench_options
+    import ctypes as C
+
+    lib = load()
+    wl = WORKLOADS[args.workload](spp=args.spp)
+    batches = (args.spp + BATCH - 1) // BATCH
+    # Disjoint noise sequences per rank: each GPU renders its own full-frame
+    # 256-spp estimate (weak scaling, no data-path collective).
+    opts = bench_options(wl, spp=BATCH, noise_seed=rank << 26)
+    tracer = PathTracer((wl.width, wl.height), opts, device=local)
+    for slot, tau in wl.ring_tables.items():
+        tracer.upload_ring_profile(slot, tau)
+    stream = torch.cuda.Stream()
+    frame = wl.frame.copy()
+
+    def step(i):
+        frame.scene_time = float(i)  # a new frame time restarts the accumulation
+        for _ in range(batches):
+            tracer.encode(frame, stream)
+
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # Algorithmic work of one launch (counting kernel, outside timing).
+    counter = PathTracer((wl.width, wl.height), opts, device=local)
+    for slot, tau in wl.ring_tables.items():
+        counter.upload_ring_profile(slot, tau)
+    totals = np.zeros(len(EVENT_ORDER), np.uint64)
+    ev = (C.c_uint64 * len(EVENT_ORDER))()
+    for _ in range(batches):
+        view = frame.view()
+        status = lib.sg_encode_counted(counter.handle, C.byref(view), C.c_void_p(stream.cuda_stream), ev)
+        assert status == 0, status
+        totals += np.array(list(ev), np.uint64)
+    counter.close()
+    ops_per_launch = float(sum(int(totals[k]) * OPS_PER_EVENT[n] for k, n in enumerate(EVENT_ORDER))) / batches
+    peak = C.c_double()
+    assert lib.sg_measure_fp32_peak(local, C.byref(peak)) == 0
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(-1 - i)
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = tracer.launch_count()
+        step_ms, launch_ms = [], []
+        with ClockSampler(local) as clocks:
+            for i in range(args.steps):
+                flush.zero_()  # evict the accumulation from L2 between steps
+                marks = [torch.cuda.Event(enable_timing=True) for _ in range(batches + 1)]
+                marks[0].record(stream)
+                frame.scene_time = float(i)
+                for b in range(batches):
+                    tracer.encode(frame, stream)
+                    marks[b + 1].record(stream)
+                stream.synchronize()
+                launch_ms += [marks[b].elapsed_time(marks[b + 1]) for b in range(batches)]
+                step_ms.append(marks[0].elapsed_time(marks[-1]))
+        torch.cuda.synchronize()
+        launches = tracer.launch_count() - launches0
+        if dist:
+            dist.barrier()
+
+        # End to end through the public API: frame from host memory, image
+        # read back to (pinned) host memory every step.
+        host_image = torch.empty((wl.width * wl.height * 4,), dtype=torch.float32, pin_memory=True)
+        e2e_ms = []
+        for i in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            frame.scene_time = float(1000 + i)
+            for _ in range(batches):
+                tracer.encode(frame, stream)
+            status = lib.sg_read_accumulation(tracer.handle, C.c_void_p(host_image.data_ptr()), 0,
+                                              C.c_void_p(stream.cuda_stream))
+            assert status == 0, status
+            b.record(stream)
+            stream.synchronize()
+            e2e_ms.append(a.elapsed_time(b))
+
+    total_ms = sum(step_ms)
+    e2e_total = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+
+    samples_per_step = wl.width * wl.height * args.spp
+    value = world * samples_per_step * args.steps / (total_ms * 1e-3) / 1e6
+    e2e_value = world * samples_per_step * args.steps / (e2e_total * 1e-3) / 1e6
+    mean_launch_s = statistics.mean(launch_ms) * 1e-3
+    achieved = ops_per_launch / mean_launch_s
+    result = None
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            base = cpu_baseline(wl, args.cpu_seconds)
+        clk = clocks.summary()
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": args.spp,
+                       "max_bounces": wl.max_bounces, "batches_per_step": batches, "samples_per_step": samples_per_step,
+                       "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps",
+                       "parallelism": f"replicas x{world}, disjoint noise sequences"},
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value, "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                         "kernel": "trace_kernel", "ops_per_launch": ops_per_launch,
+                         "launch_ms": statistics.mean(launch_ms),
+                         "events_per_launch": {n: int(totals[k]) // batches for k, n in enumerate(EVENT_ORDER)},
+                         "peak_source": "measured FMA-chain kernel (sg_measure_fp32_peak)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": batches * len(frame.bodies) * 160,
+                    "d2h_bytes_per_step": wl.width * wl.height * 16},
+            "gpu_launches": int(launches),
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "cpu_baseline": base,
+        }
+        print(json.dumps(result), flush=True)
+    tracer.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,300 @@
+/*
+ * stargaze_b200.h — C ABI of the B200 path-tracing integrator.
+ *
+ * Drop-in boundary for the wgpu compute pass that stargaze builds in
+ * `PathTracer::new_with_guided_ground` and drives from `PathTracer::encode`
+ * (src/pathtracer.rs:305-671, :789-1009). Scene buffers keep the reference's
+ * byte layouts, so a caller that already packs `renderer::Frame` hands the
+ * same bytes across this boundary.
+ *
+ * Conventions
+ *   - Every entry point returns an `int` status: SG_OK (0) or a negative
+ *     SG_ERR_* code. Nothing aborts the process; the reference's `assert!`
+ *     panics (src/pathtracer.rs:795-800, :279-282) become status codes.
+ *   - The library owns all device memory of a context. Host pointers passed
+ *     in are borrowed for the duration of the call only.
+ *   - One context per thread; calls on one context are not thread-safe.
+ *   - `stream` arguments are `cudaStream_t` values passed as `void*`
+ *     (NULL = legacy default stream).
+ */
+#ifndef STARGAZE_B200_H
+#define STARGAZE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SG_API __attribute__((visibility("default")))
+#else
+#define SG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes                                                        */
+/* ------------------------------------------------------------------ */
+#define SG_OK 0
+#define SG_ERR_INVALID -1   /* bad argument, size or pointer            */
+#define SG_ERR_CAPACITY -2  /* body / primitive / table capacity         */
+#define SG_ERR_CUDA -3      /* a CUDA runtime call failed                */
+#define SG_ERR_OOM -4       /* device allocation failed                  */
+#define SG_ERR_STATE -5     /* call not valid in the context's state     */
+#define SG_ERR_TIMEOUT -6   /* a bounded device loop gave up             */
+
+/* Capacities of the reference (src/pathtracer.rs:21-22, src/ground.rs:8). */
+#define SG_BODY_CAPACITY 256
+#define SG_MAX_BATCH_SAMPLES 64
+#define SG_GROUND_CAPACITY 256
+/* 2^24: the f32 sample-weight limit (src/graphics.rs:11). */
+#define SG_MAX_SAMPLES 16777216u
+/* Extension: radial optical-depth tables for rings (no reference
+ * counterpart; the reference has only a scalar or banded profile). */
+#define SG_RING_TABLE_SLOTS 8
+#define SG_RING_TABLE_MAX_BINS 4096
+/* Marker for "no body" in Ray.anchor / Hit.index (pathtrace.wgsl:60). */
+#define SG_MISS 0xffffffffu
+/* Local landscape ids (ground.wgsl:14, terrain.wgsl:23). */
+#define SG_LOCAL_BASE 0x80000000u
+#define SG_TERRAIN_ID 0x80100000u
+
+/* ------------------------------------------------------------------ */
+/* Scene layouts (byte-identical to the reference)                     */
+/* ------------------------------------------------------------------ */
+
+/* renderer::Globals, src/renderer.rs:15-31 / pathtrace.wgsl:5-18. 176 B. */
+typedef struct sg_globals {
+    float cam_right[4];
+    float cam_up[4];
+    float cam_forward[4];   /* w = tan(vertical fov / 2)                     */
+    float viewport[4];      /* trace width, height, exposure, display aspect  */
+    float atmo_center[4];   /* xyz host centre (AU), w host radius            */
+    float atmo_rayleigh[4]; /* rgb Rayleigh (1/AU), w Mie                     */
+    float atmo_params[4];   /* Mie g, scale height, top, host index + 1       */
+    float ground_east[4];   /* w = observer height (m)                        */
+    float ground_up[4];     /* w = host radius (m)                            */
+    float ground_north[4];  /* w = host index + 1 (0 disables the landscape)  */
+    uint32_t ground_counts[4]; /* props, terrain on, theme | log2 cells << 8,
+                                  prop top (f32 bits)                         */
+} sg_globals;
+
+/* pathtracer::Settings, src/pathtracer.rs:46-52 / pathtrace.wgsl:19-25. 240 B. */
+typedef struct sg_settings {
+    sg_globals g;
+    uint32_t counts[4];   /* bodies, samples so far, samples now, max vertices */
+    uint32_t sampling[4]; /* x = noise seed + sequence                         */
+    float background[4];  /* Milky Way brightness, map w, map h, point gain    */
+    uint32_t lights[4];   /* first three emissive indices, emissive count      */
+} sg_settings;
+
+/* renderer::Sphere, src/renderer.rs:35-48 / pathtrace.wgsl:26-37 (Body). 160 B. */
+typedef struct sg_sphere {
+    float center[3];          /* high part of the telescope-space centre (AU) */
+    float radius;             /* AU                                            */
+    float color[3];           /* reflectance or emitted radiance               */
+    float emissive;           /* >= 0.5 : star                                 */
+    float center_low[4];      /* xyz residual centre, w mottle strength        */
+    float ring_plane[4];      /* xyz unit pole, w inner radius / body radius   */
+    float ring_params[4];     /* outer / body radius, tau, banded,
+                                 w: extension, ring-table slot + 1 (0 = none)  */
+    float ring_color[4];      /* rgb single-scattering albedo                  */
+    float axis_x[4];          /* xyz body X axis, w surface style              */
+    float axis_y[4];          /* xyz body Y axis, w pattern seed               */
+    float surface_color[4];
+    float surface_params[4];
+} sg_sphere;
+
+/* ground::Primitive, src/ground.rs / ground.wgsl:3-7. 48 B. */
+typedef struct sg_primitive {
+    float center[4]; /* xyz surface-frame metres, w kind (<0 group marker)  */
+    float extent[4]; /* xyz half extents, w yaw or packed tumble angles     */
+    float albedo[4]; /* rgb tint, w material kind                           */
+} sg_primitive;
+
+/* pathtracer::Options, src/pathtracer.rs:77-111 (same defaults). */
+typedef struct sg_options {
+    uint32_t noise_seed;        /* 0                                   */
+    uint32_t samples_per_frame; /* 1                                   */
+    uint32_t max_bounces;       /* 8                                   */
+    uint32_t sample_limit;      /* SG_MAX_SAMPLES                      */
+    float exposure;             /* 1.0 (display only)                  */
+    int32_t auto_exposure;      /* 0   (display only)                  */
+    float ev_bias;              /* 0.0 (display only)                  */
+    float auto_key;             /* 0.25 (display only)                 */
+    float auto_percentile;      /* 0.9 (display only)                  */
+    float milky_way;            /* 4e-4 camera-only backdrop brightness */
+} sg_options;
+
+/* renderer::Frame, src/renderer.rs:50-56 (HUD labels are not part of it). */
+typedef struct sg_frame {
+    const sg_globals *globals;
+    const sg_sphere *bodies;
+    uint32_t n_bodies;
+    const sg_primitive *ground;
+    uint32_t n_ground;
+    double scene_time;
+} sg_frame;
+
+/* WGSL Ray (pathtrace.wgsl:70-76): origin = bodies[anchor] centre + offset,
+ * anchor == SG_MISS means the camera origin. 28 B. */
+typedef struct sg_ray {
+    float offset[3];
+    float direction[3];
+    uint32_t anchor;
+} sg_ray;
+
+/* WGSL Hit (pathtrace.wgsl:77-81). 20 B. */
+typedef struct sg_hit {
+    float distance;
+    uint32_t index;
+    float normal[3];
+} sg_hit;
+
+typedef struct sg_context sg_context;
+
+/* ------------------------------------------------------------------ */
+/* Lifecycle — PathTracer::new / resize / drop                         */
+/* ------------------------------------------------------------------ */
+
+/* Fill `options` with the reference defaults (Options::default,
+ * src/pathtracer.rs:95-111). */
+SG_API int sg_default_options(sg_options *options);
+
+/* PathTracer::new (src/pathtracer.rs:292-302): allocate the accumulation
+ * for a width x height trace on CUDA device `device`. `options` may be NULL
+ * for the defaults. */
+SG_API int sg_create(int device, uint32_t width, uint32_t height,
+              const sg_options *options, sg_context **out);
+
+SG_API int sg_destroy(sg_context *ctx);
+
+/* PathTracer::resize (src/pathtracer.rs:673-741): a new size reallocates the
+ * accumulation and resets the sample history but keeps the noise sequence;
+ * an unchanged size is a no-op. */
+SG_API int sg_resize(sg_context *ctx, uint32_t width, uint32_t height);
+
+/* ------------------------------------------------------------------ */
+/* Progressive rendering — PathTracer::prepare_frame / set_quality /   */
+/* encode / samples / needs_redraw                                     */
+/* ------------------------------------------------------------------ */
+
+/* PathTracer::prepare_frame (src/pathtracer.rs:756-759): update the
+ * history key; *fresh = 1 when the accumulation was reset. */
+SG_API int sg_prepare_frame(sg_context *ctx, const sg_frame *frame, int *fresh);
+
+/* PathTracer::set_quality (src/pathtracer.rs:761-773). */
+SG_API int sg_set_quality(sg_context *ctx, uint32_t samples, uint32_t bounces,
+                   uint32_t limit);
+
+/* Replace the whole option block (the reference's tests assign
+ * `tracer.options` fields directly). Transport-relevant changes reset the
+ * accumulation on the next encode through the history key. */
+SG_API int sg_set_options(sg_context *ctx, const sg_options *options);
+SG_API int sg_get_options(const sg_context *ctx, sg_options *options);
+
+/* PathTracer::encode (src/pathtracer.rs:789-1009): validate capacities,
+ * update the history, clamp the batch to SG_MAX_BATCH_SAMPLES and the
+ * sample limit, upload the frame and enqueue the trace kernel on `stream`.
+ * The call returns once the work is enqueued. */
+SG_API int sg_encode(sg_context *ctx, const sg_frame *frame, void *stream);
+
+/* History counters (PathTracer::samples, src/pathtracer.rs:742-744;
+ * History::sequence, :166-171). */
+SG_API int sg_get_samples(const sg_context *ctx, uint32_t *samples,
+                   uint32_t *sequence);
+
+/* PathTracer::needs_redraw (src/pathtracer.rs:749-752). */
+SG_API int sg_needs_redraw(const sg_context *ctx, int *redraw);
+
+SG_API int sg_get_size(const sg_context *ctx, uint32_t *width, uint32_t *height);
+
+/* Read the running-mean accumulation: width*height float4 (rgb radiance,
+ * w backdrop luminance), the buffer pathtracer_tests.rs:160-182 reads back.
+ * `dst_on_device` selects a device or host destination; the call
+ * synchronises `stream` before returning. */
+SG_API int sg_read_accumulation(sg_context *ctx, float *dst, int dst_on_device,
+                         void *stream);
+
+/* Read the backdrop accumulation (binding 7): width*height float4. */
+SG_API int sg_read_backdrop(sg_context *ctx, float *dst, int dst_on_device,
+                     void *stream);
+
+/* Resume support: restore an accumulation (width*height float4 means) with
+ * its sample count and noise sequence. */
+SG_API int sg_set_accumulation(sg_context *ctx, const float *src, int src_on_device,
+                        uint32_t samples, uint32_t sequence, void *stream);
+
+/* Device pointer of the accumulation (width*height float4), valid until the
+ * next sg_resize / sg_destroy. */
+SG_API int sg_accumulation_device_ptr(sg_context *ctx, void **ptr);
+
+/* ------------------------------------------------------------------ */
+/* Extension tables                                                    */
+/* ------------------------------------------------------------------ */
+
+/* Radial optical-depth profile for ring-table slot `slot`
+ * (0 <= slot < SG_RING_TABLE_SLOTS). A body with ring_params.w == slot + 1
+ * takes tau = ring_params.y * table[min(floor(x * bins), bins - 1)] at
+ * normalised ring radius x, and its albedo from ring_color. Uploading bumps
+ * the history key. No reference counterpart: rings.wgsl:50-81 has only the
+ * scalar and banded profiles. */
+SG_API int sg_upload_ring_profile(sg_context *ctx, uint32_t slot, const float *tau,
+                           uint32_t bins);
+
+/* ------------------------------------------------------------------ */
+/* Geometric queries (the reference's WGSL probe entry points)         */
+/* ------------------------------------------------------------------ */
+
+/* closest_hit over the frame (pathtrace.wgsl:173-185) for `n` rays.
+ * rays/hits live on the device when `on_device`, else on the host. */
+SG_API int sg_closest_hit(sg_context *ctx, const sg_frame *frame, const sg_ray *rays,
+                   uint32_t n, sg_hit *hits, int on_device, void *stream);
+
+/* light_visibility (rings.wgsl:90-115) of light body `lights[i]` along
+ * rays[i]; out[i] in [0, 1]. */
+SG_API int sg_light_visibility(sg_context *ctx, const sg_frame *frame,
+                        const sg_ray *rays, const uint32_t *lights, uint32_t n,
+                        float *out, int on_device, void *stream);
+
+/* ring_hit of body `body` along rays[i] (rings.wgsl:8-34): out[4*i..] =
+ * (distance, radius / body radius, ring_transmission, hit ? 1 : 0). */
+SG_API int sg_ring_probe(sg_context *ctx, const sg_frame *frame, const sg_ray *rays,
+                  uint32_t body, uint32_t n, float *out, int on_device,
+                  void *stream);
+
+/* Energy of the ring slab BSDF (ring_tests.rs:352-413 probe): unscattered
+ * transmission plus the cosine-weighted integral of ring_bsdf over both
+ * hemispheres at outgoing cosine `mu`, midpoint rule with `steps` bins. */
+SG_API int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu,
+                   uint32_t steps, float *energy);
+
+/* ------------------------------------------------------------------ */
+/* Diagnostics                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Last error message of the context (or of the library when ctx is NULL). */
+SG_API const char *sg_last_error(const sg_context *ctx);
+SG_API const char *sg_status_string(int status);
+/* Number of integrator kernel launches issued by this context so far. */
+SG_API int sg_launch_count(const sg_context *ctx, uint64_t *launches);
+
+/* sg_encode through the event-counting variant of the integrator kernel:
+ * same image and history effect, plus per-dispatch event totals in
+ * `events[SG_EVENT_COUNT]` (vertices, sphere tests, sphere hits, ring tests,
+ * light samples, shadow rays, ring events, surface events, RNG draws).
+ * Synchronises `stream`. Used to model the algorithmic work of a launch. */
+#define SG_EVENT_COUNT 9
+SG_API int sg_encode_counted(sg_context *ctx, const sg_frame *frame,
+                             void *stream, uint64_t *events);
+
+/* Measure the FP32 FMA issue peak of `device`: an FMA-chain kernel over
+ * every SM, timed with CUDA events. Returns FLOP/s (2 per FMA). */
+SG_API int sg_measure_fp32_peak(int device, double *flops_per_second);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* STARGAZE_B200_H */

@@ -1,0 +1,276 @@
+"""ctypes binding of oracle/liboracle.so plus a CPU `PathTracer` stand-in.
+
+TEST INFRASTRUCTURE ONLY (the checker). `OracleTracer` restates the host
+logic of stargaze's `PathTracer` (src/pathtracer.rs:164-188 History,
+:761-773 set_quality, :789-1009 encode) on top of `oracle_dispatch`, so the
+reference's known-answer tests run unchanged against both the oracle and the
+CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from stargaze_b200 import abi
+from stargaze_b200.pathtracer import HIT_DTYPE
+from stargaze_b200.scene import Frame
+
+ORACLE_DIR = Path(__file__).resolve().parent
+LIBRARY = ORACLE_DIR / "liboracle.so"
+
+
+class Tables(C.Structure):
+    _fields_ = [
+        ("ring_tau", C.c_void_p * abi.RING_TABLE_SLOTS),
+        ("ring_bins", C.c_uint32 * abi.RING_TABLE_SLOTS),
+    ]
+
+
+class Events(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in (
+        "samples", "vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples",
+        "shadow_rays", "ring_events", "surface_events", "rng_draws")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    return LIBRARY
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBRARY.exists():
+        build()
+    lib = C.CDLL(str(LIBRARY))
+    P = C.c_void_p
+    S = C.POINTER(abi.Settings)
+    lib.oracle_dispatch.argtypes = [S, P, C.POINTER(Tables), P, P, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(Events)]
+    lib.oracle_trace_sample.argtypes = [S, P, C.POINTER(Tables), C.c_uint32, C.c_uint32, C.c_uint32, P]
+    lib.oracle_closest_hit.argtypes = [S, P, C.POINTER(Tables), P, C.c_uint32, P]
+    lib.oracle_light_visibility.argtypes = [S, P, C.POINTER(Tables), P, P, C.c_uint32, P]
+    lib.oracle_reference_visibility.argtypes = [S, P, C.POINTER(Tables), P, P, C.c_uint32, P]
+    lib.oracle_ring_probe.argtypes = [S, P, C.POINTER(Tables), P, C.c_uint32, C.c_uint32, P]
+    lib.oracle_ring_energy.argtypes = [C.c_float, C.c_float, C.c_float, C.c_uint32]
+    lib.oracle_ring_energy.restype = C.c_float
+    lib.oracle_sample_light.argtypes = [S, P, P, C.c_uint32, C.POINTER(C.c_uint32), P, C.POINTER(C.c_float)]
+    lib.oracle_hash.argtypes = [C.c_uint32]
+    lib.oracle_hash.restype = C.c_uint32
+    lib.oracle_random.argtypes = [C.POINTER(C.c_uint32)]
+    lib.oracle_random.restype = C.c_float
+    for name in ("oracle_dispatch", "oracle_trace_sample", "oracle_closest_hit", "oracle_light_visibility",
+                 "oracle_reference_visibility", "oracle_ring_probe", "oracle_sample_light"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _check(status: int, what: str) -> None:
+    if status != 0:
+        raise RuntimeError(f"{what} failed with {abi.status_name(status)}")
+
+
+class TableSet:
+    """Ring optical-depth tables shared with the CUDA context."""
+
+    def __init__(self):
+        self.tables: dict[int, np.ndarray] = {}
+        self.version = 0
+
+    def upload(self, slot: int, tau) -> None:
+        self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
+        self.version += 1
+
+    def struct(self) -> Tables:
+        t = Tables()
+        for slot, arr in self.tables.items():
+            t.ring_tau[slot] = arr.ctypes.data
+            t.ring_bins[slot] = arr.size
+        return t
+
+
+def frame_bytes(frame: Frame) -> bytes:
+    out = bytes(frame.globals)
+    out += b"".join(bytes(b) for b in frame.bodies)
+    out += b"".join(bytes(p) for p in frame.ground)
+    out += np.float64(frame.scene_time).tobytes()
+    return out
+
+
+class OracleTracer:
+    """CPU restatement of the `PathTracer` host contract on the oracle."""
+
+    def __init__(self, dimensions, options: abi.Options | None = None, threads: int = 0):
+        self.lib = load()
+        self.width, self.height = int(dimensions[0]), int(dimensions[1])
+        self.opts = abi.Options.from_buffer_copy(options if options is not None else abi.default_options())
+        self.threads = threads
+        self.key = None
+        self.samples_ = 0
+        self.sequence_ = 0
+        self.idle = 0
+        self.tables = TableSet()
+        self.acc = np.zeros((self.width * self.height, 4), dtype=np.float32)
+        self.backdrop = np.zeros_like(self.acc)
+        self.events = Events()
+
+    # options mirror
+    @property
+    def options(self) -> abi.Options:
+        return abi.Options.from_buffer_copy(self.opts)
+
+    @options.setter
+    def options(self, value: abi.Options) -> None:
+        self.opts = abi.Options.from_buffer_copy(value)
+
+    def update_options(self, **fields) -> None:
+        for k, v in fields.items():
+            setattr(self.opts, k, v)
+
+    def resize(self, dimensions) -> None:
+        w, h = int(dimensions[0]), int(dimensions[1])
+        if (w, h) == (self.width, self.height):
+            return
+        self.width, self.height = w, h
+        self.acc = np.zeros((w * h, 4), dtype=np.float32)
+        self.backdrop = np.zeros_like(self.acc)
+        self.key = None
+        self.samples_ = 0
+        self.idle = 0
+
+    def samples(self) -> int:
+        return self.samples_
+
+    def sequence(self) -> int:
+        return self.sequence_
+
+    def size(self):
+        return self.width, self.height
+
+    def needs_redraw(self) -> bool:
+        return self.samples_ < self.opts.sample_limit or (bool(self.opts.auto_exposure) and self.idle < 60)
+
+    def _update_history(self, frame: Frame) -> None:
+        key = frame_bytes(frame) + np.uint32(self.opts.max_bounces).tobytes() + \
+            np.float32(self.opts.milky_way).tobytes() + np.uint64(self.tables.version).tobytes()
+        if key != self.key:
+            self.key = key
+            self.samples_ = 0
+
+    def prepare_frame(self, frame: Frame) -> bool:
+        self._update_history(frame)
+        return self.samples_ == 0
+
+    def set_quality(self, samples: int, bounces: int, limit: int) -> None:
+        bounces = min(max(bounces, 1), 64)
+        if self.opts.max_bounces != bounces:
+            self.key = None
+            self.samples_ = 0
+            self.idle = 0
+        self.opts.samples_per_frame = min(max(samples, 1), 64)
+        self.opts.max_bounces = bounces
+        self.opts.sample_limit = min(max(limit, 1), abi.MAX_SAMPLES)
+
+    def upload_ring_profile(self, slot: int, tau) -> None:
+        self.tables.upload(slot, tau)
+
+    def settings_for(self, frame: Frame, count: int) -> abi.Settings:
+        return frame.settings(self.width, self.height, self.samples_, count, self.opts.max_bounces,
+                              self.opts.noise_seed + self.sequence_, self.opts.milky_way)
+
+    def encode(self, frame: Frame, stream=None, rows=None) -> None:
+        if len(frame.bodies) > abi.BODY_CAPACITY:
+            raise RuntimeError("too many scene bodies")
+        self._update_history(frame)
+        count = min(self.opts.samples_per_frame, abi.MAX_BATCH_SAMPLES, max(self.opts.sample_limit - self.samples_, 0))
+        if count > 0:
+            s = self.settings_for(frame, count)
+            bodies = frame.bodies_array()
+            t = self.tables.struct()
+            y0, y1 = rows if rows is not None else (0, self.height)
+            _check(self.lib.oracle_dispatch(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(self.acc),
+                                            _ptr(self.backdrop), y0, y1, self.threads, C.byref(self.events)),
+                   "oracle_dispatch")
+        self.samples_ += count
+        self.sequence_ = (self.sequence_ + count) & 0xFFFFFFFF
+        self.idle = 0 if count > 0 else self.idle + 1
+
+    def read_pixels(self) -> np.ndarray:
+        return self.acc.copy()
+
+    def read_backdrop(self) -> np.ndarray:
+        return self.backdrop.copy()
+
+    # probes -------------------------------------------------------------
+    def _probe_args(self, frame: Frame):
+        s = self.settings_for(frame, 0)
+        return s, frame.bodies_array(), self.tables.struct()
+
+    def closest_hit(self, frame: Frame, rays: np.ndarray) -> np.ndarray:
+        s, bodies, t = self._probe_args(frame)
+        rays = np.ascontiguousarray(rays)
+        hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+        _check(self.lib.oracle_closest_hit(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(rays), len(rays),
+                                           _ptr(hits)), "oracle_closest_hit")
+        return hits
+
+    def light_visibility(self, frame: Frame, rays: np.ndarray, lights) -> np.ndarray:
+        s, bodies, t = self._probe_args(frame)
+        rays = np.ascontiguousarray(rays)
+        lights = np.ascontiguousarray(lights, dtype=np.uint32)
+        out = np.zeros(len(rays), dtype=np.float32)
+        _check(self.lib.oracle_light_visibility(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(rays),
+                                                _ptr(lights), len(rays), _ptr(out)), "oracle_light_visibility")
+        return out
+
+    def reference_visibility(self, frame: Frame, rays: np.ndarray, lights) -> np.ndarray:
+        s, bodies, t = self._probe_args(frame)
+        rays = np.ascontiguousarray(rays)
+        lights = np.ascontiguousarray(lights, dtype=np.uint32)
+        out = np.zeros(len(rays), dtype=np.float32)
+        _check(self.lib.oracle_reference_visibility(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(rays),
+                                                    _ptr(lights), len(rays), _ptr(out)), "oracle_reference_visibility")
+        return out
+
+    def ring_probe(self, frame: Frame, rays: np.ndarray, body: int) -> np.ndarray:
+        s, bodies, t = self._probe_args(frame)
+        rays = np.ascontiguousarray(rays)
+        out = np.zeros((len(rays), 4), dtype=np.float32)
+        _check(self.lib.oracle_ring_probe(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(rays), body,
+                                          len(rays), _ptr(out)), "oracle_ring_probe")
+        return out
+
+    def ring_energy(self, albedo: float, tau: float, mu: float, steps: int = 4096) -> float:
+        return float(self.lib.oracle_ring_energy(albedo, tau, mu, steps))
+
+    def trace_sample(self, frame: Frame, x: int, y: int, s: int) -> np.ndarray:
+        st, bodies, t = self._probe_args(frame)
+        st.counts[2] = 1
+        out = np.zeros(4, dtype=np.float32)
+        _check(self.lib.oracle_trace_sample(C.byref(st), C.cast(bodies, C.c_void_p), C.byref(t), x, y, s, _ptr(out)),
+               "oracle_trace_sample")
+        return out
+
+
+def oracle_hash(value: int) -> int:
+    return int(load().oracle_hash(value & 0xFFFFFFFF))
+
+
+def oracle_random(state: int) -> tuple[float, int]:
+    st = C.c_uint32(state & 0xFFFFFFFF)
+    value = load().oracle_random(C.byref(st))
+    return float(value), st.value

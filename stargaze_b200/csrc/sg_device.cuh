@@ -1,0 +1,540 @@
+// sg_device.cuh — device-side integrator for the B200 (sm_100a).
+//
+// Behaviour follows stargaze's progressive integrator:
+//   src/shaders/pathtrace.wgsl  (sample loop, spheres, stellar NEE + MIS,
+//                                ringshine, point discs, Russian roulette)
+//   src/shaders/rings.wgsl      (zero-thickness Beer-Lambert ring slabs)
+//
+// Design for the B200:
+//   * Settings travel as a __grid_constant__ kernel parameter (constant
+//     bank, uniform broadcast); the body table (160 B per body) and the ring
+//     optical-depth tables are staged once per CTA in shared memory.
+//   * The geometric core (sphere and ring intersection distances, the
+//     discriminant and the annulus test) is evaluated with explicit
+//     round-to-nearest intrinsics, never contracted into FMAs, so hit ids and
+//     distances are bit-identical to an IEEE f32 evaluation of the WGSL
+//     expressions. Shading arithmetic is free to use FMA.
+//   * Closest-hit loops track only (distance, index, root offset); the
+//     surface normal is formed once for the winning body.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/stargaze_b200.h"
+
+namespace sg {
+
+constexpr float kPi = 3.141592653589793f;
+constexpr float kTau = 6.283185307179586f;
+constexpr uint32_t kMiss = SG_MISS;
+constexpr float kStarDotPixels = 3.0f;
+constexpr float kPointDiscRadius = 0.00136f;
+constexpr float kRingIndirectCap = 0.003f;
+constexpr int kBodyVec4 = 10;  // float4 words per sg_sphere
+
+// Field order inside one staged body (pathtrace.wgsl:26-37).
+enum BodyField : int {
+    kCenter = 0,      // xyz high part, w radius
+    kMaterial = 1,    // rgb, w emissive
+    kLow = 2,         // xyz low part, w mottle strength
+    kRingPlane = 3,   // pole, inner
+    kRingParams = 4,  // outer, tau, banded, table slot + 1
+    kRingColor = 5,
+    kAxisX = 6,
+    kAxisY = 7,
+};
+
+// ---------------------------------------------------------------------------
+// float3 algebra
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 normalize(float3 a) { return a * (1.0f / sqrtf(dot(a, a))); }
+__device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ float luminance(float3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
+__device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+__device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+// Strict (never contracted) forms for the geometric core.
+__device__ __forceinline__ float3 add_rn(float3 a, float3 b) {
+    return f3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 sub_rn(float3 a, float3 b) {
+    return f3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 mul_rn(float3 a, float s) {
+    return f3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s));
+}
+__device__ __forceinline__ float dot_rn(float3 a, float3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 cross_rn(float3 a, float3 b) {
+    return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+              __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float3 div_rn(float3 a, float s) {
+    return f3(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s));
+}
+__device__ __forceinline__ float length_rn(float3 a) { return __fsqrt_rn(dot_rn(a, a)); }
+
+// ---------------------------------------------------------------------------
+// RNG (pathtrace.wgsl:87-98): PCG-style LCG step with a 24-bit output.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+    x = (x ^ (x >> 16)) * 0x7feb352du;
+    x = (x ^ (x >> 15)) * 0x846ca68bu;
+    return x ^ (x >> 16);
+}
+
+// Event counters for the algorithmic-work model (compiled out unless the
+// counting kernel variant is instantiated).
+struct Events {
+    uint32_t vertices, sphere_tests, sphere_hits, ring_tests, light_samples, shadow_rays,
+        ring_events, surface_events, rng_draws;
+};
+
+// ---------------------------------------------------------------------------
+// Scene view inside a CTA
+// ---------------------------------------------------------------------------
+struct Scene {
+    const sg_settings *s;   // kernel parameter space
+    const float4 *B;        // staged bodies, kBodyVec4 float4 each
+    const float *tables;    // ring optical-depth tables (slot-major)
+    const uint32_t *bins;   // bins per slot
+    uint32_t table_stride;  // floats between slots
+};
+
+template <bool COUNT>
+struct Ctx {
+    Scene sc;
+    Events ev;
+    __device__ __forceinline__ void count(uint32_t Events::*f) {
+        if constexpr (COUNT) ev.*f += 1u;
+    }
+};
+
+struct Ray {
+    float3 o;  // offset from bodies[anchor] centre, or camera origin for kMiss
+    float3 d;
+    uint32_t anchor;
+};
+
+__device__ __forceinline__ float4 bf(const Scene &S, uint32_t i, int f) { return S.B[i * kBodyVec4 + f]; }
+__device__ __forceinline__ float b_radius(const Scene &S, uint32_t i) { return S.B[i * kBodyVec4 + kCenter].w; }
+
+template <bool C>
+__device__ __forceinline__ float rnd(Ctx<C> &X, uint32_t &state) {
+    X.count(&Events::rng_draws);
+    state = state * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
+    return (float)(((word >> 22) ^ word) >> 8) * (1.0f / 16777216.0f);
+}
+
+// relative_center (pathtrace.wgsl:100-113), strict.
+__device__ __forceinline__ float3 relative_center(const Scene &S, const Ray &r, uint32_t i) {
+    if (r.anchor == i) return -r.o;
+    float3 ci = xyz(bf(S, i, kCenter));
+    float3 li = xyz(bf(S, i, kLow));
+    if (r.anchor == kMiss) return add_rn(ci, sub_rn(li, r.o));
+    float3 ca = xyz(bf(S, r.anchor, kCenter));
+    float3 la = xyz(bf(S, r.anchor, kLow));
+    return add_rn(sub_rn(ci, ca), sub_rn(sub_rn(li, la), r.o));
+}
+
+// Distance part of sphere_hit_radius (pathtrace.wgsl:134-166). Returns the
+// hit distance (1e30 on a miss) and the signed root offset `delta` that the
+// normal needs.
+template <bool C>
+__device__ __forceinline__ float sphere_distance(Ctx<C> &X, const Ray &r, uint32_t i, float radius,
+                                                 float &delta) {
+    X.count(&Events::sphere_tests);
+    const float3 oc = relative_center(X.sc, r, i);
+    const float a = dot_rn(r.d, r.d);
+    const float b = dot_rn(oc, r.d);
+    const float3 pc = cross_rn(oc, r.d);
+    const float h = __fsub_rn(__fmul_rn(__fmul_rn(a, radius), radius), dot_rn(pc, pc));
+    if (h < 0.0f) return 1.0e30f;
+    const float root = __fsqrt_rn(h);
+    const float q = __fadd_rn(b, b >= 0.0f ? root : -root);
+    if (q == 0.0f) return 1.0e30f;
+    const float c = __fsub_rn(dot_rn(oc, oc), __fmul_rn(radius, radius));
+    const float cq = __fdiv_rn(c, q);
+    const float qa = __fdiv_rn(q, a);
+    float distance = b < 0.0f ? qa : cq;
+    delta = __fdiv_rn(-root, a);
+    if (distance <= 0.0f) {
+        distance = b < 0.0f ? cq : qa;
+        delta = __fdiv_rn(root, a);
+    }
+    if (distance <= 0.0f) return 1.0e30f;
+    X.count(&Events::sphere_hits);
+    return distance;
+}
+
+// Body-local normal of sphere_hit_radius (pathtrace.wgsl:167-170).
+__device__ __forceinline__ float3 sphere_normal(const Scene &S, const Ray &r, uint32_t i, float delta) {
+    const float3 oc = relative_center(S, r, i);
+    const float a = dot_rn(r.d, r.d);
+    const float3 pc = cross_rn(oc, r.d);
+    const float3 perpendicular = div_rn(cross_rn(r.d, pc), a);
+    return normalize(-perpendicular + r.d * delta);
+}
+
+struct Hit {
+    float t;
+    uint32_t index;
+    float delta;
+};
+
+// closest_hit (pathtrace.wgsl:173-185). The local landscape is disabled in
+// the frames this build accepts (ground_north.w == 0).
+template <bool C>
+__device__ __forceinline__ Hit closest_hit(Ctx<C> &X, const Ray &r) {
+    Hit best{1.0e30f, kMiss, 0.0f};
+    const uint32_t n = X.sc.s->counts[0];
+    const float host = X.sc.s->g.ground_north[3];
+    for (uint32_t i = 0; i < n; ++i) {
+        if (host == (float)(i + 1u)) continue;
+        float delta;
+        const float t = sphere_distance(X, r, i, b_radius(X.sc, i), delta);
+        if (t < best.t) best = Hit{t, i, delta};
+    }
+    return best;
+}
+
+// basis_direction (pathtrace.wgsl:187-194).
+__device__ __forceinline__ float3 basis_direction(float3 axis, float x, float y, float z) {
+    const float3 helper = fabsf(axis.z) > 0.9f ? f3(0.0f, 1.0f, 0.0f) : f3(0.0f, 0.0f, 1.0f);
+    const float3 tangent = normalize(cross(helper, axis));
+    return normalize(tangent * x + cross(axis, tangent) * y + axis * z);
+}
+
+// cone_width (pathtrace.wgsl:197-202): 1 - cos(theta_max) without cancellation.
+__device__ __forceinline__ float cone_width_oc(float3 oc, float r) {
+    const float sin2 = clampf(r * r / dot(oc, oc), 1.0e-20f, 1.0f);
+    return sin2 / (1.0f + sqrtf(1.0f - sin2));
+}
+
+__device__ __forceinline__ uint32_t light_count(const sg_settings *s) {
+    return s->lights[3] <= 3u ? s->lights[3] : s->counts[0];
+}
+__device__ __forceinline__ uint32_t light_index(const sg_settings *s, uint32_t slot) {
+    return s->lights[3] <= 3u ? s->lights[slot] : slot;
+}
+
+struct LightSample {
+    float3 d;
+    float pdf;
+};
+
+// sample_light (pathtrace.wgsl:214-234), one stratum: uniform cone sampling.
+template <bool C>
+__device__ __forceinline__ LightSample sample_light(Ctx<C> &X, const Ray &r, uint32_t i, uint32_t &rng) {
+    X.count(&Events::light_samples);
+    const float3 oc = relative_center(X.sc, r, i);
+    const float3 axis = normalize(oc);
+    const float width = cone_width_oc(oc, b_radius(X.sc, i));
+    const float radial = rnd(X, rng);
+    const float azimuth = rnd(X, rng);
+    const float one_minus_cos = radial * width;
+    const float sin_theta = sqrtf(one_minus_cos * (2.0f - one_minus_cos));
+    float sp, cp;
+    sincosf(kTau * azimuth, &sp, &cp);
+    LightSample ls;
+    ls.d = basis_direction(axis, sin_theta * cp, sin_theta * sp, 1.0f - one_minus_cos);
+    ls.pdf = 1.0f / (kTau * width);
+    return ls;
+}
+
+// power_weight (pathtrace.wgsl:264-267): power heuristic, beta = 2.
+__device__ __forceinline__ float power_weight(float a, float b) {
+    const float ratio = b / fmaxf(a, 1.0e-30f);
+    return 1.0f / (1.0f + ratio * ratio);
+}
+
+// ---------------------------------------------------------------------------
+// Rings (rings.wgsl)
+// ---------------------------------------------------------------------------
+struct RingHit {
+    float t;
+    uint32_t index;
+    float3 p;  // planet-local point
+};
+
+__device__ __forceinline__ bool has_ring(const Scene &S, uint32_t i) {
+    const float4 rp = bf(S, i, kRingParams);
+    return !(rp.x <= bf(S, i, kRingPlane).w || rp.y <= 0.0f);
+}
+
+// ring_hit (rings.wgsl:8-34), strict.
+template <bool C>
+__device__ __forceinline__ RingHit ring_hit(Ctx<C> &X, const Ray &r, uint32_t i) {
+    RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
+    const float4 plane = bf(X.sc, i, kRingPlane);
+    const float4 params = bf(X.sc, i, kRingParams);
+    if (params.x <= plane.w || params.y <= 0.0f) return miss;
+    X.count(&Events::ring_tests);
+    const float3 n = xyz(plane);
+    const float denom = dot_rn(r.d, n);
+    if (fabsf(denom) < 1.0e-7f) return miss;
+    const float3 oc = relative_center(X.sc, r, i);
+    const float a = dot_rn(r.d, r.d);
+    const float3 perpendicular = div_rn(cross_rn(r.d, cross_rn(r.d, oc)), a);
+    const float along = __fdiv_rn(-dot_rn(perpendicular, n), denom);
+    const float distance = __fadd_rn(__fdiv_rn(dot_rn(oc, r.d), a), along);
+    if (distance <= 0.0f) return miss;
+    const float3 point = add_rn(perpendicular, mul_rn(r.d, along));
+    const float radius = __fdiv_rn(length_rn(point), b_radius(X.sc, i));
+    if (radius < plane.w || radius > params.x) return miss;
+    return RingHit{distance, i, point};
+}
+
+// closest_ring (rings.wgsl:36-45).
+template <bool C>
+__device__ __forceinline__ RingHit closest_ring(Ctx<C> &X, const Ray &r, float limit) {
+    RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
+    const uint32_t n = X.sc.s->counts[0];
+    for (uint32_t i = 0; i < n; ++i) {
+        const RingHit h = ring_hit(X, r, i);
+        if (h.index != kMiss && h.t < best.t) best = h;
+    }
+    return best;
+}
+
+struct Optics {
+    float3 color;
+    float tau;
+};
+
+// ring_optics (rings.wgsl:50-81) plus the tabulated profile extension.
+__device__ __forceinline__ Optics ring_optics(const Scene &S, uint32_t i, float3 point) {
+    const float4 plane = bf(S, i, kRingPlane);
+    const float4 params = bf(S, i, kRingParams);
+    const float radius = __fdiv_rn(length_rn(point), b_radius(S, i));
+    const float x = __fdiv_rn(__fsub_rn(radius, plane.w), __fsub_rn(params.x, plane.w));
+    float tau = params.y;
+    float3 color = xyz(bf(S, i, kRingColor));
+    if (params.w >= 0.5f) {
+        const uint32_t slot = (uint32_t)params.w - 1u;
+        const uint32_t bins = slot < SG_RING_TABLE_SLOTS ? S.bins[slot] : 0u;
+        if (bins > 0u) {
+            const float fb = x * (float)bins;
+            uint32_t bin = fb <= 0.0f ? 0u : (uint32_t)fb;
+            bin = bin > bins - 1u ? bins - 1u : bin;
+            tau *= S.tables[slot * S.table_stride + bin];
+        } else {
+            tau = 0.0f;
+        }
+    } else if (params.z > 0.5f) {
+        const float broad = 0.5f + 0.5f * sinf(43.0f * x + 1.8f * sinf(17.0f * x));
+        const float fine = 0.5f + 0.5f * sinf(1900.0f * x + 2.0f * sinf(311.0f * x));
+        const float micro = 0.5f + 0.5f * sinf(6100.0f * x);
+        float density = 0.12f;
+        float3 tint = f3(0.70f, 0.68f, 0.65f);
+        if (x >= 0.2792f && x < 0.6910f) {
+            density = 1.25f + 1.1f * broad;
+            tint = f3(1.0f, 1.0f, 1.0f);
+        } else if (x >= 0.6910f && x < 0.7649f) {
+            density = 0.025f;
+            tint = f3(0.75f, 0.75f, 0.75f);
+        } else if (x >= 0.7649f) {
+            density = 0.48f + 0.22f * broad;
+            tint = f3(0.92f, 0.94f, 0.98f);
+        }
+        density *= 0.65f + 0.45f * fine + 0.12f * micro;
+        if (fabsf(x - 0.9487f) < 0.00262f || fabsf(x - 0.99565f) < 0.00034f) density = 0.0f;
+        tau *= density;
+        color = color * tint * (0.94f + 0.06f * broad);
+    }
+    return Optics{color, tau};
+}
+
+__device__ __forceinline__ float ring_transmission_tau(float3 d, float3 pole, float tau) {
+    const float mu = fmaxf(fabsf(dot(d, pole)), 1.0e-7f);
+    return expf(-tau / mu);
+}
+
+// ring_transmission (rings.wgsl:83-86).
+__device__ __forceinline__ float ring_transmission(const Scene &S, const Ray &r, const RingHit &h) {
+    return ring_transmission_tau(r.d, xyz(bf(S, h.index, kRingPlane)), ring_optics(S, h.index, h.p).tau);
+}
+
+// light_visibility (rings.wgsl:90-115): distance to the light, any-hit over
+// the other spheres (ties broken by index), then ring transmissions before
+// the light.
+template <bool C>
+__device__ __forceinline__ float light_visibility(Ctx<C> &X, const Ray &r, uint32_t light) {
+    X.count(&Events::shadow_rays);
+    float delta;
+    const float surface = sphere_distance(X, r, light, b_radius(X.sc, light), delta);
+    if (surface >= 1.0e30f) return 0.0f;
+    const sg_settings *s = X.sc.s;
+    const float host = s->g.ground_north[3];
+    const uint32_t n = s->counts[0];
+    if (host == (float)(light + 1u) && closest_hit(X, r).index != light) return 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (i == light || host == (float)(i + 1u)) continue;
+        const float t = sphere_distance(X, r, i, b_radius(X.sc, i), delta);
+        if (t < 1.0e30f && (t < surface || (t == surface && i < light))) return 0.0f;
+    }
+    float transmission = 1.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        const RingHit h = ring_hit(X, r, i);
+        if (h.index != kMiss && h.t < surface) transmission *= ring_transmission(X.sc, r, h);
+    }
+    return transmission;
+}
+
+// one_minus_exp (rings.wgsl:143-145).
+__device__ __forceinline__ float one_minus_exp(float x) {
+    return x < 1.0e-3f ? x * (1.0f - 0.5f * x) : 1.0f - expf(-x);
+}
+
+// ring_bsdf (rings.wgsl:151-166): exact single scattering in a finite slab.
+__device__ __forceinline__ float3 ring_bsdf(const Optics &o, float outgoing, float incoming) {
+    const float mo = fmaxf(fabsf(outgoing), 1.0e-7f);
+    const float mi = fmaxf(fabsf(incoming), 1.0e-7f);
+    const float a = o.tau / mo;
+    const float b = o.tau / mi;
+    if (outgoing * incoming < 0.0f) {
+        const float delta = fabsf(a - b);
+        const float integral =
+            delta < 1.0e-3f ? 1.0f - 0.5f * delta : one_minus_exp(delta) / fmaxf(delta, 1.0e-20f);
+        const float factor = o.tau / (mo * mi) * expf(-fminf(a, b)) * integral;
+        return o.color * (factor / (4.0f * kPi));
+    }
+    const float factor = one_minus_exp(a + b) / (mo + mi);
+    return o.color * (factor / (4.0f * kPi));
+}
+
+// ring_origin (rings.wgsl:168-175): reproject onto the plane, then offset
+// by 2e-6 planet radii towards the outgoing side.
+__device__ __forceinline__ Ray ring_origin(const Scene &S, uint32_t index, float3 point, float3 direction) {
+    const float3 n = xyz(bf(S, index, kRingPlane));
+    const float sign = dot(direction, n) >= 0.0f ? 1.0f : -1.0f;
+    const float3 p = point - n * dot(point, n);
+    return Ray{p + n * (sign * b_radius(S, index) * 2.0e-6f), direction, index};
+}
+
+// ring_area (pathtrace.wgsl:1237-1241).
+__device__ __forceinline__ float ring_area(const Scene &S, uint32_t i) {
+    const float r = b_radius(S, i);
+    const float outer = bf(S, i, kRingParams).x;
+    const float inner = bf(S, i, kRingPlane).w;
+    return kPi * r * r * (outer * outer - inner * inner);
+}
+
+// ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
+template <bool C>
+__device__ float3 ringshine(Ctx<C> &X, uint32_t index, float3 origin, float3 normal, bool last_vertex,
+                            uint32_t &rng) {
+    const Scene &S = X.sc;
+    if (!has_ring(S, index)) return f3(0.0f, 0.0f, 0.0f);
+    const float3 n = xyz(bf(S, index, kRingPlane));
+    const float inner = bf(S, index, kRingPlane).w;
+    const float outer = bf(S, index, kRingParams).x;
+    const float radius = sqrtf(mixf(inner * inner, outer * outer, rnd(X, rng))) * b_radius(S, index);
+    float sp, cp;
+    sincosf(kTau * rnd(X, rng), &sp, &cp);
+    const float3 point = basis_direction(n, cp, sp, 0.0f) * radius;
+    const float3 offset = point - origin;
+    const float distance2 = dot(offset, offset);
+    const float distance = sqrtf(distance2);
+    const float3 direction = offset / distance;
+    const float cos_surface = dot(normal, direction);
+    const float cos_ring = fabsf(dot(direction, n));
+    if (cos_surface <= 0.0f || cos_ring < 1.0e-6f) return f3(0.0f, 0.0f, 0.0f);
+    float delta;
+    const float blocker = sphere_distance(X, Ray{origin, direction, index}, index, b_radius(S, index), delta);
+    if (blocker < distance) return f3(0.0f, 0.0f, 0.0f);
+    const Optics optics = ring_optics(S, index, point);
+    if (optics.tau == 0.0f) return f3(0.0f, 0.0f, 0.0f);
+    const float mu_out = dot(-direction, n);
+    float3 shine = f3(0.0f, 0.0f, 0.0f);
+    const uint32_t count = light_count(S.s);
+    for (uint32_t slot = 0; slot < count; ++slot) {
+        const uint32_t i = light_index(S.s, slot);
+        if (bf(S, i, kMaterial).w < 0.5f) continue;
+        const LightSample light = sample_light(X, Ray{point, n, index}, i, rng);
+        const float mu_in = dot(light.d, n);
+        const float visibility = light_visibility(X, ring_origin(S, index, point, light.d), i);
+        shine = shine + ring_bsdf(optics, mu_out, mu_in) * xyz(bf(S, i, kMaterial)) *
+                            (fabsf(mu_in) * visibility / light.pdf);
+    }
+    const float pdf = distance2 / (ring_area(S, index) * cos_ring);
+    const float weight = last_vertex ? 1.0f : power_weight(pdf, cos_surface / kPi);
+    return shine * (cos_surface * weight / (kPi * pdf));
+}
+
+// point_gain (pathtrace.wgsl:1341-1345).
+__device__ __forceinline__ float point_gain(const sg_settings *s, float extent, float distance) {
+    const float pixel = 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);
+    const float pixels = 2.0f * extent / fmaxf(distance, 1.0e-30f) / pixel;
+    return mixf(s->background[3], 1.0f, smoothstepf(1.0f, 3.0f, pixels));
+}
+
+// ---------------------------------------------------------------------------
+// Surface albedo, style 0 with optional value-noise mottle
+// (pathtrace.wgsl:338-354, :377-389, :897-925).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fractf(float x) { return x - floorf(x); }
+__device__ __forceinline__ float hash31(float3 p) {
+    float3 q = f3(fractf(p.x * 0.1031f), fractf(p.y * 0.1030f), fractf(p.z * 0.0973f));
+    const float d = dot(q, f3(q.y + 33.33f, q.x + 33.33f, q.z + 33.33f));
+    q = f3(q.x + d, q.y + d, q.z + d);
+    return fractf((q.x + q.y) * q.z);
+}
+__device__ float vnoise(float3 p) {
+    const float3 i = f3(floorf(p.x), floorf(p.y), floorf(p.z));
+    const float3 f = p - i;
+    const float3 u = f3(f.x * f.x * (3.0f - 2.0f * f.x), f.y * f.y * (3.0f - 2.0f * f.y),
+                        f.z * f.z * (3.0f - 2.0f * f.z));
+    const float a = mixf(hash31(i), hash31(i + f3(1, 0, 0)), u.x);
+    const float b = mixf(hash31(i + f3(0, 1, 0)), hash31(i + f3(1, 1, 0)), u.x);
+    const float c = mixf(hash31(i + f3(0, 0, 1)), hash31(i + f3(1, 0, 1)), u.x);
+    const float d = mixf(hash31(i + f3(0, 1, 1)), hash31(i + f3(1, 1, 1)), u.x);
+    return mixf(mixf(a, b, u.y), mixf(c, d, u.y), u.z);
+}
+__device__ __forceinline__ float3 surface_albedo(const Scene &S, uint32_t i, float3 normal) {
+    const float4 material = bf(S, i, kMaterial);
+    const float mottle_strength = bf(S, i, kLow).w;
+    float mottle = 1.0f;
+    if (mottle_strength > 0.0f) {
+        const float3 x = xyz(bf(S, i, kAxisX));
+        const float4 ay = bf(S, i, kAxisY);
+        const float3 y = xyz(ay);
+        const float3 local = f3(dot(normal, x), dot(normal, y), dot(normal, cross(x, y)));
+        const float seed = ay.w;
+        const float3 off =
+            f3(hash31(f3(seed, 1.0f, 7.0f)), hash31(f3(3.0f, seed, 5.0f)), hash31(f3(9.0f, 2.0f, seed))) *
+            512.0f;
+        float3 p = local * 2.4f + off;
+        float amplitude = 0.5f, noise = 0.0f;
+        for (int octave = 0; octave < 5; ++octave) {
+            noise += amplitude * vnoise(p);
+            p = p * 2.07f;
+            amplitude *= 0.5f;
+        }
+        mottle = mixf(1.0f, 0.68f + 0.64f * noise, mottle_strength);
+    }
+    return f3(clampf(material.x * mottle, 0.0f, 1.0f), clampf(material.y * mottle, 0.0f, 1.0f),
+              clampf(material.z * mottle, 0.0f, 1.0f));
+}
+
+}  // namespace sg

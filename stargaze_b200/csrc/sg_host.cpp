@@ -1,0 +1,671 @@
+// sg_host.cpp — C-ABI host runtime of the B200 integrator.
+//
+// Mirrors the host side of stargaze's `PathTracer` (src/pathtracer.rs):
+// options and their defaults (:77-111), the sample History and its reset key
+// (:164-188), quality control (:761-773), and `encode` (:789-1009): capacity
+// checks, batch clamping, Settings packing and the trace dispatch. wgpu
+// buffers become device allocations owned by the context; `assert!` panics
+// become SG_ERR_* status codes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/stargaze_b200.h"
+#include "sg_internal.h"
+
+namespace {
+
+// sky::WIDTH / sky::HEIGHT (Milky Way map size, src/sky.rs) and
+// stars::POINT_SOURCE_GAIN (src/stars.rs:130), as packed into
+// Settings.background by encode (src/pathtracer.rs:853-858).
+constexpr float kMilkyWayWidth = 1024.0f;
+constexpr float kMilkyWayHeight = 512.0f;
+constexpr float kPointSourceGain = 100.0f;
+// Default terrain grid of the forest ground (src/terrain.rs:10), packed as
+// log2(cells) into ground_counts.z bits 8..15 (src/pathtracer.rs:825-828).
+constexpr uint32_t kDefaultTerrainCells = 512;
+
+thread_local std::string g_last_error;
+
+struct History {
+    std::vector<uint8_t> key;
+    uint32_t samples = 0;
+    uint32_t sequence = 0;
+};
+
+}  // namespace
+
+struct sg_context {
+    int device = 0;
+    uint32_t width = 0, height = 0;
+    sg_options options{};
+    History history;
+    uint32_t exposure_idle_frames = 0;
+    float4 *mean = nullptr;
+    float4 *sum = nullptr;
+    float4 *comp = nullptr;
+    float4 *backdrop = nullptr;
+    sg_sphere *bodies = nullptr;  // SG_BODY_CAPACITY
+    float *ring_tables = nullptr; // SG_RING_TABLE_SLOTS * SG_RING_TABLE_MAX_BINS
+    uint32_t ring_bins[SG_RING_TABLE_SLOTS] = {};
+    uint64_t table_version = 0;
+    unsigned long long *events = nullptr;  // kEventCount counters
+    void *scratch = nullptr;               // query staging
+    size_t scratch_bytes = 0;
+    uint64_t launches = 0;
+    std::string last_error;
+};
+
+namespace {
+
+int fail(sg_context *ctx, int status, const std::string &message) {
+    if (ctx) ctx->last_error = message;
+    g_last_error = message;
+    return status;
+}
+
+int cuda_fail(sg_context *ctx, cudaError_t e, const char *what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(ctx, e == cudaErrorMemoryAllocation ? SG_ERR_OOM : SG_ERR_CUDA, msg);
+}
+
+#define SG_CUDA(ctx, call)                                   \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+struct DeviceGuard {
+    int previous = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+        if (previous != device) cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        if (previous >= 0) cudaSetDevice(previous);
+    }
+};
+
+void free_image(sg_context *ctx) {
+    cudaFree(ctx->mean);
+    cudaFree(ctx->sum);
+    cudaFree(ctx->comp);
+    cudaFree(ctx->backdrop);
+    ctx->mean = ctx->sum = ctx->comp = ctx->backdrop = nullptr;
+}
+
+int alloc_image(sg_context *ctx) {
+    // accumulation() in src/pathtracer.rs:277-289 sizes at least 16 bytes.
+    const size_t pixels = std::max<size_t>((size_t)ctx->width * ctx->height, 1);
+    const size_t bytes = pixels * sizeof(float4);
+    SG_CUDA(ctx, cudaMalloc(&ctx->mean, bytes));
+    SG_CUDA(ctx, cudaMalloc(&ctx->sum, bytes));
+    SG_CUDA(ctx, cudaMalloc(&ctx->comp, bytes));
+    SG_CUDA(ctx, cudaMalloc(&ctx->backdrop, bytes));
+    SG_CUDA(ctx, cudaMemset(ctx->mean, 0, bytes));
+    SG_CUDA(ctx, cudaMemset(ctx->sum, 0, bytes));
+    SG_CUDA(ctx, cudaMemset(ctx->comp, 0, bytes));
+    SG_CUDA(ctx, cudaMemset(ctx->backdrop, 0, bytes));
+    return SG_OK;
+}
+
+void reset_history(sg_context *ctx) {
+    const uint32_t sequence = ctx->history.sequence;
+    ctx->history = History{};
+    ctx->history.sequence = sequence;
+}
+
+template <typename T>
+void append(std::vector<uint8_t> &key, const T &value) {
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(&value);
+    key.insert(key.end(), p, p + sizeof(T));
+}
+
+// History::update (src/pathtracer.rs:173-187): the accumulation survives
+// only while globals, bodies, ground, scene time, bounces, Milky Way
+// brightness (and here the ring tables) are byte-identical.
+void update_history(sg_context *ctx, const sg_frame *frame) {
+    std::vector<uint8_t> key;
+    key.reserve(sizeof(sg_globals) + frame->n_bodies * sizeof(sg_sphere) + frame->n_ground * sizeof(sg_primitive) + 32);
+    append(key, *frame->globals);
+    if (frame->n_bodies)
+        key.insert(key.end(), reinterpret_cast<const uint8_t *>(frame->bodies),
+                   reinterpret_cast<const uint8_t *>(frame->bodies + frame->n_bodies));
+    if (frame->n_ground)
+        key.insert(key.end(), reinterpret_cast<const uint8_t *>(frame->ground),
+                   reinterpret_cast<const uint8_t *>(frame->ground + frame->n_ground));
+    append(key, frame->scene_time);
+    append(key, ctx->options.max_bounces);
+    append(key, ctx->options.milky_way);
+    append(key, ctx->table_version);
+    if (key != ctx->history.key) {
+        ctx->history.key = std::move(key);
+        ctx->history.samples = 0;
+    }
+}
+
+// Validation shared by encode and the probes (src/pathtracer.rs:795-800
+// plus the features this build does not implement yet).
+int validate_frame(sg_context *ctx, const sg_frame *frame) {
+    if (!frame || !frame->globals) return fail(ctx, SG_ERR_INVALID, "frame or frame->globals is NULL");
+    if (frame->n_bodies > SG_BODY_CAPACITY) return fail(ctx, SG_ERR_CAPACITY, "too many scene bodies");
+    if (frame->n_bodies && !frame->bodies) return fail(ctx, SG_ERR_INVALID, "frame->bodies is NULL");
+    if (frame->n_ground > SG_GROUND_CAPACITY) return fail(ctx, SG_ERR_CAPACITY, "too many local primitives");
+    if (frame->n_ground && !frame->ground) return fail(ctx, SG_ERR_INVALID, "frame->ground is NULL");
+    if (frame->globals->ground_counts[0] != frame->n_ground)
+        return fail(ctx, SG_ERR_INVALID, "ground_counts.x does not match the primitive count");
+    if (frame->globals->atmo_params[3] >= 0.5f)
+        return fail(ctx, SG_ERR_INVALID, "the host atmosphere (atmo_params.w >= 0.5) is not implemented");
+    if (frame->globals->ground_north[3] != 0.0f)
+        return fail(ctx, SG_ERR_INVALID, "the local landscape (ground_north.w != 0) is not implemented");
+    for (uint32_t i = 0; i < frame->n_bodies; ++i) {
+        const float slot = frame->bodies[i].ring_params[3];
+        if (slot >= 0.5f && (slot > (float)SG_RING_TABLE_SLOTS || slot != std::floor(slot)))
+            return fail(ctx, SG_ERR_INVALID, "ring_params.w must be 0 or a ring-table slot + 1");
+    }
+    return SG_OK;
+}
+
+// The Settings packing of encode (src/pathtracer.rs:812-859).
+sg_settings pack_settings(const sg_context *ctx, const sg_frame *frame, uint32_t count) {
+    sg_settings s;
+    std::memset(&s, 0, sizeof(s));
+    s.g = *frame->globals;
+    s.g.viewport[3] = s.g.viewport[0] / std::max(s.g.viewport[1], 1.0f);
+    s.g.viewport[0] = (float)ctx->width;
+    s.g.viewport[1] = (float)ctx->height;
+    s.g.viewport[2] = ctx->options.exposure;
+    float prop_top = 0.0f;
+    for (uint32_t i = 0; i < frame->n_ground; ++i) {
+        const float *e = frame->ground[i].extent;
+        const float len = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        prop_top = std::max(prop_top, frame->ground[i].center[1] + len);
+    }
+    std::memcpy(&s.g.ground_counts[3], &prop_top, sizeof(float));
+    uint32_t cells = kDefaultTerrainCells, log2 = 0;
+    while ((1u << log2) < cells) ++log2;
+    s.g.ground_counts[2] |= log2 << 8;
+    for (uint32_t i = 0; i < frame->n_bodies; ++i) {
+        if (frame->bodies[i].emissive >= 0.5f) {
+            if (s.lights[3] < 3u) s.lights[s.lights[3]] = i;
+            s.lights[3] += 1u;
+        }
+    }
+    s.sampling[0] = ctx->options.noise_seed + ctx->history.sequence;
+    s.counts[0] = frame->n_bodies;
+    s.counts[1] = ctx->history.samples;
+    s.counts[2] = count;
+    s.counts[3] = ctx->options.max_bounces;
+    s.background[0] = ctx->options.milky_way;
+    s.background[1] = kMilkyWayWidth;
+    s.background[2] = kMilkyWayHeight;
+    s.background[3] = kPointSourceGain;
+    return s;
+}
+
+int upload_bodies(sg_context *ctx, const sg_frame *frame, cudaStream_t stream) {
+    if (frame->n_bodies == 0) return SG_OK;
+    SG_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, frame->bodies, frame->n_bodies * sizeof(sg_sphere),
+                                 cudaMemcpyHostToDevice, stream));
+    return SG_OK;
+}
+
+sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
+    sg::TraceParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.s = s;
+    p.bodies = reinterpret_cast<const float4 *>(ctx->bodies);
+    p.tables = ctx->ring_tables;
+    uint32_t used_floats = 0;
+    for (int k = 0; k < SG_RING_TABLE_SLOTS; ++k) {
+        p.bins[k] = ctx->ring_bins[k];
+        if (ctx->ring_bins[k]) used_floats = (uint32_t)(k + 1) * SG_RING_TABLE_MAX_BINS;
+    }
+    p.table_stride = SG_RING_TABLE_MAX_BINS;
+    // Stage the tables in shared memory when the used slots fit in 32 KB.
+    p.staged_table_floats = used_floats * sizeof(float) <= 32u * 1024u ? used_floats : 0u;
+    p.mean = ctx->mean;
+    p.sum = ctx->sum;
+    p.comp = ctx->comp;
+    p.width = ctx->width;
+    p.height = ctx->height;
+    p.events = nullptr;
+    return p;
+}
+
+int ensure_scratch(sg_context *ctx, size_t bytes) {
+    if (ctx->scratch_bytes >= bytes) return SG_OK;
+    cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    SG_CUDA(ctx, cudaMalloc(&ctx->scratch, bytes));
+    ctx->scratch_bytes = bytes;
+    return SG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sg_default_options(sg_options *o) {
+    if (!o) return SG_ERR_INVALID;
+    o->noise_seed = 0;
+    o->samples_per_frame = 1;
+    o->max_bounces = 8;
+    o->sample_limit = SG_MAX_SAMPLES;
+    o->exposure = 1.0f;
+    o->auto_exposure = 0;
+    o->ev_bias = 0.0f;
+    o->auto_key = 0.25f;
+    o->auto_percentile = 0.9f;
+    o->milky_way = 4.0e-4f;
+    return SG_OK;
+}
+
+int sg_create(int device, uint32_t width, uint32_t height, const sg_options *options, sg_context **out) {
+    if (!out) return fail(nullptr, SG_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return fail(nullptr, SG_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= count) return fail(nullptr, SG_ERR_INVALID, "no such CUDA device");
+    if ((uint64_t)width * height > (1ull << 31)) return fail(nullptr, SG_ERR_INVALID, "viewport too large");
+    sg_context *ctx = new (std::nothrow) sg_context();
+    if (!ctx) return fail(nullptr, SG_ERR_OOM, "host allocation failed");
+    ctx->device = device;
+    ctx->width = width;
+    ctx->height = height;
+    if (options) ctx->options = *options;
+    else sg_default_options(&ctx->options);
+    DeviceGuard guard(device);
+    int status = alloc_image(ctx);
+    if (status == SG_OK) {
+        if ((e = cudaMalloc(&ctx->bodies, SG_BODY_CAPACITY * sizeof(sg_sphere))) != cudaSuccess ||
+            (e = cudaMalloc(&ctx->ring_tables, SG_RING_TABLE_SLOTS * SG_RING_TABLE_MAX_BINS * sizeof(float))) !=
+                cudaSuccess ||
+            (e = cudaMalloc(&ctx->events, sg::kEventCount * sizeof(unsigned long long))) != cudaSuccess)
+            status = cuda_fail(ctx, e, "cudaMalloc");
+    }
+    if (status == SG_OK) {
+        e = cudaMemset(ctx->ring_tables, 0, SG_RING_TABLE_SLOTS * SG_RING_TABLE_MAX_BINS * sizeof(float));
+        if (e != cudaSuccess) status = cuda_fail(ctx, e, "cudaMemset");
+    }
+    if (status != SG_OK) {
+        sg_destroy(ctx);
+        return status;
+    }
+    *out = ctx;
+    return SG_OK;
+}
+
+int sg_destroy(sg_context *ctx) {
+    if (!ctx) return SG_OK;
+    DeviceGuard guard(ctx->device);
+    free_image(ctx);
+    cudaFree(ctx->bodies);
+    cudaFree(ctx->ring_tables);
+    cudaFree(ctx->events);
+    cudaFree(ctx->scratch);
+    delete ctx;
+    return SG_OK;
+}
+
+int sg_resize(sg_context *ctx, uint32_t width, uint32_t height) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (width == ctx->width && height == ctx->height) return SG_OK;
+    if ((uint64_t)width * height > (1ull << 31)) return fail(ctx, SG_ERR_INVALID, "viewport too large");
+    DeviceGuard guard(ctx->device);
+    cudaDeviceSynchronize();
+    free_image(ctx);
+    ctx->width = width;
+    ctx->height = height;
+    int status = alloc_image(ctx);
+    if (status != SG_OK) return status;
+    reset_history(ctx);
+    ctx->exposure_idle_frames = 0;
+    return SG_OK;
+}
+
+int sg_prepare_frame(sg_context *ctx, const sg_frame *frame, int *fresh) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    int status = validate_frame(ctx, frame);
+    if (status != SG_OK) return status;
+    update_history(ctx, frame);
+    if (fresh) *fresh = ctx->history.samples == 0;
+    return SG_OK;
+}
+
+int sg_set_quality(sg_context *ctx, uint32_t samples, uint32_t bounces, uint32_t limit) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    bounces = std::clamp<uint32_t>(bounces, 1u, 64u);
+    if (ctx->options.max_bounces != bounces) {
+        reset_history(ctx);
+        ctx->exposure_idle_frames = 0;
+    }
+    ctx->options.samples_per_frame = std::clamp<uint32_t>(samples, 1u, 64u);
+    ctx->options.max_bounces = bounces;
+    ctx->options.sample_limit = std::clamp<uint32_t>(limit, 1u, SG_MAX_SAMPLES);
+    return SG_OK;
+}
+
+int sg_set_options(sg_context *ctx, const sg_options *options) {
+    if (!ctx || !options) return fail(ctx, SG_ERR_INVALID, "ctx or options is NULL");
+    ctx->options = *options;
+    return SG_OK;
+}
+
+int sg_get_options(const sg_context *ctx, sg_options *options) {
+    if (!ctx || !options) return SG_ERR_INVALID;
+    *options = ctx->options;
+    return SG_OK;
+}
+
+static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr, uint64_t *events) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    int status = validate_frame(ctx, frame);
+    if (status != SG_OK) return status;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    update_history(ctx, frame);
+    // Avoid counter wrap and loss of integer resolution in f32 weights
+    // (src/pathtracer.rs:802-811).
+    const uint32_t remaining =
+        ctx->options.sample_limit > ctx->history.samples ? ctx->options.sample_limit - ctx->history.samples : 0u;
+    const uint32_t count = std::min({ctx->options.samples_per_frame, (uint32_t)SG_MAX_BATCH_SAMPLES, remaining});
+    if (events) std::memset(events, 0, SG_EVENT_COUNT * sizeof(uint64_t));
+    if (count > 0 && ctx->width > 0 && ctx->height > 0) {
+        DeviceGuard guard(ctx->device);
+        const sg_settings s = pack_settings(ctx, frame, count);
+        status = upload_bodies(ctx, frame, stream);
+        if (status != SG_OK) return status;
+        sg::TraceParams p = make_params(ctx, s);
+        if (events) {
+            SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
+            p.events = ctx->events;
+        }
+        cudaError_t e = sg::launch_trace(p, events != nullptr, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
+        ctx->launches += 1;
+        if (events) {
+            unsigned long long host[sg::kEventCount];
+            SG_CUDA(ctx, cudaMemcpyAsync(host, ctx->events, sizeof(host), cudaMemcpyDeviceToHost, stream));
+            SG_CUDA(ctx, cudaStreamSynchronize(stream));
+            for (int k = 0; k < sg::kEventCount; ++k) events[k] = host[k];
+        }
+    }
+    ctx->history.samples += count;
+    ctx->history.sequence += count;
+    ctx->exposure_idle_frames = count > 0 ? 0u : (ctx->exposure_idle_frames == UINT32_MAX ? UINT32_MAX : ctx->exposure_idle_frames + 1u);
+    return SG_OK;
+}
+
+int sg_encode(sg_context *ctx, const sg_frame *frame, void *stream_ptr) {
+    return encode_impl(ctx, frame, stream_ptr, nullptr);
+}
+
+int sg_encode_counted(sg_context *ctx, const sg_frame *frame, void *stream_ptr, uint64_t *events) {
+    if (!events) return fail(ctx, SG_ERR_INVALID, "events is NULL");
+    return encode_impl(ctx, frame, stream_ptr, events);
+}
+
+int sg_measure_fp32_peak(int device, double *flops_per_second) {
+    if (!flops_per_second) return fail(nullptr, SG_ERR_INVALID, "flops_per_second is NULL");
+    DeviceGuard guard(device);
+    int sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaDeviceGetAttribute");
+    float *out = nullptr;
+    if ((e = cudaMalloc(&out, sizeof(float))) != cudaSuccess) return cuda_fail(nullptr, e, "cudaMalloc");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, iters = 4096;
+    double best = 0.0;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+        cudaEventRecord(a, nullptr);
+        e = sg::launch_fma_peak(blocks, iters, out, nullptr);
+        cudaEventRecord(b, nullptr);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+        const double flops = 2.0 * 128.0 * iters * 256.0 * blocks;
+        if (rep > 0 && ms > 0.0f) best = std::max(best, flops / (ms * 1e-3));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "fma peak kernel");
+    *flops_per_second = best;
+    return SG_OK;
+}
+
+int sg_get_samples(const sg_context *ctx, uint32_t *samples, uint32_t *sequence) {
+    if (!ctx) return SG_ERR_INVALID;
+    if (samples) *samples = ctx->history.samples;
+    if (sequence) *sequence = ctx->history.sequence;
+    return SG_OK;
+}
+
+int sg_needs_redraw(const sg_context *ctx, int *redraw) {
+    if (!ctx || !redraw) return SG_ERR_INVALID;
+    *redraw = ctx->history.samples < ctx->options.sample_limit ||
+              (ctx->options.auto_exposure && ctx->exposure_idle_frames < 60u);
+    return SG_OK;
+}
+
+int sg_get_size(const sg_context *ctx, uint32_t *width, uint32_t *height) {
+    if (!ctx) return SG_ERR_INVALID;
+    if (width) *width = ctx->width;
+    if (height) *height = ctx->height;
+    return SG_OK;
+}
+
+static int read_image(sg_context *ctx, const float4 *src, float *dst, int on_device, void *stream_ptr) {
+    if (!ctx || !dst) return fail(ctx, SG_ERR_INVALID, "ctx or dst is NULL");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t bytes = (size_t)ctx->width * ctx->height * sizeof(float4);
+    if (bytes == 0) return SG_OK;
+    SG_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                 stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    return SG_OK;
+}
+
+int sg_read_accumulation(sg_context *ctx, float *dst, int dst_on_device, void *stream) {
+    return read_image(ctx, ctx ? ctx->mean : nullptr, dst, dst_on_device, stream);
+}
+
+int sg_read_backdrop(sg_context *ctx, float *dst, int dst_on_device, void *stream) {
+    return read_image(ctx, ctx ? ctx->backdrop : nullptr, dst, dst_on_device, stream);
+}
+
+int sg_set_accumulation(sg_context *ctx, const float *src, int src_on_device, uint32_t samples,
+                        uint32_t sequence, void *stream_ptr) {
+    if (!ctx || !src) return fail(ctx, SG_ERR_INVALID, "ctx or src is NULL");
+    if (samples > SG_MAX_SAMPLES) return fail(ctx, SG_ERR_INVALID, "samples exceed the f32 weight limit");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t n = (size_t)ctx->width * ctx->height;
+    if (n == 0) return SG_OK;
+    std::vector<float> host(n * 4);
+    if (src_on_device) {
+        SG_CUDA(ctx, cudaMemcpyAsync(host.data(), src, n * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    } else {
+        std::memcpy(host.data(), src, n * sizeof(float4));
+    }
+    // The compensated sum restarts from mean * samples.
+    std::vector<float> sums(n * 4);
+    for (size_t k = 0; k < n * 4; ++k) sums[k] = host[k] * (float)samples;
+    SG_CUDA(ctx, cudaMemcpyAsync(ctx->mean, host.data(), n * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    SG_CUDA(ctx, cudaMemcpyAsync(ctx->sum, sums.data(), n * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    SG_CUDA(ctx, cudaMemsetAsync(ctx->comp, 0, n * sizeof(float4), stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    ctx->history.samples = samples;
+    ctx->history.sequence = sequence;
+    return SG_OK;
+}
+
+int sg_accumulation_device_ptr(sg_context *ctx, void **ptr) {
+    if (!ctx || !ptr) return SG_ERR_INVALID;
+    *ptr = ctx->mean;
+    return SG_OK;
+}
+
+int sg_upload_ring_profile(sg_context *ctx, uint32_t slot, const float *tau, uint32_t bins) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (slot >= SG_RING_TABLE_SLOTS) return fail(ctx, SG_ERR_INVALID, "ring-table slot out of range");
+    if (bins > SG_RING_TABLE_MAX_BINS) return fail(ctx, SG_ERR_CAPACITY, "too many ring-table bins");
+    if (bins > 0 && !tau) return fail(ctx, SG_ERR_INVALID, "tau is NULL");
+    for (uint32_t k = 0; k < bins; ++k)
+        if (!(tau[k] >= 0.0f) || !std::isfinite(tau[k]))
+            return fail(ctx, SG_ERR_INVALID, "ring optical depths must be finite and non-negative");
+    DeviceGuard guard(ctx->device);
+    if (bins)
+        SG_CUDA(ctx, cudaMemcpy(ctx->ring_tables + (size_t)slot * SG_RING_TABLE_MAX_BINS, tau, bins * sizeof(float),
+                                cudaMemcpyHostToDevice));
+    ctx->ring_bins[slot] = bins;
+    ctx->table_version += 1;
+    return SG_OK;
+}
+
+// Shared set-up of the probe entry points: settings as encode would pack
+// them (without touching the history), bodies uploaded.
+static int probe_setup(sg_context *ctx, const sg_frame *frame, cudaStream_t stream, sg::TraceParams *p) {
+    int status = validate_frame(ctx, frame);
+    if (status != SG_OK) return status;
+    const sg_settings s = pack_settings(ctx, frame, 0);
+    status = upload_bodies(ctx, frame, stream);
+    if (status != SG_OK) return status;
+    *p = make_params(ctx, s);
+    return SG_OK;
+}
+
+int sg_closest_hit(sg_context *ctx, const sg_frame *frame, const sg_ray *rays, uint32_t n, sg_hit *hits,
+                   int on_device, void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (n && (!rays || !hits)) return fail(ctx, SG_ERR_INVALID, "rays or hits is NULL");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    sg::TraceParams p;
+    int status = probe_setup(ctx, frame, stream, &p);
+    if (status != SG_OK || n == 0) return status;
+    const sg_ray *d_rays = rays;
+    sg_hit *d_hits = hits;
+    if (!on_device) {
+        status = ensure_scratch(ctx, (size_t)n * (sizeof(sg_ray) + sizeof(sg_hit)) + 256);
+        if (status != SG_OK) return status;
+        d_rays = static_cast<const sg_ray *>(ctx->scratch);
+        d_hits = reinterpret_cast<sg_hit *>(static_cast<char *>(ctx->scratch) + (((size_t)n * sizeof(sg_ray) + 255) & ~size_t(255)));
+        SG_CUDA(ctx, cudaMemcpyAsync((void *)d_rays, rays, n * sizeof(sg_ray), cudaMemcpyHostToDevice, stream));
+    }
+    cudaError_t e = sg::launch_closest_hit(p, d_rays, d_hits, n, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "closest_hit launch");
+    if (!on_device) SG_CUDA(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(sg_hit), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    return SG_OK;
+}
+
+int sg_light_visibility(sg_context *ctx, const sg_frame *frame, const sg_ray *rays, const uint32_t *lights,
+                        uint32_t n, float *out, int on_device, void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (n && (!rays || !lights || !out)) return fail(ctx, SG_ERR_INVALID, "rays, lights or out is NULL");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    sg::TraceParams p;
+    int status = probe_setup(ctx, frame, stream, &p);
+    if (status != SG_OK || n == 0) return status;
+    const sg_ray *d_rays = rays;
+    const uint32_t *d_lights = lights;
+    float *d_out = out;
+    if (!on_device) {
+        const size_t ray_bytes = ((size_t)n * sizeof(sg_ray) + 255) & ~size_t(255);
+        const size_t light_bytes = ((size_t)n * sizeof(uint32_t) + 255) & ~size_t(255);
+        status = ensure_scratch(ctx, ray_bytes + light_bytes + (size_t)n * sizeof(float));
+        if (status != SG_OK) return status;
+        char *base = static_cast<char *>(ctx->scratch);
+        d_rays = reinterpret_cast<const sg_ray *>(base);
+        d_lights = reinterpret_cast<const uint32_t *>(base + ray_bytes);
+        d_out = reinterpret_cast<float *>(base + ray_bytes + light_bytes);
+        SG_CUDA(ctx, cudaMemcpyAsync((void *)d_rays, rays, n * sizeof(sg_ray), cudaMemcpyHostToDevice, stream));
+        SG_CUDA(ctx, cudaMemcpyAsync((void *)d_lights, lights, n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    }
+    cudaError_t e = sg::launch_light_visibility(p, d_rays, d_lights, d_out, n, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "light_visibility launch");
+    if (!on_device) SG_CUDA(ctx, cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    return SG_OK;
+}
+
+int sg_ring_probe(sg_context *ctx, const sg_frame *frame, const sg_ray *rays, uint32_t body, uint32_t n, float *out,
+                  int on_device, void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (n && (!rays || !out)) return fail(ctx, SG_ERR_INVALID, "rays or out is NULL");
+    if (frame && body >= frame->n_bodies) return fail(ctx, SG_ERR_INVALID, "body index out of range");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    sg::TraceParams p;
+    int status = probe_setup(ctx, frame, stream, &p);
+    if (status != SG_OK || n == 0) return status;
+    const sg_ray *d_rays = rays;
+    float *d_out = out;
+    if (!on_device) {
+        const size_t ray_bytes = ((size_t)n * sizeof(sg_ray) + 255) & ~size_t(255);
+        status = ensure_scratch(ctx, ray_bytes + (size_t)n * sizeof(float4));
+        if (status != SG_OK) return status;
+        char *base = static_cast<char *>(ctx->scratch);
+        d_rays = reinterpret_cast<const sg_ray *>(base);
+        d_out = reinterpret_cast<float *>(base + ray_bytes);
+        SG_CUDA(ctx, cudaMemcpyAsync((void *)d_rays, rays, n * sizeof(sg_ray), cudaMemcpyHostToDevice, stream));
+    }
+    cudaError_t e = sg::launch_ring_probe(p, d_rays, body, d_out, n, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ring_probe launch");
+    if (!on_device) SG_CUDA(ctx, cudaMemcpyAsync(out, d_out, n * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    return SG_OK;
+}
+
+int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu, uint32_t steps, float *energy) {
+    if (!ctx || !energy) return fail(ctx, SG_ERR_INVALID, "ctx or energy is NULL");
+    if (!(mu > 0.0f) || steps == 0) return fail(ctx, SG_ERR_INVALID, "mu must be positive and steps non-zero");
+    DeviceGuard guard(ctx->device);
+    int status = ensure_scratch(ctx, sizeof(float));
+    if (status != SG_OK) return status;
+    float *d = static_cast<float *>(ctx->scratch);
+    cudaError_t e = sg::launch_ring_energy(albedo, tau, mu, steps, d, nullptr);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ring_energy launch");
+    SG_CUDA(ctx, cudaMemcpy(energy, d, sizeof(float), cudaMemcpyDeviceToHost));
+    return SG_OK;
+}
+
+const char *sg_last_error(const sg_context *ctx) {
+    if (ctx) return ctx->last_error.c_str();
+    return g_last_error.c_str();
+}
+
+const char *sg_status_string(int status) {
+    switch (status) {
+        case SG_OK: return "ok";
+        case SG_ERR_INVALID: return "invalid argument";
+        case SG_ERR_CAPACITY: return "capacity exceeded";
+        case SG_ERR_CUDA: return "CUDA error";
+        case SG_ERR_OOM: return "out of device memory";
+        case SG_ERR_STATE: return "invalid state";
+        case SG_ERR_TIMEOUT: return "device loop gave up";
+        default: return "unknown status";
+    }
+}
+
+int sg_launch_count(const sg_context *ctx, uint64_t *launches) {
+    if (!ctx || !launches) return SG_ERR_INVALID;
+    *launches = ctx->launches;
+    return SG_OK;
+}
+
+}  // extern "C"

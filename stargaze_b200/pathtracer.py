@@ -1,0 +1,197 @@
+"""Python mirror of stargaze's `PathTracer` host interface (src/pathtracer.rs).
+
+Every method is a thin call into the C-ABI library; the progressive
+rendering state (history key, sample count, noise sequence) lives in the
+native context, exactly where `PathTracer` keeps it in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import StargazeError, check, load
+from .scene import Frame
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(0)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    handle = getattr(stream, "cuda_stream", None)  # torch.cuda.Stream
+    if handle is not None:
+        return C.c_void_p(handle)
+    raise TypeError(f"unsupported stream object {stream!r}")
+
+
+def _ptr(array: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(array.ctypes.data)
+
+
+class PathTracer:
+    """`PathTracer::new(device, format, dimensions, stars, options)`
+    (src/pathtracer.rs:292-302), on CUDA device `device`."""
+
+    def __init__(self, dimensions: tuple[int, int], options: abi.Options | None = None, device: int = 0):
+        self._lib = load()
+        self._ctx = C.c_void_p()
+        opts = options if options is not None else abi.default_options()
+        check(self._lib.sg_create(device, int(dimensions[0]), int(dimensions[1]), C.byref(opts), C.byref(self._ctx)))
+
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.sg_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._ctx
+
+    # -- options ----------------------------------------------------------
+    @property
+    def options(self) -> abi.Options:
+        o = abi.Options()
+        check(self._lib.sg_get_options(self._ctx, C.byref(o)), self._ctx)
+        return o
+
+    @options.setter
+    def options(self, value: abi.Options) -> None:
+        check(self._lib.sg_set_options(self._ctx, C.byref(value)), self._ctx)
+
+    def update_options(self, **fields) -> None:
+        o = self.options
+        for k, v in fields.items():
+            setattr(o, k, v)
+        self.options = o
+
+    # -- PathTracer API ---------------------------------------------------
+    def resize(self, dimensions: tuple[int, int]) -> None:
+        check(self._lib.sg_resize(self._ctx, int(dimensions[0]), int(dimensions[1])), self._ctx)
+
+    def samples(self) -> int:
+        s = C.c_uint32()
+        check(self._lib.sg_get_samples(self._ctx, C.byref(s), None), self._ctx)
+        return s.value
+
+    def sequence(self) -> int:
+        s = C.c_uint32()
+        check(self._lib.sg_get_samples(self._ctx, None, C.byref(s)), self._ctx)
+        return s.value
+
+    def size(self) -> tuple[int, int]:
+        w, h = C.c_uint32(), C.c_uint32()
+        check(self._lib.sg_get_size(self._ctx, C.byref(w), C.byref(h)), self._ctx)
+        return w.value, h.value
+
+    def needs_redraw(self) -> bool:
+        r = C.c_int()
+        check(self._lib.sg_needs_redraw(self._ctx, C.byref(r)), self._ctx)
+        return bool(r.value)
+
+    def prepare_frame(self, frame: Frame) -> bool:
+        fresh = C.c_int()
+        view = frame.view()
+        check(self._lib.sg_prepare_frame(self._ctx, C.byref(view), C.byref(fresh)), self._ctx)
+        return bool(fresh.value)
+
+    def set_quality(self, samples: int, bounces: int, limit: int) -> None:
+        check(self._lib.sg_set_quality(self._ctx, samples, bounces, limit), self._ctx)
+
+    def encode(self, frame: Frame, stream=None) -> None:
+        view = frame.view()
+        check(self._lib.sg_encode(self._ctx, C.byref(view), _stream_handle(stream)), self._ctx)
+
+    def upload_ring_profile(self, slot: int, tau) -> None:
+        t = np.ascontiguousarray(tau, dtype=np.float32)
+        check(self._lib.sg_upload_ring_profile(self._ctx, slot, _ptr(t), t.size), self._ctx)
+
+    def read_pixels(self, stream=None) -> np.ndarray:
+        """The accumulation as a (height*width, 4) float32 array."""
+        w, h = self.size()
+        out = np.zeros((w * h, 4), dtype=np.float32)
+        check(self._lib.sg_read_accumulation(self._ctx, _ptr(out), 0, _stream_handle(stream)), self._ctx)
+        return out
+
+    def read_backdrop(self, stream=None) -> np.ndarray:
+        w, h = self.size()
+        out = np.zeros((w * h, 4), dtype=np.float32)
+        check(self._lib.sg_read_backdrop(self._ctx, _ptr(out), 0, _stream_handle(stream)), self._ctx)
+        return out
+
+    def set_accumulation(self, pixels: np.ndarray, samples: int, sequence: int) -> None:
+        p = np.ascontiguousarray(pixels, dtype=np.float32)
+        check(self._lib.sg_set_accumulation(self._ctx, _ptr(p), 0, samples, sequence, None), self._ctx)
+
+    def accumulation_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self._lib.sg_accumulation_device_ptr(self._ctx, C.byref(p)), self._ctx)
+        return int(p.value or 0)
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        check(self._lib.sg_launch_count(self._ctx, C.byref(n)), self._ctx)
+        return n.value
+
+    # -- probes -----------------------------------------------------------
+    def closest_hit(self, frame: Frame, rays: np.ndarray) -> np.ndarray:
+        """rays: structured array of abi.Ray records (see rays_array)."""
+        rays = np.ascontiguousarray(rays)
+        hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+        view = frame.view()
+        check(self._lib.sg_closest_hit(self._ctx, C.byref(view), _ptr(rays), len(rays), _ptr(hits), 0, None), self._ctx)
+        return hits
+
+    def light_visibility(self, frame: Frame, rays: np.ndarray, lights) -> np.ndarray:
+        rays = np.ascontiguousarray(rays)
+        lights = np.ascontiguousarray(lights, dtype=np.uint32)
+        out = np.zeros(len(rays), dtype=np.float32)
+        view = frame.view()
+        check(self._lib.sg_light_visibility(self._ctx, C.byref(view), _ptr(rays), _ptr(lights), len(rays), _ptr(out),
+                                            0, None), self._ctx)
+        return out
+
+    def ring_probe(self, frame: Frame, rays: np.ndarray, body: int) -> np.ndarray:
+        rays = np.ascontiguousarray(rays)
+        out = np.zeros((len(rays), 4), dtype=np.float32)
+        view = frame.view()
+        check(self._lib.sg_ring_probe(self._ctx, C.byref(view), _ptr(rays), body, len(rays), _ptr(out), 0, None),
+              self._ctx)
+        return out
+
+    def ring_energy(self, albedo: float, tau: float, mu: float, steps: int = 4096) -> float:
+        e = C.c_float()
+        check(self._lib.sg_ring_energy(self._ctx, albedo, tau, mu, steps, C.byref(e)), self._ctx)
+        return e.value
+
+
+RAY_DTYPE = np.dtype([("offset", "<f4", 3), ("direction", "<f4", 3), ("anchor", "<u4")])
+HIT_DTYPE = np.dtype([("distance", "<f4"), ("index", "<u4"), ("normal", "<f4", 3)])
+assert RAY_DTYPE.itemsize == C.sizeof(abi.Ray) and HIT_DTYPE.itemsize == C.sizeof(abi.Hit)
+
+
+def rays_array(offsets, directions, anchors) -> np.ndarray:
+    offsets = np.asarray(offsets, dtype=np.float32).reshape(-1, 3)
+    directions = np.asarray(directions, dtype=np.float32).reshape(-1, 3)
+    anchors = np.broadcast_to(np.asarray(anchors, dtype=np.uint32), (len(directions),))
+    rays = np.zeros(len(directions), dtype=RAY_DTYPE)
+    rays["offset"] = np.broadcast_to(offsets, (len(directions), 3))
+    rays["direction"] = directions
+    rays["anchor"] = anchors
+    return rays
+
+
+__all__ = ["PathTracer", "StargazeError", "RAY_DTYPE", "HIT_DTYPE", "rays_array"]

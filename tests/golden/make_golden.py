@@ -1,0 +1,133 @@
+"""Generate the golden fixtures under tests/golden/ with the CPU oracle.
+
+    python tests/golden/make_golden.py
+
+The oracle is itself pinned against the reference's known-answer tests
+(tests/test_oracle_known_answers.py); these fixtures freeze its outputs on
+seeded inputs so the CUDA library (tests/test_cuda_parity.py) and any later
+oracle change (tests/test_golden.py) are checked against the same numbers
+on a machine where the oracle is not rebuilt.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+from oracle.binding import OracleTracer  # noqa: E402
+from rays import light_targets, seeded_rays  # noqa: E402
+import known_answers as ka  # noqa: E402
+from stargaze_b200 import abi  # noqa: E402
+from stargaze_b200.pathtracer import rays_array  # noqa: E402
+from stargaze_b200.scene import body, frame  # noqa: E402
+from stargaze_b200.workloads import rings_1080p, spheres_256  # noqa: E402
+
+N_RAYS = 2048
+
+
+def transport_scene():
+    f = frame()
+    f.bodies = [
+        body([0.0, 0.0, -3.0], 1.0, [0.8] * 3, False),
+        body([0.0, 4.0, 2.0], 0.8, [10.0] * 3, True),
+        body([0.0, 2.0, 0.0], 0.5, [0.0] * 3, False),
+        body([2.0, 0.0, -1.0], 1.0, [0.9] * 3, False),
+    ]
+    return f, {}
+
+
+def scenes():
+    s = spheres_256()
+    r = rings_1080p()
+    return {
+        "transport": transport_scene(),
+        "spheres_256": (s.frame, s.ring_tables),
+        "rings_1080p": (r.frame, r.ring_tables),
+        "shadow_ring": (ka.shadow_ring_scene(), {}),
+    }
+
+
+def visibility_rays(f, rays, seed):
+    """Re-aim each ray at a jittered point of a target body's disc."""
+    rng = np.random.default_rng(seed + 7)
+    lights = light_targets(f, len(rays), seed)
+    dirs = np.zeros((len(rays), 3), np.float64)
+    for k, (ray, light) in enumerate(zip(rays, lights)):
+        b = f.bodies[light]
+        c = np.array(b.center, np.float64) + np.array(b.center_low[:3], np.float64)
+        if ray["anchor"] != abi.MISS:
+            a = f.bodies[ray["anchor"]]
+            c = c - (np.array(a.center, np.float64) + np.array(a.center_low[:3], np.float64))
+        c = c - ray["offset"].astype(np.float64)
+        jitter = rng.normal(size=3)
+        jitter *= b.radius * rng.uniform(0.0, 1.3) / np.linalg.norm(jitter)
+        d = c + jitter
+        dirs[k] = d / np.linalg.norm(d)
+    out = rays.copy()
+    out["direction"] = dirs.astype(np.float32)
+    return out, lights
+
+
+def make_tracer(f, tables, dims=(1, 1), **opts):
+    t = OracleTracer(dims, ka.test_options(**opts))
+    for slot, tau in tables.items():
+        t.upload_ring_profile(slot, tau)
+    return t
+
+
+def ray_fixtures():
+    out = {}
+    for k, (name, (f, tables)) in enumerate(scenes().items()):
+        rays = seeded_rays(f, N_RAYS, seed=100 + k)
+        t = make_tracer(f, tables)
+        hits = t.closest_hit(f, rays)
+        vrays, lights = visibility_rays(f, rays, seed=200 + k)
+        vis = t.light_visibility(f, vrays, lights)
+        ring_out = np.zeros((len(f.bodies), len(rays), 4), np.float32)
+        for i in range(len(f.bodies)):
+            ring_out[i] = t.ring_probe(f, rays, i)
+        np.savez_compressed(
+            HERE / f"rays_{name}.npz",
+            rays=rays.view(np.uint8).reshape(len(rays), -1),
+            hit_distance=hits["distance"], hit_index=hits["index"], hit_normal=hits["normal"],
+            vis_rays=vrays.view(np.uint8).reshape(len(vrays), -1), vis_lights=lights, visibility=vis,
+            ring=ring_out,
+        )
+        out[name] = (int((hits["index"] != abi.MISS).sum()), int((vis > 0).sum()))
+    return out
+
+
+IMAGES = {
+    # name: (workload factory, width, height, spp, batches)
+    "spheres_64": (spheres_256, 64, 64, 16, 2),
+    "rings_96x54": (rings_1080p, 96, 54, 16, 2),
+}
+
+
+def image_fixture(name):
+    factory, w, h, spp, batches = IMAGES[name]
+    wl = factory(width=w, height=h)
+    t = make_tracer(wl.frame, wl.ring_tables, dims=(w, h), samples_per_frame=spp, max_bounces=wl.max_bounces)
+    for _ in range(batches):
+        t.encode(wl.frame)
+    return t.read_pixels()
+
+
+def image_fixtures():
+    out = {}
+    for name in IMAGES:
+        img = image_fixture(name)
+        np.savez_compressed(HERE / f"image_{name}.npz", image=img)
+        out[name] = float(img[:, :3].mean())
+    return out
+
+
+if __name__ == "__main__":
+    print(ray_fixtures())
+    print(image_fixtures())

@@ -1,0 +1,344 @@
+"""The reference's known-answer tests, written once for any tracer.
+
+Each scenario restates one of stargaze's GPU tests (file:line cited) and
+runs against a `make(dimensions, options)` factory, so the same assertions
+pin the CPU oracle (tests/test_oracle_known_answers.py) and the CUDA library
+(tests/test_cuda_known_answers.py). Where a reference tolerance cannot hold
+for two independent noise sequences, the scenario uses common random numbers
+and says so.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from stargaze_b200 import abi
+from stargaze_b200.pathtracer import rays_array
+from stargaze_b200.scene import body, frame, ringed
+
+
+def test_options(**fields) -> abi.Options:
+    """`test_options()` (src/pathtracer_tests.rs:25-30): no Milky Way."""
+    o = abi.default_options()
+    o.milky_way = 0.0
+    for k, v in fields.items():
+        setattr(o, k, v)
+    return o
+
+
+def sample(tracer, f, batches: int) -> np.ndarray:
+    """`sample()` (src/pathtracer_tests.rs:184-197)."""
+    for _ in range(batches):
+        tracer.encode(f)
+    return tracer.read_pixels()
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:441-600 — gpu_transport
+# ---------------------------------------------------------------------------
+def transport(make) -> dict:
+    tracer = make((1, 1), test_options(samples_per_frame=64, max_bounces=1, exposure=1.0))
+    f = frame()
+    black = sample(tracer, f, 1)[0]
+    assert np.array_equal(black, np.zeros(4, np.float32)), black
+    # An unchanged size preserves the image and the history.
+    tracer.resize((1, 1))
+    assert tracer.samples() == 64
+    assert np.array_equal(tracer.read_pixels()[0], black)
+    sample(tracer, f, 1)
+    assert tracer.samples() == 128
+
+    # Emission, true silhouettes and inside-sphere roots.
+    f.bodies = [body([0.0, 0.0, -1.0], 1e-6, [2.0, 3.0, 4.0], True)]
+    assert np.array_equal(sample(tracer, f, 1)[0], np.array([2, 3, 4, 0], np.float32))
+    f.bodies[0].center[:] = [0.0, 0.0, 0.0]
+    f.bodies[0].radius = 1.0
+    assert np.array_equal(sample(tracer, f, 1)[0], np.array([2, 3, 4, 0], np.float32))
+
+    f.bodies = [body([0.0, 0.0, -3.0], 1.0, [0.8] * 3, False), body([0.0, 4.0, 2.0], 0.8, [10.0] * 3, True)]
+    seq0 = tracer.sequence()
+    full = float(sample(tracer, f, 32)[0][0])
+    expected = 0.8 * 10.0 * 0.8**2 / 32.0 * math.sqrt(0.5)
+    assert abs(full - expected) < expected * 0.03, (full, expected)
+    assert tracer.samples() == 2048
+
+    # An occluder behind the emitter cannot shadow it. The reference compares
+    # two independent noise sequences to 1e-6, tighter than their Monte Carlo
+    # spread (~2e-4 at 2048 spp); with common random numbers the estimates
+    # must be identical.
+    crn = make((1, 1), test_options(samples_per_frame=64, max_bounces=1, noise_seed=seq0))
+    g = f.copy()
+    g.bodies.append(body([0.0, 8.0, 6.0], 1.0, [0.0] * 3, False))
+    behind = float(sample(crn, g, 32)[0][0])
+    assert abs(behind - full) < 1e-6, (behind, full)
+    behind_independent = float(sample(tracer, g, 32)[0][0])
+    assert abs(behind_independent - full) < full * 0.01
+
+    # Aligned occluder covers the stellar disc.
+    f.bodies.append(body([0.0, 2.0, 0.0], 0.5, [0.0] * 3, False))
+    umbra = float(sample(tracer, f, 32)[0][0])
+    assert umbra < full * 0.001, (umbra, full)
+    # Equal angular discs shifted sideways: partial shadow.
+    f.bodies[2].center[0] = 0.4
+    f.bodies[2].radius = 0.4
+    penumbra = float(sample(tracer, f, 32)[0][0])
+    assert full * 0.2 < penumbra < full * 0.85, (penumbra, full)
+    # Small aligned disc: annular eclipse.
+    f.bodies[2].center[0] = 0.0
+    f.bodies[2].radius = 0.2
+    annular = float(sample(tracer, f, 32)[0][0])
+    assert full * 0.6 < annular < full * 0.85, (annular, full)
+    # Multiple emitters add.
+    f.bodies.pop()
+    f.bodies.append(body([0.0, -4.0, 2.0], 0.8, [10.0] * 3, True))
+    binary = float(sample(tracer, f, 32)[0][0])
+    assert abs(binary / full - 2.0) < 0.05, (binary, full)
+    # MIS does not double count emission reached by BSDF paths.
+    tracer.update_options(max_bounces=8)
+    bounced = float(sample(tracer, f, 128)[0][0])
+    assert abs(bounced / binary - 1.0) < 0.05, (bounced, binary)
+    # A white reflector adds indirect light to a directly shadowed point.
+    f.bodies = [
+        body([0.0, 0.0, -3.0], 1.0, [0.8] * 3, False),
+        body([0.0, 4.0, 2.0], 0.8, [10.0] * 3, True),
+        body([0.0, 2.0, 0.0], 0.5, [0.0] * 3, False),
+        body([2.0, 0.0, -1.0], 1.0, [0.9] * 3, False),
+    ]
+    indirect = float(sample(tracer, f, 128)[0][0])
+    assert indirect > 0.0001, indirect
+    tracer.update_options(max_bounces=1)
+    direct_only = float(sample(tracer, f, 32)[0][0])
+    assert direct_only < 1e-6, direct_only
+    # Resizing resets the history and allocates a fresh image.
+    tracer.resize((3, 2))
+    assert tracer.samples() == 0
+    f.globals.viewport[0] = 3.0
+    f.globals.viewport[1] = 2.0
+    assert len(sample(tracer, f, 1)) == 6
+    return dict(full=full, umbra=umbra, penumbra=penumbra, annular=annular, binary=binary,
+                bounced=bounced, indirect=indirect, direct_only=direct_only)
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:604-642 — gpu_distant_surface
+# ---------------------------------------------------------------------------
+def distant_surface(make, size: int = 256) -> dict:
+    tracer = make((size, size), test_options(samples_per_frame=16, max_bounces=1, exposure=1.0))
+    f = frame()
+    f.globals.viewport[:] = [float(size), float(size), 1.0, 0.0]
+    dark_counts = {}
+    for radius in (1e-4, 1e-6, 1e-7):
+        f.globals.cam_forward[3] = radius / 10.0 * 1.3
+        f.bodies = [body([0.0, 0.0, -10.0], radius, [0.8] * 3, False),
+                    body([5.0, 0.0, -5.0], 0.05, [10000.0] * 3, True)]
+        pixels = sample(tracer, f, 4).reshape(size, size, 4)
+        lo, hi = size * 100 // 256, size * 156 // 256
+        dark = int((pixels[lo:hi, lo:hi, 0] < 0.05).sum())
+        dark_counts[radius] = dark
+        assert dark == 0, (radius, dark)
+    return dark_counts
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:201-237 — noise sequence
+# ---------------------------------------------------------------------------
+def noise_sequence(make) -> None:
+    f = frame()
+    f.globals.viewport[:] = [32.0, 32.0, 1.0, 1.0]
+    f.globals.cam_forward[3] = 0.5
+    f.bodies = [body([0.0, 0.0, -3.0], 1.0, [1.0] * 3, True)]
+
+    def new(seed):
+        return make((32, 32), test_options(noise_seed=seed, samples_per_frame=1))
+
+    tracer = new(0)
+    first = sample(tracer, f, 1)
+    f.scene_time = 1.0  # same geometry, fresh accumulation
+    reset = sample(tracer, f, 1)
+    assert tracer.samples() == 1
+    assert not np.array_equal(first, reset)
+    same_seed = new(0)
+    assert np.array_equal(first, sample(same_seed, f, 1))
+    other_seed = new(12345)
+    assert not np.array_equal(first, sample(other_seed, f, 1))
+    tracer.set_quality(1, 4, 10)
+    quality_reset = sample(tracer, f, 1)
+    assert tracer.samples() == 1
+    assert not np.array_equal(first, quality_reset)
+    assert not np.array_equal(reset, quality_reset)
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:241-314 — quality limits, rest and resume
+# ---------------------------------------------------------------------------
+def quality_limits(make) -> None:
+    tracer = make((1, 1), test_options(samples_per_frame=64, max_bounces=1, sample_limit=65, auto_exposure=1))
+    f = frame()
+    f.bodies = [body([0.0, 0.0, -1.0], 0.1, [2.0, 3.0, 4.0], True)]
+    initial = sample(tracer, f, 1)
+    assert tracer.samples() == 64
+    assert tracer.needs_redraw()
+    sample(tracer, f, 1)
+    assert tracer.samples() == 65, "last batch must stop exactly at the limit"
+    assert tracer.needs_redraw(), "exposure still needs to settle"
+    assert np.array_equal(sample(tracer, f, 60), initial)
+    assert tracer.samples() == 65
+    assert not tracer.needs_redraw(), "a completed still view should sleep"
+    tracer.set_quality(8, 1, 32)
+    assert tracer.samples() == 65, "lowering the target preserves the better image"
+    assert not tracer.needs_redraw()
+    sample(tracer, f, 1)
+    assert tracer.samples() == 65, "a lower target must not underflow the counter"
+    tracer.set_quality(8, 1, 256)
+    assert tracer.needs_redraw()
+    sample(tracer, f, 1)
+    assert tracer.samples() == 73, "a higher target resumes the existing average"
+    tracer.set_quality(8, 2, 256)
+    assert tracer.samples() == 0, "changing light transport invalidates the image"
+    sample(tracer, f, 1)
+    assert tracer.samples() == 8
+    tracer.set_quality(8, 2, 8)
+    sample(tracer, f, 60)
+    assert not tracer.needs_redraw()
+    f.scene_time += 1.0
+    sample(tracer, f, 1)
+    assert tracer.samples() == 8
+    assert tracer.needs_redraw(), "a changed scene starts refinement again"
+
+
+# ---------------------------------------------------------------------------
+# src/ring_tests.rs:57-135 — gpu_rings_geometry (probe)
+# ---------------------------------------------------------------------------
+def rings_geometry(make) -> None:
+    tracer = make((1, 1), test_options())
+    f = frame()
+    r = 0.0004
+    f.bodies = [ringed([1.8 * r, 0.0, -10.0], r, [0.0, 0.8, 0.6], 0.7), body([0.0, 0.0, -12.0], 0.1, [1.0] * 3, True)]
+    ray = rays_array([0, 0, 0], [[0.0, 0.0, -1.0]], abi.MISS)
+
+    def probe():
+        p = tracer.ring_probe(f, ray, 0)[0]
+        if p[3] == 0.0:
+            return np.zeros(4, np.float32)
+        vis = tracer.light_visibility(f, ray, [1])[0]
+        return np.array([p[0], p[1], p[2], vis], np.float32)
+
+    p = probe()
+    expected = math.exp(-0.7 / 0.6)
+    assert abs(p[0] - 10.0) < 1e-5 and abs(p[1] - 1.8) < 1e-4, p
+    assert abs(p[2] - expected) < 1e-5 and abs(p[3] - expected) < 1e-5, p
+    for offset, pole in ((0.5, [0.0, 0.0, 1.0]), (2.6, [0.0, 0.0, 1.0]), (1.8, [0.0, 1.0, 0.0])):
+        f.bodies[0] = ringed([offset * r, 0.0, -10.0], r, pole, 0.7)
+        assert np.array_equal(probe(), np.zeros(4, np.float32)), (offset, pole)
+    f.bodies[0] = ringed([1.8 * r, 0.0, -10.0], r, [0.0, 0.0, 1.0], 0.7)
+    f.bodies[1].center[2] = -9.0
+    p = probe()
+    assert abs(p[3] - 1.0) < 1e-6, p
+
+
+# ---------------------------------------------------------------------------
+# src/ring_tests.rs:137-202 — gpu_rings_transport
+# ---------------------------------------------------------------------------
+def rings_transport(make) -> None:
+    tracer = make((1, 1), test_options(samples_per_frame=64, max_bounces=1, exposure=1.0))
+    f = frame()
+    f.bodies = [ringed([1.8, 0.0, -5.0], 1.0, [0.0, 0.0, 1.0], 0.7), body([0.0, 0.0, -9.0], 0.5, [1.0] * 3, True)]
+    f.bodies[0].ring_color[:] = [0.0, 0.0, 0.0, 0.0]
+    for pole, expected in (([0.0, 0.0, 1.0], math.exp(-0.7)), ([0.0, 0.8, 0.6], math.exp(-0.7 / 0.6))):
+        f.bodies[0].ring_plane[0:3] = pole
+        p = sample(tracer, f, 256)[0]
+        assert abs(p[0] - expected) < 0.02, (p, expected)
+    f.bodies[0] = ringed([1.8, 0.0, -5.0], 1.0, [0.0, 0.0, 1.0], 0.7)
+    for star_z, same_side in ((15.0, True), (-25.0, False)):
+        f.bodies[1] = body([10.0, 0.0, star_z], 0.05, [100_000.0] * 3, True)
+        mu = 20.0 / math.sqrt(500.0)
+        if same_side:
+            factor = (1.0 - math.exp(-0.7 * (1.0 + 1.0 / mu))) / (1.0 + mu)
+        else:
+            factor = (math.exp(-0.7 / mu) - math.exp(-0.7)) / (mu - 1.0)
+        solid_angle = 2.0 * math.pi * (0.05**2 / 500.0) / (1.0 + math.sqrt(1.0 - 0.05**2 / 500.0))
+        expected = 0.8 * factor / (4.0 * math.pi) * mu * 100_000.0 * solid_angle
+        p = sample(tracer, f, 32)[0]
+        assert abs(p[0] / expected - 1.0) < 0.02, (p, expected)
+        f.bodies.append(body([5.0, 0.0, (star_z - 5.0) * 0.5], 0.5, [0.0] * 3, False))
+        dark = sample(tracer, f, 8)[0]
+        assert dark[0] < p[0] * 0.001, (dark, p)
+        f.bodies.pop()
+
+
+# ---------------------------------------------------------------------------
+# src/ring_tests.rs:352-413 — gpu_rings_conserve_energy
+# ---------------------------------------------------------------------------
+def rings_conserve_energy(make) -> list:
+    tracer = make((1, 1), test_options())
+    energies = []
+    for albedo in (0.8, 0.88, 1.0):
+        for tau in (0.001, 0.1, 0.7, 2.0):
+            for mu in (0.05, 0.5, 1.0):
+                e = tracer.ring_energy(albedo, tau, mu, 4096)
+                assert 0.0 <= e <= 1.0001, (albedo, tau, mu, e)
+                energies.append(e)
+    return energies
+
+
+# ---------------------------------------------------------------------------
+# src/ring_tests.rs:415-453 — gpu_rings_null_crossings_preserve_mis
+# ---------------------------------------------------------------------------
+def rings_null_crossings_preserve_mis(make, size: int = 64) -> tuple[float, float]:
+    tracer = make((size, size), test_options(samples_per_frame=64, max_bounces=1))
+    f = frame()
+    f.globals.viewport[0] = float(size)
+    f.globals.viewport[1] = float(size)
+    ring = ringed([0.0, 4.0, -2.0], 0.1, [0.0, 0.0, 1.0], 0.4)
+    ring.ring_params[0] = 100.0
+    ring.ring_color[:] = [0.0, 0.0, 0.0, 0.0]
+    f.bodies = [body([0.0, 0.0, -5.0], 1.0, [0.8] * 3, False), body([0.0, 4.0, 2.0], 3.8, [1.0] * 3, True), ring]
+    direct = float(sample(tracer, f, 4)[:, 0].astype(np.float64).mean())
+    tracer.update_options(max_bounces=2)
+    mis = float(sample(tracer, f, 4)[:, 0].astype(np.float64).mean())
+    assert abs(mis / direct - 1.0) < 0.01, (mis, direct)
+    return direct, mis
+
+
+# ---------------------------------------------------------------------------
+# src/ground_tests.rs:1052-1153 — gpu_shadow_queries_match_closest_hits
+# (the ring scene; the surface scene needs the local landscape)
+# ---------------------------------------------------------------------------
+def shadow_ring_scene():
+    f = frame()
+    ring = body([1.8, 0.0, -5.0], 1.0, [0.0] * 3, False)
+    ring.ring_plane[:] = [0.0, 0.8, 0.6, 1.25]
+    ring.ring_params[:] = [2.4, 0.7, 0.0, 0.0]
+    f.bodies = [
+        ring,
+        body([0.0, 0.0, -10.0], 0.5, [1.0] * 3, True),
+        body([0.0, 0.0, -10.0], 0.5, [1.0] * 3, True),  # equal-distance tie
+        body([0.0, 0.0, -20.0], 1.0, [0.5] * 3, False),
+    ]
+    return f
+
+
+def shadow_rays(tracer_like_sample_light, f, width: int = 64, height: int = 16):
+    """Rays of the shadow probe (src/ground_tests.rs:1079-1093): toward a
+    sampled point of light `x % bodies`, or a random direction on rows with
+    bit 2 set. `tracer_like_sample_light(f, ray, light, rng) -> (dir, rng)`."""
+    n_bodies = len(f.bodies)
+    offsets, dirs, lights = [], [], []
+    from oracle.binding import oracle_random  # test infrastructure
+    for y in range(height):
+        for x in range(width):
+            pixel = y * width + x
+            rng = (pixel * 747796405 + 2891336453) & 0xFFFFFFFF
+            light = x % n_bodies
+            d, rng = tracer_like_sample_light(f, light, rng)
+            if y & 4:
+                a, rng = oracle_random(rng)
+                b, rng = oracle_random(rng)
+                c, rng = oracle_random(rng)
+                v = np.array([a, b, c], np.float32) - np.float32(0.5)
+                d = v * (np.float32(1.0) / np.sqrt(np.float32(v @ v)))
+            offsets.append([0.0, 0.0, 0.0])
+            dirs.append(d)
+            lights.append(light)
+    return rays_array(offsets, dirs, abi.MISS), np.array(lights, np.uint32)

@@ -1,0 +1,89 @@
+"""The reference's known-answer tests against the CUDA library (B200)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import known_answers as ka
+from stargaze_b200 import PathTracer, abi
+
+pytestmark = pytest.mark.gpu
+
+
+def make(dimensions, options):
+    return PathTracer(dimensions, options)
+
+
+def test_transport():
+    r = ka.transport(make)
+    assert r["umbra"] < r["penumbra"] < r["annular"] < r["full"]
+
+
+def test_distant_surface():
+    counts = ka.distant_surface(make, size=256)
+    assert all(v == 0 for v in counts.values())
+
+
+def test_noise_sequence():
+    ka.noise_sequence(make)
+
+
+def test_quality_limits_rest_resume():
+    ka.quality_limits(make)
+
+
+def test_rings_geometry():
+    ka.rings_geometry(make)
+
+
+def test_rings_transport():
+    ka.rings_transport(make)
+
+
+def test_rings_conserve_energy():
+    assert len(ka.rings_conserve_energy(make)) == 36
+
+
+def test_rings_null_crossings_preserve_mis():
+    ka.rings_null_crossings_preserve_mis(make, size=64)
+
+
+@pytest.mark.parametrize("stars", range(6))
+def test_shadow_queries_match_closest_hits(stars):
+    """Any-hit visibility == closest-hit reference, bit-equal
+    (src/ground_tests.rs:1052-1153, ring scene)."""
+    from oracle.binding import load as load_oracle
+
+    tracer = PathTracer((64, 16), ka.test_options())
+    f = ka.shadow_ring_scene()
+    for i, b in enumerate(f.bodies):
+        b.emissive = 1.0 if i < stars else 0.0
+    s = f.settings(64, 16, 0, 0, 8, 0)
+    lib = load_oracle()
+
+    def sample_light(frame_, light, rng):
+        st = C.c_uint32(rng)
+        d = np.zeros(3, np.float32)
+        pdf = C.c_float()
+        ray = abi.Ray()
+        ray.anchor = abi.MISS
+        bodies = frame_.bodies_array()
+        lib.oracle_sample_light(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(ray), light, C.byref(st),
+                                C.c_void_p(d.ctypes.data), C.byref(pdf))
+        return d, st.value
+
+    rays, lights = ka.shadow_rays(sample_light, f)
+    vis = tracer.light_visibility(f, rays, lights)
+    hits = tracer.closest_hit(f, rays)
+    ref = np.zeros_like(vis)
+    rings = [tracer.ring_probe(f, rays, i) for i in range(len(f.bodies))]
+    for k in range(len(rays)):
+        if hits["index"][k] != lights[k]:
+            continue
+        t = np.float32(1.0)
+        for i in range(len(f.bodies)):
+            p = rings[i][k]
+            if p[3] != 0.0 and p[0] < hits["distance"][k]:
+                t = np.float32(t * p[2])
+        ref[k] = t
+    assert np.array_equal(vis, ref)

@@ -1,0 +1,118 @@
+"""The reference's known-answer tests against the CPU oracle (no GPU).
+
+These pin the oracle: every assertion is the reference's own
+(src/pathtracer_tests.rs, src/ring_tests.rs, src/ground_tests.rs).
+"""
+import numpy as np
+import pytest
+
+import known_answers as ka
+from oracle.binding import OracleTracer, oracle_hash, oracle_random
+from stargaze_b200 import abi
+
+
+def make(dimensions, options):
+    return OracleTracer(dimensions, options)
+
+
+def test_transport():
+    r = ka.transport(make)
+    assert r["umbra"] < r["penumbra"] < r["annular"] < r["full"]
+
+
+def test_distant_surface():
+    counts = ka.distant_surface(make, size=128)
+    assert all(v == 0 for v in counts.values())
+
+
+def test_noise_sequence():
+    ka.noise_sequence(make)
+
+
+def test_quality_limits_rest_resume():
+    ka.quality_limits(make)
+
+
+def test_rings_geometry():
+    ka.rings_geometry(make)
+
+
+def test_rings_transport():
+    ka.rings_transport(make)
+
+
+def test_rings_conserve_energy():
+    energies = ka.rings_conserve_energy(make)
+    assert len(energies) == 36
+
+
+def test_rings_null_crossings_preserve_mis():
+    ka.rings_null_crossings_preserve_mis(make, size=32)
+
+
+@pytest.mark.parametrize("stars", range(6))
+def test_shadow_queries_match_closest_hits(stars):
+    tracer = OracleTracer((64, 16), ka.test_options())
+    f = ka.shadow_ring_scene()
+    for i, b in enumerate(f.bodies):
+        b.emissive = 1.0 if i < stars else 0.0
+    s = f.settings(64, 16, 0, 0, 8, 0)
+
+    def sample_light(frame_, light, rng):
+        import ctypes as C
+        from oracle.binding import load
+        lib = load()
+        st = C.c_uint32(rng)
+        d = np.zeros(3, np.float32)
+        pdf = C.c_float()
+        ray = abi.Ray()
+        ray.anchor = abi.MISS
+        bodies = frame_.bodies_array()
+        lib.oracle_sample_light(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(ray), light, C.byref(st),
+                                C.c_void_p(d.ctypes.data), C.byref(pdf))
+        return d, st.value
+
+    rays, lights = ka.shadow_rays(sample_light, f)
+    vis = tracer.light_visibility(f, rays, lights)
+    ref = tracer.reference_visibility(f, rays, lights)
+    assert np.array_equal(vis, ref)
+    # Compact light list == full scan (src/ground_tests.rs:1094-1103).
+    compact = 0
+    count = s.lights[3] if s.lights[3] <= 3 else s.counts[0]
+    for slot in range(count):
+        i = s.lights[slot] if s.lights[3] <= 3 else slot
+        if f.bodies[i].emissive >= 0.5:
+            compact = (compact * 31 + i + 1) & 0xFFFFFFFF
+    reference = 0
+    for i, b in enumerate(f.bodies):
+        if b.emissive >= 0.5:
+            reference = (reference * 31 + i + 1) & 0xFFFFFFFF
+    assert compact == reference
+
+
+def _hash_np(x: int) -> int:
+    """Independent restatement of hash() (pathtrace.wgsl:87-92)."""
+    m = 0xFFFFFFFF
+    x &= m
+    x = ((x ^ (x >> 16)) * 0x7FEB352D) & m
+    x = ((x ^ (x >> 15)) * 0x846CA68B) & m
+    return x ^ (x >> 16)
+
+
+def _random_np(state: int):
+    m = 0xFFFFFFFF
+    state = (state * 747796405 + 2891336453) & m
+    word = (((state >> ((state >> 28) + 4)) ^ state) * 277803737) & m
+    return float(np.float32(((word >> 22) ^ word) >> 8) * np.float32(1.0 / 16777216.0)), state
+
+
+@pytest.mark.parametrize("seed", [0, 1, 0x9E3779B9, 0xFFFFFFFF, 123456789])
+def test_rng_matches_wgsl(seed):
+    assert oracle_hash(seed) == _hash_np(seed)
+    state = _hash_np(seed)
+    ostate = state
+    for _ in range(16):
+        a, state = _random_np(state)
+        b, ostate = oracle_random(ostate)
+        assert a == b and state == ostate
+        assert 0.0 <= a < 1.0
