@@ -16,12 +16,23 @@
 //     expressions. Shading arithmetic is free to use FMA.
 //   * Closest-hit loops track only (distance, index, root offset); the
 //     surface normal is formed once for the winning body.
+//   * Instruction footprint: the light-sampling, shadow-ray, slab-BSDF,
+//     ringshine and point-disc helpers are out of line so their several call
+//     sites share one copy (divergent warps otherwise stall on instruction
+//     fetch). They take and return values only — nothing whose address
+//     escapes — so calls cost no local memory.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "../../include/stargaze_b200.h"
+
+// Call attribute of the multi-site helpers (sample_light, light_visibility,
+// ring_bsdf, ringshine, point_disc_hit): out of line by default.
+#ifndef SG_HELPER
+#define SG_HELPER __noinline__
+#endif
 
 namespace sg {
 
@@ -65,6 +76,7 @@ __device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
 __device__ __forceinline__ float luminance(float3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
 __device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+__device__ __forceinline__ float max3(float3 v) { return fmaxf(v.x, fmaxf(v.y, v.z)); }
 __device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
     float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
     return t * t * (3.0f - 2.0f * t);
@@ -93,6 +105,10 @@ __device__ __forceinline__ float3 div_rn(float3 a, float s) {
 }
 __device__ __forceinline__ float length_rn(float3 a) { return __fsqrt_rn(dot_rn(a, a)); }
 
+// sin and cos of 2*pi*u for u in [0, 1): sincospif needs no Payne-Hanek
+// range reduction, so the code stays small and branch-free.
+__device__ __forceinline__ void sincos_turn(float u, float *s, float *c) { sincospif(2.0f * u, s, c); }
+
 // ---------------------------------------------------------------------------
 // RNG (pathtrace.wgsl:87-98): PCG-style LCG step with a 24-bit output.
 // ---------------------------------------------------------------------------
@@ -102,12 +118,28 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
     return x ^ (x >> 16);
 }
 
-// Event counters for the algorithmic-work model (compiled out unless the
-// counting kernel variant is instantiated).
+// Event counters for the algorithmic-work model.
 struct Events {
     uint32_t vertices, sphere_tests, sphere_hits, ring_tests, light_samples, shadow_rays,
         ring_events, surface_events, rng_draws;
 };
+
+// Counting is compiled out of the production variant (C == false).
+template <bool C>
+struct Counter {
+    Events *ev;
+    __device__ __forceinline__ void add(uint32_t Events::*f) const {
+        if constexpr (C) ev->*f += 1u;
+    }
+};
+
+template <bool C>
+__device__ __forceinline__ float rnd(Counter<C> K, uint32_t &state) {
+    K.add(&Events::rng_draws);
+    state = state * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
+    return (float)(((word >> 22) ^ word) >> 8) * (1.0f / 16777216.0f);
+}
 
 // ---------------------------------------------------------------------------
 // Scene view inside a CTA
@@ -120,15 +152,6 @@ struct Scene {
     uint32_t table_stride;  // floats between slots
 };
 
-template <bool COUNT>
-struct Ctx {
-    Scene sc;
-    Events ev;
-    __device__ __forceinline__ void count(uint32_t Events::*f) {
-        if constexpr (COUNT) ev.*f += 1u;
-    }
-};
-
 struct Ray {
     float3 o;  // offset from bodies[anchor] centre, or camera origin for kMiss
     float3 d;
@@ -138,22 +161,14 @@ struct Ray {
 __device__ __forceinline__ float4 bf(const Scene &S, uint32_t i, int f) { return S.B[i * kBodyVec4 + f]; }
 __device__ __forceinline__ float b_radius(const Scene &S, uint32_t i) { return S.B[i * kBodyVec4 + kCenter].w; }
 
-template <bool C>
-__device__ __forceinline__ float rnd(Ctx<C> &X, uint32_t &state) {
-    X.count(&Events::rng_draws);
-    state = state * 747796405u + 2891336453u;
-    uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
-    return (float)(((word >> 22) ^ word) >> 8) * (1.0f / 16777216.0f);
-}
-
 // relative_center (pathtrace.wgsl:100-113), strict.
 __device__ __forceinline__ float3 relative_center(const Scene &S, const Ray &r, uint32_t i) {
     if (r.anchor == i) return -r.o;
-    float3 ci = xyz(bf(S, i, kCenter));
-    float3 li = xyz(bf(S, i, kLow));
+    const float3 ci = xyz(bf(S, i, kCenter));
+    const float3 li = xyz(bf(S, i, kLow));
     if (r.anchor == kMiss) return add_rn(ci, sub_rn(li, r.o));
-    float3 ca = xyz(bf(S, r.anchor, kCenter));
-    float3 la = xyz(bf(S, r.anchor, kLow));
+    const float3 ca = xyz(bf(S, r.anchor, kCenter));
+    const float3 la = xyz(bf(S, r.anchor, kLow));
     return add_rn(sub_rn(ci, ca), sub_rn(sub_rn(li, la), r.o));
 }
 
@@ -161,10 +176,10 @@ __device__ __forceinline__ float3 relative_center(const Scene &S, const Ray &r, 
 // hit distance (1e30 on a miss) and the signed root offset `delta` that the
 // normal needs.
 template <bool C>
-__device__ __forceinline__ float sphere_distance(Ctx<C> &X, const Ray &r, uint32_t i, float radius,
-                                                 float &delta) {
-    X.count(&Events::sphere_tests);
-    const float3 oc = relative_center(X.sc, r, i);
+__device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C> K, const Ray &r, uint32_t i,
+                                                 float radius, float &delta) {
+    K.add(&Events::sphere_tests);
+    const float3 oc = relative_center(S, r, i);
     const float a = dot_rn(r.d, r.d);
     const float b = dot_rn(oc, r.d);
     const float3 pc = cross_rn(oc, r.d);
@@ -174,16 +189,17 @@ __device__ __forceinline__ float sphere_distance(Ctx<C> &X, const Ray &r, uint32
     const float q = __fadd_rn(b, b >= 0.0f ? root : -root);
     if (q == 0.0f) return 1.0e30f;
     const float c = __fsub_rn(dot_rn(oc, oc), __fmul_rn(radius, radius));
-    const float cq = __fdiv_rn(c, q);
-    const float qa = __fdiv_rn(q, a);
-    float distance = b < 0.0f ? qa : cq;
-    delta = __fdiv_rn(-root, a);
+    // The far root is divided out only when the near one is behind the
+    // origin; the values are those of the WGSL's c/q and q/a.
+    float distance = b < 0.0f ? __fdiv_rn(q, a) : __fdiv_rn(c, q);
+    float signed_root = -root;
     if (distance <= 0.0f) {
-        distance = b < 0.0f ? cq : qa;
-        delta = __fdiv_rn(root, a);
+        distance = b < 0.0f ? __fdiv_rn(c, q) : __fdiv_rn(q, a);
+        signed_root = root;
     }
     if (distance <= 0.0f) return 1.0e30f;
-    X.count(&Events::sphere_hits);
+    delta = __fdiv_rn(signed_root, a);
+    K.add(&Events::sphere_hits);
     return distance;
 }
 
@@ -205,14 +221,14 @@ struct Hit {
 // closest_hit (pathtrace.wgsl:173-185). The local landscape is disabled in
 // the frames this build accepts (ground_north.w == 0).
 template <bool C>
-__device__ __forceinline__ Hit closest_hit(Ctx<C> &X, const Ray &r) {
+__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C> K, const Ray &r) {
     Hit best{1.0e30f, kMiss, 0.0f};
-    const uint32_t n = X.sc.s->counts[0];
-    const float host = X.sc.s->g.ground_north[3];
+    const uint32_t n = S.s->counts[0];
+    const float host = S.s->g.ground_north[3];
     for (uint32_t i = 0; i < n; ++i) {
         if (host == (float)(i + 1u)) continue;
         float delta;
-        const float t = sphere_distance(X, r, i, b_radius(X.sc, i), delta);
+        const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
         if (t < best.t) best = Hit{t, i, delta};
     }
     return best;
@@ -241,24 +257,26 @@ __device__ __forceinline__ uint32_t light_index(const sg_settings *s, uint32_t s
 struct LightSample {
     float3 d;
     float pdf;
+    uint32_t rng;  // the state after the two draws
 };
 
 // sample_light (pathtrace.wgsl:214-234), one stratum: uniform cone sampling.
 template <bool C>
-__device__ __forceinline__ LightSample sample_light(Ctx<C> &X, const Ray &r, uint32_t i, uint32_t &rng) {
-    X.count(&Events::light_samples);
-    const float3 oc = relative_center(X.sc, r, i);
+__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C> K, Ray r, uint32_t i, uint32_t rng) {
+    K.add(&Events::light_samples);
+    const float3 oc = relative_center(S, r, i);
     const float3 axis = normalize(oc);
-    const float width = cone_width_oc(oc, b_radius(X.sc, i));
-    const float radial = rnd(X, rng);
-    const float azimuth = rnd(X, rng);
+    const float width = cone_width_oc(oc, b_radius(S, i));
+    const float radial = rnd(K, rng);
+    const float azimuth = rnd(K, rng);
     const float one_minus_cos = radial * width;
     const float sin_theta = sqrtf(one_minus_cos * (2.0f - one_minus_cos));
     float sp, cp;
-    sincosf(kTau * azimuth, &sp, &cp);
+    sincos_turn(azimuth, &sp, &cp);
     LightSample ls;
     ls.d = basis_direction(axis, sin_theta * cp, sin_theta * sp, 1.0f - one_minus_cos);
     ls.pdf = 1.0f / (kTau * width);
+    ls.rng = rng;
     return ls;
 }
 
@@ -284,34 +302,34 @@ __device__ __forceinline__ bool has_ring(const Scene &S, uint32_t i) {
 
 // ring_hit (rings.wgsl:8-34), strict.
 template <bool C>
-__device__ __forceinline__ RingHit ring_hit(Ctx<C> &X, const Ray &r, uint32_t i) {
-    RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
-    const float4 plane = bf(X.sc, i, kRingPlane);
-    const float4 params = bf(X.sc, i, kRingParams);
+__device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C> K, const Ray &r, uint32_t i) {
+    const RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
+    const float4 plane = bf(S, i, kRingPlane);
+    const float4 params = bf(S, i, kRingParams);
     if (params.x <= plane.w || params.y <= 0.0f) return miss;
-    X.count(&Events::ring_tests);
+    K.add(&Events::ring_tests);
     const float3 n = xyz(plane);
     const float denom = dot_rn(r.d, n);
     if (fabsf(denom) < 1.0e-7f) return miss;
-    const float3 oc = relative_center(X.sc, r, i);
+    const float3 oc = relative_center(S, r, i);
     const float a = dot_rn(r.d, r.d);
     const float3 perpendicular = div_rn(cross_rn(r.d, cross_rn(r.d, oc)), a);
     const float along = __fdiv_rn(-dot_rn(perpendicular, n), denom);
     const float distance = __fadd_rn(__fdiv_rn(dot_rn(oc, r.d), a), along);
     if (distance <= 0.0f) return miss;
     const float3 point = add_rn(perpendicular, mul_rn(r.d, along));
-    const float radius = __fdiv_rn(length_rn(point), b_radius(X.sc, i));
+    const float radius = __fdiv_rn(length_rn(point), b_radius(S, i));
     if (radius < plane.w || radius > params.x) return miss;
     return RingHit{distance, i, point};
 }
 
 // closest_ring (rings.wgsl:36-45).
 template <bool C>
-__device__ __forceinline__ RingHit closest_ring(Ctx<C> &X, const Ray &r, float limit) {
+__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C> K, const Ray &r, float limit) {
     RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
-    const uint32_t n = X.sc.s->counts[0];
+    const uint32_t n = S.s->counts[0];
     for (uint32_t i = 0; i < n; ++i) {
-        const RingHit h = ring_hit(X, r, i);
+        const RingHit h = ring_hit(S, K, r, i);
         if (h.index != kMiss && h.t < best.t) best = h;
     }
     return best;
@@ -322,52 +340,67 @@ struct Optics {
     float tau;
 };
 
+// The illustrative banded profile of rings.wgsl:56-79 (C/B/A rings,
+// Cassini division, Encke and Keeler gaps). Out of line: its accurate sinf
+// calls carry a large range-reduction path that the table and scalar
+// profiles never need.
+__device__ __noinline__ Optics banded_optics(float x, float tau, float3 color) {
+    const float broad = 0.5f + 0.5f * sinf(43.0f * x + 1.8f * sinf(17.0f * x));
+    const float fine = 0.5f + 0.5f * sinf(1900.0f * x + 2.0f * sinf(311.0f * x));
+    const float micro = 0.5f + 0.5f * sinf(6100.0f * x);
+    float density = 0.12f;
+    float3 tint = f3(0.70f, 0.68f, 0.65f);
+    if (x >= 0.2792f && x < 0.6910f) {
+        density = 1.25f + 1.1f * broad;
+        tint = f3(1.0f, 1.0f, 1.0f);
+    } else if (x >= 0.6910f && x < 0.7649f) {
+        density = 0.025f;
+        tint = f3(0.75f, 0.75f, 0.75f);
+    } else if (x >= 0.7649f) {
+        density = 0.48f + 0.22f * broad;
+        tint = f3(0.92f, 0.94f, 0.98f);
+    }
+    density *= 0.65f + 0.45f * fine + 0.12f * micro;
+    if (fabsf(x - 0.9487f) < 0.00262f || fabsf(x - 0.99565f) < 0.00034f) density = 0.0f;
+    return Optics{color * tint * (0.94f + 0.06f * broad), tau * density};
+}
+
+// Normalised ring radius x of a planet-local point (rings.wgsl:52-53).
+__device__ __forceinline__ float ring_x(const Scene &S, uint32_t i, float3 point) {
+    const float inner = bf(S, i, kRingPlane).w;
+    const float outer = bf(S, i, kRingParams).x;
+    const float radius = __fdiv_rn(length_rn(point), b_radius(S, i));
+    return __fdiv_rn(__fsub_rn(radius, inner), __fsub_rn(outer, inner));
+}
+
+// Table bin of x for a ring-table slot (extension).
+__device__ __forceinline__ uint32_t ring_bin(float x, uint32_t bins) {
+    const float fb = x * (float)bins;
+    const uint32_t bin = fb <= 0.0f ? 0u : (uint32_t)fb;
+    return bin > bins - 1u ? bins - 1u : bin;
+}
+
 // ring_optics (rings.wgsl:50-81) plus the tabulated profile extension.
 __device__ __forceinline__ Optics ring_optics(const Scene &S, uint32_t i, float3 point) {
-    const float4 plane = bf(S, i, kRingPlane);
     const float4 params = bf(S, i, kRingParams);
-    const float radius = __fdiv_rn(length_rn(point), b_radius(S, i));
-    const float x = __fdiv_rn(__fsub_rn(radius, plane.w), __fsub_rn(params.x, plane.w));
-    float tau = params.y;
-    float3 color = xyz(bf(S, i, kRingColor));
+    const float x = ring_x(S, i, point);
+    const float tau = params.y;
+    const float3 color = xyz(bf(S, i, kRingColor));
     if (params.w >= 0.5f) {
         const uint32_t slot = (uint32_t)params.w - 1u;
         const uint32_t bins = slot < SG_RING_TABLE_SLOTS ? S.bins[slot] : 0u;
-        if (bins > 0u) {
-            const float fb = x * (float)bins;
-            uint32_t bin = fb <= 0.0f ? 0u : (uint32_t)fb;
-            bin = bin > bins - 1u ? bins - 1u : bin;
-            tau *= S.tables[slot * S.table_stride + bin];
-        } else {
-            tau = 0.0f;
-        }
-    } else if (params.z > 0.5f) {
-        const float broad = 0.5f + 0.5f * sinf(43.0f * x + 1.8f * sinf(17.0f * x));
-        const float fine = 0.5f + 0.5f * sinf(1900.0f * x + 2.0f * sinf(311.0f * x));
-        const float micro = 0.5f + 0.5f * sinf(6100.0f * x);
-        float density = 0.12f;
-        float3 tint = f3(0.70f, 0.68f, 0.65f);
-        if (x >= 0.2792f && x < 0.6910f) {
-            density = 1.25f + 1.1f * broad;
-            tint = f3(1.0f, 1.0f, 1.0f);
-        } else if (x >= 0.6910f && x < 0.7649f) {
-            density = 0.025f;
-            tint = f3(0.75f, 0.75f, 0.75f);
-        } else if (x >= 0.7649f) {
-            density = 0.48f + 0.22f * broad;
-            tint = f3(0.92f, 0.94f, 0.98f);
-        }
-        density *= 0.65f + 0.45f * fine + 0.12f * micro;
-        if (fabsf(x - 0.9487f) < 0.00262f || fabsf(x - 0.99565f) < 0.00034f) density = 0.0f;
-        tau *= density;
-        color = color * tint * (0.94f + 0.06f * broad);
+        if (bins == 0u) return Optics{color, 0.0f};
+        return Optics{color, tau * S.tables[slot * S.table_stride + ring_bin(x, bins)]};
     }
+    if (params.z > 0.5f) return banded_optics(x, tau, color);
     return Optics{color, tau};
 }
 
+// exp(-tau / |mu|); mu uses the strict dot so the optical path tau/|mu|
+// rounds exactly as in an IEEE evaluation of the WGSL.
 __device__ __forceinline__ float ring_transmission_tau(float3 d, float3 pole, float tau) {
-    const float mu = fmaxf(fabsf(dot(d, pole)), 1.0e-7f);
-    return expf(-tau / mu);
+    const float mu = fmaxf(fabsf(dot_rn(d, pole)), 1.0e-7f);
+    return expf(__fdiv_rn(-tau, mu));
 }
 
 // ring_transmission (rings.wgsl:83-86).
@@ -379,24 +412,23 @@ __device__ __forceinline__ float ring_transmission(const Scene &S, const Ray &r,
 // the other spheres (ties broken by index), then ring transmissions before
 // the light.
 template <bool C>
-__device__ __forceinline__ float light_visibility(Ctx<C> &X, const Ray &r, uint32_t light) {
-    X.count(&Events::shadow_rays);
+__device__ SG_HELPER float light_visibility(Scene S, Counter<C> K, Ray r, uint32_t light) {
+    K.add(&Events::shadow_rays);
     float delta;
-    const float surface = sphere_distance(X, r, light, b_radius(X.sc, light), delta);
+    const float surface = sphere_distance(S, K, r, light, b_radius(S, light), delta);
     if (surface >= 1.0e30f) return 0.0f;
-    const sg_settings *s = X.sc.s;
-    const float host = s->g.ground_north[3];
-    const uint32_t n = s->counts[0];
-    if (host == (float)(light + 1u) && closest_hit(X, r).index != light) return 0.0f;
+    const float host = S.s->g.ground_north[3];
+    const uint32_t n = S.s->counts[0];
+    if (host == (float)(light + 1u) && closest_hit(S, K, r).index != light) return 0.0f;
     for (uint32_t i = 0; i < n; ++i) {
         if (i == light || host == (float)(i + 1u)) continue;
-        const float t = sphere_distance(X, r, i, b_radius(X.sc, i), delta);
+        const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
         if (t < 1.0e30f && (t < surface || (t == surface && i < light))) return 0.0f;
     }
     float transmission = 1.0f;
     for (uint32_t i = 0; i < n; ++i) {
-        const RingHit h = ring_hit(X, r, i);
-        if (h.index != kMiss && h.t < surface) transmission *= ring_transmission(X.sc, r, h);
+        const RingHit h = ring_hit(S, K, r, i);
+        if (h.index != kMiss && h.t < surface) transmission *= ring_transmission(S, r, h);
     }
     return transmission;
 }
@@ -407,7 +439,7 @@ __device__ __forceinline__ float one_minus_exp(float x) {
 }
 
 // ring_bsdf (rings.wgsl:151-166): exact single scattering in a finite slab.
-__device__ __forceinline__ float3 ring_bsdf(const Optics &o, float outgoing, float incoming) {
+__device__ SG_HELPER float3 ring_bsdf(Optics o, float outgoing, float incoming) {
     const float mo = fmaxf(fabsf(outgoing), 1.0e-7f);
     const float mi = fmaxf(fabsf(incoming), 1.0e-7f);
     const float a = o.tau / mo;
@@ -440,18 +472,23 @@ __device__ __forceinline__ float ring_area(const Scene &S, uint32_t i) {
     return kPi * r * r * (outer * outer - inner * inner);
 }
 
+struct Shine {
+    float3 radiance;
+    uint32_t rng;
+};
+
 // ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
 template <bool C>
-__device__ float3 ringshine(Ctx<C> &X, uint32_t index, float3 origin, float3 normal, bool last_vertex,
-                            uint32_t &rng) {
-    const Scene &S = X.sc;
-    if (!has_ring(S, index)) return f3(0.0f, 0.0f, 0.0f);
+__device__ SG_HELPER Shine ringshine(Scene S, Counter<C> K, uint32_t index, float3 origin, float3 normal,
+                                        bool last_vertex, uint32_t rng) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    if (!has_ring(S, index)) return Shine{zero, rng};
     const float3 n = xyz(bf(S, index, kRingPlane));
     const float inner = bf(S, index, kRingPlane).w;
     const float outer = bf(S, index, kRingParams).x;
-    const float radius = sqrtf(mixf(inner * inner, outer * outer, rnd(X, rng))) * b_radius(S, index);
+    const float radius = sqrtf(mixf(inner * inner, outer * outer, rnd(K, rng))) * b_radius(S, index);
     float sp, cp;
-    sincosf(kTau * rnd(X, rng), &sp, &cp);
+    sincos_turn(rnd(K, rng), &sp, &cp);
     const float3 point = basis_direction(n, cp, sp, 0.0f) * radius;
     const float3 offset = point - origin;
     const float distance2 = dot(offset, offset);
@@ -459,27 +496,28 @@ __device__ float3 ringshine(Ctx<C> &X, uint32_t index, float3 origin, float3 nor
     const float3 direction = offset / distance;
     const float cos_surface = dot(normal, direction);
     const float cos_ring = fabsf(dot(direction, n));
-    if (cos_surface <= 0.0f || cos_ring < 1.0e-6f) return f3(0.0f, 0.0f, 0.0f);
+    if (cos_surface <= 0.0f || cos_ring < 1.0e-6f) return Shine{zero, rng};
     float delta;
-    const float blocker = sphere_distance(X, Ray{origin, direction, index}, index, b_radius(S, index), delta);
-    if (blocker < distance) return f3(0.0f, 0.0f, 0.0f);
+    const float blocker = sphere_distance(S, K, Ray{origin, direction, index}, index, b_radius(S, index), delta);
+    if (blocker < distance) return Shine{zero, rng};
     const Optics optics = ring_optics(S, index, point);
-    if (optics.tau == 0.0f) return f3(0.0f, 0.0f, 0.0f);
+    if (optics.tau == 0.0f) return Shine{zero, rng};
     const float mu_out = dot(-direction, n);
-    float3 shine = f3(0.0f, 0.0f, 0.0f);
+    float3 shine = zero;
     const uint32_t count = light_count(S.s);
     for (uint32_t slot = 0; slot < count; ++slot) {
         const uint32_t i = light_index(S.s, slot);
-        if (bf(S, i, kMaterial).w < 0.5f) continue;
-        const LightSample light = sample_light(X, Ray{point, n, index}, i, rng);
+        const float4 material = bf(S, i, kMaterial);
+        if (material.w < 0.5f) continue;
+        const LightSample light = sample_light(S, K, Ray{point, n, index}, i, rng);
+        rng = light.rng;
         const float mu_in = dot(light.d, n);
-        const float visibility = light_visibility(X, ring_origin(S, index, point, light.d), i);
-        shine = shine + ring_bsdf(optics, mu_out, mu_in) * xyz(bf(S, i, kMaterial)) *
-                            (fabsf(mu_in) * visibility / light.pdf);
+        const float visibility = light_visibility(S, K, ring_origin(S, index, point, light.d), i);
+        shine = shine + ring_bsdf(optics, mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * visibility / light.pdf);
     }
     const float pdf = distance2 / (ring_area(S, index) * cos_ring);
     const float weight = last_vertex ? 1.0f : power_weight(pdf, cos_surface / kPi);
-    return shine * (cos_surface * weight / (kPi * pdf));
+    return Shine{shine * (cos_surface * weight / (kPi * pdf)), rng};
 }
 
 // point_gain (pathtrace.wgsl:1341-1345).
@@ -487,6 +525,40 @@ __device__ __forceinline__ float point_gain(const sg_settings *s, float extent, 
     const float pixel = 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);
     const float pixels = 2.0f * extent / fmaxf(distance, 1.0e-30f) / pixel;
     return mixf(s->background[3], 1.0f, smoothstepf(1.0f, 3.0f, pixels));
+}
+
+struct DiscHit {
+    Hit hit;
+    float scale;
+    uint32_t rng;
+};
+
+// point_disc_hit (pathtrace.wgsl:1308-1333): depth-0 camera rays see an
+// unresolved body as a disc of at least a bright star's size.
+template <bool C>
+__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C> K, Ray r, Hit closest, uint32_t rng) {
+    const sg_settings *s = S.s;
+    DiscHit out{closest, 1.0f, rng};
+    float total = 0.0f;
+    const float pixel = 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);
+    const float angle = clampf(kPointDiscRadius, 0.7f * pixel, kStarDotPixels * pixel);
+    const uint32_t host = (uint32_t)s->g.atmo_params[3] - 1u;
+    const uint32_t n = s->counts[0];
+    for (uint32_t i = 0; i < n; ++i) {
+        if (i == host || s->g.ground_north[3] == (float)(i + 1u)) continue;
+        const float radius = b_radius(S, i);
+        const float drawn = __fmul_rn(angle, length_rn(relative_center(S, r, i)));
+        if (radius <= 0.0f || drawn <= radius) continue;
+        float delta;
+        const float t = sphere_distance(S, K, r, i, drawn, delta);
+        if (t < closest.t) {
+            const float ratio = (radius / drawn) * (radius / drawn);
+            total += ratio;
+            if (rnd(K, out.rng) * total < ratio) out.hit = Hit{t, i, delta};
+        }
+    }
+    if (total > 0.0f) out.scale = total;
+    return out;
 }
 
 // ---------------------------------------------------------------------------
@@ -500,7 +572,7 @@ __device__ __forceinline__ float hash31(float3 p) {
     q = f3(q.x + d, q.y + d, q.z + d);
     return fractf((q.x + q.y) * q.z);
 }
-__device__ float vnoise(float3 p) {
+__device__ __forceinline__ float vnoise(float3 p) {
     const float3 i = f3(floorf(p.x), floorf(p.y), floorf(p.z));
     const float3 f = p - i;
     const float3 u = f3(f.x * f.x * (3.0f - 2.0f * f.x), f.y * f.y * (3.0f - 2.0f * f.y),
@@ -511,30 +583,31 @@ __device__ float vnoise(float3 p) {
     const float d = mixf(hash31(i + f3(0, 1, 1)), hash31(i + f3(1, 1, 1)), u.x);
     return mixf(mixf(a, b, u.y), mixf(c, d, u.y), u.z);
 }
+
+// Mottle factor of surface_albedo (pathtrace.wgsl:912-923), out of line:
+// five octaves of value noise that the constant-albedo path never runs.
+__device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float strength, float3 normal) {
+    const float3 y = xyz(axis_y);
+    const float3 local = f3(dot(normal, axis_x), dot(normal, y), dot(normal, cross(axis_x, y)));
+    const float seed = axis_y.w;
+    const float3 off =
+        f3(hash31(f3(seed, 1.0f, 7.0f)), hash31(f3(3.0f, seed, 5.0f)), hash31(f3(9.0f, 2.0f, seed))) * 512.0f;
+    float3 p = local * 2.4f + off;
+    float amplitude = 0.5f, noise = 0.0f;
+    for (int octave = 0; octave < 5; ++octave) {
+        noise += amplitude * vnoise(p);
+        p = p * 2.07f;
+        amplitude *= 0.5f;
+    }
+    return mixf(1.0f, 0.68f + 0.64f * noise, strength);
+}
+
 __device__ __forceinline__ float3 surface_albedo(const Scene &S, uint32_t i, float3 normal) {
     const float4 material = bf(S, i, kMaterial);
-    const float mottle_strength = bf(S, i, kLow).w;
-    float mottle = 1.0f;
-    if (mottle_strength > 0.0f) {
-        const float3 x = xyz(bf(S, i, kAxisX));
-        const float4 ay = bf(S, i, kAxisY);
-        const float3 y = xyz(ay);
-        const float3 local = f3(dot(normal, x), dot(normal, y), dot(normal, cross(x, y)));
-        const float seed = ay.w;
-        const float3 off =
-            f3(hash31(f3(seed, 1.0f, 7.0f)), hash31(f3(3.0f, seed, 5.0f)), hash31(f3(9.0f, 2.0f, seed))) *
-            512.0f;
-        float3 p = local * 2.4f + off;
-        float amplitude = 0.5f, noise = 0.0f;
-        for (int octave = 0; octave < 5; ++octave) {
-            noise += amplitude * vnoise(p);
-            p = p * 2.07f;
-            amplitude *= 0.5f;
-        }
-        mottle = mixf(1.0f, 0.68f + 0.64f * noise, mottle_strength);
-    }
-    return f3(clampf(material.x * mottle, 0.0f, 1.0f), clampf(material.y * mottle, 0.0f, 1.0f),
-              clampf(material.z * mottle, 0.0f, 1.0f));
+    const float strength = bf(S, i, kLow).w;
+    const float m = strength > 0.0f ? mottle(xyz(bf(S, i, kAxisX)), bf(S, i, kAxisY), strength, normal) : 1.0f;
+    return f3(clampf(material.x * m, 0.0f, 1.0f), clampf(material.y * m, 0.0f, 1.0f),
+              clampf(material.z * m, 0.0f, 1.0f));
 }
 
 }  // namespace sg

@@ -239,6 +239,17 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     return p;
 }
 
+// Options the integrator can run: the reference clamps bounces to 1..64
+// (src/pathtracer.rs:114-122, :761-773); zero bounces would leave the path
+// loop to Russian roulette alone.
+int validate_options(sg_context *ctx, const sg_options *o) {
+    if (o->max_bounces < 1u || o->max_bounces > 64u)
+        return fail(ctx, SG_ERR_INVALID, "max_bounces must be in 1..64");
+    if (!std::isfinite(o->milky_way) || o->milky_way < 0.0f)
+        return fail(ctx, SG_ERR_INVALID, "milky_way must be finite and non-negative");
+    return SG_OK;
+}
+
 int ensure_scratch(sg_context *ctx, size_t bytes) {
     if (ctx->scratch_bytes >= bytes) return SG_OK;
     cudaFree(ctx->scratch);
@@ -276,6 +287,7 @@ int sg_create(int device, uint32_t width, uint32_t height, const sg_options *opt
     if (e != cudaSuccess) return fail(nullptr, SG_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
     if (device < 0 || device >= count) return fail(nullptr, SG_ERR_INVALID, "no such CUDA device");
     if ((uint64_t)width * height > (1ull << 31)) return fail(nullptr, SG_ERR_INVALID, "viewport too large");
+    if (options && validate_options(nullptr, options) != SG_OK) return SG_ERR_INVALID;
     sg_context *ctx = new (std::nothrow) sg_context();
     if (!ctx) return fail(nullptr, SG_ERR_OOM, "host allocation failed");
     ctx->device = device;
@@ -356,6 +368,8 @@ int sg_set_quality(sg_context *ctx, uint32_t samples, uint32_t bounces, uint32_t
 
 int sg_set_options(sg_context *ctx, const sg_options *options) {
     if (!ctx || !options) return fail(ctx, SG_ERR_INVALID, "ctx or options is NULL");
+    int status = validate_options(ctx, options);
+    if (status != SG_OK) return status;
     ctx->options = *options;
     return SG_OK;
 }
@@ -633,7 +647,8 @@ int sg_ring_probe(sg_context *ctx, const sg_frame *frame, const sg_ray *rays, ui
 
 int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu, uint32_t steps, float *energy) {
     if (!ctx || !energy) return fail(ctx, SG_ERR_INVALID, "ctx or energy is NULL");
-    if (!(mu > 0.0f) || steps == 0) return fail(ctx, SG_ERR_INVALID, "mu must be positive and steps non-zero");
+    if (!(mu > 0.0f) || steps == 0 || steps > (1u << 20))
+        return fail(ctx, SG_ERR_INVALID, "mu must be positive and steps in 1..2^20");
     DeviceGuard guard(ctx->device);
     int status = ensure_scratch(ctx, sizeof(float));
     if (status != SG_OK) return status;

@@ -15,39 +15,9 @@ namespace {
 constexpr int kTile = 16;
 constexpr int kThreads = 256;
 
-template <bool C>
-__device__ Hit point_disc_hit(Ctx<C> &X, const Ray &r, Hit closest, float &scale, uint32_t &rng) {
-    // point_disc_hit (pathtrace.wgsl:1308-1333).
-    const sg_settings *s = X.sc.s;
-    Hit result = closest;
-    float total = 0.0f;
-    const float pixel = 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);
-    const float angle = clampf(kPointDiscRadius, 0.7f * pixel, kStarDotPixels * pixel);
-    const uint32_t host = (uint32_t)s->g.atmo_params[3] - 1u;
-    const uint32_t n = s->counts[0];
-    for (uint32_t i = 0; i < n; ++i) {
-        if (i == host || s->g.ground_north[3] == (float)(i + 1u)) continue;
-        const float radius = b_radius(X.sc, i);
-        const float drawn = __fmul_rn(angle, length_rn(relative_center(X.sc, r, i)));
-        if (radius <= 0.0f || drawn <= radius) continue;
-        float delta;
-        const float t = sphere_distance(X, r, i, drawn, delta);
-        if (t < closest.t) {
-            const float ratio = (radius / drawn) * (radius / drawn);
-            total += ratio;
-            if (rnd(X, rng) * total < ratio) result = Hit{t, i, delta};
-        }
-    }
-    if (total > 0.0f) scale = total;
-    return result;
-}
-
-__device__ __forceinline__ float max3(float3 v) { return fmaxf(v.x, fmaxf(v.y, v.z)); }
-
 // trace (pathtrace.wgsl:1347-1617), airless, landscape off.
 template <bool C>
-__device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
-    const Scene &S = X.sc;
+__device__ float4 trace(const Scene &S, Counter<C> K, Ray ray, uint32_t &rng) {
     const sg_settings *s = S.s;
     float3 throughput = f3(1.0f, 1.0f, 1.0f);
     float3 radiance = f3(0.0f, 0.0f, 0.0f);
@@ -62,17 +32,27 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
     const uint32_t n_bodies = s->counts[0];
     const float gain = s->background[3];
     const uint32_t n_lights = light_count(s);
+    // Static bound: each of at most max_vertices vertices is preceded by at
+    // most n_bodies + 1 null crossings, so valid inputs never reach it.
+    const uint32_t max_iterations = max_vertices * (n_bodies + 2u) + 1u;
+    uint32_t iterations = 0;
 
     for (;;) {
-        X.count(&Events::vertices);
-        Hit hit = closest_hit(X, ray);
+        if (++iterations > max_iterations) break;
+        K.add(&Events::vertices);
+        Hit hit = closest_hit(S, K, ray);
         float disc_scale = 1.0f;
-        if (depth == 0u && null_crossings == 0u && gain > 0.0f) hit = point_disc_hit(X, ray, hit, disc_scale, rng);
-        const RingHit ring = closest_ring(X, ray, hit.t);
+        if (depth == 0u && null_crossings == 0u && gain > 0.0f) {
+            const DiscHit disc = point_disc_hit(S, K, ray, hit, rng);
+            hit = disc.hit;
+            disc_scale = disc.scale;
+            rng = disc.rng;
+        }
+        const RingHit ring = closest_ring(S, K, ray, hit.t);
 
         if (ring.index != kMiss) {
             // Ring event (pathtrace.wgsl:1415-1493).
-            X.count(&Events::ring_events);
+            K.add(&Events::ring_events);
             const uint32_t ri = ring.index;
             if (depth == 0u && !point_gained && gain > 0.0f) {
                 point_gained = true;
@@ -97,9 +77,10 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
                 const uint32_t i = light_index(s, slot);
                 const float4 material = bf(S, i, kMaterial);
                 if (material.w < 0.5f || optics.tau == 0.0f) continue;
-                const LightSample light = sample_light(X, Ray{ring.p, n, ri}, i, rng);
+                const LightSample light = sample_light(S, K, Ray{ring.p, n, ri}, i, rng);
+                rng = light.rng;
                 const float mu_in = dot(light.d, n);
-                const float visibility = light_visibility(X, ring_origin(S, ri, ring.p, light.d), i);
+                const float visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
                 const float weight = last_vertex ? 1.0f : power_weight(light.pdf, bsdf_pdf);
                 const float3 lit = throughput * ring_bsdf(optics, mu_out, mu_in) * xyz(material) *
                                    (fabsf(mu_in) / light.pdf);
@@ -108,7 +89,7 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
                 unshadowed += l;
                 direct += l * visibility;
             }
-            if (rnd(X, rng) < transmission) {
+            if (rnd(K, rng) < transmission) {
                 // Null event: no depth consumed, MIS stays with the last vertex.
                 ray = ring_origin(S, ri, ring.p, ray.d);
                 null_crossings += 1u;
@@ -120,9 +101,9 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
                 ring_cap = fmaxf(direct, kRingIndirectCap * unshadowed);
                 ring_base = radiance;
             }
-            const float z = 1.0f - 2.0f * rnd(X, rng);
+            const float z = 1.0f - 2.0f * rnd(K, rng);
             float sp, cp;
-            sincosf(kTau * rnd(X, rng), &sp, &cp);
+            sincos_turn(rnd(K, rng), &sp, &cp);
             const float radial = sqrtf(fmaxf(0.0f, 1.0f - z * z));
             const float3 direction = basis_direction(n, radial * cp, radial * sp, z);
             throughput = throughput * ring_bsdf(optics, mu_out, z) * (fabsf(z) / bsdf_pdf);
@@ -133,7 +114,7 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
             null_crossings = 0u;
             if (depth >= 3u) {
                 const float survival = clampf(max3(throughput), 0.05f, 0.95f);
-                if (rnd(X, rng) >= survival) break;
+                if (rnd(K, rng) >= survival) break;
                 throughput = throughput / survival;
             }
             continue;
@@ -156,7 +137,7 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
             radiance = radiance + throughput * xyz(material) * weight;
             break;
         }
-        X.count(&Events::surface_events);
+        K.add(&Events::surface_events);
         const float radius = b_radius(S, bi);
         if (depth == 0u && !point_gained && gain > 0.0f) {
             point_gained = true;
@@ -171,11 +152,12 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
             const uint32_t i = light_index(s, slot);
             const float4 light_material = bf(S, i, kMaterial);
             if (light_material.w < 0.5f) continue;
-            const LightSample sample = sample_light(X, outgoing, i, rng);
+            const LightSample sample = sample_light(S, K, outgoing, i, rng);
+            rng = sample.rng;
             const float cosine = fmaxf(dot(normal, sample.d), 0.0f);
             if (cosine <= 0.0f) continue;
             outgoing.d = sample.d;
-            const float visibility = light_visibility(X, outgoing, i);
+            const float visibility = light_visibility(S, K, outgoing, i);
             if (visibility > 0.0f) {
                 const float bsdf_pdf = cosine / kPi;
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
@@ -184,12 +166,16 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
         }
         const float3 albedo = surface_albedo(S, bi, normal);
         radiance = radiance + throughput * albedo * direct_light;
-        radiance = radiance + throughput * albedo * ringshine(X, bi, outgoing.o, normal, last_vertex, rng);
+        if (has_ring(S, bi)) {
+            const Shine shine = ringshine(S, K, bi, outgoing.o, normal, last_vertex, rng);
+            rng = shine.rng;
+            radiance = radiance + throughput * albedo * shine.radiance;
+        }
         shine_body = bi;
         if (last_vertex) break;
-        const float u = rnd(X, rng);
+        const float u = rnd(K, rng);
         float sp, cp;
-        sincosf(kTau * rnd(X, rng), &sp, &cp);
+        sincos_turn(rnd(K, rng), &sp, &cp);
         const float cosine = sqrtf(1.0f - u);
         const float su = sqrtf(u);
         outgoing.d = basis_direction(normal, su * cp, su * sp, cosine);
@@ -197,7 +183,7 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
         throughput = throughput * albedo;
         if (depth >= 2u) {
             const float survival = clampf(max3(throughput), 0.05f, 0.95f);
-            if (rnd(X, rng) >= survival) break;
+            if (rnd(K, rng) >= survival) break;
             throughput = throughput / survival;
         }
         ray = outgoing;
@@ -216,10 +202,10 @@ __device__ float4 trace(Ctx<C> &X, Ray ray, uint32_t &rng) {
 
 // camera_direction (pathtrace.wgsl:1619-1626).
 template <bool C>
-__device__ __forceinline__ float3 camera_direction(Ctx<C> &X, uint32_t x, uint32_t y, uint32_t &rng) {
-    const sg_settings *s = X.sc.s;
-    const float jx = rnd(X, rng);
-    const float jy = rnd(X, rng);
+__device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter<C> K, uint32_t x, uint32_t y,
+                                                   uint32_t &rng) {
+    const float jx = rnd(K, rng);
+    const float jy = rnd(K, rng);
     const float u = ((float)x + jx) / s->g.viewport[0];
     const float v = ((float)y + jy) / s->g.viewport[1];
     const float tangent = s->g.cam_forward[3];
@@ -242,40 +228,36 @@ __device__ __forceinline__ Scene stage_scene(const TraceParams &P, float4 *smem)
     return sc;
 }
 
-template <bool C>
-__device__ __forceinline__ void flush_events(Ctx<C> &X, unsigned long long *events) {
-    if constexpr (C) {
-        uint32_t v[kEventCount] = {X.ev.vertices,    X.ev.sphere_tests, X.ev.sphere_hits,
-                                   X.ev.ring_tests,  X.ev.light_samples, X.ev.shadow_rays,
-                                   X.ev.ring_events, X.ev.surface_events, X.ev.rng_draws};
+__device__ __forceinline__ void flush_events(const Events &ev, unsigned long long *events) {
+    const uint32_t v[kEventCount] = {ev.vertices,    ev.sphere_tests,  ev.sphere_hits,
+                                     ev.ring_tests,  ev.light_samples, ev.shadow_rays,
+                                     ev.ring_events, ev.surface_events, ev.rng_draws};
 #pragma unroll
-        for (int k = 0; k < kEventCount; ++k) {
-            unsigned long long x = v[k];
+    for (int k = 0; k < kEventCount; ++k) {
+        unsigned long long x = v[k];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if ((threadIdx.x & 31u) == 0u && events) atomicAdd(&events[k], x);
-        }
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31u) == 0u && events) atomicAdd(&events[k], x);
     }
 }
 
 template <bool C>
 __global__ void __launch_bounds__(kThreads) trace_kernel(const __grid_constant__ TraceParams P) {
     extern __shared__ float4 smem[];
-    Ctx<C> X;
-    X.sc = stage_scene(P, smem);
-    X.ev = Events{};
+    const Scene S = stage_scene(P, smem);
+    Events ev{};
+    const Counter<C> K{&ev};
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
-    const bool inside = x < P.width && y < P.height;
-    if (inside) {
+    if (x < P.width && y < P.height) {
         const uint32_t pixel = y * P.width + x;
         const uint32_t z = P.s.counts[2];
         float4 total = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         for (uint32_t smp = 0; smp < z; ++smp) {
             uint32_t rng = hash_u32(pixel ^ hash_u32(P.s.sampling[0] + smp + 0x9e3779b9u));
-            const float3 d = camera_direction(X, x, y, rng);
-            const float4 r = trace(X, Ray{f3(0.0f, 0.0f, 0.0f), d, kMiss}, rng);
+            const float3 d = camera_direction(&P.s, K, x, y, rng);
+            const float4 r = trace(S, K, Ray{f3(0.0f, 0.0f, 0.0f), d, kMiss}, rng);
             total.x += r.x;
             total.y += r.y;
             total.z += r.z;
@@ -294,10 +276,10 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(const __grid_constant__
             sum = P.sum[pixel];
             comp = P.comp[pixel];
             float yv, t;
-            yv = total.x - comp.x; t = sum.x + yv; comp.x = (t - sum.x) - yv; sum.x = t;
-            yv = total.y - comp.y; t = sum.y + yv; comp.y = (t - sum.y) - yv; sum.y = t;
-            yv = total.z - comp.z; t = sum.z + yv; comp.z = (t - sum.z) - yv; sum.z = t;
-            yv = total.w - comp.w; t = sum.w + yv; comp.w = (t - sum.w) - yv; sum.w = t;
+            yv = __fsub_rn(total.x, comp.x); t = __fadd_rn(sum.x, yv); comp.x = __fsub_rn(__fsub_rn(t, sum.x), yv); sum.x = t;
+            yv = __fsub_rn(total.y, comp.y); t = __fadd_rn(sum.y, yv); comp.y = __fsub_rn(__fsub_rn(t, sum.y), yv); sum.y = t;
+            yv = __fsub_rn(total.z, comp.z); t = __fadd_rn(sum.z, yv); comp.z = __fsub_rn(__fsub_rn(t, sum.z), yv); sum.z = t;
+            yv = __fsub_rn(total.w, comp.w); t = __fadd_rn(sum.w, yv); comp.w = __fsub_rn(__fsub_rn(t, sum.w), yv); sum.w = t;
         }
         P.sum[pixel] = sum;
         P.comp[pixel] = comp;
@@ -306,25 +288,31 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(const __grid_constant__
                                     __fdiv_rn(__fsub_rn(sum.z, comp.z), new_count),
                                     __fdiv_rn(__fsub_rn(sum.w, comp.w), new_count));
     }
-    flush_events(X, P.events);
+    if constexpr (C) flush_events(ev, P.events);
+}
+
+__device__ __forceinline__ Ray load_ray(const sg_ray &in) {
+    return Ray{f3(in.offset[0], in.offset[1], in.offset[2]), f3(in.direction[0], in.direction[1], in.direction[2]),
+               in.anchor};
 }
 
 __global__ void __launch_bounds__(kThreads) closest_hit_kernel(const __grid_constant__ TraceParams P,
                                                                const sg_ray *rays, sg_hit *hits, uint32_t n) {
     extern __shared__ float4 smem[];
-    Ctx<false> X;
-    X.sc = stage_scene(P, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
-    const Ray r{f3(in.offset[0], in.offset[1], in.offset[2]), f3(in.direction[0], in.direction[1], in.direction[2]),
-                in.anchor};
-    const Hit h = closest_hit(X, r);
+    const Ray r = load_ray(in);
+    // An anchor outside the body table would index past the staged bodies.
+    const bool valid = in.anchor == kMiss || in.anchor < P.s.counts[0];
+    const Hit h = valid ? closest_hit(S, K, r) : Hit{1.0e30f, kMiss, 0.0f};
     sg_hit out;
     out.distance = h.t;
     out.index = h.index;
     float3 nrm = f3(0.0f, 0.0f, 0.0f);
-    if (h.index != kMiss) nrm = sphere_normal(X.sc, r, h.index, h.delta);
+    if (h.index != kMiss) nrm = sphere_normal(S, r, h.index, h.delta);
     out.normal[0] = nrm.x;
     out.normal[1] = nrm.y;
     out.normal[2] = nrm.z;
@@ -335,36 +323,37 @@ __global__ void __launch_bounds__(kThreads) visibility_kernel(const __grid_const
                                                               const sg_ray *rays, const uint32_t *lights,
                                                               float *out, uint32_t n) {
     extern __shared__ float4 smem[];
-    Ctx<false> X;
-    X.sc = stage_scene(P, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
-    const Ray r{f3(in.offset[0], in.offset[1], in.offset[2]), f3(in.direction[0], in.direction[1], in.direction[2]),
-                in.anchor};
     const uint32_t light = lights[k];
-    out[k] = light < P.s.counts[0] ? light_visibility(X, r, light) : 0.0f;
+    const bool valid = (in.anchor == kMiss || in.anchor < P.s.counts[0]) && light < P.s.counts[0];
+    out[k] = valid ? light_visibility(S, K, load_ray(in), light) : 0.0f;
 }
 
 __global__ void __launch_bounds__(kThreads) ring_probe_kernel(const __grid_constant__ TraceParams P,
                                                               const sg_ray *rays, uint32_t body, float *out,
                                                               uint32_t n) {
     extern __shared__ float4 smem[];
-    Ctx<false> X;
-    X.sc = stage_scene(P, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
-    const Ray r{f3(in.offset[0], in.offset[1], in.offset[2]), f3(in.direction[0], in.direction[1], in.direction[2]),
-                in.anchor};
+    const Ray r = load_ray(in);
     float4 result = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (body < P.s.counts[0]) {
-        const RingHit h = ring_hit(X, r, body);
+    if (body < P.s.counts[0] && (in.anchor == kMiss || in.anchor < P.s.counts[0])) {
+        const RingHit h = ring_hit(S, K, r, body);
         if (h.index != kMiss)
-            result = make_float4(h.t, __fdiv_rn(length_rn(h.p), b_radius(X.sc, body)),
-                                 ring_transmission(X.sc, r, h), 1.0f);
+            result = make_float4(h.t, __fdiv_rn(length_rn(h.p), b_radius(S, body)), ring_transmission(S, r, h), 1.0f);
     }
-    reinterpret_cast<float4 *>(out)[k] = result;
+    // Scalar stores: a caller's device pointer need only be 4-byte aligned.
+    out[4 * k + 0] = result.x;
+    out[4 * k + 1] = result.y;
+    out[4 * k + 2] = result.z;
+    out[4 * k + 3] = result.w;
 }
 
 __global__ void ring_energy_kernel(float albedo, float tau, float mu, uint32_t steps, float *out) {
