@@ -225,6 +225,7 @@ __device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C> K, const R
     Hit best{1.0e30f, kMiss, 0.0f};
     const uint32_t n = S.s->counts[0];
     const float host = S.s->g.ground_north[3];
+#pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         if (host == (float)(i + 1u)) continue;
         float delta;
@@ -328,6 +329,7 @@ template <bool C>
 __device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C> K, const Ray &r, float limit) {
     RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
+#pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         const RingHit h = ring_hit(S, K, r, i);
         if (h.index != kMiss && h.t < best.t) best = h;
@@ -420,12 +422,14 @@ __device__ SG_HELPER float light_visibility(Scene S, Counter<C> K, Ray r, uint32
     const float host = S.s->g.ground_north[3];
     const uint32_t n = S.s->counts[0];
     if (host == (float)(light + 1u) && closest_hit(S, K, r).index != light) return 0.0f;
+#pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         if (i == light || host == (float)(i + 1u)) continue;
         const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
         if (t < 1.0e30f && (t < surface || (t == surface && i < light))) return 0.0f;
     }
     float transmission = 1.0f;
+#pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         const RingHit h = ring_hit(S, K, r, i);
         if (h.index != kMiss && h.t < surface) transmission *= ring_transmission(S, r, h);
@@ -505,6 +509,7 @@ __device__ SG_HELPER Shine ringshine(Scene S, Counter<C> K, uint32_t index, floa
     const float mu_out = dot(-direction, n);
     float3 shine = zero;
     const uint32_t count = light_count(S.s);
+#pragma unroll 1
     for (uint32_t slot = 0; slot < count; ++slot) {
         const uint32_t i = light_index(S.s, slot);
         const float4 material = bf(S, i, kMaterial);
@@ -544,6 +549,7 @@ __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C> K, Ray r, Hit cl
     const float angle = clampf(kPointDiscRadius, 0.7f * pixel, kStarDotPixels * pixel);
     const uint32_t host = (uint32_t)s->g.atmo_params[3] - 1u;
     const uint32_t n = s->counts[0];
+#pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         if (i == host || s->g.ground_north[3] == (float)(i + 1u)) continue;
         const float radius = b_radius(S, i);
