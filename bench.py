@@ -142,9 +142,10 @@ def cpu_baseline(wl, seconds: float, threads: int = 0) -> dict:
     from oracle.binding import OracleTracer
     from stargaze_b200.workloads import render_options as bench_options
 
+    from stargaze_b200.workloads import upload_workload
+
     t = OracleTracer((wl.width, wl.height), bench_options(wl, spp=8), threads=threads)
-    for slot, tau in wl.ring_tables.items():
-        t.upload_ring_profile(slot, tau)
+    upload_workload(t, wl)
     rows_per_chunk = max(1, wl.height // 27)
     samples = 0
     start = time.perf_counter()
@@ -219,9 +220,10 @@ def run_ours(args):
     # Disjoint noise sequences per rank: each GPU renders its own full-frame
     # 256-spp estimate (weak scaling, no data-path collective).
     opts = bench_options(wl, spp=BATCH, noise_seed=rank << 26)
+    from stargaze_b200.workloads import upload_workload
+
     tracer = PathTracer((wl.width, wl.height), opts, device=local)
-    for slot, tau in wl.ring_tables.items():
-        tracer.upload_ring_profile(slot, tau)
+    upload_workload(tracer, wl)
     stream = torch.cuda.Stream()
     frame = wl.frame.copy()
 
@@ -234,8 +236,7 @@ def run_ours(args):
 
     # Algorithmic work of one launch (counting kernel, outside timing).
     counter = PathTracer((wl.width, wl.height), opts, device=local)
-    for slot, tau in wl.ring_tables.items():
-        counter.upload_ring_profile(slot, tau)
+    upload_workload(counter, wl)
     totals = np.zeros(len(EVENT_ORDER), np.uint64)
     ev = (C.c_uint64 * len(EVENT_ORDER))()
     for _ in range(batches):
@@ -324,7 +325,8 @@ def run_ours(args):
                          "launch_ms": statistics.mean(launch_ms),
                          "events_per_launch": {n: int(totals[k]) // batches for k, n in enumerate(EVENT_ORDER)},
                          "peak_source": "measured FMA-chain kernel (sg_measure_fp32_peak)"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": batches * len(frame.bodies) * 160,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": batches * (len(frame.bodies) * 160 + len(frame.ground) * (48 + 32)),
                     "d2h_bytes_per_step": wl.width * wl.height * 16},
             "gpu_launches": int(launches),
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},

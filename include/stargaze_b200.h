@@ -50,6 +50,14 @@ extern "C" {
 #define SG_GROUND_CAPACITY 256
 /* 2^24: the f32 sample-weight limit (src/graphics.rs:11). */
 #define SG_MAX_SAMPLES 16777216u
+/* Extension: landscape primitives this library accepts per frame. The
+ * reference caps the list at SG_GROUND_CAPACITY; nested group markers
+ * (center.w < 0) turn a longer list into a bounding-volume hierarchy that
+ * the reference's own traversal (ground.wgsl:167-178) walks. */
+#define SG_PROP_CAPACITY 65536
+/* Extension: terrain grids up to 4096 cells per side (the reference stops
+ * at 2048, src/terrain.rs:20). */
+#define SG_TERRAIN_MAX_CELLS 4096
 /* Extension: radial optical-depth tables for rings (no reference
  * counterpart; the reference has only a scalar or banded profile). */
 #define SG_RING_TABLE_SLOTS 8
@@ -243,6 +251,28 @@ SG_API int sg_accumulation_device_ptr(sg_context *ctx, void **ptr);
 SG_API int sg_upload_ring_profile(sg_context *ctx, uint32_t slot, const float *tau,
                            uint32_t bins);
 
+/* Heightfield for the local landscape: `data` is the reference's
+ * `terrain::Terrain::data` vector (src/terrain.rs:781-838) for a grid of
+ * `cells` cells per side (power of two, 2..SG_TERRAIN_MAX_CELLS):
+ * (cells+1)^2 heights, then (cells <= 1024 only) x and z derivatives, then
+ * (min, max) per quadtree node in breadth-first order; `n_floats` must be
+ * exactly that length. The device appends the geometry cache of
+ * cache_terrain_geometry (terrain.wgsl:242-285) on the next encode and
+ * whenever the host radius (ground_up.w) changes. Frames with
+ * ground_counts.y != 0 need an uploaded terrain. Uploading bumps the
+ * history key. Replaces the ground buffer writes of src/pathtracer.rs:914-945. */
+SG_API int sg_upload_terrain(sg_context *ctx, const float *data, size_t n_floats,
+                             uint32_t cells);
+
+/* Extension (no reference counterpart): a width x height scalar albedo map
+ * over the surface frame; texel (i, j) covers x in
+ * [-extent + 2*extent*i/width, ...) and likewise z, nearest-texel lookup.
+ * When present it replaces the theme floor of the host ground and terrain
+ * (ground.wgsl:601-610). width = 0 removes it. Bumps the history key. */
+SG_API int sg_upload_albedo_map(sg_context *ctx, const float *albedo,
+                                uint32_t width, uint32_t height,
+                                float extent_m);
+
 /* ------------------------------------------------------------------ */
 /* Geometric queries (the reference's WGSL probe entry points)         */
 /* ------------------------------------------------------------------ */
@@ -263,6 +293,14 @@ SG_API int sg_light_visibility(sg_context *ctx, const sg_frame *frame,
 SG_API int sg_ring_probe(sg_context *ctx, const sg_frame *frame, const sg_ray *rays,
                   uint32_t body, uint32_t n, float *out, int on_device,
                   void *stream);
+
+/* terrain_hit in the surface frame (the terrain_probe entry point of
+ * src/ground_tests.rs:700-705): rays[6*i..] = (origin xyz in metres,
+ * direction xyz); out[4*i..] = (normal xyz, distance), distance 1e30 on a
+ * miss. Uses the uploaded terrain, cached for the frame's host radius. */
+SG_API int sg_terrain_probe(sg_context *ctx, const sg_frame *frame,
+                            const float *rays, uint32_t n, float *out,
+                            int on_device, void *stream);
 
 /* Energy of the ring slab BSDF (ring_tests.rs:352-413 probe): unscattered
  * transmission plus the cosine-weighted integral of ring_bsdf over both

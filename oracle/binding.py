@@ -26,6 +26,14 @@ class Tables(C.Structure):
     _fields_ = [
         ("ring_tau", C.c_void_p * abi.RING_TABLE_SLOTS),
         ("ring_bins", C.c_uint32 * abi.RING_TABLE_SLOTS),
+        ("terrain", C.c_void_p),
+        ("terrain_cells", C.c_uint32),
+        ("ground", C.c_void_p),
+        ("n_ground", C.c_uint32),
+        ("albedo_map", C.c_void_p),
+        ("map_width", C.c_uint32),
+        ("map_height", C.c_uint32),
+        ("map_extent", C.c_float),
     ]
 
 
@@ -64,6 +72,12 @@ def load() -> C.CDLL:
     lib.oracle_ring_energy.argtypes = [C.c_float, C.c_float, C.c_float, C.c_uint32]
     lib.oracle_ring_energy.restype = C.c_float
     lib.oracle_sample_light.argtypes = [S, P, P, C.c_uint32, C.POINTER(C.c_uint32), P, C.POINTER(C.c_float)]
+    lib.oracle_terrain_floats.argtypes = [C.c_uint32]
+    lib.oracle_terrain_floats.restype = C.c_size_t
+    lib.oracle_cache_terrain.argtypes = [P, C.c_uint32, C.c_float]
+    lib.oracle_cache_terrain.restype = C.c_int
+    lib.oracle_terrain_query.argtypes = [S, C.POINTER(Tables), P, P, C.c_float, C.c_int, P]
+    lib.oracle_terrain_query.restype = C.c_int
     lib.oracle_hash.argtypes = [C.c_uint32]
     lib.oracle_hash.restype = C.c_uint32
     lib.oracle_random.argtypes = [C.POINTER(C.c_uint32)]
@@ -85,21 +99,66 @@ def _check(status: int, what: str) -> None:
 
 
 class TableSet:
-    """Ring optical-depth tables shared with the CUDA context."""
+    """Scene data beyond the bodies, mirroring the CUDA context: ring
+    tables, the heightfield (with its CPU-computed geometry cache) and the
+    albedo map."""
 
     def __init__(self):
         self.tables: dict[int, np.ndarray] = {}
         self.version = 0
+        self.terrain: np.ndarray | None = None
+        self.terrain_cells = 0
+        self.terrain_radius: float | None = None
+        self.albedo: np.ndarray | None = None
+        self.map_extent = 0.0
+        self._ground = None
 
     def upload(self, slot: int, tau) -> None:
         self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
         self.version += 1
 
-    def struct(self) -> Tables:
+    def upload_terrain(self, data, cells: int) -> None:
+        lib = load()
+        full = np.zeros(lib.oracle_terrain_floats(cells), dtype=np.float32)
+        data = np.asarray(data, dtype=np.float32)
+        full[: data.size] = data
+        self.terrain = full
+        self.terrain_cells = cells
+        self.terrain_radius = None
+        self.version += 1
+
+    def upload_albedo_map(self, albedo, extent_m: float) -> None:
+        self.albedo = None if albedo is None else np.ascontiguousarray(albedo, dtype=np.float32)
+        self.map_extent = float(extent_m)
+        self.version += 1
+
+    def prepare(self, frame: Frame) -> None:
+        """Rebuild the terrain cache when the host radius changed (as
+        src/pathtracer.rs:933-945 does on the GPU)."""
+        g = frame.globals
+        if self.terrain is not None and g.ground_north[3] != 0.0 and g.ground_counts[1] != 0:
+            radius = float(np.float32(g.ground_up[3]))
+            if self.terrain_radius != radius:
+                _check(load().oracle_cache_terrain(_ptr(self.terrain), self.terrain_cells, radius), "oracle_cache_terrain")
+                self.terrain_radius = radius
+
+    def struct(self, frame: Frame | None = None) -> Tables:
         t = Tables()
         for slot, arr in self.tables.items():
             t.ring_tau[slot] = arr.ctypes.data
             t.ring_bins[slot] = arr.size
+        if self.terrain is not None:
+            t.terrain = self.terrain.ctypes.data
+            t.terrain_cells = self.terrain_cells
+        if frame is not None and frame.ground:
+            self._ground = (abi.Primitive * len(frame.ground))(*frame.ground)
+            t.ground = C.cast(self._ground, C.c_void_p)
+            t.n_ground = len(frame.ground)
+        if self.albedo is not None:
+            t.albedo_map = self.albedo.ctypes.data
+            t.map_width = self.albedo.shape[1]
+            t.map_height = self.albedo.shape[0]
+            t.map_extent = self.map_extent
         return t
 
 
@@ -188,9 +247,16 @@ class OracleTracer:
     def upload_ring_profile(self, slot: int, tau) -> None:
         self.tables.upload(slot, tau)
 
+    def upload_terrain(self, data, cells: int) -> None:
+        self.tables.upload_terrain(data, cells)
+
+    def upload_albedo_map(self, albedo, extent_m: float) -> None:
+        self.tables.upload_albedo_map(albedo, extent_m)
+
     def settings_for(self, frame: Frame, count: int) -> abi.Settings:
         return frame.settings(self.width, self.height, self.samples_, count, self.opts.max_bounces,
-                              self.opts.noise_seed + self.sequence_, self.opts.milky_way)
+                              self.opts.noise_seed + self.sequence_, self.opts.milky_way,
+                              terrain_cells=self.tables.terrain_cells or 512)
 
     def encode(self, frame: Frame, stream=None, rows=None) -> None:
         if len(frame.bodies) > abi.BODY_CAPACITY:
@@ -200,7 +266,8 @@ class OracleTracer:
         if count > 0:
             s = self.settings_for(frame, count)
             bodies = frame.bodies_array()
-            t = self.tables.struct()
+            self.tables.prepare(frame)
+            t = self.tables.struct(frame)
             y0, y1 = rows if rows is not None else (0, self.height)
             _check(self.lib.oracle_dispatch(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(self.acc),
                                             _ptr(self.backdrop), y0, y1, self.threads, C.byref(self.events)),
@@ -218,7 +285,24 @@ class OracleTracer:
     # probes -------------------------------------------------------------
     def _probe_args(self, frame: Frame):
         s = self.settings_for(frame, 0)
-        return s, frame.bodies_array(), self.tables.struct()
+        self.tables.prepare(frame)
+        return s, frame.bodies_array(), self.tables.struct(frame)
+
+    def terrain_probe(self, frame: Frame, origins, directions) -> np.ndarray:
+        """Mirror of PathTracer.terrain_probe: terrain_hit per ray."""
+        o = np.asarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.asarray(directions, dtype=np.float32).reshape(-1, 3)
+        return np.array([self.terrain_query(frame, o[k], d[k]) for k in range(len(o))], dtype=np.float32)
+
+    def terrain_query(self, frame: Frame, o, d, limit: float = 1.0e29, occlusion: bool = False) -> np.ndarray:
+        """terrain_query in the surface frame: (normal xyz, distance)."""
+        s, _bodies, t = self._probe_args(frame)
+        o = np.ascontiguousarray(o, dtype=np.float32)
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        out = np.zeros(4, dtype=np.float32)
+        _check(self.lib.oracle_terrain_query(C.byref(s), C.byref(t), _ptr(o), _ptr(d), limit, int(occlusion),
+                                             _ptr(out)), "oracle_terrain_query")
+        return out
 
     def closest_hit(self, frame: Frame, rays: np.ndarray) -> np.ndarray:
         s, bodies, t = self._probe_args(frame)

@@ -138,14 +138,8 @@ static inline hit_t sphere_hit(const scene *S, ray_t ray, uint32_t index) {
     return sphere_hit_radius(S, ray, index, b_radius(S, index));
 }
 
-/* landscape_query: ground.wgsl:123-242. The oracle accepts only frames
- * with the landscape disabled (ground_north.w == 0), where it returns the
- * initial closest record (ground.wgsl:124-125). */
-static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusion) {
-    (void)ray; (void)occlusion; (void)S;
-    hit_t h = {limit, MISS, {0, 0, 0}};
-    return h;
-}
+/* landscape_query: ground.wgsl:123-242 (defined with the landscape code). */
+static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusion);
 
 /* closest_hit: pathtrace.wgsl:173-185 */
 static hit_t closest_hit(const scene *S, ray_t ray) {
@@ -482,7 +476,621 @@ static v3 surface_albedo(const scene *S, uint32_t index, v3 normal) {
 }
 
 /* ---------------------------------------------------------------- */
-/* trace: pathtrace.wgsl:1347-1617 (airless, landscape off)          */
+/* Local landscape: ground.wgsl:14-242, :597-666; terrain.wgsl       */
+/* ---------------------------------------------------------------- */
+#define METRES_PER_AU 149597870700.0f
+#define TERRAIN_ID SG_TERRAIN_ID
+
+static inline v3 g_east(const scene *S) { return V(S->s->g.ground_east[0], S->s->g.ground_east[1], S->s->g.ground_east[2]); }
+static inline v3 g_up(const scene *S) { return V(S->s->g.ground_up[0], S->s->g.ground_up[1], S->s->g.ground_up[2]); }
+static inline v3 g_north(const scene *S) { return V(S->s->g.ground_north[0], S->s->g.ground_north[1], S->s->g.ground_north[2]); }
+
+/* camera_origin, to_ground, from_ground, ground_origin: ground.wgsl:17-32 */
+static v3 camera_origin(const scene *S, ray_t ray) {
+    if (ray.anchor == MISS) return ray.offset;
+    return vadd(b_center(S, ray.anchor), vadd(b_low(S, ray.anchor), ray.offset));
+}
+static v3 to_ground(const scene *S, v3 v) { return V(vdot(v, g_east(S)), vdot(v, g_up(S)), vdot(v, g_north(S))); }
+static v3 from_ground(const scene *S, v3 v) {
+    return vadd(vadd(vmul(g_east(S), v.x), vmul(g_up(S), v.y)), vmul(g_north(S), v.z));
+}
+static v3 ground_origin(const scene *S, ray_t ray) {
+    v3 g = to_ground(S, vmul(camera_origin(S, ray), METRES_PER_AU));
+    return vadd(g, V(0.0f, S->s->g.ground_east[3], 0.0f));
+}
+/* Rotation sines and cosines are evaluated in double and rounded to f32,
+ * a rounding the CUDA path reproduces exactly (it precomputes the same
+ * values per primitive on the host). */
+static inline float sin_r(float angle) { return (float)sin((double)angle); }
+static inline float cos_r(float angle) { return (float)cos((double)angle); }
+static v3 rotate_north(v3 p, float angle) {
+    float c = cos_r(angle), s = sin_r(angle);
+    return V(c * p.x - s * p.y, s * p.x + c * p.y, p.z);
+}
+static v3 rotate_east(v3 p, float angle) {
+    float c = cos_r(angle), s = sin_r(angle);
+    return V(p.x, c * p.y - s * p.z, s * p.y + c * p.z);
+}
+static v3 rotate_up(v3 p, float angle) {
+    float c = cos_r(angle), s = sin_r(angle);
+    return V(c * p.x + s * p.z, p.y, -s * p.x + c * p.z);
+}
+/* rock_angles, rock_to_local, rock_from_local: ground.wgsl:41-61 */
+static v3 rock_angles(float packed) {
+    uint32_t bits = (uint32_t)packed;
+    return vmul(V((float)(bits & 255u), (float)((bits >> 8) & 255u), (float)((bits >> 16) & 255u)), TAU_F / 256.0f);
+}
+static v3 rock_to_local(v3 p, v3 a) { return rotate_east(rotate_up(rotate_north(p, -a.z), -a.y), -a.x); }
+static v3 rock_from_local(v3 p, v3 a) { return rotate_north(rotate_up(rotate_east(p, a.x), a.y), a.z); }
+
+static inline float vcomp(v3 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+
+/* box_interval: ground.wgsl:64-78 */
+static void box_interval(v3 p, v3 d, v3 extent, float *near_, float *far_) {
+    float n = -1.0e30f, f = 1.0e30f;
+    for (int axis = 0; axis < 3; axis++) {
+        float pa = vcomp(p, axis), da = vcomp(d, axis), ea = vcomp(extent, axis);
+        if (fabsf(da) < 1.0e-12f) {
+            if (fabsf(pa) > ea) { *near_ = 1.0e30f; *far_ = -1.0e30f; return; }
+        } else {
+            float a = (-ea - pa) / da;
+            float b = (ea - pa) / da;
+            n = maxf_(n, minf_(a, b));
+            f = minf_(f, maxf_(a, b));
+        }
+    }
+    *near_ = n;
+    *far_ = f;
+}
+
+/* rock_hit: ground.wgsl:82-121, returns the distance, normal in *n */
+static float rock_hit(v3 p, v3 d, v3 e, v3 *normal) {
+    v3 origin = V(p.x / e.x, p.y / e.y, p.z / e.z);
+    v3 direction = V(d.x / e.x, d.y / e.y, d.z / e.z);
+    float near_ = -1.0e30f, far_ = 1.0e30f;
+    v3 near_normal = V(0, 0, 0), far_normal = V(0, 0, 0);
+    for (uint32_t face = 0; face < 14u; face++) {
+        v3 n = V(0, 0, 0);
+        float limit = 1.0f;
+        if (face < 6u) {
+            float s = (face & 1u) == 1u ? 1.0f : -1.0f;
+            if (face / 2u == 0) n.x = s; else if (face / 2u == 1) n.y = s; else n.z = s;
+        } else {
+            uint32_t bits = face - 6u;
+            n = V((bits & 1u) ? 1.0f : -1.0f, (bits & 2u) ? 1.0f : -1.0f, (bits & 4u) ? 1.0f : -1.0f);
+            limit = 1.65f + 0.08f * (float)(bits % 3u);
+        }
+        float denominator = vdot(n, direction);
+        float gap = limit - vdot(n, origin);
+        if (fabsf(denominator) < 1.0e-12f) {
+            if (gap < 0.0f) return 1.0e30f;
+        } else {
+            float distance = gap / denominator;
+            if (denominator < 0.0f && distance > near_) { near_ = distance; near_normal = V(n.x / e.x, n.y / e.y, n.z / e.z); }
+            if (denominator > 0.0f && distance < far_) { far_ = distance; far_normal = V(n.x / e.x, n.y / e.y, n.z / e.z); }
+        }
+        if (near_ > far_) return 1.0e30f;
+    }
+    if (far_ <= 0.001f) return 1.0e30f;
+    if (near_ > 0.001f) { *normal = vnormalize(near_normal); return near_; }
+    *normal = vnormalize(far_normal);
+    return far_;
+}
+
+/* Terrain layout helpers: terrain.wgsl:6-36 */
+static uint32_t t_cells(const scene *S) {
+    uint32_t log2 = S->s->g.ground_counts[2] >> 8;
+    return log2 != 0u ? (1u << log2) : 512u;
+}
+static inline uint32_t t_width(uint32_t cells) { return cells + 1u; }
+static inline uint32_t t_vertices(uint32_t cells) { return t_width(cells) * t_width(cells); }
+static inline int t_compact(uint32_t cells) { return cells > 1024u; }
+static inline uint32_t t_vertex_stride(uint32_t cells) { return t_compact(cells) ? 2u : 6u; }
+static inline uint32_t t_nodes(uint32_t cells) { uint32_t leaves = cells / 2u; return (4u * leaves * leaves - 1u) / 3u; }
+static inline uint32_t t_bounds(uint32_t cells) { return (t_compact(cells) ? 1u : 3u) * t_vertices(cells); }
+static inline uint32_t t_cache(uint32_t cells) { return t_bounds(cells) + 2u * t_nodes(cells); }
+static inline uint32_t t_vertex_cache(uint32_t cells) { return t_cache(cells) + 6u * t_nodes(cells); }
+static inline uint32_t ground_theme(const scene *S) { return S->s->g.ground_counts[2] & 255u; }
+
+size_t oracle_terrain_floats(uint32_t cells) {
+    return (size_t)t_vertex_cache(cells) + (size_t)t_vertices(cells) * t_vertex_stride(cells);
+}
+
+static inline float t_scale_r(float r) { return clampf_(r / 200000.0f, 0.0001f, 1.0f); }
+static inline float t_coordinate(uint32_t i, uint32_t cells, float scale) {
+    float u = 2.0f * (float)i / (float)cells - 1.0f;
+    return u * fabsf(u) * 16000.0f * scale;
+}
+static inline float t_curvature(float px, float pz, float r) {
+    float d2 = px * px + pz * pz;
+    return -d2 / (r + sqrtf(maxf_(r * r - d2, 0.0f)));
+}
+/* De-interleave one Morton axis (terrain.wgsl:134-140). */
+static inline uint32_t compact_bits(uint32_t value) {
+    uint32_t x = value & 0x55555555u;
+    x = (x | (x >> 1)) & 0x33333333u;
+    x = (x | (x >> 2)) & 0x0f0f0f0fu;
+    x = (x | (x >> 4)) & 0x00ff00ffu;
+    return (x | (x >> 8)) & 0x0000ffffu;
+}
+static inline uint32_t first_leading_bit(uint32_t v) { uint32_t n = 0; while (v >>= 1) n++; return n; }
+static void node_of(uint32_t index, uint32_t cells, uint32_t node[4]) {
+    uint32_t level = first_leading_bit(3u * index + 1u) / 2u;
+    uint32_t size = cells >> level;
+    uint32_t morton = index - ((1u << (2u * level)) - 1u) / 3u;
+    node[0] = index;
+    node[1] = compact_bits(morton) * size;
+    node[2] = compact_bits(morton >> 1) * size;
+    node[3] = size;
+}
+
+/* cache_terrain_geometry: terrain.wgsl:242-285 with the uncached helpers
+ * :37-61 and :85-95. */
+int oracle_cache_terrain(float *T, uint32_t cells, float r) {
+    if (!T || cells < 2u || (cells & (cells - 1u)) != 0u) return SG_ERR_INVALID;
+    float scale = t_scale_r(r);
+    uint32_t width = t_width(cells), nodes = t_nodes(cells), vertices = t_vertices(cells);
+    for (uint32_t index = 0; index < nodes; index++) {
+        uint32_t node[4];
+        node_of(index, cells, node);
+        float lo_x = t_coordinate(node[1], cells, scale), lo_z = t_coordinate(node[2], cells, scale);
+        float hi_x = t_coordinate(node[1] + node[3], cells, scale), hi_z = t_coordinate(node[2] + node[3], cells, scale);
+        float near_x = clampf_(0.0f, lo_x, hi_x), near_z = clampf_(0.0f, lo_z, hi_z);
+        float far_x = maxf_(fabsf(lo_x), fabsf(hi_x)), far_z = maxf_(fabsf(lo_z), fabsf(hi_z));
+        float lower = T[t_bounds(cells) + index * 2u] * scale + t_curvature(far_x, far_z, r) - 0.02f;
+        float upper = T[t_bounds(cells) + index * 2u + 1u] * scale + t_curvature(near_x, near_z, r) + 0.02f;
+        float *c = T + t_cache(cells) + (size_t)index * 6u;
+        c[0] = lo_x; c[1] = lower; c[2] = lo_z; c[3] = hi_x; c[4] = upper; c[5] = hi_z;
+    }
+    for (uint32_t index = 0; index < vertices; index++) {
+        uint32_t x = index % width, z = index / width;
+        float px = t_coordinate(x, cells, scale), pz = t_coordinate(z, cells, scale);
+        v3 vertex = V(px, T[z * width + x] * scale + t_curvature(px, pz, r), pz);
+        float denom = sqrtf(maxf_(r * r - (px * px + pz * pz), 1.0f));
+        float gx = px / denom, gz = pz / denom;
+        v3 normal;
+        if (t_compact(cells)) {
+            uint32_t lox = x > 0 ? x - 1u : 0u, loz = z > 0 ? z - 1u : 0u;
+            uint32_t hix = x + 1u < cells ? x + 1u : cells, hiz = z + 1u < cells ? z + 1u : cells;
+            float dx = (T[z * width + hix] - T[z * width + lox]) /
+                       ((t_coordinate(hix, cells, scale) - t_coordinate(lox, cells, scale)) / scale);
+            float dz = (T[hiz * width + x] - T[loz * width + x]) /
+                       ((t_coordinate(hiz, cells, scale) - t_coordinate(loz, cells, scale)) / scale);
+            normal = vnormalize(V(-dx + gx, 1.0f, -dz + gz));
+        } else {
+            normal = vnormalize(V(-T[vertices + index] + gx, 1.0f, -T[2u * vertices + index] + gz));
+        }
+        float *v = T + t_vertex_cache(cells) + (size_t)index * t_vertex_stride(cells);
+        if (t_compact(cells)) {
+            v[0] = vertex.y;
+            /* WGSL round() rounds half to even, as rintf does. */
+            float ux = rintf(clampf_(normal.x * 0.5f + 0.5f, 0.0f, 1.0f) * 4095.0f);
+            float uz = rintf(clampf_(normal.z * 0.5f + 0.5f, 0.0f, 1.0f) * 4095.0f);
+            v[1] = (float)((uint32_t)ux | ((uint32_t)uz << 12));
+        } else {
+            v[0] = vertex.x; v[1] = vertex.y; v[2] = vertex.z;
+            v[3] = normal.x; v[4] = normal.y; v[5] = normal.z;
+        }
+    }
+    return SG_OK;
+}
+
+/* terrain_vertex / terrain_normal: terrain.wgsl:97-115 */
+static v3 t_vertex(const float *T, uint32_t cells, float scale, uint32_t x, uint32_t z) {
+    const float *v = T + t_vertex_cache(cells) + (size_t)(z * t_width(cells) + x) * t_vertex_stride(cells);
+    if (t_compact(cells)) return V(t_coordinate(x, cells, scale), v[0], t_coordinate(z, cells, scale));
+    return V(v[0], v[1], v[2]);
+}
+static v3 t_normal(const float *T, uint32_t cells, uint32_t x, uint32_t z) {
+    const float *v = T + t_vertex_cache(cells) + (size_t)(z * t_width(cells) + x) * t_vertex_stride(cells);
+    if (t_compact(cells)) {
+        uint32_t packed = (uint32_t)v[1];
+        float xx = (float)(packed & 4095u) / 4095.0f * 2.0f - 1.0f;
+        float zz = (float)(packed >> 12) / 4095.0f * 2.0f - 1.0f;
+        return vnormalize(V(xx, sqrtf(maxf_(1.0f - (xx * xx + zz * zz), 1.0e-6f)), zz));
+    }
+    return V(v[3], v[4], v[5]);
+}
+
+/* terrain_triangle: terrain.wgsl:65-81 -> (u, v, distance) */
+static v3 t_triangle(v3 o, v3 d, v3 a, v3 b, v3 c) {
+    v3 ab = vsub(b, a), ac = vsub(c, a);
+    v3 p = vcross(d, ac);
+    float determinant = vdot(ab, p);
+    if (fabsf(determinant) < 1.0e-12f) return V(0, 0, 1.0e30f);
+    float inverse = 1.0f / determinant;
+    v3 relative = vsub(o, a);
+    float u = vdot(relative, p) * inverse;
+    v3 q = vcross(relative, ab);
+    float v = vdot(d, q) * inverse;
+    float distance = vdot(ac, q) * inverse;
+    if (u < -1.0e-6f || v < -1.0e-6f || u + v > 1.000001f || distance <= 0.001f) return V(0, 0, 1.0e30f);
+    return V(u, v, distance);
+}
+
+/* terrain_interval: terrain.wgsl:118-130 */
+static void t_interval(const float *T, uint32_t cells, v3 o, v3 inv, uint32_t index, float *entry, float *exit_) {
+    const float *c = T + t_cache(cells) + (size_t)index * 6u;
+    float lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[3], c[4], c[5]};
+    float oo[3] = {o.x, o.y, o.z}, ii[3] = {inv.x, inv.y, inv.z};
+    float e0[3], e1[3];
+    for (int k = 0; k < 3; k++) {
+        int parallel = fabsf(ii[k]) >= 1.0e29f;
+        if (parallel && (oo[k] < lo[k] || oo[k] > hi[k])) { *entry = 1.0e30f; *exit_ = -1.0e30f; return; }
+    }
+    for (int k = 0; k < 3; k++) {
+        int parallel = fabsf(ii[k]) >= 1.0e29f;
+        float a = (lo[k] - oo[k]) * ii[k];
+        float b = (hi[k] - oo[k]) * ii[k];
+        e0[k] = parallel ? -1.0e30f : minf_(a, b);
+        e1[k] = parallel ? 1.0e30f : maxf_(a, b);
+    }
+    *entry = maxf_(e0[0], maxf_(e0[1], e0[2]));
+    *exit_ = minf_(e1[0], minf_(e1[1], e1[2]));
+}
+
+static int is_terrain_alpine(const scene *S) { return ground_theme(S) == 3u; }
+
+/* terrain_query: terrain.wgsl:152-234 (stack widened to 40 slots so 4096
+ * cells, eleven internal levels, fit: 3 * 11 + 1 = 34 entries). */
+static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d, float initial_limit, int occlusion,
+                     v3 *normal) {
+    float limit = initial_limit;
+    float result = 1.0e30f;
+    float scale = t_scale_r(S->s->g.ground_up[3]);
+    v3 inv = V((d.x >= 0.0f ? 1.0f : -1.0f) / maxf_(fabsf(d.x), 1.0e-30f),
+               (d.y >= 0.0f ? 1.0f : -1.0f) / maxf_(fabsf(d.y), 1.0e-30f),
+               (d.z >= 0.0f ? 1.0f : -1.0f) / maxf_(fabsf(d.z), 1.0e-30f));
+    float re, rx;
+    t_interval(T, cells, o, inv, 0u, &re, &rx);
+    if (re > rx || rx <= 0.001f || re >= limit) return result;
+    uint32_t stack_node[40];
+    float stack_t[40];
+    stack_node[0] = 0u;
+    stack_t[0] = maxf_(re, 0.0f);
+    uint32_t count = 1;
+    (void)is_terrain_alpine;
+    while (count > 0u) {
+        count--;
+        if (stack_t[count] >= limit) continue;
+        uint32_t node[4];
+        node_of(stack_node[count], cells, node);
+        if (node[3] == 2u) {
+            for (uint32_t z = node[2]; z < node[2] + 2u; z++) {
+                for (uint32_t x = node[1]; x < node[1] + 2u; x++) {
+                    v3 a = t_vertex(T, cells, scale, x, z);
+                    v3 b = t_vertex(T, cells, scale, x + 1u, z);
+                    v3 c = t_vertex(T, cells, scale, x, z + 1u);
+                    v3 e = t_vertex(T, cells, scale, x + 1u, z + 1u);
+                    v3 first = t_triangle(o, d, a, c, b);
+                    v3 second = t_triangle(o, d, e, b, c);
+                    if (first.z < limit) {
+                        if (occlusion) { *normal = V(0, 0, 0); return first.z; }
+                        v3 n = vnormalize(vadd(vadd(vmul(t_normal(T, cells, x, z), 1.0f - first.x - first.y),
+                                                    vmul(t_normal(T, cells, x, z + 1u), first.x)),
+                                               vmul(t_normal(T, cells, x + 1u, z), first.y)));
+                        *normal = n;
+                        result = first.z;
+                        limit = first.z;
+                    }
+                    if (second.z < limit) {
+                        if (occlusion) { *normal = V(0, 0, 0); return second.z; }
+                        v3 n = vnormalize(vadd(vadd(vmul(t_normal(T, cells, x + 1u, z + 1u), 1.0f - second.x - second.y),
+                                                    vmul(t_normal(T, cells, x + 1u, z), second.x)),
+                                               vmul(t_normal(T, cells, x, z + 1u), second.y)));
+                        *normal = n;
+                        result = second.z;
+                        limit = second.z;
+                    }
+                }
+            }
+        } else {
+            uint32_t children[4];
+            float distances[4];
+            uint32_t half_size = node[3] / 2u;
+            for (uint32_t child = 0; child < 4u; child++) {
+                children[child] = node[0] * 4u + child + 1u;
+                float be, bx;
+                t_interval(T, cells, o, inv, children[child], &be, &bx);
+                distances[child] = (be <= bx && bx > 0.001f && be < limit) ? maxf_(be, 0.0f) : 1.0e30f;
+                (void)half_size;
+            }
+            for (uint32_t i = 1; i < 4u; i++) {
+                uint32_t j = i;
+                while (!(j == 0u || distances[j - 1u] >= distances[j])) {
+                    float dd = distances[j - 1u];
+                    uint32_t cc = children[j - 1u];
+                    distances[j - 1u] = distances[j];
+                    children[j - 1u] = children[j];
+                    distances[j] = dd;
+                    children[j] = cc;
+                    j--;
+                }
+            }
+            for (uint32_t i = 0; i < 4u; i++) {
+                if (distances[i] < limit && count < 40u) {
+                    stack_node[count] = children[i];
+                    stack_t[count] = distances[i];
+                    count++;
+                }
+            }
+        }
+    }
+    return result;
+}
+
+int oracle_terrain_query(const sg_settings *settings, const oracle_tables *tables, const float o[3], const float d[3],
+                         float limit, int occlusion, float out[4]) {
+    if (!settings || !tables || !tables->terrain) return SG_ERR_INVALID;
+    scene S = {settings, NULL, tables, NULL};
+    v3 n = V(0, 0, 0);
+    float t = t_query(&S, tables->terrain, t_cells(&S), V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), limit, occlusion, &n);
+    out[0] = n.x; out[1] = n.y; out[2] = n.z; out[3] = t;
+    return SG_OK;
+}
+
+/* landscape_top: ground.wgsl:244-251 */
+static float landscape_top(const scene *S) {
+    float top;
+    uint32_t bits = S->s->g.ground_counts[3];
+    memcpy(&top, &bits, sizeof(top));
+    if (S->s->g.ground_counts[1] != 0u && S->t && S->t->terrain)
+        top = maxf_(top, S->t->terrain[t_cache(t_cells(S)) + 4u]);
+    return top;
+}
+
+/* landscape_query: ground.wgsl:123-242 (vegetation kinds > 2.5 are not
+ * restated; frames carrying them are rejected). */
+static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusion) {
+    hit_t closest = {limit, MISS, {0, 0, 0}};
+    if (S->s->g.ground_north[3] == 0.0f) return closest;
+    v3 o = ground_origin(S, ray);
+    v3 d = to_ground(S, ray.dir);
+    float radius = S->s->g.ground_up[3];
+    if (vdot(o, o) > 4.0f * radius * radius) return sphere_hit(S, ray, (uint32_t)S->s->g.ground_north[3] - 1u);
+    if (d.y >= 0.0f && o.y > landscape_top(S)) return closest;
+    float a = vdot(d, d);
+    float b = -radius * d.y - vdot(o, d);
+    float c = (o.x * o.x + o.z * o.z) + o.y * (2.0f * radius + o.y);
+    float h = b * b - a * c;
+    if (h >= 0.0f) {
+        float root = sqrtf(h);
+        float q = b + (b >= 0.0f ? root : -root);
+        if (q != 0.0f) {
+            float t0 = minf_(c / q, q / a);
+            float t1 = maxf_(c / q, q / a);
+            float distance = t0 > 0.001f ? t0 : t1;
+            if (distance > 0.001f && distance / METRES_PER_AU < closest.distance) {
+                if (occlusion) { hit_t r = {distance / METRES_PER_AU, LOCAL_BASE, {0, 0, 0}}; return r; }
+                v3 p = vadd(o, vmul(d, distance));
+                v3 n = vnormalize(V(p.x / radius, 1.0f + p.y / radius, p.z / radius));
+                closest.distance = distance / METRES_PER_AU;
+                closest.index = LOCAL_BASE;
+                closest.normal = from_ground(S, n);
+            }
+        }
+    }
+    if (S->s->g.ground_counts[1] != 0u && S->t && S->t->terrain) {
+        float tl = minf_(closest.distance, 1.0e18f) * METRES_PER_AU;
+        v3 tn = V(0, 0, 0);
+        float tt = t_query(S, S->t->terrain, t_cells(S), o, d, tl, occlusion, &tn);
+        if (tt < tl && tt < 1.0e29f) {
+            closest.distance = tt / METRES_PER_AU;
+            closest.index = TERRAIN_ID;
+            closest.normal = from_ground(S, tn);
+            if (occlusion) return closest;
+        }
+    }
+    const sg_primitive *objects = S->t ? S->t->ground : NULL;
+    uint32_t n_objects = S->s->g.ground_counts[0];
+    for (uint32_t i = 0; objects && i < n_objects; i++) {
+        const sg_primitive *object = &objects[i];
+        v3 center = V(object->center[0], object->center[1], object->center[2]);
+        v3 e = V(object->extent[0], object->extent[1], object->extent[2]);
+        float kind = object->center[3];
+        if (kind < 0.0f) {
+            float bn, bf_;
+            box_interval(vsub(o, center), d, e, &bn, &bf_);
+            if (bn > bf_ || bf_ <= 0.001f || bn / METRES_PER_AU > closest.distance) i += (uint32_t)(-kind);
+            continue;
+        }
+        v3 p = vsub(o, center), v = d;
+        v3 angles = V(0, 0, 0);
+        if (kind == 2.25f) {
+            angles = rock_angles(object->extent[3]);
+            p = rock_to_local(p, angles);
+            v = rock_to_local(v, angles);
+        } else {
+            p = rotate_north(p, -object->extent[3]);
+            v = rotate_north(v, -object->extent[3]);
+        }
+        float distance = 1.0e30f;
+        v3 n = V(0, 0, 0);
+        if (kind > 2.5f) {
+            continue; /* vegetation: rejected by check_frame */
+        } else if (kind > 1.5f) {
+            float bn, bf_;
+            box_interval(p, v, e, &bn, &bf_);
+            if (bn > bf_ || bf_ <= 0.001f || bn / METRES_PER_AU > closest.distance) continue;
+            distance = rock_hit(p, v, e, &n);
+        } else if (kind > 0.5f) {
+            v3 sp = V(p.x / e.x, p.y / e.y, p.z / e.z);
+            v3 sd = V(v.x / e.x, v.y / e.y, v.z / e.z);
+            float aa = vdot(sd, sd), bb = vdot(sp, sd), cc = vdot(sp, sp) - 1.0f;
+            float hh = bb * bb - aa * cc;
+            if (hh >= 0.0f) {
+                float root = sqrtf(hh);
+                distance = (-bb - root) / aa;
+                if (distance <= 0.001f) distance = (-bb + root) / aa;
+                v3 hp = vadd(p, vmul(v, distance));
+                n = vnormalize(V(hp.x / (e.x * e.x), hp.y / (e.y * e.y), hp.z / (e.z * e.z)));
+            }
+        } else {
+            float in_, out_;
+            box_interval(p, v, e, &in_, &out_);
+            if (in_ <= out_ && out_ > 0.001f) {
+                distance = in_ > 0.001f ? in_ : out_;
+                v3 hp = vadd(p, vmul(v, distance));
+                v3 point = V(hp.x / e.x, hp.y / e.y, hp.z / e.z);
+                v3 ap = V(fabsf(point.x), fabsf(point.y), fabsf(point.z));
+                float sx = point.x > 0 ? 1.0f : (point.x < 0 ? -1.0f : 0.0f);
+                float sy = point.y > 0 ? 1.0f : (point.y < 0 ? -1.0f : 0.0f);
+                float sz = point.z > 0 ? 1.0f : (point.z < 0 ? -1.0f : 0.0f);
+                if (ap.x >= ap.y && ap.x >= ap.z) n.x = sx;
+                else if (ap.y >= ap.z) n.y = sy;
+                else n.z = sz;
+            }
+        }
+        if (distance > 0.001f && distance < 1.0e29f && distance / METRES_PER_AU < closest.distance) {
+            if (occlusion) { hit_t r = {distance / METRES_PER_AU, LOCAL_BASE + 1u + i, {0, 0, 0}}; return r; }
+            if (kind == 2.25f) n = rock_from_local(n, angles);
+            else n = rotate_north(n, object->extent[3]);
+            closest.distance = distance / METRES_PER_AU;
+            closest.index = LOCAL_BASE + 1u + i;
+            closest.normal = from_ground(S, n);
+        }
+    }
+    return closest;
+}
+
+/* landscape_point: ground.wgsl:252-254 */
+static v3 landscape_point(const scene *S, ray_t ray, hit_t hit) {
+    return vadd(ground_origin(S, ray), vmul(to_ground(S, ray.dir), hit.distance * METRES_PER_AU));
+}
+
+static float smooth_footprint(const scene *S, float distance) {
+    return distance * 2.0f * S->s->g.cam_forward[3] / maxf_(S->s->g.viewport[1], 1.0f);
+}
+
+/* forest_floor, desert_floor, crater_floor: ground.wgsl:256-317 */
+static v3 v3mix(v3 a, v3 b, float t) { return V(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
+static v3 forest_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float broad = vnoise(vadd(vmul(p, 0.045f), V(7.0f, 0.0f, 13.0f)));
+    float middle = vnoise(vmul(p, 0.7f));
+    float grain = vnoise(vmul(p, 18.0f));
+    float footprint = smooth_footprint(S, distance);
+    float detail = 1.0f - smoothstepf(0.006f, 0.055f, footprint);
+    v3 moss = v3mix(V(0.028f, 0.054f, 0.014f), V(0.105f, 0.14f, 0.039f), middle);
+    v3 earth = v3mix(V(0.055f, 0.029f, 0.013f), V(0.17f, 0.115f, 0.057f), middle);
+    v3 color = v3mix(earth, moss, smoothstepf(0.35f, 0.63f, broad));
+    float needles = powf(maxf_(0.0f, sinf(p.x * 92.0f + p.z * 137.0f + middle * 7.0f)), 18.0f) *
+                    smoothstepf(0.50f, 0.68f, grain);
+    color = v3mix(color, V(0.22f, 0.145f, 0.067f), needles * detail * 0.5f);
+    color = vmul(color, 1.0f + (grain - 0.5f) * 0.38f * detail);
+    float slope = 1.0f - maxf_(normal.y, 0.0f);
+    v3 stone = v3mix(V(0.095f, 0.105f, 0.10f), V(0.24f, 0.23f, 0.20f), middle);
+    color = v3mix(color, stone, smoothstepf(0.10f, 0.43f, slope + (broad - 0.5f) * 0.17f));
+    float center = 2.0f + 0.30f * p.z + 2.0f * sinf(p.z * 0.055f);
+    float edge = fabsf(p.x - center) + (middle - 0.5f) * 0.55f;
+    float path = (1.0f - smoothstepf(0.8f, 2.1f, edge)) * (1.0f - smoothstepf(45.0f, 95.0f, p.z)) *
+                 smoothstepf(-10.0f, 0.0f, p.z);
+    v3 gravel = v3mix(V(0.12f, 0.095f, 0.062f), V(0.26f, 0.23f, 0.17f), grain * detail + 0.5f * (1.0f - detail));
+    return v3mix(color, gravel, path * 0.85f);
+}
+static v3 desert_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float broad = vnoise(vadd(vmul(p, 0.007f), V(19.0f, 2.0f, 4.0f)));
+    float gravel = vnoise(vmul(p, 2.8f));
+    float footprint = smooth_footprint(S, distance);
+    float detail = 1.0f - smoothstepf(0.025f, 0.2f, footprint);
+    v3 sand = v3mix(V(0.31f, 0.21f, 0.125f), V(0.53f, 0.40f, 0.26f), broad);
+    v3 rock = v3mix(V(0.18f, 0.10f, 0.055f), V(0.38f, 0.245f, 0.145f), broad);
+    v3 color = v3mix(sand, rock, smoothstepf(0.08f, 0.4f, 1.0f - maxf_(normal.y, 0.0f)));
+    color = vmul(color, 1.0f + (gravel - 0.5f) * 0.32f * detail);
+    float center = 2.8f + 0.55f * sinf(p.z / 38.0f) + 1.4f * sinf(p.z / 210.0f);
+    float edge = fabsf(p.x - center);
+    float aa = maxf_(0.015f, footprint * 0.5f);
+    float fade = (1.0f - smoothstepf(0.25f, 0.9f, footprint)) * (1.0f - smoothstepf(1000.0f, 2200.0f, fabsf(p.z))) *
+                 (1.0f - smoothstepf(0.12f, 0.35f, 1.0f - maxf_(normal.y, 0.0f)));
+    float worn = 1.0f - smoothstepf(0.8f, 1.2f, edge);
+    float rut_edge = fabsf(edge - 0.68f) + (gravel - 0.5f) * 0.1f * detail;
+    float tracks = 1.0f - smoothstepf(0.12f - aa, 0.23f + aa, rut_edge);
+    v3 packed = vmul(sand, 0.72f + 0.10f * gravel * detail);
+    color = v3mix(color, vmul(sand, 0.93f), worn * fade * 0.35f);
+    return v3mix(color, packed, tracks * fade * 0.8f);
+}
+static v3 crater_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float broad = vnoise(vadd(vmul(p, 0.004f), V(3.0f, 0.0f, 8.0f)));
+    float middle = vnoise(vmul(p, 0.09f));
+    float grain = vnoise(vmul(p, 3.1f));
+    float footprint = smooth_footprint(S, distance);
+    float detail = 1.0f - smoothstepf(0.025f, 0.2f, footprint);
+    float tone = mixf(0.11f, 0.21f, broad) * (0.86f + 0.28f * middle);
+    tone *= 1.0f + 0.35f * smoothstepf(0.15f, 0.5f, 1.0f - maxf_(normal.y, 0.0f));
+    tone *= 1.0f + (grain - 0.5f) * 0.3f * detail;
+    return V(tone, tone * 0.97f, tone * 0.93f);
+}
+
+/* Albedo-map extension: nearest texel at surface-frame (x, z). */
+static float map_albedo(const scene *S, v3 p) {
+    const oracle_tables *t = S->t;
+    float u = (p.x / t->map_extent + 1.0f) * 0.5f * (float)t->map_width;
+    float w = (p.z / t->map_extent + 1.0f) * 0.5f * (float)t->map_height;
+    int32_t i = (int32_t)floorf(u), j = (int32_t)floorf(w);
+    if (i < 0) i = 0;
+    if (j < 0) j = 0;
+    if (i > (int32_t)t->map_width - 1) i = (int32_t)t->map_width - 1;
+    if (j > (int32_t)t->map_height - 1) j = (int32_t)t->map_height - 1;
+    return t->albedo_map[(size_t)j * t->map_width + (size_t)i];
+}
+
+/* landscape_albedo: ground.wgsl:597-632 (themes 0-2; vegetation kinds are
+ * rejected), with the albedo-map extension for the ground itself. */
+static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
+    v3 p = landscape_point(S, ray, hit);
+    float distance = hit.distance * METRES_PER_AU;
+    v3 n = to_ground(S, hit.normal);
+    if (hit.index == LOCAL_BASE || hit.index == TERRAIN_ID) {
+        if (S->t && S->t->albedo_map) { float a = map_albedo(S, p); return V(a, a, a); }
+        switch (ground_theme(S)) {
+            case 1u: return desert_floor(S, p, distance, n);
+            case 2u: return crater_floor(S, p, distance, n);
+            default: return forest_floor(S, p, distance, n);
+        }
+    }
+    const sg_primitive *object = &S->t->ground[hit.index - LOCAL_BASE - 1u];
+    v3 tint = V(object->albedo[0], object->albedo[1], object->albedo[2]);
+    float kind = object->albedo[3];
+    if (kind == 0.0f) return tint;
+    float middle = vnoise(vmul(p, 1.7f));
+    float fine = mixf(vnoise(vmul(p, 12.0f)), 0.5f, smoothstepf(18.0f, 110.0f, distance));
+    if (kind > 4.5f) return vmul(tint, 0.65f + 0.6f * middle);
+    float strata = sinf(p.y * 8.0f + 2.5f * middle);
+    float lichen = smoothstepf(0.52f, 0.76f, middle) * maxf_(n.y, 0.0f);
+    v3 stone = vmul(tint, 0.7f + 0.45f * fine + 0.07f * strata);
+    if (ground_theme(S) != 0u) return stone;
+    return v3mix(stone, V(0.11f, 0.145f, 0.037f), lichen * 0.65f);
+}
+
+/* landscape_shading_normal: ground.wgsl:633-648 (themes 0-2) */
+static v3 landscape_shading_normal(const scene *S, ray_t ray, hit_t hit) {
+    if (hit.index != LOCAL_BASE && hit.index != TERRAIN_ID) return hit.normal;
+    v3 p = landscape_point(S, ray, hit);
+    float distance = hit.distance * METRES_PER_AU;
+    float strength = 0.11f * (1.0f - smoothstepf(8.0f, 65.0f, distance));
+    float dx = vnoise(vmul(vadd(p, V(0.025f, 0.0f, 0.0f)), 6.0f)) - vnoise(vmul(vsub(p, V(0.025f, 0.0f, 0.0f)), 6.0f));
+    float dz = vnoise(vmul(vadd(p, V(0.0f, 0.0f, 0.025f)), 6.0f)) - vnoise(vmul(vsub(p, V(0.0f, 0.0f, 0.025f)), 6.0f));
+    return vnormalize(vadd(hit.normal, vmul(from_ground(S, V(-dx, 0.0f, -dz)), strength)));
+}
+
+/* landscape_outgoing: ground.wgsl:649-662 */
+static ray_t landscape_outgoing(const scene *S, ray_t ray, hit_t hit) {
+    v3 p = landscape_point(S, ray, hit);
+    if (hit.index == LOCAL_BASE) {
+        float radius = S->s->g.ground_up[3];
+        float d2 = p.x * p.x + p.z * p.z;
+        if (p.y > -radius && d2 < radius * radius) p.y = -d2 / (radius + sqrtf(radius * radius - d2));
+    }
+    p = vadd(p, vmul(to_ground(S, hit.normal), 0.005f));
+    p.y -= S->s->g.ground_east[3];
+    ray_t r;
+    r.offset = vdivs(from_ground(S, p), METRES_PER_AU);
+    r.dir = hit.normal;
+    r.anchor = MISS;
+    return r;
+}
+
+/* ---------------------------------------------------------------- */
+/* trace: pathtrace.wgsl:1347-1617 (airless)                         */
 /* ---------------------------------------------------------------- */
 static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
     const sg_settings *st = S->s;
@@ -577,10 +1185,10 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
              * bound, so both contribute zero radiance (pathtrace.wgsl:1494-1508). */
             break;
         }
-        /* hit.index < LOCAL_BASE: the landscape is off. */
+        int local = hit.index >= LOCAL_BASE;
         uint32_t bi = hit.index;
         throughput = vmul(throughput, disc_scale);
-        if (b_emissive(S, bi) > 0.5f) {
+        if (!local && b_emissive(S, bi) > 0.5f) {
             float weight = 1.0f;
             if (depth > 0u) {
                 float light_pdf = 1.0f / (TAU_F * cone_width(S, previous_vertex, hit.index));
@@ -590,16 +1198,20 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
             break;
         }
         EV(surface_events);
-        if (depth == 0u && !point_gained && st->background[3] > 0.0f) {
+        if (!local && depth == 0u && !point_gained && st->background[3] > 0.0f) {
             point_gained = 1;
             float extent = S->b[bi].radius * maxf_(1.0f, S->b[bi].ring_params[0]);
             throughput = vmul(throughput, point_gain(S, extent, hit.distance));
         }
-        v3 normal = hit.normal;
+        v3 normal = local ? landscape_shading_normal(S, ray, hit) : hit.normal;
         ray_t outgoing;
-        outgoing.offset = vmul(normal, S->b[bi].radius * (1.0f + 2.0e-6f));
-        outgoing.dir = normal;
-        outgoing.anchor = hit.index;
+        if (local) {
+            outgoing = landscape_outgoing(S, ray, hit);
+        } else {
+            outgoing.offset = vmul(normal, S->b[bi].radius * (1.0f + 2.0e-6f));
+            outgoing.dir = normal;
+            outgoing.anchor = hit.index;
+        }
         v3 direct_light = V(0, 0, 0);
         int last_vertex = depth + 1u == st->counts[3];
         uint32_t count = light_count(S);
@@ -619,12 +1231,15 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 direct_light = vadd(direct_light, vmul(b_color(S, i), bsdf_pdf * weight * visibility / sample.pdf));
             }
         }
-        v3 albedo = surface_albedo(S, bi, normal);
+        v3 albedo = local ? landscape_albedo(S, ray, hit) : surface_albedo(S, bi, normal);
         radiance = vadd(radiance, vmulv(vmulv(throughput, albedo), direct_light));
         shine_body = MISS;
-        radiance = vadd(radiance, vmulv(vmulv(throughput, albedo),
-                                        ringshine(S, hit.index, outgoing.offset, normal, last_vertex, rng)));
-        shine_body = hit.index;
+        if (!local) {
+            radiance = vadd(radiance, vmulv(vmulv(throughput, albedo),
+                                            ringshine(S, hit.index, outgoing.offset, normal, last_vertex, rng)));
+            shine_body = hit.index;
+        }
+        /* sky_lit needs the host atmosphere (pathtrace.wgsl:1578-1584): off. */
         if (last_vertex) break;
         float u = rnd(S, rng);
         float phi = TAU_F * rnd(S, rng);
@@ -665,13 +1280,22 @@ static v3 camera_direction(const scene *S, uint32_t x, uint32_t y, uint32_t *rng
     return vnormalize(V(ndc_x * tangent * S->s->g.viewport[3], ndc_y * tangent, -1.0f));
 }
 
-static int check_frame(const sg_settings *s) {
+/* Frames the restatement covers: no host atmosphere; landscape themes 0-2;
+ * no vegetation primitives; terrain only with a terrain table. */
+static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
     if (!s) return SG_ERR_INVALID;
     if (s->g.atmo_params[3] >= 0.5f) return SG_ERR_INVALID;
-    if (s->g.ground_north[3] != 0.0f) return SG_ERR_INVALID;
     if (s->counts[0] > SG_BODY_CAPACITY) return SG_ERR_CAPACITY;
+    if (s->g.ground_north[3] != 0.0f) {
+        if ((s->g.ground_counts[2] & 255u) > 2u) return SG_ERR_INVALID;
+        if (s->g.ground_counts[1] != 0u && (!t || !t->terrain)) return SG_ERR_INVALID;
+        if (s->g.ground_counts[0] > 0u && (!t || !t->ground || t->n_ground < s->g.ground_counts[0])) return SG_ERR_INVALID;
+        for (uint32_t i = 0; t && t->ground && i < s->g.ground_counts[0]; i++)
+            if (t->ground[i].center[3] > 2.5f) return SG_ERR_INVALID;
+    }
     return SG_OK;
 }
+#define check_frame(s) check_frame_t((s), tables)
 
 static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4]) {
     uint32_t width = (uint32_t)S->s->g.viewport[0];

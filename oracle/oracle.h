@@ -25,11 +25,38 @@
 extern "C" {
 #endif
 
-/* Extension tables the oracle shares with the CUDA path. */
+/* Scene data beyond the body table, shared with the CUDA path. */
 typedef struct oracle_tables {
     const float *ring_tau[SG_RING_TABLE_SLOTS];
     uint32_t ring_bins[SG_RING_TABLE_SLOTS];
+    /* Heightfield in the reference layout (src/shaders/terrain.wgsl:1-20):
+     * heights, [x/z derivatives], min/max per quadtree node, node AABBs,
+     * vertex cache. NULL disables terrain. The cache part is filled by
+     * oracle_cache_terrain. */
+    const float *terrain;
+    uint32_t terrain_cells;
+    /* Landscape primitives of the frame (ground.wgsl:3-12). */
+    const sg_primitive *ground;
+    uint32_t n_ground;
+    /* Extension: scalar albedo map over the surface frame, texel (i, j)
+     * covers x, z in [-extent, extent]; NULL uses the theme floor. */
+    const float *albedo_map;
+    uint32_t map_width, map_height;
+    float map_extent;
 } oracle_tables;
+
+/* Floats of the reference terrain layout for `cells` cells per side
+ * (terrain.wgsl:6-20): everything up to and including the vertex cache. */
+size_t oracle_terrain_floats(uint32_t cells);
+
+/* cache_terrain_geometry (terrain.wgsl:242-285) for host radius
+ * `radius_m`: fills the node AABBs and the vertex cache of `terrain`. */
+int oracle_cache_terrain(float *terrain, uint32_t cells, float radius_m);
+
+/* terrain_query (terrain.wgsl:152-234) in the surface frame: out =
+ * (normal xyz, distance), distance 1e30 on a miss. */
+int oracle_terrain_query(const sg_settings *settings, const oracle_tables *tables, const float o[3],
+                         const float d[3], float limit, int occlusion, float out[4]);
 
 /* Per-sample event counters (used to pin the CUDA event counts). */
 typedef struct oracle_events {

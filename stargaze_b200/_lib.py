@@ -32,10 +32,13 @@ _SIGNATURES = {
     "sg_set_accumulation": (C.c_int, [_P, _P, C.c_int, C.c_uint32, C.c_uint32, _P]),
     "sg_accumulation_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "sg_upload_ring_profile": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32]),
+    "sg_upload_terrain": (C.c_int, [_P, _P, C.c_size_t, C.c_uint32]),
+    "sg_upload_albedo_map": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_float]),
     "sg_closest_hit": (C.c_int, [_P, C.POINTER(abi.FrameView), _P, C.c_uint32, _P, C.c_int, _P]),
     "sg_light_visibility": (C.c_int, [_P, C.POINTER(abi.FrameView), _P, _P, C.c_uint32, _P, C.c_int, _P]),
     "sg_ring_probe": (C.c_int, [_P, C.POINTER(abi.FrameView), _P, C.c_uint32, C.c_uint32, _P, C.c_int, _P]),
     "sg_ring_energy": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_uint32, C.POINTER(C.c_float)]),
+    "sg_terrain_probe": (C.c_int, [_P, C.POINTER(abi.FrameView), _P, C.c_uint32, _P, C.c_int, _P]),
     "sg_last_error": (C.c_char_p, [_P]),
     "sg_status_string": (C.c_char_p, [C.c_int]),
     "sg_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/stargaze_b200.h"
+#include "sg_internal.h"
 
 // Call attribute of the multi-site helpers (sample_light, light_visibility,
 // ring_bsdf, ringshine, point_disc_hit): out of line by default.
@@ -125,7 +126,7 @@ struct Events {
 };
 
 // Counting is compiled out of the production variant (C == false).
-template <bool C>
+template <bool C, bool L>
 struct Counter {
     Events *ev;
     __device__ __forceinline__ void add(uint32_t Events::*f) const {
@@ -133,8 +134,8 @@ struct Counter {
     }
 };
 
-template <bool C>
-__device__ __forceinline__ float rnd(Counter<C> K, uint32_t &state) {
+template <bool C, bool L>
+__device__ __forceinline__ float rnd(Counter<C, L> K, uint32_t &state) {
     K.add(&Events::rng_draws);
     state = state * 747796405u + 2891336453u;
     const uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
@@ -145,11 +146,10 @@ __device__ __forceinline__ float rnd(Counter<C> K, uint32_t &state) {
 // Scene view inside a CTA
 // ---------------------------------------------------------------------------
 struct Scene {
-    const sg_settings *s;   // kernel parameter space
+    const TraceParams *p;   // the launch's parameters (kernel parameter space)
+    const sg_settings *s;   // &p->s
     const float4 *B;        // staged bodies, kBodyVec4 float4 each
     const float *tables;    // ring optical-depth tables (slot-major)
-    const uint32_t *bins;   // bins per slot
-    uint32_t table_stride;  // floats between slots
 };
 
 struct Ray {
@@ -175,8 +175,8 @@ __device__ __forceinline__ float3 relative_center(const Scene &S, const Ray &r, 
 // Distance part of sphere_hit_radius (pathtrace.wgsl:134-166). Returns the
 // hit distance (1e30 on a miss) and the signed root offset `delta` that the
 // normal needs.
-template <bool C>
-__device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C> K, const Ray &r, uint32_t i,
+template <bool C, bool L>
+__device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t i,
                                                  float radius, float &delta) {
     K.add(&Events::sphere_tests);
     const float3 oc = relative_center(S, r, i);
@@ -215,14 +215,25 @@ __device__ __forceinline__ float3 sphere_normal(const Scene &S, const Ray &r, ui
 struct Hit {
     float t;
     uint32_t index;
-    float delta;
+    float delta;  // sphere root offset (body hits)
+    float3 n;     // telescope-space normal (local landscape hits)
 };
 
-// closest_hit (pathtrace.wgsl:173-185). The local landscape is disabled in
-// the frames this build accepts (ground_north.w == 0).
-template <bool C>
-__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C> K, const Ray &r) {
-    Hit best{1.0e30f, kMiss, 0.0f};
+// Result of landscape_query (ground.wgsl:123-242; sg_landscape.cuh).
+struct LandHit {
+    float t;
+    uint32_t index;
+    float delta;  // root offset when the distant path returns the host sphere
+    float3 n;
+};
+template <bool C, bool L>
+__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L> K, Ray ray, float limit, bool occlusion);
+
+// closest_hit (pathtrace.wgsl:173-185): every body except the landscape
+// host, then the landscape.
+template <bool C, bool L>
+__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C, L> K, const Ray &r) {
+    Hit best{1.0e30f, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
     const float host = S.s->g.ground_north[3];
 #pragma unroll 1
@@ -230,7 +241,13 @@ __device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C> K, const R
         if (host == (float)(i + 1u)) continue;
         float delta;
         const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
-        if (t < best.t) best = Hit{t, i, delta};
+        if (t < best.t) best = Hit{t, i, delta, f3(0.0f, 0.0f, 0.0f)};
+    }
+    if constexpr (L) {
+        if (host != 0.0f) {
+            const LandHit local = landscape_query(S, K, r, 1.0e30f, false);
+            if (local.t < best.t) best = Hit{local.t, local.index, local.delta, local.n};
+        }
     }
     return best;
 }
@@ -262,8 +279,8 @@ struct LightSample {
 };
 
 // sample_light (pathtrace.wgsl:214-234), one stratum: uniform cone sampling.
-template <bool C>
-__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C> K, Ray r, uint32_t i, uint32_t rng) {
+template <bool C, bool L>
+__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C, L> K, Ray r, uint32_t i, uint32_t rng) {
     K.add(&Events::light_samples);
     const float3 oc = relative_center(S, r, i);
     const float3 axis = normalize(oc);
@@ -302,8 +319,8 @@ __device__ __forceinline__ bool has_ring(const Scene &S, uint32_t i) {
 }
 
 // ring_hit (rings.wgsl:8-34), strict.
-template <bool C>
-__device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C> K, const Ray &r, uint32_t i) {
+template <bool C, bool L>
+__device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t i) {
     const RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const float4 plane = bf(S, i, kRingPlane);
     const float4 params = bf(S, i, kRingParams);
@@ -325,8 +342,8 @@ __device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C> K, const 
 }
 
 // closest_ring (rings.wgsl:36-45).
-template <bool C>
-__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C> K, const Ray &r, float limit) {
+template <bool C, bool L>
+__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C, L> K, const Ray &r, float limit) {
     RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
 #pragma unroll 1
@@ -390,9 +407,9 @@ __device__ __forceinline__ Optics ring_optics(const Scene &S, uint32_t i, float3
     const float3 color = xyz(bf(S, i, kRingColor));
     if (params.w >= 0.5f) {
         const uint32_t slot = (uint32_t)params.w - 1u;
-        const uint32_t bins = slot < SG_RING_TABLE_SLOTS ? S.bins[slot] : 0u;
+        const uint32_t bins = slot < SG_RING_TABLE_SLOTS ? S.p->bins[slot] : 0u;
         if (bins == 0u) return Optics{color, 0.0f};
-        return Optics{color, tau * S.tables[slot * S.table_stride + ring_bin(x, bins)]};
+        return Optics{color, tau * S.tables[slot * S.p->table_stride + ring_bin(x, bins)]};
     }
     if (params.z > 0.5f) return banded_optics(x, tau, color);
     return Optics{color, tau};
@@ -413,8 +430,8 @@ __device__ __forceinline__ float ring_transmission(const Scene &S, const Ray &r,
 // light_visibility (rings.wgsl:90-115): distance to the light, any-hit over
 // the other spheres (ties broken by index), then ring transmissions before
 // the light.
-template <bool C>
-__device__ SG_HELPER float light_visibility(Scene S, Counter<C> K, Ray r, uint32_t light) {
+template <bool C, bool L>
+__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
     K.add(&Events::shadow_rays);
     float delta;
     const float surface = sphere_distance(S, K, r, light, b_radius(S, light), delta);
@@ -427,6 +444,12 @@ __device__ SG_HELPER float light_visibility(Scene S, Counter<C> K, Ray r, uint32
         if (i == light || host == (float)(i + 1u)) continue;
         const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
         if (t < 1.0e30f && (t < surface || (t == surface && i < light))) return 0.0f;
+    }
+    if constexpr (L) {
+        if (host != 0.0f) {
+            const LandHit local = landscape_query(S, K, r, surface, true);
+            if (local.index != kMiss && local.t < surface) return 0.0f;
+        }
     }
     float transmission = 1.0f;
 #pragma unroll 1
@@ -482,8 +505,8 @@ struct Shine {
 };
 
 // ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
-template <bool C>
-__device__ SG_HELPER Shine ringshine(Scene S, Counter<C> K, uint32_t index, float3 origin, float3 normal,
+template <bool C, bool L>
+__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
                                         bool last_vertex, uint32_t rng) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     if (!has_ring(S, index)) return Shine{zero, rng};
@@ -540,8 +563,8 @@ struct DiscHit {
 
 // point_disc_hit (pathtrace.wgsl:1308-1333): depth-0 camera rays see an
 // unresolved body as a disc of at least a bright star's size.
-template <bool C>
-__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C> K, Ray r, Hit closest, uint32_t rng) {
+template <bool C, bool L>
+__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L> K, Ray r, Hit closest, uint32_t rng) {
     const sg_settings *s = S.s;
     DiscHit out{closest, 1.0f, rng};
     float total = 0.0f;
@@ -560,7 +583,7 @@ __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C> K, Ray r, Hit cl
         if (t < closest.t) {
             const float ratio = (radius / drawn) * (radius / drawn);
             total += ratio;
-            if (rnd(K, out.rng) * total < ratio) out.hit = Hit{t, i, delta};
+            if (rnd(K, out.rng) * total < ratio) out.hit = Hit{t, i, delta, f3(0.0f, 0.0f, 0.0f)};
         }
     }
     if (total > 0.0f) out.scale = total;
@@ -571,34 +594,42 @@ __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C> K, Ray r, Hit cl
 // Surface albedo, style 0 with optional value-noise mottle
 // (pathtrace.wgsl:338-354, :377-389, :897-925).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float fractf(float x) { return x - floorf(x); }
-__device__ __forceinline__ float hash31(float3 p) {
-    float3 q = f3(fractf(p.x * 0.1031f), fractf(p.y * 0.1030f), fractf(p.z * 0.0973f));
-    const float d = dot(q, f3(q.y + 33.33f, q.x + 33.33f, q.z + 33.33f));
-    q = f3(q.x + d, q.y + d, q.z + d);
-    return fractf((q.x + q.y) * q.z);
+// Value noise is strict: fract() of scaled coordinates amplifies any
+// contraction difference into a different lattice hash, so the noise is
+// evaluated exactly as an IEEE reading of the WGSL.
+__device__ __forceinline__ float fractf(float x) { return __fsub_rn(x, floorf(x)); }
+__device__ __forceinline__ float mix_rn(float a, float b, float t) {
+    return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t));
 }
-__device__ __forceinline__ float vnoise(float3 p) {
+__device__ __forceinline__ float hash31(float3 p) {
+    float3 q = f3(fractf(__fmul_rn(p.x, 0.1031f)), fractf(__fmul_rn(p.y, 0.1030f)), fractf(__fmul_rn(p.z, 0.0973f)));
+    const float d = dot_rn(q, f3(__fadd_rn(q.y, 33.33f), __fadd_rn(q.x, 33.33f), __fadd_rn(q.z, 33.33f)));
+    q = f3(__fadd_rn(q.x, d), __fadd_rn(q.y, d), __fadd_rn(q.z, d));
+    return fractf(__fmul_rn(__fadd_rn(q.x, q.y), q.z));
+}
+__device__ __forceinline__ float smooth_rn(float f) {
+    return __fmul_rn(__fmul_rn(f, f), __fsub_rn(3.0f, __fmul_rn(2.0f, f)));
+}
+__device__ __noinline__ float vnoise(float3 p) {
     const float3 i = f3(floorf(p.x), floorf(p.y), floorf(p.z));
-    const float3 f = p - i;
-    const float3 u = f3(f.x * f.x * (3.0f - 2.0f * f.x), f.y * f.y * (3.0f - 2.0f * f.y),
-                        f.z * f.z * (3.0f - 2.0f * f.z));
-    const float a = mixf(hash31(i), hash31(i + f3(1, 0, 0)), u.x);
-    const float b = mixf(hash31(i + f3(0, 1, 0)), hash31(i + f3(1, 1, 0)), u.x);
-    const float c = mixf(hash31(i + f3(0, 0, 1)), hash31(i + f3(1, 0, 1)), u.x);
-    const float d = mixf(hash31(i + f3(0, 1, 1)), hash31(i + f3(1, 1, 1)), u.x);
-    return mixf(mixf(a, b, u.y), mixf(c, d, u.y), u.z);
+    const float3 f = sub_rn(p, i);
+    const float3 u = f3(smooth_rn(f.x), smooth_rn(f.y), smooth_rn(f.z));
+    const float a = mix_rn(hash31(i), hash31(add_rn(i, f3(1, 0, 0))), u.x);
+    const float b = mix_rn(hash31(add_rn(i, f3(0, 1, 0))), hash31(add_rn(i, f3(1, 1, 0))), u.x);
+    const float c = mix_rn(hash31(add_rn(i, f3(0, 0, 1))), hash31(add_rn(i, f3(1, 0, 1))), u.x);
+    const float d = mix_rn(hash31(add_rn(i, f3(0, 1, 1))), hash31(add_rn(i, f3(1, 1, 1))), u.x);
+    return mix_rn(mix_rn(a, b, u.y), mix_rn(c, d, u.y), u.z);
 }
 
 // Mottle factor of surface_albedo (pathtrace.wgsl:912-923), out of line:
 // five octaves of value noise that the constant-albedo path never runs.
 __device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float strength, float3 normal) {
     const float3 y = xyz(axis_y);
-    const float3 local = f3(dot(normal, axis_x), dot(normal, y), dot(normal, cross(axis_x, y)));
+    const float3 local = f3(dot_rn(normal, axis_x), dot_rn(normal, y), dot_rn(normal, cross_rn(axis_x, y)));
     const float seed = axis_y.w;
     const float3 off =
         f3(hash31(f3(seed, 1.0f, 7.0f)), hash31(f3(3.0f, seed, 5.0f)), hash31(f3(9.0f, 2.0f, seed))) * 512.0f;
-    float3 p = local * 2.4f + off;
+    float3 p = add_rn(mul_rn(local, 2.4f), off);
     float amplitude = 0.5f, noise = 0.0f;
     for (int octave = 0; octave < 5; ++octave) {
         noise += amplitude * vnoise(p);

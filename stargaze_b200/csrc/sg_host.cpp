@@ -60,6 +60,17 @@ struct sg_context {
     size_t scratch_bytes = 0;
     uint64_t launches = 0;
     std::string last_error;
+    // Local landscape.
+    sg_primitive *props = nullptr;  // SG_PROP_CAPACITY
+    float4 *prop_trig = nullptr;    // 2 float4 per prop
+    std::vector<float4> trig_host;
+    float *terrain = nullptr;       // full layout incl. the geometry cache
+    uint32_t terrain_cells = 0;
+    bool terrain_cached = false;
+    float terrain_radius = 0.0f;    // host radius the cache was built for
+    float *albedo_map = nullptr;
+    uint32_t map_width = 0, map_height = 0;
+    float map_extent = 0.0f;
 };
 
 namespace {
@@ -156,14 +167,30 @@ int validate_frame(sg_context *ctx, const sg_frame *frame) {
     if (!frame || !frame->globals) return fail(ctx, SG_ERR_INVALID, "frame or frame->globals is NULL");
     if (frame->n_bodies > SG_BODY_CAPACITY) return fail(ctx, SG_ERR_CAPACITY, "too many scene bodies");
     if (frame->n_bodies && !frame->bodies) return fail(ctx, SG_ERR_INVALID, "frame->bodies is NULL");
-    if (frame->n_ground > SG_GROUND_CAPACITY) return fail(ctx, SG_ERR_CAPACITY, "too many local primitives");
+    if (frame->n_ground > SG_PROP_CAPACITY) return fail(ctx, SG_ERR_CAPACITY, "too many local primitives");
     if (frame->n_ground && !frame->ground) return fail(ctx, SG_ERR_INVALID, "frame->ground is NULL");
     if (frame->globals->ground_counts[0] != frame->n_ground)
         return fail(ctx, SG_ERR_INVALID, "ground_counts.x does not match the primitive count");
     if (frame->globals->atmo_params[3] >= 0.5f)
         return fail(ctx, SG_ERR_INVALID, "the host atmosphere (atmo_params.w >= 0.5) is not implemented");
-    if (frame->globals->ground_north[3] != 0.0f)
-        return fail(ctx, SG_ERR_INVALID, "the local landscape (ground_north.w != 0) is not implemented");
+    const float host = frame->globals->ground_north[3];
+    if (host != 0.0f) {
+        if (host != std::floor(host) || host < 1.0f || host > (float)frame->n_bodies)
+            return fail(ctx, SG_ERR_INVALID, "ground_north.w must be 0 or a body index + 1");
+        if ((frame->globals->ground_counts[2] & 255u) > 2u)
+            return fail(ctx, SG_ERR_INVALID, "landscape themes 3-5 (alpine, basalt, dunes) are not implemented");
+        if (frame->globals->ground_counts[1] != 0u && !ctx->terrain)
+            return fail(ctx, SG_ERR_STATE, "terrain is enabled but no terrain was uploaded");
+        if (!(frame->globals->ground_up[3] > 0.0f))
+            return fail(ctx, SG_ERR_INVALID, "ground_up.w (host radius in metres) must be positive");
+        for (uint32_t i = 0; i < frame->n_ground; ++i) {
+            const float kind = frame->ground[i].center[3];
+            if (kind > 2.5f)
+                return fail(ctx, SG_ERR_INVALID, "vegetation primitives (kind > 2.5) are not implemented");
+            if (kind < 0.0f && (kind != std::floor(kind) || (double)i - (double)kind >= (double)frame->n_ground + 1.0))
+                return fail(ctx, SG_ERR_INVALID, "a group marker skips past the end of the primitive list");
+        }
+    }
     for (uint32_t i = 0; i < frame->n_bodies; ++i) {
         const float slot = frame->bodies[i].ring_params[3];
         if (slot >= 0.5f && (slot > (float)SG_RING_TABLE_SLOTS || slot != std::floor(slot)))
@@ -188,9 +215,12 @@ sg_settings pack_settings(const sg_context *ctx, const sg_frame *frame, uint32_t
         prop_top = std::max(prop_top, frame->ground[i].center[1] + len);
     }
     std::memcpy(&s.g.ground_counts[3], &prop_top, sizeof(float));
-    uint32_t cells = kDefaultTerrainCells, log2 = 0;
+    uint32_t cells = ctx->terrain_cells ? ctx->terrain_cells : kDefaultTerrainCells, log2 = 0;
     while ((1u << log2) < cells) ++log2;
-    s.g.ground_counts[2] |= log2 << 8;
+    // The reference ORs log2(cells) over the theme byte; stale grid bits in
+    // the caller's frame are cleared first so they cannot name a grid that
+    // was not uploaded.
+    s.g.ground_counts[2] = (s.g.ground_counts[2] & 255u) | (log2 << 8);
     for (uint32_t i = 0; i < frame->n_bodies; ++i) {
         if (frame->bodies[i].emissive >= 0.5f) {
             if (s.lights[3] < 3u) s.lights[s.lights[3]] = i;
@@ -209,10 +239,52 @@ sg_settings pack_settings(const sg_context *ctx, const sg_frame *frame, uint32_t
     return s;
 }
 
+// Write the frame's bodies and landscape primitives (src/pathtracer.rs:
+// 907-913) and refresh the terrain geometry cache when the host radius
+// changed (:933-945).
 int upload_bodies(sg_context *ctx, const sg_frame *frame, cudaStream_t stream) {
-    if (frame->n_bodies == 0) return SG_OK;
-    SG_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, frame->bodies, frame->n_bodies * sizeof(sg_sphere),
-                                 cudaMemcpyHostToDevice, stream));
+    if (frame->n_bodies)
+        SG_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, frame->bodies, frame->n_bodies * sizeof(sg_sphere),
+                                     cudaMemcpyHostToDevice, stream));
+    if (frame->globals->ground_north[3] == 0.0f) return SG_OK;
+    if (frame->n_ground) {
+        if (!ctx->props) SG_CUDA(ctx, cudaMalloc(&ctx->props, SG_PROP_CAPACITY * sizeof(sg_primitive)));
+        if (!ctx->prop_trig) SG_CUDA(ctx, cudaMalloc(&ctx->prop_trig, SG_PROP_CAPACITY * 2 * sizeof(float4)));
+        SG_CUDA(ctx, cudaMemcpyAsync(ctx->props, frame->ground, frame->n_ground * sizeof(sg_primitive),
+                                     cudaMemcpyHostToDevice, stream));
+        // Rotation sines and cosines per primitive (ground.wgsl:33-61): the
+        // tumble angles of kind 2.25 (24 packed bits, TAU/256 steps) or the
+        // yaw, each evaluated in double and rounded to f32 once per frame.
+        ctx->trig_host.resize((size_t)frame->n_ground * 2);
+        const float step = 6.283185307179586f / 256.0f;
+        for (uint32_t i = 0; i < frame->n_ground; ++i) {
+            const sg_primitive &p = frame->ground[i];
+            float4 t0 = make_float4(0.0f, 1.0f, 0.0f, 1.0f), t1 = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+            if (p.center[3] == 2.25f) {
+                const uint32_t bits = (uint32_t)p.extent[3];
+                const float ax = (float)(bits & 255u) * step, ay = (float)((bits >> 8) & 255u) * step;
+                const float az = (float)((bits >> 16) & 255u) * step;
+                t0 = make_float4((float)std::sin((double)ax), (float)std::cos((double)ax), (float)std::sin((double)ay),
+                                 (float)std::cos((double)ay));
+                t1 = make_float4((float)std::sin((double)az), (float)std::cos((double)az), 0.0f, 0.0f);
+            } else if (p.center[3] >= 0.0f) {
+                const double yaw = (double)p.extent[3];
+                t1 = make_float4((float)std::sin(yaw), (float)std::cos(yaw), 0.0f, 0.0f);
+            }
+            ctx->trig_host[2 * i] = t0;
+            ctx->trig_host[2 * i + 1] = t1;
+        }
+        SG_CUDA(ctx, cudaMemcpyAsync(ctx->prop_trig, ctx->trig_host.data(), ctx->trig_host.size() * sizeof(float4),
+                                     cudaMemcpyHostToDevice, stream));
+    }
+    const float radius = frame->globals->ground_up[3];
+    if (ctx->terrain && frame->globals->ground_counts[1] != 0u &&
+        (!ctx->terrain_cached || ctx->terrain_radius != radius)) {
+        cudaError_t e = sg::launch_terrain_cache(ctx->terrain, ctx->terrain_cells, radius, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "terrain cache launch");
+        ctx->terrain_cached = true;
+        ctx->terrain_radius = radius;
+    }
     return SG_OK;
 }
 
@@ -236,6 +308,15 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.width = ctx->width;
     p.height = ctx->height;
     p.events = nullptr;
+    p.terrain = ctx->terrain;
+    p.terrain_cells = ctx->terrain_cells;
+    p.props = reinterpret_cast<const float4 *>(ctx->props);
+    p.prop_trig = ctx->prop_trig;
+    p.n_props = s.g.ground_counts[0];
+    p.albedo_map = ctx->albedo_map;
+    p.map_width = ctx->map_width;
+    p.map_height = ctx->map_height;
+    p.map_extent = ctx->map_extent;
     return p;
 }
 
@@ -324,7 +405,59 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->ring_tables);
     cudaFree(ctx->events);
     cudaFree(ctx->scratch);
+    cudaFree(ctx->props);
+    cudaFree(ctx->prop_trig);
+    cudaFree(ctx->terrain);
+    cudaFree(ctx->albedo_map);
     delete ctx;
+    return SG_OK;
+}
+
+int sg_upload_terrain(sg_context *ctx, const float *data, size_t n_floats, uint32_t cells) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (cells < 2u || cells > SG_TERRAIN_MAX_CELLS || (cells & (cells - 1u)) != 0u)
+        return fail(ctx, SG_ERR_INVALID, "cells must be a power of two in 2..4096");
+    if (!data) return fail(ctx, SG_ERR_INVALID, "data is NULL");
+    const size_t source = sg::terrain_source_floats(cells);
+    if (n_floats != source) return fail(ctx, SG_ERR_INVALID, "terrain data length does not match the grid");
+    DeviceGuard guard(ctx->device);
+    cudaDeviceSynchronize();
+    cudaFree(ctx->terrain);
+    ctx->terrain = nullptr;
+    ctx->terrain_cells = 0;
+    ctx->terrain_cached = false;
+    SG_CUDA(ctx, cudaMalloc(&ctx->terrain, sg::terrain_floats(cells) * sizeof(float)));
+    SG_CUDA(ctx, cudaMemcpy(ctx->terrain, data, source * sizeof(float), cudaMemcpyHostToDevice));
+    ctx->terrain_cells = cells;
+    ctx->table_version += 1;
+    return SG_OK;
+}
+
+int sg_upload_albedo_map(sg_context *ctx, const float *albedo, uint32_t width, uint32_t height, float extent_m) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    DeviceGuard guard(ctx->device);
+    if (width == 0 || height == 0) {
+        cudaDeviceSynchronize();
+        cudaFree(ctx->albedo_map);
+        ctx->albedo_map = nullptr;
+        ctx->map_width = ctx->map_height = 0;
+        ctx->table_version += 1;
+        return SG_OK;
+    }
+    if (!albedo || !(extent_m > 0.0f) || (uint64_t)width * height > (1ull << 26))
+        return fail(ctx, SG_ERR_INVALID, "albedo map needs data, a positive extent and at most 2^26 texels");
+    for (size_t k = 0; k < (size_t)width * height; ++k)
+        if (!(albedo[k] >= 0.0f && albedo[k] <= 1.0f))
+            return fail(ctx, SG_ERR_INVALID, "albedo texels must lie in [0, 1]");
+    cudaDeviceSynchronize();
+    cudaFree(ctx->albedo_map);
+    ctx->albedo_map = nullptr;
+    SG_CUDA(ctx, cudaMalloc(&ctx->albedo_map, (size_t)width * height * sizeof(float)));
+    SG_CUDA(ctx, cudaMemcpy(ctx->albedo_map, albedo, (size_t)width * height * sizeof(float), cudaMemcpyHostToDevice));
+    ctx->map_width = width;
+    ctx->map_height = height;
+    ctx->map_extent = extent_m;
+    ctx->table_version += 1;
     return SG_OK;
 }
 
@@ -641,6 +774,37 @@ int sg_ring_probe(sg_context *ctx, const sg_frame *frame, const sg_ray *rays, ui
     cudaError_t e = sg::launch_ring_probe(p, d_rays, body, d_out, n, stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "ring_probe launch");
     if (!on_device) SG_CUDA(ctx, cudaMemcpyAsync(out, d_out, n * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    return SG_OK;
+}
+
+int sg_terrain_probe(sg_context *ctx, const sg_frame *frame, const float *rays, uint32_t n, float *out, int on_device,
+                     void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (n && (!rays || !out)) return fail(ctx, SG_ERR_INVALID, "rays or out is NULL");
+    if (!ctx->terrain) return fail(ctx, SG_ERR_STATE, "no terrain was uploaded");
+    if (frame && frame->globals && (frame->globals->ground_north[3] == 0.0f || frame->globals->ground_counts[1] == 0u))
+        return fail(ctx, SG_ERR_INVALID, "the frame must enable the landscape and its terrain");
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    sg::TraceParams p;
+    int status = probe_setup(ctx, frame, stream, &p);
+    if (status != SG_OK || n == 0) return status;
+    const float *d_rays = rays;
+    float *d_out = out;
+    if (!on_device) {
+        const size_t ray_bytes = ((size_t)n * 6 * sizeof(float) + 255) & ~size_t(255);
+        status = ensure_scratch(ctx, ray_bytes + (size_t)n * 4 * sizeof(float));
+        if (status != SG_OK) return status;
+        char *base = static_cast<char *>(ctx->scratch);
+        d_rays = reinterpret_cast<const float *>(base);
+        d_out = reinterpret_cast<float *>(base + ray_bytes);
+        SG_CUDA(ctx, cudaMemcpyAsync((void *)d_rays, rays, (size_t)n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream));
+    }
+    cudaError_t e = sg::launch_terrain_probe(p, d_rays, d_out, n, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "terrain_probe launch");
+    if (!on_device)
+        SG_CUDA(ctx, cudaMemcpyAsync(out, d_out, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SG_CUDA(ctx, cudaStreamSynchronize(stream));
     return SG_OK;
 }

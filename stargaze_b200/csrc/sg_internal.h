@@ -23,7 +23,26 @@ struct TraceParams {
     float4 *comp;                            // Kahan compensation
     uint32_t width, height;
     unsigned long long *events;              // optional event counters (9)
+    // Local landscape (ground.wgsl, terrain.wgsl): heightfield in the
+    // reference layout with its device-computed cache, props as 3 float4
+    // (center, extent, albedo) each, optional scalar albedo map.
+    const float *terrain;
+    uint32_t terrain_cells;
+    const float4 *props;
+    const float4 *prop_trig;  // 2 float4 per prop: (sin, cos) of x, y; z
+    uint32_t n_props;
+    const float *albedo_map;
+    uint32_t map_width, map_height;
+    float map_extent;
 };
+
+// Geometry cache of the heightfield (cache_terrain_geometry,
+// terrain.wgsl:242-285) for host radius `radius_m`, in place.
+cudaError_t launch_terrain_cache(float *terrain, uint32_t cells, float radius_m, cudaStream_t stream);
+
+// Floats of the full device terrain layout for `cells` cells per side.
+size_t terrain_floats(uint32_t cells);
+size_t terrain_source_floats(uint32_t cells);
 
 constexpr int kEventCount = 9;
 
@@ -37,6 +56,8 @@ cudaError_t launch_light_visibility(const TraceParams &p, const sg_ray *rays, co
                                     float *out, uint32_t n, cudaStream_t stream);
 cudaError_t launch_ring_probe(const TraceParams &p, const sg_ray *rays, uint32_t body, float *out,
                               uint32_t n, cudaStream_t stream);
+cudaError_t launch_terrain_probe(const TraceParams &p, const float *rays, float *out, uint32_t n,
+                                 cudaStream_t stream);
 // FMA-chain kernel of `blocks` x 256 threads, 128 * iters FMAs per thread.
 cudaError_t launch_fma_peak(int blocks, int iters, float *out, cudaStream_t stream);
 cudaError_t launch_ring_energy(float albedo, float tau, float mu, uint32_t steps, float *out,

@@ -7,6 +7,7 @@
 // take the same branches as long as possible.
 #include "sg_device.cuh"
 #include "sg_internal.h"
+#include "sg_landscape.cuh"
 
 namespace sg {
 
@@ -34,8 +35,8 @@ struct Path {
 };
 
 // camera_direction (pathtrace.wgsl:1619-1626).
-template <bool C>
-__device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter<C> K, uint32_t x, uint32_t y,
+template <bool C, bool L>
+__device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter<C, L> K, uint32_t x, uint32_t y,
                                                    uint32_t &rng) {
     const float jx = rnd(K, rng);
     const float jy = rnd(K, rng);
@@ -47,8 +48,8 @@ __device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter
 
 // Sample `smp` of a pixel: seeding (pathtrace.wgsl:1656), the jittered
 // camera ray, and trace()'s initial state.
-template <bool C>
-__device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counter<C> K, uint32_t pixel, uint32_t x,
+template <bool C, bool L>
+__device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counter<C, L> K, uint32_t pixel, uint32_t x,
                                            uint32_t y, uint32_t smp) {
     p.rng = hash_u32(pixel ^ hash_u32(s->sampling[0] + smp + 0x9e3779b9u));
     const float3 d = camera_direction(s, K, x, y, p.rng);
@@ -80,8 +81,8 @@ __device__ __forceinline__ float4 finish_path(const Path &p) {
 
 // One iteration of trace()'s loop (pathtrace.wgsl:1380-1607), airless,
 // landscape off. Returns true when the path has ended.
-template <bool C>
-__device__ __forceinline__ bool step(const Scene &S, Counter<C> K, Path &p) {
+template <bool C, bool L>
+__device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
     const sg_settings *s = S.s;
     const uint32_t max_vertices = s->counts[3];
     const uint32_t n_bodies = s->counts[0];
@@ -188,9 +189,11 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C> K, Path &p) {
         if (hit.index == kMiss) return true;
 
         const uint32_t bi = hit.index;
-        const float4 material = bf(S, bi, kMaterial);
+        // Local ids (host sphere, terrain, props) never index the bodies;
+        // the landscape-free instantiation (L == false) never sees them.
+        const bool local = L && bi >= kLocalBase;
         throughput = throughput * disc_scale;
-        if (material.w > 0.5f) {
+        if (!local && bf(S, bi, kMaterial).w > 0.5f) {
             // Emitter hit with MIS against the previous vertex's light sample.
             float weight = 1.0f;
             if (depth > 0u) {
@@ -198,18 +201,30 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C> K, Path &p) {
                 const float light_pdf = 1.0f / (kTau * cone_width_oc(oc, b_radius(S, bi)));
                 weight = power_weight(previous_pdf, light_pdf);
             }
-            radiance = radiance + throughput * xyz(material) * weight;
+            radiance = radiance + throughput * xyz(bf(S, bi, kMaterial)) * weight;
             return true;
         }
         K.add(&Events::surface_events);
-        const float radius = b_radius(S, bi);
-        if (depth == 0u && !point_gained && gain > 0.0f) {
-            point_gained = true;
-            const float extent = radius * fmaxf(1.0f, bf(S, bi, kRingParams).x);
-            throughput = throughput * point_gain(s, extent, hit.t);
+        float3 normal;
+        Ray outgoing;
+        if (local) {
+            // Metre-scale surface: bumped shading normal and the 5 mm
+            // offset origin (ground.wgsl:633-662).
+            if constexpr (L) {
+                normal = landscape_shading_normal(S, ray, hit.t, bi, hit.n);
+                outgoing = landscape_outgoing(S, ray, hit.t, bi, hit.n);
+            }
+        } else {
+            const float radius = b_radius(S, bi);
+            if (depth == 0u && !point_gained && gain > 0.0f) {
+                point_gained = true;
+                const float extent = radius * fmaxf(1.0f, bf(S, bi, kRingParams).x);
+                throughput = throughput * point_gain(s, extent, hit.t);
+            }
+            normal = sphere_normal(S, ray, bi, hit.delta);
+            // Celestial surfaces keep a body-relative origin.
+            outgoing = Ray{normal * (radius * (1.0f + 2.0e-6f)), normal, bi};
         }
-        const float3 normal = sphere_normal(S, ray, bi, hit.delta);
-        Ray outgoing{normal * (radius * (1.0f + 2.0e-6f)), normal, bi};
         const bool last_vertex = depth + 1u == max_vertices;
         float3 direct_light = f3(0.0f, 0.0f, 0.0f);
         #pragma unroll 1
@@ -229,14 +244,21 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C> K, Path &p) {
                 direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
             }
         }
-        const float3 albedo = surface_albedo(S, bi, normal);
+        float3 albedo;
+        if constexpr (L) {
+            albedo = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+        } else {
+            albedo = surface_albedo(S, bi, normal);
+        }
         radiance = radiance + throughput * albedo * direct_light;
-        if (has_ring(S, bi)) {
+        if (!local && has_ring(S, bi)) {
             const Shine shine = ringshine(S, K, bi, outgoing.o, normal, last_vertex, rng);
             rng = shine.rng;
             radiance = radiance + throughput * albedo * shine.radiance;
         }
-        shine_body = bi;
+        // Sky lighting of local surfaces needs the host atmosphere
+        // (pathtrace.wgsl:1578-1584), which frames here never enable.
+        shine_body = local ? kMiss : bi;
         if (last_vertex) return true;
         const float u = rnd(K, rng);
         float sp, cp;
@@ -267,11 +289,10 @@ __device__ __forceinline__ Scene stage_scene(const TraceParams &P, float4 *smem)
     for (uint32_t k = threadIdx.x; k < P.staged_table_floats; k += blockDim.x) staged[k] = P.tables[k];
     __syncthreads();
     Scene sc;
+    sc.p = &P;
     sc.s = &P.s;
     sc.B = smem;
     sc.tables = P.staged_table_floats > 0u ? staged : P.tables;
-    sc.bins = P.bins;
-    sc.table_stride = P.table_stride;
     return sc;
 }
 
@@ -297,12 +318,12 @@ __device__ __forceinline__ void flush_events(const Events &ev, unsigned long lon
 #define SG_TRACE_MIN_BLOCKS 4
 #endif
 
-template <bool C>
+template <bool C, bool L>
 __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(const __grid_constant__ TraceParams P) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
     Events ev{};
-    const Counter<C> K{&ev};
+    const Counter<C, L> K{&ev};
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
@@ -362,19 +383,19 @@ __global__ void __launch_bounds__(kThreads) closest_hit_kernel(const __grid_cons
                                                                const sg_ray *rays, sg_hit *hits, uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false> K{nullptr};
+    const Counter<false, true> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
     const Ray r = load_ray(in);
     // An anchor outside the body table would index past the staged bodies.
     const bool valid = in.anchor == kMiss || in.anchor < P.s.counts[0];
-    const Hit h = valid ? closest_hit(S, K, r) : Hit{1.0e30f, kMiss, 0.0f};
+    const Hit h = valid ? closest_hit(S, K, r) : Hit{1.0e30f, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     sg_hit out;
     out.distance = h.t;
     out.index = h.index;
     float3 nrm = f3(0.0f, 0.0f, 0.0f);
-    if (h.index != kMiss) nrm = sphere_normal(S, r, h.index, h.delta);
+    if (h.index != kMiss) nrm = h.index >= kLocalBase ? h.n : sphere_normal(S, r, h.index, h.delta);
     out.normal[0] = nrm.x;
     out.normal[1] = nrm.y;
     out.normal[2] = nrm.z;
@@ -386,7 +407,7 @@ __global__ void __launch_bounds__(kThreads) visibility_kernel(const __grid_const
                                                               float *out, uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false> K{nullptr};
+    const Counter<false, true> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
@@ -400,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) ring_probe_kernel(const __grid_const
                                                               uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false> K{nullptr};
+    const Counter<false, true> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
@@ -412,6 +433,22 @@ __global__ void __launch_bounds__(kThreads) ring_probe_kernel(const __grid_const
             result = make_float4(h.t, __fdiv_rn(length_rn(h.p), b_radius(S, body)), ring_transmission(S, r, h), 1.0f);
     }
     // Scalar stores: a caller's device pointer need only be 4-byte aligned.
+    out[4 * k + 0] = result.x;
+    out[4 * k + 1] = result.y;
+    out[4 * k + 2] = result.z;
+    out[4 * k + 3] = result.w;
+}
+
+__global__ void __launch_bounds__(kThreads) terrain_probe_kernel(const __grid_constant__ TraceParams P,
+                                                                 const float *rays, float *out, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float4 result = make_float4(0.0f, 0.0f, 0.0f, 1.0e30f);
+    if (P.terrain) {
+        const float3 o = f3(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]);
+        const float3 d = f3(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
+        result = terrain_query(P.terrain, P.terrain_cells, P.s.g.ground_up[3], o, d, 1.0e29f, false);
+    }
     out[4 * k + 0] = result.x;
     out[4 * k + 1] = result.y;
     out[4 * k + 2] = result.z;
@@ -449,7 +486,83 @@ __global__ void __launch_bounds__(256) fma_peak_kernel(float seed, int iters, fl
     if (s == 1234.5678f) out[0] = s;
 }
 
+// cache_terrain_geometry (terrain.wgsl:242-285): node AABBs with curvature
+// and a +-0.02 m margin, curved vertices and normals (12+12-bit packed on
+// grids over 1024 cells). One thread per vertex; the first N threads also
+// write one node each. Strict arithmetic keeps the cache bit-identical to an
+// IEEE evaluation, so traversal decisions match the oracle.
+__global__ void __launch_bounds__(256) terrain_cache_kernel(float *T, uint32_t cells, float r) {
+    const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t width = t_width(cells);
+    const float scale = t_scale_r(r);
+    if (index < t_nodes(cells)) {
+        const uint3 node = t_node(index, cells);
+        const float lo_x = t_coordinate(node.x, cells, scale), lo_z = t_coordinate(node.y, cells, scale);
+        const float hi_x = t_coordinate(node.x + node.z, cells, scale), hi_z = t_coordinate(node.y + node.z, cells, scale);
+        const float near_x = clampf(0.0f, lo_x, hi_x), near_z = clampf(0.0f, lo_z, hi_z);
+        const float far_x = fmaxf(fabsf(lo_x), fabsf(hi_x)), far_z = fmaxf(fabsf(lo_z), fabsf(hi_z));
+        const float lower = __fsub_rn(__fadd_rn(__fmul_rn(T[t_bounds(cells) + index * 2u], scale),
+                                                t_curvature(far_x, far_z, r)), 0.02f);
+        const float upper = __fadd_rn(__fadd_rn(__fmul_rn(T[t_bounds(cells) + index * 2u + 1u], scale),
+                                                t_curvature(near_x, near_z, r)), 0.02f);
+        float *c = T + t_cache(cells) + (size_t)index * 6u;
+        c[0] = lo_x;
+        c[1] = lower;
+        c[2] = lo_z;
+        c[3] = hi_x;
+        c[4] = upper;
+        c[5] = hi_z;
+    }
+    if (index >= t_vertices(cells)) return;
+    const uint32_t x = index % width, z = index / width;
+    const float px = t_coordinate(x, cells, scale), pz = t_coordinate(z, cells, scale);
+    const float vy = __fadd_rn(__fmul_rn(T[z * width + x], scale), t_curvature(px, pz, r));
+    const float denom =
+        __fsqrt_rn(fmaxf(__fsub_rn(__fmul_rn(r, r), __fadd_rn(__fmul_rn(px, px), __fmul_rn(pz, pz))), 1.0f));
+    const float gx = __fdiv_rn(px, denom), gz = __fdiv_rn(pz, denom);
+    float3 normal;
+    if (t_compact(cells)) {
+        const uint32_t lox = x > 0u ? x - 1u : 0u, loz = z > 0u ? z - 1u : 0u;
+        const uint32_t hix = x + 1u < cells ? x + 1u : cells, hiz = z + 1u < cells ? z + 1u : cells;
+        const float dx = __fdiv_rn(__fsub_rn(T[z * width + hix], T[z * width + lox]),
+                                   __fdiv_rn(__fsub_rn(t_coordinate(hix, cells, scale), t_coordinate(lox, cells, scale)), scale));
+        const float dz = __fdiv_rn(__fsub_rn(T[hiz * width + x], T[loz * width + x]),
+                                   __fdiv_rn(__fsub_rn(t_coordinate(hiz, cells, scale), t_coordinate(loz, cells, scale)), scale));
+        normal = f3(__fadd_rn(-dx, gx), 1.0f, __fadd_rn(-dz, gz));
+    } else {
+        const uint32_t vertices = t_vertices(cells);
+        normal = f3(__fadd_rn(-T[vertices + index], gx), 1.0f, __fadd_rn(-T[2u * vertices + index], gz));
+    }
+    normal = mul_rn(normal, __fdiv_rn(1.0f, length_rn(normal)));
+    float *v = T + t_vertex_cache(cells) + (size_t)index * t_vertex_stride(cells);
+    if (t_compact(cells)) {
+        v[0] = vy;
+        // WGSL round() is round-half-to-even, as rintf.
+        const float ux = rintf(__fmul_rn(clampf(__fadd_rn(__fmul_rn(normal.x, 0.5f), 0.5f), 0.0f, 1.0f), 4095.0f));
+        const float uz = rintf(__fmul_rn(clampf(__fadd_rn(__fmul_rn(normal.z, 0.5f), 0.5f), 0.0f, 1.0f), 4095.0f));
+        v[1] = (float)((uint32_t)ux | ((uint32_t)uz << 12));
+    } else {
+        v[0] = px;
+        v[1] = vy;
+        v[2] = pz;
+        v[3] = normal.x;
+        v[4] = normal.y;
+        v[5] = normal.z;
+    }
+}
+
 }  // namespace
+
+size_t terrain_source_floats(uint32_t cells) { return (size_t)t_cache(cells); }
+size_t terrain_floats(uint32_t cells) {
+    return (size_t)t_vertex_cache(cells) + (size_t)t_vertices(cells) * t_vertex_stride(cells);
+}
+
+cudaError_t launch_terrain_cache(float *terrain, uint32_t cells, float radius_m, cudaStream_t stream) {
+    const uint32_t threads = t_vertices(cells) > t_nodes(cells) ? t_vertices(cells) : t_nodes(cells);
+    terrain_cache_kernel<<<(threads + 255u) / 256u, 256, 0, stream>>>(terrain, cells, radius_m);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fma_peak(int blocks, int iters, float *out, cudaStream_t stream) {
     fma_peak_kernel<<<blocks, 256, 0, stream>>>(1.0f, iters, out);
@@ -468,14 +581,19 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
 cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t stream) {
     const size_t smem = trace_smem_bytes(p);
     const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
+    // The landscape instantiation only for frames that enable it: the
+    // celestial one carries neither its registers nor its code.
+    const bool land = p.s.g.ground_north[3] != 0.0f;
+    const void *fn = count_events ? (land ? (const void *)trace_kernel<true, true> : (const void *)trace_kernel<true, false>)
+                                  : (land ? (const void *)trace_kernel<false, true> : (const void *)trace_kernel<false, false>);
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return e;
     if (count_events) {
-        cudaError_t e = set_smem((const void *)trace_kernel<true>, smem);
-        if (e != cudaSuccess) return e;
-        trace_kernel<true><<<grid, kThreads, smem, stream>>>(p);
+        if (land) trace_kernel<true, true><<<grid, kThreads, smem, stream>>>(p);
+        else trace_kernel<true, false><<<grid, kThreads, smem, stream>>>(p);
     } else {
-        cudaError_t e = set_smem((const void *)trace_kernel<false>, smem);
-        if (e != cudaSuccess) return e;
-        trace_kernel<false><<<grid, kThreads, smem, stream>>>(p);
+        if (land) trace_kernel<false, true><<<grid, kThreads, smem, stream>>>(p);
+        else trace_kernel<false, false><<<grid, kThreads, smem, stream>>>(p);
     }
     return cudaGetLastError();
 }
@@ -507,6 +625,13 @@ cudaError_t launch_ring_probe(const TraceParams &p, const sg_ray *rays, uint32_t
     cudaError_t e = set_smem((const void *)ring_probe_kernel, smem);
     if (e != cudaSuccess) return e;
     ring_probe_kernel<<<(n + kThreads - 1) / kThreads, kThreads, smem, stream>>>(p, rays, body, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_terrain_probe(const TraceParams &p, const float *rays, float *out, uint32_t n,
+                                 cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    terrain_probe_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, stream>>>(p, rays, out, n);
     return cudaGetLastError();
 }
 

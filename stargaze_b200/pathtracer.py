@@ -119,6 +119,20 @@ class PathTracer:
         t = np.ascontiguousarray(tau, dtype=np.float32)
         check(self._lib.sg_upload_ring_profile(self._ctx, slot, _ptr(t), t.size), self._ctx)
 
+    def upload_terrain(self, data, cells: int) -> None:
+        """`Terrain::data` for a grid of `cells` cells (see terrain.py)."""
+        d = np.ascontiguousarray(data, dtype=np.float32)
+        check(self._lib.sg_upload_terrain(self._ctx, _ptr(d), d.size, cells), self._ctx)
+
+    def upload_albedo_map(self, albedo, extent_m: float) -> None:
+        """Scalar albedo map [height, width] over [-extent, extent]^2 of the
+        surface frame; None removes it."""
+        if albedo is None:
+            check(self._lib.sg_upload_albedo_map(self._ctx, None, 0, 0, 0.0), self._ctx)
+            return
+        a = np.ascontiguousarray(albedo, dtype=np.float32)
+        check(self._lib.sg_upload_albedo_map(self._ctx, _ptr(a), a.shape[1], a.shape[0], extent_m), self._ctx)
+
     def read_pixels(self, stream=None) -> np.ndarray:
         """The accumulation as a (height*width, 4) float32 array."""
         w, h = self.size()
@@ -169,6 +183,18 @@ class PathTracer:
         out = np.zeros((len(rays), 4), dtype=np.float32)
         view = frame.view()
         check(self._lib.sg_ring_probe(self._ctx, C.byref(view), _ptr(rays), body, len(rays), _ptr(out), 0, None),
+              self._ctx)
+        return out
+
+    def terrain_probe(self, frame: Frame, origins, directions) -> np.ndarray:
+        """terrain_hit in the surface frame for each (origin, direction):
+        rows of (normal xyz, distance)."""
+        o = np.asarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.asarray(directions, dtype=np.float32).reshape(-1, 3)
+        rays = np.ascontiguousarray(np.concatenate([o, d], axis=1))
+        out = np.zeros((len(rays), 4), dtype=np.float32)
+        view = frame.view()
+        check(self._lib.sg_terrain_probe(self._ctx, C.byref(view), _ptr(rays), len(rays), _ptr(out), 0, None),
               self._ctx)
         return out
 

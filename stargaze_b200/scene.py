@@ -57,7 +57,7 @@ class Frame:
         )
 
     def settings(self, width: int, height: int, samples_so_far: int, count: int, max_bounces: int,
-                 sampling: int, milky_way: float = 0.0) -> abi.Settings:
+                 sampling: int, milky_way: float = 0.0, terrain_cells: int = 512) -> abi.Settings:
         """Settings exactly as `PathTracer::encode` packs them
         (src/pathtracer.rs:812-859) for a tracer of this size."""
         s = abi.Settings()
@@ -71,7 +71,7 @@ class Frame:
             e = np.array(p.extent[:3], dtype=np.float32)
             top = max(top, np.float32(p.center[1]) + np.sqrt(np.float32(e @ e)))
         g.ground_counts[3] = int(np.array([top], dtype=np.float32).view(np.uint32)[0])
-        g.ground_counts[2] |= 9 << 8
+        g.ground_counts[2] = (g.ground_counts[2] & 255) | (int(terrain_cells).bit_length() - 1) << 8
         s.g = g
         lights = [0, 0, 0, 0]
         for i, b in enumerate(self.bodies):

@@ -57,6 +57,7 @@ class Workload:
     max_bounces: int
     ring_tables: dict[int, np.ndarray]
     description: str
+    landscape: object = None  # LandscapeData for scenes with terrain
 
     @property
     def samples(self) -> int:
@@ -131,7 +132,102 @@ def rings_1080p(width: int = 1920, height: int = 1080, spp: int = 256, max_bounc
                     "ringed giant, 512-bin tau table, binary star, moon eclipse")
 
 
-WORKLOADS = {"spheres_256": spheres_256, "rings_1080p": rings_1080p}
+@dataclass
+class LandscapeData:
+    heights: np.ndarray
+    terrain: np.ndarray  # reference layout (heights, bounds)
+    cells: int
+    albedo_map: np.ndarray | None = None
+    map_extent: float = 0.0
+
+
+def terrain_1080p(width: int = 1920, height: int = 1080, spp: int = 128, cells: int = 4096,
+                  rocks: int = 2000, foliage: int = 5000, max_bounces: int = 6, seed: int = 0,
+                  prop_range: tuple[float, float] = (25.0, 2000.0)):
+    """Terrain and precision scene: a 6.4e6 m host carrying a `cells`^2
+    seeded fBm heightfield (8 octaves, 300 m amplitude) under the min/max
+    quadtree, lifted so its lowest vertex is 0.5 m above the host sphere,
+    `rocks` faceted rocks and boxes and `foliage` ellipsoids in a
+    group-marker BVH between `prop_range` metres of the observer, one star 20
+    degrees above the horizon; the camera 2 m above the terrain, looking 4
+    degrees down, 70 degree field of view. Returns (Workload, LandscapeData)."""
+    from . import terrain as T
+
+    heights = T.fbm_heights(cells, seed=seed)
+    heights = (heights - heights.min() + 0.5).astype(np.float32)
+    centre = (cells + 1) * (cells // 2) + cells // 2
+    observer_m = float(heights[centre]) + 2.0  # 2 m above the terrain
+    terrain = T.pack_terrain(heights, cells)
+
+    R = 6.4e6
+    host = Body(np.zeros(3), R, albedo=(0.3, 0.3, 0.3))
+    lat, lon = math.radians(35.0), math.radians(30.0)
+    base = aim(host, lat, lon, observer_m, np.array([1.0e9, 0.0, 0.0]))
+    # Star: azimuth 140 degrees (south-east), 20 degrees above the horizon.
+    alt, az = math.radians(20.0), math.radians(140.0)
+    sdir = math.cos(alt) * (math.cos(az) * base.north + math.sin(az) * base.east) + math.sin(alt) * base.zenith
+    star = Body(base.position_au * AU_M + 1.5e11 * sdir, 7.0e8, luminosity_w=3.8e26)
+    # View: azimuth 100 degrees, 4 degrees down.
+    valt, vaz = math.radians(-4.0), math.radians(100.0)
+    target = base.position_au * AU_M + 1.0e4 * (math.cos(valt) * (math.cos(vaz) * base.north +
+                                                               math.sin(vaz) * base.east) + math.sin(valt) * base.zenith)
+    view = aim(host, lat, lon, observer_m, target)
+    bodies = [star, host]
+    frame = pack_frame(bodies, view, width, height, math.radians(70.0), host_index=1, height_m=observer_m)
+    frame.globals.ground_north[3] = 2.0  # host index + 1: the landscape is on
+
+    gen = splitmix64(seed + 11)
+    near, far = prop_range
+    # View direction in the surface frame (x east, z north).
+    fwd = np.array([math.sin(vaz), 0.0, math.cos(vaz)])
+    side = np.array([fwd[2], 0.0, -fwd[0]])
+    props = []
+    for k in range(rocks + foliage):
+        u = uniform01(gen, 4)
+        dist = near + (far - near) * math.sqrt(u[0])  # uniform over the ground area
+        lateral = (u[1] - 0.5) * 1.8 * dist
+        x, z = fwd[0] * dist + side[0] * lateral, fwd[2] * dist + side[2] * lateral
+        ground = T.height_at(heights, cells, x, z, R)
+        if k < rocks:
+            e = np.array([0.3 + 1.5 * u[2], 0.25 + 1.0 * u[3], 0.3 + 1.5 * u[2] * 0.8])
+            if k % 3 == 0:
+                kind, yaw = 0.0, 0.0  # plain box
+            elif k % 3 == 1:
+                kind, yaw = 2.0, (u[3] - 0.5) * 0.6  # faceted rock, leaning
+            else:
+                angles = [int(255 * v) for v in uniform01(gen, 3)]
+                kind, yaw = 2.25, float(angles[0] | (angles[1] << 8) | (angles[2] << 16))
+            tint = (0.28 + 0.1 * u[3], 0.27 + 0.08 * u[2], 0.25 + 0.06 * u[1])
+            props.append(T.primitive([x, ground + 0.6 * e[1], z], kind, e, yaw, tint, 1.0))
+        else:
+            e = np.array([0.6 + 1.4 * u[2], 1.0 + 3.0 * u[3], 0.6 + 1.4 * u[2]])
+            tint = (0.05 + 0.05 * u[3], 0.12 + 0.1 * u[2], 0.04 + 0.03 * u[1])
+            props.append(T.primitive([x, ground + 0.9 * e[1], z], 1.0, e, 0.0, tint, 0.0))
+    ground = T.build_prop_bvh(props, leaf_size=4)
+    frame.ground = ground
+    frame.globals.ground_counts[:] = [len(ground), 1, 0, 0]
+    land = LandscapeData(heights, terrain, cells)
+    wl = Workload("terrain_1080p", frame, width, height, spp, max_bounces, {},
+                  f"{cells}^2 fBm terrain, {rocks} rocks + {foliage} ellipsoids (BVH of {len(ground)} entries)", land)
+    return wl, land
+
+
+WORKLOADS = {
+    "spheres_256": spheres_256,
+    "rings_1080p": rings_1080p,
+    "terrain_1080p": lambda **kw: terrain_1080p(**kw)[0],
+}
+
+
+def upload_workload(tracer, wl: Workload) -> None:
+    """Upload a workload's extension tables (ring profiles, terrain) to a
+    PathTracer or any object with the same upload methods."""
+    for slot, tau in wl.ring_tables.items():
+        tracer.upload_ring_profile(slot, tau)
+    if wl.landscape is not None:
+        tracer.upload_terrain(wl.landscape.terrain, wl.landscape.cells)
+        if wl.landscape.albedo_map is not None:
+            tracer.upload_albedo_map(wl.landscape.albedo_map, wl.landscape.map_extent)
 
 
 def render_options(wl: Workload, spp: int = 64, noise_seed: int = 0) -> abi.Options:

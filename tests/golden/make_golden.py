@@ -21,12 +21,12 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 from oracle.binding import OracleTracer  # noqa: E402
-from rays import light_targets, seeded_rays  # noqa: E402
+from rays import landscape_rays, light_targets, seeded_rays  # noqa: E402
 import known_answers as ka  # noqa: E402
 from stargaze_b200 import abi  # noqa: E402
 from stargaze_b200.pathtracer import rays_array  # noqa: E402
 from stargaze_b200.scene import body, frame  # noqa: E402
-from stargaze_b200.workloads import rings_1080p, spheres_256  # noqa: E402
+from stargaze_b200.workloads import rings_1080p, spheres_256, terrain_1080p  # noqa: E402
 
 N_RAYS = 2048
 
@@ -42,15 +42,28 @@ def transport_scene():
     return f, {}
 
 
+def terrain_small(width=96, height=54):
+    """The terrain workload at fixture size: 256 cells, 200 + 500 props
+    within 10-200 m of the observer."""
+    return terrain_1080p(width=width, height=height, cells=256, rocks=200, foliage=500, prop_range=(10.0, 200.0))
+
+
 def scenes():
     s = spheres_256()
     r = rings_1080p()
+    t, _land = terrain_small()
     return {
         "transport": transport_scene(),
         "spheres_256": (s.frame, s.ring_tables),
         "rings_1080p": (r.frame, r.ring_tables),
         "shadow_ring": (ka.shadow_ring_scene(), {}),
+        "terrain": (t.frame, {}),
     }
+
+
+def landscape_of(name):
+    """Terrain data a ray scene needs (None for scenes without terrain)."""
+    return terrain_small()[1] if name == "terrain" else None
 
 
 def visibility_rays(f, rays, seed):
@@ -74,18 +87,26 @@ def visibility_rays(f, rays, seed):
     return out, lights
 
 
-def make_tracer(f, tables, dims=(1, 1), **opts):
+def make_tracer(f, tables, dims=(1, 1), land=None, **opts):
     t = OracleTracer(dims, ka.test_options(**opts))
     for slot, tau in tables.items():
         t.upload_ring_profile(slot, tau)
+    if land is not None:
+        t.upload_terrain(land.terrain, land.cells)
     return t
 
 
 def ray_fixtures():
     out = {}
     for k, (name, (f, tables)) in enumerate(scenes().items()):
-        rays = seeded_rays(f, N_RAYS, seed=100 + k)
-        t = make_tracer(f, tables)
+        land = landscape_of(name)
+        if land is None:
+            rays = seeded_rays(f, N_RAYS, seed=100 + k)
+        else:
+            half = N_RAYS // 2
+            rays = np.concatenate([seeded_rays(f, half, seed=100 + k),
+                                   landscape_rays(f, land.heights, land.cells, N_RAYS - half, seed=300 + k)])
+        t = make_tracer(f, tables, land=land)
         hits = t.closest_hit(f, rays)
         vrays, lights = visibility_rays(f, rays, seed=200 + k)
         vis = t.light_visibility(f, vrays, lights)
@@ -107,13 +128,23 @@ IMAGES = {
     # name: (workload factory, width, height, spp, batches)
     "spheres_64": (spheres_256, 64, 64, 16, 2),
     "rings_96x54": (rings_1080p, 96, 54, 16, 2),
+    "terrain_96x54": (None, 96, 54, 16, 2),
 }
 
 
-def image_fixture(name):
+def image_workload(name):
     factory, w, h, spp, batches = IMAGES[name]
-    wl = factory(width=w, height=h)
-    t = make_tracer(wl.frame, wl.ring_tables, dims=(w, h), samples_per_frame=spp, max_bounces=wl.max_bounces)
+    if factory is None:
+        wl, land = terrain_small(width=w, height=h)
+        return wl, land
+    return factory(width=w, height=h), None
+
+
+def image_fixture(name):
+    _factory, w, h, spp, batches = IMAGES[name]
+    wl, land = image_workload(name)
+    t = make_tracer(wl.frame, wl.ring_tables, dims=(w, h), land=land, samples_per_frame=spp,
+                    max_bounces=wl.max_bounces)
     for _ in range(batches):
         t.encode(wl.frame)
     return t.read_pixels()

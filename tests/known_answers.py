@@ -342,3 +342,145 @@ def shadow_rays(tracer_like_sample_light, f, width: int = 64, height: int = 16):
             dirs.append(d)
             lights.append(light)
     return rays_array(offsets, dirs, abi.MISS), np.array(lights, np.uint32)
+
+
+# ---------------------------------------------------------------------------
+# Local landscape (src/ground_tests.rs)
+# ---------------------------------------------------------------------------
+def local_frame(radius_m: float):
+    """`local_frame` (src/ground_tests.rs:191-206): a camera 2 m above a host
+    sphere, looking 26.6 degrees down, a star up and to the south."""
+    f32 = np.float32
+    f = frame()
+    metre = f32(1.0) / f32(149_597_870_700.0)
+    up = np.array([0.0, np.sqrt(f32(0.8)), np.sqrt(f32(0.2))], dtype=np.float32)
+    north = np.array([0.0, -up[2], up[1]], dtype=np.float32)
+    f.globals.ground_east[:] = [1.0, 0.0, 0.0, 2.0]
+    f.globals.ground_up[:] = [float(up[0]), float(up[1]), float(up[2]), float(radius_m)]
+    f.globals.ground_north[:] = [float(north[0]), float(north[1]), float(north[2]), 1.0]
+    center = -up * ((f32(radius_m) + f32(2.0)) * metre)
+    sun = (up * f32(8.0) - north * f32(4.0)) * metre
+    f.bodies = [body(center, f32(radius_m) * metre, [0.3] * 3, False), body(sun, f32(0.5) * metre, [100.0] * 3, True)]
+    return f
+
+
+def local_ground_shadows(make) -> dict:
+    """`gpu_local_ground_shadows` (src/ground_tests.rs:229-269)."""
+    from stargaze_b200.terrain import primitive
+
+    tracer = make((1, 1), test_options(samples_per_frame=64, max_bounces=1))
+    out = {}
+    for radius in (6_371_000.0, 1_500_000.0):
+        scene = local_frame(radius)
+        full = float(sample(tracer, scene, 8)[0][0])
+        assert full > 0.01 and np.isfinite(full), ("ground unlit", radius, full)
+        # A nearby box blocks the star without blocking the camera's ground ray.
+        scene.ground.append(primitive([0.0, 4.0, -4.0], 0.0, [0.8, 0.8, 0.8], 0.0, [0, 0, 0], 0.0))
+        scene.globals.ground_counts[0] = 1
+        box = float(sample(tracer, scene, 8)[0][0])
+        assert box < full * 0.001, ("box shadow", radius, box, full)
+        scene.ground[0].center[3] = 1.0
+        ellipsoid = float(sample(tracer, scene, 8)[0][0])
+        assert ellipsoid < full * 0.001, ("ellipsoid shadow", radius, ellipsoid, full)
+        # A blocker two centimetres above the surface must also shadow it.
+        scene.ground[0].center[:] = [0.0, 0.02, -4.0, 0.0]
+        scene.ground[0].extent[:] = [0.2, 0.004, 0.005, 0.0]
+        small = float(sample(tracer, scene, 8)[0][0])
+        assert small < full * 0.01, ("centimetre shadow", radius, small, full)
+        # Rotated boxes take part in visibility too.
+        scene.ground[0].center[:] = [0.0, 4.0, -4.0, 0.0]
+        scene.ground[0].extent[:] = [0.8, 0.8, 0.8, 0.4]
+        rotated = float(sample(tracer, scene, 8)[0][0])
+        assert rotated < full * 0.001, ("rotated box shadow", radius, rotated, full)
+        out[radius] = dict(full=full, box=box, ellipsoid=ellipsoid, small=small, rotated=rotated)
+    return out
+
+
+# Rays of heightfield_oracle (src/ground_tests.rs:749-760), surface frame at
+# terrain scale 1; origins are multiplied by the terrain scale.
+HEIGHTFIELD_RAYS = [
+    ([0.0, 300.0, 0.0], [0.0, -1.0, 0.0]),
+    ([0.0, 2.0, 0.0], [0.0, 0.03, 1.0]),
+    ([0.0, 2.0, 0.0], [1.0, 0.08, 0.25]),
+    ([0.0, 2.0, 0.0], [-1.0, 0.1, -0.4]),
+    ([0.0, 2.0, 0.0], [0.0, 1.0, 0.0]),
+    ([1_000.0, 2_000.0, -3_000.0], [0.0, -1.0, 0.0]),
+    ([-4_000.0, 1_500.0, 2_000.0], [1.0, -0.2, 0.1]),
+    ([16_000.0, 100.0, 0.0], [0.0, -1.0, 0.0]),
+    ([16_100.0, 100.0, 0.0], [0.0, -1.0, 0.0]),
+    ([0.0, 0.1, 0.0], [0.5, -0.01, -1.0]),
+]
+
+
+def terrain_frame(radius_m: float):
+    """A frame whose landscape uses the uploaded terrain (forest theme)."""
+    f = local_frame(radius_m)
+    f.globals.ground_counts[1] = 1
+    return f
+
+
+def exhaustive_terrain_hit(heights: np.ndarray, cells: int, radius_m: float, o, d) -> float:
+    """Independent f64 exhaustive intersection of the triangulated
+    heightfield, as src/ground_tests.rs:738-747 and :817-848 do: no quadtree,
+    bounds or traversal."""
+    from stargaze_b200.terrain import coordinates, terrain_scale
+
+    scale = terrain_scale(radius_m)
+    c = coordinates(cells, 1.0).astype(np.float64) * scale
+    width = cells + 1
+    x, z = np.meshgrid(c, c)
+    r = float(np.float32(radius_m))
+    curvature = -(x * x + z * z) / (r + np.sqrt(r * r - x * x - z * z))
+    y = np.asarray(heights, np.float64).reshape(width, width) * scale + curvature
+    V = np.stack([x, y, z], axis=-1)
+    a, b, cc, e = V[:-1, :-1], V[:-1, 1:], V[1:, :-1], V[1:, 1:]
+    o = np.asarray(o, np.float64)
+    d = np.asarray(d, np.float64)
+
+    def tri(A, B, C):
+        ab, ac = B - A, C - A
+        p = np.cross(d, ac)
+        det = np.sum(ab * p, axis=-1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rel = o - A
+            u = np.sum(rel * p, axis=-1) / det
+            q = np.cross(rel, ab)
+            v = np.sum(d * q, axis=-1) / det
+            t = np.sum(ac * q, axis=-1) / det
+        ok = (np.abs(det) >= 1e-15) & (u >= -1e-9) & (v >= -1e-9) & (u + v <= 1 + 1e-9) & (t > 0.001)
+        return np.where(ok, t, np.inf)
+
+    return float(min(tri(a, cc, b).min(), tri(e, b, cc).min()))
+
+
+def heightfield_oracle(make, heights: np.ndarray, data: np.ndarray, cells: int, rays=None) -> list:
+    """`heightfield_oracle` (src/ground_tests.rs:691-903) on a seeded fBm grid:
+    quadtree hits within 0.005 m + 1e-5 t of the exhaustive f64 scan, misses
+    where it misses, unit normals pointing up."""
+    from stargaze_b200.terrain import terrain_scale
+
+    rays = HEIGHTFIELD_RAYS if rays is None else rays
+    results = []
+    for radius in (6_371_000.0, 5_000.0):
+        tracer = make((1, 1), test_options())
+        tracer.upload_terrain(data, cells)
+        f = terrain_frame(radius)
+        scale = np.float32(terrain_scale(radius))
+        origins = np.array([np.float32(o) * scale for o, _ in [(np.array(o, np.float32), d) for o, d in rays]])
+        dirs = []
+        for _, d in rays:
+            d = np.array(d, np.float32)
+            dirs.append(d * (np.float32(1.0) / np.sqrt(np.float32(d @ d))))
+        dirs = np.array(dirs, np.float32)
+        out = tracer.terrain_probe(f, origins, dirs)
+        for k in range(len(rays)):
+            expected = exhaustive_terrain_hit(heights, cells, radius, origins[k], dirs[k])
+            actual = float(out[k][3])
+            if np.isinf(expected):
+                assert actual > 1e29, (radius, k, out[k])
+            else:
+                assert abs(actual - expected) < 0.005 + expected * 1e-5, (radius, k, actual, expected)
+                n = out[k][:3]
+                assert np.all(np.isfinite(n)) and abs(np.linalg.norm(n) - 1.0) < 1e-4 and n[1] > 0.0, (radius, k, n)
+            results.append((radius, k, actual, expected))
+    return results

@@ -96,3 +96,31 @@ def seeded_rays(frame: Frame, n: int, seed: int) -> np.ndarray:
 def light_targets(frame: Frame, n: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed + 1)
     return rng.integers(0, len(frame.bodies), size=n).astype(np.uint32)
+
+
+def landscape_rays(frame: Frame, heights: np.ndarray, cells: int, n: int, seed: int) -> np.ndarray:
+    """Rays leaving the local ground the way landscape_outgoing builds them
+    (ground.wgsl:649-662): origins 0.5 cm to 3 m above seeded ground points
+    within 200 m, expressed as camera-relative AU offsets (anchor MISS);
+    directions spread over the sphere with a bias towards the horizon."""
+    from stargaze_b200.terrain import height_at
+
+    rng = np.random.default_rng(seed)
+    g = frame.globals
+    east = np.array(g.ground_east[:3], np.float64)
+    up = np.array(g.ground_up[:3], np.float64)
+    north = np.array(g.ground_north[:3], np.float64)
+    h = float(g.ground_east[3])
+    radius = float(g.ground_up[3])
+    metres_per_au = 149597870700.0
+    offs, dirs = [], []
+    for _ in range(n):
+        x, z = rng.uniform(-200.0, 200.0, size=2)
+        y = height_at(heights, cells, x, z, radius) + rng.uniform(0.005, 3.0)
+        p = np.array([x, y - h, z])
+        offs.append((east * p[0] + up * p[1] + north * p[2]) / metres_per_au)
+        d = rng.normal(size=3)
+        d[1] = d[1] * 0.4 + 0.05
+        d /= np.linalg.norm(d)
+        dirs.append(east * d[0] + up * d[1] + north * d[2])
+    return rays_array(np.array(offs, np.float32), np.array(dirs, np.float32), abi.MISS)

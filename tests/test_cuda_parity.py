@@ -11,16 +11,18 @@ import pytest
 
 import golden_io as gio
 import known_answers as ka
-from golden.make_golden import IMAGES, scenes
+from golden.make_golden import IMAGES, image_workload, landscape_of, scenes
 from stargaze_b200 import PathTracer, abi
 
 pytestmark = pytest.mark.gpu
 
 
-def cuda_tracer(tables, dims=(1, 1), **opts):
+def cuda_tracer(tables, dims=(1, 1), land=None, **opts):
     t = PathTracer(dims, ka.test_options(**opts))
     for slot, tau in tables.items():
         t.upload_ring_profile(slot, tau)
+    if land is not None:
+        t.upload_terrain(land.terrain, land.cells)
     return t
 
 
@@ -28,7 +30,7 @@ def cuda_tracer(tables, dims=(1, 1), **opts):
 def test_closest_hit_ids_and_distances_bit_exact(name):
     f, tables = scenes()[name]
     g = gio.load_rays(name)
-    t = cuda_tracer(tables)
+    t = cuda_tracer(tables, land=landscape_of(name))
     hits = t.closest_hit(f, g["rays"])
     assert np.array_equal(hits["index"], g["hit_index"]), (hits["index"] != g["hit_index"]).sum()
     assert np.array_equal(hits["distance"], g["hit_distance"])
@@ -40,7 +42,7 @@ def test_closest_hit_ids_and_distances_bit_exact(name):
 def test_light_visibility_matches_oracle(name):
     f, tables = scenes()[name]
     g = gio.load_rays(name)
-    t = cuda_tracer(tables)
+    t = cuda_tracer(tables, land=landscape_of(name))
     vis = t.light_visibility(f, g["vis_rays"], g["vis_lights"])
     ref = g["visibility"]
     assert np.array_equal(vis == 0, ref == 0)
@@ -57,7 +59,7 @@ def test_light_visibility_matches_oracle(name):
 def test_ring_probe_matches_oracle(name):
     f, tables = scenes()[name]
     g = gio.load_rays(name)
-    t = cuda_tracer(tables)
+    t = cuda_tracer(tables, land=landscape_of(name))
     for i in range(len(f.bodies)):
         out = t.ring_probe(f, g["rays"], i)
         ref = g["ring"][i]
@@ -72,9 +74,9 @@ def test_ring_probe_matches_oracle(name):
 
 @pytest.mark.parametrize("name", gio.IMAGE_NAMES)
 def test_images_match_oracle_with_common_random_numbers(name):
-    factory, w, h, spp, batches = IMAGES[name]
-    wl = factory(width=w, height=h)
-    t = cuda_tracer(wl.ring_tables, (w, h), samples_per_frame=spp, max_bounces=wl.max_bounces)
+    _factory, w, h, spp, batches = IMAGES[name]
+    wl, land = image_workload(name)
+    t = cuda_tracer(wl.ring_tables, (w, h), land=land, samples_per_frame=spp, max_bounces=wl.max_bounces)
     for _ in range(batches):
         t.encode(wl.frame)
     img = t.read_pixels()

@@ -3,14 +3,14 @@ import numpy as np
 import pytest
 
 import golden_io as gio
-from golden.make_golden import IMAGES, image_fixture, make_tracer, scenes
+from golden.make_golden import IMAGES, image_fixture, landscape_of, make_tracer, scenes
 
 
 @pytest.mark.parametrize("name", gio.RAY_SCENES)
 def test_oracle_reproduces_ray_fixtures(name):
     f, tables = scenes()[name]
     g = gio.load_rays(name)
-    t = make_tracer(f, tables)
+    t = make_tracer(f, tables, land=landscape_of(name))
     hits = t.closest_hit(f, g["rays"])
     assert np.array_equal(hits["index"], g["hit_index"])
     assert np.array_equal(hits["distance"], g["hit_distance"])
@@ -38,3 +38,11 @@ def test_fixtures_are_not_degenerate():
         img = gio.load_image(name)
         assert np.isfinite(img).all() and (img >= 0).all()
         assert (img[:, :3].sum(axis=1) > 0).mean() > 0.05, name
+
+
+def test_terrain_fixture_exercises_every_landscape_kind():
+    g = gio.load_rays("terrain")
+    idx = g["hit_index"]
+    assert (idx == 0x80000000).sum() > 0 or (idx == 0x80100000).sum() > 0  # ground
+    assert (idx == 0x80100000).sum() > 100  # terrain
+    assert ((idx > 0x80000000) & (idx < 0x80100000)).sum() > 20  # props
