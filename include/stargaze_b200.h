@@ -309,6 +309,62 @@ SG_API int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu,
                    uint32_t steps, float *energy);
 
 /* ------------------------------------------------------------------ */
+/* Path-replay adjoint (extension: the reference renders forward only) */
+/* ------------------------------------------------------------------ */
+
+#define SG_TAPE_RANGES 16
+
+/* What the forward saves for the backward: the noise keys of every sample
+ * behind the current accumulation — runs of consecutive keys, a sample's
+ * key being the dispatch's sampling.x plus its index in the batch — and a
+ * hash of the history key (frame, options, uploaded tables) they were
+ * rendered with. The backward replays exactly these samples. */
+typedef struct sg_tape {
+    uint32_t width, height;
+    uint32_t samples;                /* samples behind the accumulation      */
+    uint32_t n_ranges;
+    uint32_t first[SG_TAPE_RANGES];  /* first noise key of each run          */
+    uint32_t count[SG_TAPE_RANGES];  /* samples of each run                  */
+    uint64_t history_hash;
+} sg_tape;
+
+/* Gradient destinations of sg_backward; a NULL pointer skips that block.
+ * All values are d loss / d parameter, summed over the image. */
+typedef struct sg_gradients {
+    /* SG_RING_TABLE_SLOTS * SG_RING_TABLE_MAX_BINS, slot-major: the ring
+     * optical-depth table values of sg_upload_ring_profile. */
+    float *ring_tau;
+    /* n_bodies * 3: sg_sphere.ring_color (single-scattering albedo). */
+    float *ring_albedo;
+    /* n_bodies * 3: sg_sphere.color — albedo of a surface, emitted radiance
+     * of an emitter (luminosity follows by the chain rule). */
+    float *body_color;
+    /* map width * height: the texels of sg_upload_albedo_map. */
+    float *albedo_map;
+    /* out: derivative entries dropped because a path's list was full (a
+     * path with more than 32 throughput factors); 0 in normal scenes. */
+    uint64_t dropped;
+} sg_gradients;
+
+/* The tape of the current accumulation (the forward's saved state, the
+ * torch.autograd.Function contract's ctx.save_for_backward). SG_ERR_STATE
+ * when the accumulation cannot be replayed: restored by
+ * sg_set_accumulation, or mixing more than SG_TAPE_RANGES key runs. */
+SG_API int sg_get_tape(const sg_context *ctx, sg_tape *tape);
+
+/* Backward pass: replay every sample of `tape` on `frame` (which must hash
+ * to the tape's history key: same frame, options and tables as the forward)
+ * and accumulate the gradient of a loss with d loss / d image =
+ * `dl_dimage` (width*height float4, the w channel ignored) into `grads`.
+ * Sampling is detached (the estimator's random decisions are held fixed),
+ * so the result is an unbiased estimate of the gradient of the expected
+ * image. `on_device` applies to dl_dimage and to every gradient pointer.
+ * The accumulation is not modified. Synchronises `stream`. */
+SG_API int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape,
+                       const float *dl_dimage, int on_device, sg_gradients *grads,
+                       void *stream);
+
+/* ------------------------------------------------------------------ */
 /* Diagnostics                                                         */
 /* ------------------------------------------------------------------ */
 

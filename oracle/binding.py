@@ -37,6 +37,15 @@ class Tables(C.Structure):
     ]
 
 
+class Direction(C.Structure):
+    _fields_ = [
+        ("ring_tau", C.c_void_p * abi.RING_TABLE_SLOTS),
+        ("ring_albedo", C.c_void_p),
+        ("body_color", C.c_void_p),
+        ("albedo_map", C.c_void_p),
+    ]
+
+
 class Events(C.Structure):
     _fields_ = [(name, C.c_uint64) for name in (
         "samples", "vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples",
@@ -78,6 +87,9 @@ def load() -> C.CDLL:
     lib.oracle_cache_terrain.restype = C.c_int
     lib.oracle_terrain_query.argtypes = [S, C.POINTER(Tables), P, P, C.c_float, C.c_int, P]
     lib.oracle_terrain_query.restype = C.c_int
+    lib.oracle_tangent.argtypes = [S, P, C.POINTER(Tables), C.POINTER(Direction), P, P, C.c_uint32, C.c_uint32,
+                                   C.c_int]
+    lib.oracle_tangent.restype = C.c_int
     lib.oracle_hash.argtypes = [C.c_uint32]
     lib.oracle_hash.restype = C.c_uint32
     lib.oracle_random.argtypes = [C.POINTER(C.c_uint32)]
@@ -340,6 +352,47 @@ class OracleTracer:
 
     def ring_energy(self, albedo: float, tau: float, mu: float, steps: int = 4096) -> float:
         return float(self.lib.oracle_ring_energy(albedo, tau, mu, steps))
+
+    def tangent(self, frame: Frame, first: int, count: int, ring_tau=None, ring_albedo=None, body_color=None,
+                albedo_map=None, rows=None):
+        """Forward-mode derivative of the samples with noise keys
+        [first, first + count) along a parameter direction: ring_tau maps a
+        table slot to per-bin tangents, ring_albedo / body_color are
+        (bodies, 3), albedo_map matches the uploaded map. Returns the
+        per-pixel sums (primal, tangent), each (height*width, 4)."""
+        n = len(frame.bodies)
+        keep = []
+
+        def arr(a, shape=None):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            if shape is not None:
+                a = a.reshape(shape)
+            keep.append(a)
+            return a.ctypes.data
+
+        d = Direction()
+        for slot, t in (ring_tau or {}).items():
+            d.ring_tau[slot] = arr(t)
+        d.ring_albedo = arr(ring_albedo, (n, 3))
+        d.body_color = arr(body_color, (n, 3))
+        d.albedo_map = arr(albedo_map)
+        primal = np.zeros((self.width * self.height, 4), dtype=np.float32)
+        tangent = np.zeros_like(primal)
+        bodies = frame.bodies_array()
+        self.tables.prepare(frame)
+        t = self.tables.struct(frame)
+        y0, y1 = rows if rows is not None else (0, self.height)
+        done = 0
+        while done < count:
+            batch = min(abi.MAX_BATCH_SAMPLES, count - done)
+            s = self.settings_for(frame, batch)
+            s.sampling[0] = (first + done) & 0xFFFFFFFF
+            _check(self.lib.oracle_tangent(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), C.byref(d),
+                                           _ptr(primal), _ptr(tangent), y0, y1, self.threads), "oracle_tangent")
+            done += batch
+        return primal, tangent
 
     def trace_sample(self, frame: Frame, x: int, y: int, s: int) -> np.ndarray:
         st, bodies, t = self._probe_args(frame)

@@ -326,21 +326,116 @@ static inline float one_minus_exp(float x) {
     return x < 1.0e-3f ? x * (1.0f - 0.5f * x) : 1.0f - expf(-x);
 }
 
-/* ring_bsdf: rings.wgsl:151-166 */
-static v3 ring_bsdf(optics_t optics, float outgoing, float incoming) {
+/* ring_bsdf: rings.wgsl:151-166; ring_factor is its scalar part. */
+static float ring_factor(float tau, float outgoing, float incoming) {
     float mo = maxf_(fabsf(outgoing), 1.0e-7f);
     float mi = maxf_(fabsf(incoming), 1.0e-7f);
-    float a = optics.tau / mo;
-    float b = optics.tau / mi;
+    float a = tau / mo;
+    float b = tau / mi;
     if (outgoing * incoming < 0.0f) {
         float delta = fabsf(a - b);
         float integral = delta < 1.0e-3f ? 1.0f - 0.5f * delta
                                          : one_minus_exp(delta) / maxf_(delta, 1.0e-20f);
-        float factor = optics.tau / (mo * mi) * expf(-minf_(a, b)) * integral;
-        return vmul(optics.color, factor / (4.0f * PI_F));
+        return tau / (mo * mi) * expf(-minf_(a, b)) * integral;
     }
-    float factor = one_minus_exp(a + b) / (mo + mi);
-    return vmul(optics.color, factor / (4.0f * PI_F));
+    return one_minus_exp(a + b) / (mo + mi);
+}
+static v3 ring_bsdf(optics_t optics, float outgoing, float incoming) {
+    return vmul(optics.color, ring_factor(optics.tau, outgoing, incoming) / (4.0f * PI_F));
+}
+
+/* ---------------------------------------------------------------- */
+/* Forward-mode tangents of the detached estimator (adjoint check).   */
+/* A direction D assigns a tangent to every material parameter; the   */
+/* functions below return d(value) along D with geometry and every    */
+/* sampling decision held fixed.                                      */
+/* ---------------------------------------------------------------- */
+static inline v3 dir_body_color(const oracle_direction *D, uint32_t i) {
+    if (!D || !D->body_color) return V(0, 0, 0);
+    return V(D->body_color[3 * i], D->body_color[3 * i + 1], D->body_color[3 * i + 2]);
+}
+
+/* Tangent of ring_optics at a ring point. */
+static optics_t ring_optics_dot(const scene *S, const oracle_direction *D, uint32_t index, v3 point) {
+    const sg_sphere *body = &S->b[index];
+    optics_t d = {V(0, 0, 0), 0.0f};
+    if (!D) return d;
+    v3 dcolor = D->ring_albedo ? V(D->ring_albedo[3 * index], D->ring_albedo[3 * index + 1], D->ring_albedo[3 * index + 2])
+                               : V(0, 0, 0);
+    float radius = vlength(point) / body->radius;
+    float x = (radius - body->ring_plane[3]) / (body->ring_params[0] - body->ring_plane[3]);
+    if (body->ring_params[3] >= 0.5f) {
+        uint32_t slot = (uint32_t)body->ring_params[3] - 1u;
+        uint32_t bins = (S->t && slot < SG_RING_TABLE_SLOTS && S->t->ring_tau[slot]) ? S->t->ring_bins[slot] : 0u;
+        if (bins > 0u) {
+            float fb = x * (float)bins;
+            uint32_t bin = fb <= 0.0f ? 0u : (uint32_t)fb;
+            if (bin > bins - 1u) bin = bins - 1u;
+            if (D->ring_tau[slot]) d.tau = body->ring_params[1] * D->ring_tau[slot][bin];
+        }
+        d.color = dcolor;
+    } else if (body->ring_params[2] > 0.5f) {
+        float broad = 0.5f + 0.5f * sinf(43.0f * x + 1.8f * sinf(17.0f * x));
+        v3 tint = V(0.70f, 0.68f, 0.65f);
+        if (x >= 0.2792f && x < 0.6910f) tint = V(1.0f, 1.0f, 1.0f);
+        else if (x >= 0.6910f && x < 0.7649f) tint = V(0.75f, 0.75f, 0.75f);
+        else if (x >= 0.7649f) tint = V(0.92f, 0.94f, 0.98f);
+        d.color = vmul(vmulv(dcolor, tint), 0.94f + 0.06f * broad);
+    } else {
+        d.color = dcolor;
+    }
+    return d;
+}
+
+/* d factor / d tau of ring_bsdf, differentiating the same piecewise forms
+ * (one_minus_exp's series below 1e-3, the integral's series below 1e-3). */
+static float ring_factor_dtau(float tau, float outgoing, float incoming) {
+    float mo = maxf_(fabsf(outgoing), 1.0e-7f);
+    float mi = maxf_(fabsf(incoming), 1.0e-7f);
+    if (outgoing * incoming < 0.0f) {
+        float a = tau / mo, b = tau / mi;
+        float delta = fabsf(a - b);
+        float k = fabsf(1.0f / mo - 1.0f / mi);
+        float m = minf_(1.0f / mo, 1.0f / mi);
+        float integral, dintegral; /* value and d/d delta */
+        if (delta < 1.0e-3f) {
+            integral = 1.0f - 0.5f * delta;
+            dintegral = -0.5f;
+        } else {
+            double dd = (double)delta, e = exp(-dd);
+            integral = one_minus_exp(delta) / maxf_(delta, 1.0e-20f);
+            dintegral = (float)((e * dd - (1.0 - e)) / (dd * dd));
+        }
+        float g = expf(-minf_(a, b));
+        /* factor = tau / (mo mi) * g * integral */
+        return (g * integral - tau * m * g * integral + tau * g * dintegral * k) / (mo * mi);
+    }
+    float k = 1.0f / mo + 1.0f / mi;
+    float x = tau / mo + tau / mi;
+    float dome = x < 1.0e-3f ? 1.0f - x : expf(-x);
+    return k * dome / (mo + mi);
+}
+
+/* Tangent of ring_bsdf(optics, outgoing, incoming). */
+static v3 ring_bsdf_dot(optics_t optics, optics_t doptics, float outgoing, float incoming) {
+    float factor = ring_factor(optics.tau, outgoing, incoming);
+    float dfactor = doptics.tau != 0.0f ? ring_factor_dtau(optics.tau, outgoing, incoming) * doptics.tau : 0.0f;
+    return vadd(vmul(doptics.color, factor / (4.0f * PI_F)), vmul(optics.color, dfactor / (4.0f * PI_F)));
+}
+
+/* Tangent of light_visibility: the transmissions of the ring crossings
+ * before the light (rings.wgsl:107-114), given the visibility `vis`. */
+static float light_visibility_dot(const scene *S, const oracle_direction *D, ray_t ray, uint32_t light, float vis) {
+    if (!D || vis <= 0.0f) return 0.0f;
+    hit_t surface = sphere_hit(S, ray, light);
+    float sum = 0.0f;
+    for (uint32_t i = 0; i < S->s->counts[0]; i++) {
+        ring_hit_t hit = ring_hit(S, ray, i);
+        if (hit.index == MISS || !(hit.distance < surface.distance)) continue;
+        float mu = maxf_(fabsf(vdot(ray.dir, b_pole(S, i))), 1.0e-7f);
+        sum += -ring_optics_dot(S, D, i, hit.point).tau / mu;
+    }
+    return vis * sum;
 }
 
 /* ring_origin: rings.wgsl:168-175 */
@@ -362,8 +457,11 @@ static float ring_area(const scene *S, uint32_t index) {
     return PI_F * r * r * (body->ring_params[0] * body->ring_params[0] - body->ring_plane[3] * body->ring_plane[3]);
 }
 
-/* ringshine: pathtrace.wgsl:1248-1296 */
-static v3 ringshine(const scene *S, uint32_t index, v3 origin, v3 normal, int last_vertex, uint32_t *rng) {
+/* ringshine: pathtrace.wgsl:1248-1296. With a direction D, *dshine
+ * receives the tangent of the result. */
+static v3 ringshine(const scene *S, uint32_t index, v3 origin, v3 normal, int last_vertex, uint32_t *rng,
+                    const oracle_direction *D, v3 *dshine) {
+    if (dshine) *dshine = V(0, 0, 0);
     const sg_sphere *body = &S->b[index];
     if (body->ring_params[0] <= body->ring_plane[3] || body->ring_params[1] <= 0.0f) return V(0, 0, 0);
     v3 n = b_pole(S, index);
@@ -384,8 +482,9 @@ static v3 ringshine(const scene *S, uint32_t index, v3 origin, v3 normal, int la
     if (blocker.index != MISS && blocker.distance < distance) return V(0, 0, 0);
     optics_t optics = ring_optics(S, index, point);
     if (optics.tau == 0.0f) return V(0, 0, 0);
+    optics_t doptics = ring_optics_dot(S, D, index, point);
     float mu_out = vdot(vneg(direction), n);
-    v3 shine = V(0, 0, 0);
+    v3 shine = V(0, 0, 0), dsum = V(0, 0, 0);
     uint32_t count = light_count(S);
     for (uint32_t slot = 0; slot < count; slot++) {
         uint32_t i = light_index(S, slot);
@@ -394,13 +493,24 @@ static v3 ringshine(const scene *S, uint32_t index, v3 origin, v3 normal, int la
         light_sample light = sample_light(S, from_ring, i, rng);
         float mu_in = vdot(light.dir, n);
         ring_hit_t rh = {0.0f, index, point};
-        float visibility = light_visibility(S, ring_origin(S, rh, light.dir), i);
+        ray_t shadow = ring_origin(S, rh, light.dir);
+        float visibility = light_visibility(S, shadow, i);
         shine = vadd(shine, vmul(vmulv(ring_bsdf(optics, mu_out, mu_in), b_color(S, i)),
                                  fabsf(mu_in) * visibility / light.pdf));
+        if (D) {
+            v3 bsdf = ring_bsdf(optics, mu_out, mu_in);
+            v3 dbsdf = ring_bsdf_dot(optics, doptics, mu_out, mu_in);
+            float dvis = light_visibility_dot(S, D, shadow, i, visibility);
+            v3 dterm = vadd(vmul(vadd(vmulv(dbsdf, b_color(S, i)), vmulv(bsdf, dir_body_color(D, i))),
+                                 fabsf(mu_in) * visibility / light.pdf),
+                            vmul(vmulv(bsdf, b_color(S, i)), fabsf(mu_in) * dvis / light.pdf));
+            dsum = vadd(dsum, dterm);
+        }
     }
     float pdf = distance2 / (ring_area(S, index) * cos_ring);
     float weight = power_weight(pdf, cos_surface / PI_F);
     if (last_vertex) weight = 1.0f;
+    if (dshine) *dshine = vmul(dsum, cos_surface * weight / (PI_F * pdf));
     return vmul(shine, cos_surface * weight / (PI_F * pdf));
 }
 
@@ -453,7 +563,7 @@ static float vnoise(v3 p) {
     float d = mixf(hash31(vadd(i, V(0, 1, 1))), hash31(vadd(i, V(1, 1, 1))), u.x);
     return mixf(mixf(a, b, u.y), mixf(c, d, u.y), u.z);
 }
-static v3 surface_albedo(const scene *S, uint32_t index, v3 normal) {
+static v3 surface_albedo_m(const scene *S, uint32_t index, v3 normal, float *mottle_out) {
     const sg_sphere *body = &S->b[index];
     v3 x = V(body->axis_x[0], body->axis_x[1], body->axis_x[2]);
     v3 y = V(body->axis_y[0], body->axis_y[1], body->axis_y[2]);
@@ -471,8 +581,24 @@ static v3 surface_albedo(const scene *S, uint32_t index, v3 normal) {
         }
         mottle = mixf(1.0f, 0.68f + 0.64f * noise, body->center_low[3]);
     }
+    if (mottle_out) *mottle_out = mottle;
     v3 c = vmul(b_color(S, index), mottle);
     return V(clampf_(c.x, 0, 1), clampf_(c.y, 0, 1), clampf_(c.z, 0, 1));
+}
+
+static v3 surface_albedo(const scene *S, uint32_t index, v3 normal) {
+    return surface_albedo_m(S, index, normal, NULL);
+}
+
+/* Tangent of surface_albedo: the colour scaled by the mottle where the
+ * clamp to [0, 1] is inactive. */
+static v3 surface_albedo_dot(const scene *S, const oracle_direction *D, uint32_t index, v3 normal) {
+    float m = 1.0f;
+    (void)surface_albedo_m(S, index, normal, &m);
+    v3 c = vmul(b_color(S, index), m);
+    v3 d = vmul(dir_body_color(D, index), m);
+    return V(c.x > 0.0f && c.x < 1.0f ? d.x : 0.0f, c.y > 0.0f && c.y < 1.0f ? d.y : 0.0f,
+             c.z > 0.0f && c.z < 1.0f ? d.z : 0.0f);
 }
 
 /* ---------------------------------------------------------------- */
@@ -1021,7 +1147,7 @@ static v3 crater_floor(const scene *S, v3 p, float distance, v3 normal) {
 }
 
 /* Albedo-map extension: nearest texel at surface-frame (x, z). */
-static float map_albedo(const scene *S, v3 p) {
+static size_t map_texel(const scene *S, v3 p) {
     const oracle_tables *t = S->t;
     float u = (p.x / t->map_extent + 1.0f) * 0.5f * (float)t->map_width;
     float w = (p.z / t->map_extent + 1.0f) * 0.5f * (float)t->map_height;
@@ -1030,8 +1156,9 @@ static float map_albedo(const scene *S, v3 p) {
     if (j < 0) j = 0;
     if (i > (int32_t)t->map_width - 1) i = (int32_t)t->map_width - 1;
     if (j > (int32_t)t->map_height - 1) j = (int32_t)t->map_height - 1;
-    return t->albedo_map[(size_t)j * t->map_width + (size_t)i];
+    return (size_t)j * t->map_width + (size_t)i;
 }
+static float map_albedo(const scene *S, v3 p) { return S->t->albedo_map[map_texel(S, p)]; }
 
 /* landscape_albedo: ground.wgsl:597-632 (themes 0-2; vegetation kinds are
  * rejected), with the albedo-map extension for the ground itself. */
@@ -1059,6 +1186,14 @@ static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
     v3 stone = vmul(tint, 0.7f + 0.45f * fine + 0.07f * strata);
     if (ground_theme(S) != 0u) return stone;
     return v3mix(stone, V(0.11f, 0.145f, 0.037f), lichen * 0.65f);
+}
+
+/* Tangent of landscape_albedo: only the albedo-map texels are parameters. */
+static v3 landscape_albedo_dot(const scene *S, const oracle_direction *D, ray_t ray, hit_t hit) {
+    if (!D || !D->albedo_map || !S->t || !S->t->albedo_map) return V(0, 0, 0);
+    if (hit.index != LOCAL_BASE && hit.index != TERRAIN_ID) return V(0, 0, 0);
+    float d = D->albedo_map[map_texel(S, landscape_point(S, ray, hit))];
+    return V(d, d, d);
 }
 
 /* landscape_shading_normal: ground.wgsl:633-648 (themes 0-2) */
@@ -1089,10 +1224,31 @@ static ray_t landscape_outgoing(const scene *S, ray_t ray, hit_t hit) {
     return r;
 }
 
+/* Russian roulette with survival s = clamp(max channel, 0.05, 0.95) of the
+ * throughput t: its full tangent (t / s after survival) and the score of
+ * the decision. The max channel is the first one reaching the maximum. */
+static void roulette_tangent(v3 t, float s, int survived, v3 *dt_full, float *score) {
+    float m = maxf_(t.x, maxf_(t.y, t.z));
+    float dm = t.x >= m ? dt_full->x : (t.y >= m ? dt_full->y : dt_full->z);
+    float ds = (m > 0.05f && m < 0.95f) ? dm : 0.0f;
+    if (survived) {
+        *score += ds / s;
+        *dt_full = vdivs(vsub(*dt_full, vmul(vdivs(t, s), ds)), s);
+    } else {
+        *score += -ds / (1.0f - s);
+    }
+}
+
 /* ---------------------------------------------------------------- */
 /* trace: pathtrace.wgsl:1347-1617 (airless)                         */
+/* With a direction D (adjoint check), dout receives the tangent of  */
+/* the returned radiance along D: every sampling decision, pdf, MIS   */
+/* weight and Russian-roulette survival keeps its value, only the     */
+/* material factors (ring tables and albedo, colours, albedo map)     */
+/* carry tangents. The ring-indirect cap is differentiated exactly.   */
 /* ---------------------------------------------------------------- */
-static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
+static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4], const oracle_direction *D,
+                  float dout[3]) {
     const sg_settings *st = S->s;
     ray_t ray = initial;
     v3 throughput = V(1, 1, 1);
@@ -1105,6 +1261,15 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
     float ring_cap = 1.0e30f;
     v3 ring_base = V(0, 0, 0);
     uint32_t shine_body = MISS;
+    /* tangents: detached (sampling held fixed) everywhere; after the first
+     * ring scatter also the full tangent (pdfs and MIS weights attached)
+     * of the throughput and of the radiance gathered since, and the score
+     * (d log probability) of the decisions taken since. */
+    v3 dthroughput = V(0, 0, 0), dradiance = V(0, 0, 0);
+    float dring_cap = 0.0f;
+    int captured = 0;
+    v3 dthroughput_full = V(0, 0, 0), dindirect_full = V(0, 0, 0);
+    float score = 0.0f, dlog_previous_pdf = 0.0f;
     for (;;) {
         EV(vertices);
         hit_t hit = closest_hit(S, ray);
@@ -1119,15 +1284,27 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
             const sg_sphere *planet = &S->b[ring.index];
             if (depth == 0u && !point_gained && st->background[3] > 0.0f) {
                 point_gained = 1;
-                throughput = vmul(throughput, point_gain(S, planet->radius * planet->ring_params[0], ring.distance));
+                float gain = point_gain(S, planet->radius * planet->ring_params[0], ring.distance);
+                throughput = vmul(throughput, gain);
+                if (D) dthroughput = vmul(dthroughput, gain);
             }
             v3 n = b_pole(S, ring.index);
             optics_t optics = ring_optics(S, ring.index, ring.point);
+            optics_t doptics = ring_optics_dot(S, D, ring.index, ring.point);
             float mu_out = vdot(vneg(ray.dir), n);
             float transmission = ring_transmission(S, ray, ring);
             float scatter_probability = one_minus_exp(optics.tau / maxf_(fabsf(mu_out), 1.0e-7f));
             float bsdf_pdf = scatter_probability / (4.0f * PI_F);
             int last_vertex = depth + 1u == st->counts[3];
+            /* d log scatter_probability and d log T along D */
+            float dlog_pdf = 0.0f, dlog_t = 0.0f;
+            if (D) {
+                float m_out = maxf_(fabsf(mu_out), 1.0e-7f);
+                float x = optics.tau / m_out;
+                if (scatter_probability > 0.0f)
+                    dlog_pdf = (x < 1.0e-3f ? 1.0f - x : expf(-x)) * (doptics.tau / m_out) / scatter_probability;
+                dlog_t = -doptics.tau / maxf_(fabsf(vdot(ray.dir, n)), 1.0e-7f);
+            }
             float ring_mis = 1.0f;
             if (shine_body == ring.index && null_crossings == 0u) {
                 float cos_ring = maxf_(fabsf(vdot(ray.dir, n)), 1.0e-6f);
@@ -1135,7 +1312,7 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 ring_mis = power_weight(previous_pdf, shine_pdf);
             }
             shine_body = MISS;
-            float unshadowed = 0.0f, direct = 0.0f;
+            float unshadowed = 0.0f, direct = 0.0f, dunshadowed = 0.0f, ddirect = 0.0f;
             uint32_t count = light_count(S);
             for (uint32_t slot = 0; slot < count; slot++) {
                 uint32_t i = light_index(S, slot);
@@ -1143,7 +1320,8 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 ray_t origin = {ring.point, n, ring.index};
                 light_sample light = sample_light(S, origin, i, rng);
                 float mu_in = vdot(light.dir, n);
-                float visibility = light_visibility(S, ring_origin(S, ring, light.dir), i);
+                ray_t shadow = ring_origin(S, ring, light.dir);
+                float visibility = light_visibility(S, shadow, i);
                 float weight = power_weight(light.pdf, bsdf_pdf);
                 if (last_vertex) weight = 1.0f;
                 v3 lit = vmul(vmulv(vmulv(throughput, ring_bsdf(optics, mu_out, mu_in)), b_color(S, i)),
@@ -1151,8 +1329,39 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 radiance = vadd(radiance, vmul(lit, visibility * weight * ring_mis));
                 unshadowed += lum(lit);
                 direct += lum(lit) * visibility;
+                if (D) {
+                    v3 bsdf = ring_bsdf(optics, mu_out, mu_in);
+                    v3 dbsdf = ring_bsdf_dot(optics, doptics, mu_out, mu_in);
+                    v3 color = b_color(S, i), dcolor = dir_body_color(D, i);
+                    v3 dlit = vmul(vadd(vadd(vmulv(vmulv(dthroughput, bsdf), color), vmulv(vmulv(throughput, dbsdf), color)),
+                                        vmulv(vmulv(throughput, bsdf), dcolor)),
+                                   fabsf(mu_in) / light.pdf);
+                    float dvis = light_visibility_dot(S, D, shadow, i, visibility);
+                    dradiance = vadd(dradiance, vadd(vmul(dlit, visibility * weight * ring_mis),
+                                                     vmul(lit, dvis * weight * ring_mis)));
+                    dunshadowed += lum(dlit);
+                    ddirect += lum(dlit) * visibility + lum(lit) * dvis;
+                    if (captured) {
+                        v3 dlit_full = vmul(vadd(vadd(vmulv(vmulv(dthroughput_full, bsdf), color),
+                                                      vmulv(vmulv(throughput, dbsdf), color)),
+                                                 vmulv(vmulv(throughput, bsdf), dcolor)),
+                                            fabsf(mu_in) / light.pdf);
+                        float dweight = last_vertex ? 0.0f : weight * (-2.0f * (1.0f - weight)) * dlog_pdf;
+                        dindirect_full = vadd(dindirect_full,
+                                              vadd(vadd(vmul(dlit_full, visibility * weight * ring_mis),
+                                                        vmul(lit, dvis * weight * ring_mis)),
+                                                   vmul(lit, visibility * dweight * ring_mis)));
+                    }
+                }
             }
             if (rnd(S, rng) < transmission) {
+                /* The crossing weighs exp(-tau / |mu|) at that probability:
+                 * a detached factor; attached, the value is unchanged and
+                 * the decision's score is d log T. */
+                if (D) {
+                    dthroughput = vadd(dthroughput, vmul(throughput, dlog_t));
+                    score += dlog_t;
+                }
                 ray = ring_origin(S, ring, ray.dir);
                 null_crossings += 1u;
                 if (null_crossings > st->counts[0]) break;
@@ -1162,11 +1371,28 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
             if (ring_cap > 1.0e29f) {
                 ring_cap = maxf_(direct, RING_INDIRECT_CAP * unshadowed);
                 ring_base = radiance;
+                dring_cap = direct >= RING_INDIRECT_CAP * unshadowed ? ddirect : RING_INDIRECT_CAP * dunshadowed;
+                captured = 1;
+                dthroughput_full = dthroughput;
+                score = 0.0f;
             }
             float z = 1.0f - 2.0f * rnd(S, rng);
             float phi = TAU_F * rnd(S, rng);
             float radial = sqrtf(maxf_(0.0f, 1.0f - z * z));
             v3 direction = basis_direction(n, radial * cosf(phi), radial * sinf(phi), z);
+            if (D) {
+                v3 bsdf = ring_bsdf(optics, mu_out, z);
+                v3 dbsdf = ring_bsdf_dot(optics, doptics, mu_out, z);
+                dthroughput = vmul(vadd(vmulv(dthroughput, bsdf), vmulv(throughput, dbsdf)), fabsf(z) / bsdf_pdf);
+                if (captured) {
+                    v3 next = vmul(vmulv(throughput, bsdf), fabsf(z) / bsdf_pdf);
+                    dthroughput_full = vsub(vmul(vadd(vmulv(dthroughput_full, bsdf), vmulv(throughput, dbsdf)),
+                                                 fabsf(z) / bsdf_pdf),
+                                            vmul(next, dlog_pdf));
+                    score += transmission < 1.0f ? -dlog_t * transmission / (1.0f - transmission) : 0.0f;
+                }
+                dlog_previous_pdf = dlog_pdf;
+            }
             throughput = vmul(vmulv(throughput, ring_bsdf(optics, mu_out, z)), fabsf(z) / bsdf_pdf);
             previous_pdf = bsdf_pdf;
             ray = ring_origin(S, ring, direction);
@@ -1175,8 +1401,11 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
             null_crossings = 0u;
             if (depth >= 3u) {
                 float survival = clampf_(maxf_(throughput.x, maxf_(throughput.y, throughput.z)), 0.05f, 0.95f);
-                if (rnd(S, rng) >= survival) break;
+                int survived = rnd(S, rng) < survival;
+                if (D && captured) roulette_tangent(throughput, survival, survived, &dthroughput_full, &score);
+                if (!survived) break;
                 throughput = vdivs(throughput, survival);
+                if (D) dthroughput = vdivs(dthroughput, survival);
             }
             continue;
         }
@@ -1188,6 +1417,8 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
         int local = hit.index >= LOCAL_BASE;
         uint32_t bi = hit.index;
         throughput = vmul(throughput, disc_scale);
+        if (D) dthroughput = vmul(dthroughput, disc_scale);
+        if (D && captured) dthroughput_full = vmul(dthroughput_full, disc_scale);
         if (!local && b_emissive(S, bi) > 0.5f) {
             float weight = 1.0f;
             if (depth > 0u) {
@@ -1195,13 +1426,26 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 weight = power_weight(previous_pdf, light_pdf);
             }
             radiance = vadd(radiance, vmul(vmulv(throughput, b_color(S, bi)), weight));
+            if (D)
+                dradiance = vadd(dradiance, vmul(vadd(vmulv(dthroughput, b_color(S, bi)),
+                                                      vmulv(throughput, dir_body_color(D, bi))), weight));
+            if (D && captured) {
+                float dweight = depth > 0u ? weight * 2.0f * (1.0f - weight) * dlog_previous_pdf : 0.0f;
+                dindirect_full = vadd(dindirect_full,
+                                      vadd(vmul(vadd(vmulv(dthroughput_full, b_color(S, bi)),
+                                                     vmulv(throughput, dir_body_color(D, bi))), weight),
+                                           vmul(vmulv(throughput, b_color(S, bi)), dweight)));
+            }
             break;
         }
         EV(surface_events);
         if (!local && depth == 0u && !point_gained && st->background[3] > 0.0f) {
             point_gained = 1;
             float extent = S->b[bi].radius * maxf_(1.0f, S->b[bi].ring_params[0]);
-            throughput = vmul(throughput, point_gain(S, extent, hit.distance));
+            float gain = point_gain(S, extent, hit.distance);
+            throughput = vmul(throughput, gain);
+            if (D) dthroughput = vmul(dthroughput, gain);
+            if (D && captured) dthroughput_full = vmul(dthroughput_full, gain);
         }
         v3 normal = local ? landscape_shading_normal(S, ray, hit) : hit.normal;
         ray_t outgoing;
@@ -1212,7 +1456,7 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
             outgoing.dir = normal;
             outgoing.anchor = hit.index;
         }
-        v3 direct_light = V(0, 0, 0);
+        v3 direct_light = V(0, 0, 0), ddirect_light = V(0, 0, 0);
         int last_vertex = depth + 1u == st->counts[3];
         uint32_t count = light_count(S);
         for (uint32_t slot = 0; slot < count; slot++) {
@@ -1229,14 +1473,37 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
                 if (last_vertex) weight = 1.0f;
                 /* air_transmittance(...) == 1 without air. */
                 direct_light = vadd(direct_light, vmul(b_color(S, i), bsdf_pdf * weight * visibility / sample.pdf));
+                if (D) {
+                    float dvis = light_visibility_dot(S, D, outgoing, i, visibility);
+                    ddirect_light = vadd(ddirect_light,
+                                         vadd(vmul(dir_body_color(D, i), bsdf_pdf * weight * visibility / sample.pdf),
+                                              vmul(b_color(S, i), bsdf_pdf * weight * dvis / sample.pdf)));
+                }
             }
         }
         v3 albedo = local ? landscape_albedo(S, ray, hit) : surface_albedo(S, bi, normal);
+        v3 dalbedo = V(0, 0, 0);
+        if (D) dalbedo = local ? landscape_albedo_dot(S, D, ray, hit) : surface_albedo_dot(S, D, bi, normal);
         radiance = vadd(radiance, vmulv(vmulv(throughput, albedo), direct_light));
+        if (D)
+            dradiance = vadd(dradiance, vadd(vmulv(vadd(vmulv(dthroughput, albedo), vmulv(throughput, dalbedo)), direct_light),
+                                             vmulv(vmulv(throughput, albedo), ddirect_light)));
+        if (D && captured)
+            dindirect_full = vadd(dindirect_full,
+                                  vadd(vmulv(vadd(vmulv(dthroughput_full, albedo), vmulv(throughput, dalbedo)), direct_light),
+                                       vmulv(vmulv(throughput, albedo), ddirect_light)));
         shine_body = MISS;
         if (!local) {
-            radiance = vadd(radiance, vmulv(vmulv(throughput, albedo),
-                                            ringshine(S, hit.index, outgoing.offset, normal, last_vertex, rng)));
+            v3 dshine = V(0, 0, 0);
+            v3 shine = ringshine(S, hit.index, outgoing.offset, normal, last_vertex, rng, D, D ? &dshine : NULL);
+            radiance = vadd(radiance, vmulv(vmulv(throughput, albedo), shine));
+            if (D)
+                dradiance = vadd(dradiance, vadd(vmulv(vadd(vmulv(dthroughput, albedo), vmulv(throughput, dalbedo)), shine),
+                                                 vmulv(vmulv(throughput, albedo), dshine)));
+            if (D && captured)
+                dindirect_full = vadd(dindirect_full,
+                                      vadd(vmulv(vadd(vmulv(dthroughput_full, albedo), vmulv(throughput, dalbedo)), shine),
+                                           vmulv(vmulv(throughput, albedo), dshine)));
             shine_body = hit.index;
         }
         /* sky_lit needs the host atmosphere (pathtrace.wgsl:1578-1584): off. */
@@ -1246,26 +1513,52 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4]) {
         float cosine = sqrtf(1.0f - u);
         outgoing.dir = basis_direction(normal, sqrtf(u) * cosf(phi), sqrtf(u) * sinf(phi), cosine);
         previous_pdf = cosine / PI_F;
+        if (D) dthroughput = vadd(vmulv(dthroughput, albedo), vmulv(throughput, dalbedo));
+        if (D && captured) dthroughput_full = vadd(vmulv(dthroughput_full, albedo), vmulv(throughput, dalbedo));
+        dlog_previous_pdf = 0.0f;
         throughput = vmulv(throughput, albedo);
         if (depth >= 2u) {
             float survival = clampf_(maxf_(throughput.x, maxf_(throughput.y, throughput.z)), 0.05f, 0.95f);
-            if (rnd(S, rng) >= survival) break;
+            int survived = rnd(S, rng) < survival;
+            if (D && captured) roulette_tangent(throughput, survival, survived, &dthroughput_full, &score);
+            if (!survived) break;
             throughput = vdivs(throughput, survival);
+            if (D) dthroughput = vdivs(dthroughput, survival);
         }
         ray = outgoing;
         previous_vertex = outgoing;
         depth += 1u;
         null_crossings = 0u;
     }
+    v3 dfinal = dradiance;
     if (ring_cap < 1.0e29f) {
         v3 indirect = vsub(radiance, ring_base);
         float luminance = lum(indirect);
-        if (luminance > ring_cap) radiance = vadd(ring_base, vmul(indirect, ring_cap / luminance));
+        if (luminance > ring_cap) {
+            radiance = vadd(ring_base, vmul(indirect, ring_cap / luminance));
+            /* The clamp makes the estimator nonlinear in the radiance
+             * gathered after the cap vertex (I), so holding that part's
+             * sampling fixed is no longer unbiased. Split the result into
+             * base + I (linear: detached tangent) and the correction
+             * C = I (cap / lum(I) - 1), whose tangent is the attached one
+             * plus C times the score of the decisions from the cap vertex's
+             * scatter on (likelihood ratio). */
+            v3 hat = vdivs(indirect, luminance);
+            v3 dq = vadd(vmul(hat, dring_cap),
+                         vmul(vsub(dindirect_full, vmul(hat, lum(dindirect_full))), ring_cap / luminance));
+            v3 correction = vmul(indirect, ring_cap / luminance - 1.0f);
+            dfinal = vadd(vadd(dradiance, vsub(dq, dindirect_full)), vmul(correction, score));
+        }
     }
     out[0] = radiance.x;
     out[1] = radiance.y;
     out[2] = radiance.z;
     out[3] = lum(backdrop);
+    if (dout) {
+        dout[0] = dfinal.x;
+        dout[1] = dfinal.y;
+        dout[2] = dfinal.z;
+    }
 }
 
 /* camera_direction: pathtrace.wgsl:1619-1626 */
@@ -1297,7 +1590,8 @@ static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
 }
 #define check_frame(s) check_frame_t((s), tables)
 
-static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4]) {
+static void sample_pixel_d(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4],
+                           const oracle_direction *D, float dout[3]) {
     uint32_t width = (uint32_t)S->s->g.viewport[0];
     uint32_t pixel = y * width + x;
     uint32_t rng = hash_u32(pixel ^ hash_u32(S->s->sampling[0] + s + 0x9e3779b9u));
@@ -1305,7 +1599,10 @@ static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, flo
     ray.offset = V(0, 0, 0);
     ray.dir = camera_direction(S, x, y, &rng);
     ray.anchor = MISS;
-    trace(S, ray, &rng, out);
+    trace(S, ray, &rng, out, D, dout);
+}
+static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4]) {
+    sample_pixel_d(S, x, y, s, out, NULL, NULL);
 }
 
 /* main: pathtrace.wgsl:1645-1675 */
@@ -1380,6 +1677,41 @@ int oracle_dispatch(const sg_settings *settings, const sg_sphere *bodies, const 
             for (size_t f = 0; f < sizeof(oracle_events) / sizeof(uint64_t); f++) dst[f] += src[f];
         }
         free(per_thread);
+    }
+    return SG_OK;
+}
+
+int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies, const oracle_tables *tables,
+                   const oracle_direction *direction, float *primal, float *tangent, uint32_t y0, uint32_t y1,
+                   int threads) {
+    int status = check_frame(settings);
+    if (status != SG_OK) return status;
+    uint32_t width = (uint32_t)settings->g.viewport[0];
+    uint32_t height = (uint32_t)settings->g.viewport[1];
+    if (y1 > height) y1 = height;
+    if (!primal || !tangent || !direction || y0 > y1) return SG_ERR_INVALID;
+    uint32_t z = settings->counts[2];
+    long total = (long)(y1 - y0) * (long)width;
+#ifdef _OPENMP
+    int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#else
+    int nthreads = 1;
+    (void)threads;
+#endif
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (long k = 0; k < total; k++) {
+        scene S = {settings, bodies, tables, NULL};
+        uint32_t x = (uint32_t)(k % width);
+        uint32_t y = y0 + (uint32_t)(k / width);
+        size_t pixel = (size_t)y * width + x;
+        for (uint32_t s = 0; s < z; s++) {
+            float r[4], d[3];
+            sample_pixel_d(&S, x, y, s, r, direction, d);
+            for (int c = 0; c < 4; c++) primal[4 * pixel + c] += r[c];
+            for (int c = 0; c < 3; c++) tangent[4 * pixel + c] += d[c];
+        }
     }
     return SG_OK;
 }

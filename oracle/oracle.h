@@ -122,6 +122,28 @@ int oracle_sample_light(const sg_settings *settings, const sg_sphere *bodies,
                         const sg_ray *ray, uint32_t light, uint32_t *rng,
                         float direction[3], float *pdf);
 
+/* Checker of the CUDA adjoint (an extension without reference
+ * counterpart). A direction assigns a tangent to each material parameter
+ * (NULL blocks are zero): per-bin ring-table values, ring albedo and body
+ * colour (3 floats per body), albedo-map texels. */
+typedef struct oracle_direction {
+    const float *ring_tau[SG_RING_TABLE_SLOTS];
+    const float *ring_albedo;
+    const float *body_color;
+    const float *albedo_map;
+} oracle_direction;
+
+/* Forward-mode derivative of the detached-sampling estimator: for pixel
+ * rows [y0, y1) and the counts.z samples of the dispatch, adds the radiance
+ * (primal, 4 floats per pixel) and its tangent along `direction` (tangent,
+ * 4 floats per pixel, w unused) to the output sums. Sampling decisions,
+ * pdfs, MIS weights and Russian-roulette survivals keep their values;
+ * the ring-indirect cap is differentiated exactly. */
+int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies,
+                   const oracle_tables *tables, const oracle_direction *direction,
+                   float *primal, float *tangent, uint32_t y0, uint32_t y1,
+                   int threads);
+
 /* hash / random of pathtrace.wgsl:87-98, exported for RNG-stream checks. */
 uint32_t oracle_hash(uint32_t value);
 float oracle_random(uint32_t *state);

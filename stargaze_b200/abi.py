@@ -117,6 +117,33 @@ class Hit(C.Structure):
     _fields_ = [("distance", C.c_float), ("index", C.c_uint32), ("normal", F3)]
 
 
+TAPE_RANGES = 16
+
+
+class Tape(C.Structure):
+    """Replay record of an accumulation (extension: the adjoint's saved state)."""
+
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("samples", C.c_uint32),
+        ("n_ranges", C.c_uint32),
+        ("first", C.c_uint32 * TAPE_RANGES),
+        ("count", C.c_uint32 * TAPE_RANGES),
+        ("history_hash", C.c_uint64),
+    ]
+
+
+class Gradients(C.Structure):
+    _fields_ = [
+        ("ring_tau", C.c_void_p),
+        ("ring_albedo", C.c_void_p),
+        ("body_color", C.c_void_p),
+        ("albedo_map", C.c_void_p),
+        ("dropped", C.c_uint64),
+    ]
+
+
 LAYOUT_SIZES = {
     "Globals": (Globals, 176),
     "Settings": (Settings, 240),
@@ -124,6 +151,8 @@ LAYOUT_SIZES = {
     "Primitive": (Primitive, 48),
     "Ray": (Ray, 28),
     "Hit": (Hit, 20),
+    "Tape": (Tape, 152),
+    "Gradients": (Gradients, 40),
 }
 
 

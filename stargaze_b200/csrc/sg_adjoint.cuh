@@ -1,0 +1,568 @@
+// sg_adjoint.cuh — derivative bookkeeping of the path-replay adjoint (an
+// extension: stargaze renders forward only).
+//
+// The backward pass replays every sample of the accumulated image from its
+// noise key, so each path takes exactly the forward's decisions. Sampling is
+// detached: Russian roulette, the ring null-versus-scatter choice, point-disc
+// picks, MIS weights and the pdfs that divide the estimator are held at
+// their forward values, and only the integrand is differentiated. That
+// keeps the estimator unbiased wherever the sampling pdf is positive:
+// E[(df/dtheta) / p] is the derivative of the integral of f. (A ring bin at
+// tau = 0 is never scattered in, so its gradient carries the transmission
+// term only.)
+//
+// Path-replay backpropagation: a factor multiplied into the path throughput
+// (surface albedo at a bounce, the slab BSDF at a ring scatter, the
+// transmission of a null crossing) scales every radiance contribution after
+// it, so its gradient is d log(factor) times the weighted radiance the path
+// gathers from there on: A_total - A, where A is the running sum of
+// w_c * c over the contributions c so far. A first replay of the sample
+// (pass 1, no derivatives) finds A_total; the second (pass 2) scatters each
+// factor once when it is created and each contribution's own factors
+// (albedo of the shading point, emitted radiance of the light, slab BSDF at
+// the ring point, ring transmissions along the shadow ray) when it is made.
+//
+// The ring-indirect cap (pathtrace.wgsl:1609-1615) clamps the radiance I
+// gathered after a path's first ring scatter to luminance `cap`:
+// R = base + I * min(1, cap / lum(I)). The clamp makes R nonlinear in I, so
+// on paths where it binds the detached form is biased. There the result is
+// split into base + I (linear, detached) and C = I * (cap / lum(I) - 1),
+// differentiated by the likelihood-ratio rule: the attached derivative of C
+// (pdfs, Russian-roulette survivals and MIS weights varying with the
+// parameters) plus C times the score — d log probability — of every
+// decision from the cap vertex's scatter on. With s = cap / lum(I),
+// w_c = (w . I) / lum(I) for the pixel weight w, the contribution weights
+// are w before the cap vertex's scatter, s * (w - lum * w_c) after it
+// (detached), that minus w for attached-only terms, lum * w_c for the cap's
+// own luminance sum, and w . C for the scores. Pass 1 records the cap
+// vertex, base, I, the cap sum and the Russian-roulette events after it.
+//
+// Parameters are indexed in the flat space of sg_internal.h (kGradColor,
+// kGradMap). A parameter whose value is zero gets no gradient through its
+// own log derivative.
+#pragma once
+
+#include "sg_device.cuh"
+#include "sg_landscape.cuh"
+
+namespace sg {
+
+constexpr uint32_t kNoParam = 0xffffffffu;
+constexpr uint32_t kVectorBit = 0x80000000u;  // entry spans an rgb triple
+constexpr uint32_t kPdfBit = 0x40000000u;     // attached-only (scalar) entry
+constexpr uint32_t kParamMask = 0x3fffffffu;
+constexpr int kMaxRoulette = 6;               // recorded events after a cap vertex
+constexpr int kMaxLocal = 8;                  // factors of one contribution
+constexpr int kMaxCrossings = 2;              // ring crossings of one shadow ray
+
+struct GradEntry {
+    uint32_t param;  // kNoParam: none
+    float3 dlog;     // scalar parameters use dlog.x for all channels
+};
+
+__device__ __forceinline__ GradEntry no_entry() { return GradEntry{kNoParam, make_float3(0.0f, 0.0f, 0.0f)}; }
+
+// Where gradients land: shared-memory windows over the hot parameters (the
+// ring tables in use and the body colours), global memory for the rest.
+struct GradSink {
+    float *tau;
+    uint32_t tau_n;
+    float *color;
+    uint32_t color_n;
+    float *global;
+    __device__ __forceinline__ void add(uint32_t param, float value) const {
+        if (value == 0.0f) return;
+        if (param < tau_n) atomicAdd(tau + param, value);
+        else if (param - kGradColor < color_n) atomicAdd(color + (param - kGradColor), value);
+        else atomicAdd(global + param, value);
+    }
+};
+
+// The forward integrator: no hooks.
+struct NoGrad {
+    static constexpr bool records = false;
+    static constexpr bool grads = false;
+};
+
+// A Russian-roulette decision after the cap vertex (pathtrace.wgsl:
+// 1484-1490, :1600-1604).
+struct Roulette {
+    uint32_t iteration;
+    uint32_t bits;  // max channel (0-2) | 4 survived | 8 survival clamped
+    float s;        // survival probability
+    float3 before;  // radiance gathered since the cap vertex, before it
+};
+
+// Pass 1: the summary pass 2 needs.
+struct Recorder {
+    static constexpr bool records = true;
+    static constexpr bool grads = false;
+    uint32_t capture_iter;  // iteration of the cap vertex, 0 when none
+    float cap;
+    bool cap_direct;        // cap = shadowed sum (else 0.003 * unshadowed)
+    float3 base;            // radiance at the cap vertex's scatter
+    float3 cap_light;       // the rgb sum whose luminance is the cap
+    float3 lit_sum, lit_vis_sum;  // at the current ring vertex
+    uint32_t n_rr, dropped;
+    Roulette rr[kMaxRoulette];
+};
+
+// Pass 2: weights and running sums.
+struct Prb {
+    static constexpr bool records = false;
+    static constexpr bool grads = true;
+    GradSink sink;
+    float3 w_pre, w_post, w_pdf, w_cap;  // contribution weights (see above)
+    float score;
+    float3 a_total, b_total;  // weighted radiance of the whole path
+    float3 a, b;              // ... gathered so far (detached, attached-only)
+    uint32_t capture_iter;
+    bool binding, cap_direct;
+    uint32_t iteration;       // the current step's
+    uint32_t prev_param;      // tau parameter of the last ring scatter
+    float prev_dlog_pdf;      // ... and d log of its scatter pdf
+    uint32_t n_rr;
+    Roulette rr[kMaxRoulette];
+    float rr_coef[kMaxRoulette];
+    GradEntry local[kMaxLocal];
+    uint32_t n_local, dropped;
+
+    __device__ __forceinline__ bool post() const { return capture_iter != 0u && iteration > capture_iter; }
+    __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
+    __device__ __forceinline__ void local_factor(GradEntry e) {
+        if (e.param == kNoParam) return;
+        if (n_local < (uint32_t)kMaxLocal) local[n_local++] = e;
+        else dropped += 1u;
+    }
+};
+
+__device__ __forceinline__ float inv_or_zero(float v) { return v != 0.0f ? 1.0f / v : 0.0f; }
+__device__ __forceinline__ float3 inv3(float3 v) { return f3(inv_or_zero(v.x), inv_or_zero(v.y), inv_or_zero(v.z)); }
+__device__ __forceinline__ float3 mul3(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float sum3(float3 a) { return a.x + a.y + a.z; }
+__device__ __forceinline__ float channel(float3 v, uint32_t m) { return m == 0u ? v.x : (m == 1u ? v.y : v.z); }
+
+__device__ __forceinline__ GradEntry vector_entry(uint32_t base, float3 dlog) {
+    return GradEntry{base | kVectorBit, dlog};
+}
+__device__ __forceinline__ GradEntry scalar_entry(uint32_t param, float dlog) {
+    return GradEntry{param, f3(dlog, dlog, dlog)};
+}
+__device__ __forceinline__ uint32_t ring_albedo_param(uint32_t body) { return kGradColor + 6u * body; }
+__device__ __forceinline__ uint32_t body_color_param(uint32_t body) { return kGradColor + 6u * body + 3u; }
+
+// Emitted radiance of a light (or an emitter hit): d log / d colour.
+__device__ __forceinline__ GradEntry emitter_entry(const Scene &S, uint32_t body) {
+    return vector_entry(body_color_param(body), inv3(xyz(bf(S, body, kMaterial))));
+}
+
+// Scatter `w . dlog` of one entry: per channel for a vector entry, the
+// channel sum for a scalar one.
+__device__ __forceinline__ void scatter_entry(const GradSink &sink, const GradEntry &e, float3 w, float3 w_pdf) {
+    if (e.param & kPdfBit) {
+        sink.add(e.param & kParamMask, sum3(w_pdf) * e.dlog.x);
+    } else if (e.param & kVectorBit) {
+        const uint32_t base = e.param & ~kVectorBit;
+        sink.add(base + 0u, w.x * e.dlog.x);
+        sink.add(base + 1u, w.y * e.dlog.y);
+        sink.add(base + 2u, w.z * e.dlog.z);
+    } else {
+        sink.add(e.param, sum3(w) * e.dlog.x);
+    }
+}
+
+// A radiance contribution `value` and its pending local factors (consumed).
+// `cap_term`: the cap vertex's light sample as a term of the cap.
+__device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
+    const bool post = G.post();
+    const float3 w = mul3(cap_term ? G.w_cap : (post ? G.w_post : G.w_pre), value);
+    const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : f3(0.0f, 0.0f, 0.0f);
+#pragma unroll 1
+    for (uint32_t k = 0; k < G.n_local; ++k) scatter_entry(G.sink, G.local[k], w, wp);
+    G.n_local = 0;
+    G.a = G.a + w;
+    G.b = G.b + wp;
+}
+
+// A factor multiplied into the throughput now: its share of everything the
+// path gathers from here on, plus — past a binding cap vertex — its part in
+// the later Russian-roulette survivals (score and attached 1 / s).
+__device__ __noinline__ void factor(Prb &G, GradEntry e) {
+    if (e.param == kNoParam) return;
+    const bool pdf = (e.param & kPdfBit) != 0u, vec = (e.param & kVectorBit) != 0u;
+    float3 add;
+    if (pdf) add = f3(sum3(G.b_total - G.b) * e.dlog.x, 0.0f, 0.0f);
+    else if (vec) add = mul3(G.a_total - G.a, e.dlog);
+    else add = f3(sum3(G.a_total - G.a) * e.dlog.x, 0.0f, 0.0f);
+    if (G.binding) {
+        // d log s of a survival s = clamp(t_m) is d log t_m: channel m of a
+        // vector entry, the whole scalar entry for the first unclamped
+        // survival (later ones see t / s, which no scalar factor moves).
+        int prev = -1;
+#pragma unroll 1
+        for (uint32_t r = 0; r < G.n_rr; ++r) {
+            const Roulette ev = G.rr[r];
+            if (ev.iteration < G.iteration || (ev.bits & 8u)) continue;
+            const uint32_t m = ev.bits & 3u;
+            const float c = G.rr_coef[r];
+            if (vec) {
+                const float dm = c * channel(e.dlog, m);
+                add = f3(add.x + (m == 0u ? dm : 0.0f), add.y + (m == 1u ? dm : 0.0f), add.z + (m == 2u ? dm : 0.0f));
+                if (prev >= 0) {
+                    const float dp = c * channel(e.dlog, (uint32_t)prev);
+                    add = f3(add.x - (prev == 0 ? dp : 0.0f), add.y - (prev == 1 ? dp : 0.0f),
+                             add.z - (prev == 2 ? dp : 0.0f));
+                }
+            } else if (prev < 0) {
+                add.x += c * e.dlog.x;
+            }
+            if (!(ev.bits & 4u)) break;
+            prev = (int)m;
+        }
+    }
+    if (vec) {
+        const uint32_t base = e.param & ~kVectorBit;
+        G.sink.add(base + 0u, add.x);
+        G.sink.add(base + 1u, add.y);
+        G.sink.add(base + 2u, add.z);
+    } else {
+        G.sink.add(e.param & kParamMask, add.x);
+    }
+}
+
+// The score of a decision after a binding cap vertex.
+__device__ __forceinline__ void score(Prb &G, uint32_t param, float dlog_p) {
+    if (G.binding && G.after_capture() && param != kNoParam) G.sink.add(param, G.score * dlog_p);
+}
+
+// d log(ring_bsdf) / d tau, differentiating the piecewise forms of
+// rings.wgsl:143-166 exactly as ring_bsdf evaluates them.
+__device__ __forceinline__ float ring_bsdf_dlog_tau(float tau, float outgoing, float incoming) {
+    if (!(tau > 0.0f)) return 0.0f;
+    const float mo = fmaxf(fabsf(outgoing), 1.0e-7f);
+    const float mi = fmaxf(fabsf(incoming), 1.0e-7f);
+    if (outgoing * incoming < 0.0f) {
+        // tau / (mo mi) * exp(-tau min(1/mo, 1/mi)) * integral(delta),
+        // delta = tau |1/mo - 1/mi|.
+        const float k = fabsf(1.0f / mo - 1.0f / mi);
+        const float delta = fabsf(tau / mo - tau / mi);
+        float dlog_integral;
+        if (delta < 1.0e-3f) dlog_integral = -0.5f / (1.0f - 0.5f * delta);
+        else if (delta < 0.05f) dlog_integral = -0.5f + delta / 12.0f - delta * delta * delta / 720.0f;
+        else dlog_integral = 1.0f / expm1f(delta) - 1.0f / delta;
+        return 1.0f / tau - fminf(1.0f / mo, 1.0f / mi) + k * dlog_integral;
+    }
+    // one_minus_exp(tau (1/mo + 1/mi)) / (mo + mi)
+    const float k = 1.0f / mo + 1.0f / mi;
+    const float x = tau / mo + tau / mi;
+    if (x < 1.0e-3f) return 1.0f / tau - 0.5f * k / (1.0f - 0.5f * x);
+    return k / expm1f(x);
+}
+
+// The table parameter behind a ring point (kNoParam when the ring has no
+// tabulated profile); `scale` is d tau / d table value (ring_params.y).
+__device__ __forceinline__ uint32_t tau_param(const Scene &S, uint32_t body, float3 point, float *scale) {
+    const float4 params = bf(S, body, kRingParams);
+    if (params.w < 0.5f) return kNoParam;
+    const uint32_t slot = (uint32_t)params.w - 1u;
+    const uint32_t bins = slot < SG_RING_TABLE_SLOTS ? S.p->bins[slot] : 0u;
+    if (bins == 0u) return kNoParam;
+    *scale = params.y;
+    return slot * SG_RING_TABLE_MAX_BINS + ring_bin(ring_x(S, body, point), bins);
+}
+
+// d log scatter_probability / d table value: one_minus_exp(tau / |mu|)
+// (rings.wgsl:143-145, pathtrace.wgsl:1423-1425) with tau = scale * table.
+__device__ __forceinline__ float scatter_pdf_dlog(float tau, float mu_out, float scale) {
+    const float m = fmaxf(fabsf(mu_out), 1.0e-7f);
+    const float x = tau / m;
+    const float p = one_minus_exp(x);
+    if (!(p > 0.0f)) return 0.0f;
+    return (x < 1.0e-3f ? 1.0f - x : expf(-x)) * (scale / m) / p;
+}
+
+// The slab BSDF's entries at a ring point: optical depth and albedo.
+__device__ __forceinline__ void ring_point_entries(const Scene &S, uint32_t body, float3 point, const Optics &o,
+                                                   float outgoing, float incoming, GradEntry &tau_e,
+                                                   GradEntry &albedo_e) {
+    float scale = 0.0f;
+    const uint32_t tp = tau_param(S, body, point, &scale);
+    tau_e = tp == kNoParam ? no_entry() : scalar_entry(tp, scale * ring_bsdf_dlog_tau(o.tau, outgoing, incoming));
+    albedo_e = vector_entry(ring_albedo_param(body), inv3(xyz(bf(S, body, kRingColor))));
+}
+
+// A crossing multiplies by exp(-tau / |mu|) (rings.wgsl:83-86):
+// d log / d table = -scale / |mu|.
+__device__ __forceinline__ GradEntry crossing_entry(const Scene &S, uint32_t body, float3 point, float3 d) {
+    float scale = 0.0f;
+    const uint32_t tp = tau_param(S, body, point, &scale);
+    if (tp == kNoParam) return no_entry();
+    const float mu = fmaxf(fabsf(dot_rn(d, xyz(bf(S, body, kRingPlane)))), 1.0e-7f);
+    return scalar_entry(tp, -scale / mu);
+}
+
+// light_visibility (rings.wgsl:90-115) that also returns the ring crossings
+// behind its transmission, for the adjoint.
+struct Visibility {
+    float v;
+    uint32_t n;
+    GradEntry cross[kMaxCrossings];
+};
+
+template <bool C, bool L>
+__device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
+    Visibility out;
+    out.v = light_visibility(S, K, r, light);
+    out.n = 0;
+    if (out.v <= 0.0f) return out;
+    float delta;
+    const float surface = sphere_distance(S, K, r, light, b_radius(S, light), delta);
+    const uint32_t n = S.s->counts[0];
+#pragma unroll 1
+    for (uint32_t i = 0; i < n; ++i) {
+        const RingHit h = ring_hit(S, K, r, i);
+        if (h.index == kMiss || !(h.t < surface)) continue;
+        const GradEntry e = crossing_entry(S, i, h.p, r.d);
+        if (e.param == kNoParam) continue;
+        if (out.n < (uint32_t)kMaxCrossings) out.cross[out.n] = e;
+        out.n += 1u;  // more than kMaxCrossings: counted as dropped
+    }
+    return out;
+}
+
+__device__ __forceinline__ void crossing_factors(Prb &G, const Visibility &vis) {
+#pragma unroll
+    for (int k = 0; k < kMaxCrossings; ++k)
+        if ((uint32_t)k < vis.n) G.local_factor(vis.cross[k]);
+    if (vis.n > (uint32_t)kMaxCrossings) G.dropped += vis.n - (uint32_t)kMaxCrossings;
+}
+
+// The adjoint's view of a ring vertex: its table parameter, d tau / d
+// table value, and d log of the vertex's scatter pdf.
+struct RingVertexGrad {
+    uint32_t param;
+    float scale;
+    float dlog_pdf;
+};
+
+__device__ __noinline__ RingVertexGrad ring_vertex_grad(Scene S, uint32_t ring, float3 point, float tau,
+                                                        float mu_out) {
+    RingVertexGrad v{kNoParam, 0.0f, 0.0f};
+    v.param = tau_param(S, ring, point, &v.scale);
+    if (v.param != kNoParam) v.dlog_pdf = scatter_pdf_dlog(tau, mu_out, v.scale);
+    return v;
+}
+
+// One light sample at a ring vertex (pathtrace.wgsl:1437-1450): its
+// radiance, and at the cap vertex of a binding path its term of the cap
+// (max(shadowed, 0.003 * unshadowed) luminance of `lit`). After the cap
+// vertex the MIS weight's dependence on the vertex's scatter pdf is an
+// attached entry.
+__device__ __noinline__ void ring_light_grad(Scene S, Prb &G, uint32_t ring, float3 point, Optics optics,
+                                             float mu_out, float mu_in, uint32_t light, float3 lit, Visibility vis,
+                                             float weight, float ring_mis, bool last_vertex, RingVertexGrad vg) {
+    GradEntry tau_e, albedo_e;
+    ring_point_entries(S, ring, point, optics, mu_out, mu_in, tau_e, albedo_e);
+    const GradEntry light_e = emitter_entry(S, light);
+    const float3 value = lit * (vis.v * weight * ring_mis);
+    if (value.x != 0.0f || value.y != 0.0f || value.z != 0.0f) {
+        G.local_factor(tau_e);
+        G.local_factor(albedo_e);
+        G.local_factor(light_e);
+        crossing_factors(G, vis);
+        if (G.post() && G.binding && !last_vertex && vg.param != kNoParam)
+            G.local_factor(scalar_entry(vg.param | kPdfBit, -2.0f * (1.0f - weight) * vg.dlog_pdf));
+        contribute(G, value, false);
+    }
+    if (G.binding && G.iteration == G.capture_iter) {
+        const float3 cap_value = G.cap_direct ? lit * vis.v : lit * kRingIndirectCap;
+        if (cap_value.x != 0.0f || cap_value.y != 0.0f || cap_value.z != 0.0f) {
+            G.local_factor(tau_e);
+            G.local_factor(albedo_e);
+            G.local_factor(light_e);
+            if (G.cap_direct) crossing_factors(G, vis);
+            contribute(G, cap_value, true);
+        }
+    }
+}
+
+// A null crossing (pathtrace.wgsl:1451-1456): the transmission factor, and
+// after a binding cap vertex the decision's score d log T.
+__device__ __noinline__ void ring_null_grad(Scene S, Prb &G, uint32_t ring, float3 point, float3 d) {
+    const GradEntry ce = crossing_entry(S, ring, point, d);
+    factor(G, ce);
+    score(G, ce.param, ce.dlog.x);
+}
+
+// A ring scatter (pathtrace.wgsl:1466-1483): the slab BSDF's factors; after
+// a binding cap vertex also the decision's score d log(1 - T) and the
+// attached 1 / scatter pdf. Records the vertex for the MIS weight of an
+// emitter reached next.
+__device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, float3 point, Optics optics,
+                                               float mu_out, float z, RingVertexGrad v, float transmission,
+                                               float3 d) {
+    GradEntry tau_e, albedo_e;
+    ring_point_entries(S, ring, point, optics, mu_out, z, tau_e, albedo_e);
+    factor(G, tau_e);
+    factor(G, albedo_e);
+    if (G.binding && v.param != kNoParam) {
+        const float dlog_t = -v.scale / fmaxf(fabsf(dot_rn(d, xyz(bf(S, ring, kRingPlane)))), 1.0e-7f);
+        if (transmission < 1.0f) score(G, v.param, -dlog_t * transmission / (1.0f - transmission));
+        factor(G, scalar_entry(v.param | kPdfBit, -v.dlog_pdf));
+    }
+    G.prev_param = v.param;
+    G.prev_dlog_pdf = v.dlog_pdf;
+}
+
+// One light sample at a surface vertex (pathtrace.wgsl:1545-1565).
+__device__ __noinline__ void surface_light_grad(Scene S, Prb &G, GradEntry albedo_e, uint32_t light, float3 value,
+                                                Visibility vis) {
+    G.local_factor(albedo_e);
+    G.local_factor(emitter_entry(S, light));
+    crossing_factors(G, vis);
+    contribute(G, value, false);
+}
+
+// An emitter reached by the path (pathtrace.wgsl:1516-1526); `mis` is the
+// MIS weight against the previous vertex's light sample, whose bsdf pdf
+// (a ring scatter's) moves with that vertex's optical depth.
+__device__ __noinline__ void emitter_grad(Scene S, Prb &G, uint32_t body, float3 value, float mis, bool weighted) {
+    G.local_factor(emitter_entry(S, body));
+    if (G.binding && G.post() && weighted && G.prev_param != kNoParam)
+        G.local_factor(scalar_entry(G.prev_param | kPdfBit, 2.0f * (1.0f - mis) * G.prev_dlog_pdf));
+    contribute(G, value, false);
+}
+
+// The albedo entry of a surface vertex: body colour of a celestial surface
+// (zero where the clamp of surface_albedo is active), or the albedo-map
+// texel of the host ground.
+template <bool L>
+__device__ __noinline__ GradEntry albedo_entry(Scene S, Ray ray, float t, uint32_t index, float3 albedo) {
+    if (index < kLocalBase) {
+        const float3 m = xyz(bf(S, index, kMaterial));
+        const float3 d = f3(albedo.x > 0.0f && albedo.x < 1.0f ? inv_or_zero(m.x) : 0.0f,
+                            albedo.y > 0.0f && albedo.y < 1.0f ? inv_or_zero(m.y) : 0.0f,
+                            albedo.z > 0.0f && albedo.z < 1.0f ? inv_or_zero(m.z) : 0.0f);
+        return vector_entry(body_color_param(index), d);
+    }
+    if constexpr (L) {
+        if ((index == kLocalBase || index == kTerrainId) && S.p->albedo_map) {
+            const uint32_t texel = map_texel(S.p, landscape_point(S, ray, t));
+            return scalar_entry(kGradMap + texel, inv_or_zero(S.p->albedo_map[texel]));
+        }
+    }
+    return no_entry();
+}
+
+// ringshine with derivatives (pathtrace.wgsl:1248-1296): the same draws and
+// result as ringshine(), plus one contribution per light. `carried` is the
+// path throughput times the surface albedo.
+template <bool C, bool L>
+__device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
+                                             bool last_vertex, uint32_t rng, Prb &G, float3 carried,
+                                             GradEntry albedo_e) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    if (!has_ring(S, index)) return Shine{zero, rng};
+    const ShinePoint sp = shine_point(S, K, index, origin, normal, last_vertex, rng);
+    rng = sp.rng;
+    if (!sp.valid) return Shine{zero, rng};
+    const float3 n = xyz(bf(S, index, kRingPlane));
+    float3 shine = zero;
+    const uint32_t count = light_count(S.s);
+#pragma unroll 1
+    for (uint32_t slot = 0; slot < count; ++slot) {
+        const uint32_t i = light_index(S.s, slot);
+        const float4 material = bf(S, i, kMaterial);
+        if (material.w < 0.5f) continue;
+        const LightSample light = sample_light(S, K, Ray{sp.point, n, index}, i, rng);
+        rng = light.rng;
+        const float mu_in = dot(light.d, n);
+        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i);
+        const float3 term = ring_bsdf(sp.optics, sp.mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * vis.v / light.pdf);
+        shine = shine + term;
+        if (vis.v > 0.0f) {
+            GradEntry tau_e, ring_albedo_e;
+            ring_point_entries(S, index, sp.point, sp.optics, sp.mu_out, mu_in, tau_e, ring_albedo_e);
+            G.local_factor(albedo_e);
+            G.local_factor(tau_e);
+            G.local_factor(ring_albedo_e);
+            G.local_factor(emitter_entry(S, i));
+            crossing_factors(G, vis);
+            contribute(G, carried * term * sp.scale, false);
+        }
+    }
+    return Shine{shine * sp.scale, rng};
+}
+
+// Pass 1 hooks.
+__device__ __forceinline__ void record_capture(Recorder &R, uint32_t iteration, float cap, bool cap_direct,
+                                              float3 base) {
+    R.capture_iter = iteration;
+    R.cap = cap;
+    R.cap_direct = cap_direct;
+    R.base = base;
+    R.cap_light = cap_direct ? R.lit_vis_sum : R.lit_sum * kRingIndirectCap;
+}
+
+__device__ __forceinline__ void record_roulette(Recorder &R, uint32_t iteration, float3 t, float s, bool survived,
+                                                float3 radiance) {
+    if (R.capture_iter == 0u) return;
+    if (R.n_rr >= (uint32_t)kMaxRoulette) {
+        R.dropped += 1u;
+        return;
+    }
+    const float mx = fmaxf(t.x, fmaxf(t.y, t.z));
+    const uint32_t m = t.x >= mx ? 0u : (t.y >= mx ? 1u : 2u);
+    const bool clamped = !(mx > 0.05f && mx < 0.95f);
+    R.rr[R.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - R.base};
+}
+
+// Pass 2's weights from pass 1's summary, the path's total radiance and the
+// pixel weight w.
+__device__ __forceinline__ void prb_setup(Prb &G, const Recorder &R, float3 total, float3 w) {
+    const float3 lum = f3(0.2126f, 0.7152f, 0.0722f);
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    G.w_pre = w;
+    G.w_post = w;
+    G.w_pdf = zero;
+    G.w_cap = zero;
+    G.score = 0.0f;
+    G.a = zero;
+    G.b = zero;
+    G.b_total = zero;
+    G.capture_iter = R.capture_iter;
+    G.cap_direct = R.cap_direct;
+    G.binding = false;
+    G.n_rr = 0;
+    G.prev_param = kNoParam;
+    G.prev_dlog_pdf = 0.0f;
+    G.iteration = 0;
+    G.n_local = 0;
+    if (R.capture_iter == 0u) {
+        G.a_total = mul3(w, total);
+        return;
+    }
+    const float3 indirect = total - R.base;
+    const float l = luminance(indirect);
+    if (l > R.cap) {
+        const float s = R.cap / l;
+        const float wc = dot(w, indirect) / l;
+        G.binding = true;
+        G.w_post = (w - lum * wc) * s;
+        G.w_pdf = G.w_post - w;
+        G.w_cap = lum * wc;
+        G.score = (s - 1.0f) * dot(w, indirect);
+        G.b_total = mul3(G.w_pdf, indirect);
+        G.n_rr = R.n_rr;
+        for (uint32_t r = 0; r < R.n_rr && r < (uint32_t)kMaxRoulette; ++r) {
+            const Roulette ev = R.rr[r];
+            G.rr[r] = ev;
+            const bool survived = (ev.bits & 4u) != 0u;
+            G.rr_coef[r] = survived ? G.score - dot(G.w_pdf, indirect - ev.before)
+                                    : -G.score * ev.s / (1.0f - ev.s);
+        }
+    }
+    G.a_total = mul3(w, R.base) + mul3(G.w_post, indirect) + mul3(G.w_cap, R.cap_light);
+}
+
+}  // namespace sg

@@ -504,18 +504,30 @@ struct Shine {
     uint32_t rng;
 };
 
-// ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
+// The ring point ringshine samples (pathtrace.wgsl:1252-1280) and the
+// per-point factors its light loop needs; `valid` false when the point
+// contributes nothing.
+struct ShinePoint {
+    float3 point;
+    Optics optics;
+    float mu_out;
+    float scale;  // cos_surface * weight / (pi * pdf)
+    uint32_t rng;
+    bool valid;
+};
+
 template <bool C, bool L>
-__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
-                                        bool last_vertex, uint32_t rng) {
-    const float3 zero = f3(0.0f, 0.0f, 0.0f);
-    if (!has_ring(S, index)) return Shine{zero, rng};
+__device__ __forceinline__ ShinePoint shine_point(const Scene &S, Counter<C, L> K, uint32_t index, float3 origin,
+                                                  float3 normal, bool last_vertex, uint32_t rng) {
+    ShinePoint out;
+    out.valid = false;
     const float3 n = xyz(bf(S, index, kRingPlane));
     const float inner = bf(S, index, kRingPlane).w;
     const float outer = bf(S, index, kRingParams).x;
     const float radius = sqrtf(mixf(inner * inner, outer * outer, rnd(K, rng))) * b_radius(S, index);
     float sp, cp;
     sincos_turn(rnd(K, rng), &sp, &cp);
+    out.rng = rng;
     const float3 point = basis_direction(n, cp, sp, 0.0f) * radius;
     const float3 offset = point - origin;
     const float distance2 = dot(offset, offset);
@@ -523,13 +535,31 @@ __device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, f
     const float3 direction = offset / distance;
     const float cos_surface = dot(normal, direction);
     const float cos_ring = fabsf(dot(direction, n));
-    if (cos_surface <= 0.0f || cos_ring < 1.0e-6f) return Shine{zero, rng};
+    if (cos_surface <= 0.0f || cos_ring < 1.0e-6f) return out;
     float delta;
     const float blocker = sphere_distance(S, K, Ray{origin, direction, index}, index, b_radius(S, index), delta);
-    if (blocker < distance) return Shine{zero, rng};
-    const Optics optics = ring_optics(S, index, point);
-    if (optics.tau == 0.0f) return Shine{zero, rng};
-    const float mu_out = dot(-direction, n);
+    if (blocker < distance) return out;
+    out.optics = ring_optics(S, index, point);
+    if (out.optics.tau == 0.0f) return out;
+    out.point = point;
+    out.mu_out = dot(-direction, n);
+    const float pdf = distance2 / (ring_area(S, index) * cos_ring);
+    const float weight = last_vertex ? 1.0f : power_weight(pdf, cos_surface / kPi);
+    out.scale = cos_surface * weight / (kPi * pdf);
+    out.valid = true;
+    return out;
+}
+
+// ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
+template <bool C, bool L>
+__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
+                                        bool last_vertex, uint32_t rng) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    if (!has_ring(S, index)) return Shine{zero, rng};
+    const ShinePoint sp = shine_point(S, K, index, origin, normal, last_vertex, rng);
+    rng = sp.rng;
+    if (!sp.valid) return Shine{zero, rng};
+    const float3 n = xyz(bf(S, index, kRingPlane));
     float3 shine = zero;
     const uint32_t count = light_count(S.s);
 #pragma unroll 1
@@ -537,15 +567,13 @@ __device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, f
         const uint32_t i = light_index(S.s, slot);
         const float4 material = bf(S, i, kMaterial);
         if (material.w < 0.5f) continue;
-        const LightSample light = sample_light(S, K, Ray{point, n, index}, i, rng);
+        const LightSample light = sample_light(S, K, Ray{sp.point, n, index}, i, rng);
         rng = light.rng;
         const float mu_in = dot(light.d, n);
-        const float visibility = light_visibility(S, K, ring_origin(S, index, point, light.d), i);
-        shine = shine + ring_bsdf(optics, mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * visibility / light.pdf);
+        const float visibility = light_visibility(S, K, ring_origin(S, index, sp.point, light.d), i);
+        shine = shine + ring_bsdf(sp.optics, sp.mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * visibility / light.pdf);
     }
-    const float pdf = distance2 / (ring_area(S, index) * cos_ring);
-    const float weight = last_vertex ? 1.0f : power_weight(pdf, cos_surface / kPi);
-    return Shine{shine * (cos_surface * weight / (kPi * pdf)), rng};
+    return Shine{shine * sp.scale, rng};
 }
 
 // point_gain (pathtrace.wgsl:1341-1345).

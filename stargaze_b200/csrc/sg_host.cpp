@@ -14,6 +14,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/stargaze_b200.h"
@@ -35,8 +36,14 @@ thread_local std::string g_last_error;
 
 struct History {
     std::vector<uint8_t> key;
+    uint64_t key_hash = 0;
     uint32_t samples = 0;
     uint32_t sequence = 0;
+    // Noise-key runs (first key, count) of the samples behind the
+    // accumulation, for the adjoint's replay; `replayable` false once the
+    // accumulation was restored from outside or the runs overflowed.
+    std::vector<std::pair<uint32_t, uint32_t>> runs;
+    bool replayable = true;
 };
 
 }  // namespace
@@ -71,6 +78,12 @@ struct sg_context {
     float *albedo_map = nullptr;
     uint32_t map_width = 0, map_height = 0;
     float map_extent = 0.0f;
+    // Adjoint buffers, allocated on first use.
+    float *grad = nullptr;                  // kGradMap + texels floats
+    size_t grad_floats = 0;
+    float4 *dl_dimage = nullptr;            // staging of a host d loss / d image
+    size_t dl_pixels = 0;
+    unsigned long long *dropped = nullptr;  // one counter
 };
 
 namespace {
@@ -138,10 +151,18 @@ void append(std::vector<uint8_t> &key, const T &value) {
     key.insert(key.end(), p, p + sizeof(T));
 }
 
+// FNV-1a over the history key: the tape's check that a backward replays
+// the frame its samples were rendered with.
+uint64_t key_hash(const std::vector<uint8_t> &key) {
+    uint64_t h = 1469598103934665603ull;
+    for (uint8_t b : key) h = (h ^ b) * 1099511628211ull;
+    return h;
+}
+
 // History::update (src/pathtracer.rs:173-187): the accumulation survives
 // only while globals, bodies, ground, scene time, bounces, Milky Way
 // brightness (and here the ring tables) are byte-identical.
-void update_history(sg_context *ctx, const sg_frame *frame) {
+std::vector<uint8_t> history_key(const sg_context *ctx, const sg_frame *frame) {
     std::vector<uint8_t> key;
     key.reserve(sizeof(sg_globals) + frame->n_bodies * sizeof(sg_sphere) + frame->n_ground * sizeof(sg_primitive) + 32);
     append(key, *frame->globals);
@@ -155,9 +176,29 @@ void update_history(sg_context *ctx, const sg_frame *frame) {
     append(key, ctx->options.max_bounces);
     append(key, ctx->options.milky_way);
     append(key, ctx->table_version);
+    return key;
+}
+
+void update_history(sg_context *ctx, const sg_frame *frame) {
+    std::vector<uint8_t> key = history_key(ctx, frame);
     if (key != ctx->history.key) {
+        ctx->history.key_hash = key_hash(key);
         ctx->history.key = std::move(key);
         ctx->history.samples = 0;
+        ctx->history.runs.clear();
+        ctx->history.replayable = true;
+    }
+}
+
+// Record a dispatch's noise keys [first, first + count) for the tape.
+void record_run(sg_context *ctx, uint32_t first, uint32_t count) {
+    auto &runs = ctx->history.runs;
+    if (!runs.empty() && runs.back().first + runs.back().second == first) {
+        runs.back().second += count;
+    } else if (runs.size() < SG_TAPE_RANGES) {
+        runs.emplace_back(first, count);
+    } else {
+        ctx->history.replayable = false;
     }
 }
 
@@ -409,6 +450,9 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->prop_trig);
     cudaFree(ctx->terrain);
     cudaFree(ctx->albedo_map);
+    cudaFree(ctx->grad);
+    cudaFree(ctx->dl_dimage);
+    cudaFree(ctx->dropped);
     delete ctx;
     return SG_OK;
 }
@@ -538,6 +582,7 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
         cudaError_t e = sg::launch_trace(p, events != nullptr, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
         ctx->launches += 1;
+        record_run(ctx, s.sampling[0], count);
         if (events) {
             unsigned long long host[sg::kEventCount];
             SG_CUDA(ctx, cudaMemcpyAsync(host, ctx->events, sizeof(host), cudaMemcpyDeviceToHost, stream));
@@ -656,6 +701,9 @@ int sg_set_accumulation(sg_context *ctx, const float *src, int src_on_device, ui
     SG_CUDA(ctx, cudaStreamSynchronize(stream));
     ctx->history.samples = samples;
     ctx->history.sequence = sequence;
+    // The restored samples' noise keys are unknown: no replay.
+    ctx->history.runs.clear();
+    ctx->history.replayable = samples == 0;
     return SG_OK;
 }
 
@@ -820,6 +868,115 @@ int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu, uint32_t 
     cudaError_t e = sg::launch_ring_energy(albedo, tau, mu, steps, d, nullptr);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "ring_energy launch");
     SG_CUDA(ctx, cudaMemcpy(energy, d, sizeof(float), cudaMemcpyDeviceToHost));
+    return SG_OK;
+}
+
+int sg_get_tape(const sg_context *ctx, sg_tape *tape) {
+    if (!ctx || !tape) return fail(nullptr, SG_ERR_INVALID, "ctx or tape is NULL");
+    if (!ctx->history.replayable)
+        return fail(const_cast<sg_context *>(ctx), SG_ERR_STATE,
+                    "the accumulation was restored or mixes too many noise runs and cannot be replayed");
+    std::memset(tape, 0, sizeof(*tape));
+    tape->width = ctx->width;
+    tape->height = ctx->height;
+    tape->samples = ctx->history.samples;
+    tape->n_ranges = (uint32_t)ctx->history.runs.size();
+    for (size_t k = 0; k < ctx->history.runs.size(); ++k) {
+        tape->first[k] = ctx->history.runs[k].first;
+        tape->count[k] = ctx->history.runs[k].second;
+    }
+    tape->history_hash = ctx->history.key_hash;
+    return SG_OK;
+}
+
+int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, const float *dl_dimage, int on_device,
+                sg_gradients *grads, void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (!tape || !dl_dimage || !grads) return fail(ctx, SG_ERR_INVALID, "tape, dl_dimage or grads is NULL");
+    if (tape->width != ctx->width || tape->height != ctx->height)
+        return fail(ctx, SG_ERR_STATE, "the tape was recorded at another viewport size");
+    if (tape->n_ranges > SG_TAPE_RANGES) return fail(ctx, SG_ERR_INVALID, "tape n_ranges exceeds SG_TAPE_RANGES");
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < tape->n_ranges; ++k) total += tape->count[k];
+    if (total != tape->samples || total == 0 || total > SG_MAX_SAMPLES)
+        return fail(ctx, SG_ERR_INVALID, "tape runs must hold 1..SG_MAX_SAMPLES samples in total");
+    int status = validate_frame(ctx, frame);
+    if (status != SG_OK) return status;
+    if (key_hash(history_key(ctx, frame)) != tape->history_hash)
+        return fail(ctx, SG_ERR_STATE, "frame, options or tables differ from the ones the tape was recorded with");
+    grads->dropped = 0;
+    const size_t pixels = (size_t)ctx->width * ctx->height;
+    if (pixels == 0) return SG_OK;
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t texels = ctx->albedo_map ? (size_t)ctx->map_width * ctx->map_height : 0;
+    const size_t floats = sg::kGradMap + texels;
+    if (ctx->grad_floats < floats) {
+        cudaStreamSynchronize(stream);
+        cudaFree(ctx->grad);
+        ctx->grad = nullptr;
+        ctx->grad_floats = 0;
+        SG_CUDA(ctx, cudaMalloc(&ctx->grad, floats * sizeof(float)));
+        ctx->grad_floats = floats;
+    }
+    if (!ctx->dropped) SG_CUDA(ctx, cudaMalloc(&ctx->dropped, sizeof(unsigned long long)));
+    const float4 *d_dl = reinterpret_cast<const float4 *>(dl_dimage);
+    if (!on_device) {
+        if (ctx->dl_pixels < pixels) {
+            cudaStreamSynchronize(stream);
+            cudaFree(ctx->dl_dimage);
+            ctx->dl_dimage = nullptr;
+            ctx->dl_pixels = 0;
+            SG_CUDA(ctx, cudaMalloc(&ctx->dl_dimage, pixels * sizeof(float4)));
+            ctx->dl_pixels = pixels;
+        }
+        SG_CUDA(ctx, cudaMemcpyAsync(ctx->dl_dimage, dl_dimage, pixels * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        d_dl = ctx->dl_dimage;
+    }
+    SG_CUDA(ctx, cudaMemsetAsync(ctx->grad, 0, floats * sizeof(float), stream));
+    SG_CUDA(ctx, cudaMemsetAsync(ctx->dropped, 0, sizeof(unsigned long long), stream));
+    sg_settings s = pack_settings(ctx, frame, 0);
+    status = upload_bodies(ctx, frame, stream);
+    if (status != SG_OK) return status;
+    sg::AdjointParams a;
+    a.dl_dimage = d_dl;
+    a.inv_samples = 1.0f / (float)tape->samples;
+    a.grad = ctx->grad;
+    a.overflow = ctx->dropped;
+    // Shared-memory windows: the used ring-table range (when it is small)
+    // and the per-body colours.
+    uint32_t tau_used = 0;
+    for (uint32_t k = 0; k < SG_RING_TABLE_SLOTS; ++k)
+        if (ctx->ring_bins[k]) tau_used = k * SG_RING_TABLE_MAX_BINS + ctx->ring_bins[k];
+    a.tau_window = tau_used <= 8192u ? tau_used : 0u;
+    a.color_window = 6u * frame->n_bodies;
+    for (uint32_t k = 0; k < tape->n_ranges; ++k) {
+        for (uint32_t done = 0; done < tape->count[k]; done += SG_MAX_BATCH_SAMPLES) {
+            s.sampling[0] = tape->first[k] + done;
+            s.counts[2] = std::min<uint32_t>(SG_MAX_BATCH_SAMPLES, tape->count[k] - done);
+            const sg::TraceParams p = make_params(ctx, s);
+            cudaError_t e = sg::launch_adjoint(p, a, stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
+            ctx->launches += 1;
+        }
+    }
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (grads->ring_tau)
+        SG_CUDA(ctx, cudaMemcpyAsync(grads->ring_tau, ctx->grad, sg::kGradColor * sizeof(float), kind, stream));
+    const float *colors = ctx->grad + sg::kGradColor;
+    if (grads->ring_albedo && frame->n_bodies)
+        SG_CUDA(ctx, cudaMemcpy2DAsync(grads->ring_albedo, 3 * sizeof(float), colors, 6 * sizeof(float),
+                                       3 * sizeof(float), frame->n_bodies, kind, stream));
+    if (grads->body_color && frame->n_bodies)
+        SG_CUDA(ctx, cudaMemcpy2DAsync(grads->body_color, 3 * sizeof(float), colors + 3, 6 * sizeof(float),
+                                       3 * sizeof(float), frame->n_bodies, kind, stream));
+    if (grads->albedo_map && texels)
+        SG_CUDA(ctx, cudaMemcpyAsync(grads->albedo_map, ctx->grad + sg::kGradMap, texels * sizeof(float), kind,
+                                     stream));
+    unsigned long long dropped = 0;
+    SG_CUDA(ctx, cudaMemcpyAsync(&dropped, ctx->dropped, sizeof(dropped), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    grads->dropped = dropped;
     return SG_OK;
 }
 

@@ -63,4 +63,28 @@ cudaError_t launch_fma_peak(int blocks, int iters, float *out, cudaStream_t stre
 cudaError_t launch_ring_energy(float albedo, float tau, float mu, uint32_t steps, float *out,
                                cudaStream_t stream);
 
+// Flat parameter space of the adjoint's gradient buffer:
+//   [0, kGradColor)          ring-table optical depths, slot * MAX_BINS + bin
+//   [kGradColor, kGradMap)   per body: ring albedo rgb, then body colour rgb
+//   [kGradMap, + texels)     albedo-map texels
+constexpr uint32_t kGradColor = SG_RING_TABLE_SLOTS * SG_RING_TABLE_MAX_BINS;
+constexpr uint32_t kGradMap = kGradColor + 6u * SG_BODY_CAPACITY;
+
+// What an adjoint launch reads beyond the integrator's parameters.
+struct AdjointParams {
+    const float4 *dl_dimage;          // d loss / d accumulated pixel (w ignored)
+    float inv_samples;                // 1 / samples behind the accumulation
+    float *grad;                      // kGradMap + texels floats, accumulated
+    uint32_t tau_window;              // shared-memory window over [0, tau_window)
+    uint32_t color_window;            // ... and over [kGradColor, + color_window)
+    unsigned long long *overflow;     // derivative entries dropped (full lists)
+};
+
+// Dynamic shared memory of an adjoint launch.
+size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a);
+
+// Replay the launch's samples (sampling.x, counts.z as for launch_trace)
+// and accumulate the loss gradient into a.grad; the image is not touched.
+cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStream_t stream);
+
 }  // namespace sg

@@ -5,6 +5,7 @@
 // Kahan-compensated per-pixel sum. CTAs cover 16x16 pixel tiles and each
 // warp an 8x4 sub-tile, so neighbouring lanes trace neighbouring pixels and
 // take the same branches as long as possible.
+#include "sg_adjoint.cuh"
 #include "sg_device.cuh"
 #include "sg_internal.h"
 #include "sg_landscape.cuh"
@@ -79,10 +80,14 @@ __device__ __forceinline__ float4 finish_path(const Path &p) {
     return make_float4(radiance.x, radiance.y, radiance.z, 0.0f);
 }
 
-// One iteration of trace()'s loop (pathtrace.wgsl:1380-1607), airless,
-// landscape off. Returns true when the path has ended.
-template <bool C, bool L>
-__device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
+// One iteration of trace()'s loop (pathtrace.wgsl:1380-1607), airless.
+// Returns true when the path has ended. G is the hook set: NoGrad for the
+// forward integrator (every hook compiles out), Recorder for the adjoint's
+// first replay (records the ring-cap vertex and later Russian roulette),
+// Prb for its second (scatters derivatives). Hooks never change the path's
+// own arithmetic or random draws, so all three take the same decisions.
+template <bool C, bool L, class G>
+__device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G &grad) {
     const sg_settings *s = S.s;
     const uint32_t max_vertices = s->counts[3];
     const uint32_t n_bodies = s->counts[0];
@@ -91,6 +96,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
     // Static bound: each of at most max_vertices vertices is preceded by at
     // most n_bodies + 1 null crossings, so valid inputs never reach it.
     if (++p.iterations > max_vertices * (n_bodies + 2u) + 1u) return true;
+    if constexpr (G::grads) grad.iteration = p.iterations;
     K.add(&Events::vertices);
     Ray &ray = p.ray;
     uint32_t &rng = p.rng;
@@ -137,6 +143,12 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
                 ring_mis = power_weight(previous_pdf, shine_pdf);
             }
             shine_body = kMiss;
+            [[maybe_unused]] RingVertexGrad vg{kNoParam, 0.0f, 0.0f};
+            if constexpr (G::grads) vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
+            if constexpr (G::records) {
+                grad.lit_sum = f3(0.0f, 0.0f, 0.0f);
+                grad.lit_vis_sum = f3(0.0f, 0.0f, 0.0f);
+            }
             float unshadowed = 0.0f, direct = 0.0f;
             #pragma unroll 1
             for (uint32_t slot = 0; slot < n_lights; ++slot) {
@@ -146,17 +158,32 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
                 const LightSample light = sample_light(S, K, Ray{ring.p, n, ri}, i, rng);
                 rng = light.rng;
                 const float mu_in = dot(light.d, n);
-                const float visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
+                float visibility;
+                [[maybe_unused]] Visibility vis;
+                if constexpr (G::grads) {
+                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i);
+                    visibility = vis.v;
+                } else {
+                    visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
+                }
                 const float weight = last_vertex ? 1.0f : power_weight(light.pdf, bsdf_pdf);
                 const float3 lit = throughput * ring_bsdf(optics, mu_out, mu_in) * xyz(material) *
                                    (fabsf(mu_in) / light.pdf);
                 radiance = radiance + lit * (visibility * weight * ring_mis);
+                if constexpr (G::grads)
+                    ring_light_grad(S, grad, ri, ring.p, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis,
+                                    last_vertex, vg);
+                if constexpr (G::records) {
+                    grad.lit_sum = grad.lit_sum + lit;
+                    grad.lit_vis_sum = grad.lit_vis_sum + lit * visibility;
+                }
                 const float l = luminance(lit);
                 unshadowed += l;
                 direct += l * visibility;
             }
             if (rnd(K, rng) < transmission) {
                 // Null event: no depth consumed, MIS stays with the last vertex.
+                if constexpr (G::grads) ring_null_grad(S, grad, ri, ring.p, ray.d);
                 ray = ring_origin(S, ri, ring.p, ray.d);
                 null_crossings += 1u;
                 return null_crossings > n_bodies;
@@ -165,6 +192,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
             if (ring_cap > 1.0e29f) {
                 ring_cap = fmaxf(direct, kRingIndirectCap * unshadowed);
                 ring_base = radiance;
+                if constexpr (G::records)
+                    record_capture(grad, p.iterations, ring_cap, direct >= kRingIndirectCap * unshadowed, radiance);
             }
             const float z = 1.0f - 2.0f * rnd(K, rng);
             float sp, cp;
@@ -172,6 +201,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
             const float radial = sqrtf(fmaxf(0.0f, 1.0f - z * z));
             const float3 direction = basis_direction(n, radial * cp, radial * sp, z);
             throughput = throughput * ring_bsdf(optics, mu_out, z) * (fabsf(z) / bsdf_pdf);
+            if constexpr (G::grads) ring_scatter_grad(S, grad, ri, ring.p, optics, mu_out, z, vg, transmission, ray.d);
             previous_pdf = bsdf_pdf;
             ray = ring_origin(S, ri, ring.p, direction);
             previous_vertex = ray;
@@ -179,7 +209,9 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
             null_crossings = 0u;
             if (depth >= 3u) {
                 const float survival = clampf(max3(throughput), 0.05f, 0.95f);
-                if (rnd(K, rng) >= survival) return true;
+                const bool survived = !(rnd(K, rng) >= survival);
+                if constexpr (G::records) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+                if (!survived) return true;
                 throughput = throughput / survival;
             }
             return false;
@@ -202,6 +234,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
                 weight = power_weight(previous_pdf, light_pdf);
             }
             radiance = radiance + throughput * xyz(bf(S, bi, kMaterial)) * weight;
+            if constexpr (G::grads)
+                emitter_grad(S, grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
             return true;
         }
         K.add(&Events::surface_events);
@@ -226,6 +260,18 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
             outgoing = Ray{normal * (radius * (1.0f + 2.0e-6f)), normal, bi};
         }
         const bool last_vertex = depth + 1u == max_vertices;
+        // The adjoint needs the albedo (and its parameter) before the light
+        // loop; the forward evaluates it after, as the WGSL does.
+        [[maybe_unused]] float3 albedo_g = f3(0.0f, 0.0f, 0.0f);
+        [[maybe_unused]] GradEntry albedo_e = no_entry();
+        if constexpr (G::grads) {
+            if constexpr (L) {
+                albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+            } else {
+                albedo_g = surface_albedo(S, bi, normal);
+            }
+            albedo_e = albedo_entry<L>(S, ray, hit.t, bi, albedo_g);
+        }
         float3 direct_light = f3(0.0f, 0.0f, 0.0f);
         #pragma unroll 1
             for (uint32_t slot = 0; slot < n_lights; ++slot) {
@@ -237,11 +283,23 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
             const float cosine = fmaxf(dot(normal, sample.d), 0.0f);
             if (cosine <= 0.0f) continue;
             outgoing.d = sample.d;
-            const float visibility = light_visibility(S, K, outgoing, i);
+            float visibility;
+            [[maybe_unused]] Visibility vis;
+            if constexpr (G::grads) {
+                vis = light_visibility_grad(S, K, outgoing, i);
+                visibility = vis.v;
+            } else {
+                visibility = light_visibility(S, K, outgoing, i);
+            }
             if (visibility > 0.0f) {
                 const float bsdf_pdf = cosine / kPi;
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
                 direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
+                if constexpr (G::grads)
+                    surface_light_grad(S, grad, albedo_e, i,
+                                       throughput * albedo_g * xyz(light_material) *
+                                           (bsdf_pdf * weight * visibility / sample.pdf),
+                                       vis);
             }
         }
         float3 albedo;
@@ -252,7 +310,12 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
         }
         radiance = radiance + throughput * albedo * direct_light;
         if (!local && has_ring(S, bi)) {
-            const Shine shine = ringshine(S, K, bi, outgoing.o, normal, last_vertex, rng);
+            Shine shine;
+            if constexpr (G::grads)
+                shine = ringshine_grad(S, K, bi, outgoing.o, normal, last_vertex, rng, grad, throughput * albedo,
+                                       albedo_e);
+            else
+                shine = ringshine(S, K, bi, outgoing.o, normal, last_vertex, rng);
             rng = shine.rng;
             radiance = radiance + throughput * albedo * shine.radiance;
         }
@@ -268,9 +331,15 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p) {
         outgoing.d = basis_direction(normal, su * cp, su * sp, cosine);
         previous_pdf = cosine / kPi;
         throughput = throughput * albedo;
+        if constexpr (G::grads) {
+            factor(grad, albedo_e);
+            grad.prev_param = kNoParam;
+        }
         if (depth >= 2u) {
             const float survival = clampf(max3(throughput), 0.05f, 0.95f);
-            if (rnd(K, rng) >= survival) return true;
+            const bool survived = !(rnd(K, rng) >= survival);
+            if constexpr (G::records) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+            if (!survived) return true;
             throughput = throughput / survival;
         }
         ray = outgoing;
@@ -294,6 +363,11 @@ __device__ __forceinline__ Scene stage_scene(const TraceParams &P, float4 *smem)
     sc.B = smem;
     sc.tables = P.staged_table_floats > 0u ? staged : P.tables;
     return sc;
+}
+
+// Floats of dynamic shared memory stage_scene fills.
+__device__ __forceinline__ uint32_t trace_smem_floats(const TraceParams &P) {
+    return P.s.counts[0] * (uint32_t)kBodyVec4 * 4u + P.staged_table_floats;
 }
 
 __device__ __forceinline__ void flush_events(const Events &ev, unsigned long long *events) {
@@ -336,9 +410,10 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
         // measured 20 % slower on the ring workload.
         float4 total = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         Path path;
+        NoGrad nograd;
         for (uint32_t smp = 0; smp < z; ++smp) {
             start_path(path, &P.s, K, pixel, x, y, smp);
-            while (!step(S, K, path)) {
+            while (!step(S, K, path, nograd)) {
             }
             const float4 r = finish_path(path);
             total.x += r.x;
@@ -372,6 +447,80 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
                                     __fdiv_rn(__fsub_rn(sum.w, comp.w), new_count));
     }
     if constexpr (C) flush_events(ev, P.events);
+}
+
+// ---------------------------------------------------------------------------
+// Path-replay adjoint
+// ---------------------------------------------------------------------------
+// One sample's derivative: pass 1 replays the path without derivatives and
+// records what pass 2 needs to weigh each factor by the radiance gathered
+// after it (sg_adjoint.cuh); pass 2 replays it again and scatters.
+// `lanes`: the warp's lanes that run the same samples; they meet after
+// each pass so that a warp replays one pass at a time (lanes left to drift
+// between the two passes would run two copies of the integrator apart).
+template <bool L>
+__device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L> K, Recorder &R, Prb &G, float3 w,
+                                               uint32_t pixel, uint32_t x, uint32_t y, uint32_t smp,
+                                               unsigned lanes) {
+    Path path;
+    start_path(path, S.s, K, pixel, x, y, smp);
+    R.capture_iter = 0;
+    R.n_rr = 0;
+    while (!step(S, K, path, R)) {
+    }
+    __syncwarp(lanes);
+    prb_setup(G, R, path.radiance, w);
+    start_path(path, S.s, K, pixel, x, y, smp);
+    while (!step(S, K, path, G)) {
+    }
+    __syncwarp(lanes);
+}
+
+// Resident CTAs per SM the adjoint is compiled for.
+#ifndef SG_ADJOINT_MIN_BLOCKS
+#define SG_ADJOINT_MIN_BLOCKS 2
+#endif
+
+template <bool L>
+__global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
+    adjoint_kernel(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A) {
+    extern __shared__ float4 smem[];
+    float *window = reinterpret_cast<float *>(smem) + trace_smem_floats(P);
+    const uint32_t window_n = A.tau_window + A.color_window;
+    for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) window[k] = 0.0f;
+    const Scene S = stage_scene(P, smem);  // synchronises the block
+    const Counter<false, L> K{nullptr};
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
+    Recorder R;
+    R.dropped = 0;
+    Prb G;
+    G.sink = GradSink{window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.dropped = 0;
+    const bool inside = x < P.width && y < P.height;
+    const uint32_t pixel = inside ? y * P.width + x : 0u;
+    float3 w = f3(0.0f, 0.0f, 0.0f);
+    if (inside) {
+        const float4 d = A.dl_dimage[pixel];
+        w = f3(d.x, d.y, d.z) * A.inv_samples;
+    }
+    const bool busy = w.x != 0.0f || w.y != 0.0f || w.z != 0.0f;
+    const unsigned lanes = __ballot_sync(0xffffffffu, busy);
+    if (busy) {
+        const uint32_t z = P.s.counts[2];
+#pragma unroll 1
+        for (uint32_t smp = 0; smp < z; ++smp) adjoint_sample(S, K, R, G, w, pixel, x, y, smp, lanes);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) {
+        const float v = window[k];
+        if (v != 0.0f) atomicAdd(A.grad + (k < A.tau_window ? k : kGradColor + (k - A.tau_window)), v);
+    }
+    unsigned long long dropped = (unsigned long long)G.dropped + R.dropped;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dropped += __shfl_down_sync(0xffffffffu, dropped, o);
+    if (lane == 0u && dropped != 0ull && A.overflow) atomicAdd(A.overflow, dropped);
 }
 
 __device__ __forceinline__ Ray load_ray(const sg_ray &in) {
@@ -595,6 +744,22 @@ cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t s
         if (land) trace_kernel<false, true><<<grid, kThreads, smem, stream>>>(p);
         else trace_kernel<false, false><<<grid, kThreads, smem, stream>>>(p);
     }
+    return cudaGetLastError();
+}
+
+size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a) {
+    return trace_smem_bytes(p) + (size_t)(a.tau_window + a.color_window) * sizeof(float);
+}
+
+cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStream_t stream) {
+    const size_t smem = adjoint_smem_bytes(p, a);
+    const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
+    const bool land = p.s.g.ground_north[3] != 0.0f;
+    const void *fn = land ? (const void *)adjoint_kernel<true> : (const void *)adjoint_kernel<false>;
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    if (land) adjoint_kernel<true><<<grid, kThreads, smem, stream>>>(p, a);
+    else adjoint_kernel<false><<<grid, kThreads, smem, stream>>>(p, a);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,7 @@ class PathTracer:
     def __init__(self, dimensions: tuple[int, int], options: abi.Options | None = None, device: int = 0):
         self._lib = load()
         self._ctx = C.c_void_p()
+        self._map_shape: tuple[int, int] | None = None
         opts = options if options is not None else abi.default_options()
         check(self._lib.sg_create(device, int(dimensions[0]), int(dimensions[1]), C.byref(opts), C.byref(self._ctx)))
 
@@ -129,9 +130,11 @@ class PathTracer:
         surface frame; None removes it."""
         if albedo is None:
             check(self._lib.sg_upload_albedo_map(self._ctx, None, 0, 0, 0.0), self._ctx)
+            self._map_shape = None
             return
         a = np.ascontiguousarray(albedo, dtype=np.float32)
         check(self._lib.sg_upload_albedo_map(self._ctx, _ptr(a), a.shape[1], a.shape[0], extent_m), self._ctx)
+        self._map_shape = (a.shape[0], a.shape[1])
 
     def read_pixels(self, stream=None) -> np.ndarray:
         """The accumulation as a (height*width, 4) float32 array."""
@@ -203,6 +206,45 @@ class PathTracer:
         check(self._lib.sg_ring_energy(self._ctx, albedo, tau, mu, steps, C.byref(e)), self._ctx)
         return e.value
 
+    # -- adjoint (extension) ----------------------------------------------
+    def tape(self) -> abi.Tape:
+        """The replay record of the current accumulation."""
+        t = abi.Tape()
+        check(self._lib.sg_get_tape(self._ctx, C.byref(t)), self._ctx)
+        return t
+
+    def backward(self, frame: Frame, tape: abi.Tape, dl_dimage, stream=None) -> "Gradients":
+        """Gradient of a loss with d loss / d image = `dl_dimage` ((h*w, 4) or
+        (h, w, 4) float32; w channel ignored) w.r.t. the ring tables, ring
+        albedos, body colours and albedo map, replaying `tape` on `frame`."""
+        w, h = self.size()
+        dl = np.ascontiguousarray(np.asarray(dl_dimage, dtype=np.float32).reshape(w * h, 4))
+        n = len(frame.bodies)
+        out = Gradients(
+            ring_tau=np.zeros((abi.RING_TABLE_SLOTS, abi.RING_TABLE_MAX_BINS), dtype=np.float32),
+            ring_albedo=np.zeros((n, 3), dtype=np.float32),
+            body_color=np.zeros((n, 3), dtype=np.float32),
+            albedo_map=np.zeros(self._map_shape, dtype=np.float32) if self._map_shape else None,
+        )
+        g = abi.Gradients(_ptr(out.ring_tau), _ptr(out.ring_albedo), _ptr(out.body_color),
+                          _ptr(out.albedo_map) if out.albedo_map is not None else None, 0)
+        view = frame.view()
+        check(self._lib.sg_backward(self._ctx, C.byref(view), C.byref(tape), _ptr(dl), 0, C.byref(g),
+                                    _stream_handle(stream)), self._ctx)
+        out.dropped = int(g.dropped)
+        return out
+
+
+class Gradients:
+    """d loss / d parameter blocks returned by PathTracer.backward."""
+
+    def __init__(self, ring_tau, ring_albedo, body_color, albedo_map):
+        self.ring_tau = ring_tau        # (slots, max bins)
+        self.ring_albedo = ring_albedo  # (bodies, 3)
+        self.body_color = body_color    # (bodies, 3)
+        self.albedo_map = albedo_map    # (map height, map width) or None
+        self.dropped = 0
+
 
 RAY_DTYPE = np.dtype([("offset", "<f4", 3), ("direction", "<f4", 3), ("anchor", "<u4")])
 HIT_DTYPE = np.dtype([("distance", "<f4"), ("index", "<u4"), ("normal", "<f4", 3)])
@@ -220,4 +262,4 @@ def rays_array(offsets, directions, anchors) -> np.ndarray:
     return rays
 
 
-__all__ = ["PathTracer", "StargazeError", "RAY_DTYPE", "HIT_DTYPE", "rays_array"]
+__all__ = ["PathTracer", "Gradients", "StargazeError", "RAY_DTYPE", "HIT_DTYPE", "rays_array"]
