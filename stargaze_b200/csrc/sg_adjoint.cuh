@@ -53,7 +53,8 @@ constexpr uint32_t kPdfBit = 0x40000000u;     // attached-only (scalar) entry
 constexpr uint32_t kParamMask = 0x3fffffffu;
 constexpr int kMaxRoulette = 6;               // recorded events after a cap vertex
 constexpr int kMaxLocal = 8;                  // factors of one contribution
-constexpr int kMaxCrossings = 2;              // ring crossings of one shadow ray
+constexpr int kMaxCrossings = kMaxRecordedCrossings;  // of one shadow ray
+constexpr uint32_t kColorSlots = 4;           // bodies with per-thread colour sums
 
 struct GradEntry {
     uint32_t param;  // kNoParam: none
@@ -62,9 +63,14 @@ struct GradEntry {
 
 __device__ __forceinline__ GradEntry no_entry() { return GradEntry{kNoParam, make_float3(0.0f, 0.0f, 0.0f)}; }
 
-// Where gradients land: shared-memory windows over the hot parameters (the
-// ring tables in use and the body colours), global memory for the rest.
+// Where gradients land: the colours of the first kColorSlots bodies in
+// per-thread sums (every lane of a warp hits the same few of them; the
+// kernel reduces them once at its end), shared-memory windows over the
+// ring tables in use and the other body colours, global memory for the
+// rest.
 struct GradSink {
+    float *own;         // per-thread sums over [kGradColor, kGradColor + own_n)
+    uint32_t own_n;
     float *tau;
     uint32_t tau_n;
     float *color;
@@ -72,16 +78,17 @@ struct GradSink {
     float *global;
     __device__ __forceinline__ void add(uint32_t param, float value) const {
         if (value == 0.0f) return;
-        if (param < tau_n) atomicAdd(tau + param, value);
-        else if (param - kGradColor < color_n) atomicAdd(color + (param - kGradColor), value);
+        const uint32_t c = param - kGradColor;
+        if (c < own_n) own[c] += value;
+        else if (param < tau_n) atomicAdd(tau + param, value);
+        else if (c < color_n) atomicAdd(color + c, value);
         else atomicAdd(global + param, value);
     }
 };
 
 // The forward integrator: no hooks.
 struct NoGrad {
-    static constexpr bool records = false;
-    static constexpr bool grads = false;
+    static constexpr bool adjoint = false;
 };
 
 // A Russian-roulette decision after the cap vertex (pathtrace.wgsl:
@@ -93,25 +100,21 @@ struct Roulette {
     float3 before;  // radiance gathered since the cap vertex, before it
 };
 
-// Pass 1: the summary pass 2 needs.
-struct Recorder {
-    static constexpr bool records = true;
-    static constexpr bool grads = false;
-    uint32_t capture_iter;  // iteration of the cap vertex, 0 when none
+// The adjoint's state. Both passes run the same integrator code (one
+// instantiation, so a warp's instruction footprint is that of one replay);
+// `pass2` selects the hooks: pass 1 records the summary pass 2 needs, pass 2
+// scatters derivatives.
+struct Prb {
+    static constexpr bool adjoint = true;
+    bool pass2;
+    // Pass 1's summary.
     float cap;
-    bool cap_direct;        // cap = shadowed sum (else 0.003 * unshadowed)
     float3 base;            // radiance at the cap vertex's scatter
     float3 cap_light;       // the rgb sum whose luminance is the cap
     float3 lit_sum, lit_vis_sum;  // at the current ring vertex
-    uint32_t n_rr, dropped;
-    Roulette rr[kMaxRoulette];
-};
-
-// Pass 2: weights and running sums.
-struct Prb {
-    static constexpr bool records = false;
-    static constexpr bool grads = true;
+    // Pass 2.
     GradSink sink;
+    const float4 *inv;        // per body: 1 / colour, 1 / ring colour
     float3 w_pre, w_post, w_pdf, w_cap;  // contribution weights (see above)
     float score;
     float3 a_total, b_total;  // weighted radiance of the whole path
@@ -128,6 +131,7 @@ struct Prb {
     uint32_t n_local, dropped;
 
     __device__ __forceinline__ bool post() const { return capture_iter != 0u && iteration > capture_iter; }
+    __device__ __forceinline__ bool grads() const { return pass2; }
     __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
     __device__ __forceinline__ void local_factor(GradEntry e) {
         if (e.param == kNoParam) return;
@@ -152,8 +156,11 @@ __device__ __forceinline__ uint32_t ring_albedo_param(uint32_t body) { return kG
 __device__ __forceinline__ uint32_t body_color_param(uint32_t body) { return kGradColor + 6u * body + 3u; }
 
 // Emitted radiance of a light (or an emitter hit): d log / d colour.
-__device__ __forceinline__ GradEntry emitter_entry(const Scene &S, uint32_t body) {
-    return vector_entry(body_color_param(body), inv3(xyz(bf(S, body, kMaterial))));
+__device__ __forceinline__ GradEntry emitter_entry(const Prb &G, uint32_t body) {
+    return vector_entry(body_color_param(body), xyz(G.inv[2u * body]));
+}
+__device__ __forceinline__ GradEntry ring_albedo_entry(const Prb &G, uint32_t body) {
+    return vector_entry(ring_albedo_param(body), xyz(G.inv[2u * body + 1u]));
 }
 
 // Scatter `w . dlog` of one entry: per channel for a vector entry, the
@@ -281,15 +288,6 @@ __device__ __forceinline__ float scatter_pdf_dlog(float tau, float mu_out, float
     return (x < 1.0e-3f ? 1.0f - x : expf(-x)) * (scale / m) / p;
 }
 
-// The slab BSDF's entries at a ring point: optical depth and albedo.
-__device__ __forceinline__ void ring_point_entries(const Scene &S, uint32_t body, float3 point, const Optics &o,
-                                                   float outgoing, float incoming, GradEntry &tau_e,
-                                                   GradEntry &albedo_e) {
-    float scale = 0.0f;
-    const uint32_t tp = tau_param(S, body, point, &scale);
-    tau_e = tp == kNoParam ? no_entry() : scalar_entry(tp, scale * ring_bsdf_dlog_tau(o.tau, outgoing, incoming));
-    albedo_e = vector_entry(ring_albedo_param(body), inv3(xyz(bf(S, body, kRingColor))));
-}
 
 // A crossing multiplies by exp(-tau / |mu|) (rings.wgsl:83-86):
 // d log / d table = -scale / |mu|.
@@ -302,7 +300,7 @@ __device__ __forceinline__ GradEntry crossing_entry(const Scene &S, uint32_t bod
 }
 
 // light_visibility (rings.wgsl:90-115) that also returns the ring crossings
-// behind its transmission, for the adjoint.
+// behind its transmission as derivative entries, for the adjoint.
 struct Visibility {
     float v;
     uint32_t n;
@@ -310,23 +308,22 @@ struct Visibility {
 };
 
 template <bool C, bool L>
-__device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
+__device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L> K, Ray r, uint32_t light,
+                                                         bool entries) {
+    Crossings rec;
+    rec.n = 0;
     Visibility out;
-    out.v = light_visibility(S, K, r, light);
+    out.v = visibility_core(S, K, r, light, &rec);
     out.n = 0;
-    if (out.v <= 0.0f) return out;
-    float delta;
-    const float surface = sphere_distance(S, K, r, light, b_radius(S, light), delta);
-    const uint32_t n = S.s->counts[0];
-#pragma unroll 1
-    for (uint32_t i = 0; i < n; ++i) {
-        const RingHit h = ring_hit(S, K, r, i);
-        if (h.index == kMiss || !(h.t < surface)) continue;
-        const GradEntry e = crossing_entry(S, i, h.p, r.d);
-        if (e.param == kNoParam) continue;
-        if (out.n < (uint32_t)kMaxCrossings) out.cross[out.n] = e;
-        out.n += 1u;  // more than kMaxCrossings: counted as dropped
+    if (out.v <= 0.0f || !entries) return out;
+#pragma unroll
+    for (int k = 0; k < kMaxCrossings; ++k) {
+        if ((uint32_t)k >= rec.n) break;
+        const GradEntry e = crossing_entry(S, rec.body[k], rec.point[k], r.d);
+        if (e.param != kNoParam) out.cross[out.n++] = e;
     }
+    // Crossings beyond the record are counted as dropped.
+    if (rec.n > (uint32_t)kMaxCrossings) out.n += rec.n - (uint32_t)kMaxCrossings;
     return out;
 }
 
@@ -353,17 +350,24 @@ __device__ __noinline__ RingVertexGrad ring_vertex_grad(Scene S, uint32_t ring, 
     return v;
 }
 
+// The slab BSDF's optical-depth entry at a ring vertex for an incoming
+// cosine.
+__device__ __forceinline__ GradEntry ring_tau_entry(const RingVertexGrad &v, float tau, float outgoing,
+                                                    float incoming) {
+    return v.param == kNoParam ? no_entry() : scalar_entry(v.param, v.scale * ring_bsdf_dlog_tau(tau, outgoing, incoming));
+}
+
 // One light sample at a ring vertex (pathtrace.wgsl:1437-1450): its
 // radiance, and at the cap vertex of a binding path its term of the cap
 // (max(shadowed, 0.003 * unshadowed) luminance of `lit`). After the cap
 // vertex the MIS weight's dependence on the vertex's scatter pdf is an
 // attached entry.
-__device__ __noinline__ void ring_light_grad(Scene S, Prb &G, uint32_t ring, float3 point, Optics optics,
-                                             float mu_out, float mu_in, uint32_t light, float3 lit, Visibility vis,
-                                             float weight, float ring_mis, bool last_vertex, RingVertexGrad vg) {
-    GradEntry tau_e, albedo_e;
-    ring_point_entries(S, ring, point, optics, mu_out, mu_in, tau_e, albedo_e);
-    const GradEntry light_e = emitter_entry(S, light);
+__device__ __noinline__ void ring_light_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
+                                             float mu_in, uint32_t light, float3 lit, Visibility vis, float weight,
+                                             float ring_mis, bool last_vertex, RingVertexGrad vg) {
+    const GradEntry tau_e = ring_tau_entry(vg, optics.tau, mu_out, mu_in);
+    const GradEntry albedo_e = ring_albedo_entry(G, ring);
+    const GradEntry light_e = emitter_entry(G, light);
     const float3 value = lit * (vis.v * weight * ring_mis);
     if (value.x != 0.0f || value.y != 0.0f || value.z != 0.0f) {
         G.local_factor(tau_e);
@@ -398,13 +402,10 @@ __device__ __noinline__ void ring_null_grad(Scene S, Prb &G, uint32_t ring, floa
 // a binding cap vertex also the decision's score d log(1 - T) and the
 // attached 1 / scatter pdf. Records the vertex for the MIS weight of an
 // emitter reached next.
-__device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, float3 point, Optics optics,
-                                               float mu_out, float z, RingVertexGrad v, float transmission,
-                                               float3 d) {
-    GradEntry tau_e, albedo_e;
-    ring_point_entries(S, ring, point, optics, mu_out, z, tau_e, albedo_e);
-    factor(G, tau_e);
-    factor(G, albedo_e);
+__device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
+                                               float z, RingVertexGrad v, float transmission, float3 d) {
+    factor(G, ring_tau_entry(v, optics.tau, mu_out, z));
+    factor(G, ring_albedo_entry(G, ring));
     if (G.binding && v.param != kNoParam) {
         const float dlog_t = -v.scale / fmaxf(fabsf(dot_rn(d, xyz(bf(S, ring, kRingPlane)))), 1.0e-7f);
         if (transmission < 1.0f) score(G, v.param, -dlog_t * transmission / (1.0f - transmission));
@@ -415,10 +416,10 @@ __device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, f
 }
 
 // One light sample at a surface vertex (pathtrace.wgsl:1545-1565).
-__device__ __noinline__ void surface_light_grad(Scene S, Prb &G, GradEntry albedo_e, uint32_t light, float3 value,
+__device__ __noinline__ void surface_light_grad(Prb &G, GradEntry albedo_e, uint32_t light, float3 value,
                                                 Visibility vis) {
     G.local_factor(albedo_e);
-    G.local_factor(emitter_entry(S, light));
+    G.local_factor(emitter_entry(G, light));
     crossing_factors(G, vis);
     contribute(G, value, false);
 }
@@ -426,8 +427,8 @@ __device__ __noinline__ void surface_light_grad(Scene S, Prb &G, GradEntry albed
 // An emitter reached by the path (pathtrace.wgsl:1516-1526); `mis` is the
 // MIS weight against the previous vertex's light sample, whose bsdf pdf
 // (a ring scatter's) moves with that vertex's optical depth.
-__device__ __noinline__ void emitter_grad(Scene S, Prb &G, uint32_t body, float3 value, float mis, bool weighted) {
-    G.local_factor(emitter_entry(S, body));
+__device__ __noinline__ void emitter_grad(Prb &G, uint32_t body, float3 value, float mis, bool weighted) {
+    G.local_factor(emitter_entry(G, body));
     if (G.binding && G.post() && weighted && G.prev_param != kNoParam)
         G.local_factor(scalar_entry(G.prev_param | kPdfBit, 2.0f * (1.0f - mis) * G.prev_dlog_pdf));
     contribute(G, value, false);
@@ -437,12 +438,13 @@ __device__ __noinline__ void emitter_grad(Scene S, Prb &G, uint32_t body, float3
 // (zero where the clamp of surface_albedo is active), or the albedo-map
 // texel of the host ground.
 template <bool L>
-__device__ __noinline__ GradEntry albedo_entry(Scene S, Ray ray, float t, uint32_t index, float3 albedo) {
+__device__ __noinline__ GradEntry albedo_entry(Scene S, const float4 *inv, Ray ray, float t, uint32_t index,
+                                               float3 albedo) {
     if (index < kLocalBase) {
-        const float3 m = xyz(bf(S, index, kMaterial));
-        const float3 d = f3(albedo.x > 0.0f && albedo.x < 1.0f ? inv_or_zero(m.x) : 0.0f,
-                            albedo.y > 0.0f && albedo.y < 1.0f ? inv_or_zero(m.y) : 0.0f,
-                            albedo.z > 0.0f && albedo.z < 1.0f ? inv_or_zero(m.z) : 0.0f);
+        const float4 m = inv[2u * index];
+        const float3 d = f3(albedo.x > 0.0f && albedo.x < 1.0f ? m.x : 0.0f,
+                            albedo.y > 0.0f && albedo.y < 1.0f ? m.y : 0.0f,
+                            albedo.z > 0.0f && albedo.z < 1.0f ? m.z : 0.0f);
         return vector_entry(body_color_param(index), d);
     }
     if constexpr (L) {
@@ -467,6 +469,9 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
     rng = sp.rng;
     if (!sp.valid) return Shine{zero, rng};
     const float3 n = xyz(bf(S, index, kRingPlane));
+    float scale = 0.0f;
+    const uint32_t tp = G.pass2 ? tau_param(S, index, sp.point, &scale) : kNoParam;
+    const RingVertexGrad vg{tp, scale, 0.0f};
     float3 shine = zero;
     const uint32_t count = light_count(S.s);
 #pragma unroll 1
@@ -477,16 +482,14 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
         const LightSample light = sample_light(S, K, Ray{sp.point, n, index}, i, rng);
         rng = light.rng;
         const float mu_in = dot(light.d, n);
-        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i);
+        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i, G.pass2);
         const float3 term = ring_bsdf(sp.optics, sp.mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * vis.v / light.pdf);
         shine = shine + term;
-        if (vis.v > 0.0f) {
-            GradEntry tau_e, ring_albedo_e;
-            ring_point_entries(S, index, sp.point, sp.optics, sp.mu_out, mu_in, tau_e, ring_albedo_e);
+        if (G.pass2 && vis.v > 0.0f) {
             G.local_factor(albedo_e);
-            G.local_factor(tau_e);
-            G.local_factor(ring_albedo_e);
-            G.local_factor(emitter_entry(S, i));
+            G.local_factor(ring_tau_entry(vg, sp.optics.tau, sp.mu_out, mu_in));
+            G.local_factor(ring_albedo_entry(G, index));
+            G.local_factor(emitter_entry(G, i));
             crossing_factors(G, vis);
             contribute(G, carried * term * sp.scale, false);
         }
@@ -495,33 +498,42 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
 }
 
 // Pass 1 hooks.
-__device__ __forceinline__ void record_capture(Recorder &R, uint32_t iteration, float cap, bool cap_direct,
-                                              float3 base) {
-    R.capture_iter = iteration;
-    R.cap = cap;
-    R.cap_direct = cap_direct;
-    R.base = base;
-    R.cap_light = cap_direct ? R.lit_vis_sum : R.lit_sum * kRingIndirectCap;
+__device__ __forceinline__ void record_capture(Prb &G, uint32_t iteration, float cap, bool cap_direct, float3 base) {
+    G.capture_iter = iteration;
+    G.cap = cap;
+    G.cap_direct = cap_direct;
+    G.base = base;
+    G.cap_light = cap_direct ? G.lit_vis_sum : G.lit_sum * kRingIndirectCap;
 }
 
-__device__ __forceinline__ void record_roulette(Recorder &R, uint32_t iteration, float3 t, float s, bool survived,
-                                                float3 radiance) {
-    if (R.capture_iter == 0u) return;
-    if (R.n_rr >= (uint32_t)kMaxRoulette) {
-        R.dropped += 1u;
+__device__ __noinline__ void record_roulette(Prb &G, uint32_t iteration, float3 t, float s, bool survived,
+                                             float3 radiance) {
+    if (G.capture_iter == 0u) return;
+    if (G.n_rr >= (uint32_t)kMaxRoulette) {
+        G.dropped += 1u;
         return;
     }
     const float mx = fmaxf(t.x, fmaxf(t.y, t.z));
     const uint32_t m = t.x >= mx ? 0u : (t.y >= mx ? 1u : 2u);
     const bool clamped = !(mx > 0.05f && mx < 0.95f);
-    R.rr[R.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - R.base};
+    G.rr[G.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - G.base};
+}
+
+// Start of pass 1.
+__device__ __forceinline__ void pass1_setup(Prb &G) {
+    G.pass2 = false;
+    G.capture_iter = 0;
+    G.n_rr = 0;
+    G.binding = false;
+    G.iteration = 0;
 }
 
 // Pass 2's weights from pass 1's summary, the path's total radiance and the
 // pixel weight w.
-__device__ __forceinline__ void prb_setup(Prb &G, const Recorder &R, float3 total, float3 w) {
+__device__ __noinline__ void pass2_setup(Prb &G, float3 total, float3 w) {
     const float3 lum = f3(0.2126f, 0.7152f, 0.0722f);
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    G.pass2 = true;
     G.w_pre = w;
     G.w_post = w;
     G.w_pdf = zero;
@@ -530,22 +542,19 @@ __device__ __forceinline__ void prb_setup(Prb &G, const Recorder &R, float3 tota
     G.a = zero;
     G.b = zero;
     G.b_total = zero;
-    G.capture_iter = R.capture_iter;
-    G.cap_direct = R.cap_direct;
     G.binding = false;
-    G.n_rr = 0;
     G.prev_param = kNoParam;
     G.prev_dlog_pdf = 0.0f;
     G.iteration = 0;
     G.n_local = 0;
-    if (R.capture_iter == 0u) {
+    if (G.capture_iter == 0u) {
         G.a_total = mul3(w, total);
         return;
     }
-    const float3 indirect = total - R.base;
+    const float3 indirect = total - G.base;
     const float l = luminance(indirect);
-    if (l > R.cap) {
-        const float s = R.cap / l;
+    if (l > G.cap) {
+        const float s = G.cap / l;
         const float wc = dot(w, indirect) / l;
         G.binding = true;
         G.w_post = (w - lum * wc) * s;
@@ -553,16 +562,16 @@ __device__ __forceinline__ void prb_setup(Prb &G, const Recorder &R, float3 tota
         G.w_cap = lum * wc;
         G.score = (s - 1.0f) * dot(w, indirect);
         G.b_total = mul3(G.w_pdf, indirect);
-        G.n_rr = R.n_rr;
-        for (uint32_t r = 0; r < R.n_rr && r < (uint32_t)kMaxRoulette; ++r) {
-            const Roulette ev = R.rr[r];
-            G.rr[r] = ev;
+        for (uint32_t r = 0; r < G.n_rr && r < (uint32_t)kMaxRoulette; ++r) {
+            const Roulette ev = G.rr[r];
             const bool survived = (ev.bits & 4u) != 0u;
             G.rr_coef[r] = survived ? G.score - dot(G.w_pdf, indirect - ev.before)
                                     : -G.score * ev.s / (1.0f - ev.s);
         }
+    } else {
+        G.n_rr = 0;
     }
-    G.a_total = mul3(w, R.base) + mul3(G.w_post, indirect) + mul3(G.w_cap, R.cap_light);
+    G.a_total = mul3(w, G.base) + mul3(G.w_post, indirect) + mul3(G.w_cap, G.cap_light);
 }
 
 }  // namespace sg

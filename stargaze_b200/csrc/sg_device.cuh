@@ -427,11 +427,21 @@ __device__ __forceinline__ float ring_transmission(const Scene &S, const Ray &r,
     return ring_transmission_tau(r.d, xyz(bf(S, h.index, kRingPlane)), ring_optics(S, h.index, h.p).tau);
 }
 
+// The ring crossings behind a visibility, for the adjoint: body and
+// planet-local point of each (the first kMaxRecordedCrossings).
+constexpr int kMaxRecordedCrossings = 2;
+struct Crossings {
+    uint32_t n;
+    uint32_t body[kMaxRecordedCrossings];
+    float3 point[kMaxRecordedCrossings];
+};
+
 // light_visibility (rings.wgsl:90-115): distance to the light, any-hit over
 // the other spheres (ties broken by index), then ring transmissions before
-// the light.
+// the light. With a Crossings record it also lists the ring crossings.
 template <bool C, bool L>
-__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
+__device__ __forceinline__ float visibility_core(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t light,
+                                                 Crossings *record) {
     K.add(&Events::shadow_rays);
     float delta;
     const float surface = sphere_distance(S, K, r, light, b_radius(S, light), delta);
@@ -455,9 +465,23 @@ __device__ SG_HELPER float light_visibility(Scene S, Counter<C, L> K, Ray r, uin
 #pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
         const RingHit h = ring_hit(S, K, r, i);
-        if (h.index != kMiss && h.t < surface) transmission *= ring_transmission(S, r, h);
+        if (h.index != kMiss && h.t < surface) {
+            transmission *= ring_transmission(S, r, h);
+            if (record) {
+                if (record->n < (uint32_t)kMaxRecordedCrossings) {
+                    record->body[record->n] = i;
+                    record->point[record->n] = h.p;
+                }
+                record->n += 1u;
+            }
+        }
     }
     return transmission;
+}
+
+template <bool C, bool L>
+__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
+    return visibility_core(S, K, r, light, nullptr);
 }
 
 // one_minus_exp (rings.wgsl:143-145).

@@ -82,10 +82,10 @@ __device__ __forceinline__ float4 finish_path(const Path &p) {
 
 // One iteration of trace()'s loop (pathtrace.wgsl:1380-1607), airless.
 // Returns true when the path has ended. G is the hook set: NoGrad for the
-// forward integrator (every hook compiles out), Recorder for the adjoint's
-// first replay (records the ring-cap vertex and later Russian roulette),
-// Prb for its second (scatters derivatives). Hooks never change the path's
-// own arithmetic or random draws, so all three take the same decisions.
+// forward integrator (every hook compiles out), Prb for the adjoint, whose
+// first replay records the ring-cap vertex and later Russian roulette and
+// whose second scatters derivatives. Hooks never change the path's own
+// arithmetic or random draws, so every replay takes the same decisions.
 template <bool C, bool L, class G>
 __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G &grad) {
     const sg_settings *s = S.s;
@@ -96,7 +96,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
     // Static bound: each of at most max_vertices vertices is preceded by at
     // most n_bodies + 1 null crossings, so valid inputs never reach it.
     if (++p.iterations > max_vertices * (n_bodies + 2u) + 1u) return true;
-    if constexpr (G::grads) grad.iteration = p.iterations;
+    if constexpr (G::adjoint) grad.iteration = p.iterations;
     K.add(&Events::vertices);
     Ray &ray = p.ray;
     uint32_t &rng = p.rng;
@@ -144,10 +144,13 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             }
             shine_body = kMiss;
             [[maybe_unused]] RingVertexGrad vg{kNoParam, 0.0f, 0.0f};
-            if constexpr (G::grads) vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
-            if constexpr (G::records) {
-                grad.lit_sum = f3(0.0f, 0.0f, 0.0f);
-                grad.lit_vis_sum = f3(0.0f, 0.0f, 0.0f);
+            if constexpr (G::adjoint) {
+                if (grad.pass2) {
+                    vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
+                } else {
+                    grad.lit_sum = f3(0.0f, 0.0f, 0.0f);
+                    grad.lit_vis_sum = f3(0.0f, 0.0f, 0.0f);
+                }
             }
             float unshadowed = 0.0f, direct = 0.0f;
             #pragma unroll 1
@@ -160,8 +163,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 const float mu_in = dot(light.d, n);
                 float visibility;
                 [[maybe_unused]] Visibility vis;
-                if constexpr (G::grads) {
-                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i);
+                if constexpr (G::adjoint) {
+                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i, grad.pass2);
                     visibility = vis.v;
                 } else {
                     visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
@@ -170,12 +173,14 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 const float3 lit = throughput * ring_bsdf(optics, mu_out, mu_in) * xyz(material) *
                                    (fabsf(mu_in) / light.pdf);
                 radiance = radiance + lit * (visibility * weight * ring_mis);
-                if constexpr (G::grads)
-                    ring_light_grad(S, grad, ri, ring.p, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis,
-                                    last_vertex, vg);
-                if constexpr (G::records) {
-                    grad.lit_sum = grad.lit_sum + lit;
-                    grad.lit_vis_sum = grad.lit_vis_sum + lit * visibility;
+                if constexpr (G::adjoint) {
+                    if (grad.pass2) {
+                        ring_light_grad(S, grad, ri, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis,
+                                        last_vertex, vg);
+                    } else {
+                        grad.lit_sum = grad.lit_sum + lit;
+                        grad.lit_vis_sum = grad.lit_vis_sum + lit * visibility;
+                    }
                 }
                 const float l = luminance(lit);
                 unshadowed += l;
@@ -183,7 +188,9 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             }
             if (rnd(K, rng) < transmission) {
                 // Null event: no depth consumed, MIS stays with the last vertex.
-                if constexpr (G::grads) ring_null_grad(S, grad, ri, ring.p, ray.d);
+                if constexpr (G::adjoint) {
+                    if (grad.pass2) ring_null_grad(S, grad, ri, ring.p, ray.d);
+                }
                 ray = ring_origin(S, ri, ring.p, ray.d);
                 null_crossings += 1u;
                 return null_crossings > n_bodies;
@@ -192,8 +199,10 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             if (ring_cap > 1.0e29f) {
                 ring_cap = fmaxf(direct, kRingIndirectCap * unshadowed);
                 ring_base = radiance;
-                if constexpr (G::records)
-                    record_capture(grad, p.iterations, ring_cap, direct >= kRingIndirectCap * unshadowed, radiance);
+                if constexpr (G::adjoint) {
+                    if (!grad.pass2)
+                        record_capture(grad, p.iterations, ring_cap, direct >= kRingIndirectCap * unshadowed, radiance);
+                }
             }
             const float z = 1.0f - 2.0f * rnd(K, rng);
             float sp, cp;
@@ -201,7 +210,9 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             const float radial = sqrtf(fmaxf(0.0f, 1.0f - z * z));
             const float3 direction = basis_direction(n, radial * cp, radial * sp, z);
             throughput = throughput * ring_bsdf(optics, mu_out, z) * (fabsf(z) / bsdf_pdf);
-            if constexpr (G::grads) ring_scatter_grad(S, grad, ri, ring.p, optics, mu_out, z, vg, transmission, ray.d);
+            if constexpr (G::adjoint) {
+                if (grad.pass2) ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
+            }
             previous_pdf = bsdf_pdf;
             ray = ring_origin(S, ri, ring.p, direction);
             previous_vertex = ray;
@@ -210,7 +221,9 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             if (depth >= 3u) {
                 const float survival = clampf(max3(throughput), 0.05f, 0.95f);
                 const bool survived = !(rnd(K, rng) >= survival);
-                if constexpr (G::records) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+                if constexpr (G::adjoint) {
+                    if (!grad.pass2) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+                }
                 if (!survived) return true;
                 throughput = throughput / survival;
             }
@@ -234,8 +247,10 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 weight = power_weight(previous_pdf, light_pdf);
             }
             radiance = radiance + throughput * xyz(bf(S, bi, kMaterial)) * weight;
-            if constexpr (G::grads)
-                emitter_grad(S, grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
+            if constexpr (G::adjoint) {
+                if (grad.pass2)
+                    emitter_grad(grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
+            }
             return true;
         }
         K.add(&Events::surface_events);
@@ -264,13 +279,15 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         // loop; the forward evaluates it after, as the WGSL does.
         [[maybe_unused]] float3 albedo_g = f3(0.0f, 0.0f, 0.0f);
         [[maybe_unused]] GradEntry albedo_e = no_entry();
-        if constexpr (G::grads) {
-            if constexpr (L) {
-                albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
-            } else {
-                albedo_g = surface_albedo(S, bi, normal);
+        if constexpr (G::adjoint) {
+            if (grad.pass2) {
+                if constexpr (L) {
+                    albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+                } else {
+                    albedo_g = surface_albedo(S, bi, normal);
+                }
+                albedo_e = albedo_entry<L>(S, grad.inv, ray, hit.t, bi, albedo_g);
             }
-            albedo_e = albedo_entry<L>(S, ray, hit.t, bi, albedo_g);
         }
         float3 direct_light = f3(0.0f, 0.0f, 0.0f);
         #pragma unroll 1
@@ -285,8 +302,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             outgoing.d = sample.d;
             float visibility;
             [[maybe_unused]] Visibility vis;
-            if constexpr (G::grads) {
-                vis = light_visibility_grad(S, K, outgoing, i);
+            if constexpr (G::adjoint) {
+                vis = light_visibility_grad(S, K, outgoing, i, grad.pass2);
                 visibility = vis.v;
             } else {
                 visibility = light_visibility(S, K, outgoing, i);
@@ -295,8 +312,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 const float bsdf_pdf = cosine / kPi;
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
                 direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
-                if constexpr (G::grads)
-                    surface_light_grad(S, grad, albedo_e, i,
+                if constexpr (G::adjoint)
+                    if (grad.pass2) surface_light_grad(grad, albedo_e, i,
                                        throughput * albedo_g * xyz(light_material) *
                                            (bsdf_pdf * weight * visibility / sample.pdf),
                                        vis);
@@ -311,7 +328,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         radiance = radiance + throughput * albedo * direct_light;
         if (!local && has_ring(S, bi)) {
             Shine shine;
-            if constexpr (G::grads)
+            if constexpr (G::adjoint)
                 shine = ringshine_grad(S, K, bi, outgoing.o, normal, last_vertex, rng, grad, throughput * albedo,
                                        albedo_e);
             else
@@ -331,14 +348,18 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         outgoing.d = basis_direction(normal, su * cp, su * sp, cosine);
         previous_pdf = cosine / kPi;
         throughput = throughput * albedo;
-        if constexpr (G::grads) {
-            factor(grad, albedo_e);
-            grad.prev_param = kNoParam;
+        if constexpr (G::adjoint) {
+            if (grad.pass2) {
+                factor(grad, albedo_e);
+                grad.prev_param = kNoParam;
+            }
         }
         if (depth >= 2u) {
             const float survival = clampf(max3(throughput), 0.05f, 0.95f);
             const bool survived = !(rnd(K, rng) >= survival);
-            if constexpr (G::records) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+            if constexpr (G::adjoint) {
+                if (!grad.pass2) record_roulette(grad, p.iterations, throughput, survival, survived, radiance);
+            }
             if (!survived) return true;
             throughput = throughput / survival;
         }
@@ -459,21 +480,17 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // each pass so that a warp replays one pass at a time (lanes left to drift
 // between the two passes would run two copies of the integrator apart).
 template <bool L>
-__device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L> K, Recorder &R, Prb &G, float3 w,
-                                               uint32_t pixel, uint32_t x, uint32_t y, uint32_t smp,
-                                               unsigned lanes) {
-    Path path;
-    start_path(path, S.s, K, pixel, x, y, smp);
-    R.capture_iter = 0;
-    R.n_rr = 0;
-    while (!step(S, K, path, R)) {
+__device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L> K, Prb &G, float3 w, uint32_t pixel,
+                                               uint32_t x, uint32_t y, uint32_t smp, unsigned lanes) {
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        Path path;
+        start_path(path, S.s, K, pixel, x, y, smp);
+        while (!step(S, K, path, G)) {
+        }
+        if (pass == 0) pass2_setup(G, path.radiance, w);
+        __syncwarp(lanes);
     }
-    __syncwarp(lanes);
-    prb_setup(G, R, path.radiance, w);
-    start_path(path, S.s, K, pixel, x, y, smp);
-    while (!step(S, K, path, G)) {
-    }
-    __syncwarp(lanes);
 }
 
 // Resident CTAs per SM the adjoint is compiled for.
@@ -485,18 +502,30 @@ template <bool L>
 __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     adjoint_kernel(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A) {
     extern __shared__ float4 smem[];
-    float *window = reinterpret_cast<float *>(smem) + trace_smem_floats(P);
+    // Dynamic shared memory: bodies and staged tables (stage_scene), the
+    // inverse colours (2 float4 per body), then the gradient windows.
+    const uint32_t n_bodies = P.s.counts[0];
+    float4 *inv = smem + trace_smem_floats(P) / 4u;
+    float *window = reinterpret_cast<float *>(inv + 2u * n_bodies);
     const uint32_t window_n = A.tau_window + A.color_window;
     for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) window[k] = 0.0f;
+    for (uint32_t k = threadIdx.x; k < n_bodies; k += blockDim.x) {
+        const float4 m = P.bodies[k * kBodyVec4 + kMaterial], r = P.bodies[k * kBodyVec4 + kRingColor];
+        inv[2u * k] = make_float4(inv_or_zero(m.x), inv_or_zero(m.y), inv_or_zero(m.z), 0.0f);
+        inv[2u * k + 1u] = make_float4(inv_or_zero(r.x), inv_or_zero(r.y), inv_or_zero(r.z), 0.0f);
+    }
     const Scene S = stage_scene(P, smem);  // synchronises the block
     const Counter<false, L> K{nullptr};
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
-    Recorder R;
-    R.dropped = 0;
+    float own[6u * kColorSlots];
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
+    const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
     Prb G;
-    G.sink = GradSink{window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.inv = inv;
     G.dropped = 0;
     const bool inside = x < P.width && y < P.height;
     const uint32_t pixel = inside ? y * P.width + x : 0u;
@@ -510,14 +539,28 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     if (busy) {
         const uint32_t z = P.s.counts[2];
 #pragma unroll 1
-        for (uint32_t smp = 0; smp < z; ++smp) adjoint_sample(S, K, R, G, w, pixel, x, y, smp, lanes);
+        for (uint32_t smp = 0; smp < z; ++smp) {
+            pass1_setup(G);
+            adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes);
+        }
+    }
+    // Per-thread colour sums: reduce over the warp, then into the window.
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) {
+        float v = own[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0u && v != 0.0f) {
+            if (k < A.color_window) atomicAdd(window + A.tau_window + k, v);
+            else atomicAdd(A.grad + kGradColor + k, v);
+        }
     }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) {
         const float v = window[k];
         if (v != 0.0f) atomicAdd(A.grad + (k < A.tau_window ? k : kGradColor + (k - A.tau_window)), v);
     }
-    unsigned long long dropped = (unsigned long long)G.dropped + R.dropped;
+    unsigned long long dropped = G.dropped;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dropped += __shfl_down_sync(0xffffffffu, dropped, o);
     if (lane == 0u && dropped != 0ull && A.overflow) atomicAdd(A.overflow, dropped);
@@ -748,7 +791,8 @@ cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t s
 }
 
 size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a) {
-    return trace_smem_bytes(p) + (size_t)(a.tau_window + a.color_window) * sizeof(float);
+    return trace_smem_bytes(p) + (size_t)p.s.counts[0] * 2u * sizeof(float4) +
+           (size_t)(a.tau_window + a.color_window) * sizeof(float);
 }
 
 cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStream_t stream) {
