@@ -17,7 +17,7 @@ INCLUDE = PACKAGE_DIR.parent / "include"
 LIBRARY = PACKAGE_DIR / "libstargaze_b200.so"
 
 SOURCES = ["sg_kernels.cu", "sg_host.cpp"]
-HEADERS = ["sg_device.cuh", "sg_internal.h", "sg_landscape.cuh"]
+HEADERS = ["sg_adjoint.cuh", "sg_device.cuh", "sg_internal.h", "sg_landscape.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
