@@ -302,6 +302,30 @@ SG_API int sg_terrain_probe(sg_context *ctx, const sg_frame *frame,
                             const float *rays, uint32_t n, float *out,
                             int on_device, void *stream);
 
+/* closest_hit without device allocation. No counterpart in the reference.
+ * For callers that cannot let the library allocate device memory at query
+ * time: a host application that gives the whole device to its own
+ * allocator or memory pool, where a library cudaMalloc fails or splits the
+ * pool, and latency-bound callers, for which cudaMalloc synchronises the
+ * device. The results equal sg_closest_hit's. Unlike it, this call needs no
+ * context and stages the frame's bodies, the rays and the hits in one
+ * fixed device array of SG_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until the process exits.
+ *   - rays and hits live in host memory; n <= SG_NOALLOC_MAX_RAYS, larger
+ *     queries fail with SG_ERR_CAPACITY (split them);
+ *   - frames with a local landscape (ground_north.w != 0) need a context
+ *     and fail with SG_ERR_INVALID: use sg_closest_hit;
+ *   - the first call on a device looks up the array's device address; make
+ *     it before any stream capture;
+ *   - every call on a device shares the array, so calls whose work
+ *     overlaps on the GPU (other host threads, other streams) race;
+ *   - errors are reported by sg_last_error(NULL).
+ * Synchronises `stream` before returning. */
+#define SG_NOALLOC_MAX_RAYS 65536u
+#define SG_NOALLOC_SCRATCH_BYTES (4u << 20)
+SG_API int sg_closest_hit_noalloc(int device, const sg_frame *frame, const sg_ray *rays,
+                                  uint32_t n, sg_hit *hits, void *stream);
+
 /* Energy of the ring slab BSDF (ring_tests.rs:352-413 probe): unscattered
  * transmission plus the cosine-weighted integral of ring_bsdf over both
  * hemispheres at outgoing cosine `mu`, midpoint rule with `steps` bins. */

@@ -117,6 +117,8 @@ class Hit(C.Structure):
     _fields_ = [("distance", C.c_float), ("index", C.c_uint32), ("normal", F3)]
 
 
+NOALLOC_MAX_RAYS = 65536
+NOALLOC_SCRATCH_BYTES = 4 << 20
 TAPE_RANGES = 16
 
 

@@ -980,6 +980,12 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
     return SG_OK;
 }
 
+}  // extern "C"
+
+void sg::set_library_error(const char *message) { g_last_error = message ? message : ""; }
+
+extern "C" {
+
 const char *sg_last_error(const sg_context *ctx) {
     if (ctx) return ctx->last_error.c_str();
     return g_last_error.c_str();

@@ -49,6 +49,10 @@ constexpr int kEventCount = 9;
 // Shared-memory bytes a launch with these parameters needs.
 size_t trace_smem_bytes(const TraceParams &p);
 
+// Sets the message sg_last_error(NULL) returns (entry points without a
+// context report through it).
+void set_library_error(const char *message);
+
 cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t stream);
 cudaError_t launch_closest_hit(const TraceParams &p, const sg_ray *rays, sg_hit *hits, uint32_t n,
                                cudaStream_t stream);
