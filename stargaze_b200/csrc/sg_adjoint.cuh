@@ -21,6 +21,12 @@
 // factor once when it is created and each contribution's own factors
 // (albedo of the shading point, emitted radiance of the light, slab BSDF at
 // the ring point, ring transmissions along the shadow ray) when it is made.
+// Most paths never scatter in a ring, and for them pass 1 is enough: it
+// scatters each contribution's own factors at once and defers each
+// throughput factor with the running sum A at its creation, scattering
+// d log(factor) * (A_final - A) when the path ends. Only a path that reaches
+// a ring scatter (or overflows the deferral list) runs pass 2, which then
+// skips the contributions pass 1 already scattered.
 //
 // The ring-indirect cap (pathtrace.wgsl:1609-1615) clamps the radiance I
 // gathered after a path's first ring scatter to luminance `cap`:
@@ -55,6 +61,7 @@ constexpr int kMaxRoulette = 6;               // recorded events after a cap ver
 constexpr int kMaxLocal = 8;                  // factors of one contribution
 constexpr int kMaxCrossings = kMaxRecordedCrossings;  // of one shadow ray
 constexpr uint32_t kColorSlots = 4;           // bodies with per-thread colour sums
+constexpr int kMaxDeferred = 16;              // throughput factors pass 1 can defer
 
 struct GradEntry {
     uint32_t param;  // kNoParam: none
@@ -102,8 +109,9 @@ struct Roulette {
 
 // The adjoint's state. Both passes run the same integrator code (one
 // instantiation, so a warp's instruction footprint is that of one replay);
-// `pass2` selects the hooks: pass 1 records the summary pass 2 needs, pass 2
-// scatters derivatives.
+// `pass2` selects the hooks: pass 1 records the summary pass 2 needs and,
+// until the first ring scatter, scatters derivatives; pass 2 scatters the
+// rest.
 struct Prb {
     static constexpr bool adjoint = true;
     bool pass2;
@@ -129,9 +137,15 @@ struct Prb {
     float rr_coef[kMaxRoulette];
     GradEntry local[kMaxLocal];
     uint32_t n_local, dropped;
+    // Pass 1's deferred throughput factors and the running sum at each.
+    GradEntry fac[kMaxDeferred];
+    float3 fac_at[kMaxDeferred];
+    uint32_t n_fac;
+    bool deferral_full;
 
     __device__ __forceinline__ bool post() const { return capture_iter != 0u && iteration > capture_iter; }
-    __device__ __forceinline__ bool grads() const { return pass2; }
+    // Derivative hooks run in pass 2, and in pass 1 before a ring scatter.
+    __device__ __forceinline__ bool grads() const { return pass2 || capture_iter == 0u; }
     __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
     __device__ __forceinline__ void local_factor(GradEntry e) {
         if (e.param == kNoParam) return;
@@ -180,12 +194,15 @@ __device__ __forceinline__ void scatter_entry(const GradSink &sink, const GradEn
 
 // A radiance contribution `value` and its pending local factors (consumed).
 // `cap_term`: the cap vertex's light sample as a term of the cap.
+// Pass 2 skips the local factors of contributions before the cap vertex's
+// scatter: pass 1 scattered those.
 __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
     const bool post = G.post();
     const float3 w = mul3(cap_term ? G.w_cap : (post ? G.w_post : G.w_pre), value);
     const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : f3(0.0f, 0.0f, 0.0f);
+    const uint32_t n = (G.pass2 && !post && !cap_term) ? 0u : G.n_local;
 #pragma unroll 1
-    for (uint32_t k = 0; k < G.n_local; ++k) scatter_entry(G.sink, G.local[k], w, wp);
+    for (uint32_t k = 0; k < n; ++k) scatter_entry(G.sink, G.local[k], w, wp);
     G.n_local = 0;
     G.a = G.a + w;
     G.b = G.b + wp;
@@ -196,6 +213,17 @@ __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
 // the later Russian-roulette survivals (score and attached 1 / s).
 __device__ __noinline__ void factor(Prb &G, GradEntry e) {
     if (e.param == kNoParam) return;
+    if (!G.pass2) {
+        // Pass 1 (before any ring scatter): defer until the path's end.
+        if (G.n_fac < (uint32_t)kMaxDeferred) {
+            G.fac[G.n_fac] = e;
+            G.fac_at[G.n_fac] = G.a;
+            G.n_fac += 1u;
+        } else {
+            G.deferral_full = true;
+        }
+        return;
+    }
     const bool pdf = (e.param & kPdfBit) != 0u, vec = (e.param & kVectorBit) != 0u;
     float3 add;
     if (pdf) add = f3(sum3(G.b_total - G.b) * e.dlog.x, 0.0f, 0.0f);
@@ -470,7 +498,7 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
     if (!sp.valid) return Shine{zero, rng};
     const float3 n = xyz(bf(S, index, kRingPlane));
     float scale = 0.0f;
-    const uint32_t tp = G.pass2 ? tau_param(S, index, sp.point, &scale) : kNoParam;
+    const uint32_t tp = G.grads() ? tau_param(S, index, sp.point, &scale) : kNoParam;
     const RingVertexGrad vg{tp, scale, 0.0f};
     float3 shine = zero;
     const uint32_t count = light_count(S.s);
@@ -482,10 +510,10 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
         const LightSample light = sample_light(S, K, Ray{sp.point, n, index}, i, rng);
         rng = light.rng;
         const float mu_in = dot(light.d, n);
-        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i, G.pass2);
+        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i, G.grads());
         const float3 term = ring_bsdf(sp.optics, sp.mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * vis.v / light.pdf);
         shine = shine + term;
-        if (G.pass2 && vis.v > 0.0f) {
+        if (G.grads() && vis.v > 0.0f) {
             G.local_factor(albedo_e);
             G.local_factor(ring_tau_entry(vg, sp.optics.tau, sp.mu_out, mu_in));
             G.local_factor(ring_albedo_entry(G, index));
@@ -519,13 +547,44 @@ __device__ __noinline__ void record_roulette(Prb &G, uint32_t iteration, float3 
     G.rr[G.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - G.base};
 }
 
-// Start of pass 1.
-__device__ __forceinline__ void pass1_setup(Prb &G) {
+// Start of pass 1 for a pixel weight w.
+__device__ __forceinline__ void pass1_setup(Prb &G, float3 w) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = false;
     G.capture_iter = 0;
     G.n_rr = 0;
     G.binding = false;
     G.iteration = 0;
+    G.w_pre = w;
+    G.w_post = w;
+    G.w_pdf = zero;
+    G.w_cap = zero;
+    G.score = 0.0f;
+    G.a = zero;
+    G.b = zero;
+    G.prev_param = kNoParam;
+    G.prev_dlog_pdf = 0.0f;
+    G.n_local = 0;
+    G.n_fac = 0;
+    G.deferral_full = false;
+}
+
+// End of a path that pass 1 finished alone: each deferred factor's share of
+// the weighted radiance gathered after it.
+__device__ __noinline__ void flush_deferred(Prb &G) {
+#pragma unroll 1
+    for (uint32_t k = 0; k < G.n_fac; ++k) {
+        const GradEntry e = G.fac[k];
+        const float3 rem = G.a - G.fac_at[k];
+        if (e.param & kVectorBit) {
+            const uint32_t base = e.param & ~kVectorBit;
+            G.sink.add(base + 0u, rem.x * e.dlog.x);
+            G.sink.add(base + 1u, rem.y * e.dlog.y);
+            G.sink.add(base + 2u, rem.z * e.dlog.z);
+        } else {
+            G.sink.add(e.param & kParamMask, sum3(rem) * e.dlog.x);
+        }
+    }
 }
 
 // Pass 2's weights from pass 1's summary, the path's total radiance and the

@@ -145,9 +145,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             shine_body = kMiss;
             [[maybe_unused]] RingVertexGrad vg{kNoParam, 0.0f, 0.0f};
             if constexpr (G::adjoint) {
-                if (grad.pass2) {
-                    vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
-                } else {
+                if (grad.grads()) vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
+                if (!grad.pass2) {
                     grad.lit_sum = f3(0.0f, 0.0f, 0.0f);
                     grad.lit_vis_sum = f3(0.0f, 0.0f, 0.0f);
                 }
@@ -164,7 +163,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 float visibility;
                 [[maybe_unused]] Visibility vis;
                 if constexpr (G::adjoint) {
-                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i, grad.pass2);
+                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i, grad.grads());
                     visibility = vis.v;
                 } else {
                     visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
@@ -174,10 +173,10 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                                    (fabsf(mu_in) / light.pdf);
                 radiance = radiance + lit * (visibility * weight * ring_mis);
                 if constexpr (G::adjoint) {
-                    if (grad.pass2) {
+                    if (grad.grads())
                         ring_light_grad(S, grad, ri, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis,
                                         last_vertex, vg);
-                    } else {
+                    if (!grad.pass2) {
                         grad.lit_sum = grad.lit_sum + lit;
                         grad.lit_vis_sum = grad.lit_vis_sum + lit * visibility;
                     }
@@ -189,7 +188,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             if (rnd(K, rng) < transmission) {
                 // Null event: no depth consumed, MIS stays with the last vertex.
                 if constexpr (G::adjoint) {
-                    if (grad.pass2) ring_null_grad(S, grad, ri, ring.p, ray.d);
+                    if (grad.grads()) ring_null_grad(S, grad, ri, ring.p, ray.d);
                 }
                 ray = ring_origin(S, ri, ring.p, ray.d);
                 null_crossings += 1u;
@@ -211,7 +210,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             const float3 direction = basis_direction(n, radial * cp, radial * sp, z);
             throughput = throughput * ring_bsdf(optics, mu_out, z) * (fabsf(z) / bsdf_pdf);
             if constexpr (G::adjoint) {
-                if (grad.pass2) ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
+                if (grad.grads()) ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
             }
             previous_pdf = bsdf_pdf;
             ray = ring_origin(S, ri, ring.p, direction);
@@ -248,7 +247,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             }
             radiance = radiance + throughput * xyz(bf(S, bi, kMaterial)) * weight;
             if constexpr (G::adjoint) {
-                if (grad.pass2)
+                if (grad.grads())
                     emitter_grad(grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
             }
             return true;
@@ -280,7 +279,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         [[maybe_unused]] float3 albedo_g = f3(0.0f, 0.0f, 0.0f);
         [[maybe_unused]] GradEntry albedo_e = no_entry();
         if constexpr (G::adjoint) {
-            if (grad.pass2) {
+            if (grad.grads()) {
                 if constexpr (L) {
                     albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
                 } else {
@@ -303,7 +302,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             float visibility;
             [[maybe_unused]] Visibility vis;
             if constexpr (G::adjoint) {
-                vis = light_visibility_grad(S, K, outgoing, i, grad.pass2);
+                vis = light_visibility_grad(S, K, outgoing, i, grad.grads());
                 visibility = vis.v;
             } else {
                 visibility = light_visibility(S, K, outgoing, i);
@@ -313,7 +312,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
                 direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
                 if constexpr (G::adjoint)
-                    if (grad.pass2) surface_light_grad(grad, albedo_e, i,
+                    if (grad.grads()) surface_light_grad(grad, albedo_e, i,
                                        throughput * albedo_g * xyz(light_material) *
                                            (bsdf_pdf * weight * visibility / sample.pdf),
                                        vis);
@@ -349,7 +348,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         previous_pdf = cosine / kPi;
         throughput = throughput * albedo;
         if constexpr (G::adjoint) {
-            if (grad.pass2) {
+            if (grad.grads()) {
                 factor(grad, albedo_e);
                 grad.prev_param = kNoParam;
             }
@@ -476,19 +475,28 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // One sample's derivative: pass 1 replays the path without derivatives and
 // records what pass 2 needs to weigh each factor by the radiance gathered
 // after it (sg_adjoint.cuh); pass 2 replays it again and scatters.
-// `lanes`: the warp's lanes that run the same samples; they meet after
-// each pass so that a warp replays one pass at a time (lanes left to drift
-// between the two passes would run two copies of the integrator apart).
+// A path that never reaches a ring scatter ends after pass 1 (its
+// deferred factors flushed); the others replay once more. `lanes`: the
+// warp's lanes that run the same samples; they meet after each pass so that
+// a warp replays one pass at a time (lanes left to drift between the two
+// passes would run two copies of the integrator apart).
 template <bool L>
 __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L> K, Prb &G, float3 w, uint32_t pixel,
                                                uint32_t x, uint32_t y, uint32_t smp, unsigned lanes) {
+    bool again = true;
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
-        Path path;
-        start_path(path, S.s, K, pixel, x, y, smp);
-        while (!step(S, K, path, G)) {
+        if (again) {
+            Path path;
+            start_path(path, S.s, K, pixel, x, y, smp);
+            while (!step(S, K, path, G)) {
+            }
+            if (pass == 0) {
+                again = G.capture_iter != 0u || G.deferral_full;
+                if (again) pass2_setup(G, path.radiance, w);
+                else flush_deferred(G);
+            }
         }
-        if (pass == 0) pass2_setup(G, path.radiance, w);
         __syncwarp(lanes);
     }
 }
@@ -540,7 +548,7 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
         const uint32_t z = P.s.counts[2];
 #pragma unroll 1
         for (uint32_t smp = 0; smp < z; ++smp) {
-            pass1_setup(G);
+            pass1_setup(G, w);
             adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes);
         }
     }
