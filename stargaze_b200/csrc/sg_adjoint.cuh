@@ -21,12 +21,14 @@
 // factor once when it is created and each contribution's own factors
 // (albedo of the shading point, emitted radiance of the light, slab BSDF at
 // the ring point, ring transmissions along the shadow ray) when it is made.
-// Most paths never scatter in a ring, and for them pass 1 is enough: it
-// scatters each contribution's own factors at once and defers each
-// throughput factor with the running sum A at its creation, scattering
-// d log(factor) * (A_final - A) when the path ends. Only a path that reaches
-// a ring scatter (or overflows the deferral list) runs pass 2, which then
-// skips the contributions pass 1 already scattered.
+// Most paths need only pass 1: it weighs every contribution by the pixel
+// weight w — right unless the ring-indirect cap binds — scatters each
+// contribution's own factors at once, and defers each throughput factor
+// with the running sum A at its creation, scattering d log(factor) *
+// (A_final - A) when the path ends. Only a path whose cap binds (or that
+// overflows the deferral list) runs pass 2, which adds to the contributions
+// after the cap vertex the difference between their weight and the w
+// pass 1 gave them.
 //
 // The ring-indirect cap (pathtrace.wgsl:1609-1615) clamps the radiance I
 // gathered after a path's first ring scatter to luminance `cap`:
@@ -109,9 +111,7 @@ struct Roulette {
 
 // The adjoint's state. Both passes run the same integrator code (one
 // instantiation, so a warp's instruction footprint is that of one replay);
-// `pass2` selects the hooks: pass 1 records the summary pass 2 needs and,
-// until the first ring scatter, scatters derivatives; pass 2 scatters the
-// rest.
+// pass 1 also records the summary pass 2 needs (`pass2` false).
 struct Prb {
     static constexpr bool adjoint = true;
     bool pass2;
@@ -144,8 +144,6 @@ struct Prb {
     bool deferral_full;
 
     __device__ __forceinline__ bool post() const { return capture_iter != 0u && iteration > capture_iter; }
-    // Derivative hooks run in pass 2, and in pass 1 before a ring scatter.
-    __device__ __forceinline__ bool grads() const { return pass2 || capture_iter == 0u; }
     __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
     __device__ __forceinline__ void local_factor(GradEntry e) {
         if (e.param == kNoParam) return;
@@ -194,17 +192,23 @@ __device__ __forceinline__ void scatter_entry(const GradSink &sink, const GradEn
 
 // A radiance contribution `value` and its pending local factors (consumed).
 // `cap_term`: the cap vertex's light sample as a term of the cap.
-// Pass 2 skips the local factors of contributions before the cap vertex's
-// scatter: pass 1 scattered those.
+// Pass 1 scattered every contribution's local factors with weight w, so
+// pass 2 scatters only what differs: nothing before the cap vertex's
+// scatter, w_post - w after it, and the cap terms and attached entries in
+// full. The running sums take each contribution's full weight.
 __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
     const bool post = G.post();
-    const float3 w = mul3(cap_term ? G.w_cap : (post ? G.w_post : G.w_pre), value);
-    const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : f3(0.0f, 0.0f, 0.0f);
-    const uint32_t n = (G.pass2 && !post && !cap_term) ? 0u : G.n_local;
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    const float3 full = cap_term ? G.w_cap : (post ? G.w_post : G.w_pre);
+    const float3 local = !G.pass2 ? full : (cap_term ? G.w_cap : (post ? G.w_post - G.w_pre : zero));
+    const float3 w = mul3(local, value);
+    const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : zero;
+    if (w.x != 0.0f || w.y != 0.0f || w.z != 0.0f || wp.x != 0.0f || wp.y != 0.0f || wp.z != 0.0f) {
 #pragma unroll 1
-    for (uint32_t k = 0; k < n; ++k) scatter_entry(G.sink, G.local[k], w, wp);
+        for (uint32_t k = 0; k < G.n_local; ++k) scatter_entry(G.sink, G.local[k], w, wp);
+    }
     G.n_local = 0;
-    G.a = G.a + w;
+    G.a = G.a + mul3(full, value);
     G.b = G.b + wp;
 }
 
@@ -214,7 +218,7 @@ __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
 __device__ __noinline__ void factor(Prb &G, GradEntry e) {
     if (e.param == kNoParam) return;
     if (!G.pass2) {
-        // Pass 1 (before any ring scatter): defer until the path's end.
+        // Pass 1: defer until the path's end.
         if (G.n_fac < (uint32_t)kMaxDeferred) {
             G.fac[G.n_fac] = e;
             G.fac_at[G.n_fac] = G.a;
@@ -498,7 +502,7 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
     if (!sp.valid) return Shine{zero, rng};
     const float3 n = xyz(bf(S, index, kRingPlane));
     float scale = 0.0f;
-    const uint32_t tp = G.grads() ? tau_param(S, index, sp.point, &scale) : kNoParam;
+    const uint32_t tp = tau_param(S, index, sp.point, &scale);
     const RingVertexGrad vg{tp, scale, 0.0f};
     float3 shine = zero;
     const uint32_t count = light_count(S.s);
@@ -510,10 +514,10 @@ __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t 
         const LightSample light = sample_light(S, K, Ray{sp.point, n, index}, i, rng);
         rng = light.rng;
         const float mu_in = dot(light.d, n);
-        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i, G.grads());
+        const Visibility vis = light_visibility_grad(S, K, ring_origin(S, index, sp.point, light.d), i, true);
         const float3 term = ring_bsdf(sp.optics, sp.mu_out, mu_in) * xyz(material) * (fabsf(mu_in) * vis.v / light.pdf);
         shine = shine + term;
-        if (G.grads() && vis.v > 0.0f) {
+        if (vis.v > 0.0f) {
             G.local_factor(albedo_e);
             G.local_factor(ring_tau_entry(vg, sp.optics.tau, sp.mu_out, mu_in));
             G.local_factor(ring_albedo_entry(G, index));
@@ -567,6 +571,12 @@ __device__ __forceinline__ void pass1_setup(Prb &G, float3 w) {
     G.n_local = 0;
     G.n_fac = 0;
     G.deferral_full = false;
+}
+
+// Whether the ring-indirect cap binds on a path that pass 1 finished with
+// radiance `total` (before the clamp).
+__device__ __forceinline__ bool cap_binds(const Prb &G, float3 total) {
+    return G.capture_iter != 0u && luminance(total - G.base) > G.cap;
 }
 
 // End of a path that pass 1 finished alone: each deferred factor's share of

@@ -145,7 +145,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             shine_body = kMiss;
             [[maybe_unused]] RingVertexGrad vg{kNoParam, 0.0f, 0.0f};
             if constexpr (G::adjoint) {
-                if (grad.grads()) vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
+                vg = ring_vertex_grad(S, ri, ring.p, optics.tau, mu_out);
                 if (!grad.pass2) {
                     grad.lit_sum = f3(0.0f, 0.0f, 0.0f);
                     grad.lit_vis_sum = f3(0.0f, 0.0f, 0.0f);
@@ -163,7 +163,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 float visibility;
                 [[maybe_unused]] Visibility vis;
                 if constexpr (G::adjoint) {
-                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i, grad.grads());
+                    vis = light_visibility_grad(S, K, ring_origin(S, ri, ring.p, light.d), i, true);
                     visibility = vis.v;
                 } else {
                     visibility = light_visibility(S, K, ring_origin(S, ri, ring.p, light.d), i);
@@ -173,9 +173,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                                    (fabsf(mu_in) / light.pdf);
                 radiance = radiance + lit * (visibility * weight * ring_mis);
                 if constexpr (G::adjoint) {
-                    if (grad.grads())
-                        ring_light_grad(S, grad, ri, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis,
-                                        last_vertex, vg);
+                    ring_light_grad(S, grad, ri, optics, mu_out, mu_in, i, lit, vis, weight, ring_mis, last_vertex, vg);
                     if (!grad.pass2) {
                         grad.lit_sum = grad.lit_sum + lit;
                         grad.lit_vis_sum = grad.lit_vis_sum + lit * visibility;
@@ -188,7 +186,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             if (rnd(K, rng) < transmission) {
                 // Null event: no depth consumed, MIS stays with the last vertex.
                 if constexpr (G::adjoint) {
-                    if (grad.grads()) ring_null_grad(S, grad, ri, ring.p, ray.d);
+                    ring_null_grad(S, grad, ri, ring.p, ray.d);
                 }
                 ray = ring_origin(S, ri, ring.p, ray.d);
                 null_crossings += 1u;
@@ -210,7 +208,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             const float3 direction = basis_direction(n, radial * cp, radial * sp, z);
             throughput = throughput * ring_bsdf(optics, mu_out, z) * (fabsf(z) / bsdf_pdf);
             if constexpr (G::adjoint) {
-                if (grad.grads()) ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
+                ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
             }
             previous_pdf = bsdf_pdf;
             ray = ring_origin(S, ri, ring.p, direction);
@@ -247,8 +245,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             }
             radiance = radiance + throughput * xyz(bf(S, bi, kMaterial)) * weight;
             if constexpr (G::adjoint) {
-                if (grad.grads())
-                    emitter_grad(grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
+                emitter_grad(grad, bi, throughput * xyz(bf(S, bi, kMaterial)) * weight, weight, depth > 0u);
             }
             return true;
         }
@@ -279,14 +276,12 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         [[maybe_unused]] float3 albedo_g = f3(0.0f, 0.0f, 0.0f);
         [[maybe_unused]] GradEntry albedo_e = no_entry();
         if constexpr (G::adjoint) {
-            if (grad.grads()) {
-                if constexpr (L) {
-                    albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
-                } else {
-                    albedo_g = surface_albedo(S, bi, normal);
-                }
-                albedo_e = albedo_entry<L>(S, grad.inv, ray, hit.t, bi, albedo_g);
+            if constexpr (L) {
+                albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+            } else {
+                albedo_g = surface_albedo(S, bi, normal);
             }
+            albedo_e = albedo_entry<L>(S, grad.inv, ray, hit.t, bi, albedo_g);
         }
         float3 direct_light = f3(0.0f, 0.0f, 0.0f);
         #pragma unroll 1
@@ -302,7 +297,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             float visibility;
             [[maybe_unused]] Visibility vis;
             if constexpr (G::adjoint) {
-                vis = light_visibility_grad(S, K, outgoing, i, grad.grads());
+                vis = light_visibility_grad(S, K, outgoing, i, true);
                 visibility = vis.v;
             } else {
                 visibility = light_visibility(S, K, outgoing, i);
@@ -312,7 +307,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
                 direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
                 if constexpr (G::adjoint)
-                    if (grad.grads()) surface_light_grad(grad, albedo_e, i,
+                    surface_light_grad(grad, albedo_e, i,
                                        throughput * albedo_g * xyz(light_material) *
                                            (bsdf_pdf * weight * visibility / sample.pdf),
                                        vis);
@@ -348,10 +343,8 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
         previous_pdf = cosine / kPi;
         throughput = throughput * albedo;
         if constexpr (G::adjoint) {
-            if (grad.grads()) {
-                factor(grad, albedo_e);
-                grad.prev_param = kNoParam;
-            }
+            factor(grad, albedo_e);
+            grad.prev_param = kNoParam;
         }
         if (depth >= 2u) {
             const float survival = clampf(max3(throughput), 0.05f, 0.95f);
@@ -475,7 +468,7 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // One sample's derivative: pass 1 replays the path without derivatives and
 // records what pass 2 needs to weigh each factor by the radiance gathered
 // after it (sg_adjoint.cuh); pass 2 replays it again and scatters.
-// A path that never reaches a ring scatter ends after pass 1 (its
+// A path whose ring-indirect cap does not bind ends after pass 1 (its
 // deferred factors flushed); the others replay once more. `lanes`: the
 // warp's lanes that run the same samples; they meet after each pass so that
 // a warp replays one pass at a time (lanes left to drift between the two
@@ -492,7 +485,7 @@ __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L>
             while (!step(S, K, path, G)) {
             }
             if (pass == 0) {
-                again = G.capture_iter != 0u || G.deferral_full;
+                again = G.deferral_full || cap_binds(G, path.radiance);
                 if (again) pass2_setup(G, path.radiance, w);
                 else flush_deferred(G);
             }
