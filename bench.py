@@ -13,6 +13,13 @@ same metric through the public API with the frame handed over from host
 memory and the 33 MB accumulation read back to the host every step.
 `--impl reference` times the CPU restatement of the reference integrator
 (the oracle; the reference's own Rust/WGSL cannot run here) on the host.
+
+After the timed region (one GPU only) two further figures of the metric are
+measured: `convergence`, the relative RMSE of the 256-spp image against a
+4096-spp image of disjoint noise and the samples (and time) it takes to reach
+1 %; and `adjoint`, the path-replay adjoint's time against the forward's at
+equal spp on the ring scene (512x512, 64 spp) and on the terrain scene
+(1920x1080, 256 spp, 1024^2 albedo map).
 """
 from __future__ import annotations
 
@@ -68,6 +75,7 @@ def parse_args():
     p.add_argument("--spp", type=int, default=256)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the convergence and adjoint figures")
     return p.parse_args()
 
 
@@ -165,6 +173,79 @@ def cpu_baseline(wl, seconds: float, threads: int = 0) -> dict:
     return {"value": samples / elapsed / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{samples} samples ({wl.width}x{wl.height} frame, 8-sample dispatches, row bands) "
                       f"in {elapsed:.1f} s"}
+
+
+def relative_rmse(x: np.ndarray, reference: np.ndarray) -> float:
+    """sqrt(sum (x - ref)^2 / sum ref^2) over rgb (scripts/benchmark.py:219-232)."""
+    d = x[:, :3].astype(np.float64) - reference[:, :3].astype(np.float64)
+    return float(np.sqrt((d * d).sum() / (reference[:, :3].astype(np.float64) ** 2).sum()))
+
+
+def convergence(wl, image: np.ndarray, spp: int, msamples_per_s: float, device: int, stream) -> dict:
+    """Relative RMSE of a `spp`-sample image against a 4096-sample image of
+    the same workload with disjoint noise keys, and the samples per pixel
+    (and time at `msamples_per_s`) for 1 % relative RMSE, from the
+    1 / sqrt(spp) law."""
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    ref_spp = 4096
+    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH, noise_seed=0x40000000), device=device)
+    upload_workload(t, wl)
+    frame = wl.frame.copy()
+    frame.scene_time = -12345.0
+    for _ in range(ref_spp // BATCH):
+        t.encode(frame, stream)
+    reference = t.read_pixels(stream)
+    t.close()
+    err = relative_rmse(image, reference)
+    # The reference's own noise adds err_ref^2 = err^2 * spp / ref_spp.
+    own = err * np.sqrt(max(1.0 - spp / ref_spp, 1e-6))
+    spp_1pct = spp * (own / 0.01) ** 2
+    return {"relative_rmse": err, "spp": spp, "reference_spp": ref_spp,
+            "spp_to_1pct": spp_1pct,
+            "ms_to_1pct": spp_1pct * wl.width * wl.height / (msamples_per_s * 1e6) * 1e3,
+            "reference": "this integrator at 4096 spp, disjoint noise (parity with the oracle is tested at small sizes)"}
+
+
+def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
+    """Forward (spp samples from a fresh accumulation) and path-replay
+    adjoint (sg_backward for a seeded d loss / d image) times, CUDA events on
+    the launching stream, median over `reps`."""
+    import torch
+
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
+    upload_workload(t, wl)
+    dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
+    fwd, bwd = [], []
+    for r in range(reps + 1):
+        frame = wl.frame.copy()
+        frame.scene_time = float(-1 - r)
+        t.prepare_frame(frame)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        while t.samples() < wl.spp:
+            t.encode(frame, stream)
+        e[1].record(stream)
+        tape = t.tape()
+        e[2].record(stream)
+        g = t.backward(frame, tape, dl, stream)
+        e[3].record(stream)
+        stream.synchronize()
+        if r > 0:  # the first round loads the kernels
+            fwd.append(e[0].elapsed_time(e[1]))
+            bwd.append(e[2].elapsed_time(e[3]))
+    t.close()
+    f, b = statistics.median(fwd), statistics.median(bwd)
+    params = int(sum(v.size for v in wl.ring_tables.values())) + 6 * len(wl.frame.bodies)
+    if wl.landscape is not None and wl.landscape.albedo_map is not None:
+        params += int(wl.landscape.albedo_map.size)
+    return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp, "forward_ms": f,
+            "backward_ms": b, "ratio": b / f, "forward_plus_adjoint_over_forward": (f + b) / f,
+            "parameters": params, "dropped_entries": int(g.dropped)}
 
 
 def run_reference(args):
@@ -311,6 +392,19 @@ def run_ours(args):
         if world == 1 and not args.no_cpu_baseline:
             base = cpu_baseline(wl, args.cpu_seconds)
         clk = clocks.summary()
+        extras = {}
+        if world == 1 and not args.no_extras:
+            from stargaze_b200 import workloads as W
+
+            image = tracer.read_pixels(stream)
+            extras["convergence"] = convergence(wl, image, args.spp, value, local, stream)
+            ring = adjoint_ratio(W.rings_1080p(512, 512, 64), local, stream)
+            land_wl, land = W.terrain_1080p(1920, 1080, 256)
+            land.albedo_map = np.random.default_rng(1).uniform(0.05, 0.6, (1024, 1024)).astype(np.float32)
+            land.map_extent = 2000.0
+            terrain = adjoint_ratio(land_wl, local, stream, reps=2)
+            extras["adjoint"] = {"ratio": ring["ratio"], "ring_512": ring, "terrain_1080p": terrain,
+                                 "note": "ratio = adjoint time / forward time at equal spp (ring scene)"}
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -331,6 +425,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "cpu_baseline": base,
+            **extras,
         }
         print(json.dumps(result), flush=True)
     tracer.close()
