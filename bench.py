@@ -65,6 +65,40 @@ TRAFFIC_BYTES_PER_LAUNCH = None
 L2_FLUSH_BYTES = 256 << 20
 
 
+def profile_terrain_640x360():
+    """Terrain workload at 640x360, 64 spp: two frames (the first also runs
+    the terrain-cache kernel)."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl, _land = W.terrain_1080p(640, 360, 64)
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.encode(frame)
+    t.read_pixels()
+
+
+def profile_adjoint_ring_512():
+    """Ring workload at 512x512: render 64 spp and run the adjoint, twice."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl = W.rings_1080p(512, 512, 64)
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.prepare_frame(frame)
+        t.encode(frame)
+        t.backward(frame, t.tape(), dl)
+
+
+PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512}
+
+
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__)
     p.add_argument("--gpus", type=int, default=1)
@@ -76,6 +110,8 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the convergence and adjoint figures")
+    p.add_argument("--profile-case", choices=sorted(PROFILE_CASES),
+                   help="run one small case for an ncu capture (profiles/) and exit")
     return p.parse_args()
 
 
@@ -437,6 +473,10 @@ def run_ours(args):
 
 def main():
     args = parse_args()
+    if args.profile_case:
+        PROFILE_CASES[args.profile_case]()
+        print(f"profile case {args.profile_case}: done", flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
