@@ -211,6 +211,31 @@ def cpu_baseline(wl, seconds: float, threads: int = 0) -> dict:
                       f"in {elapsed:.1f} s"}
 
 
+# Replicas: rank r renders noise keys from RANK_KEY_STRIDE * r on, so ranks
+# never share a sample while each renders fewer than RANK_KEY_STRIDE.
+RANK_KEY_STRIDE = 1 << 26
+
+
+def rank_noise_seed(rank: int) -> int:
+    return (rank * RANK_KEY_STRIDE) & 0xFFFFFFFF
+
+
+def max_over_ranks(values, dist, device) -> list[float]:
+    """Element-wise maximum of per-rank timings (every rank gets it)."""
+    import torch
+
+    if dist is None:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_msamples_per_s(world: int, samples_per_step: int, steps: int, total_ms: float) -> float:
+    """Whole-job throughput of `world` replicas, timed by the slowest rank."""
+    return world * samples_per_step * steps / (total_ms * 1e-3) / 1e6
+
+
 def relative_rmse(x: np.ndarray, reference: np.ndarray) -> float:
     """sqrt(sum (x - ref)^2 / sum ref^2) over rgb (scripts/benchmark.py:219-232)."""
     d = x[:, :3].astype(np.float64) - reference[:, :3].astype(np.float64)
@@ -336,7 +361,7 @@ def run_ours(args):
     batches = (args.spp + BATCH - 1) // BATCH
     # Disjoint noise sequences per rank: each GPU renders its own full-frame
     # 256-spp estimate (weak scaling, no data-path collective).
-    opts = bench_options(wl, spp=BATCH, noise_seed=rank << 26)
+    opts = bench_options(wl, spp=BATCH, noise_seed=rank_noise_seed(rank))
     from stargaze_b200.workloads import upload_workload
 
     tracer = PathTracer((wl.width, wl.height), opts, device=local)
@@ -410,16 +435,11 @@ def run_ours(args):
             stream.synchronize()
             e2e_ms.append(a.elapsed_time(b))
 
-    total_ms = sum(step_ms)
-    e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = float(t[0]), float(t[1])
+    total_ms, e2e_total = max_over_ranks([sum(step_ms), sum(e2e_ms)], dist, "cuda")
 
     samples_per_step = wl.width * wl.height * args.spp
-    value = world * samples_per_step * args.steps / (total_ms * 1e-3) / 1e6
-    e2e_value = world * samples_per_step * args.steps / (e2e_total * 1e-3) / 1e6
+    value = job_msamples_per_s(world, samples_per_step, args.steps, total_ms)
+    e2e_value = job_msamples_per_s(world, samples_per_step, args.steps, e2e_total)
     mean_launch_s = statistics.mean(launch_ms) * 1e-3
     achieved = ops_per_launch / mean_launch_s
     result = None
