@@ -309,6 +309,44 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
             "parameters": params, "dropped_entries": int(g.dropped)}
 
 
+def fp64_sites(wl, device: int, stream, reps: int = 2) -> dict:
+    """The FP64 sites against the reference's f32 arithmetic: hit-distance
+    error of both at the host-sphere and ring-plane sites against double,
+    and the ring workload's time per step with each."""
+    import torch
+
+    from stargaze_b200 import PathTracer, precision
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    out = {"host_sphere": {}, "ring_plane": {}, "ms_per_step": {}}
+    for mode, fp64 in (("f32", False), ("fp64", True)):
+        out["host_sphere"][mode] = precision.host_sphere_precision(10**7, fp64, device)
+        out["ring_plane"][mode] = precision.ring_plane_precision(wl.frame, 10**6, fp64, wl.ring_tables, device)
+        t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
+        upload_workload(t, wl)
+        t.set_fp64_sites(fp64)
+        times = []
+        for r in range(reps + 1):
+            frame = wl.frame.copy()
+            frame.scene_time = float(-1 - r)
+            t.prepare_frame(frame)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            while t.samples() < wl.spp:
+                t.encode(frame, stream)
+            b.record(stream)
+            stream.synchronize()
+            if r > 0:
+                times.append(a.elapsed_time(b))
+        t.close()
+        out["ms_per_step"][mode] = statistics.median(times)
+    out["slowdown"] = out["ms_per_step"]["fp64"] / out["ms_per_step"]["f32"]
+    out["note"] = ("relative error of the device's hit distance (and ring radius) against the exact "
+                   "intersection of the same f32 rays; host sphere 6.4e6 m, camera 2 m up, 1e7 rays grazing "
+                   "to nadir; ring plane 1e6 camera rays per ringed body of the ring workload")
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -461,6 +499,7 @@ def run_ours(args):
             terrain = adjoint_ratio(land_wl, local, stream, reps=2)
             extras["adjoint"] = {"ratio": ring["ratio"], "ring_512": ring, "terrain_1080p": terrain,
                                  "note": "ratio = adjoint time / forward time at equal spp (ring scene)"}
+            extras["fp64_sites"] = fp64_sites(wl, local, stream)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -332,6 +332,15 @@ SG_API int sg_closest_hit_noalloc(int device, const sg_frame *frame, const sg_ra
 SG_API int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu,
                    uint32_t steps, float *energy);
 
+/* Extension (no reference counterpart): evaluate the three precision-
+ * critical sites in FP64 from the same f32 inputs — the ring-plane
+ * intersection (rings.wgsl:8-34), the host-sphere intersection of the local
+ * landscape (ground.wgsl:138-158) and the 5 mm bounce offset with its
+ * reprojection (ground.wgsl:649-662). Off by default, where the library
+ * follows the reference's f32 arithmetic bit for bit. Changing it resets the
+ * accumulation on the next encode. */
+SG_API int sg_set_fp64_sites(sg_context *ctx, int enable);
+
 /* ------------------------------------------------------------------ */
 /* Path-replay adjoint (extension: the reference renders forward only) */
 /* ------------------------------------------------------------------ */

@@ -339,8 +339,8 @@ struct Visibility {
     GradEntry cross[kMaxCrossings];
 };
 
-template <bool C, bool L>
-__device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L> K, Ray r, uint32_t light,
+template <bool C, bool L, bool F>
+__device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L, F> K, Ray r, uint32_t light,
                                                          bool entries) {
     Crossings rec;
     rec.n = 0;
@@ -491,8 +491,8 @@ __device__ __noinline__ GradEntry albedo_entry(Scene S, const float4 *inv, Ray r
 // ringshine with derivatives (pathtrace.wgsl:1248-1296): the same draws and
 // result as ringshine(), plus one contribution per light. `carried` is the
 // path throughput times the surface albedo.
-template <bool C, bool L>
-__device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
+template <bool C, bool L, bool F>
+__device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
                                              bool last_vertex, uint32_t rng, Prb &G, float3 carried,
                                              GradEntry albedo_e) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);

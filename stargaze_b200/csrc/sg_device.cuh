@@ -125,8 +125,9 @@ struct Events {
         ring_events, surface_events, rng_draws;
 };
 
-// Counting is compiled out of the production variant (C == false).
-template <bool C, bool L>
+// Counting is compiled out of the production variant (C == false); L turns
+// the local landscape on, F the FP64 sites (sg_set_fp64_sites).
+template <bool C, bool L, bool F>
 struct Counter {
     Events *ev;
     __device__ __forceinline__ void add(uint32_t Events::*f) const {
@@ -134,8 +135,8 @@ struct Counter {
     }
 };
 
-template <bool C, bool L>
-__device__ __forceinline__ float rnd(Counter<C, L> K, uint32_t &state) {
+template <bool C, bool L, bool F>
+__device__ __forceinline__ float rnd(Counter<C, L, F> K, uint32_t &state) {
     K.add(&Events::rng_draws);
     state = state * 747796405u + 2891336453u;
     const uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
@@ -175,8 +176,8 @@ __device__ __forceinline__ float3 relative_center(const Scene &S, const Ray &r, 
 // Distance part of sphere_hit_radius (pathtrace.wgsl:134-166). Returns the
 // hit distance (1e30 on a miss) and the signed root offset `delta` that the
 // normal needs.
-template <bool C, bool L>
-__device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t i,
+template <bool C, bool L, bool F>
+__device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C, L, F> K, const Ray &r, uint32_t i,
                                                  float radius, float &delta) {
     K.add(&Events::sphere_tests);
     const float3 oc = relative_center(S, r, i);
@@ -226,13 +227,13 @@ struct LandHit {
     float delta;  // root offset when the distant path returns the host sphere
     float3 n;
 };
-template <bool C, bool L>
-__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L> K, Ray ray, float limit, bool occlusion);
+template <bool C, bool L, bool F>
+__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion);
 
 // closest_hit (pathtrace.wgsl:173-185): every body except the landscape
 // host, then the landscape.
-template <bool C, bool L>
-__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C, L> K, const Ray &r) {
+template <bool C, bool L, bool F>
+__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C, L, F> K, const Ray &r) {
     Hit best{1.0e30f, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
     const float host = S.s->g.ground_north[3];
@@ -279,8 +280,8 @@ struct LightSample {
 };
 
 // sample_light (pathtrace.wgsl:214-234), one stratum: uniform cone sampling.
-template <bool C, bool L>
-__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C, L> K, Ray r, uint32_t i, uint32_t rng) {
+template <bool C, bool L, bool F>
+__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C, L, F> K, Ray r, uint32_t i, uint32_t rng) {
     K.add(&Events::light_samples);
     const float3 oc = relative_center(S, r, i);
     const float3 axis = normalize(oc);
@@ -318,14 +319,63 @@ __device__ __forceinline__ bool has_ring(const Scene &S, uint32_t i) {
     return !(rp.x <= bf(S, i, kRingPlane).w || rp.y <= 0.0f);
 }
 
+// ---------------------------------------------------------------------------
+// FP64 sites (extension, sg_set_fp64_sites): the ring-plane intersection, the
+// host-sphere intersection of the landscape and the 5 mm bounce offset
+// evaluated in double from the same f32 inputs. Off by default: the f32
+// forms are the reference's arithmetic.
+// ---------------------------------------------------------------------------
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 D(float3 v) { return d3{(double)v.x, (double)v.y, (double)v.z}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return d3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator*(d3 a, double s) { return d3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross(d3 a, d3 b) {
+    return d3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float3 F(d3 v) { return f3((float)v.x, (float)v.y, (float)v.z); }
+
+// ring_hit in double: the centre difference from the hi/lo parts, the
+// perpendicular, the plane distance and the annulus test.
+__device__ __noinline__ RingHit ring_hit_fp64(Scene S, Ray r, uint32_t i) {
+    const RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
+    const float4 plane = bf(S, i, kRingPlane);
+    const float4 params = bf(S, i, kRingParams);
+    const d3 n = D(xyz(plane)), d = D(r.d);
+    const double denom = dot(d, n);
+    if (fabs(denom) < 1.0e-7) return miss;
+    d3 oc;
+    if (r.anchor == i) {
+        oc = D(-r.o);
+    } else if (r.anchor == kMiss) {
+        oc = D(xyz(bf(S, i, kCenter))) + D(xyz(bf(S, i, kLow))) - D(r.o);
+    } else {
+        oc = (D(xyz(bf(S, i, kCenter))) - D(xyz(bf(S, r.anchor, kCenter)))) +
+             (D(xyz(bf(S, i, kLow))) - D(xyz(bf(S, r.anchor, kLow)))) - D(r.o);
+    }
+    const double a = dot(d, d);
+    const d3 perpendicular = cross(d, cross(d, oc)) * (1.0 / a);
+    const double along = -dot(perpendicular, n) / denom;
+    const double distance = dot(oc, d) / a + along;
+    if (distance <= 0.0) return miss;
+    const d3 point = perpendicular + d * along;
+    const double radius = sqrt(dot(point, point)) / (double)b_radius(S, i);
+    if (radius < (double)plane.w || radius > (double)params.x) return miss;
+    return RingHit{(float)distance, i, F(point)};
+}
+
 // ring_hit (rings.wgsl:8-34), strict.
-template <bool C, bool L>
-__device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t i) {
+template <bool C, bool L, bool F>
+__device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L, F> K, const Ray &r, uint32_t i) {
     const RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const float4 plane = bf(S, i, kRingPlane);
     const float4 params = bf(S, i, kRingParams);
     if (params.x <= plane.w || params.y <= 0.0f) return miss;
     K.add(&Events::ring_tests);
+    if constexpr (F) return ring_hit_fp64(S, r, i);
     const float3 n = xyz(plane);
     const float denom = dot_rn(r.d, n);
     if (fabsf(denom) < 1.0e-7f) return miss;
@@ -342,8 +392,8 @@ __device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L> K, con
 }
 
 // closest_ring (rings.wgsl:36-45).
-template <bool C, bool L>
-__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C, L> K, const Ray &r, float limit) {
+template <bool C, bool L, bool F>
+__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C, L, F> K, const Ray &r, float limit) {
     RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
 #pragma unroll 1
@@ -439,8 +489,8 @@ struct Crossings {
 // light_visibility (rings.wgsl:90-115): distance to the light, any-hit over
 // the other spheres (ties broken by index), then ring transmissions before
 // the light. With a Crossings record it also lists the ring crossings.
-template <bool C, bool L>
-__device__ __forceinline__ float visibility_core(const Scene &S, Counter<C, L> K, const Ray &r, uint32_t light,
+template <bool C, bool L, bool F>
+__device__ __forceinline__ float visibility_core(const Scene &S, Counter<C, L, F> K, const Ray &r, uint32_t light,
                                                  Crossings *record) {
     K.add(&Events::shadow_rays);
     float delta;
@@ -479,8 +529,8 @@ __device__ __forceinline__ float visibility_core(const Scene &S, Counter<C, L> K
     return transmission;
 }
 
-template <bool C, bool L>
-__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L> K, Ray r, uint32_t light) {
+template <bool C, bool L, bool F>
+__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L, F> K, Ray r, uint32_t light) {
     return visibility_core(S, K, r, light, nullptr);
 }
 
@@ -540,8 +590,8 @@ struct ShinePoint {
     bool valid;
 };
 
-template <bool C, bool L>
-__device__ __forceinline__ ShinePoint shine_point(const Scene &S, Counter<C, L> K, uint32_t index, float3 origin,
+template <bool C, bool L, bool F>
+__device__ __forceinline__ ShinePoint shine_point(const Scene &S, Counter<C, L, F> K, uint32_t index, float3 origin,
                                                   float3 normal, bool last_vertex, uint32_t rng) {
     ShinePoint out;
     out.valid = false;
@@ -575,8 +625,8 @@ __device__ __forceinline__ ShinePoint shine_point(const Scene &S, Counter<C, L> 
 }
 
 // ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
-template <bool C, bool L>
-__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L> K, uint32_t index, float3 origin, float3 normal,
+template <bool C, bool L, bool F>
+__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
                                         bool last_vertex, uint32_t rng) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     if (!has_ring(S, index)) return Shine{zero, rng};
@@ -615,8 +665,8 @@ struct DiscHit {
 
 // point_disc_hit (pathtrace.wgsl:1308-1333): depth-0 camera rays see an
 // unresolved body as a disc of at least a bright star's size.
-template <bool C, bool L>
-__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L> K, Ray r, Hit closest, uint32_t rng) {
+template <bool C, bool L, bool F>
+__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, Ray r, Hit closest, uint32_t rng) {
     const sg_settings *s = S.s;
     DiscHit out{closest, 1.0f, rng};
     float total = 0.0f;

@@ -78,6 +78,7 @@ struct sg_context {
     float *albedo_map = nullptr;
     uint32_t map_width = 0, map_height = 0;
     float map_extent = 0.0f;
+    bool fp64_sites = false;                // ring plane, host sphere, 5 mm offset in FP64
     // Adjoint buffers, allocated on first use.
     float *grad = nullptr;                  // kGradMap + texels floats
     size_t grad_floats = 0;
@@ -176,6 +177,7 @@ std::vector<uint8_t> history_key(const sg_context *ctx, const sg_frame *frame) {
     append(key, ctx->options.max_bounces);
     append(key, ctx->options.milky_way);
     append(key, ctx->table_version);
+    append(key, ctx->fp64_sites);
     return key;
 }
 
@@ -358,6 +360,7 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.map_width = ctx->map_width;
     p.map_height = ctx->map_height;
     p.map_extent = ctx->map_extent;
+    p.fp64_sites = ctx->fp64_sites ? 1u : 0u;
     return p;
 }
 
@@ -868,6 +871,12 @@ int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu, uint32_t 
     cudaError_t e = sg::launch_ring_energy(albedo, tau, mu, steps, d, nullptr);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "ring_energy launch");
     SG_CUDA(ctx, cudaMemcpy(energy, d, sizeof(float), cudaMemcpyDeviceToHost));
+    return SG_OK;
+}
+
+int sg_set_fp64_sites(sg_context *ctx, int enable) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    ctx->fp64_sites = enable != 0;
     return SG_OK;
 }
 

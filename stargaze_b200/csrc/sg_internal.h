@@ -34,6 +34,7 @@ struct TraceParams {
     const float *albedo_map;
     uint32_t map_width, map_height;
     float map_extent;
+    uint32_t fp64_sites;  // ring plane, host sphere and 5 mm offset in FP64
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,

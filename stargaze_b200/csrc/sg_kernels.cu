@@ -36,8 +36,8 @@ struct Path {
 };
 
 // camera_direction (pathtrace.wgsl:1619-1626).
-template <bool C, bool L>
-__device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter<C, L> K, uint32_t x, uint32_t y,
+template <bool C, bool L, bool F>
+__device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter<C, L, F> K, uint32_t x, uint32_t y,
                                                    uint32_t &rng) {
     const float jx = rnd(K, rng);
     const float jy = rnd(K, rng);
@@ -49,8 +49,8 @@ __device__ __forceinline__ float3 camera_direction(const sg_settings *s, Counter
 
 // Sample `smp` of a pixel: seeding (pathtrace.wgsl:1656), the jittered
 // camera ray, and trace()'s initial state.
-template <bool C, bool L>
-__device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counter<C, L> K, uint32_t pixel, uint32_t x,
+template <bool C, bool L, bool F>
+__device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counter<C, L, F> K, uint32_t pixel, uint32_t x,
                                            uint32_t y, uint32_t smp) {
     p.rng = hash_u32(pixel ^ hash_u32(s->sampling[0] + smp + 0x9e3779b9u));
     const float3 d = camera_direction(s, K, x, y, p.rng);
@@ -86,8 +86,8 @@ __device__ __forceinline__ float4 finish_path(const Path &p) {
 // first replay records the ring-cap vertex and later Russian roulette and
 // whose second scatters derivatives. Hooks never change the path's own
 // arithmetic or random draws, so every replay takes the same decisions.
-template <bool C, bool L, class G>
-__device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G &grad) {
+template <bool C, bool L, bool F, class G>
+__device__ __forceinline__ bool step(const Scene &S, Counter<C, L, F> K, Path &p, G &grad) {
     const sg_settings *s = S.s;
     const uint32_t max_vertices = s->counts[3];
     const uint32_t n_bodies = s->counts[0];
@@ -257,7 +257,7 @@ __device__ __forceinline__ bool step(const Scene &S, Counter<C, L> K, Path &p, G
             // offset origin (ground.wgsl:633-662).
             if constexpr (L) {
                 normal = landscape_shading_normal(S, ray, hit.t, bi, hit.n);
-                outgoing = landscape_outgoing(S, ray, hit.t, bi, hit.n);
+                outgoing = landscape_outgoing<F>(S, ray, hit.t, bi, hit.n);
             }
         } else {
             const float radius = b_radius(S, bi);
@@ -405,12 +405,12 @@ __device__ __forceinline__ void flush_events(const Events &ev, unsigned long lon
 #define SG_TRACE_MIN_BLOCKS 4
 #endif
 
-template <bool C, bool L>
+template <bool C, bool L, bool F>
 __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(const __grid_constant__ TraceParams P) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
     Events ev{};
-    const Counter<C, L> K{&ev};
+    const Counter<C, L, F> K{&ev};
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
@@ -473,8 +473,8 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // warp's lanes that run the same samples; they meet after each pass so that
 // a warp replays one pass at a time (lanes left to drift between the two
 // passes would run two copies of the integrator apart).
-template <bool L>
-__device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L> K, Prb &G, float3 w, uint32_t pixel,
+template <bool L, bool F>
+__device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L, F> K, Prb &G, float3 w, uint32_t pixel,
                                                uint32_t x, uint32_t y, uint32_t smp, unsigned lanes) {
     bool again = true;
 #pragma unroll 1
@@ -499,7 +499,7 @@ __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L>
 #define SG_ADJOINT_MIN_BLOCKS 2
 #endif
 
-template <bool L>
+template <bool L, bool F>
 __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     adjoint_kernel(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A) {
     extern __shared__ float4 smem[];
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
         inv[2u * k + 1u] = make_float4(inv_or_zero(r.x), inv_or_zero(r.y), inv_or_zero(r.z), 0.0f);
     }
     const Scene S = stage_scene(P, smem);  // synchronises the block
-    const Counter<false, L> K{nullptr};
+    const Counter<false, L, F> K{nullptr};
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t x = blockIdx.x * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = blockIdx.y * kTile + (warp >> 1) * 4u + (lane >> 3);
@@ -572,11 +572,12 @@ __device__ __forceinline__ Ray load_ray(const sg_ray &in) {
                in.anchor};
 }
 
+template <bool F>
 __global__ void __launch_bounds__(kThreads) closest_hit_kernel(const __grid_constant__ TraceParams P,
                                                                const sg_ray *rays, sg_hit *hits, uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false, true> K{nullptr};
+    const Counter<false, true, F> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
@@ -595,12 +596,13 @@ __global__ void __launch_bounds__(kThreads) closest_hit_kernel(const __grid_cons
     hits[k] = out;
 }
 
+template <bool F>
 __global__ void __launch_bounds__(kThreads) visibility_kernel(const __grid_constant__ TraceParams P,
                                                               const sg_ray *rays, const uint32_t *lights,
                                                               float *out, uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false, true> K{nullptr};
+    const Counter<false, true, F> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
@@ -609,12 +611,13 @@ __global__ void __launch_bounds__(kThreads) visibility_kernel(const __grid_const
     out[k] = valid ? light_visibility(S, K, load_ray(in), light) : 0.0f;
 }
 
+template <bool F>
 __global__ void __launch_bounds__(kThreads) ring_probe_kernel(const __grid_constant__ TraceParams P,
                                                               const sg_ray *rays, uint32_t body, float *out,
                                                               uint32_t n) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
-    const Counter<false, true> K{nullptr};
+    const Counter<false, true, F> K{nullptr};
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const sg_ray in = rays[k];
@@ -771,24 +774,33 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Launch one instantiation of a kernel with `smem` bytes of dynamic shared
+// memory and 256-thread CTAs.
+template <typename... K, typename... A>
+static cudaError_t launch_variant(void (*kernel)(K...), dim3 grid, size_t smem, cudaStream_t stream, A &&...args) {
+    cudaError_t e = set_smem((const void *)kernel, smem);
+    if (e != cudaSuccess) return e;
+    kernel<<<grid, kThreads, smem, stream>>>(args...);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t stream) {
     const size_t smem = trace_smem_bytes(p);
     const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
     // The landscape instantiation only for frames that enable it: the
     // celestial one carries neither its registers nor its code.
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const void *fn = count_events ? (land ? (const void *)trace_kernel<true, true> : (const void *)trace_kernel<true, false>)
-                                  : (land ? (const void *)trace_kernel<false, true> : (const void *)trace_kernel<false, false>);
-    cudaError_t e = set_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    if (count_events) {
-        if (land) trace_kernel<true, true><<<grid, kThreads, smem, stream>>>(p);
-        else trace_kernel<true, false><<<grid, kThreads, smem, stream>>>(p);
-    } else {
-        if (land) trace_kernel<false, true><<<grid, kThreads, smem, stream>>>(p);
-        else trace_kernel<false, false><<<grid, kThreads, smem, stream>>>(p);
+    const int which = (count_events ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    switch (which) {
+        case 0: return launch_variant(trace_kernel<false, false, false>, grid, smem, stream, p);
+        case 1: return launch_variant(trace_kernel<false, false, true>, grid, smem, stream, p);
+        case 2: return launch_variant(trace_kernel<false, true, false>, grid, smem, stream, p);
+        case 3: return launch_variant(trace_kernel<false, true, true>, grid, smem, stream, p);
+        case 4: return launch_variant(trace_kernel<true, false, false>, grid, smem, stream, p);
+        case 5: return launch_variant(trace_kernel<true, false, true>, grid, smem, stream, p);
+        case 6: return launch_variant(trace_kernel<true, true, false>, grid, smem, stream, p);
+        default: return launch_variant(trace_kernel<true, true, true>, grid, smem, stream, p);
     }
-    return cudaGetLastError();
 }
 
 size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a) {
@@ -800,42 +812,39 @@ cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStr
     const size_t smem = adjoint_smem_bytes(p, a);
     const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const void *fn = land ? (const void *)adjoint_kernel<true> : (const void *)adjoint_kernel<false>;
-    cudaError_t e = set_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    if (land) adjoint_kernel<true><<<grid, kThreads, smem, stream>>>(p, a);
-    else adjoint_kernel<false><<<grid, kThreads, smem, stream>>>(p, a);
-    return cudaGetLastError();
+    switch ((land ? 2 : 0) | (p.fp64_sites ? 1 : 0)) {
+        case 0: return launch_variant(adjoint_kernel<false, false>, grid, smem, stream, p, a);
+        case 1: return launch_variant(adjoint_kernel<false, true>, grid, smem, stream, p, a);
+        case 2: return launch_variant(adjoint_kernel<true, false>, grid, smem, stream, p, a);
+        default: return launch_variant(adjoint_kernel<true, true>, grid, smem, stream, p, a);
+    }
 }
 
 cudaError_t launch_closest_hit(const TraceParams &p, const sg_ray *rays, sg_hit *hits, uint32_t n,
                                cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const size_t smem = trace_smem_bytes(p);
-    cudaError_t e = set_smem((const void *)closest_hit_kernel, smem);
-    if (e != cudaSuccess) return e;
-    closest_hit_kernel<<<(n + kThreads - 1) / kThreads, kThreads, smem, stream>>>(p, rays, hits, n);
-    return cudaGetLastError();
+    const dim3 grid((n + kThreads - 1) / kThreads);
+    if (p.fp64_sites) return launch_variant(closest_hit_kernel<true>, grid, smem, stream, p, rays, hits, n);
+    return launch_variant(closest_hit_kernel<false>, grid, smem, stream, p, rays, hits, n);
 }
 
 cudaError_t launch_light_visibility(const TraceParams &p, const sg_ray *rays, const uint32_t *lights,
                                     float *out, uint32_t n, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const size_t smem = trace_smem_bytes(p);
-    cudaError_t e = set_smem((const void *)visibility_kernel, smem);
-    if (e != cudaSuccess) return e;
-    visibility_kernel<<<(n + kThreads - 1) / kThreads, kThreads, smem, stream>>>(p, rays, lights, out, n);
-    return cudaGetLastError();
+    const dim3 grid((n + kThreads - 1) / kThreads);
+    if (p.fp64_sites) return launch_variant(visibility_kernel<true>, grid, smem, stream, p, rays, lights, out, n);
+    return launch_variant(visibility_kernel<false>, grid, smem, stream, p, rays, lights, out, n);
 }
 
 cudaError_t launch_ring_probe(const TraceParams &p, const sg_ray *rays, uint32_t body, float *out,
                               uint32_t n, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const size_t smem = trace_smem_bytes(p);
-    cudaError_t e = set_smem((const void *)ring_probe_kernel, smem);
-    if (e != cudaSuccess) return e;
-    ring_probe_kernel<<<(n + kThreads - 1) / kThreads, kThreads, smem, stream>>>(p, rays, body, out, n);
-    return cudaGetLastError();
+    const dim3 grid((n + kThreads - 1) / kThreads);
+    if (p.fp64_sites) return launch_variant(ring_probe_kernel<true>, grid, smem, stream, p, rays, body, out, n);
+    return launch_variant(ring_probe_kernel<false>, grid, smem, stream, p, rays, body, out, n);
 }
 
 cudaError_t launch_terrain_probe(const TraceParams &p, const float *rays, float *out, uint32_t n,

@@ -44,6 +44,22 @@ __device__ __forceinline__ float3 ground_origin(const Scene &S, const Ray &r) {
     return f3(g.x, __fadd_rn(g.y, S.s->g.ground_east[3]), g.z);
 }
 
+// The same in double for the FP64 sites (metres per AU exact).
+constexpr double kMetresPerAuD = 149597870700.0;
+__device__ __forceinline__ d3 to_ground_d(const Scene &S, d3 v) {
+    return d3{dot(v, D(g_east(S))), dot(v, D(g_up(S))), dot(v, D(g_north(S)))};
+}
+__device__ __forceinline__ d3 from_ground_d(const Scene &S, d3 v) {
+    return D(g_east(S)) * v.x + D(g_up(S)) * v.y + D(g_north(S)) * v.z;
+}
+__device__ __forceinline__ d3 ground_origin_d(const Scene &S, const Ray &r) {
+    d3 c = D(r.o);
+    if (r.anchor != kMiss) c = D(xyz(bf(S, r.anchor, kCenter))) + D(xyz(bf(S, r.anchor, kLow))) + c;
+    d3 g = to_ground_d(S, c * kMetresPerAuD);
+    g.y += (double)S.s->g.ground_east[3];
+    return g;
+}
+
 // rotate_north / rotate_east / rotate_up and the tumbled-rock frame
 // (ground.wgsl:33-61). Sines and cosines come precomputed per primitive
 // (TraceParams::prop_trig: (sin, cos) of the x, y and z angles, the yaw in
@@ -319,10 +335,37 @@ __device__ __forceinline__ float landscape_top(const Scene &S) {
     return top;
 }
 
+// The host-sphere intersection of landscape_query (ground.wgsl:138-158) in
+// double; the returned distance (AU) and normal are rounded to f32.
+__device__ __noinline__ LandHit host_sphere_fp64(Scene S, Ray ray, float limit, bool occlusion) {
+    const LandHit miss{limit, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
+    const double radius = (double)S.s->g.ground_up[3];
+    const d3 o = ground_origin_d(S, ray);
+    const d3 d = to_ground_d(S, D(ray.d));
+    const double a = dot(d, d);
+    const double b = -radius * d.y - dot(o, d);
+    const double c = o.x * o.x + o.z * o.z + o.y * (2.0 * radius + o.y);
+    const double h = b * b - a * c;
+    if (h < 0.0) return miss;
+    const double root = sqrt(h);
+    const double q = b + (b >= 0.0 ? root : -root);
+    if (q == 0.0) return miss;
+    const double cq = c / q, qa = q / a;
+    const double t0 = fmin(cq, qa), t1 = fmax(cq, qa);
+    const double distance = t0 > 0.001 ? t0 : t1;
+    const float au = (float)(distance / kMetresPerAuD);
+    if (!(distance > 0.001) || !(au < limit)) return miss;
+    if (occlusion) return LandHit{au, kLocalBase, 0.0f, f3(0.0f, 0.0f, 0.0f)};
+    const d3 p = o + d * distance;
+    d3 n = d3{p.x / radius, 1.0 + p.y / radius, p.z / radius};
+    n = n * (1.0 / sqrt(dot(n, n)));
+    return LandHit{au, kLocalBase, 0.0f, F(from_ground_d(S, n))};
+}
+
 // landscape_query (ground.wgsl:123-242). Vegetation kinds (> 2.5) are
 // rejected on the host and never reach the device.
-template <bool C, bool L>
-__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L> K, Ray ray, float limit, bool occlusion) {
+template <bool C, bool L, bool F>
+__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion) {
     LandHit closest{limit, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const sg_settings *s = S.s;
     if (s->g.ground_north[3] == 0.0f) return closest;
@@ -338,6 +381,13 @@ __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L> K, Ray ray, 
         return LandHit{t, host, delta, sphere_normal(S, ray, host, delta)};
     }
     if (d.y >= 0.0f && o.y > landscape_top(S)) return closest;
+    if constexpr (F) {
+        const LandHit host = host_sphere_fp64(S, ray, closest.t, occlusion);
+        if (host.index != kMiss) {
+            if (occlusion) return host;
+            closest = host;
+        }
+    } else {
     // Host sphere in the surface frame (ground.wgsl:138-158).
     const float a = dot_rn(d, d);
     const float b = __fsub_rn(__fmul_rn(-radius, d.y), dot_rn(o, d));
@@ -359,6 +409,7 @@ __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L> K, Ray ray, 
                 closest = LandHit{au, kLocalBase, 0.0f, from_ground(S, n)};
             }
         }
+    }
     }
     if (s->g.ground_counts[1] != 0u && S.p->terrain) {
         const float tl = __fmul_rn(fminf(closest.t, 1.0e18f), kMetresPerAu);
@@ -555,10 +606,26 @@ __device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float 
     return normalize(normal + g * strength);
 }
 
+// landscape_outgoing in double (FP64 sites): the hit point, its reprojection
+// onto the host sphere and the 5 mm step, rounded to f32 AU at the end.
+__device__ __noinline__ Ray landscape_outgoing_fp64(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
+    d3 p = ground_origin_d(S, ray) + to_ground_d(S, D(ray.d)) * ((double)t * kMetresPerAuD);
+    if (index == kLocalBase) {
+        const double radius = (double)S.s->g.ground_up[3];
+        const double d2 = p.x * p.x + p.z * p.z;
+        if (p.y > -radius && d2 < radius * radius) p.y = -d2 / (radius + sqrt(radius * radius - d2));
+    }
+    p = p + to_ground_d(S, D(normal)) * 0.005;
+    p.y -= (double)S.s->g.ground_east[3];
+    return Ray{F(from_ground_d(S, p) * (1.0 / kMetresPerAuD)), normal, kMiss};
+}
+
 // landscape_outgoing (ground.wgsl:649-662): reproject a host-sphere hit
 // without radius cancellation, step 5 mm along the normal, back to AU.
+template <bool F>
 __device__ __forceinline__ Ray landscape_outgoing(const Scene &S, const Ray &ray, float t, uint32_t index,
                                                   float3 normal) {
+    if constexpr (F) return landscape_outgoing_fp64(S, ray, t, index, normal);
     float3 p = landscape_point(S, ray, t);
     if (index == kLocalBase) {
         const float radius = S.s->g.ground_up[3];

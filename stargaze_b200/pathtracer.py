@@ -109,6 +109,11 @@ class PathTracer:
         check(self._lib.sg_prepare_frame(self._ctx, C.byref(view), C.byref(fresh)), self._ctx)
         return bool(fresh.value)
 
+    def set_fp64_sites(self, enable: bool) -> None:
+        """Ring-plane and host-sphere intersections and the 5 mm offset in
+        FP64 (extension; off: the reference's f32 arithmetic)."""
+        check(self._lib.sg_set_fp64_sites(self._ctx, int(bool(enable))), self._ctx)
+
     def set_quality(self, samples: int, bounces: int, limit: int) -> None:
         check(self._lib.sg_set_quality(self._ctx, samples, bounces, limit), self._ctx)
 
