@@ -3,7 +3,9 @@
 
 A step renders the ring workload (1920x1080, 256 spp: a ringed giant with a
 512-bin optical-depth table, a binary star and a moon eclipse) from a fresh
-accumulation: four 64-sample dispatches of the reference's encode contract.
+accumulation: four 64-sample dispatches of the reference's encode contract,
+through the wavefront integrator (the library default; `--integrator
+megakernel` times the per-pixel megakernel instead).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -96,7 +98,27 @@ def profile_adjoint_ring_512():
         t.backward(frame, t.tape(), dl)
 
 
-PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512}
+def profile_wavefront_rings_1080p():
+    """Ring workload at 1920x1080 through the wavefront integrator with a
+    4 Mi-path pool (3.4 GB on the device, small enough for multi-pass
+    captures): two 64-sample dispatches (the first allocates the pool)."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl = W.rings_1080p()
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    t.set_integrator("wavefront", 1 << 22)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.prepare_frame(frame)
+        t.encode(frame)
+    t.read_pixels()
+    print(t.integrator(), flush=True)
+
+
+PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512,
+                 "wavefront_rings_1080p": profile_wavefront_rings_1080p}
 
 
 def parse_args():
@@ -106,6 +128,7 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", default="rings_1080p")
+    p.add_argument("--integrator", choices=["wavefront", "megakernel"], default="wavefront")
     p.add_argument("--spp", type=int, default=256)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -269,10 +292,26 @@ def convergence(wl, image: np.ndarray, spp: int, msamples_per_s: float, device: 
             "reference": "this integrator at 4096 spp, disjoint noise (parity with the oracle is tested at small sizes)"}
 
 
+def timed_forward(t, wl, frame, stream) -> float:
+    """Milliseconds (CUDA events on `stream`) to render `wl.spp` samples
+    from a fresh accumulation of `frame`."""
+    import torch
+
+    t.prepare_frame(frame)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    while t.samples() < wl.spp:
+        t.encode(frame, stream)
+    b.record(stream)
+    stream.synchronize()
+    return a.elapsed_time(b)
+
+
 def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
     """Forward (spp samples from a fresh accumulation) and path-replay
     adjoint (sg_backward for a seeded d loss / d image) times, CUDA events on
-    the launching stream, median over `reps`."""
+    the launching stream, median over `reps`; the forward with both
+    integrators (the adjoint replays the same samples either way)."""
     import torch
 
     from stargaze_b200 import PathTracer
@@ -281,32 +320,76 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
     t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
     upload_workload(t, wl)
     dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
-    fwd, bwd = [], []
+    fwd, mega, bwd = [], [], []
     for r in range(reps + 1):
         frame = wl.frame.copy()
         frame.scene_time = float(-1 - r)
-        t.prepare_frame(frame)
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        e[0].record(stream)
-        while t.samples() < wl.spp:
-            t.encode(frame, stream)
-        e[1].record(stream)
+        t.set_integrator("megakernel")
+        m = timed_forward(t, wl, frame, stream)
+        t.set_integrator("wavefront")
+        frame.scene_time = float(-100 - r)
+        f = timed_forward(t, wl, frame, stream)
         tape = t.tape()
-        e[2].record(stream)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e[0].record(stream)
         g = t.backward(frame, tape, dl, stream)
-        e[3].record(stream)
+        e[1].record(stream)
         stream.synchronize()
         if r > 0:  # the first round loads the kernels
-            fwd.append(e[0].elapsed_time(e[1]))
-            bwd.append(e[2].elapsed_time(e[3]))
+            fwd.append(f)
+            mega.append(m)
+            bwd.append(e[0].elapsed_time(e[1]))
     t.close()
-    f, b = statistics.median(fwd), statistics.median(bwd)
+    f, m, b = statistics.median(fwd), statistics.median(mega), statistics.median(bwd)
     params = int(sum(v.size for v in wl.ring_tables.values())) + 6 * len(wl.frame.bodies)
     if wl.landscape is not None and wl.landscape.albedo_map is not None:
         params += int(wl.landscape.albedo_map.size)
     return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp, "forward_ms": f,
-            "backward_ms": b, "ratio": b / f, "forward_plus_adjoint_over_forward": (f + b) / f,
+            "forward_megakernel_ms": m, "backward_ms": b, "ratio": b / f,
+            "forward_plus_adjoint_over_forward": (f + b) / f, "ratio_vs_megakernel_forward": b / m,
             "parameters": params, "dropped_entries": int(g.dropped)}
+
+
+def integrator_comparison(wl, device: int, stream, reps: int = 3) -> dict:
+    """The workload's step (spp samples from a fresh accumulation) with each
+    integrator, and the wavefront's time per stage on one more step."""
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
+    upload_workload(t, wl)
+    out = {}
+    for name in ("megakernel", "wavefront"):
+        t.set_integrator(name)
+        times = []
+        for r in range(reps + 1):
+            frame = wl.frame.copy()
+            frame.scene_time = float(-7 - r)
+            ms = timed_forward(t, wl, frame, stream)
+            if r > 0:
+                times.append(ms)
+        out[f"{name}_ms_per_step"] = statistics.median(times)
+    out["wavefront_speedup"] = out["megakernel_ms_per_step"] / out["wavefront_ms_per_step"]
+    info = t.integrator()
+    out["wavefront_pool_paths"] = info["pool_paths"]
+    out["wavefront_iterations_per_dispatch"] = info["iterations"]
+    t.close()
+    return out
+
+
+def stage_times(tracer, wl, frame, stream, batches: int) -> dict:
+    """Milliseconds per wavefront stage over one step (events around every
+    stage launch; outside the timed region)."""
+    tracer.set_stage_timing(True)
+    frame.scene_time = -55.0
+    tracer.prepare_frame(frame)
+    total = dict.fromkeys(tracer.STAGES, 0.0)
+    for _ in range(batches):
+        tracer.encode(frame, stream)
+        for k, v in tracer.stage_times().items():
+            total[k] += v
+    tracer.set_stage_timing(False)
+    return total
 
 
 def fp64_sites(wl, device: int, stream, reps: int = 2) -> dict:
@@ -404,6 +487,7 @@ def run_ours(args):
 
     tracer = PathTracer((wl.width, wl.height), opts, device=local)
     upload_workload(tracer, wl)
+    tracer.set_integrator(args.integrator)
     stream = torch.cuda.Stream()
     frame = wl.frame.copy()
 
@@ -472,6 +556,7 @@ def run_ours(args):
             b.record(stream)
             stream.synchronize()
             e2e_ms.append(a.elapsed_time(b))
+        stages = stage_times(tracer, wl, frame, stream, batches) if args.integrator == "wavefront" else None
 
     total_ms, e2e_total = max_over_ranks([sum(step_ms), sum(e2e_ms)], dist, "cuda")
 
@@ -500,6 +585,7 @@ def run_ours(args):
             extras["adjoint"] = {"ratio": ring["ratio"], "ring_512": ring, "terrain_1080p": terrain,
                                  "note": "ratio = adjoint time / forward time at equal spp (ring scene)"}
             extras["fp64_sites"] = fp64_sites(wl, local, stream)
+            extras["integrators"] = integrator_comparison(wl, local, stream)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -507,11 +593,15 @@ def run_ours(args):
             "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": args.spp,
                        "max_bounces": wl.max_bounces, "batches_per_step": batches, "samples_per_step": samples_per_step,
                        "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps",
-                       "parallelism": f"replicas x{world}, disjoint noise sequences"},
+                       "parallelism": f"replicas x{world}, disjoint noise sequences",
+                       "integrator": args.integrator},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak.value, "traffic": TRAFFIC_BYTES_PER_LAUNCH,
-                         "kernel": "trace_kernel", "ops_per_launch": ops_per_launch,
+                         "kernel": ("wavefront dispatch (extend, ring and surface stages, resolve)"
+                                    if args.integrator == "wavefront" else "trace_kernel (megakernel)"),
+                         "ops_per_launch": ops_per_launch,
                          "launch_ms": statistics.mean(launch_ms),
+                         "stages_ms_per_step": stages,
                          "events_per_launch": {n: int(totals[k]) // batches for k, n in enumerate(EVENT_ORDER)},
                          "peak_source": "measured FMA-chain kernel (sg_measure_fp32_peak)"},
             "e2e": {"value": e2e_value, "unit": UNIT,

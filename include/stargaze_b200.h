@@ -341,6 +341,43 @@ SG_API int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu,
  * accumulation on the next encode. */
 SG_API int sg_set_fp64_sites(sg_context *ctx, int enable);
 
+/* Extension (no reference counterpart; the reference has one WGSL compute
+ * pass, pathtrace.wgsl:1645-1675): which CUDA integrator sg_encode runs.
+ *   SG_INTEGRATOR_MEGAKERNEL  one thread per pixel walks every path of the
+ *                             dispatch to its end;
+ *   SG_INTEGRATOR_WAVEFRONT   (default) paths live in a pool of `pool_paths`
+ *                             slots in device memory (0: 16 Mi, about 280 B
+ *                             each, or the dispatch's sample count if that is
+ *                             smaller) and advance one vertex per stage
+ *                             iteration through extend / ring / surface
+ *                             kernels over compacted queues.
+ * Both run the same per-path code on the same random sequences; their
+ * accumulations agree to a few ulps (the compiler fuses shading multiply-
+ * adds differently in the two kernels). The wavefront allocates its pool
+ * and a per-sample radiance buffer (16 B per pixel and sample, up to
+ * 2.25 GiB; larger dispatches run in sample chunks) on first use, and its
+ * sg_encode returns once the dispatch's stages have drained (it reads a
+ * 32-byte counter back every few iterations). sg_encode_counted always runs
+ * the megakernel. The choice does not reset the accumulation. */
+#define SG_INTEGRATOR_MEGAKERNEL 0
+#define SG_INTEGRATOR_WAVEFRONT 1
+#define SG_WAVE_MAX_POOL (1u << 26)
+SG_API int sg_set_integrator(sg_context *ctx, int integrator, uint32_t pool_paths);
+
+/* The integrator in use, the wavefront pool of the last dispatch and the
+ * stage iterations it ran (0 for the megakernel). Any pointer may be NULL. */
+SG_API int sg_get_integrator(const sg_context *ctx, int *integrator, uint32_t *pool_paths,
+                             uint32_t *iterations);
+
+/* Extension (measurement): with timing on, every wavefront stage launch is
+ * bracketed by CUDA events and sg_encode waits for the dispatch to finish;
+ * sg_get_stage_times then gives the milliseconds of the last timed
+ * dispatch spent in ms[0] extend, ms[1] ring, ms[2] surface, ms[3] resolve
+ * and ms[4] between stages (launch gaps and host checks). */
+#define SG_STAGE_COUNT 5
+SG_API int sg_set_stage_timing(sg_context *ctx, int enable);
+SG_API int sg_get_stage_times(const sg_context *ctx, float *ms);
+
 /* ------------------------------------------------------------------ */
 /* Path-replay adjoint (extension: the reference renders forward only) */
 /* ------------------------------------------------------------------ */
@@ -404,7 +441,9 @@ SG_API int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *ta
 /* Last error message of the context (or of the library when ctx is NULL). */
 SG_API const char *sg_last_error(const sg_context *ctx);
 SG_API const char *sg_status_string(int status);
-/* Number of integrator kernel launches issued by this context so far. */
+/* Number of integrator kernel launches issued by this context so far (one
+ * per megakernel dispatch; three per wavefront iteration plus one resolve
+ * per sample chunk). */
 SG_API int sg_launch_count(const sg_context *ctx, uint64_t *launches);
 
 /* sg_encode through the event-counting variant of the integrator kernel:

@@ -46,6 +46,10 @@ _SIGNATURES = {
     "sg_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "sg_closest_hit_noalloc": (C.c_int, [C.c_int, C.POINTER(abi.FrameView), _P, C.c_uint32, _P, _P]),
     "sg_set_fp64_sites": (C.c_int, [_P, C.c_int]),
+    "sg_set_integrator": (C.c_int, [_P, C.c_int, C.c_uint32]),
+    "sg_get_integrator": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "sg_set_stage_timing": (C.c_int, [_P, C.c_int]),
+    "sg_get_stage_times": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "sg_get_tape": (C.c_int, [_P, C.POINTER(abi.Tape)]),
     "sg_backward": (C.c_int, [_P, C.POINTER(abi.FrameView), C.POINTER(abi.Tape), _P, C.c_int,
                               C.POINTER(abi.Gradients), _P]),

@@ -118,6 +118,9 @@ class Hit(C.Structure):
 
 
 NOALLOC_MAX_RAYS = 65536
+INTEGRATOR_MEGAKERNEL = 0
+INTEGRATOR_WAVEFRONT = 1
+WAVE_MAX_POOL = 1 << 26
 NOALLOC_SCRATCH_BYTES = 4 << 20
 TAPE_RANGES = 16
 

@@ -228,7 +228,7 @@ struct LandHit {
     float3 n;
 };
 template <bool C, bool L, bool F>
-__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion);
+static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion);
 
 // closest_hit (pathtrace.wgsl:173-185): every body except the landscape
 // host, then the landscape.
@@ -281,7 +281,7 @@ struct LightSample {
 
 // sample_light (pathtrace.wgsl:214-234), one stratum: uniform cone sampling.
 template <bool C, bool L, bool F>
-__device__ SG_HELPER LightSample sample_light(Scene S, Counter<C, L, F> K, Ray r, uint32_t i, uint32_t rng) {
+static __device__ SG_HELPER LightSample sample_light(Scene S, Counter<C, L, F> K, Ray r, uint32_t i, uint32_t rng) {
     K.add(&Events::light_samples);
     const float3 oc = relative_center(S, r, i);
     const float3 axis = normalize(oc);
@@ -340,7 +340,7 @@ __device__ __forceinline__ float3 F(d3 v) { return f3((float)v.x, (float)v.y, (f
 
 // ring_hit in double: the centre difference from the hi/lo parts, the
 // perpendicular, the plane distance and the annulus test.
-__device__ __noinline__ RingHit ring_hit_fp64(Scene S, Ray r, uint32_t i) {
+static __device__ __noinline__ RingHit ring_hit_fp64(Scene S, Ray r, uint32_t i) {
     const RingHit miss{1.0e30f, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const float4 plane = bf(S, i, kRingPlane);
     const float4 params = bf(S, i, kRingParams);
@@ -413,7 +413,7 @@ struct Optics {
 // Cassini division, Encke and Keeler gaps). Out of line: its accurate sinf
 // calls carry a large range-reduction path that the table and scalar
 // profiles never need.
-__device__ __noinline__ Optics banded_optics(float x, float tau, float3 color) {
+static __device__ __noinline__ Optics banded_optics(float x, float tau, float3 color) {
     const float broad = 0.5f + 0.5f * sinf(43.0f * x + 1.8f * sinf(17.0f * x));
     const float fine = 0.5f + 0.5f * sinf(1900.0f * x + 2.0f * sinf(311.0f * x));
     const float micro = 0.5f + 0.5f * sinf(6100.0f * x);
@@ -530,7 +530,7 @@ __device__ __forceinline__ float visibility_core(const Scene &S, Counter<C, L, F
 }
 
 template <bool C, bool L, bool F>
-__device__ SG_HELPER float light_visibility(Scene S, Counter<C, L, F> K, Ray r, uint32_t light) {
+static __device__ SG_HELPER float light_visibility(Scene S, Counter<C, L, F> K, Ray r, uint32_t light) {
     return visibility_core(S, K, r, light, nullptr);
 }
 
@@ -540,7 +540,7 @@ __device__ __forceinline__ float one_minus_exp(float x) {
 }
 
 // ring_bsdf (rings.wgsl:151-166): exact single scattering in a finite slab.
-__device__ SG_HELPER float3 ring_bsdf(Optics o, float outgoing, float incoming) {
+static __device__ SG_HELPER float3 ring_bsdf(Optics o, float outgoing, float incoming) {
     const float mo = fmaxf(fabsf(outgoing), 1.0e-7f);
     const float mi = fmaxf(fabsf(incoming), 1.0e-7f);
     const float a = o.tau / mo;
@@ -626,7 +626,7 @@ __device__ __forceinline__ ShinePoint shine_point(const Scene &S, Counter<C, L, 
 
 // ringshine (pathtrace.wgsl:1248-1296): NEE of a planet's own sunlit ring.
 template <bool C, bool L, bool F>
-__device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
+static __device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
                                         bool last_vertex, uint32_t rng) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     if (!has_ring(S, index)) return Shine{zero, rng};
@@ -666,7 +666,7 @@ struct DiscHit {
 // point_disc_hit (pathtrace.wgsl:1308-1333): depth-0 camera rays see an
 // unresolved body as a disc of at least a bright star's size.
 template <bool C, bool L, bool F>
-__device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, Ray r, Hit closest, uint32_t rng) {
+static __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, Ray r, Hit closest, uint32_t rng) {
     const sg_settings *s = S.s;
     DiscHit out{closest, 1.0f, rng};
     float total = 0.0f;
@@ -712,7 +712,7 @@ __device__ __forceinline__ float hash31(float3 p) {
 __device__ __forceinline__ float smooth_rn(float f) {
     return __fmul_rn(__fmul_rn(f, f), __fsub_rn(3.0f, __fmul_rn(2.0f, f)));
 }
-__device__ __noinline__ float vnoise(float3 p) {
+static __device__ __noinline__ float vnoise(float3 p) {
     const float3 i = f3(floorf(p.x), floorf(p.y), floorf(p.z));
     const float3 f = sub_rn(p, i);
     const float3 u = f3(smooth_rn(f.x), smooth_rn(f.y), smooth_rn(f.z));
@@ -725,7 +725,7 @@ __device__ __noinline__ float vnoise(float3 p) {
 
 // Mottle factor of surface_albedo (pathtrace.wgsl:912-923), out of line:
 // five octaves of value noise that the constant-albedo path never runs.
-__device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float strength, float3 normal) {
+static __device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float strength, float3 normal) {
     const float3 y = xyz(axis_y);
     const float3 local = f3(dot_rn(normal, axis_x), dot_rn(normal, y), dot_rn(normal, cross_rn(axis_x, y)));
     const float seed = axis_y.w;

@@ -3,6 +3,8 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "../../include/stargaze_b200.h"
@@ -55,6 +57,69 @@ size_t trace_smem_bytes(const TraceParams &p);
 void set_library_error(const char *message);
 
 cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Wavefront integrator (sg_wavefront.cu): the same per-path arithmetic as
+// launch_trace, run as extend / ring / surface stages over queues
+// of paths whose state lives in HBM, then an in-order per-pixel resolve.
+// ---------------------------------------------------------------------------
+
+// Counters of one iteration of the stage loop.
+struct WaveCounters {
+    uint32_t cont;     // paths the previous iteration's shade stages kept
+    uint32_t unused;
+    uint32_t ring;     // ring-queue entries extend wrote
+    uint32_t surface;  // surface-queue entries extend wrote
+    uint32_t next;     // first sample index (within the chunk) not taken yet
+    uint32_t pad[3];
+};
+// Iteration t uses counter sets t and t + 1 (mod this) and clears t + 2.
+constexpr uint32_t kWaveCounterSets = 8;
+// Float4 planes of one path's state, and of one extend result.
+constexpr uint32_t kWavePlanes = 7;
+constexpr uint32_t kWaveHitPlanes = 3;
+
+struct WaveParams {
+    float4 *state[2];         // kWavePlanes planes of `pool` float4 each
+    float4 *hits;             // kWaveHitPlanes planes of `pool` float4
+    uint32_t *ring_queue;     // `pool` path indices
+    uint32_t *surface_queue;  // `pool` path indices
+    WaveCounters *counters;   // kWaveCounterSets sets
+    float4 *results;          // chunk_samples planes of width * height radiance samples
+    float4 *totals;           // per-pixel running sums between chunks
+    uint32_t pool;            // path slots
+    uint32_t tiles_x, tiles_y;
+    uint32_t chunk_first;     // first sample of the chunk within the dispatch
+    uint32_t chunk_samples;   // samples of the chunk
+};
+
+// Bytes of the per-context wavefront buffers for `pool` path slots and
+// results for `chunk_samples` samples of `pixels` pixels.
+size_t wave_state_bytes(uint32_t pool);
+size_t wave_result_bytes(uint32_t pixels, uint32_t chunk_samples);
+
+// Optional per-stage timing of a wavefront dispatch: an event is recorded
+// at every stage boundary; stage[k] names what runs from mark k to k + 1.
+enum WaveStage : int { kStageExtend = 0, kStageRing, kStageSurface, kStageResolve, kStageGap, kStageCount };
+struct StageMarks {
+    std::vector<cudaEvent_t> events;  // owned; grown on demand, reused
+    std::vector<int> stage;
+    size_t used = 0;
+};
+
+// What one wavefront dispatch ran.
+struct WaveRun {
+    uint32_t iterations = 0;  // stage iterations over all chunks
+    uint32_t kernels = 0;     // kernel launches
+};
+
+// Runs the dispatch described by `p` (counts.z samples) in chunks of at
+// most w.chunk_samples samples. Between groups of iterations it copies the
+// live counters into `pinned` (host memory) and waits on `ready` to decide
+// whether the chunk has drained, so it returns once the GPU has finished
+// all but the final resolve. With `marks`, events bracket every stage.
+cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *pinned, cudaEvent_t ready,
+                             cudaStream_t stream, WaveRun *run, StageMarks *marks);
 cudaError_t launch_closest_hit(const TraceParams &p, const sg_ray *rays, sg_hit *hits, uint32_t n,
                                cudaStream_t stream);
 cudaError_t launch_light_visibility(const TraceParams &p, const sg_ray *rays, const uint32_t *lights,

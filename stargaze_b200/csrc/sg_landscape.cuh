@@ -105,7 +105,7 @@ __device__ __forceinline__ float2 box_interval(float3 p, float3 d, float3 extent
 }
 
 // rock_hit (ground.wgsl:82-121): a box with clipped corners; 14 planes.
-__device__ __noinline__ float4 rock_hit(float3 p, float3 d, float3 e) {
+static __device__ __noinline__ float4 rock_hit(float3 p, float3 d, float3 e) {
     const float3 origin = div3_rn(p, e);
     const float3 direction = div3_rn(d, e);
     float near_ = -1.0e30f, far_ = 1.0e30f;
@@ -242,7 +242,7 @@ __device__ __forceinline__ float2 t_interval(const float *T, uint32_t cells, flo
 
 // terrain_query (terrain.wgsl:152-234): near-to-far min/max quadtree.
 // Returns (normal, distance); distance 1e30 on a miss.
-__device__ __noinline__ float4 terrain_query(const float *T, uint32_t cells, float radius, float3 o, float3 d,
+static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cells, float radius, float3 o, float3 d,
                                              float initial_limit, bool occlusion) {
     float4 result = make_float4(0.0f, 0.0f, 0.0f, 1.0e30f);
     float limit = initial_limit;
@@ -337,7 +337,7 @@ __device__ __forceinline__ float landscape_top(const Scene &S) {
 
 // The host-sphere intersection of landscape_query (ground.wgsl:138-158) in
 // double; the returned distance (AU) and normal are rounded to f32.
-__device__ __noinline__ LandHit host_sphere_fp64(Scene S, Ray ray, float limit, bool occlusion) {
+static __device__ __noinline__ LandHit host_sphere_fp64(Scene S, Ray ray, float limit, bool occlusion) {
     const LandHit miss{limit, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const double radius = (double)S.s->g.ground_up[3];
     const d3 o = ground_origin_d(S, ray);
@@ -365,7 +365,7 @@ __device__ __noinline__ LandHit host_sphere_fp64(Scene S, Ray ray, float limit, 
 // landscape_query (ground.wgsl:123-242). Vegetation kinds (> 2.5) are
 // rejected on the host and never reach the device.
 template <bool C, bool L, bool F>
-__device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion) {
+static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion) {
     LandHit closest{limit, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const sg_settings *s = S.s;
     if (s->g.ground_north[3] == 0.0f) return closest;
@@ -499,7 +499,7 @@ __device__ __forceinline__ float footprint_of(const sg_settings *s, float distan
     return distance * 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);
 }
 
-__device__ __noinline__ float3 forest_floor(float3 p, float footprint, float3 normal) {
+static __device__ __noinline__ float3 forest_floor(float3 p, float footprint, float3 normal) {
     const float broad = vnoise(add_rn(mul_rn(p, 0.045f), f3(7.0f, 0.0f, 13.0f)));
     const float middle = vnoise(p * 0.7f);
     const float grain = vnoise(p * 18.0f);
@@ -522,7 +522,7 @@ __device__ __noinline__ float3 forest_floor(float3 p, float footprint, float3 no
         mix3(f3(0.12f, 0.095f, 0.062f), f3(0.26f, 0.23f, 0.17f), grain * detail + 0.5f * (1.0f - detail));
     return mix3(color, gravel, path * 0.85f);
 }
-__device__ __noinline__ float3 desert_floor(float3 p, float footprint, float3 normal) {
+static __device__ __noinline__ float3 desert_floor(float3 p, float footprint, float3 normal) {
     const float broad = vnoise(add_rn(mul_rn(p, 0.007f), f3(19.0f, 2.0f, 4.0f)));
     const float gravel = vnoise(p * 2.8f);
     const float detail = 1.0f - smoothstepf(0.025f, 0.2f, footprint);
@@ -543,7 +543,7 @@ __device__ __noinline__ float3 desert_floor(float3 p, float footprint, float3 no
     color = mix3(color, sand * 0.93f, worn * fade * 0.35f);
     return mix3(color, packed, tracks * fade * 0.8f);
 }
-__device__ __noinline__ float3 crater_floor(float3 p, float footprint, float3 normal) {
+static __device__ __noinline__ float3 crater_floor(float3 p, float footprint, float3 normal) {
     const float broad = vnoise(add_rn(mul_rn(p, 0.004f), f3(3.0f, 0.0f, 8.0f)));
     const float middle = vnoise(p * 0.09f);
     const float grain = vnoise(p * 3.1f);
@@ -565,7 +565,7 @@ __device__ __forceinline__ uint32_t map_texel(const TraceParams *P, float3 p) {
 }
 
 // landscape_albedo (ground.wgsl:597-632), themes 0-2, plus the map.
-__device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
+static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
     const float3 n = to_ground(S, normal);
@@ -595,7 +595,7 @@ __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t, uint3
 }
 
 // landscape_shading_normal (ground.wgsl:633-648), themes 0-2.
-__device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
+static __device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     if (index != kLocalBase && index != kTerrainId) return normal;
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
@@ -608,7 +608,7 @@ __device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float 
 
 // landscape_outgoing in double (FP64 sites): the hit point, its reprojection
 // onto the host sphere and the 5 mm step, rounded to f32 AU at the end.
-__device__ __noinline__ Ray landscape_outgoing_fp64(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
+static __device__ __noinline__ Ray landscape_outgoing_fp64(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     d3 p = ground_origin_d(S, ray) + to_ground_d(S, D(ray.d)) * ((double)t * kMetresPerAuD);
     if (index == kLocalBase) {
         const double radius = (double)S.s->g.ground_up[3];

@@ -1,0 +1,466 @@
+// sg_wavefront.cu — the integrator in wavefront form.
+//
+// The per-pixel megakernel (sg_kernels.cu) keeps a whole path in registers
+// and walks it to the end, so a warp's lanes idle while the longest path of
+// the 32 finishes and every lane drags the code of every vertex kind
+// through the instruction cache. Here a dispatch's samples become paths in
+// a pool whose state lives in HBM (seven float4 planes per path, read and
+// written as 16-byte vectors, consecutive paths in consecutive slots), and
+// each iteration runs three small kernels over it:
+//
+//   extend    tops the pool up with new camera paths (16x16 pixel tiles,
+//             8x4 per warp, as the megakernel orders its lanes), then finds
+//             the closest hit, point disc and ring crossing of every live
+//             path; splits the paths into a ring queue and a surface queue
+//             and finishes those that escaped;
+//   ring      ring events (next-event estimation through the slab, null or
+//             scatter), for the ring queue only;
+//   surface   emitter hits and surface vertices (next-event estimation,
+//             ringshine, cosine bounce), for the surface queue only.
+//
+// The shade stages append surviving paths, compacted, to the other state
+// buffer. Queues are appended with one atomic per CTA and round (warp
+// ballots, then a CTA prefix), so the order within a CTA is the order of
+// its input. A new camera path is built in registers and stored only if it
+// survives its first extend. Finished paths write their radiance to a
+// per-(sample, pixel) slot; resolve sums each pixel's samples in sample
+// order and folds them into the compensated accumulation exactly as the
+// megakernel does. Both integrators run the same per-path functions
+// (sg_integrator.cuh) on the same random sequences; they differ only where
+// the compiler fuses a shading multiply-add in one kernel and not in the
+// other, a few ulps.
+#include <algorithm>
+
+#include "sg_integrator.cuh"
+
+namespace sg {
+
+namespace {
+
+#ifndef SG_WAVE_MIN_BLOCKS
+#define SG_WAVE_MIN_BLOCKS 4
+#endif
+
+// ---------------------------------------------------------------------------
+// Path state planes
+// ---------------------------------------------------------------------------
+//   0  ray.o, ray.anchor            4  ring_base, shine_body
+//   1  ray.d, rng                   5  previous_vertex.o, previous_vertex.anchor
+//   2  throughput, previous_pdf     6  iterations | point_gained << 31,
+//   3  radiance, ring_cap              depth | null_crossings << 16, result slot
+// The previous vertex is only ever used for its position (relative_center),
+// so its direction is not stored.
+__device__ __forceinline__ float4 pack3(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+__device__ __forceinline__ float4 pack3u(float3 v, uint32_t w) { return make_float4(v.x, v.y, v.z, __uint_as_float(w)); }
+__device__ __forceinline__ float3 xyz4(float4 v) { return f3(v.x, v.y, v.z); }
+
+__device__ __forceinline__ void store_path(float4 *st, uint32_t pool, uint32_t i, const Path &p, uint32_t slot) {
+    st[0 * pool + i] = pack3u(p.ray.o, p.ray.anchor);
+    st[1 * pool + i] = pack3u(p.ray.d, p.rng);
+    st[2 * pool + i] = pack3(p.throughput, p.previous_pdf);
+    st[3 * pool + i] = pack3(p.radiance, p.ring_cap);
+    st[4 * pool + i] = pack3u(p.ring_base, p.shine_body);
+    st[5 * pool + i] = pack3u(p.previous_vertex.o, p.previous_vertex.anchor);
+    st[6 * pool + i] = make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
+                                   __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(slot), 0.0f);
+}
+
+// Planes 0, 1 and 6: what extend reads. Returns the result slot.
+__device__ __forceinline__ uint32_t load_ray_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
+    const float4 a = st[0 * pool + i], b = st[1 * pool + i], g = st[6 * pool + i];
+    p.ray = Ray{xyz4(a), xyz4(b), __float_as_uint(a.w)};
+    p.rng = __float_as_uint(b.w);
+    const uint32_t it = __float_as_uint(g.x), dn = __float_as_uint(g.y);
+    p.iterations = it & 0x7fffffffu;
+    p.point_gained = (it >> 31) != 0u;
+    p.depth = dn & 0xffffu;
+    p.null_crossings = dn >> 16;
+    return __float_as_uint(g.z);
+}
+
+// Planes 3 and 4: radiance and the ring cap (what finish_path reads) and
+// the ringshine body.
+__device__ __forceinline__ void load_radiance_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
+    const float4 c = st[3 * pool + i], d = st[4 * pool + i];
+    p.radiance = xyz4(c);
+    p.ring_cap = c.w;
+    p.ring_base = xyz4(d);
+    p.shine_body = __float_as_uint(d.w);
+}
+
+// Planes 2 and 5: the rest of the state the shade stages need.
+__device__ __forceinline__ void load_shade_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
+    const float4 c = st[2 * pool + i], e = st[5 * pool + i];
+    p.throughput = xyz4(c);
+    p.previous_pdf = c.w;
+    p.previous_vertex = Ray{xyz4(e), f3(0.0f, 0.0f, 0.0f), __float_as_uint(e.w)};
+}
+
+// ---------------------------------------------------------------------------
+// CTA-aggregated queue appends
+// ---------------------------------------------------------------------------
+// Each thread of the CTA passes `flag[q]` for Q queues; the thread gets its
+// slot in each queue where its flag is set. One atomicAdd per queue and
+// CTA; every thread of the CTA must call it. Consecutive calls alternate
+// between two scratch blocks, so a call never overwrites counts that a
+// slower warp of the previous call has yet to read.
+template <int Q>
+struct Append {
+    uint32_t warp_counts[Q][kThreads / 32];
+    uint32_t base[Q];
+};
+
+template <int Q>
+__device__ __forceinline__ void block_append(Append<Q> &sm, const bool (&flag)[Q], uint32_t *const (&counter)[Q],
+                                             uint32_t (&slot)[Q]) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t ballot[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        ballot[q] = __ballot_sync(0xffffffffu, flag[q]);
+        if (lane == 0) sm.warp_counts[q][warp] = __popc(ballot[q]);
+    }
+    __syncthreads();
+    if (threadIdx.x < Q) {
+        const int q = threadIdx.x;
+        uint32_t total = 0;
+        for (uint32_t w = 0; w < kThreads / 32; ++w) {
+            const uint32_t c = sm.warp_counts[q][w];
+            sm.warp_counts[q][w] = total;  // exclusive prefix
+            total += c;
+        }
+        sm.base[q] = total ? atomicAdd(counter[q], total) : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) slot[q] = sm.base[q] + sm.warp_counts[q][warp] + __popc(ballot[q] & below);
+}
+
+__device__ __forceinline__ WaveCounters *counters(const WaveParams &W, uint32_t t) {
+    return W.counters + (t % kWaveCounterSets);
+}
+
+// Samples of a chunk are numbered sample-major over the padded tile grid.
+__device__ __forceinline__ uint32_t padded_pixels(const WaveParams &W) { return W.tiles_x * W.tiles_y * 256u; }
+
+// ---------------------------------------------------------------------------
+// Stages
+// ---------------------------------------------------------------------------
+template <bool L, bool F>
+__global__ void __launch_bounds__(kThreads, SG_WAVE_MIN_BLOCKS) wave_extend(const __grid_constant__ TraceParams P,
+                                                                            const __grid_constant__ WaveParams W,
+                                                                            uint32_t t) {
+    extern __shared__ float4 smem[];
+    __shared__ Append<2> sm[2];
+    WaveCounters *c = counters(W, t);
+    // Paths the previous iteration kept occupy [0, kept); new samples of the
+    // chunk fill the pool up to n.
+    const uint32_t kept = c->cont, next = c->next;
+    const uint32_t per_sample = padded_pixels(W);
+    const uint32_t take = min(W.pool - kept, per_sample * W.chunk_samples - next);
+    const uint32_t n = kept + take;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters(W, t + 1u)->next = next + take;
+        *counters(W, t + 2u) = WaveCounters{};
+    }
+    if (blockIdx.x * kThreads >= n) return;
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    NoGrad nograd;
+    float4 *st = W.state[t & 1u];
+    float4 *H = W.hits;
+    uint32_t round = 0;
+    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
+        const uint32_t i = base + threadIdx.x;
+        bool ring = false, surface = false;
+        if (i < n) {
+            Path p;
+            uint32_t slot = 0;
+            const bool fresh = i >= kept;
+            bool valid = true;
+            if (fresh) {
+                // Sample k of the chunk, numbered sample-major over the
+                // padded tile grid; padding pixels are skipped.
+                const uint32_t k = next + (i - kept);
+                const uint32_t smp = k / per_sample;
+                const uint32_t q = k - smp * per_sample;
+                const uint32_t tile = q >> 8, within = q & 255u;
+                const uint32_t warp = within >> 5, lane = within & 31u;
+                const uint32_t x = (tile % W.tiles_x) * kTile + (warp & 1u) * 8u + (lane & 7u);
+                const uint32_t y = (tile / W.tiles_x) * kTile + (warp >> 1) * 4u + (lane >> 3);
+                valid = x < P.width && y < P.height;
+                if (valid) {
+                    const uint32_t pixel = y * P.width + x;
+                    start_path(p, &P.s, K, pixel, x, y, W.chunk_first + smp);
+                    slot = smp * P.width * P.height + pixel;
+                }
+            } else {
+                slot = load_ray_part(st, W.pool, i, p);
+            }
+            if (valid) {
+                Extension e;
+                const bool alive = extend(S, K, p, nograd, e);
+                ring = alive && e.ring.index != kMiss;
+                surface = alive && !ring && e.hit.index != kMiss;
+                if (ring || surface) {
+                    if (fresh) {
+                        store_path(st, W.pool, i, p, slot);
+                    } else {
+                        st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
+                        st[6 * W.pool + i] = make_float4(
+                            __uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
+                            __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(slot), 0.0f);
+                    }
+                    if (ring) H[1 * W.pool + i] = pack3(e.ring.p, e.ring.t);
+                    else H[0 * W.pool + i] = pack3(e.hit.n, e.hit.t);
+                    H[2 * W.pool + i] = make_float4(__uint_as_float(e.hit.index), __uint_as_float(e.ring.index),
+                                                    e.hit.delta, e.disc_scale);
+                } else {
+                    // Ended at the iteration bound, or escaped: the
+                    // environment contributes nothing (surface_vertex's
+                    // miss). A new path's radiance is still zero.
+                    if (!fresh) load_radiance_part(st, W.pool, i, p);
+                    W.results[slot] = finish_path(p);
+                }
+            }
+        }
+        const bool flags[2] = {ring, surface};
+        uint32_t *const ctr[2] = {&c->ring, &c->surface};
+        uint32_t q[2];
+        block_append<2>(sm[round & 1u], flags, ctr, q);
+        if (ring) W.ring_queue[q[0]] = i;
+        if (surface) W.surface_queue[q[1]] = i;
+    }
+}
+
+// Ring (R == true) or surface stage over its queue.
+template <bool L, bool F, bool R>
+__global__ void __launch_bounds__(kThreads, SG_WAVE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
+                                                                           const __grid_constant__ WaveParams W,
+                                                                           uint32_t t) {
+    extern __shared__ float4 smem[];
+    __shared__ Append<1> sm[2];
+    WaveCounters *c = counters(W, t);
+    const uint32_t n = R ? c->ring : c->surface;
+    if (blockIdx.x * kThreads >= n) return;
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    NoGrad nograd;
+    const float4 *st = W.state[t & 1u];
+    float4 *out = W.state[(t + 1u) & 1u];
+    const float4 *H = W.hits;
+    const uint32_t *queue = R ? W.ring_queue : W.surface_queue;
+    uint32_t round = 0;
+    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
+        const uint32_t j = base + threadIdx.x;
+        bool keep = false;
+        Path p;
+        uint32_t slot = 0;
+        if (j < n) {
+            const uint32_t i = queue[j];
+            slot = load_ray_part(st, W.pool, i, p);
+            load_radiance_part(st, W.pool, i, p);
+            load_shade_part(st, W.pool, i, p);
+            const float4 h2 = H[2 * W.pool + i];
+            bool ended;
+            if constexpr (R) {
+                const float4 h1 = H[1 * W.pool + i];
+                const RingHit ring{h1.w, __float_as_uint(h2.y), xyz4(h1)};
+                ended = ring_vertex(S, K, p, ring, nograd);
+            } else {
+                const float4 h0 = H[0 * W.pool + i];
+                const Hit hit{h0.w, __float_as_uint(h2.x), h2.z, xyz4(h0)};
+                ended = surface_vertex(S, K, p, hit, h2.w, nograd);
+            }
+            keep = !ended;
+            if (ended) W.results[slot] = finish_path(p);
+        }
+        const bool flags[1] = {keep};
+        uint32_t *const ctr[1] = {&counters(W, t + 1u)->cont};
+        uint32_t q[1];
+        block_append<1>(sm[round & 1u], flags, ctr, q);
+        if (keep) store_path(out, W.pool, q[0], p, slot);
+    }
+}
+
+// Per pixel: the chunk's samples summed in sample order onto the running
+// total, and on the last chunk the megakernel's compensated fold.
+__global__ void __launch_bounds__(kThreads) wave_resolve(const __grid_constant__ TraceParams P,
+                                                         const __grid_constant__ WaveParams W, int first, int last) {
+    const uint32_t pixels = P.width * P.height;
+    const uint32_t pixel = blockIdx.x * kThreads + threadIdx.x;
+    if (pixel >= pixels) return;
+    float4 total = first ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : W.totals[pixel];
+    for (uint32_t smp = 0; smp < W.chunk_samples; ++smp) {
+        const float4 r = W.results[(size_t)smp * pixels + pixel];
+        total.x += r.x;
+        total.y += r.y;
+        total.z += r.z;
+        total.w += r.w;
+    }
+    if (!last) {
+        W.totals[pixel] = total;
+        return;
+    }
+    const uint32_t old_count = P.s.counts[1];
+    const float new_count = (float)(old_count + P.s.counts[2]);
+    float4 sum, comp;
+    if (old_count == 0u) {
+        sum = total;
+        comp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+        sum = P.sum[pixel];
+        comp = P.comp[pixel];
+        float yv, tt;
+        yv = __fsub_rn(total.x, comp.x); tt = __fadd_rn(sum.x, yv); comp.x = __fsub_rn(__fsub_rn(tt, sum.x), yv); sum.x = tt;
+        yv = __fsub_rn(total.y, comp.y); tt = __fadd_rn(sum.y, yv); comp.y = __fsub_rn(__fsub_rn(tt, sum.y), yv); sum.y = tt;
+        yv = __fsub_rn(total.z, comp.z); tt = __fadd_rn(sum.z, yv); comp.z = __fsub_rn(__fsub_rn(tt, sum.z), yv); sum.z = tt;
+        yv = __fsub_rn(total.w, comp.w); tt = __fadd_rn(sum.w, yv); comp.w = __fsub_rn(__fsub_rn(tt, sum.w), yv); sum.w = tt;
+    }
+    P.sum[pixel] = sum;
+    P.comp[pixel] = comp;
+    P.mean[pixel] = make_float4(__fdiv_rn(__fsub_rn(sum.x, comp.x), new_count),
+                                __fdiv_rn(__fsub_rn(sum.y, comp.y), new_count),
+                                __fdiv_rn(__fsub_rn(sum.z, comp.z), new_count),
+                                __fdiv_rn(__fsub_rn(sum.w, comp.w), new_count));
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct StageSet {
+    const void *extend, *ring, *surface;
+};
+
+template <bool L, bool F>
+StageSet stage_set() {
+    return StageSet{(const void *)wave_extend<L, F>, (const void *)wave_shade<L, F, true>,
+                    (const void *)wave_shade<L, F, false>};
+}
+
+cudaError_t persistent_grid(const void *fn, size_t smem, int *grid) {
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    *grid = sms * (per_sm > 0 ? per_sm : 1);
+    return cudaSuccess;
+}
+
+cudaError_t mark(StageMarks *m, int stage, cudaStream_t stream) {
+    if (!m) return cudaSuccess;
+    if (m->used == m->events.size()) {
+        cudaEvent_t e;
+        cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        m->events.push_back(e);
+        m->stage.push_back(kStageGap);
+    }
+    m->stage[m->used] = stage;
+    return cudaEventRecord(m->events[m->used++], stream);
+}
+
+template <bool L, bool F>
+cudaError_t run_iteration(const TraceParams &p, const WaveParams &w, uint32_t t, const int (&grid)[3], size_t smem,
+                          cudaStream_t stream, StageMarks *m) {
+    cudaError_t e;
+    if ((e = mark(m, kStageExtend, stream)) != cudaSuccess) return e;
+    wave_extend<L, F><<<grid[0], kThreads, smem, stream>>>(p, w, t);
+    if ((e = mark(m, kStageRing, stream)) != cudaSuccess) return e;
+    wave_shade<L, F, true><<<grid[1], kThreads, smem, stream>>>(p, w, t);
+    if ((e = mark(m, kStageSurface, stream)) != cudaSuccess) return e;
+    wave_shade<L, F, false><<<grid[2], kThreads, smem, stream>>>(p, w, t);
+    if ((e = mark(m, kStageGap, stream)) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t wave_state_bytes(uint32_t pool) {
+    return (size_t)pool * sizeof(float4) * (2 * kWavePlanes + kWaveHitPlanes) + (size_t)pool * 2 * sizeof(uint32_t) +
+           kWaveCounterSets * sizeof(WaveCounters);
+}
+
+size_t wave_result_bytes(uint32_t pixels, uint32_t chunk_samples) {
+    return (size_t)pixels * sizeof(float4) * ((size_t)chunk_samples + 1u);
+}
+
+cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *pinned, cudaEvent_t ready,
+                             cudaStream_t stream, WaveRun *run, StageMarks *marks) {
+    const uint32_t z = p.s.counts[2];
+    const uint32_t pixels = p.width * p.height;
+    *run = WaveRun{};
+    if (marks) marks->used = 0;
+    if (z == 0 || pixels == 0) return cudaSuccess;
+    const bool land = p.s.g.ground_north[3] != 0.0f;
+    const StageSet set = land ? (p.fp64_sites ? stage_set<true, true>() : stage_set<true, false>())
+                              : (p.fp64_sites ? stage_set<false, true>() : stage_set<false, false>());
+    const size_t smem = trace_smem_bytes(p);
+    const void *fns[3] = {set.extend, set.ring, set.surface};
+    int grid[3];
+    for (int k = 0; k < 3; ++k) {
+        const size_t bytes = smem;
+        if (bytes > 48u * 1024u) {
+            cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = persistent_grid(fns[k], bytes, &grid[k]);
+        if (e != cudaSuccess) return e;
+    }
+    w.tiles_x = (p.width + kTile - 1) / kTile;
+    w.tiles_y = (p.height + kTile - 1) / kTile;
+    const uint32_t chunk = w.chunk_samples;
+    const uint32_t per_sample = w.tiles_x * w.tiles_y * 256u;
+    // A path ends within max_vertices * (bodies + 2) + 1 iterations, and an
+    // iteration that takes no new sample has a full pool of paths that all
+    // advance, so a chunk drains within (samples + 1) * (that + 1)
+    // iterations: a host-side guard, the loop below never waits on the GPU
+    // for longer than one group of iterations.
+    const uint64_t cap = (uint64_t)p.s.counts[3] * (p.s.counts[0] + 2u) + 2u;
+    for (uint32_t first = 0; first < z; first += chunk) {
+        w.chunk_first = first;
+        w.chunk_samples = std::min(chunk, z - first);
+        const uint32_t samples = per_sample * w.chunk_samples;
+        const uint64_t bound = ((uint64_t)samples + 1u) * cap;
+        cudaError_t e = cudaMemsetAsync(w.counters, 0, kWaveCounterSets * sizeof(WaveCounters), stream);
+        if (e != cudaSuccess) return e;
+        // Every iteration takes at most `pool` new samples, so the chunk
+        // cannot drain before all samples could have been taken; after a
+        // check the same bound gives the next one, and once every sample is
+        // out the check runs every kTailCheck iterations.
+        constexpr uint64_t kTailCheck = 2;
+        uint64_t check_at = (samples + (uint64_t)w.pool - 1u) / w.pool;
+        for (uint64_t t = 0;; ++t) {
+            if (t >= bound) return cudaErrorLaunchTimeout;
+            const uint32_t it = (uint32_t)t;
+            e = land ? (p.fp64_sites ? run_iteration<true, true>(p, w, it, grid, smem, stream, marks)
+                                     : run_iteration<true, false>(p, w, it, grid, smem, stream, marks))
+                     : (p.fp64_sites ? run_iteration<false, true>(p, w, it, grid, smem, stream, marks)
+                                     : run_iteration<false, false>(p, w, it, grid, smem, stream, marks));
+            if (e != cudaSuccess) return e;
+            run->iterations += 1;
+            run->kernels += 3;
+            if (t + 1 < check_at) continue;
+            const WaveCounters *dev = w.counters + ((t + 1) % kWaveCounterSets);
+            if ((e = cudaMemcpyAsync(pinned, dev, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream)) !=
+                    cudaSuccess ||
+                (e = cudaEventRecord(ready, stream)) != cudaSuccess || (e = cudaEventSynchronize(ready)) != cudaSuccess)
+                return e;
+            if (pinned->cont == 0 && pinned->next >= samples) break;
+            const uint64_t left = pinned->next >= samples ? 0u : samples - pinned->next;
+            check_at = t + 1 + (left ? (left + w.pool - 1u) / w.pool : kTailCheck);
+        }
+        const bool first_chunk = first == 0, last_chunk = first + w.chunk_samples >= z;
+        if ((e = mark(marks, kStageResolve, stream)) != cudaSuccess) return e;
+        wave_resolve<<<(pixels + kThreads - 1) / kThreads, kThreads, 0, stream>>>(p, w, first_chunk, last_chunk);
+        if ((e = mark(marks, kStageGap, stream)) != cudaSuccess) return e;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        run->kernels += 1;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace sg

@@ -114,6 +114,36 @@ class PathTracer:
         FP64 (extension; off: the reference's f32 arithmetic)."""
         check(self._lib.sg_set_fp64_sites(self._ctx, int(bool(enable))), self._ctx)
 
+    def set_integrator(self, integrator: str, pool_paths: int = 0) -> None:
+        """"wavefront" (default; stage kernels over a pool of `pool_paths`
+        paths in device memory, 0 = default pool) or "megakernel" (one
+        thread per pixel); both run the same per-path code and agree to a
+        few ulps (extension: the reference has one compute pass)."""
+        kinds = {"megakernel": abi.INTEGRATOR_MEGAKERNEL, "wavefront": abi.INTEGRATOR_WAVEFRONT}
+        if integrator not in kinds:
+            raise ValueError(f"unknown integrator {integrator!r}")
+        check(self._lib.sg_set_integrator(self._ctx, kinds[integrator], int(pool_paths)), self._ctx)
+
+    def integrator(self) -> dict:
+        """The integrator in use, the wavefront pool of the last dispatch and
+        the stage iterations it ran."""
+        kind, pool, iterations = C.c_int(), C.c_uint32(), C.c_uint32()
+        check(self._lib.sg_get_integrator(self._ctx, C.byref(kind), C.byref(pool), C.byref(iterations)), self._ctx)
+        name = "wavefront" if kind.value == abi.INTEGRATOR_WAVEFRONT else "megakernel"
+        return {"integrator": name, "pool_paths": pool.value, "iterations": iterations.value}
+
+    STAGES = ("extend", "ring", "surface", "resolve", "gaps")
+
+    def set_stage_timing(self, enable: bool) -> None:
+        """Bracket every wavefront stage with CUDA events (measurement)."""
+        check(self._lib.sg_set_stage_timing(self._ctx, int(bool(enable))), self._ctx)
+
+    def stage_times(self) -> dict:
+        """Milliseconds per wavefront stage of the last timed dispatch."""
+        ms = (C.c_float * len(self.STAGES))()
+        check(self._lib.sg_get_stage_times(self._ctx, ms), self._ctx)
+        return dict(zip(self.STAGES, (float(v) for v in ms)))
+
     def set_quality(self, samples: int, bounces: int, limit: int) -> None:
         check(self._lib.sg_set_quality(self._ctx, samples, bounces, limit), self._ctx)
 

@@ -72,11 +72,13 @@ def test_ring_probe_matches_oracle(name):
             assert np.all(np.abs(out[hit, 2] - trans) <= tol * np.maximum(trans, 1e-38))
 
 
+@pytest.mark.parametrize("integrator", ["megakernel", "wavefront"])
 @pytest.mark.parametrize("name", gio.IMAGE_NAMES)
-def test_images_match_oracle_with_common_random_numbers(name):
+def test_images_match_oracle_with_common_random_numbers(name, integrator):
     _factory, w, h, spp, batches = IMAGES[name]
     wl, land = image_workload(name)
     t = cuda_tracer(wl.ring_tables, (w, h), land=land, samples_per_frame=spp, max_bounces=wl.max_bounces)
+    t.set_integrator(integrator)
     for _ in range(batches):
         t.encode(wl.frame)
     img = t.read_pixels()
