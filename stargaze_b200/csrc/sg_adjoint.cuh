@@ -109,6 +109,18 @@ struct Roulette {
     float3 before;  // radiance gathered since the cap vertex, before it
 };
 
+// The lists a path's adjoint appends to: Russian-roulette events after the
+// cap vertex (with pass 2's coefficient of each) and pass 1's deferred
+// throughput factors with the running sum at each. The per-pixel adjoint
+// keeps them in the thread's local memory, the staged adjoint in a device
+// slot that stays with the path across stages.
+struct PrbLists {
+    Roulette rr[kMaxRoulette];
+    float rr_coef[kMaxRoulette];
+    GradEntry fac[kMaxDeferred];
+    float3 fac_at[kMaxDeferred];
+};
+
 // The adjoint's state. Both passes run the same integrator code (one
 // instantiation, so a warp's instruction footprint is that of one replay);
 // pass 1 also records the summary pass 2 needs (`pass2` false).
@@ -133,15 +145,12 @@ struct Prb {
     uint32_t prev_param;      // tau parameter of the last ring scatter
     float prev_dlog_pdf;      // ... and d log of its scatter pdf
     uint32_t n_rr;
-    Roulette rr[kMaxRoulette];
-    float rr_coef[kMaxRoulette];
     GradEntry local[kMaxLocal];
     uint32_t n_local, dropped;
-    // Pass 1's deferred throughput factors and the running sum at each.
-    GradEntry fac[kMaxDeferred];
-    float3 fac_at[kMaxDeferred];
+    // Pass 1's deferred throughput factors (count), and where the lists live.
     uint32_t n_fac;
     bool deferral_full;
+    PrbLists *lists;
 
     __device__ __forceinline__ bool post() const { return capture_iter != 0u && iteration > capture_iter; }
     __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
@@ -220,8 +229,8 @@ static __device__ __noinline__ void factor(Prb &G, GradEntry e) {
     if (!G.pass2) {
         // Pass 1: defer until the path's end.
         if (G.n_fac < (uint32_t)kMaxDeferred) {
-            G.fac[G.n_fac] = e;
-            G.fac_at[G.n_fac] = G.a;
+            G.lists->fac[G.n_fac] = e;
+            G.lists->fac_at[G.n_fac] = G.a;
             G.n_fac += 1u;
         } else {
             G.deferral_full = true;
@@ -240,10 +249,10 @@ static __device__ __noinline__ void factor(Prb &G, GradEntry e) {
         int prev = -1;
 #pragma unroll 1
         for (uint32_t r = 0; r < G.n_rr; ++r) {
-            const Roulette ev = G.rr[r];
+            const Roulette ev = G.lists->rr[r];
             if (ev.iteration < G.iteration || (ev.bits & 8u)) continue;
             const uint32_t m = ev.bits & 3u;
-            const float c = G.rr_coef[r];
+            const float c = G.lists->rr_coef[r];
             if (vec) {
                 const float dm = c * channel(e.dlog, m);
                 add = f3(add.x + (m == 0u ? dm : 0.0f), add.y + (m == 1u ? dm : 0.0f), add.z + (m == 2u ? dm : 0.0f));
@@ -548,7 +557,7 @@ static __device__ __noinline__ void record_roulette(Prb &G, uint32_t iteration, 
     const float mx = fmaxf(t.x, fmaxf(t.y, t.z));
     const uint32_t m = t.x >= mx ? 0u : (t.y >= mx ? 1u : 2u);
     const bool clamped = !(mx > 0.05f && mx < 0.95f);
-    G.rr[G.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - G.base};
+    G.lists->rr[G.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - G.base};
 }
 
 // Start of pass 1 for a pixel weight w.
@@ -584,8 +593,8 @@ __device__ __forceinline__ bool cap_binds(const Prb &G, float3 total) {
 static __device__ __noinline__ void flush_deferred(Prb &G) {
 #pragma unroll 1
     for (uint32_t k = 0; k < G.n_fac; ++k) {
-        const GradEntry e = G.fac[k];
-        const float3 rem = G.a - G.fac_at[k];
+        const GradEntry e = G.lists->fac[k];
+        const float3 rem = G.a - G.lists->fac_at[k];
         if (e.param & kVectorBit) {
             const uint32_t base = e.param & ~kVectorBit;
             G.sink.add(base + 0u, rem.x * e.dlog.x);
@@ -632,9 +641,9 @@ static __device__ __noinline__ void pass2_setup(Prb &G, float3 total, float3 w) 
         G.score = (s - 1.0f) * dot(w, indirect);
         G.b_total = mul3(G.w_pdf, indirect);
         for (uint32_t r = 0; r < G.n_rr && r < (uint32_t)kMaxRoulette; ++r) {
-            const Roulette ev = G.rr[r];
+            const Roulette ev = G.lists->rr[r];
             const bool survived = (ev.bits & 4u) != 0u;
-            G.rr_coef[r] = survived ? G.score - dot(G.w_pdf, indirect - ev.before)
+            G.lists->rr_coef[r] = survived ? G.score - dot(G.w_pdf, indirect - ev.before)
                                     : -G.score * ev.s / (1.0f - ev.s);
         }
     } else {

@@ -86,6 +86,8 @@ struct sg_context {
     size_t wave_state_size = 0;
     uint32_t wave_pool = 0;
     float4 *wave_results = nullptr;         // per-sample radiance + running totals
+    void *adjoint_slots = nullptr;          // staged adjoint: slot state, lists, free ring
+    size_t adjoint_slots_size = 0;
     size_t wave_results_size = 0;
     sg::WaveCounters *wave_pinned = nullptr;
     cudaEvent_t wave_ready = nullptr;
@@ -472,6 +474,7 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->dropped);
     cudaFree(ctx->wave_state);
     cudaFree(ctx->wave_results);
+    cudaFree(ctx->adjoint_slots);
     if (ctx->wave_pinned) cudaFreeHost(ctx->wave_pinned);
     if (ctx->wave_ready) cudaEventDestroy(ctx->wave_ready);
     for (cudaEvent_t e : ctx->stage_marks.events) cudaEventDestroy(e);
@@ -588,13 +591,22 @@ constexpr uint32_t kDefaultWavePool = 1u << 24;
 // a 1080p dispatch of 64 samples fits in one chunk.
 constexpr size_t kWaveResultBudget = (size_t)9 << 28;
 
-// Sizes the wavefront buffers for a dispatch of `samples` samples and
-// fills `w`; the state buffer grows only, the result buffer likewise.
-static int ensure_wave(sg_context *ctx, uint32_t samples, sg::WaveParams &w) {
+// Default pool of the staged adjoint: 4 Mi paths (about 1.1 KB each with
+// the adjoint slot).
+constexpr uint32_t kDefaultAdjointPool = 1u << 22;
+
+// The pool for `samples` samples per pixel: the request (or `fallback`),
+// at most the padded sample count, a multiple of 256.
+static uint32_t wave_pool_for(const sg_context *ctx, uint32_t samples, uint32_t fallback) {
     const uint32_t tiles = ((ctx->width + 15u) / 16u) * ((ctx->height + 15u) / 16u);
     const uint64_t work = (uint64_t)tiles * 256u * samples;
-    const uint32_t want = ctx->wave_pool_request ? ctx->wave_pool_request : kDefaultWavePool;
-    const uint32_t pool = (uint32_t)std::min<uint64_t>(want, (work + 255u) & ~(uint64_t)255u);
+    const uint32_t want = ctx->wave_pool_request ? ctx->wave_pool_request : fallback;
+    return (uint32_t)std::min<uint64_t>(want, (work + 255u) & ~(uint64_t)255u);
+}
+
+// Path state planes, extend results, queues and counters for `pool` paths
+// (the buffer grows only; forward and backward share it).
+static int ensure_wave_state(sg_context *ctx, uint32_t pool, sg::WaveParams &w) {
     const size_t state_bytes = sg::wave_state_bytes(pool);
     if (state_bytes > ctx->wave_state_size) {
         cudaFree(ctx->wave_state);
@@ -603,6 +615,27 @@ static int ensure_wave(sg_context *ctx, uint32_t samples, sg::WaveParams &w) {
         SG_CUDA(ctx, cudaMalloc(&ctx->wave_state, state_bytes));
         ctx->wave_state_size = state_bytes;
     }
+    if (!ctx->wave_pinned) SG_CUDA(ctx, cudaMallocHost(&ctx->wave_pinned, sizeof(sg::WaveCounters)));
+    if (!ctx->wave_ready) SG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->wave_ready, cudaEventDisableTiming));
+    float4 *base = ctx->wave_state;
+    w.state[0] = base;
+    w.state[1] = base + (size_t)sg::kWavePlanes * pool;
+    w.hits = base + (size_t)2 * sg::kWavePlanes * pool;
+    w.ring_queue = reinterpret_cast<uint32_t *>(w.hits + (size_t)sg::kWaveHitPlanes * pool);
+    w.surface_queue = w.ring_queue + pool;
+    w.counters = reinterpret_cast<sg::WaveCounters *>(w.surface_queue + pool);
+    w.pool = pool;
+    w.tiles_x = w.tiles_y = 0;
+    w.chunk_first = 0;
+    return SG_OK;
+}
+
+// Sizes the wavefront buffers for a dispatch of `samples` samples and
+// fills `w`; the state buffer grows only, the result buffer likewise.
+static int ensure_wave(sg_context *ctx, uint32_t samples, sg::WaveParams &w) {
+    const uint32_t pool = wave_pool_for(ctx, samples, kDefaultWavePool);
+    int status = ensure_wave_state(ctx, pool, w);
+    if (status != SG_OK) return status;
     ctx->wave_pool = pool;
     const uint32_t pixels = ctx->width * ctx->height;
     const size_t per_sample = (size_t)pixels * sizeof(float4);
@@ -615,21 +648,31 @@ static int ensure_wave(sg_context *ctx, uint32_t samples, sg::WaveParams &w) {
         SG_CUDA(ctx, cudaMalloc(&ctx->wave_results, result_bytes));
         ctx->wave_results_size = result_bytes;
     }
-    if (!ctx->wave_pinned) SG_CUDA(ctx, cudaMallocHost(&ctx->wave_pinned, sizeof(sg::WaveCounters)));
-    if (!ctx->wave_ready) SG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->wave_ready, cudaEventDisableTiming));
-    float4 *base = ctx->wave_state;
-    w.state[0] = base;
-    w.state[1] = base + (size_t)sg::kWavePlanes * pool;
-    w.hits = base + (size_t)2 * sg::kWavePlanes * pool;
-    w.ring_queue = reinterpret_cast<uint32_t *>(w.hits + (size_t)sg::kWaveHitPlanes * pool);
-    w.surface_queue = w.ring_queue + pool;
-    w.counters = reinterpret_cast<sg::WaveCounters *>(w.surface_queue + pool);
     w.results = ctx->wave_results;
     w.totals = ctx->wave_results + (size_t)chunk * pixels;
-    w.pool = pool;
-    w.tiles_x = w.tiles_y = 0;
-    w.chunk_first = 0;
     w.chunk_samples = chunk;
+    return SG_OK;
+}
+
+// Buffers of the staged adjoint for batches of up to `samples` samples.
+static int ensure_adjoint(sg_context *ctx, uint32_t samples, sg::WaveParams &w, sg::AdjointWave &x) {
+    const uint32_t pool = wave_pool_for(ctx, samples, kDefaultAdjointPool);
+    int status = ensure_wave_state(ctx, pool, w);
+    if (status != SG_OK) return status;
+    const size_t bytes = sg::adjoint_slot_bytes(pool);
+    if (bytes > ctx->adjoint_slots_size) {
+        cudaFree(ctx->adjoint_slots);
+        ctx->adjoint_slots = nullptr;
+        ctx->adjoint_slots_size = 0;
+        SG_CUDA(ctx, cudaMalloc(&ctx->adjoint_slots, bytes));
+        ctx->adjoint_slots_size = bytes;
+    }
+    char *base = static_cast<char *>(ctx->adjoint_slots);
+    x.side = reinterpret_cast<float4 *>(base);
+    x.lists = base + (size_t)pool * sg::kAdjointSideVec4 * sizeof(float4);
+    x.free_ring = reinterpret_cast<uint32_t *>(base + sg::adjoint_slot_bytes(pool) - (size_t)pool * sizeof(uint32_t) -
+                                               4 * sizeof(uint32_t));
+    x.free_ends = x.free_ring + pool;
     return SG_OK;
 }
 
@@ -1088,14 +1131,36 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         if (ctx->ring_bins[k]) tau_used = k * SG_RING_TABLE_MAX_BINS + ctx->ring_bins[k];
     a.tau_window = tau_used <= 8192u ? tau_used : 0u;
     a.color_window = 6u * frame->n_bodies;
+    const bool staged = ctx->integrator == SG_INTEGRATOR_WAVEFRONT;
+    sg::WaveParams w{};
+    sg::AdjointWave x{};
+    if (staged) {
+        uint32_t largest = 0;
+        for (uint32_t k = 0; k < tape->n_ranges; ++k)
+            largest = std::max(largest, std::min<uint32_t>(SG_MAX_BATCH_SAMPLES, tape->count[k]));
+        status = ensure_adjoint(ctx, largest, w, x);
+        if (status != SG_OK) return status;
+        cudaError_t e = sg::reset_adjoint_slots(x, w.pool, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint slot reset");
+    }
     for (uint32_t k = 0; k < tape->n_ranges; ++k) {
         for (uint32_t done = 0; done < tape->count[k]; done += SG_MAX_BATCH_SAMPLES) {
             s.sampling[0] = tape->first[k] + done;
             s.counts[2] = std::min<uint32_t>(SG_MAX_BATCH_SAMPLES, tape->count[k] - done);
             const sg::TraceParams p = make_params(ctx, s);
-            cudaError_t e = sg::launch_adjoint(p, a, stream);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
-            ctx->launches += 1;
+            if (staged) {
+                sg::WaveRun run;
+                cudaError_t e =
+                    sg::launch_adjoint_wavefront(p, a, w, x, ctx->wave_pinned, ctx->wave_ready, stream, &run);
+                ctx->launches += run.kernels;
+                if (e == cudaErrorLaunchTimeout)
+                    return fail(ctx, SG_ERR_TIMEOUT, "staged adjoint did not drain within its iteration bound");
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "staged adjoint");
+            } else {
+                cudaError_t e = sg::launch_adjoint(p, a, stream);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
+                ctx->launches += 1;
+            }
         }
     }
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

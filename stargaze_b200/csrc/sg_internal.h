@@ -157,4 +157,31 @@ size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a);
 // and accumulate the loss gradient into a.grad; the image is not touched.
 cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStream_t stream);
 
+// ---------------------------------------------------------------------------
+// Staged adjoint (sg_wave_adjoint.cu): the same replay in the wavefront's
+// extend / ring / surface stages. A path holds one adjoint slot (its
+// persistent derivative state and lists) from its first surviving extend
+// to its end; free slots circulate through a ring of slot ids.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kAdjointSideVec4 = 10;  // float4 words of one slot's state
+
+struct AdjointWave {
+    float4 *side;         // kAdjointSideVec4 float4 per slot
+    void *lists;          // one PrbLists per slot
+    uint32_t *free_ring;  // `pool` slot ids
+    uint32_t *free_ends;  // [0] next allocation, [1] next free position (monotonic)
+};
+
+// Bytes of the adjoint slots for `pool` paths.
+size_t adjoint_slot_bytes(uint32_t pool);
+
+// Puts every slot of `x` on the free ring; once per backward call.
+cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t pool, cudaStream_t stream);
+
+// The samples of `p` (as launch_adjoint) through the stages; returns once
+// they have drained (host checks as launch_wavefront).
+cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &a, WaveParams w,
+                                     const AdjointWave &x, WaveCounters *pinned, cudaEvent_t ready,
+                                     cudaStream_t stream, WaveRun *run);
+
 }  // namespace sg

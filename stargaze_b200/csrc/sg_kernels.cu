@@ -152,7 +152,9 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
 #pragma unroll
     for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
     const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
+    PrbLists lists;
     Prb G;
+    G.lists = &lists;
     G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
     G.inv = inv;
     G.dropped = 0;

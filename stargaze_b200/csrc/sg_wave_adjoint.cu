@@ -1,0 +1,478 @@
+// sg_wave_adjoint.cu — the path-replay adjoint in stages.
+//
+// The per-pixel adjoint (adjoint_kernel, sg_kernels.cu) replays each sample
+// in one thread with every derivative hook inlined into the integrator, and
+// is bound by instruction fetch as the forward megakernel was. Here the
+// replay runs through the wavefront's stages (sg_wavefront.cu): extend over
+// all live paths, ring_vertex over the ring queue, surface_vertex over the
+// surface queue, the hooks of sg_adjoint.cuh running inside each.
+//
+// Each path holds an adjoint slot from its first surviving extend to its
+// end: ten float4 of persistent state (running weighted sum, cap record,
+// flags, and pass 2's weights) plus its PrbLists (Russian-roulette records
+// after the cap vertex, deferred factors). Slots are taken from and given
+// back to a ring of free slot ids. At the end of pass 1 a path either
+// scatters its deferred factors and gives its slot back, or — when the
+// ring-indirect cap binds or its deferral list overflowed — sets up pass 2
+// in the same slot and restarts from its camera ray in the next iteration,
+// exactly the two replays of the per-pixel adjoint. Gradients land in the
+// same sinks: per-thread sums for the first bodies' colours, shared-memory
+// windows over the ring tables and colours, global atomics for the rest,
+// flushed at the end of every stage launch.
+#include <algorithm>
+
+#include "sg_wave_common.cuh"
+
+namespace sg {
+
+namespace {
+
+#ifndef SG_WAVE_ADJ_MIN_BLOCKS
+#define SG_WAVE_ADJ_MIN_BLOCKS 2
+#endif
+
+// Slot state (float4 words):
+//   0  a.xyz, cap                         5  w_pdf.xyz        (pass 2)
+//   1  base.xyz, capture_iter             6  w_cap.xyz        (pass 2)
+//   2  cap_light.xyz, flags               7  b.xyz            (pass 2)
+//   3  prev_param, prev_dlog_pdf,         8  a_total.xyz      (pass 2)
+//      score, sample index                9  b_total.xyz      (pass 2)
+//   4  w_post.xyz (pass 2)
+// flags: n_fac | n_rr << 8 | deferral_full, cap_direct, binding, pass 2.
+constexpr uint32_t kFlagDeferralFull = 1u << 16;
+constexpr uint32_t kFlagCapDirect = 1u << 17;
+constexpr uint32_t kFlagBinding = 1u << 18;
+constexpr uint32_t kFlagPass2 = 1u << 19;
+
+__device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, float3 w, Prb &G, uint32_t &smp) {
+    const float4 *q = X.side + (size_t)slot * kAdjointSideVec4;
+    const float4 s0 = q[0], s1 = q[1], s2 = q[2], s3 = q[3];
+    const uint32_t flags = __float_as_uint(s2.w);
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    G.pass2 = (flags & kFlagPass2) != 0u;
+    G.a = xyz4(s0);
+    G.cap = s0.w;
+    G.base = xyz4(s1);
+    G.capture_iter = __float_as_uint(s1.w);
+    G.cap_light = xyz4(s2);
+    G.n_fac = flags & 0xffu;
+    G.n_rr = (flags >> 8) & 0xffu;
+    G.deferral_full = (flags & kFlagDeferralFull) != 0u;
+    G.cap_direct = (flags & kFlagCapDirect) != 0u;
+    G.binding = (flags & kFlagBinding) != 0u;
+    G.prev_param = __float_as_uint(s3.x);
+    G.prev_dlog_pdf = s3.y;
+    G.score = s3.z;
+    smp = __float_as_uint(s3.w);
+    G.w_pre = w;
+    if (G.pass2) {
+        G.w_post = xyz4(q[4]);
+        G.w_pdf = xyz4(q[5]);
+        G.w_cap = xyz4(q[6]);
+        G.b = xyz4(q[7]);
+        G.a_total = xyz4(q[8]);
+        G.b_total = xyz4(q[9]);
+    } else {
+        G.w_post = w;
+        G.w_pdf = zero;
+        G.w_cap = zero;
+        G.b = zero;
+        G.a_total = zero;
+        G.b_total = zero;
+    }
+    G.lists = reinterpret_cast<PrbLists *>(X.lists) + slot;
+    G.n_local = 0;
+    G.dropped = 0;
+}
+
+__device__ __forceinline__ void store_prb(const AdjointWave &X, uint32_t slot, const Prb &G, uint32_t smp) {
+    float4 *q = X.side + (size_t)slot * kAdjointSideVec4;
+    const uint32_t flags = (G.n_fac & 0xffu) | ((G.n_rr & 0xffu) << 8) | (G.deferral_full ? kFlagDeferralFull : 0u) |
+                           (G.cap_direct ? kFlagCapDirect : 0u) | (G.binding ? kFlagBinding : 0u) |
+                           (G.pass2 ? kFlagPass2 : 0u);
+    q[0] = pack3(G.a, G.cap);
+    q[1] = pack3u(G.base, G.capture_iter);
+    q[2] = pack3u(G.cap_light, flags);
+    q[3] = make_float4(__uint_as_float(G.prev_param), G.prev_dlog_pdf, G.score, __uint_as_float(smp));
+    if (G.pass2) {
+        q[4] = pack3(G.w_post, 0.0f);
+        q[5] = pack3(G.w_pdf, 0.0f);
+        q[6] = pack3(G.w_cap, 0.0f);
+        q[7] = pack3(G.b, 0.0f);
+        q[8] = pack3(G.a_total, 0.0f);
+        q[9] = pack3(G.b_total, 0.0f);
+    }
+}
+
+// Pass 1's state of a new sample (pass1_setup) with the cap record cleared.
+__device__ __forceinline__ void fresh_prb(Prb &G, float3 w) {
+    pass1_setup(G, w);
+    G.cap = 0.0f;
+    G.base = f3(0.0f, 0.0f, 0.0f);
+    G.cap_light = f3(0.0f, 0.0f, 0.0f);
+    G.cap_direct = false;
+    G.dropped = 0;
+}
+
+// The pixel weight of the loss: d loss / d pixel over the samples behind it.
+__device__ __forceinline__ float3 pixel_weight(const AdjointParams &A, uint32_t pixel) {
+    const float4 d = A.dl_dimage[pixel];
+    return f3(d.x, d.y, d.z) * A.inv_samples;
+}
+
+// Per-block gradient sinks: shared-memory windows over the ring tables and
+// the body colours, per-thread sums for the first bodies' colours.
+struct BlockSink {
+    float4 *inv;
+    float *window;
+    uint32_t window_n;
+};
+
+__device__ __forceinline__ BlockSink open_sink(const TraceParams &P, const AdjointParams &A, float4 *smem) {
+    const uint32_t n_bodies = P.s.counts[0];
+    BlockSink b;
+    b.inv = smem + trace_smem_floats(P) / 4u;
+    b.window = reinterpret_cast<float *>(b.inv + 2u * n_bodies);
+    b.window_n = A.tau_window + A.color_window;
+    for (uint32_t k = threadIdx.x; k < b.window_n; k += blockDim.x) b.window[k] = 0.0f;
+    for (uint32_t k = threadIdx.x; k < n_bodies; k += blockDim.x) {
+        const float4 m = P.bodies[k * kBodyVec4 + kMaterial], r = P.bodies[k * kBodyVec4 + kRingColor];
+        b.inv[2u * k] = make_float4(inv_or_zero(m.x), inv_or_zero(m.y), inv_or_zero(m.z), 0.0f);
+        b.inv[2u * k + 1u] = make_float4(inv_or_zero(r.x), inv_or_zero(r.y), inv_or_zero(r.z), 0.0f);
+    }
+    return b;  // stage_scene's barrier publishes both
+}
+
+// Reduce the per-thread sums over the warp, then flush the windows.
+__device__ __forceinline__ void close_sink(const AdjointParams &A, const BlockSink &b, const float *own,
+                                           unsigned long long dropped) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) {
+        float v = own[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0u && v != 0.0f) {
+            if (k < A.color_window) atomicAdd(b.window + A.tau_window + k, v);
+            else atomicAdd(A.grad + kGradColor + k, v);
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < b.window_n; k += blockDim.x) {
+        const float v = b.window[k];
+        if (v != 0.0f) atomicAdd(A.grad + (k < A.tau_window ? k : kGradColor + (k - A.tau_window)), v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dropped += __shfl_down_sync(0xffffffffu, dropped, o);
+    if (lane == 0u && dropped != 0ull && A.overflow) atomicAdd(A.overflow, dropped);
+}
+
+// End of a replay: pass 1 either scatters its deferred factors (the slot is
+// then given back) or sets up pass 2 and restarts the sample from its camera
+// ray; pass 2 just gives the slot back. Returns true on a restart.
+template <bool L, bool F>
+__device__ __forceinline__ bool end_replay(const TraceParams &P, Counter<false, L, F> K, Prb &G, Path &p,
+                                           uint32_t pixel, uint32_t smp, float3 w) {
+    if (G.pass2) return false;
+    if (G.deferral_full || cap_binds(G, p.radiance)) {
+        pass2_setup(G, p.radiance, w);
+        start_path(p, &P.s, K, pixel, pixel % P.width, pixel / P.width, smp);
+        return true;
+    }
+    flush_deferred(G);
+    return false;
+}
+
+__device__ __forceinline__ float4 plane6(const Path &p, uint32_t pixel, uint32_t slot) {
+    return make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
+                       __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(pixel),
+                       __uint_as_float(slot));
+}
+
+// Stores every plane of a path whose plane 6 carries (pixel, slot).
+__device__ __forceinline__ void store_adjoint_path(float4 *st, uint32_t pool, uint32_t i, const Path &p,
+                                                   uint32_t pixel, uint32_t slot) {
+    store_path(st, pool, i, p, 0u);
+    st[6 * pool + i] = plane6(p, pixel, slot);
+}
+
+template <bool L, bool F>
+__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
+    adj_extend(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
+               const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
+    extern __shared__ float4 smem[];
+    __shared__ Append<5> sm[2];
+    WaveCounters *c = counters(W, t);
+    const uint32_t kept = c->cont, next = c->next;
+    const uint32_t per_sample = padded_pixels(W);
+    const uint32_t take = min(W.pool - kept, per_sample * W.chunk_samples - next);
+    const uint32_t n = kept + take;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters(W, t + 1u)->next = next + take;
+        *counters(W, t + 2u) = WaveCounters{};
+    }
+    if (blockIdx.x * kThreads >= n) return;
+    const BlockSink bs = open_sink(P, A, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    float own[6u * kColorSlots];
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
+    const uint32_t n_bodies = P.s.counts[0];
+    const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
+    const GradSink sink{own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad};
+    unsigned long long dropped = 0;
+    float4 *st = W.state[t & 1u];
+    float4 *out = W.state[(t + 1u) & 1u];
+    float4 *H = W.hits;
+    uint32_t round = 0;
+    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
+        const uint32_t i = base + threadIdx.x;
+        bool ring = false, surface = false, restart = false, give = false, take_slot = false;
+        Path p;
+        Prb G;
+        Extension e;
+        uint32_t pixel = 0, slot = 0, smp = 0;
+        float3 w = f3(0.0f, 0.0f, 0.0f);
+        const bool fresh = i >= kept;
+        if (i < n) {
+            bool valid = true;
+            if (fresh) {
+                const uint32_t k = next + (i - kept);
+                smp = k / per_sample;
+                const uint32_t q = k - smp * per_sample;
+                const uint32_t tile = q >> 8, within = q & 255u;
+                const uint32_t warp = within >> 5, lane = within & 31u;
+                const uint32_t x = (tile % W.tiles_x) * kTile + (warp & 1u) * 8u + (lane & 7u);
+                const uint32_t y = (tile / W.tiles_x) * kTile + (warp >> 1) * 4u + (lane >> 3);
+                valid = x < P.width && y < P.height;
+                if (valid) {
+                    pixel = y * P.width + x;
+                    w = pixel_weight(A, pixel);
+                    // Pixels the loss does not weigh are not replayed.
+                    valid = w.x != 0.0f || w.y != 0.0f || w.z != 0.0f;
+                }
+                if (valid) start_path(p, &P.s, K, pixel, x, y, smp);
+            } else {
+                load_ray_part(st, W.pool, i, p);
+                const float4 g = st[6 * W.pool + i];
+                pixel = __float_as_uint(g.z);
+                slot = __float_as_uint(g.w);
+            }
+            if (valid) {
+                NoGrad nograd;  // extend's only hook sets the iteration
+                const bool alive = extend(S, K, p, nograd, e);
+                ring = alive && e.ring.index != kMiss;
+                surface = alive && !ring && e.hit.index != kMiss;
+                take_slot = fresh && (ring || surface);
+                if (!fresh && !ring && !surface) {
+                    // Escaped or at the iteration bound: the replay ends.
+                    load_radiance_part(st, W.pool, i, p);
+                    w = pixel_weight(A, pixel);
+                    load_prb(X, slot, w, G, smp);
+                    G.sink = sink;
+                    G.inv = bs.inv;
+                    G.iteration = p.iterations;
+                    restart = end_replay(P, K, G, p, pixel, smp, w);
+                    give = !restart;
+                    dropped += G.dropped;
+                }
+            }
+        }
+        const bool flags[5] = {ring, surface, restart, give, take_slot};
+        uint32_t *const ctr[5] = {&c->ring, &c->surface, &counters(W, t + 1u)->cont, X.free_ends + 1,
+                                  X.free_ends + 0};
+        uint32_t q[5];
+        block_append<5>(sm[round & 1u], flags, ctr, q);
+        if (take_slot) {
+            slot = X.free_ring[q[4] % W.pool];
+            fresh_prb(G, w);
+            store_prb(X, slot, G, smp);
+            store_adjoint_path(st, W.pool, i, p, pixel, slot);
+        } else if (ring || surface) {
+            st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
+            st[6 * W.pool + i] = plane6(p, pixel, slot);
+        }
+        if (ring || surface) {
+            if (ring) H[1 * W.pool + i] = pack3(e.ring.p, e.ring.t);
+            else H[0 * W.pool + i] = pack3(e.hit.n, e.hit.t);
+            H[2 * W.pool + i] = make_float4(__uint_as_float(e.hit.index), __uint_as_float(e.ring.index), e.hit.delta,
+                                            e.disc_scale);
+            if (ring) W.ring_queue[q[0]] = i;
+            else W.surface_queue[q[1]] = i;
+        }
+        if (restart) {
+            store_prb(X, slot, G, smp);
+            store_adjoint_path(out, W.pool, q[2], p, pixel, slot);
+        }
+        if (give) X.free_ring[q[3] % W.pool] = slot;
+    }
+    close_sink(A, bs, own, dropped);
+}
+
+// Ring (R == true) or surface stage of the replay over its queue.
+template <bool L, bool F, bool R>
+__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
+    adj_shade(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
+              const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
+    extern __shared__ float4 smem[];
+    __shared__ Append<2> sm[2];
+    WaveCounters *c = counters(W, t);
+    const uint32_t n = R ? c->ring : c->surface;
+    if (blockIdx.x * kThreads >= n) return;
+    const BlockSink bs = open_sink(P, A, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    float own[6u * kColorSlots];
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
+    const uint32_t n_bodies = P.s.counts[0];
+    const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
+    const GradSink sink{own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad};
+    unsigned long long dropped = 0;
+    const float4 *st = W.state[t & 1u];
+    float4 *out = W.state[(t + 1u) & 1u];
+    const float4 *H = W.hits;
+    const uint32_t *queue = R ? W.ring_queue : W.surface_queue;
+    uint32_t round = 0;
+    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
+        const uint32_t j = base + threadIdx.x;
+        bool keep = false, give = false;
+        Path p;
+        Prb G;
+        uint32_t pixel = 0, slot = 0, smp = 0;
+        if (j < n) {
+            const uint32_t i = queue[j];
+            load_ray_part(st, W.pool, i, p);
+            load_radiance_part(st, W.pool, i, p);
+            load_shade_part(st, W.pool, i, p);
+            const float4 g = st[6 * W.pool + i];
+            pixel = __float_as_uint(g.z);
+            slot = __float_as_uint(g.w);
+            const float3 w = pixel_weight(A, pixel);
+            load_prb(X, slot, w, G, smp);
+            G.sink = sink;
+            G.inv = bs.inv;
+            G.iteration = p.iterations;
+            const float4 h2 = H[2 * W.pool + i];
+            bool ended;
+            if constexpr (R) {
+                const float4 h1 = H[1 * W.pool + i];
+                const RingHit ring{h1.w, __float_as_uint(h2.y), xyz4(h1)};
+                ended = ring_vertex(S, K, p, ring, G);
+            } else {
+                const float4 h0 = H[0 * W.pool + i];
+                const Hit hit{h0.w, __float_as_uint(h2.x), h2.z, xyz4(h0)};
+                ended = surface_vertex(S, K, p, hit, h2.w, G);
+            }
+            keep = !ended || end_replay(P, K, G, p, pixel, smp, w);
+            give = !keep;
+            dropped += G.dropped;
+        }
+        const bool flags[2] = {keep, give};
+        uint32_t *const ctr[2] = {&counters(W, t + 1u)->cont, X.free_ends + 1};
+        uint32_t q[2];
+        block_append<2>(sm[round & 1u], flags, ctr, q);
+        if (keep) {
+            store_prb(X, slot, G, smp);
+            store_adjoint_path(out, W.pool, q[0], p, pixel, slot);
+        }
+        if (give) X.free_ring[q[1] % W.pool] = slot;
+    }
+    close_sink(A, bs, own, dropped);
+}
+
+__global__ void adj_reset_slots(uint32_t *ring, uint32_t *ends, uint32_t pool) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < pool) ring[k] = k;
+    if (k == 0) {
+        ends[0] = 0u;
+        ends[1] = pool;
+    }
+}
+
+template <bool L, bool F>
+cudaError_t run_adjoint_iteration(const TraceParams &p, const AdjointParams &a, const WaveParams &w,
+                                  const AdjointWave &x, uint32_t t, const int (&grid)[3], size_t smem,
+                                  cudaStream_t stream) {
+    adj_extend<L, F><<<grid[0], kThreads, smem, stream>>>(p, a, w, x, t);
+    adj_shade<L, F, true><<<grid[1], kThreads, smem, stream>>>(p, a, w, x, t);
+    adj_shade<L, F, false><<<grid[2], kThreads, smem, stream>>>(p, a, w, x, t);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t adjoint_slot_bytes(uint32_t pool) {
+    return (size_t)pool * (kAdjointSideVec4 * sizeof(float4) + sizeof(PrbLists)) + (size_t)pool * sizeof(uint32_t) +
+           4 * sizeof(uint32_t);
+}
+
+cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t pool, cudaStream_t stream) {
+    adj_reset_slots<<<(pool + 255u) / 256u, 256, 0, stream>>>(x.free_ring, x.free_ends, pool);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &a, WaveParams w,
+                                     const AdjointWave &x, WaveCounters *pinned, cudaEvent_t ready,
+                                     cudaStream_t stream, WaveRun *run) {
+    *run = WaveRun{};
+    const uint32_t z = p.s.counts[2];
+    if (z == 0 || p.width == 0 || p.height == 0) return cudaSuccess;
+    const bool land = p.s.g.ground_north[3] != 0.0f;
+    const void *fns[3];
+    if (land) {
+        fns[0] = p.fp64_sites ? (const void *)adj_extend<true, true> : (const void *)adj_extend<true, false>;
+        fns[1] = p.fp64_sites ? (const void *)adj_shade<true, true, true> : (const void *)adj_shade<true, false, true>;
+        fns[2] = p.fp64_sites ? (const void *)adj_shade<true, true, false> : (const void *)adj_shade<true, false, false>;
+    } else {
+        fns[0] = p.fp64_sites ? (const void *)adj_extend<false, true> : (const void *)adj_extend<false, false>;
+        fns[1] = p.fp64_sites ? (const void *)adj_shade<false, true, true> : (const void *)adj_shade<false, false, true>;
+        fns[2] = p.fp64_sites ? (const void *)adj_shade<false, true, false> : (const void *)adj_shade<false, false, false>;
+    }
+    const size_t smem = adjoint_smem_bytes(p, a);
+    int grid[3];
+    for (int k = 0; k < 3; ++k) {
+        if (smem > 48u * 1024u) {
+            cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = persistent_grid(fns[k], smem, &grid[k]);
+        if (e != cudaSuccess) return e;
+    }
+    w.tiles_x = (p.width + kTile - 1) / kTile;
+    w.tiles_y = (p.height + kTile - 1) / kTile;
+    w.chunk_first = 0;
+    w.chunk_samples = z;
+    const uint32_t samples = w.tiles_x * w.tiles_y * 256u * z;
+    // A sample replays at most twice, each replay ending within the
+    // iteration bound; see launch_wavefront for the host-side guard.
+    const uint64_t cap = 2ull * ((uint64_t)p.s.counts[3] * (p.s.counts[0] + 2u) + 2u);
+    const uint64_t bound = ((uint64_t)samples + 1u) * cap;
+    cudaError_t e = cudaMemsetAsync(w.counters, 0, kWaveCounterSets * sizeof(WaveCounters), stream);
+    if (e != cudaSuccess) return e;
+    constexpr uint64_t kTailCheck = 2;
+    uint64_t check_at = (samples + (uint64_t)w.pool - 1u) / w.pool;
+    for (uint64_t t = 0;; ++t) {
+        if (t >= bound) return cudaErrorLaunchTimeout;
+        const uint32_t it = (uint32_t)t;
+        e = land ? (p.fp64_sites ? run_adjoint_iteration<true, true>(p, a, w, x, it, grid, smem, stream)
+                                 : run_adjoint_iteration<true, false>(p, a, w, x, it, grid, smem, stream))
+                 : (p.fp64_sites ? run_adjoint_iteration<false, true>(p, a, w, x, it, grid, smem, stream)
+                                 : run_adjoint_iteration<false, false>(p, a, w, x, it, grid, smem, stream));
+        if (e != cudaSuccess) return e;
+        run->iterations += 1;
+        run->kernels += 3;
+        if (t + 1 < check_at) continue;
+        const WaveCounters *dev = w.counters + ((t + 1) % kWaveCounterSets);
+        if ((e = cudaMemcpyAsync(pinned, dev, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaEventRecord(ready, stream)) != cudaSuccess || (e = cudaEventSynchronize(ready)) != cudaSuccess)
+            return e;
+        if (pinned->cont == 0 && pinned->next >= samples) break;
+        const uint64_t left = pinned->next >= samples ? 0u : samples - pinned->next;
+        check_at = t + 1 + (left ? (left + w.pool - 1u) / w.pool : kTailCheck);
+    }
+    return cudaSuccess;
+}
+
+}  // namespace sg

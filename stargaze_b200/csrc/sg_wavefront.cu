@@ -31,118 +31,11 @@
 // other, a few ulps.
 #include <algorithm>
 
-#include "sg_integrator.cuh"
+#include "sg_wave_common.cuh"
 
 namespace sg {
 
 namespace {
-
-#ifndef SG_WAVE_MIN_BLOCKS
-#define SG_WAVE_MIN_BLOCKS 4
-#endif
-
-// ---------------------------------------------------------------------------
-// Path state planes
-// ---------------------------------------------------------------------------
-//   0  ray.o, ray.anchor            4  ring_base, shine_body
-//   1  ray.d, rng                   5  previous_vertex.o, previous_vertex.anchor
-//   2  throughput, previous_pdf     6  iterations | point_gained << 31,
-//   3  radiance, ring_cap              depth | null_crossings << 16, result slot
-// The previous vertex is only ever used for its position (relative_center),
-// so its direction is not stored.
-__device__ __forceinline__ float4 pack3(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
-__device__ __forceinline__ float4 pack3u(float3 v, uint32_t w) { return make_float4(v.x, v.y, v.z, __uint_as_float(w)); }
-__device__ __forceinline__ float3 xyz4(float4 v) { return f3(v.x, v.y, v.z); }
-
-__device__ __forceinline__ void store_path(float4 *st, uint32_t pool, uint32_t i, const Path &p, uint32_t slot) {
-    st[0 * pool + i] = pack3u(p.ray.o, p.ray.anchor);
-    st[1 * pool + i] = pack3u(p.ray.d, p.rng);
-    st[2 * pool + i] = pack3(p.throughput, p.previous_pdf);
-    st[3 * pool + i] = pack3(p.radiance, p.ring_cap);
-    st[4 * pool + i] = pack3u(p.ring_base, p.shine_body);
-    st[5 * pool + i] = pack3u(p.previous_vertex.o, p.previous_vertex.anchor);
-    st[6 * pool + i] = make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
-                                   __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(slot), 0.0f);
-}
-
-// Planes 0, 1 and 6: what extend reads. Returns the result slot.
-__device__ __forceinline__ uint32_t load_ray_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
-    const float4 a = st[0 * pool + i], b = st[1 * pool + i], g = st[6 * pool + i];
-    p.ray = Ray{xyz4(a), xyz4(b), __float_as_uint(a.w)};
-    p.rng = __float_as_uint(b.w);
-    const uint32_t it = __float_as_uint(g.x), dn = __float_as_uint(g.y);
-    p.iterations = it & 0x7fffffffu;
-    p.point_gained = (it >> 31) != 0u;
-    p.depth = dn & 0xffffu;
-    p.null_crossings = dn >> 16;
-    return __float_as_uint(g.z);
-}
-
-// Planes 3 and 4: radiance and the ring cap (what finish_path reads) and
-// the ringshine body.
-__device__ __forceinline__ void load_radiance_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
-    const float4 c = st[3 * pool + i], d = st[4 * pool + i];
-    p.radiance = xyz4(c);
-    p.ring_cap = c.w;
-    p.ring_base = xyz4(d);
-    p.shine_body = __float_as_uint(d.w);
-}
-
-// Planes 2 and 5: the rest of the state the shade stages need.
-__device__ __forceinline__ void load_shade_part(const float4 *st, uint32_t pool, uint32_t i, Path &p) {
-    const float4 c = st[2 * pool + i], e = st[5 * pool + i];
-    p.throughput = xyz4(c);
-    p.previous_pdf = c.w;
-    p.previous_vertex = Ray{xyz4(e), f3(0.0f, 0.0f, 0.0f), __float_as_uint(e.w)};
-}
-
-// ---------------------------------------------------------------------------
-// CTA-aggregated queue appends
-// ---------------------------------------------------------------------------
-// Each thread of the CTA passes `flag[q]` for Q queues; the thread gets its
-// slot in each queue where its flag is set. One atomicAdd per queue and
-// CTA; every thread of the CTA must call it. Consecutive calls alternate
-// between two scratch blocks, so a call never overwrites counts that a
-// slower warp of the previous call has yet to read.
-template <int Q>
-struct Append {
-    uint32_t warp_counts[Q][kThreads / 32];
-    uint32_t base[Q];
-};
-
-template <int Q>
-__device__ __forceinline__ void block_append(Append<Q> &sm, const bool (&flag)[Q], uint32_t *const (&counter)[Q],
-                                             uint32_t (&slot)[Q]) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t below = (1u << lane) - 1u;
-    uint32_t ballot[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        ballot[q] = __ballot_sync(0xffffffffu, flag[q]);
-        if (lane == 0) sm.warp_counts[q][warp] = __popc(ballot[q]);
-    }
-    __syncthreads();
-    if (threadIdx.x < Q) {
-        const int q = threadIdx.x;
-        uint32_t total = 0;
-        for (uint32_t w = 0; w < kThreads / 32; ++w) {
-            const uint32_t c = sm.warp_counts[q][w];
-            sm.warp_counts[q][w] = total;  // exclusive prefix
-            total += c;
-        }
-        sm.base[q] = total ? atomicAdd(counter[q], total) : 0u;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < Q; ++q) slot[q] = sm.base[q] + sm.warp_counts[q][warp] + __popc(ballot[q] & below);
-}
-
-__device__ __forceinline__ WaveCounters *counters(const WaveParams &W, uint32_t t) {
-    return W.counters + (t % kWaveCounterSets);
-}
-
-// Samples of a chunk are numbered sample-major over the padded tile grid.
-__device__ __forceinline__ uint32_t padded_pixels(const WaveParams &W) { return W.tiles_x * W.tiles_y * 256u; }
 
 // ---------------------------------------------------------------------------
 // Stages
@@ -337,29 +230,6 @@ template <bool L, bool F>
 StageSet stage_set() {
     return StageSet{(const void *)wave_extend<L, F>, (const void *)wave_shade<L, F, true>,
                     (const void *)wave_shade<L, F, false>};
-}
-
-cudaError_t persistent_grid(const void *fn, size_t smem, int *grid) {
-    int device = 0, sms = 0, per_sm = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem);
-    if (e != cudaSuccess) return e;
-    *grid = sms * (per_sm > 0 ? per_sm : 1);
-    return cudaSuccess;
-}
-
-cudaError_t mark(StageMarks *m, int stage, cudaStream_t stream) {
-    if (!m) return cudaSuccess;
-    if (m->used == m->events.size()) {
-        cudaEvent_t e;
-        cudaError_t err = cudaEventCreate(&e);
-        if (err != cudaSuccess) return err;
-        m->events.push_back(e);
-        m->stage.push_back(kStageGap);
-    }
-    m->stage[m->used] = stage;
-    return cudaEventRecord(m->events[m->used++], stream);
 }
 
 template <bool L, bool F>
