@@ -27,8 +27,14 @@ namespace sg {
 
 namespace {
 
-#ifndef SG_WAVE_ADJ_MIN_BLOCKS
-#define SG_WAVE_ADJ_MIN_BLOCKS 2
+// Resident CTAs per SM the stages are compiled for. The extend stage keeps
+// the adjoint state out of its main loop (extend_end), so it fits the
+// forward's register budget.
+#ifndef SG_WAVE_ADJ_EXTEND_MIN_BLOCKS
+#define SG_WAVE_ADJ_EXTEND_MIN_BLOCKS 4
+#endif
+#ifndef SG_WAVE_ADJ_SHADE_MIN_BLOCKS
+#define SG_WAVE_ADJ_SHADE_MIN_BLOCKS 2
 #endif
 
 // Slot state (float4 words):
@@ -183,6 +189,35 @@ __device__ __forceinline__ bool end_replay(const TraceParams &P, Counter<false, 
     return false;
 }
 
+// A replay that ends at extend (escaped, or at the iteration bound) with
+// path radiance `radiance`: loads its adjoint state and ends it. Returns
+// the sample index in the low word when the sample restarts for pass 2 (the
+// slot state is then stored), kMiss when the slot is given back; the high
+// word counts dropped derivative entries. Everything is passed by value so
+// that the caller's path stays in registers.
+static __device__ __noinline__ unsigned long long extend_end(const AdjointParams &A, const AdjointWave &X,
+                                                            GradSink sink, const float4 *inv, float3 radiance,
+                                                            uint32_t iterations, uint32_t pixel, uint32_t slot) {
+    const float3 w = pixel_weight(A, pixel);
+    Prb G;
+    uint32_t smp;
+    load_prb(X, slot, w, G, smp);
+    G.sink = sink;
+    G.inv = inv;
+    G.iteration = iterations;
+    uint32_t code = kMiss;
+    if (!G.pass2) {
+        if (G.deferral_full || cap_binds(G, radiance)) {
+            pass2_setup(G, radiance, w);
+            store_prb(X, slot, G, smp);
+            code = smp;
+        } else {
+            flush_deferred(G);
+        }
+    }
+    return ((unsigned long long)G.dropped << 32) | code;
+}
+
 __device__ __forceinline__ float4 plane6(const Path &p, uint32_t pixel, uint32_t slot) {
     return make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
                        __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(pixel),
@@ -197,7 +232,7 @@ __device__ __forceinline__ void store_adjoint_path(float4 *st, uint32_t pool, ui
 }
 
 template <bool L, bool F>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
     adj_extend(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
                const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
     extern __shared__ float4 smem[];
@@ -230,7 +265,6 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
         const uint32_t i = base + threadIdx.x;
         bool ring = false, surface = false, restart = false, give = false, take_slot = false;
         Path p;
-        Prb G;
         Extension e;
         uint32_t pixel = 0, slot = 0, smp = 0;
         float3 w = f3(0.0f, 0.0f, 0.0f);
@@ -267,15 +301,14 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
                 take_slot = fresh && (ring || surface);
                 if (!fresh && !ring && !surface) {
                     // Escaped or at the iteration bound: the replay ends.
-                    load_radiance_part(st, W.pool, i, p);
-                    w = pixel_weight(A, pixel);
-                    load_prb(X, slot, w, G, smp);
-                    G.sink = sink;
-                    G.inv = bs.inv;
-                    G.iteration = p.iterations;
-                    restart = end_replay(P, K, G, p, pixel, smp, w);
+                    const float3 radiance = xyz4(st[3 * W.pool + i]);
+                    const unsigned long long end =
+                        extend_end(A, X, sink, bs.inv, radiance, p.iterations, pixel, slot);
+                    dropped += end >> 32;
+                    const uint32_t code = (uint32_t)end;
+                    restart = code != kMiss;
                     give = !restart;
-                    dropped += G.dropped;
+                    if (restart) start_path(p, &P.s, K, pixel, pixel % P.width, pixel / P.width, code);
                 }
             }
         }
@@ -286,6 +319,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
         block_append<5>(sm[round & 1u], flags, ctr, q);
         if (take_slot) {
             slot = X.free_ring[q[4] % W.pool];
+            Prb G;
             fresh_prb(G, w);
             store_prb(X, slot, G, smp);
             store_adjoint_path(st, W.pool, i, p, pixel, slot);
@@ -301,10 +335,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
             if (ring) W.ring_queue[q[0]] = i;
             else W.surface_queue[q[1]] = i;
         }
-        if (restart) {
-            store_prb(X, slot, G, smp);
-            store_adjoint_path(out, W.pool, q[2], p, pixel, slot);
-        }
+        if (restart) store_adjoint_path(out, W.pool, q[2], p, pixel, slot);
         if (give) X.free_ring[q[3] % W.pool] = slot;
     }
     close_sink(A, bs, own, dropped);
@@ -312,7 +343,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
 
 // Ring (R == true) or surface stage of the replay over its queue.
 template <bool L, bool F, bool R>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     adj_shade(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
               const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
     extern __shared__ float4 smem[];
