@@ -311,7 +311,7 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
     """Forward (spp samples from a fresh accumulation) and path-replay
     adjoint (sg_backward for a seeded d loss / d image) times, CUDA events on
     the launching stream, median over `reps`; the forward with both
-    integrators (the adjoint replays the same samples either way)."""
+    integrators, and both adjoints (staged and per-pixel) on the same tape."""
     import torch
 
     from stargaze_b200 import PathTracer
@@ -320,7 +320,7 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
     t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
     upload_workload(t, wl)
     dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
-    fwd, mega, bwd = [], [], []
+    fwd, mega, bwd, per_pixel = [], [], [], []
     for r in range(reps + 1):
         frame = wl.frame.copy()
         frame.scene_time = float(-1 - r)
@@ -330,24 +330,30 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
         frame.scene_time = float(-100 - r)
         f = timed_forward(t, wl, frame, stream)
         tape = t.tape()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         e[0].record(stream)
-        g = t.backward(frame, tape, dl, stream)
+        g = t.backward(frame, tape, dl, stream)  # staged adjoint
         e[1].record(stream)
+        t.set_integrator("megakernel")
+        e[2].record(stream)
+        t.backward(frame, tape, dl, stream)  # per-pixel adjoint kernel
+        e[3].record(stream)
         stream.synchronize()
         if r > 0:  # the first round loads the kernels
             fwd.append(f)
             mega.append(m)
             bwd.append(e[0].elapsed_time(e[1]))
+            per_pixel.append(e[2].elapsed_time(e[3]))
     t.close()
     f, m, b = statistics.median(fwd), statistics.median(mega), statistics.median(bwd)
     params = int(sum(v.size for v in wl.ring_tables.values())) + 6 * len(wl.frame.bodies)
     if wl.landscape is not None and wl.landscape.albedo_map is not None:
         params += int(wl.landscape.albedo_map.size)
     return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp, "forward_ms": f,
-            "forward_megakernel_ms": m, "backward_ms": b, "ratio": b / f,
-            "forward_plus_adjoint_over_forward": (f + b) / f, "ratio_vs_megakernel_forward": b / m,
-            "parameters": params, "dropped_entries": int(g.dropped)}
+            "forward_megakernel_ms": m, "backward_ms": b, "backward_per_pixel_ms": statistics.median(per_pixel),
+            "ratio": b / f, "forward_plus_adjoint_over_forward": (f + b) / f,
+            "parameters": params, "dropped_entries": int(g.dropped),
+            "note": "forward: wavefront; backward: staged adjoint (per-pixel adjoint kernel beside it)"}
 
 
 def integrator_comparison(wl, device: int, stream, reps: int = 3) -> dict:

@@ -53,6 +53,12 @@
 #include "sg_device.cuh"
 #include "sg_landscape.cuh"
 
+// Call attribute of the derivative hooks: out of line by default, which
+// keeps the per-pixel adjoint's instruction footprint to one replay.
+#ifndef SG_ADJ_HOOK
+#define SG_ADJ_HOOK __noinline__
+#endif
+
 namespace sg {
 
 constexpr uint32_t kNoParam = 0xffffffffu;
@@ -205,7 +211,7 @@ __device__ __forceinline__ void scatter_entry(const GradSink &sink, const GradEn
 // pass 2 scatters only what differs: nothing before the cap vertex's
 // scatter, w_post - w after it, and the cap terms and attached entries in
 // full. The running sums take each contribution's full weight.
-static __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_term) {
+static __device__ SG_ADJ_HOOK void contribute(Prb &G, float3 value, bool cap_term) {
     const bool post = G.post();
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     const float3 full = cap_term ? G.w_cap : (post ? G.w_post : G.w_pre);
@@ -224,7 +230,7 @@ static __device__ __noinline__ void contribute(Prb &G, float3 value, bool cap_te
 // A factor multiplied into the throughput now: its share of everything the
 // path gathers from here on, plus — past a binding cap vertex — its part in
 // the later Russian-roulette survivals (score and attached 1 / s).
-static __device__ __noinline__ void factor(Prb &G, GradEntry e) {
+static __device__ SG_ADJ_HOOK void factor(Prb &G, GradEntry e) {
     if (e.param == kNoParam) return;
     if (!G.pass2) {
         // Pass 1: defer until the path's end.
@@ -349,7 +355,7 @@ struct Visibility {
 };
 
 template <bool C, bool L, bool F>
-static __device__ __noinline__ Visibility light_visibility_grad(Scene S, Counter<C, L, F> K, Ray r, uint32_t light,
+static __device__ SG_ADJ_HOOK Visibility light_visibility_grad(Scene S, Counter<C, L, F> K, Ray r, uint32_t light,
                                                          bool entries) {
     Crossings rec;
     rec.n = 0;
@@ -383,7 +389,7 @@ struct RingVertexGrad {
     float dlog_pdf;
 };
 
-static __device__ __noinline__ RingVertexGrad ring_vertex_grad(Scene S, uint32_t ring, float3 point, float tau,
+static __device__ SG_ADJ_HOOK RingVertexGrad ring_vertex_grad(Scene S, uint32_t ring, float3 point, float tau,
                                                         float mu_out) {
     RingVertexGrad v{kNoParam, 0.0f, 0.0f};
     v.param = tau_param(S, ring, point, &v.scale);
@@ -403,7 +409,7 @@ __device__ __forceinline__ GradEntry ring_tau_entry(const RingVertexGrad &v, flo
 // (max(shadowed, 0.003 * unshadowed) luminance of `lit`). After the cap
 // vertex the MIS weight's dependence on the vertex's scatter pdf is an
 // attached entry.
-static __device__ __noinline__ void ring_light_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
+static __device__ SG_ADJ_HOOK void ring_light_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
                                              float mu_in, uint32_t light, float3 lit, Visibility vis, float weight,
                                              float ring_mis, bool last_vertex, RingVertexGrad vg) {
     const GradEntry tau_e = ring_tau_entry(vg, optics.tau, mu_out, mu_in);
@@ -433,7 +439,7 @@ static __device__ __noinline__ void ring_light_grad(Scene S, Prb &G, uint32_t ri
 
 // A null crossing (pathtrace.wgsl:1451-1456): the transmission factor, and
 // after a binding cap vertex the decision's score d log T.
-static __device__ __noinline__ void ring_null_grad(Scene S, Prb &G, uint32_t ring, float3 point, float3 d) {
+static __device__ SG_ADJ_HOOK void ring_null_grad(Scene S, Prb &G, uint32_t ring, float3 point, float3 d) {
     const GradEntry ce = crossing_entry(S, ring, point, d);
     factor(G, ce);
     score(G, ce.param, ce.dlog.x);
@@ -443,7 +449,7 @@ static __device__ __noinline__ void ring_null_grad(Scene S, Prb &G, uint32_t rin
 // a binding cap vertex also the decision's score d log(1 - T) and the
 // attached 1 / scatter pdf. Records the vertex for the MIS weight of an
 // emitter reached next.
-static __device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
+static __device__ SG_ADJ_HOOK void ring_scatter_grad(Scene S, Prb &G, uint32_t ring, Optics optics, float mu_out,
                                                float z, RingVertexGrad v, float transmission, float3 d) {
     factor(G, ring_tau_entry(v, optics.tau, mu_out, z));
     factor(G, ring_albedo_entry(G, ring));
@@ -457,7 +463,7 @@ static __device__ __noinline__ void ring_scatter_grad(Scene S, Prb &G, uint32_t 
 }
 
 // One light sample at a surface vertex (pathtrace.wgsl:1545-1565).
-static __device__ __noinline__ void surface_light_grad(Prb &G, GradEntry albedo_e, uint32_t light, float3 value,
+static __device__ SG_ADJ_HOOK void surface_light_grad(Prb &G, GradEntry albedo_e, uint32_t light, float3 value,
                                                 Visibility vis) {
     G.local_factor(albedo_e);
     G.local_factor(emitter_entry(G, light));
@@ -468,7 +474,7 @@ static __device__ __noinline__ void surface_light_grad(Prb &G, GradEntry albedo_
 // An emitter reached by the path (pathtrace.wgsl:1516-1526); `mis` is the
 // MIS weight against the previous vertex's light sample, whose bsdf pdf
 // (a ring scatter's) moves with that vertex's optical depth.
-static __device__ __noinline__ void emitter_grad(Prb &G, uint32_t body, float3 value, float mis, bool weighted) {
+static __device__ SG_ADJ_HOOK void emitter_grad(Prb &G, uint32_t body, float3 value, float mis, bool weighted) {
     G.local_factor(emitter_entry(G, body));
     if (G.binding && G.post() && weighted && G.prev_param != kNoParam)
         G.local_factor(scalar_entry(G.prev_param | kPdfBit, 2.0f * (1.0f - mis) * G.prev_dlog_pdf));
@@ -479,7 +485,7 @@ static __device__ __noinline__ void emitter_grad(Prb &G, uint32_t body, float3 v
 // (zero where the clamp of surface_albedo is active), or the albedo-map
 // texel of the host ground.
 template <bool L>
-static __device__ __noinline__ GradEntry albedo_entry(Scene S, const float4 *inv, Ray ray, float t, uint32_t index,
+static __device__ SG_ADJ_HOOK GradEntry albedo_entry(Scene S, const float4 *inv, Ray ray, float t, uint32_t index,
                                                float3 albedo) {
     if (index < kLocalBase) {
         const float4 m = inv[2u * index];
@@ -501,7 +507,7 @@ static __device__ __noinline__ GradEntry albedo_entry(Scene S, const float4 *inv
 // result as ringshine(), plus one contribution per light. `carried` is the
 // path throughput times the surface albedo.
 template <bool C, bool L, bool F>
-static __device__ __noinline__ Shine ringshine_grad(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
+static __device__ SG_ADJ_HOOK Shine ringshine_grad(Scene S, Counter<C, L, F> K, uint32_t index, float3 origin, float3 normal,
                                              bool last_vertex, uint32_t rng, Prb &G, float3 carried,
                                              GradEntry albedo_e) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
@@ -547,7 +553,7 @@ __device__ __forceinline__ void record_capture(Prb &G, uint32_t iteration, float
     G.cap_light = cap_direct ? G.lit_vis_sum : G.lit_sum * kRingIndirectCap;
 }
 
-static __device__ __noinline__ void record_roulette(Prb &G, uint32_t iteration, float3 t, float s, bool survived,
+static __device__ SG_ADJ_HOOK void record_roulette(Prb &G, uint32_t iteration, float3 t, float s, bool survived,
                                              float3 radiance) {
     if (G.capture_iter == 0u) return;
     if (G.n_rr >= (uint32_t)kMaxRoulette) {
@@ -590,7 +596,7 @@ __device__ __forceinline__ bool cap_binds(const Prb &G, float3 total) {
 
 // End of a path that pass 1 finished alone: each deferred factor's share of
 // the weighted radiance gathered after it.
-static __device__ __noinline__ void flush_deferred(Prb &G) {
+static __device__ SG_ADJ_HOOK void flush_deferred(Prb &G) {
 #pragma unroll 1
     for (uint32_t k = 0; k < G.n_fac; ++k) {
         const GradEntry e = G.lists->fac[k];
@@ -608,7 +614,7 @@ static __device__ __noinline__ void flush_deferred(Prb &G) {
 
 // Pass 2's weights from pass 1's summary, the path's total radiance and the
 // pixel weight w.
-static __device__ __noinline__ void pass2_setup(Prb &G, float3 total, float3 w) {
+static __device__ SG_ADJ_HOOK void pass2_setup(Prb &G, float3 total, float3 w) {
     const float3 lum = f3(0.2126f, 0.7152f, 0.0722f);
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = true;
