@@ -43,6 +43,13 @@ namespace {
 #ifndef SG_WAVE_ADJ_SHADE_MIN_BLOCKS
 #define SG_WAVE_ADJ_SHADE_MIN_BLOCKS 2
 #endif
+// CTA size of the shade stages. Smaller CTAs wait at each queue append for
+// fewer slow warps but measured slower on the ring scene (64, 128, 256
+// threads at 128 registers: 11.3, 10.3, 9.8 ms).
+#ifndef SG_WAVE_ADJ_SHADE_THREADS
+#define SG_WAVE_ADJ_SHADE_THREADS 256
+#endif
+constexpr int kShadeThreads = SG_WAVE_ADJ_SHADE_THREADS;
 
 // Slot state (float4 words):
 //   0  a.xyz, cap                         5  w_pdf.xyz        (pass 2)
@@ -350,14 +357,14 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
 
 // Ring (R == true) or surface stage of the replay over its queue.
 template <bool L, bool F, bool R>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
+__global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     adj_shade(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
               const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
     extern __shared__ float4 smem[];
-    __shared__ Append<2> sm[2];
+    __shared__ Append<2, kShadeThreads> sm[2];
     WaveCounters *c = counters(W, t);
     const uint32_t n = R ? c->ring : c->surface;
-    if (blockIdx.x * kThreads >= n) return;
+    if (blockIdx.x * kShadeThreads >= n) return;
     const BlockSink bs = open_sink(P, A, smem);
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
@@ -373,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     const float4 *H = W.hits;
     const uint32_t *queue = R ? W.ring_queue : W.surface_queue;
     uint32_t round = 0;
-    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
+    for (uint32_t base = blockIdx.x * kShadeThreads; base < n; base += gridDim.x * kShadeThreads, ++round) {
         const uint32_t j = base + threadIdx.x;
         bool keep = false, give = false;
         Path p;
@@ -410,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
         const bool flags[2] = {keep, give};
         uint32_t *const ctr[2] = {&counters(W, t + 1u)->cont, X.free_ends + 1};
         uint32_t q[2];
-        block_append<2>(sm[round & 1u], flags, ctr, q);
+        block_append<2, kShadeThreads>(sm[round & 1u], flags, ctr, q);
         if (keep) {
             store_prb(X, slot, G, smp);
             store_adjoint_path(out, W.pool, q[0], p, pixel, slot);
@@ -434,8 +441,8 @@ cudaError_t run_adjoint_iteration(const TraceParams &p, const AdjointParams &a, 
                                   const AdjointWave &x, uint32_t t, const int (&grid)[3], size_t smem,
                                   cudaStream_t stream) {
     adj_extend<L, F><<<grid[0], kThreads, smem, stream>>>(p, a, w, x, t);
-    adj_shade<L, F, true><<<grid[1], kThreads, smem, stream>>>(p, a, w, x, t);
-    adj_shade<L, F, false><<<grid[2], kThreads, smem, stream>>>(p, a, w, x, t);
+    adj_shade<L, F, true><<<grid[1], kShadeThreads, smem, stream>>>(p, a, w, x, t);
+    adj_shade<L, F, false><<<grid[2], kShadeThreads, smem, stream>>>(p, a, w, x, t);
     return cudaGetLastError();
 }
 
@@ -475,7 +482,7 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
             cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        cudaError_t e = persistent_grid(fns[k], smem, &grid[k]);
+        cudaError_t e = persistent_grid(fns[k], smem, &grid[k], k == 0 ? kThreads : kShadeThreads);
         if (e != cudaSuccess) return e;
     }
     w.tiles_x = (p.width + kTile - 1) / kTile;

@@ -81,14 +81,14 @@ __device__ __forceinline__ void load_shade_part(const float4 *st, uint32_t pool,
 // without the barriers measured slower: 4 % on the ring workload's forward,
 // 30 % on the terrain's, 30 % on the ring adjoint — same-address atomics
 // from every warp serialise in L2.)
-template <int Q>
+template <int Q, int B = kThreads>
 struct Append {
-    uint32_t warp_counts[Q][kThreads / 32];
+    uint32_t warp_counts[Q][B / 32];
     uint32_t base[Q];
 };
 
-template <int Q>
-__device__ __forceinline__ void block_append(Append<Q> &sm, const bool (&flag)[Q], uint32_t *const (&counter)[Q],
+template <int Q, int B = kThreads>
+__device__ __forceinline__ void block_append(Append<Q, B> &sm, const bool (&flag)[Q], uint32_t *const (&counter)[Q],
                                              uint32_t (&slot)[Q]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
@@ -102,7 +102,7 @@ __device__ __forceinline__ void block_append(Append<Q> &sm, const bool (&flag)[Q
     if (threadIdx.x < Q) {
         const int q = threadIdx.x;
         uint32_t total = 0;
-        for (uint32_t w = 0; w < kThreads / 32; ++w) {
+        for (uint32_t w = 0; w < (uint32_t)B / 32u; ++w) {
             const uint32_t c = sm.warp_counts[q][w];
             sm.warp_counts[q][w] = total;  // exclusive prefix
             total += c;
@@ -125,11 +125,11 @@ __device__ __forceinline__ uint32_t padded_pixels(const WaveParams &W) { return 
 // (Asking for the largest L1 share through the shared-memory carveout
 // halved the forward's speed and did not help the adjoint: the driver's
 // choice stays.)
-inline cudaError_t persistent_grid(const void *fn, size_t smem, int *grid) {
+inline cudaError_t persistent_grid(const void *fn, size_t smem, int *grid, int threads = kThreads) {
     int device = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
     if (e != cudaSuccess) return e;
     *grid = sms * (per_sm > 0 ? per_sm : 1);
     return cudaSuccess;
