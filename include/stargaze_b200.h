@@ -369,6 +369,36 @@ SG_API int sg_set_integrator(sg_context *ctx, int integrator, uint32_t pool_path
 SG_API int sg_get_integrator(const sg_context *ctx, int *integrator, uint32_t *pool_paths,
                              uint32_t *iterations);
 
+/* ------------------------------------------------------------------ */
+/* Display without a graphics API                                      */
+/* ------------------------------------------------------------------ */
+
+/* The reference's display pass (display.wgsl:69-97, drawn by
+ * PathTracer::display, src/pathtracer.rs:1010-1014) into a device buffer
+ * instead of a swapchain or texture: each of width x height output pixels
+ * samples the accumulation bilinearly at its centre (any output size: the
+ * reference upscales the trace resolution to the window), applies the
+ * exposure in stops — the eased automatic value when options.auto_exposure
+ * is on, else options.exposure — plus options.ev_bias, limits the Milky Way
+ * backdrop layer and maps through the ACES curve.
+ *   SG_DISPLAY_RGBA8_SRGB  4 bytes per pixel, R G B A, sRGB-encoded as a
+ *                          Rgba8UnormSrgb target stores it (the format of
+ *                          the reference's headless PNG, src/headless.rs:13)
+ *   SG_DISPLAY_RGBA32F     4 floats per pixel, linear (the reference's
+ *                          Rgba32Float test targets)
+ * `out` lives on the device when `on_device`, else on the host (the call
+ * then synchronises `stream`). */
+#define SG_DISPLAY_RGBA8_SRGB 0
+#define SG_DISPLAY_RGBA32F 1
+SG_API int sg_display(sg_context *ctx, uint32_t width, uint32_t height, int format, void *out,
+                      int on_device, void *stream);
+
+/* The exposure the display uses now: the eased automatic value when
+ * options.auto_exposure is on (metered by every sg_encode, including ones
+ * that add no sample, as PathTracer::encode does, src/pathtracer.rs:980-
+ * 1000), else options.exposure. Synchronises `stream`. */
+SG_API int sg_get_exposure(sg_context *ctx, float *exposure, void *stream);
+
 /* Extension (measurement): with timing on, every wavefront stage launch is
  * bracketed by CUDA events and sg_encode waits for the dispatch to finish;
  * sg_get_stage_times then gives the milliseconds of the last timed

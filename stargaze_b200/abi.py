@@ -118,6 +118,8 @@ class Hit(C.Structure):
 
 
 NOALLOC_MAX_RAYS = 65536
+DISPLAY_RGBA8_SRGB = 0
+DISPLAY_RGBA32F = 1
 INTEGRATOR_MEGAKERNEL = 0
 INTEGRATOR_WAVEFRONT = 1
 WAVE_MAX_POOL = 1 << 26

@@ -92,6 +92,10 @@ struct sg_context {
     sg::WaveCounters *wave_pinned = nullptr;
     cudaEvent_t wave_ready = nullptr;
     uint32_t wave_iterations = 0;           // stage iterations of the last dispatch
+    // Display: the exposure state and histogram of the metering.
+    sg::ExposureState *exposure = nullptr;
+    uint32_t *histogram = nullptr;
+    bool exposure_was_enabled = false;
     bool stage_timing = false;              // bracket every stage with events
     sg::StageMarks stage_marks;
     float stage_ms[sg::kStageCount] = {};   // per stage, last timed dispatch
@@ -475,6 +479,8 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->wave_state);
     cudaFree(ctx->wave_results);
     cudaFree(ctx->adjoint_slots);
+    cudaFree(ctx->exposure);
+    cudaFree(ctx->histogram);
     if (ctx->wave_pinned) cudaFreeHost(ctx->wave_pinned);
     if (ctx->wave_ready) cudaEventDestroy(ctx->wave_ready);
     for (cudaEvent_t e : ctx->stage_marks.events) cudaEventDestroy(e);
@@ -676,6 +682,34 @@ static int ensure_adjoint(sg_context *ctx, uint32_t samples, sg::WaveParams &w, 
     return SG_OK;
 }
 
+// Automatic exposure (src/pathtracer.rs:883-905, :980-1000): publish the
+// controls — the whole state when metering was off, else everything but the
+// eased value — then meter the accumulation, on every encode, whether or
+// not it added samples. Nothing runs while automatic exposure is off.
+static int meter_exposure(sg_context *ctx, cudaStream_t stream) {
+    if (!ctx->options.auto_exposure) {
+        ctx->exposure_was_enabled = false;
+        return SG_OK;
+    }
+    if (ctx->width == 0 || ctx->height == 0) return SG_OK;
+    DeviceGuard guard(ctx->device);
+    if (!ctx->exposure) SG_CUDA(ctx, cudaMalloc(&ctx->exposure, sizeof(sg::ExposureState)));
+    if (!ctx->histogram) SG_CUDA(ctx, cudaMalloc(&ctx->histogram, sg::kExposureBins * sizeof(uint32_t)));
+    // Pageable source: the bytes are staged before the call returns.
+    const sg::ExposureState state{ctx->options.exposure, ctx->options.auto_key, ctx->options.auto_percentile, 1.0f,
+                                  ctx->options.ev_bias};
+    if (ctx->exposure_was_enabled) {
+        SG_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<char *>(ctx->exposure) + sizeof(float), &state.key,
+                                     sizeof(state) - sizeof(float), cudaMemcpyHostToDevice, stream));
+    } else {
+        SG_CUDA(ctx, cudaMemcpyAsync(ctx->exposure, &state, sizeof(state), cudaMemcpyHostToDevice, stream));
+    }
+    ctx->exposure_was_enabled = true;
+    cudaError_t e = sg::launch_exposure(ctx->mean, ctx->width, ctx->height, ctx->histogram, ctx->exposure, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "exposure metering");
+    return SG_OK;
+}
+
 static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr, uint64_t *events) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     int status = validate_frame(ctx, frame);
@@ -732,6 +766,8 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
             for (int k = 0; k < sg::kEventCount; ++k) events[k] = host[k];
         }
     }
+    status = meter_exposure(ctx, stream);
+    if (status != SG_OK) return status;
     ctx->history.samples += count;
     ctx->history.sequence += count;
     ctx->exposure_idle_frames = count > 0 ? 0u : (ctx->exposure_idle_frames == UINT32_MAX ? UINT32_MAX : ctx->exposure_idle_frames + 1u);
@@ -1033,6 +1069,63 @@ int sg_get_integrator(const sg_context *ctx, int *integrator, uint32_t *pool_pat
 }
 
 static_assert(sg::kStageCount == SG_STAGE_COUNT, "stage count");
+
+int sg_display(sg_context *ctx, uint32_t width, uint32_t height, int format, void *out, int on_device,
+               void *stream_ptr) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (!out) return fail(ctx, SG_ERR_INVALID, "out is NULL");
+    if (format != SG_DISPLAY_RGBA8_SRGB && format != SG_DISPLAY_RGBA32F)
+        return fail(ctx, SG_ERR_INVALID, "format must be SG_DISPLAY_RGBA8_SRGB or SG_DISPLAY_RGBA32F");
+    if (width == 0 || height == 0 || width > 16384 || height > 16384)
+        return fail(ctx, SG_ERR_INVALID, "display size must be 1..16384 on each side");
+    if (ctx->width == 0 || ctx->height == 0) return fail(ctx, SG_ERR_STATE, "the context has no viewport");
+    const bool automatic = ctx->options.auto_exposure && ctx->exposure_was_enabled;
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t bytes = (size_t)width * height * (format == SG_DISPLAY_RGBA32F ? 16u : 4u);
+    void *dst = out;
+    if (!on_device) {
+        int status = ensure_scratch(ctx, bytes);
+        if (status != SG_OK) return status;
+        dst = ctx->scratch;
+    }
+    sg::DisplayParams d{};
+    d.mean = ctx->mean;
+    d.backdrop = ctx->backdrop;
+    d.width = ctx->width;
+    d.height = ctx->height;
+    d.out_width = width;
+    d.out_height = height;
+    d.format = format;
+    d.out = dst;
+    d.automatic = automatic ? 1 : 0;
+    d.state = ctx->exposure;
+    d.manual = ctx->options.exposure;
+    d.bias = ctx->options.ev_bias;
+    d.milky_way = ctx->options.milky_way;
+    cudaError_t e = sg::launch_display(d, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "display");
+    if (!on_device) {
+        SG_CUDA(ctx, cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    }
+    return SG_OK;
+}
+
+int sg_get_exposure(sg_context *ctx, float *exposure, void *stream_ptr) {
+    if (!ctx || !exposure) return fail(ctx, SG_ERR_INVALID, "ctx or exposure is NULL");
+    if (!(ctx->options.auto_exposure && ctx->exposure_was_enabled && ctx->exposure)) {
+        *exposure = ctx->options.exposure;
+        return SG_OK;
+    }
+    DeviceGuard guard(ctx->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    float value = 0.0f;
+    SG_CUDA(ctx, cudaMemcpyAsync(&value, ctx->exposure, sizeof(float), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(ctx, cudaStreamSynchronize(stream));
+    *exposure = value;
+    return SG_OK;
+}
 
 int sg_set_stage_timing(sg_context *ctx, int enable) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");

@@ -133,6 +133,35 @@ cudaError_t launch_fma_peak(int blocks, int iters, float *out, cudaStream_t stre
 cudaError_t launch_ring_energy(float albedo, float tau, float mu, uint32_t steps, float *out,
                                cudaStream_t stream);
 
+// ---------------------------------------------------------------------------
+// Display (sg_display.cu): exposure metering and the HDR -> display resolve.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kExposureBins = 256;
+
+// The exposure state the reference shares with its shaders
+// (pathtracer.rs:54-64): `value` is eased on the device by the metering.
+struct ExposureState {
+    float value, key, percentile, enabled, bias;
+};
+
+struct DisplayParams {
+    const float4 *mean;      // width * height accumulation
+    const float4 *backdrop;  // width * height Milky Way backdrop, or null
+    uint32_t width, height;  // trace resolution
+    uint32_t out_width, out_height;
+    int format;              // SG_DISPLAY_RGBA8_SRGB or SG_DISPLAY_RGBA32F
+    void *out;               // out_width * out_height pixels
+    int automatic;           // use state->value instead of `manual`
+    const ExposureState *state;
+    float manual, bias, milky_way;
+};
+
+// Clears `histogram`, bins the central region of the accumulation and eases
+// state->value towards the metered exposure (when state->enabled).
+cudaError_t launch_exposure(const float4 *mean, uint32_t width, uint32_t height, uint32_t *histogram,
+                            ExposureState *state, cudaStream_t stream);
+cudaError_t launch_display(const DisplayParams &d, cudaStream_t stream);
+
 // Flat parameter space of the adjoint's gradient buffer:
 //   [0, kGradColor)          ring-table optical depths, slot * MAX_BINS + bin
 //   [kGradColor, kGradMap)   per body: ring albedo rgb, then body colour rgb

@@ -184,6 +184,23 @@ class PathTracer:
         check(self._lib.sg_read_backdrop(self._ctx, _ptr(out), 0, _stream_handle(stream)), self._ctx)
         return out
 
+    def display(self, size: tuple[int, int] | None = None, linear: bool = False, stream=None) -> np.ndarray:
+        """`PathTracer::display` (src/pathtracer.rs:1010-1014) into host
+        memory: the exposed, ACES-mapped accumulation at `size` (default the
+        trace size) as (height, width, 4) uint8 sRGB, or float32 linear."""
+        w, h = size if size is not None else self.size()
+        fmt = abi.DISPLAY_RGBA32F if linear else abi.DISPLAY_RGBA8_SRGB
+        out = np.zeros((h, w, 4), dtype=np.float32 if linear else np.uint8)
+        check(self._lib.sg_display(self._ctx, w, h, fmt, _ptr(out), 0, _stream_handle(stream)), self._ctx)
+        return out
+
+    def exposure(self, stream=None) -> float:
+        """The exposure the display uses: the eased automatic value, or the
+        manual one."""
+        v = C.c_float()
+        check(self._lib.sg_get_exposure(self._ctx, C.byref(v), _stream_handle(stream)), self._ctx)
+        return v.value
+
     def set_accumulation(self, pixels: np.ndarray, samples: int, sequence: int) -> None:
         p = np.ascontiguousarray(pixels, dtype=np.float32)
         check(self._lib.sg_set_accumulation(self._ctx, _ptr(p), 0, samples, sequence, None), self._ctx)
