@@ -459,7 +459,11 @@ SG_API int sg_get_tape(const sg_context *ctx, sg_tape *tape);
  * Sampling is detached (the estimator's random decisions are held fixed),
  * so the result is an unbiased estimate of the gradient of the expected
  * image. `on_device` applies to dl_dimage and to every gradient pointer.
- * The accumulation is not modified. Synchronises `stream`. */
+ * The accumulation is not modified. Synchronises `stream`. With the
+ * wavefront integrator (the default) the replay runs in the same stages as
+ * the forward, over a pool of up to 16 Mi paths (pool_paths of
+ * sg_set_integrator when set) holding about 1.1 KB of device memory each,
+ * allocated on first use; with the megakernel, one thread per pixel. */
 SG_API int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape,
                        const float *dl_dimage, int on_device, sg_gradients *grads,
                        void *stream);
