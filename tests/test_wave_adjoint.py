@@ -70,3 +70,13 @@ def test_staged_adjoint_equals_per_pixel_adjoint_on_the_terrain_scene():
     assert staged.albedo_map is not None
     assert_same_gradient(staged.albedo_map, ref.albedo_map, "albedo_map")
     assert_same_gradient(staged.body_color, ref.body_color, "body_color")
+
+
+def test_staged_adjoint_with_many_bodies():
+    """The 40-body cluster of test_wavefront.py (four stars, two rings)."""
+    from test_wavefront import cluster
+
+    wl = cluster(64, 48, 8)
+    staged, ref = both_adjoints(wl, 8, seed=14)
+    assert_same_gradient(staged.body_color, ref.body_color, "body_color")
+    assert_same_gradient(staged.ring_albedo, ref.ring_albedo, "ring_albedo")

@@ -107,3 +107,36 @@ def test_integrator_choice_is_validated():
         t.set_integrator("tiled")
     assert t.integrator()["integrator"] == "wavefront"  # the default
     t.close()
+
+
+def cluster(width=96, height=64, spp=8):
+    """40 bodies in telescope space: four stars (more than the three light
+    slots, so lights are found by scanning every body), two ringed planets,
+    34 diffuse spheres; seeded."""
+    from stargaze_b200.scene import body, frame, ringed
+
+    rng = np.random.default_rng(21)
+    f = frame()
+    f.globals.viewport[:] = [float(width), float(height), 1.0, width / height]
+    f.globals.cam_forward[3] = 0.6
+    bodies = []
+    for k in range(40):
+        c = [rng.uniform(-6, 6), rng.uniform(-4, 4), rng.uniform(-22, -7)]
+        if k < 4:
+            bodies.append(body(c, rng.uniform(0.2, 0.5), rng.uniform(5, 20, 3), True))
+        elif k < 6:
+            pole = rng.normal(size=3)
+            bodies.append(ringed(c, rng.uniform(0.5, 1.0), pole / np.linalg.norm(pole), 0.6))
+            bodies[-1].color[:] = list(rng.uniform(0.2, 0.8, 3))
+        else:
+            bodies.append(body(c, rng.uniform(0.2, 1.0), rng.uniform(0.1, 0.9, 3), False))
+    f.bodies = bodies
+    return W.Workload("cluster_40", f, width, height, spp, 8, {}, "40 bodies, 4 stars, 2 rings")
+
+
+def test_wavefront_equals_megakernel_with_many_bodies():
+    wl = cluster()
+    mega, _, _ = render(wl, "megakernel", 2, 8)
+    wave, stats, _ = render(wl, "wavefront", 2, 8)
+    assert np.abs(mega[:, :3]).sum() > 0
+    assert_same_image(wave, mega)
