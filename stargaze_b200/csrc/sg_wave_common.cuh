@@ -11,8 +11,16 @@ namespace sg {
 
 namespace {
 
+// Resident CTAs per SM the forward stages are compiled for (65536 / (256 x
+// this) registers per thread).
 #ifndef SG_WAVE_MIN_BLOCKS
 #define SG_WAVE_MIN_BLOCKS 4
+#endif
+#ifndef SG_WAVE_EXTEND_MIN_BLOCKS
+#define SG_WAVE_EXTEND_MIN_BLOCKS SG_WAVE_MIN_BLOCKS
+#endif
+#ifndef SG_WAVE_SHADE_MIN_BLOCKS
+#define SG_WAVE_SHADE_MIN_BLOCKS SG_WAVE_MIN_BLOCKS
 #endif
 
 // ---------------------------------------------------------------------------

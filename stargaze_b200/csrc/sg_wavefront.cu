@@ -48,7 +48,7 @@ namespace {
 // Stages
 // ---------------------------------------------------------------------------
 template <bool L, bool F>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_MIN_BLOCKS) wave_extend(const __grid_constant__ TraceParams P,
+__global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_extend(const __grid_constant__ TraceParams P,
                                                                             const __grid_constant__ WaveParams W,
                                                                             uint32_t t) {
     extern __shared__ float4 smem[];
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_MIN_BLOCKS) wave_extend(cons
 
 // Ring (R == true) or surface stage over its queue.
 template <bool L, bool F, bool R>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
+__global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
                                                                            const __grid_constant__ WaveParams W,
                                                                            uint32_t t) {
     extern __shared__ float4 smem[];
