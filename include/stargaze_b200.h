@@ -399,6 +399,12 @@ SG_API int sg_display(sg_context *ctx, uint32_t width, uint32_t height, int form
  * 1000), else options.exposure. Synchronises `stream`. */
 SG_API int sg_get_exposure(sg_context *ctx, float *exposure, void *stream);
 
+/* PathTracer::set_exposure_controls (src/pathtracer.rs:777-781): automatic
+ * metering on or off and the exposure compensation in stops. Display only:
+ * the accumulation is kept; the 60-frame settle of sg_needs_redraw
+ * restarts. */
+SG_API int sg_set_exposure_controls(sg_context *ctx, int automatic, float bias);
+
 /* Extension (measurement): with timing on, every wavefront stage launch is
  * bracketed by CUDA events and sg_encode waits for the dispatch to finish;
  * sg_get_stage_times then gives the milliseconds of the last timed

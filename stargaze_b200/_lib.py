@@ -51,6 +51,7 @@ _SIGNATURES = {
     "sg_set_stage_timing": (C.c_int, [_P, C.c_int]),
     "sg_display": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int, _P, C.c_int, _P]),
     "sg_get_exposure": (C.c_int, [_P, C.POINTER(C.c_float), _P]),
+    "sg_set_exposure_controls": (C.c_int, [_P, C.c_int, C.c_float]),
     "sg_get_stage_times": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "sg_get_tape": (C.c_int, [_P, C.POINTER(abi.Tape)]),
     "sg_backward": (C.c_int, [_P, C.POINTER(abi.FrameView), C.POINTER(abi.Tape), _P, C.c_int,

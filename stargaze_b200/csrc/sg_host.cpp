@@ -1114,6 +1114,15 @@ int sg_display(sg_context *ctx, uint32_t width, uint32_t height, int format, voi
     return SG_OK;
 }
 
+int sg_set_exposure_controls(sg_context *ctx, int automatic, float bias) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (!std::isfinite(bias)) return fail(ctx, SG_ERR_INVALID, "bias must be finite");
+    ctx->options.auto_exposure = automatic ? 1 : 0;
+    ctx->options.ev_bias = bias;
+    ctx->exposure_idle_frames = 0;
+    return SG_OK;
+}
+
 int sg_get_exposure(sg_context *ctx, float *exposure, void *stream_ptr) {
     if (!ctx || !exposure) return fail(ctx, SG_ERR_INVALID, "ctx or exposure is NULL");
     if (!(ctx->options.auto_exposure && ctx->exposure_was_enabled && ctx->exposure)) {

@@ -194,6 +194,10 @@ class PathTracer:
         check(self._lib.sg_display(self._ctx, w, h, fmt, _ptr(out), 0, _stream_handle(stream)), self._ctx)
         return out
 
+    def set_exposure_controls(self, automatic: bool, bias: float) -> None:
+        """`PathTracer::set_exposure_controls` (src/pathtracer.rs:777-781)."""
+        check(self._lib.sg_set_exposure_controls(self._ctx, int(bool(automatic)), float(bias)), self._ctx)
+
     def exposure(self, stream=None) -> float:
         """The exposure the display uses: the eased automatic value, or the
         manual one."""

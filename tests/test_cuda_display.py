@@ -91,7 +91,7 @@ def test_auto_exposure_keeps_metering_after_convergence():
     f.globals.viewport[:2] = [8.0, 8.0]
     t.encode(f)
     before = t.read_pixels()
-    t.update_options(auto_exposure=1)
+    t.set_exposure_controls(True, 0.0)
     for _ in range(64):
         t.encode(f)
     after = t.read_pixels()
