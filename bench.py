@@ -117,8 +117,27 @@ def profile_wavefront_rings_1080p():
     print(t.integrator(), flush=True)
 
 
+def profile_wavefront_terrain_640x360():
+    """Terrain workload at 640x360, 64 spp, through the wavefront integrator
+    with a 2 Mi-path pool (about 2 GB on the device with the terrain): two
+    frames."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl, _land = W.terrain_1080p(640, 360, 64)
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    t.set_integrator("wavefront", 1 << 21)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.encode(frame)
+    t.read_pixels()
+    print(t.integrator(), flush=True)
+
+
 PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512,
-                 "wavefront_rings_1080p": profile_wavefront_rings_1080p}
+                 "wavefront_rings_1080p": profile_wavefront_rings_1080p,
+                 "wavefront_terrain_640x360": profile_wavefront_terrain_640x360}
 
 
 def parse_args():
