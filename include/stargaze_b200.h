@@ -369,6 +369,25 @@ SG_API int sg_set_integrator(sg_context *ctx, int integrator, uint32_t pool_path
 SG_API int sg_get_integrator(const sg_context *ctx, int *integrator, uint32_t *pool_paths,
                              uint32_t *iterations);
 
+/* The camera-only sky backdrop of primary misses (pathtrace.wgsl:268-334,
+ * :1494-1508), bound in the reference as the `catalogue`, `sky_cells` and
+ * `milky_way` buffers (src/pathtracer.rs:319-368, the tables built by
+ * src/stars.rs:152-201 and src/sky.rs:103-119).
+ *   sg_upload_catalogue: `n` stars of 8 floats (direction xyz, sin^2 of the
+ *     angular radius, radiance rgb, unused) and the 256 x 128 cell table:
+ *     32,769 non-decreasing offsets (the first 0, the last the index count)
+ *     followed by the star indices of each cell. n = 0 removes it.
+ *   sg_upload_milky_way: width x height texels of 10-bit linear RGB
+ *     (r | g << 10 | b << 20), scaled by options.milky_way. A zero size
+ *     removes it.
+ * Unscattered camera paths then see the catalogue's discs and the Milky Way
+ * through their ring transmissions; the Milky Way is also accumulated apart
+ * (sg_read_backdrop) and its luminance is the accumulation's w channel.
+ * Uploads reset the accumulation. sg_backward rejects frames with a sky. */
+SG_API int sg_upload_catalogue(sg_context *ctx, const float *stars, uint32_t n, const uint32_t *cells,
+                               uint32_t n_cells);
+SG_API int sg_upload_milky_way(sg_context *ctx, const uint32_t *texels, uint32_t width, uint32_t height);
+
 /* ------------------------------------------------------------------ */
 /* Display without a graphics API                                      */
 /* ------------------------------------------------------------------ */

@@ -34,6 +34,10 @@ class Tables(C.Structure):
         ("map_width", C.c_uint32),
         ("map_height", C.c_uint32),
         ("map_extent", C.c_float),
+        ("catalogue", C.c_void_p),
+        ("catalogue_n", C.c_uint32),
+        ("sky_cells", C.c_void_p),
+        ("milky_way", C.c_void_p),
     ]
 
 
@@ -124,6 +128,9 @@ class TableSet:
         self.albedo: np.ndarray | None = None
         self.map_extent = 0.0
         self._ground = None
+        self.catalogue: np.ndarray | None = None
+        self.sky_cells: np.ndarray | None = None
+        self.milky: np.ndarray | None = None
 
     def upload(self, slot: int, tau) -> None:
         self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
@@ -142,6 +149,18 @@ class TableSet:
     def upload_albedo_map(self, albedo, extent_m: float) -> None:
         self.albedo = None if albedo is None else np.ascontiguousarray(albedo, dtype=np.float32)
         self.map_extent = float(extent_m)
+        self.version += 1
+
+    def upload_catalogue(self, stars, cells) -> None:
+        if stars is None:
+            self.catalogue = self.sky_cells = None
+        else:
+            self.catalogue = np.ascontiguousarray(stars, dtype=np.float32).reshape(-1, 8)
+            self.sky_cells = np.ascontiguousarray(cells, dtype=np.uint32)
+        self.version += 1
+
+    def upload_milky_way(self, texels) -> None:
+        self.milky = None if texels is None else np.ascontiguousarray(texels, dtype=np.uint32)
         self.version += 1
 
     def prepare(self, frame: Frame) -> None:
@@ -171,6 +190,12 @@ class TableSet:
             t.map_width = self.albedo.shape[1]
             t.map_height = self.albedo.shape[0]
             t.map_extent = self.map_extent
+        if self.catalogue is not None:
+            t.catalogue = self.catalogue.ctypes.data
+            t.catalogue_n = len(self.catalogue)
+            t.sky_cells = self.sky_cells.ctypes.data
+        if self.milky is not None:
+            t.milky_way = self.milky.ctypes.data
         return t
 
 
@@ -266,9 +291,19 @@ class OracleTracer:
         self.tables.upload_albedo_map(albedo, extent_m)
 
     def settings_for(self, frame: Frame, count: int) -> abi.Settings:
-        return frame.settings(self.width, self.height, self.samples_, count, self.opts.max_bounces,
-                              self.opts.noise_seed + self.sequence_, self.opts.milky_way,
-                              terrain_cells=self.tables.terrain_cells or 512)
+        s = frame.settings(self.width, self.height, self.samples_, count, self.opts.max_bounces,
+                           self.opts.noise_seed + self.sequence_, self.opts.milky_way,
+                           terrain_cells=self.tables.terrain_cells or 512)
+        if self.tables.milky is not None:
+            s.background[1] = float(self.tables.milky.shape[1])
+            s.background[2] = float(self.tables.milky.shape[0])
+        return s
+
+    def upload_catalogue(self, stars, cells) -> None:
+        self.tables.upload_catalogue(stars, cells)
+
+    def upload_milky_way(self, texels) -> None:
+        self.tables.upload_milky_way(texels)
 
     def encode(self, frame: Frame, stream=None, rows=None) -> None:
         if len(frame.bodies) > abi.BODY_CAPACITY:

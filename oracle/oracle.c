@@ -1240,6 +1240,78 @@ static void roulette_tangent(v3 t, float s, int survived, v3 *dt_full, float *sc
 }
 
 /* ---------------------------------------------------------------- */
+/* Camera-only sky backdrop: pathtrace.wgsl:268-334                   */
+/* ---------------------------------------------------------------- */
+static v3 cam_right(const scene *S) { return V(S->s->g.cam_right[0], S->s->g.cam_right[1], S->s->g.cam_right[2]); }
+static v3 cam_up(const scene *S) { return V(S->s->g.cam_up[0], S->s->g.cam_up[1], S->s->g.cam_up[2]); }
+static v3 cam_fwd(const scene *S) { return V(S->s->g.cam_forward[0], S->s->g.cam_forward[1], S->s->g.cam_forward[2]); }
+
+/* world_direction: :268-271 */
+static v3 world_direction(const scene *S, v3 d) {
+    return vnormalize(vsub(vadd(vmul(cam_right(S), d.x), vmul(cam_up(S), d.y)), vmul(cam_fwd(S), d.z)));
+}
+
+/* inside_star_dot: :118-128 */
+static int inside_star_dot(const scene *S, v3 view, v3 star) {
+    v3 sv = V(vdot(star, cam_right(S)), vdot(star, cam_up(S)), -vdot(star, cam_fwd(S)));
+    if (sv.z >= 0.0f) return 0;
+    float dx = view.x / -view.z - sv.x / -sv.z, dy = view.y / -view.z - sv.y / -sv.z;
+    float scale = S->s->g.viewport[1] / (2.0f * S->s->g.cam_forward[3]);
+    float px = dx * scale, py = dy * scale;
+    return px * px + py * py <= STAR_DOT_PIXELS * STAR_DOT_PIXELS;
+}
+
+/* environment: :273-300 (primary rays only) */
+static v3 environment(const scene *S, v3 view) {
+    v3 light = V(0, 0, 0);
+    const oracle_tables *t = S->t;
+    if (!t || !t->catalogue || t->catalogue_n == 0u) return light;
+    v3 dir = world_direction(S, view);
+    float phi = atan2f(dir.y, dir.x) + PI_F;
+    float theta = acosf(clampf_(dir.z, -1.0f, 1.0f));
+    uint32_t x = (uint32_t)(phi * (256.0f / TAU_F));
+    uint32_t y = (uint32_t)(theta * (128.0f / PI_F));
+    if (x > 255u) x = 255u;
+    if (y > 127u) y = 127u;
+    uint32_t cell = y * 256u + x;
+    for (uint32_t j = t->sky_cells[cell]; j < t->sky_cells[cell + 1u]; j++) {
+        const float *star = t->catalogue + 8u * t->sky_cells[32769u + j];
+        v3 sdir = V(star[0], star[1], star[2]);
+        v3 perp = vcross(dir, sdir);
+        if (vdot(dir, sdir) > 0.0f && vdot(perp, perp) <= star[3] && inside_star_dot(S, view, sdir))
+            light = vadd(light, V(star[4], star[5], star[6]));
+    }
+    return light;
+}
+
+/* milky_way_texel, milky_way: :302-334 */
+static v3 milky_way_texel(const scene *S, int x, int y) {
+    int w = (int)S->s->background[1], h = (int)S->s->background[2];
+    x = (x + w) % w;
+    y = y < 0 ? 0 : (y > h - 1 ? h - 1 : y);
+    uint32_t packed = S->t->milky_way[(uint32_t)(y * w + x)];
+    return vdivs(V((float)(packed & 1023u), (float)((packed >> 10) & 1023u), (float)((packed >> 20) & 1023u)),
+                 1023.0f);
+}
+static v3 milky_way(const scene *S, v3 view) {
+    if (S->s->background[0] == 0.0f || !S->t || !S->t->milky_way) return V(0, 0, 0);
+    v3 dir = world_direction(S, view);
+    v3 pole = vnormalize(V(0.35f, 0.82f, 0.45f));
+    float a = -1.0f / (1.0f + pole.z);
+    v3 right = V(pole.x * pole.y * a, 1.0f + pole.y * pole.y * a, -pole.y);
+    v3 forward = vcross(pole, right);
+    float longitude = atan2f(vdot(dir, forward), vdot(dir, right));
+    float u = 0.5f - longitude / TAU_F;
+    float v = acosf(clampf_(vdot(dir, pole), -1.0f, 1.0f)) / PI_F;
+    float px = u * S->s->background[1] - 0.5f, py = v * S->s->background[2] - 0.5f;
+    int lx = (int)floorf(px), ly = (int)floorf(py);
+    float wx = px - floorf(px), wy = py - floorf(py);
+    v3 top = vadd(vmul(milky_way_texel(S, lx, ly), 1.0f - wx), vmul(milky_way_texel(S, lx + 1, ly), wx));
+    v3 bot = vadd(vmul(milky_way_texel(S, lx, ly + 1), 1.0f - wx), vmul(milky_way_texel(S, lx + 1, ly + 1), wx));
+    return vmul(vadd(vmul(top, 1.0f - wy), vmul(bot, wy)), S->s->background[0]);
+}
+
+/* ---------------------------------------------------------------- */
 /* trace: pathtrace.wgsl:1347-1617 (airless)                         */
 /* With a direction D (adjoint check), dout receives the tangent of  */
 /* the returned radiance along D: every sampling decision, pdf, MIS   */
@@ -1247,7 +1319,8 @@ static void roulette_tangent(v3 t, float s, int survived, v3 *dt_full, float *sc
 /* material factors (ring tables and albedo, colours, albedo map)     */
 /* carry tangents. The ring-indirect cap is differentiated exactly.   */
 /* ---------------------------------------------------------------- */
-static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4], const oracle_direction *D,
+/* out[0..3]: radiance and the backdrop's luminance; out[4..6]: the backdrop. */
+static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], const oracle_direction *D,
                   float dout[3]) {
     const sg_settings *st = S->s;
     ray_t ray = initial;
@@ -1410,8 +1483,14 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4], co
             continue;
         }
         if (hit.index == MISS) {
-            /* environment(): the catalogue is empty; milky_way(): no map is
-             * bound, so both contribute zero radiance (pathtrace.wgsl:1494-1508). */
+            /* pathtrace.wgsl:1494-1508: background stars and the Milky Way
+             * along unscattered camera paths (straight-through ring
+             * crossings included); the backdrop is also returned apart. */
+            if (depth == 0u) {
+                radiance = vadd(radiance, vmulv(throughput, environment(S, ray.dir)));
+                backdrop = vmulv(milky_way(S, ray.dir), throughput);
+                radiance = vadd(radiance, backdrop);
+            }
             break;
         }
         int local = hit.index >= LOCAL_BASE;
@@ -1554,6 +1633,9 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[4], co
     out[1] = radiance.y;
     out[2] = radiance.z;
     out[3] = lum(backdrop);
+    out[4] = backdrop.x;
+    out[5] = backdrop.y;
+    out[6] = backdrop.z;
     if (dout) {
         dout[0] = dfinal.x;
         dout[1] = dfinal.y;
@@ -1590,7 +1672,7 @@ static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
 }
 #define check_frame(s) check_frame_t((s), tables)
 
-static void sample_pixel_d(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4],
+static void sample_pixel_d(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[7],
                            const oracle_direction *D, float dout[3]) {
     uint32_t width = (uint32_t)S->s->g.viewport[0];
     uint32_t pixel = y * width + x;
@@ -1601,7 +1683,7 @@ static void sample_pixel_d(const scene *S, uint32_t x, uint32_t y, uint32_t s, f
     ray.anchor = MISS;
     trace(S, ray, &rng, out, D, dout);
 }
-static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[4]) {
+static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[7]) {
     sample_pixel_d(S, x, y, s, out, NULL, NULL);
 }
 
@@ -1642,19 +1724,19 @@ int oracle_dispatch(const sg_settings *settings, const sg_sphere *bodies, const 
         uint32_t x = (uint32_t)(k % width);
         uint32_t y = y0 + (uint32_t)(k / width);
         uint32_t pixel = y * width + x;
-        float sum[4] = {0, 0, 0, 0};
-        /* The backdrop rgb sum stays zero: no Milky Way map is bound. */
+        float sum[4] = {0, 0, 0, 0}, bsum[3] = {0, 0, 0};
         for (uint32_t s = 0; s < z; s++) {
-            float r[4];
+            float r[7];
             if (S.ev) S.ev->samples++;
             sample_pixel(&S, x, y, s, r);
             for (int c = 0; c < 4; c++) sum[c] += r[c];
+            for (int c = 0; c < 3; c++) bsum[c] += r[4 + c];
         }
         uint32_t old_count = settings->counts[1];
         uint32_t new_count = old_count + z;
         float mean[4], bmean[3];
         for (int c = 0; c < 4; c++) mean[c] = sum[c] / (float)z;
-        for (int c = 0; c < 3; c++) bmean[c] = 0.0f / (float)z;
+        for (int c = 0; c < 3; c++) bmean[c] = bsum[c] / (float)z;
         if (old_count > 0u) {
             float w = (float)z / (float)new_count;
             for (int c = 0; c < 4; c++) {
@@ -1707,7 +1789,7 @@ int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies, const o
         uint32_t y = y0 + (uint32_t)(k / width);
         size_t pixel = (size_t)y * width + x;
         for (uint32_t s = 0; s < z; s++) {
-            float r[4], d[3];
+            float r[7], d[3];
             sample_pixel_d(&S, x, y, s, r, direction, d);
             for (int c = 0; c < 4; c++) primal[4 * pixel + c] += r[c];
             for (int c = 0; c < 3; c++) tangent[4 * pixel + c] += d[c];
@@ -1721,7 +1803,9 @@ int oracle_trace_sample(const sg_settings *settings, const sg_sphere *bodies, co
     int status = check_frame(settings);
     if (status != SG_OK) return status;
     scene S = {settings, bodies, tables, NULL};
-    sample_pixel(&S, x, y, s, out);
+    float r[7];
+    sample_pixel(&S, x, y, s, r);
+    for (int c = 0; c < 4; c++) out[c] = r[c];
     return SG_OK;
 }
 

@@ -43,6 +43,14 @@ typedef struct oracle_tables {
     const float *albedo_map;
     uint32_t map_width, map_height;
     float map_extent;
+    /* Camera-only sky backdrop (pathtrace.wgsl:268-334): catalogue rows of
+     * 8 floats (direction, sin^2 radius, radiance, unused) with the 256 x 128
+     * cell table (32,769 offsets, then indices), and the RGB10 Milky Way
+     * panorama (its size in settings.background.yz). NULL disables each. */
+    const float *catalogue;
+    uint32_t catalogue_n;
+    const uint32_t *sky_cells;
+    const uint32_t *milky_way;
 } oracle_tables;
 
 /* Floats of the reference terrain layout for `cells` cells per side

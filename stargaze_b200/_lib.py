@@ -50,6 +50,8 @@ _SIGNATURES = {
     "sg_get_integrator": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "sg_set_stage_timing": (C.c_int, [_P, C.c_int]),
     "sg_display": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int, _P, C.c_int, _P]),
+    "sg_upload_catalogue": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32]),
+    "sg_upload_milky_way": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32]),
     "sg_get_exposure": (C.c_int, [_P, C.POINTER(C.c_float), _P]),
     "sg_set_exposure_controls": (C.c_int, [_P, C.c_int, C.c_float]),
     "sg_get_stage_times": (C.c_int, [_P, C.POINTER(C.c_float)]),

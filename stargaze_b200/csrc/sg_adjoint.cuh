@@ -104,6 +104,14 @@ struct GradSink {
 // The forward integrator: no hooks.
 struct NoGrad {
     static constexpr bool adjoint = false;
+    static constexpr bool sky = true;  // surface_vertex shades an escaped path's sky
+};
+
+// The wavefront's shade stages: no hooks, and no escaped paths (extend ends
+// those), so surface_vertex's miss branch never runs there.
+struct StageGrad {
+    static constexpr bool adjoint = false;
+    static constexpr bool sky = false;
 };
 
 // A Russian-roulette decision after the cap vertex (pathtrace.wgsl:
@@ -132,6 +140,7 @@ struct PrbLists {
 // pass 1 also records the summary pass 2 needs (`pass2` false).
 struct Prb {
     static constexpr bool adjoint = true;
+    static constexpr bool sky = false;  // sg_backward rejects frames with a sky
     bool pass2;
     // Pass 1's summary.
     float cap;

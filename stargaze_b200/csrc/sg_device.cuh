@@ -650,6 +650,87 @@ static __device__ SG_HELPER Shine ringshine(Scene S, Counter<C, L, F> K, uint32_
     return Shine{shine * sp.scale, rng};
 }
 
+// ---------------------------------------------------------------------------
+// Camera-only sky backdrop (pathtrace.wgsl:268-334): catalogue star discs and
+// the Milky Way panorama, seen along unscattered camera paths.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSkyGridW = 256, kSkyGridH = 128;
+
+// world_direction (pathtrace.wgsl:268-271).
+__device__ __forceinline__ float3 world_direction(const sg_settings *s, float3 d) {
+    const float3 r = f3(s->g.cam_right[0], s->g.cam_right[1], s->g.cam_right[2]);
+    const float3 u = f3(s->g.cam_up[0], s->g.cam_up[1], s->g.cam_up[2]);
+    const float3 f = f3(s->g.cam_forward[0], s->g.cam_forward[1], s->g.cam_forward[2]);
+    return normalize(r * d.x + u * d.y - f * d.z);
+}
+
+// inside_star_dot (pathtrace.wgsl:118-128): within kStarDotPixels of the
+// star's projected centre.
+__device__ __forceinline__ bool inside_star_dot(const sg_settings *s, float3 view, float3 star) {
+    const float3 r = f3(s->g.cam_right[0], s->g.cam_right[1], s->g.cam_right[2]);
+    const float3 u = f3(s->g.cam_up[0], s->g.cam_up[1], s->g.cam_up[2]);
+    const float3 f = f3(s->g.cam_forward[0], s->g.cam_forward[1], s->g.cam_forward[2]);
+    const float3 sv = f3(dot(star, r), dot(star, u), -dot(star, f));
+    if (sv.z >= 0.0f) return false;
+    const float dx = view.x / -view.z - sv.x / -sv.z, dy = view.y / -view.z - sv.y / -sv.z;
+    const float scale = s->g.viewport[1] / (2.0f * s->g.cam_forward[3]);
+    const float px = dx * scale, py = dy * scale;
+    return px * px + py * py <= kStarDotPixels * kStarDotPixels;
+}
+
+// environment (pathtrace.wgsl:273-300) of a primary ray: the catalogue
+// discs listed in the direction's grid cell.
+static __device__ __noinline__ float3 environment(const TraceParams *P, float3 view) {
+    float3 light = f3(0.0f, 0.0f, 0.0f);
+    if (P->catalogue_n == 0u) return light;
+    const float3 dir = world_direction(&P->s, view);
+    const float phi = atan2f(dir.y, dir.x) + kPi;
+    const float theta = acosf(clampf(dir.z, -1.0f, 1.0f));
+    const uint32_t x = min((uint32_t)(phi * (256.0f / kTau)), kSkyGridW - 1u);
+    const uint32_t y = min((uint32_t)(theta * (128.0f / kPi)), kSkyGridH - 1u);
+    const uint32_t cell = y * kSkyGridW + x;
+    const uint32_t *cells = P->sky_cells;
+    for (uint32_t j = cells[cell]; j < cells[cell + 1u]; ++j) {
+        const uint32_t k = cells[kSkyGridW * kSkyGridH + 1u + j];
+        const float4 sd = P->catalogue[2u * k];
+        const float3 sdir = xyz(sd);
+        const float3 perp = cross(dir, sdir);
+        if (dot(dir, sdir) > 0.0f && dot(perp, perp) <= sd.w && inside_star_dot(&P->s, view, sdir))
+            light = light + xyz(P->catalogue[2u * k + 1u]);
+    }
+    return light;
+}
+
+// milky_way_texel / milky_way (pathtrace.wgsl:302-334): the panorama in
+// galactic coordinates (pole normalize(0.35, 0.82, 0.45), Duff basis),
+// bilinear, times the backdrop brightness.
+__device__ __forceinline__ float3 milky_way_texel(const TraceParams *P, int x, int y) {
+    const int w = (int)P->s.background[1], h = (int)P->s.background[2];
+    x = (x + w) % w;
+    y = min(max(y, 0), h - 1);
+    const uint32_t t = P->milky_way[(uint32_t)(y * w + x)];
+    return f3((float)(t & 1023u), (float)((t >> 10) & 1023u), (float)((t >> 20) & 1023u)) / 1023.0f;
+}
+static __device__ __noinline__ float3 milky_way(const TraceParams *P, float3 view) {
+    if (P->s.background[0] == 0.0f || !P->milky_way) return f3(0.0f, 0.0f, 0.0f);
+    const float3 dir = world_direction(&P->s, view);
+    const float3 pole = normalize(f3(0.35f, 0.82f, 0.45f));
+    const float a = -1.0f / (1.0f + pole.z);
+    const float3 right = f3(pole.x * pole.y * a, 1.0f + pole.y * pole.y * a, -pole.y);
+    const float3 forward = cross(pole, right);
+    const float longitude = atan2f(dot(dir, forward), dot(dir, right));
+    const float u = 0.5f - longitude / kTau;
+    const float v = acosf(clampf(dot(dir, pole), -1.0f, 1.0f)) / kPi;
+    const float px = u * P->s.background[1] - 0.5f, py = v * P->s.background[2] - 0.5f;
+    const float fx = floorf(px), fy = floorf(py);
+    const int lx = (int)fx, ly = (int)fy;
+    const float wx = px - fx, wy = py - fy;
+    const float3 t00 = milky_way_texel(P, lx, ly), t10 = milky_way_texel(P, lx + 1, ly);
+    const float3 t01 = milky_way_texel(P, lx, ly + 1), t11 = milky_way_texel(P, lx + 1, ly + 1);
+    const float3 top = t00 * (1.0f - wx) + t10 * wx, bot = t01 * (1.0f - wx) + t11 * wx;
+    return (top * (1.0f - wy) + bot * wy) * P->s.background[0];
+}
+
 // point_gain (pathtrace.wgsl:1341-1345).
 __device__ __forceinline__ float point_gain(const sg_settings *s, float extent, float distance) {
     const float pixel = 2.0f * s->g.cam_forward[3] / fmaxf(s->g.viewport[1], 1.0f);

@@ -92,6 +92,15 @@ struct sg_context {
     sg::WaveCounters *wave_pinned = nullptr;
     cudaEvent_t wave_ready = nullptr;
     uint32_t wave_iterations = 0;           // stage iterations of the last dispatch
+    // Sky backdrop: catalogue (2 float4 per star), cell table, panorama.
+    float4 *catalogue = nullptr;
+    uint32_t catalogue_n = 0;
+    uint32_t *sky_cells = nullptr;
+    uint32_t *milky_way = nullptr;
+    uint32_t milky_width = 0, milky_height = 0;
+    float4 *sky_samples = nullptr;          // wavefront: per-sample backdrop + totals
+    size_t sky_samples_size = 0;
+    bool backdrop_written = false;          // the backdrop buffer holds a sky
     // Display: the exposure state and histogram of the metering.
     sg::ExposureState *exposure = nullptr;
     uint32_t *histogram = nullptr;
@@ -296,8 +305,8 @@ sg_settings pack_settings(const sg_context *ctx, const sg_frame *frame, uint32_t
     s.counts[2] = count;
     s.counts[3] = ctx->options.max_bounces;
     s.background[0] = ctx->options.milky_way;
-    s.background[1] = kMilkyWayWidth;
-    s.background[2] = kMilkyWayHeight;
+    s.background[1] = ctx->milky_way ? (float)ctx->milky_width : kMilkyWayWidth;
+    s.background[2] = ctx->milky_way ? (float)ctx->milky_height : kMilkyWayHeight;
     s.background[3] = kPointSourceGain;
     return s;
 }
@@ -351,6 +360,12 @@ int upload_bodies(sg_context *ctx, const sg_frame *frame, cudaStream_t stream) {
     return SG_OK;
 }
 
+// Whether primary misses see a sky: a catalogue, or a panorama with a
+// positive brightness.
+bool sky_on(const sg_context *ctx) {
+    return ctx->catalogue_n > 0u || (ctx->milky_way && ctx->options.milky_way > 0.0f);
+}
+
 sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     sg::TraceParams p;
     std::memset(&p, 0, sizeof(p));
@@ -381,6 +396,12 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.map_height = ctx->map_height;
     p.map_extent = ctx->map_extent;
     p.fp64_sites = ctx->fp64_sites ? 1u : 0u;
+    p.catalogue = ctx->catalogue;
+    p.sky_cells = ctx->sky_cells;
+    p.catalogue_n = ctx->catalogue_n;
+    p.milky_way = ctx->milky_way;
+    p.sky_on = sky_on(ctx) ? 1u : 0u;
+    p.backdrop = ctx->backdrop;
     return p;
 }
 
@@ -481,6 +502,10 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->adjoint_slots);
     cudaFree(ctx->exposure);
     cudaFree(ctx->histogram);
+    cudaFree(ctx->catalogue);
+    cudaFree(ctx->sky_cells);
+    cudaFree(ctx->milky_way);
+    cudaFree(ctx->sky_samples);
     if (ctx->wave_pinned) cudaFreeHost(ctx->wave_pinned);
     if (ctx->wave_ready) cudaEventDestroy(ctx->wave_ready);
     for (cudaEvent_t e : ctx->stage_marks.events) cudaEventDestroy(e);
@@ -532,6 +557,72 @@ int sg_upload_albedo_map(sg_context *ctx, const float *albedo, uint32_t width, u
     ctx->map_width = width;
     ctx->map_height = height;
     ctx->map_extent = extent_m;
+    ctx->table_version += 1;
+    return SG_OK;
+}
+
+int sg_upload_catalogue(sg_context *ctx, const float *stars, uint32_t n, const uint32_t *cells, uint32_t n_cells) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    DeviceGuard guard(ctx->device);
+    constexpr uint32_t kOffsets = 256u * 128u + 1u;
+    if (n == 0) {
+        cudaDeviceSynchronize();
+        cudaFree(ctx->catalogue);
+        cudaFree(ctx->sky_cells);
+        ctx->catalogue = nullptr;
+        ctx->sky_cells = nullptr;
+        ctx->catalogue_n = 0;
+        ctx->table_version += 1;
+        return SG_OK;
+    }
+    if (!stars || !cells || n > (1u << 20) || n_cells < kOffsets)
+        return fail(ctx, SG_ERR_INVALID, "catalogue needs 1..2^20 stars and a cell table of at least 32,769 words");
+    if (cells[0] != 0u) return fail(ctx, SG_ERR_INVALID, "the first cell offset must be 0");
+    for (uint32_t k = 1; k < kOffsets; ++k)
+        if (cells[k] < cells[k - 1]) return fail(ctx, SG_ERR_INVALID, "cell offsets must not decrease");
+    if (cells[kOffsets - 1] != n_cells - kOffsets)
+        return fail(ctx, SG_ERR_INVALID, "the last cell offset must equal the number of indices");
+    for (uint32_t k = kOffsets; k < n_cells; ++k)
+        if (cells[k] >= n) return fail(ctx, SG_ERR_INVALID, "a cell lists a star beyond the catalogue");
+    for (size_t k = 0; k < (size_t)n * 8u; ++k)
+        if (!std::isfinite(stars[k])) return fail(ctx, SG_ERR_INVALID, "catalogue values must be finite");
+    cudaDeviceSynchronize();
+    cudaFree(ctx->catalogue);
+    cudaFree(ctx->sky_cells);
+    ctx->catalogue = nullptr;
+    ctx->sky_cells = nullptr;
+    ctx->catalogue_n = 0;
+    SG_CUDA(ctx, cudaMalloc(&ctx->catalogue, (size_t)n * 2u * sizeof(float4)));
+    SG_CUDA(ctx, cudaMalloc(&ctx->sky_cells, (size_t)n_cells * sizeof(uint32_t)));
+    SG_CUDA(ctx, cudaMemcpy(ctx->catalogue, stars, (size_t)n * 2u * sizeof(float4), cudaMemcpyHostToDevice));
+    SG_CUDA(ctx, cudaMemcpy(ctx->sky_cells, cells, (size_t)n_cells * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ctx->catalogue_n = n;
+    ctx->table_version += 1;
+    return SG_OK;
+}
+
+int sg_upload_milky_way(sg_context *ctx, const uint32_t *texels, uint32_t width, uint32_t height) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    DeviceGuard guard(ctx->device);
+    if (width == 0 || height == 0) {
+        cudaDeviceSynchronize();
+        cudaFree(ctx->milky_way);
+        ctx->milky_way = nullptr;
+        ctx->milky_width = ctx->milky_height = 0;
+        ctx->table_version += 1;
+        return SG_OK;
+    }
+    if (!texels || width > 16384 || height > 16384)
+        return fail(ctx, SG_ERR_INVALID, "the panorama needs texels and at most 16384 x 16384 of them");
+    for (size_t k = 0; k < (size_t)width * height; ++k)
+        if (texels[k] >> 30) return fail(ctx, SG_ERR_INVALID, "panorama texels are 3 x 10-bit");
+    cudaDeviceSynchronize();
+    cudaFree(ctx->milky_way);
+    ctx->milky_way = nullptr;
+    SG_CUDA(ctx, cudaMalloc(&ctx->milky_way, (size_t)width * height * sizeof(uint32_t)));
+    SG_CUDA(ctx, cudaMemcpy(ctx->milky_way, texels, (size_t)width * height * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ctx->milky_width = width;
+    ctx->milky_height = height;
     ctx->table_version += 1;
     return SG_OK;
 }
@@ -659,6 +750,18 @@ static int ensure_wave(sg_context *ctx, uint32_t samples, sg::WaveParams &w) {
     w.results = ctx->wave_results;
     w.totals = ctx->wave_results + (size_t)chunk * pixels;
     w.chunk_samples = chunk;
+    w.sky_results = w.sky_totals = nullptr;
+    if (sky_on(ctx)) {
+        if (result_bytes > ctx->sky_samples_size) {
+            cudaFree(ctx->sky_samples);
+            ctx->sky_samples = nullptr;
+            ctx->sky_samples_size = 0;
+            SG_CUDA(ctx, cudaMalloc(&ctx->sky_samples, result_bytes));
+            ctx->sky_samples_size = result_bytes;
+        }
+        w.sky_results = ctx->sky_samples;
+        w.sky_totals = ctx->sky_samples + (size_t)chunk * pixels;
+    }
     return SG_OK;
 }
 
@@ -730,6 +833,12 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
         status = upload_bodies(ctx, frame, stream);
         if (status != SG_OK) return status;
         sg::TraceParams p = make_params(ctx, s);
+        // A backdrop left by an earlier sky (the history has reset since).
+        if (!p.sky_on && ctx->backdrop_written) {
+            SG_CUDA(ctx, cudaMemsetAsync(ctx->backdrop, 0, (size_t)ctx->width * ctx->height * sizeof(float4), stream));
+            ctx->backdrop_written = false;
+        }
+        if (p.sky_on) ctx->backdrop_written = true;
         if (events) {
             SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
             p.events = ctx->events;
@@ -1187,6 +1296,8 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         return fail(ctx, SG_ERR_INVALID, "tape runs must hold 1..SG_MAX_SAMPLES samples in total");
     int status = validate_frame(ctx, frame);
     if (status != SG_OK) return status;
+    if (sky_on(ctx))
+        return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate the sky backdrop; remove the catalogue and panorama");
     if (key_hash(history_key(ctx, frame)) != tape->history_hash)
         return fail(ctx, SG_ERR_STATE, "frame, options or tables differ from the ones the tape was recorded with");
     grads->dropped = 0;

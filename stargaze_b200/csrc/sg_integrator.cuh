@@ -34,6 +34,7 @@ struct Path {
     uint32_t iterations;
     uint32_t rng;
     bool point_gained;
+    float3 backdrop;  // Milky Way radiance reached by an unscattered camera path
 };
 
 // camera_direction (pathtrace.wgsl:1619-1626).
@@ -67,10 +68,11 @@ __device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counte
     p.shine_body = kMiss;
     p.iterations = 0;
     p.point_gained = false;
+    p.backdrop = f3(0.0f, 0.0f, 0.0f);
 }
 
 // The ring-indirect cap after the loop (pathtrace.wgsl:1609-1615); W holds
-// backdrop luminance, zero without a Milky Way map.
+// the backdrop's luminance (for exposure metering and the display).
 __device__ __forceinline__ float4 finish_path(const Path &p) {
     float3 radiance = p.radiance;
     if (p.ring_cap < 1.0e29f) {
@@ -78,7 +80,41 @@ __device__ __forceinline__ float4 finish_path(const Path &p) {
         const float l = luminance(indirect);
         if (l > p.ring_cap) radiance = p.ring_base + indirect * (p.ring_cap / l);
     }
-    return make_float4(radiance.x, radiance.y, radiance.z, 0.0f);
+    return make_float4(radiance.x, radiance.y, radiance.z, luminance(p.backdrop));
+}
+
+// A camera path that escapes unscattered (pathtrace.wgsl:1494-1508): the
+// catalogue discs of its direction and the Milky Way, through its
+// throughput (null ring crossings attenuate both). Scattered paths see
+// neither. Draws no random numbers.
+struct SkyTerms {
+    float3 env;       // throughput x catalogue discs
+    float3 backdrop;  // Milky Way x throughput
+};
+// Out of line: it runs only where a camera path escapes, and keeps the
+// extend stage's register allocation that of the sky-less frames.
+static __device__ __noinline__ SkyTerms sky_terms(const TraceParams *P, float3 dir, float3 throughput) {
+    return SkyTerms{throughput * environment(P, dir), milky_way(P, dir) * throughput};
+}
+__device__ __forceinline__ void sky_miss(const Scene &S, Path &p) {
+    if (!S.p->sky_on || p.depth != 0u) return;
+    const SkyTerms t = sky_terms(S.p, p.ray.d, p.throughput);
+    p.radiance = p.radiance + t.env;
+    p.backdrop = t.backdrop;
+    p.radiance = p.radiance + p.backdrop;
+}
+
+// The backdrop accumulation (pathtrace.wgsl:1654-1674): the dispatch's mean
+// folded into the running mean.
+__device__ __forceinline__ void fold_backdrop(const TraceParams &P, uint32_t pixel, float3 sum) {
+    const float z = (float)P.s.counts[2];
+    float3 mean = sum / z;
+    if (P.s.counts[1] > 0u) {
+        const float4 old = P.backdrop[pixel];
+        const float w = z / (float)(P.s.counts[1] + P.s.counts[2]);
+        mean = f3(old.x + (mean.x - old.x) * w, old.y + (mean.y - old.y) * w, old.z + (mean.z - old.z) * w);
+    }
+    P.backdrop[pixel] = make_float4(mean.x, mean.y, mean.z, 0.0f);
 }
 
 // What extend() finds along a path's current ray.
@@ -267,9 +303,12 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
     float &previous_pdf = p.previous_pdf;
     Ray &previous_vertex = p.previous_vertex;
     {
-        // Miss: the catalogue is empty and no Milky Way map is bound, so the
-        // environment contributes nothing (pathtrace.wgsl:1494-1508).
-        if (hit.index == kMiss) return true;
+        // Miss: the sky backdrop of an unscattered camera path (the adjoint
+        // does not differentiate it; sg_backward rejects such frames).
+        if (hit.index == kMiss) {
+            if constexpr (G::sky) sky_miss(S, p);
+            return true;
+        }
 
         const uint32_t bi = hit.index;
         // Local ids (host sphere, terrain, props) never index the bodies;

@@ -37,6 +37,16 @@ struct TraceParams {
     uint32_t map_width, map_height;
     float map_extent;
     uint32_t fp64_sites;  // ring plane, host sphere and 5 mm offset in FP64
+    // Camera-only sky backdrop (pathtrace.wgsl:268-334): the star catalogue
+    // (2 float4 per star: direction + sin^2 radius, radiance) with its
+    // 256 x 128 cell table (32,769 offsets, then indices), and the Milky Way
+    // panorama (RGB10 texels); `backdrop` receives its running mean.
+    const float4 *catalogue;
+    const uint32_t *sky_cells;
+    uint32_t catalogue_n;
+    const uint32_t *milky_way;
+    uint32_t sky_on;  // catalogue or panorama bound (and the panorama's brightness > 0)
+    float4 *backdrop;
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,
@@ -87,6 +97,8 @@ struct WaveParams {
     WaveCounters *counters;   // kWaveCounterSets sets
     float4 *results;          // chunk_samples planes of width * height radiance samples
     float4 *totals;           // per-pixel running sums between chunks
+    float4 *sky_results;      // as results, the backdrop of each sample (null: no sky)
+    float4 *sky_totals;       // as totals, for the backdrop
     uint32_t pool;            // path slots
     uint32_t tiles_x, tiles_y;
     uint32_t chunk_first;     // first sample of the chunk within the dispatch

@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
         // bounce) far more often than with per-lane path regeneration, which
         // measured 20 % slower on the ring workload.
         float4 total = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float3 sky = f3(0.0f, 0.0f, 0.0f);
         Path path;
         NoGrad nograd;
         for (uint32_t smp = 0; smp < z; ++smp) {
@@ -61,7 +62,9 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
             total.y += r.y;
             total.z += r.z;
             total.w += r.w;
+            sky = sky + path.backdrop;
         }
+        if (P.sky_on) fold_backdrop(P, pixel, sky);
         // Progressive accumulation: the WGSL keeps a running mean
         // (pathtrace.wgsl:1662-1674); here the per-pixel sum is compensated
         // (Kahan) and the mean re-derived from it.

@@ -57,6 +57,7 @@ __device__ __forceinline__ uint32_t load_ray_part(const float4 *st, uint32_t poo
     p.point_gained = (it >> 31) != 0u;
     p.depth = dn & 0xffffu;
     p.null_crossings = dn >> 16;
+    p.backdrop = f3(0.0f, 0.0f, 0.0f);  // set only where a path escapes, which ends it
     return __float_as_uint(g.z);
 }
 

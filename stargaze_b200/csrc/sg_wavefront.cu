@@ -117,11 +117,17 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                     H[2 * W.pool + i] = make_float4(__uint_as_float(e.hit.index), __uint_as_float(e.ring.index),
                                                     e.hit.delta, e.disc_scale);
                 } else {
-                    // Ended at the iteration bound, or escaped: the
-                    // environment contributes nothing (surface_vertex's
-                    // miss). A new path's radiance is still zero.
+                    // Ended at the iteration bound, or escaped (then the sky
+                    // backdrop of an unscattered camera path, as
+                    // surface_vertex's miss). A new path's radiance is still
+                    // zero.
                     if (!fresh) load_radiance_part(st, W.pool, i, p);
+                    if (alive && P.sky_on) {
+                        if (!fresh) p.throughput = xyz4(st[2 * W.pool + i]);
+                        sky_miss(S, p);
+                    }
                     W.results[slot] = finish_path(p);
+                    if (W.sky_results) W.sky_results[slot] = pack3(p.backdrop, 0.0f);
                 }
             }
         }
@@ -146,7 +152,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
     if (blockIdx.x * kThreads >= n) return;
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
-    NoGrad nograd;
+    StageGrad nograd;
     const float4 *st = W.state[t & 1u];
     float4 *out = W.state[(t + 1u) & 1u];
     const float4 *H = W.hits;
@@ -174,7 +180,10 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
                 ended = surface_vertex(S, K, p, hit, h2.w, nograd);
             }
             keep = !ended;
-            if (ended) W.results[slot] = finish_path(p);
+            if (ended) {
+                W.results[slot] = finish_path(p);
+                if (W.sky_results) W.sky_results[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
         }
         const bool flags[1] = {keep};
         uint32_t *const ctr[1] = {&counters(W, t + 1u)->cont};
@@ -198,6 +207,12 @@ __global__ void __launch_bounds__(kThreads) wave_resolve(const __grid_constant__
         total.y += r.y;
         total.z += r.z;
         total.w += r.w;
+    }
+    if (W.sky_results) {
+        float3 sky = first ? f3(0.0f, 0.0f, 0.0f) : xyz4(W.sky_totals[pixel]);
+        for (uint32_t smp = 0; smp < W.chunk_samples; ++smp) sky = sky + xyz4(W.sky_results[(size_t)smp * pixels + pixel]);
+        if (last) fold_backdrop(P, pixel, sky);
+        else W.sky_totals[pixel] = pack3(sky, 0.0f);
     }
     if (!last) {
         W.totals[pixel] = total;

@@ -171,6 +171,25 @@ class PathTracer:
         check(self._lib.sg_upload_albedo_map(self._ctx, _ptr(a), a.shape[1], a.shape[0], extent_m), self._ctx)
         self._map_shape = (a.shape[0], a.shape[1])
 
+    def upload_catalogue(self, stars, cells) -> None:
+        """Catalogue rows (n, 8) and cell table of stargaze_b200.sky.ray_catalogue;
+        None removes the catalogue."""
+        if stars is None:
+            check(self._lib.sg_upload_catalogue(self._ctx, None, 0, None, 0), self._ctx)
+            return
+        st = np.ascontiguousarray(stars, dtype=np.float32).reshape(-1, 8)
+        ce = np.ascontiguousarray(cells, dtype=np.uint32)
+        check(self._lib.sg_upload_catalogue(self._ctx, _ptr(st), len(st), _ptr(ce), ce.size), self._ctx)
+
+    def upload_milky_way(self, texels) -> None:
+        """Panorama (height, width) of RGB10 texels (stargaze_b200.sky.panorama);
+        None removes it."""
+        if texels is None:
+            check(self._lib.sg_upload_milky_way(self._ctx, None, 0, 0), self._ctx)
+            return
+        t = np.ascontiguousarray(texels, dtype=np.uint32)
+        check(self._lib.sg_upload_milky_way(self._ctx, _ptr(t), t.shape[1], t.shape[0]), self._ctx)
+
     def read_pixels(self, stream=None) -> np.ndarray:
         """The accumulation as a (height*width, 4) float32 array."""
         w, h = self.size()
