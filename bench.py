@@ -455,6 +455,37 @@ def fp64_sites(wl, device: int, stream, reps: int = 2) -> dict:
     return out
 
 
+def air_terrain(device: int, stream, reps: int = 1) -> dict:
+    """The terrain workload (1080p, 128 spp, 4096^2 cells, 7,000 props) with
+    the host's earthlike air (camera-ray single scattering, sky-lit ground,
+    extinction of starlight and continuations): time per step with each
+    integrator, and without air for comparison."""
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, terrain_1080p, upload_workload, with_air
+
+    wl, land = terrain_1080p(1920, 1080, 128)
+    air_frame = with_air(wl.frame.copy(), 1)
+    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
+    upload_workload(t, wl)
+    out = {"workload": "terrain 1920x1080, 128 spp, 4096^2 cells, 7,000 props, earthlike air", "ms_per_step": {}}
+    for name, integrator, frame in (("wavefront_air", "wavefront", air_frame), ("megakernel_air", "megakernel", air_frame),
+                                    ("wavefront_airless", "wavefront", wl.frame)):
+        t.set_integrator(integrator)
+        times = []
+        for r in range(reps + 1):
+            f = frame.copy()
+            f.scene_time = float(-300 - r)
+            ms = timed_forward(t, wl, f, stream)
+            if r > 0:
+                times.append(ms)
+        out["ms_per_step"][name] = statistics.median(times)
+    t.close()
+    samples = wl.width * wl.height * wl.spp
+    out["msamples_per_s"] = {k: samples / (v * 1e3) for k, v in out["ms_per_step"].items()}
+    out["air_cost"] = out["ms_per_step"]["wavefront_air"] / out["ms_per_step"]["wavefront_airless"]
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -611,6 +642,7 @@ def run_ours(args):
                                  "note": "ratio = adjoint time / forward time at equal spp (ring scene)"}
             extras["fp64_sites"] = fp64_sites(wl, local, stream)
             extras["integrators"] = integrator_comparison(wl, local, stream)
+            extras["air"] = air_terrain(local, stream)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -63,11 +63,16 @@ static inline float lum(v3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0
 /* ---------------------------------------------------------------- */
 /* Scene access                                                      */
 /* ---------------------------------------------------------------- */
+/* What integrate_camera_air leaves for trace (pathtrace.wgsl:1629-1643). */
+typedef struct { float radiance[3]; uint32_t rng; } camera_air_t;
+
 typedef struct {
     const sg_settings *s;
     const sg_sphere *b;
     const oracle_tables *t;
     oracle_events *ev;
+    const float *sky;          /* surface sky cache, 128 x float4 (air frames) */
+    const camera_air_t *air;   /* this sample's camera air (air frames) */
 } scene;
 
 typedef struct { v3 offset; v3 dir; uint32_t anchor; } ray_t;   /* pathtrace.wgsl:70-76 */
@@ -948,7 +953,7 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
 int oracle_terrain_query(const sg_settings *settings, const oracle_tables *tables, const float o[3], const float d[3],
                          float limit, int occlusion, float out[4]) {
     if (!settings || !tables || !tables->terrain) return SG_ERR_INVALID;
-    scene S = {settings, NULL, tables, NULL};
+    scene S = {settings, NULL, tables, NULL, NULL, NULL};
     v3 n = V(0, 0, 0);
     float t = t_query(&S, tables->terrain, t_cells(&S), V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), limit, occlusion, &n);
     out[0] = n.x; out[1] = n.y; out[2] = n.z; out[3] = t;
@@ -1311,8 +1316,372 @@ static v3 milky_way(const scene *S, v3 view) {
     return vmul(vadd(vmul(top, 1.0f - wy), vmul(bot, wy)), S->s->background[0]);
 }
 
+
 /* ---------------------------------------------------------------- */
-/* trace: pathtrace.wgsl:1347-1617 (airless)                         */
+/* Host atmosphere: pathtrace.wgsl:927-1234 (single-scattering        */
+/* Rayleigh + Mie, planetshine) and the surface sky cache,            */
+/* terrain.wgsl:286-329.                                              */
+/* ---------------------------------------------------------------- */
+#define ATMO_VIEW_STEPS 8u
+#define ATMO_SUN_STEPS 4u
+#define SKY_TEXELS 128u
+
+static inline int air_on(const scene *S) { return S->s->g.atmo_params[3] >= 0.5f; }
+static inline v3 atmo_center(const scene *S) {
+    return V(S->s->g.atmo_center[0], S->s->g.atmo_center[1], S->s->g.atmo_center[2]);
+}
+static inline float host_radius(const scene *S) { return S->s->g.atmo_center[3]; }
+static inline float atmosphere_top(const scene *S) { return S->s->g.atmo_center[3] + S->s->g.atmo_params[2]; }
+static inline float atmo_scale_height(const scene *S) { return S->s->g.atmo_params[1]; }
+static inline v3 vexp_neg(v3 beta, float x) {
+    return V(expf(-beta.x * x), expf(-beta.y * x), expf(-beta.z * x));
+}
+static inline v3 beta_extinction(const scene *S) {
+    const float *r = S->s->g.atmo_rayleigh;
+    return V(r[0] + r[3], r[1] + r[3], r[2] + r[3]);
+}
+/* u32(ceil(x)) clamped to [2, ATMO_VIEW_STEPS] (the WGSL conversion
+ * saturates; C's is undefined out of range). */
+static inline uint32_t view_steps(float x) {
+    float q = ceilf(x);
+    if (!(q > 2.0f)) return 2u;
+    if (q >= (float)ATMO_VIEW_STEPS) return ATMO_VIEW_STEPS;
+    return (uint32_t)q;
+}
+
+/* shell_exit: pathtrace.wgsl:945-956 */
+static float shell_exit(const scene *S, v3 origin, v3 dir) {
+    v3 oc = vsub(origin, atmo_center(S));
+    float b = vdot(oc, dir);
+    float top = atmosphere_top(S);
+    float c = vdot(oc, oc) - top * top;
+    float disc = b * b - c;
+    if (disc < 0.0f) return 0.0f;
+    return -b + sqrtf(disc);
+}
+
+/* density_integral: pathtrace.wgsl:959-974 */
+static float density_integral(const scene *S, v3 origin, v3 dir, uint32_t steps) {
+    float distance = shell_exit(S, origin, dir);
+    if (distance <= 0.0f) return 0.0f;
+    float dt = distance / (float)steps;
+    float inv_h = 1.0f / atmo_scale_height(S);
+    float r = host_radius(S);
+    float sum = 0.0f;
+    for (uint32_t i = 0; i < steps; i++) {
+        v3 p = vadd(origin, vmul(dir, ((float)i + 0.5f) * dt));
+        float h = maxf_(vlength(vsub(p, atmo_center(S))) - r, 0.0f);
+        sum += expf(-h * inv_h);
+    }
+    return sum * dt;
+}
+
+/* host_offset, inside_air, air_transmittance: pathtrace.wgsl:976-1002 */
+static v3 host_offset(const scene *S, ray_t origin) {
+    if (origin.anchor == MISS) return vsub(origin.offset, atmo_center(S));
+    return vadd(vadd(vsub(b_center(S, origin.anchor), atmo_center(S)), b_low(S, origin.anchor)), origin.offset);
+}
+static int inside_air(const scene *S, ray_t origin) {
+    if (S->s->g.atmo_params[3] < 0.5f) return 0;
+    v3 oc = host_offset(S, origin);
+    float top = atmosphere_top(S);
+    return vdot(oc, oc) < top * top;
+}
+static v3 air_transmittance(const scene *S, ray_t origin, v3 dir) {
+    if (!inside_air(S, origin)) return V(1, 1, 1);
+    v3 p = vadd(atmo_center(S), host_offset(S, origin));
+    return vexp_neg(beta_extinction(S), density_integral(S, p, dir, ATMO_SUN_STEPS));
+}
+
+/* rayleigh_phase, mie_phase: pathtrace.wgsl:1004-1010 */
+static inline float rayleigh_phase(float cos_theta) {
+    return 3.0f / (16.0f * PI_F) * (1.0f + cos_theta * cos_theta);
+}
+static inline float mie_phase(float cos_theta, float g) {
+    float g2 = g * g;
+    return (1.0f - g2) / (4.0f * PI_F * powf(1.0f + g2 - 2.0f * g * cos_theta, 1.5f));
+}
+static v3 phase_weight(const scene *S, float cos_theta) {
+    const float *r = S->s->g.atmo_rayleigh;
+    float g = S->s->g.atmo_params[0];
+    float rp = rayleigh_phase(cos_theta), mp = mie_phase(cos_theta, g);
+    float m = r[3] * mp;
+    return V(r[0] * rp + m, r[1] * rp + m, r[2] * rp + m);
+}
+
+/* sample_reflector: pathtrace.wgsl:1017-1044 */
+typedef struct { uint32_t index; float inverse_probability; } reflector_t;
+static reflector_t sample_reflector(const scene *S, v3 origin, uint32_t *rng) {
+    ray_t ray = {origin, V(0.0f, 0.0f, -1.0f), MISS};
+    uint32_t host = (uint32_t)S->s->g.atmo_params[3] - 1u;
+    uint32_t selected = MISS;
+    float selected_weight = 0.0f, total = 0.0f;
+    for (uint32_t b = 0; b < S->s->counts[0]; b++) {
+        if (b == host || b_emissive(S, b) > 0.5f) continue;
+        v3 c = b_color(S, b);
+        float weight = cone_width(S, ray, b) * maxf_(c.x, maxf_(c.y, c.z));
+        if (weight <= 0.0f) continue;
+        total += weight;
+        if (rnd(S, rng) * total < weight) {
+            selected = b;
+            selected_weight = weight;
+        }
+    }
+    reflector_t r = {selected, total / maxf_(selected_weight, 1.0e-30f)};
+    return r;
+}
+
+/* reflected_radiance: pathtrace.wgsl:1049-1073 */
+static v3 reflected_radiance(const scene *S, ray_t ray, uint32_t index, uint32_t *rng) {
+    hit_t hit = sphere_hit(S, ray, index);
+    if (hit.index == MISS) return V(0, 0, 0);
+    v3 albedo = surface_albedo(S, index, hit.normal);
+    ray_t outgoing = {vmul(hit.normal, S->b[index].radius * (1.0f + 2.0e-6f)), hit.normal, index};
+    v3 radiance = V(0, 0, 0);
+    for (uint32_t slot = 0; slot < light_count(S); slot++) {
+        uint32_t s = light_index(S, slot);
+        if (b_emissive(S, s) < 0.5f) continue;
+        light_sample light = sample_light(S, outgoing, s, rng);
+        float cosine = maxf_(vdot(hit.normal, light.dir), 0.0f);
+        if (cosine > 0.0f) {
+            outgoing.dir = light.dir;
+            radiance = vadd(radiance, vmul(vmulv(albedo, b_color(S, s)),
+                                           cosine * light_visibility(S, outgoing, s) / (PI_F * light.pdf)));
+        }
+    }
+    return radiance;
+}
+
+/* brightest_risen_light: pathtrace.wgsl:1078-1089 */
+static float brightest_risen_light(const scene *S, v3 origin) {
+    ray_t ray = {origin, V(0.0f, 0.0f, -1.0f), MISS};
+    v3 up = V(S->s->g.ground_up[0], S->s->g.ground_up[1], S->s->g.ground_up[2]);
+    float brightest = 0.0f;
+    for (uint32_t slot = 0; slot < light_count(S); slot++) {
+        uint32_t b = light_index(S, slot);
+        if (b_emissive(S, b) < 0.5f) continue;
+        if (vdot(vnormalize(relative_center(S, ray, b)), up) <= 0.0f) continue;
+        v3 c = b_color(S, b);
+        brightest = maxf_(brightest, maxf_(c.x, maxf_(c.y, c.z)) * TAU_F * cone_width(S, ray, b));
+    }
+    return brightest;
+}
+
+/* eclipse_light_samples: pathtrace.wgsl:239-262 */
+static uint32_t eclipse_light_samples(const scene *S, ray_t ray, uint32_t index) {
+    if (S->s->counts[1] != 0u) return 1u;
+    v3 source = relative_center(S, ray, index);
+    float distance = vlength(source);
+    v3 axis = vdivs(source, distance);
+    float source_chord = sqrtf(2.0f * cone_width(S, ray, index));
+    for (uint32_t b = 0; b < S->s->counts[0]; b++) {
+        if (b == index) continue;
+        v3 offset = relative_center(S, ray, b);
+        float d2 = vdot(offset, offset);
+        float radius = S->b[b].radius;
+        if (d2 <= radius * radius) continue;
+        float d = sqrtf(d2);
+        if (d - radius >= distance + S->b[index].radius) continue;
+        float sin2 = clampf_(radius * radius / d2, 0.0f, 1.0f);
+        float limb_chord = sqrtf(2.0f * sin2 / (1.0f + sqrtf(1.0f - sin2)));
+        float separation = vlength(vsub(axis, vdivs(offset, d)));
+        if (separation < source_chord + limb_chord && separation + source_chord > limb_chord) return 4u;
+    }
+    return 1u;
+}
+
+/* air_light_visibility: rings.wgsl:121-141 */
+static float air_light_visibility(const scene *S, ray_t ray, uint32_t light) {
+    if (S->s->g.ground_north[3] == 0.0f || ground_origin(S, ray).y <= landscape_top(S))
+        return light_visibility(S, ray, light);
+    hit_t surface = sphere_hit(S, ray, light);
+    if (surface.index == MISS) return 0.0f;
+    for (uint32_t i = 0; i < S->s->counts[0]; i++) {
+        if (i == light) continue;
+        hit_t hit = sphere_hit(S, ray, i);
+        if (hit.index != MISS && (hit.distance < surface.distance ||
+                                  (hit.distance == surface.distance && i < light)))
+            return 0.0f;
+    }
+    float transmission = 1.0f;
+    for (uint32_t i = 0; i < S->s->counts[0]; i++) {
+        ring_hit_t hit = ring_hit(S, ray, i);
+        if (hit.index != MISS && hit.distance < surface.distance) transmission *= ring_transmission(S, ray, hit);
+    }
+    return transmission;
+}
+
+/* atmosphere: pathtrace.wgsl:1092-1213. Returns the in-scatter; the view
+ * transmittance goes to *transmittance when given. */
+static v3 atmosphere(const scene *S, v3 origin, v3 dir, float limit, uint32_t *rng, v3 *transmittance) {
+    if (transmittance) *transmittance = V(1, 1, 1);
+    if (S->s->g.atmo_params[3] < 0.5f) return V(0, 0, 0);
+    float exit_ = shell_exit(S, origin, dir);
+    float t_max = minf_(limit, exit_);
+    if (t_max <= 0.0f) return V(0, 0, 0);
+    v3 beta_ext = beta_extinction(S);
+    float r = host_radius(S);
+    uint32_t steps = view_steps(t_max / (0.25f * atmo_scale_height(S)));
+    float dt = t_max / (float)steps;
+    /* select() evaluates both operands: the draw is always taken. */
+    uint32_t jitter_rng = hash_u32(*rng ^ 0x3c6ef372u);
+    float jittered = rnd(S, &jitter_rng);
+    float jitter = (steps < ATMO_VIEW_STEPS || limit < exit_) ? jittered : 0.5f;
+
+    uint32_t reflected_rng = hash_u32(*rng ^ 0xa511e9b3u);
+    reflector_t reflector = sample_reflector(S, origin, &reflected_rng);
+    v3 reflected = V(0, 0, 0), reflected_direction = dir, reflected_phase = V(0, 0, 0);
+    if (reflector.index != MISS) {
+        ray_t reflected_ray = {origin, dir, MISS};
+        light_sample light = sample_light(S, reflected_ray, reflector.index, &reflected_rng);
+        reflected_ray.dir = light.dir;
+        reflected = vmul(reflected_radiance(S, reflected_ray, reflector.index, &reflected_rng),
+                         reflector.inverse_probability / light.pdf);
+        reflected_direction = light.dir;
+        reflected_phase = phase_weight(S, vdot(dir, light.dir));
+    }
+    if (reflected.x > 0.0f || reflected.y > 0.0f || reflected.z > 0.0f) {
+        float sun = brightest_risen_light(S, origin);
+        if (sun > 0.0f) {
+            float ratio = maxf_(reflected.x, maxf_(reflected.y, reflected.z)) / sun;
+            float minimum = 1.0f / sqrtf(clampf_((float)S->s->counts[1] + 1.0f, 1.0f, 4096.0f));
+            float keep = clampf_(ratio * 1.0e3f, minimum, 1.0f);
+            reflected = rnd(S, &reflected_rng) < keep ? vdivs(reflected, keep) : V(0, 0, 0);
+        }
+    }
+    int planetshine = reflected.x > 0.0f || reflected.y > 0.0f || reflected.z > 0.0f;
+
+    v3 t_view = V(1, 1, 1), inscatter = V(0, 0, 0);
+    for (uint32_t i = 0; i < steps; i++) {
+        v3 p = vadd(origin, vmul(dir, ((float)i + jitter) * dt));
+        v3 to_center = vsub(p, atmo_center(S));
+        float altitude = maxf_(vlength(to_center) - r, 0.0f);
+        float density = expf(-altitude / atmo_scale_height(S));
+        float column = density * dt;
+        v3 tau = vmul(beta_ext, column);
+        v3 step_t = V(expf(-tau.x), expf(-tau.y), expf(-tau.z));
+        v3 segment;
+        segment.x = tau.x < 1.0e-3f ? column * (1.0f - 0.5f * tau.x) : (1.0f - step_t.x) / maxf_(beta_ext.x, 1.0e-20f);
+        segment.y = tau.y < 1.0e-3f ? column * (1.0f - 0.5f * tau.y) : (1.0f - step_t.y) / maxf_(beta_ext.y, 1.0e-20f);
+        segment.z = tau.z < 1.0e-3f ? column * (1.0f - 0.5f * tau.z) : (1.0f - step_t.z) / maxf_(beta_ext.z, 1.0e-20f);
+        for (uint32_t slot = 0; slot < light_count(S); slot++) {
+            uint32_t b = light_index(S, slot);
+            if (b_emissive(S, b) < 0.5f) continue;
+            ray_t light_ray = {p, dir, MISS};
+            uint32_t light_samples = eclipse_light_samples(S, light_ray, b);
+            for (uint32_t k = 0; k < light_samples; k++) {
+                light_sample light = sample_light_stratum(S, light_ray, b, k, light_samples, rng);
+                light_ray.dir = light.dir;
+                float visibility = air_light_visibility(S, light_ray, b);
+                if (visibility == 0.0f) continue;
+                v3 e_sun = vmul(b_color(S, b), visibility / ((float)light_samples * light.pdf));
+                v3 sun_t = vexp_neg(beta_ext, density_integral(S, p, light.dir, ATMO_SUN_STEPS));
+                v3 beta_phase = phase_weight(S, vdot(dir, light.dir));
+                inscatter = vadd(inscatter, vmulv(vmulv(vmulv(vmulv(t_view, segment), beta_phase), e_sun), sun_t));
+            }
+        }
+        if (planetshine) {
+            ray_t shine = {p, reflected_direction, MISS};
+            float visibility = air_light_visibility(S, shine, reflector.index);
+            if (visibility > 0.0f) {
+                v3 light_t = vexp_neg(beta_ext, density_integral(S, p, reflected_direction, ATMO_SUN_STEPS));
+                inscatter = vadd(inscatter, vmulv(vmulv(vmulv(vmulv(t_view, segment), reflected_phase), reflected),
+                                                  vmul(light_t, visibility)));
+            }
+        }
+        t_view = vmulv(t_view, step_t);
+    }
+    if (transmittance) *transmittance = t_view;
+    return inscatter;
+}
+
+/* camera_air_transmittance: pathtrace.wgsl:1217-1234 */
+static v3 camera_air_transmittance(const scene *S, v3 origin, v3 dir, float limit, uint32_t seed) {
+    float exit_ = shell_exit(S, origin, dir);
+    float t_max = minf_(limit, exit_);
+    if (t_max <= 0.0f) return V(1, 1, 1);
+    uint32_t steps = view_steps(t_max / (0.25f * atmo_scale_height(S)));
+    float dt = t_max / (float)steps;
+    uint32_t jitter_rng = hash_u32(seed ^ 0x3c6ef372u);
+    float jittered = rnd(S, &jitter_rng);
+    float jitter = (steps < ATMO_VIEW_STEPS || limit < exit_) ? jittered : 0.5f;
+    v3 beta_ext = beta_extinction(S);
+    v3 transmittance = V(1, 1, 1);
+    for (uint32_t i = 0; i < steps; i++) {
+        v3 p = vadd(origin, vmul(dir, ((float)i + jitter) * dt));
+        float altitude = maxf_(vlength(vsub(p, atmo_center(S))) - host_radius(S), 0.0f);
+        float column = expf(-altitude / atmo_scale_height(S)) * dt;
+        transmittance = vmulv(transmittance, vexp_neg(beta_ext, column));
+    }
+    return transmittance;
+}
+
+/* cache_surface_sky: terrain.wgsl:286-302 (128 texels, 16 azimuths x 8
+ * elevations; settings of the frame's first dispatch). */
+static void cache_surface_sky(const scene *S, float *out) {
+    for (uint32_t index = 0; index < SKY_TEXELS; index++) {
+        uint32_t x = index % 16u, y = index / 16u;
+        v3 light = V(0, 0, 0);
+        if (S->s->g.atmo_params[3] > 0.5f && S->s->g.ground_counts[1] != 0u) {
+            float mu = ((float)y + 0.5f) / 8.0f;
+            float phi = TAU_F * ((float)x + 0.5f) / 16.0f;
+            float r = sqrtf(1.0f - mu * mu);
+            v3 dir = from_ground(S, V(r * cosf(phi), mu, r * sinf(phi)));
+            uint32_t rng = hash_u32(index ^ 0x91ce452du);
+            light = atmosphere(S, V(0, 0, 0), dir, 1.0e30f, &rng, NULL);
+        }
+        out[4 * index] = light.x;
+        out[4 * index + 1] = light.y;
+        out[4 * index + 2] = light.z;
+        out[4 * index + 3] = 0.0f;
+    }
+}
+
+/* surface_sky_texel, surface_sky_lookup: terrain.wgsl:303-315 */
+static v3 surface_sky_texel(const scene *S, int x, int y) {
+    int yy = y < 0 ? 0 : (y > 7 ? 7 : y);
+    const float *t = S->sky + 4 * ((uint32_t)yy * 16u + (uint32_t)((x + 16) % 16));
+    return V(t[0], t[1], t[2]);
+}
+static v3 surface_sky_lookup(const scene *S, v3 dir) {
+    if (!S->sky) return V(0, 0, 0);
+    v3 p = to_ground(S, dir);
+    if (p.y <= 0.0f) return V(0, 0, 0);
+    float ux = fmodf(atan2f(p.z, p.x) / TAU_F + 1.0f, 1.0f) * 16.0f - 0.5f;
+    float uy = p.y * 8.0f - 0.5f;
+    int cx = (int)floorf(ux), cy = (int)floorf(uy);
+    float fx = ux - floorf(ux), fy = uy - floorf(uy);
+    v3 a = v3mix(surface_sky_texel(S, cx, cy), surface_sky_texel(S, cx + 1, cy), fx);
+    v3 b = v3mix(surface_sky_texel(S, cx, cy + 1), surface_sky_texel(S, cx + 1, cy + 1), fx);
+    return v3mix(a, b, fy);
+}
+
+/* sky_blocked, surface_sky: terrain.wgsl:317-339 */
+static int sky_blocked(const scene *S, ray_t ray) {
+    for (uint32_t i = 0; i < S->s->counts[0]; i++) {
+        if (S->s->g.ground_north[3] == (float)(i + 1u)) continue;
+        if (sphere_hit(S, ray, i).index != MISS) return 1;
+    }
+    return landscape_query(S, ray, 1.0e30f, 1).index != MISS;
+}
+static v3 surface_sky(const scene *S, ray_t origin, v3 normal, uint32_t *rng) {
+    float u = rnd(S, rng);
+    float phi = TAU_F * rnd(S, rng);
+    v3 dir = basis_direction(normal, sqrtf(u) * cosf(phi), sqrtf(u) * sinf(phi), sqrtf(1.0f - u));
+    v3 light = surface_sky_lookup(S, dir);
+    if (maxf_(light.x, maxf_(light.y, light.z)) <= 0.0f) return V(0, 0, 0);
+    ray_t ray = {origin.offset, dir, origin.anchor};
+    if (sky_blocked(S, ray)) return V(0, 0, 0);
+    float transmission = 1.0f;
+    for (uint32_t i = 0; i < S->s->counts[0]; i++) {
+        ring_hit_t hit = ring_hit(S, ray, i);
+        if (hit.index != MISS) transmission *= ring_transmission(S, ray, hit);
+    }
+    return vmul(light, transmission);
+}
+
+/* ---------------------------------------------------------------- */
+/* trace: pathtrace.wgsl:1347-1617                                   */
 /* With a direction D (adjoint check), dout receives the tangent of  */
 /* the returned radiance along D: every sampling decision, pdf, MIS   */
 /* weight and Russian-roulette survival keeps its value, only the     */
@@ -1334,6 +1703,9 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
     float ring_cap = 1.0e30f;
     v3 ring_base = V(0, 0, 0);
     uint32_t shine_body = MISS;
+    /* Host air (pathtrace.wgsl:1361-1368): the previous vertex lies in the
+     * air; the previous vertex was a sky-lit local surface. */
+    int in_air = 0, sky_on_escape = 0, camera_segment = 1;
     /* tangents: detached (sampling held fixed) everywhere; after the first
      * ring scatter also the full tangent (pdfs and MIS weights attached)
      * of the throughput and of the radiance gathered since, and the score
@@ -1350,8 +1722,28 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
         if (depth == 0u && null_crossings == 0u && st->background[3] > 0.0f)
             hit = point_disc_hit(S, ray, hit, &disc_scale, rng);
         ring_hit_t ring = closest_ring(S, ray, hit.distance);
-        /* Host air and camera air (pathtrace.wgsl:1387-1414) are inert:
-         * atmo_params.w < 0.5 for every frame the oracle accepts. */
+        /* pathtrace.wgsl:1387-1414: extinction of a continuation that left
+         * the air for a celestial surface or a ring, and the camera ray's
+         * air (its in-scatter from integrate_camera_air). */
+        if (in_air) {
+            in_air = 0;
+            uint32_t host = (uint32_t)st->g.atmo_params[3] - 1u;
+            if (ring.index != MISS || (hit.index < LOCAL_BASE && hit.index != host))
+                throughput = vmulv(throughput, air_transmittance(S, ray, ray.dir));
+        }
+        if (camera_segment) {
+            camera_segment = 0;
+            float limit = 1.0e30f;
+            if (hit.index != MISS) limit = hit.distance;
+            if (ring.index != MISS) limit = minf_(limit, ring.distance);
+            if (st->g.atmo_params[3] >= 0.5f) {
+                v3 transmittance = camera_air_transmittance(S, ray.offset, ray.dir, limit, *rng);
+                radiance = vadd(radiance, vmulv(throughput, V(S->air->radiance[0], S->air->radiance[1],
+                                                              S->air->radiance[2])));
+                throughput = vmulv(throughput, transmittance);
+                *rng = S->air->rng;
+            }
+        }
         if (ring.index != MISS) {
             EV(ring_events);
             const sg_sphere *planet = &S->b[ring.index];
@@ -1468,6 +1860,7 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
             }
             throughput = vmul(vmulv(throughput, ring_bsdf(optics, mu_out, z)), fabsf(z) / bsdf_pdf);
             previous_pdf = bsdf_pdf;
+            sky_on_escape = 0;
             ray = ring_origin(S, ring, direction);
             previous_vertex = ray;
             depth += 1u;
@@ -1486,6 +1879,7 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
             /* pathtrace.wgsl:1494-1508: background stars and the Milky Way
              * along unscattered camera paths (straight-through ring
              * crossings included); the backdrop is also returned apart. */
+            if (sky_on_escape) radiance = vadd(radiance, vmulv(throughput, surface_sky_lookup(S, ray.dir)));
             if (depth == 0u) {
                 radiance = vadd(radiance, vmulv(throughput, environment(S, ray.dir)));
                 backdrop = vmulv(milky_way(S, ray.dir), throughput);
@@ -1550,8 +1944,9 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
                 float bsdf_pdf = cosine / PI_F;
                 float weight = power_weight(sample.pdf, bsdf_pdf);
                 if (last_vertex) weight = 1.0f;
-                /* air_transmittance(...) == 1 without air. */
-                direct_light = vadd(direct_light, vmul(b_color(S, i), bsdf_pdf * weight * visibility / sample.pdf));
+                v3 color = b_color(S, i);
+                if (air_on(S)) color = vmulv(color, air_transmittance(S, outgoing, sample.dir));
+                direct_light = vadd(direct_light, vmul(color, bsdf_pdf * weight * visibility / sample.pdf));
                 if (D) {
                     float dvis = light_visibility_dot(S, D, outgoing, i, visibility);
                     ddirect_light = vadd(ddirect_light,
@@ -1585,7 +1980,12 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
                                            vmulv(vmulv(throughput, albedo), dshine)));
             shine_body = hit.index;
         }
-        /* sky_lit needs the host atmosphere (pathtrace.wgsl:1578-1584): off. */
+        /* Sky light of local surfaces (pathtrace.wgsl:1578-1584): an
+         * explicit sample at the depth limit, else the continuation's
+         * escape (sky_on_escape). */
+        int sky_lit = local && st->g.ground_counts[1] != 0u && st->g.atmo_params[3] > 0.5f;
+        if (sky_lit && last_vertex)
+            radiance = vadd(radiance, vmulv(vmulv(throughput, albedo), surface_sky(S, outgoing, normal, rng)));
         if (last_vertex) break;
         float u = rnd(S, rng);
         float phi = TAU_F * rnd(S, rng);
@@ -1606,6 +2006,8 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
         }
         ray = outgoing;
         previous_vertex = outgoing;
+        in_air = inside_air(S, outgoing);
+        sky_on_escape = sky_lit;
         depth += 1u;
         null_crossings = 0u;
     }
@@ -1655,11 +2057,10 @@ static v3 camera_direction(const scene *S, uint32_t x, uint32_t y, uint32_t *rng
     return vnormalize(V(ndc_x * tangent * S->s->g.viewport[3], ndc_y * tangent, -1.0f));
 }
 
-/* Frames the restatement covers: no host atmosphere; landscape themes 0-2;
+/* Frames the restatement covers: landscape themes 0-2;
  * no vegetation primitives; terrain only with a terrain table. */
 static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
     if (!s) return SG_ERR_INVALID;
-    if (s->g.atmo_params[3] >= 0.5f) return SG_ERR_INVALID;
     if (s->counts[0] > SG_BODY_CAPACITY) return SG_ERR_CAPACITY;
     if (s->g.ground_north[3] != 0.0f) {
         if ((s->g.ground_counts[2] & 255u) > 2u) return SG_ERR_INVALID;
@@ -1687,6 +2088,42 @@ static void sample_pixel(const scene *S, uint32_t x, uint32_t y, uint32_t s, flo
     sample_pixel_d(S, x, y, s, out, NULL, NULL);
 }
 
+/* The surface sky cache as the frame's first dispatch builds it
+ * (src/pathtracer.rs:946-954: only while the history holds no samples). */
+static void prepare_sky(const sg_settings *settings, const sg_sphere *bodies, const oracle_tables *tables,
+                        float sky[4 * SKY_TEXELS]) {
+    sg_settings first = *settings;
+    first.counts[1] = 0u;
+    scene S = {&first, bodies, tables, NULL, NULL, NULL};
+    cache_surface_sky(&S, sky);
+}
+
+/* Sample `s` of a dispatch with host air: one integrate_camera_air / main
+ * pair over a settings slice whose sampling.x and counts.y carry the
+ * sample (src/pathtracer.rs:862-882, :963-968; pathtrace.wgsl:1629-1643). */
+static void sample_pixel_air(const scene *S, uint32_t x, uint32_t y, uint32_t s, float out[7]) {
+    sg_settings one = *S->s;
+    one.sampling[0] = S->s->sampling[0] + s;
+    one.counts[1] = S->s->counts[1] + s;
+    one.counts[2] = 1u;
+    scene A = *S;
+    A.s = &one;
+    uint32_t pixel = y * (uint32_t)one.g.viewport[0] + x;
+    uint32_t rng = hash_u32(pixel ^ hash_u32(one.sampling[0] + 0x9e3779b9u));
+    ray_t ray;
+    ray.offset = V(0, 0, 0);
+    ray.dir = camera_direction(&A, x, y, &rng);
+    ray.anchor = MISS;
+    hit_t hit = closest_hit(&A, ray);
+    float disc_scale = 1.0f;
+    if (one.background[3] > 0.0f) hit = point_disc_hit(&A, ray, hit, &disc_scale, &rng);
+    ring_hit_t ring = closest_ring(&A, ray, hit.distance);
+    v3 light = atmosphere(&A, ray.offset, ray.dir, minf_(hit.distance, ring.distance), &rng, NULL);
+    camera_air_t air = {{light.x, light.y, light.z}, rng};
+    A.air = &air;
+    sample_pixel(&A, x, y, 0u, out);
+}
+
 /* main: pathtrace.wgsl:1645-1675 */
 int oracle_dispatch(const sg_settings *settings, const sg_sphere *bodies, const oracle_tables *tables,
                     float *accumulation, float *backdrop, uint32_t y0, uint32_t y1, int threads,
@@ -1711,6 +2148,9 @@ int oracle_dispatch(const sg_settings *settings, const sg_sphere *bodies, const 
         per_thread = (oracle_events *)calloc((size_t)nthreads, sizeof(oracle_events));
         if (!per_thread) return SG_ERR_OOM;
     }
+    const int air = settings->g.atmo_params[3] >= 0.5f;
+    float sky[4 * SKY_TEXELS];
+    if (air) prepare_sky(settings, bodies, tables, sky);
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
 #endif
@@ -1720,10 +2160,31 @@ int oracle_dispatch(const sg_settings *settings, const sg_sphere *bodies, const 
 #else
         int tid = 0;
 #endif
-        scene S = {settings, bodies, tables, per_thread ? &per_thread[tid] : NULL};
+        scene S = {settings, bodies, tables, per_thread ? &per_thread[tid] : NULL, air ? sky : NULL, NULL};
         uint32_t x = (uint32_t)(k % width);
         uint32_t y = y0 + (uint32_t)(k / width);
         uint32_t pixel = y * width + x;
+        if (air) {
+            /* One running-mean fold per sample, as the per-sample
+             * dispatches of an air frame do. */
+            for (uint32_t s = 0; s < z; s++) {
+                float r[7];
+                if (S.ev) S.ev->samples++;
+                sample_pixel_air(&S, x, y, s, r);
+                uint32_t old_count = settings->counts[1] + s;
+                float w = 1.0f / (float)(old_count + 1u);
+                for (int c = 0; c < 4; c++) {
+                    float old = accumulation[4 * pixel + c];
+                    accumulation[4 * pixel + c] = old_count > 0u ? old + (r[c] - old) * w : r[c];
+                }
+                for (int c = 0; c < 3; c++) {
+                    float old = backdrop[4 * pixel + c];
+                    backdrop[4 * pixel + c] = old_count > 0u ? old + (r[4 + c] - old) * w : r[4 + c];
+                }
+                backdrop[4 * pixel + 3] = 0.0f;
+            }
+            continue;
+        }
         float sum[4] = {0, 0, 0, 0}, bsum[3] = {0, 0, 0};
         for (uint32_t s = 0; s < z; s++) {
             float r[7];
@@ -1768,6 +2229,8 @@ int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies, const o
                    int threads) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
+    /* The adjoint does not differentiate the host air. */
+    if (settings->g.atmo_params[3] >= 0.5f) return SG_ERR_INVALID;
     uint32_t width = (uint32_t)settings->g.viewport[0];
     uint32_t height = (uint32_t)settings->g.viewport[1];
     if (y1 > height) y1 = height;
@@ -1784,7 +2247,7 @@ int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies, const o
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
 #endif
     for (long k = 0; k < total; k++) {
-        scene S = {settings, bodies, tables, NULL};
+        scene S = {settings, bodies, tables, NULL, NULL, NULL};
         uint32_t x = (uint32_t)(k % width);
         uint32_t y = y0 + (uint32_t)(k / width);
         size_t pixel = (size_t)y * width + x;
@@ -1802,9 +2265,16 @@ int oracle_trace_sample(const sg_settings *settings, const sg_sphere *bodies, co
                         uint32_t x, uint32_t y, uint32_t s, float out[4]) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
-    scene S = {settings, bodies, tables, NULL};
+    scene S = {settings, bodies, tables, NULL, NULL, NULL};
     float r[7];
-    sample_pixel(&S, x, y, s, r);
+    if (settings->g.atmo_params[3] >= 0.5f) {
+        float sky[4 * SKY_TEXELS];
+        prepare_sky(settings, bodies, tables, sky);
+        S.sky = sky;
+        sample_pixel_air(&S, x, y, s, r);
+    } else {
+        sample_pixel(&S, x, y, s, r);
+    }
     for (int c = 0; c < 4; c++) out[c] = r[c];
     return SG_OK;
 }
@@ -1821,7 +2291,7 @@ int oracle_closest_hit(const sg_settings *settings, const sg_sphere *bodies, con
                        const sg_ray *rays, uint32_t n, sg_hit *hits) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
-    scene S = {settings, bodies, tables, NULL};
+    scene S = {settings, bodies, tables, NULL, NULL, NULL};
     for (uint32_t i = 0; i < n; i++) {
         hit_t h = closest_hit(&S, to_ray(&rays[i]));
         hits[i].distance = h.distance;
@@ -1837,7 +2307,7 @@ int oracle_light_visibility(const sg_settings *settings, const sg_sphere *bodies
                             const sg_ray *rays, const uint32_t *lights, uint32_t n, float *out) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
-    scene S = {settings, bodies, tables, NULL};
+    scene S = {settings, bodies, tables, NULL, NULL, NULL};
     for (uint32_t i = 0; i < n; i++) out[i] = light_visibility(&S, to_ray(&rays[i]), lights[i]);
     return SG_OK;
 }
@@ -1846,7 +2316,7 @@ int oracle_reference_visibility(const sg_settings *settings, const sg_sphere *bo
                                 const sg_ray *rays, const uint32_t *lights, uint32_t n, float *out) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
-    scene S = {settings, bodies, tables, NULL};
+    scene S = {settings, bodies, tables, NULL, NULL, NULL};
     for (uint32_t k = 0; k < n; k++) {
         ray_t ray = to_ray(&rays[k]);
         hit_t surface = closest_hit(&S, ray);
@@ -1866,7 +2336,7 @@ int oracle_ring_probe(const sg_settings *settings, const sg_sphere *bodies, cons
     int status = check_frame(settings);
     if (status != SG_OK) return status;
     if (body >= settings->counts[0]) return SG_ERR_INVALID;
-    scene S = {settings, bodies, tables, NULL};
+    scene S = {settings, bodies, tables, NULL, NULL, NULL};
     for (uint32_t i = 0; i < n; i++) {
         ray_t ray = to_ray(&rays[i]);
         ring_hit_t hit = ring_hit(&S, ray, body);
@@ -1895,7 +2365,7 @@ float oracle_ring_energy(float albedo, float tau, float mu, uint32_t steps) {
 
 int oracle_sample_light(const sg_settings *settings, const sg_sphere *bodies, const sg_ray *ray,
                         uint32_t light, uint32_t *rng, float direction[3], float *pdf) {
-    scene S = {settings, bodies, NULL, NULL};
+    scene S = {settings, bodies, NULL, NULL, NULL, NULL};
     light_sample ls = sample_light(&S, to_ray(ray), light, rng);
     direction[0] = ls.dir.x;
     direction[1] = ls.dir.y;
@@ -1904,8 +2374,16 @@ int oracle_sample_light(const sg_settings *settings, const sg_sphere *bodies, co
     return SG_OK;
 }
 
+int oracle_sky_cache(const sg_settings *settings, const sg_sphere *bodies, const oracle_tables *tables,
+                     float out[4 * 128]) {
+    int status = check_frame(settings);
+    if (status != SG_OK) return status;
+    prepare_sky(settings, bodies, tables, out);
+    return SG_OK;
+}
+
 uint32_t oracle_hash(uint32_t value) { return hash_u32(value); }
 float oracle_random(uint32_t *state) {
-    scene S = {NULL, NULL, NULL, NULL};
+    scene S = {NULL, NULL, NULL, NULL, NULL, NULL};
     return rnd(&S, state);
 }

@@ -153,6 +153,11 @@ int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies,
                    int threads);
 
 /* hash / random of pathtrace.wgsl:87-98, exported for RNG-stream checks. */
+/* The surface sky cache of a frame with host air (terrain.wgsl:286-302):
+ * 16 x 8 float4 texels, row-major by elevation. */
+int oracle_sky_cache(const sg_settings *settings, const sg_sphere *bodies,
+                     const oracle_tables *tables, float out[4 * 128]);
+
 uint32_t oracle_hash(uint32_t value);
 float oracle_random(uint32_t *state);
 

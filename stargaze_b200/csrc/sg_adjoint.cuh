@@ -101,17 +101,24 @@ struct GradSink {
     }
 };
 
-// The forward integrator: no hooks.
-struct NoGrad {
+// The forward integrator: no hooks. A: the host air's code is compiled in.
+// Frames with air (atmo_params.w >= 0.5) run the A instantiations; the
+// others run kernels that carry none of its code or register pressure.
+template <bool A>
+struct Forward {
     static constexpr bool adjoint = false;
     static constexpr bool sky = true;  // surface_vertex shades an escaped path's sky
+    static constexpr bool air = A;
 };
+using NoGrad = Forward<false>;
 
 // The wavefront's shade stages: no hooks, and no escaped paths (extend ends
 // those), so surface_vertex's miss branch never runs there.
-struct StageGrad {
+template <bool A>
+struct Stage {
     static constexpr bool adjoint = false;
     static constexpr bool sky = false;
+    static constexpr bool air = A;
 };
 
 // A Russian-roulette decision after the cap vertex (pathtrace.wgsl:
@@ -141,6 +148,7 @@ struct PrbLists {
 struct Prb {
     static constexpr bool adjoint = true;
     static constexpr bool sky = false;  // sg_backward rejects frames with a sky
+    static constexpr bool air = false;  // ... and frames with host air
     bool pass2;
     // Pass 1's summary.
     float cap;

@@ -101,6 +101,9 @@ struct sg_context {
     float4 *sky_samples = nullptr;          // wavefront: per-sample backdrop + totals
     size_t sky_samples_size = 0;
     bool backdrop_written = false;          // the backdrop buffer holds a sky
+    // Host air: the surface sky cache (128 float4), rebuilt when an
+    // accumulation starts.
+    float4 *sky_light = nullptr;
     // Display: the exposure state and histogram of the metering.
     sg::ExposureState *exposure = nullptr;
     uint32_t *histogram = nullptr;
@@ -243,8 +246,6 @@ int validate_frame(sg_context *ctx, const sg_frame *frame) {
     if (frame->n_ground && !frame->ground) return fail(ctx, SG_ERR_INVALID, "frame->ground is NULL");
     if (frame->globals->ground_counts[0] != frame->n_ground)
         return fail(ctx, SG_ERR_INVALID, "ground_counts.x does not match the primitive count");
-    if (frame->globals->atmo_params[3] >= 0.5f)
-        return fail(ctx, SG_ERR_INVALID, "the host atmosphere (atmo_params.w >= 0.5) is not implemented");
     const float host = frame->globals->ground_north[3];
     if (host != 0.0f) {
         if (host != std::floor(host) || host < 1.0f || host > (float)frame->n_bodies)
@@ -402,6 +403,8 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.milky_way = ctx->milky_way;
     p.sky_on = sky_on(ctx) ? 1u : 0u;
     p.backdrop = ctx->backdrop;
+    p.air_on = s.g.atmo_params[3] >= 0.5f ? 1u : 0u;
+    p.sky_light = ctx->sky_light;
     return p;
 }
 
@@ -506,6 +509,7 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->sky_cells);
     cudaFree(ctx->milky_way);
     cudaFree(ctx->sky_samples);
+    cudaFree(ctx->sky_light);
     if (ctx->wave_pinned) cudaFreeHost(ctx->wave_pinned);
     if (ctx->wave_ready) cudaEventDestroy(ctx->wave_ready);
     for (cudaEvent_t e : ctx->stage_marks.events) cudaEventDestroy(e);
@@ -839,6 +843,19 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
             ctx->backdrop_written = false;
         }
         if (p.sky_on) ctx->backdrop_written = true;
+        // The surface sky cache, built by an accumulation's first dispatch
+        // (src/pathtracer.rs:946-954).
+        if (p.air_on) {
+            if (!ctx->sky_light) {
+                SG_CUDA(ctx, cudaMalloc(&ctx->sky_light, sg::kSkyCacheTexels * sizeof(float4)));
+                p.sky_light = ctx->sky_light;
+            }
+            if (ctx->history.samples == 0u) {
+                cudaError_t e = sg::launch_sky_cache(p, ctx->sky_light, stream);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "surface sky cache");
+                ctx->launches += 1;
+            }
+        }
         if (events) {
             SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
             p.events = ctx->events;
@@ -1298,6 +1315,8 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
     if (status != SG_OK) return status;
     if (sky_on(ctx))
         return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate the sky backdrop; remove the catalogue and panorama");
+    if (frame->globals->atmo_params[3] >= 0.5f)
+        return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate the host air (atmo_params.w >= 0.5)");
     if (key_hash(history_key(ctx, frame)) != tape->history_hash)
         return fail(ctx, SG_ERR_STATE, "frame, options or tables differ from the ones the tape was recorded with");
     grads->dropped = 0;

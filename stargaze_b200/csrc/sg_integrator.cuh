@@ -7,6 +7,7 @@
 #pragma once
 
 #include "sg_adjoint.cuh"
+#include "sg_air.cuh"
 #include "sg_device.cuh"
 #include "sg_internal.h"
 #include "sg_landscape.cuh"
@@ -35,6 +36,11 @@ struct Path {
     uint32_t rng;
     bool point_gained;
     float3 backdrop;  // Milky Way radiance reached by an unscattered camera path
+    // Host air (pathtrace.wgsl:1361-1368): the previous vertex lies in the
+    // air; the previous vertex was a sky-lit local surface.
+    bool in_air;
+    bool sky_on_escape;
+    uint32_t sample;  // the sample's index in its dispatch (its counts.y offset)
 };
 
 // camera_direction (pathtrace.wgsl:1619-1626).
@@ -69,6 +75,9 @@ __device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counte
     p.iterations = 0;
     p.point_gained = false;
     p.backdrop = f3(0.0f, 0.0f, 0.0f);
+    p.in_air = false;
+    p.sky_on_escape = false;
+    p.sample = smp;
 }
 
 // The ring-indirect cap after the loop (pathtrace.wgsl:1609-1615); W holds
@@ -117,6 +126,29 @@ __device__ __forceinline__ void fold_backdrop(const TraceParams &P, uint32_t pix
     P.backdrop[pixel] = make_float4(mean.x, mean.y, mean.z, 0.0f);
 }
 
+// The host air at the start of an iteration (pathtrace.wgsl:1387-1414):
+// extinction of a continuation that left the air for a celestial surface
+// or a ring, and on the camera ray its in-scatter and view transmittance.
+template <bool C, bool L, bool F>
+__device__ __forceinline__ void air_extend(const Scene &S, Counter<C, L, F> K, Path &p, const Hit &hit,
+                                           const RingHit &ring) {
+    if (p.in_air) {
+        p.in_air = false;
+        const uint32_t host = (uint32_t)S.s->g.atmo_params[3] - 1u;
+        if (ring.index != kMiss || (hit.index < kLocalBase && hit.index != host))
+            p.throughput = p.throughput * air_transmittance(S, p.ray, p.ray.d);
+    }
+    if (p.iterations == 1u) {
+        float limit = 1.0e30f;
+        if (hit.index != kMiss) limit = hit.t;
+        if (ring.index != kMiss) limit = fminf(limit, ring.t);
+        const AirScatter a = atmosphere(S, K, p.ray.o, p.ray.d, limit, p.rng, S.s->counts[1] + p.sample);
+        p.radiance = p.radiance + p.throughput * a.inscatter;
+        p.throughput = p.throughput * a.transmittance;
+        p.rng = a.rng;
+    }
+}
+
 // What extend() finds along a path's current ray.
 struct Extension {
     Hit hit;          // closest body or landscape hit (after the disc test)
@@ -147,6 +179,9 @@ __device__ __forceinline__ bool extend(const Scene &S, Counter<C, L, F> K, Path 
         p.rng = disc.rng;
     }
     e.ring = closest_ring(S, K, p.ray, e.hit.t);
+    if constexpr (G::air) {
+        if (S.p->air_on) air_extend(S, K, p, e.hit, e.ring);
+    }
     return true;
 }
 
@@ -263,6 +298,7 @@ __device__ __forceinline__ bool ring_vertex(const Scene &S, Counter<C, L, F> K, 
                 ring_scatter_grad(S, grad, ri, optics, mu_out, z, vg, transmission, ray.d);
             }
             previous_pdf = bsdf_pdf;
+            if constexpr (G::air) p.sky_on_escape = false;
             ray = ring_origin(S, ri, ring.p, direction);
             previous_vertex = ray;
             depth += 1u;
@@ -306,6 +342,9 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
         // Miss: the sky backdrop of an unscattered camera path (the adjoint
         // does not differentiate it; sg_backward rejects such frames).
         if (hit.index == kMiss) {
+            if constexpr (G::air) {
+                if (p.sky_on_escape) radiance = radiance + throughput * surface_sky_lookup(S, ray.d);
+            }
             if constexpr (G::sky) sky_miss(S, p);
             return true;
         }
@@ -385,7 +424,11 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
             if (visibility > 0.0f) {
                 const float bsdf_pdf = cosine / kPi;
                 const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
-                direct_light = direct_light + xyz(light_material) * (bsdf_pdf * weight * visibility / sample.pdf);
+                float3 color = xyz(light_material);
+                if constexpr (G::air) {
+                    if (S.p->air_on) color = color * air_transmittance(S, outgoing, sample.d);
+                }
+                direct_light = direct_light + color * (bsdf_pdf * weight * visibility / sample.pdf);
                 if constexpr (G::adjoint)
                     surface_light_grad(grad, albedo_e, i,
                                        throughput * albedo_g * xyz(light_material) *
@@ -410,8 +453,17 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
             rng = shine.rng;
             radiance = radiance + throughput * albedo * shine.radiance;
         }
-        // Sky lighting of local surfaces needs the host atmosphere
-        // (pathtrace.wgsl:1578-1584), which frames here never enable.
+        // Sky light of local surfaces (pathtrace.wgsl:1578-1584): an explicit
+        // sample at the depth limit, else the continuation's escape.
+        bool sky_lit = false;
+        if constexpr (G::air && L) {
+            sky_lit = local && s->g.ground_counts[1] != 0u && s->g.atmo_params[3] > 0.5f;
+            if (sky_lit && last_vertex) {
+                const SkySample sky = surface_sky(S, K, outgoing, normal, rng);
+                rng = sky.rng;
+                radiance = radiance + throughput * albedo * sky.radiance;
+            }
+        }
         shine_body = local ? kMiss : bi;
         if (last_vertex) return true;
         const float u = rnd(K, rng);
@@ -437,13 +489,17 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
         }
         ray = outgoing;
         previous_vertex = outgoing;
+        if constexpr (G::air) {
+            p.in_air = inside_air(S, outgoing);
+            p.sky_on_escape = sky_lit;
+        }
         depth += 1u;
         null_crossings = 0u;
         return false;
     }
 }
 
-// One iteration of trace()'s loop (pathtrace.wgsl:1380-1607), airless.
+// One iteration of trace()'s loop (pathtrace.wgsl:1380-1607).
 // Returns true when the path has ended. G is the hook set: NoGrad for the
 // forward integrator (every hook compiles out), Prb for the adjoint, whose
 // first replay records the ring-cap vertex and later Russian roulette and

@@ -47,6 +47,10 @@ struct TraceParams {
     const uint32_t *milky_way;
     uint32_t sky_on;  // catalogue or panorama bound (and the panorama's brightness > 0)
     float4 *backdrop;
+    // Host air (atmo_params.w >= 0.5): its surface sky cache, 16 x 8 float4
+    // texels (terrain.wgsl:286-302), built when an accumulation starts.
+    uint32_t air_on;
+    const float4 *sky_light;
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,
@@ -67,6 +71,11 @@ size_t trace_smem_bytes(const TraceParams &p);
 void set_library_error(const char *message);
 
 cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t stream);
+
+// cache_surface_sky (terrain.wgsl:286-302) into `out` (128 float4): the
+// in-scatter of 16 x 8 directions of the local sky, seen from the camera.
+constexpr uint32_t kSkyCacheTexels = 128;
+cudaError_t launch_sky_cache(const TraceParams &p, float4 *out, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
 // Wavefront integrator (sg_wavefront.cu): the same per-path arithmetic as

@@ -33,7 +33,7 @@ __device__ __forceinline__ void flush_events(const Events &ev, unsigned long lon
 #define SG_TRACE_MIN_BLOCKS 4
 #endif
 
-template <bool C, bool L, bool F>
+template <bool C, bool L, bool F, bool A>
 __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(const __grid_constant__ TraceParams P) {
     extern __shared__ float4 smem[];
     const Scene S = stage_scene(P, smem);
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
         float4 total = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         float3 sky = f3(0.0f, 0.0f, 0.0f);
         Path path;
-        NoGrad nograd;
+        Forward<A> nograd;
         for (uint32_t smp = 0; smp < z; ++smp) {
             start_path(path, &P.s, K, pixel, x, y, smp);
             while (!step(S, K, path, nograd)) {
@@ -398,6 +398,30 @@ cudaError_t launch_fma_peak(int blocks, int iters, float *out, cudaStream_t stre
     return cudaGetLastError();
 }
 
+// cache_surface_sky (terrain.wgsl:286-302): texel (x, y) holds the air's
+// in-scatter along the local direction at azimuth 2 pi (x + 0.5) / 16 and
+// elevation sine (y + 0.5) / 8, seen from the camera, with the random state
+// the reference seeds per texel. Zero without terrain. Built with the
+// settings of an accumulation's first dispatch (counts.y = 0).
+template <bool F>
+__global__ void __launch_bounds__(kThreads) sky_cache_kernel(const __grid_constant__ TraceParams P, float4 *out) {
+    extern __shared__ float4 smem[];
+    const Scene S = stage_scene(P, smem);
+    const uint32_t index = threadIdx.x;
+    if (index >= kSkyTexels) return;
+    float3 light = f3(0.0f, 0.0f, 0.0f);
+    if (P.s.g.atmo_params[3] > 0.5f && P.s.g.ground_counts[1] != 0u) {
+        const uint32_t x = index % 16u, y = index / 16u;
+        const float mu = ((float)y + 0.5f) / 8.0f;
+        const float phi = kTau * ((float)x + 0.5f) / 16.0f;
+        const float r = sqrtf(1.0f - mu * mu);
+        const float3 dir = from_ground(S, f3(r * cosf(phi), mu, r * sinf(phi)));
+        const Counter<false, true, F> K{nullptr};
+        light = atmosphere(S, K, f3(0.0f, 0.0f, 0.0f), dir, 1.0e30f, hash_u32(index ^ 0x91ce452du), 0u).inscatter;
+    }
+    out[index] = make_float4(light.x, light.y, light.z, 0.0f);
+}
+
 size_t trace_smem_bytes(const TraceParams &p) {
     return (size_t)p.s.counts[0] * kBodyVec4 * sizeof(float4) + (size_t)p.staged_table_floats * sizeof(float);
 }
@@ -422,18 +446,30 @@ cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t s
     const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
     // The landscape instantiation only for frames that enable it: the
     // celestial one carries neither its registers nor its code.
+    // Frames with host air run the instantiations that carry its code; the
+    // event-counting ones always do (it is gated at run time there).
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const int which = (count_events ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    const int which = (count_events ? 8 : 0) | (p.air_on ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
     switch (which) {
-        case 0: return launch_variant(trace_kernel<false, false, false>, grid, smem, stream, p);
-        case 1: return launch_variant(trace_kernel<false, false, true>, grid, smem, stream, p);
-        case 2: return launch_variant(trace_kernel<false, true, false>, grid, smem, stream, p);
-        case 3: return launch_variant(trace_kernel<false, true, true>, grid, smem, stream, p);
-        case 4: return launch_variant(trace_kernel<true, false, false>, grid, smem, stream, p);
-        case 5: return launch_variant(trace_kernel<true, false, true>, grid, smem, stream, p);
-        case 6: return launch_variant(trace_kernel<true, true, false>, grid, smem, stream, p);
-        default: return launch_variant(trace_kernel<true, true, true>, grid, smem, stream, p);
+        case 0: return launch_variant(trace_kernel<false, false, false, false>, grid, smem, stream, p);
+        case 1: return launch_variant(trace_kernel<false, false, true, false>, grid, smem, stream, p);
+        case 2: return launch_variant(trace_kernel<false, true, false, false>, grid, smem, stream, p);
+        case 3: return launch_variant(trace_kernel<false, true, true, false>, grid, smem, stream, p);
+        case 4: return launch_variant(trace_kernel<false, false, false, true>, grid, smem, stream, p);
+        case 5: return launch_variant(trace_kernel<false, false, true, true>, grid, smem, stream, p);
+        case 6: return launch_variant(trace_kernel<false, true, false, true>, grid, smem, stream, p);
+        case 7: return launch_variant(trace_kernel<false, true, true, true>, grid, smem, stream, p);
+        case 8: case 12: return launch_variant(trace_kernel<true, false, false, true>, grid, smem, stream, p);
+        case 9: case 13: return launch_variant(trace_kernel<true, false, true, true>, grid, smem, stream, p);
+        case 10: case 14: return launch_variant(trace_kernel<true, true, false, true>, grid, smem, stream, p);
+        default: return launch_variant(trace_kernel<true, true, true, true>, grid, smem, stream, p);
     }
+}
+
+cudaError_t launch_sky_cache(const TraceParams &p, float4 *out, cudaStream_t stream) {
+    const size_t smem = trace_smem_bytes(p);
+    if (p.fp64_sites) return launch_variant(sky_cache_kernel<true>, dim3(1), smem, stream, p, out);
+    return launch_variant(sky_cache_kernel<false>, dim3(1), smem, stream, p, out);
 }
 
 size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a) {

@@ -233,9 +233,7 @@ static __device__ __noinline__ unsigned long long extend_end(const AdjointParams
 }
 
 __device__ __forceinline__ float4 plane6(const Path &p, uint32_t pixel, uint32_t slot) {
-    return make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
-                       __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(pixel),
-                       __uint_as_float(slot));
+    return make_float4(iteration_word(p), depth_word(p), __uint_as_float(pixel), __uint_as_float(slot));
 }
 
 // Stores every plane of a path whose plane 6 carries (pixel, slot).

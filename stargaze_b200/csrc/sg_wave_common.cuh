@@ -29,12 +29,22 @@ namespace {
 //   0  ray.o, ray.anchor            4  ring_base, shine_body
 //   1  ray.d, rng                   5  previous_vertex.o, previous_vertex.anchor
 //   2  throughput, previous_pdf     6  iterations | point_gained << 31,
-//   3  radiance, ring_cap              depth | null_crossings << 16, result slot
+//   3  radiance, ring_cap              depth | null_crossings << 16 | in_air << 30
+//                                      | sky_on_escape << 31, result slot
 // The previous vertex is only ever used for its position (relative_center),
 // so its direction is not stored.
 __device__ __forceinline__ float4 pack3(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 __device__ __forceinline__ float4 pack3u(float3 v, uint32_t w) { return make_float4(v.x, v.y, v.z, __uint_as_float(w)); }
 __device__ __forceinline__ float3 xyz4(float4 v) { return f3(v.x, v.y, v.z); }
+
+// Plane 6's first two words.
+__device__ __forceinline__ float iteration_word(const Path &p) {
+    return __uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u));
+}
+__device__ __forceinline__ float depth_word(const Path &p) {
+    return __uint_as_float(p.depth | (p.null_crossings << 16) | (p.in_air ? 0x40000000u : 0u) |
+                           (p.sky_on_escape ? 0x80000000u : 0u));
+}
 
 __device__ __forceinline__ void store_path(float4 *st, uint32_t pool, uint32_t i, const Path &p, uint32_t slot) {
     st[0 * pool + i] = pack3u(p.ray.o, p.ray.anchor);
@@ -43,8 +53,7 @@ __device__ __forceinline__ void store_path(float4 *st, uint32_t pool, uint32_t i
     st[3 * pool + i] = pack3(p.radiance, p.ring_cap);
     st[4 * pool + i] = pack3u(p.ring_base, p.shine_body);
     st[5 * pool + i] = pack3u(p.previous_vertex.o, p.previous_vertex.anchor);
-    st[6 * pool + i] = make_float4(__uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
-                                   __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(slot), 0.0f);
+    st[6 * pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot), 0.0f);
 }
 
 // Planes 0, 1 and 6: what extend reads. Returns the result slot.
@@ -56,7 +65,9 @@ __device__ __forceinline__ uint32_t load_ray_part(const float4 *st, uint32_t poo
     p.iterations = it & 0x7fffffffu;
     p.point_gained = (it >> 31) != 0u;
     p.depth = dn & 0xffffu;
-    p.null_crossings = dn >> 16;
+    p.null_crossings = (dn >> 16) & 0x3fffu;
+    p.in_air = (dn & 0x40000000u) != 0u;
+    p.sky_on_escape = (dn & 0x80000000u) != 0u;
     p.backdrop = f3(0.0f, 0.0f, 0.0f);  // set only where a path escapes, which ends it
     return __float_as_uint(g.z);
 }

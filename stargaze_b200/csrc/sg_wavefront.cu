@@ -47,7 +47,8 @@ namespace {
 // ---------------------------------------------------------------------------
 // Stages
 // ---------------------------------------------------------------------------
-template <bool L, bool F>
+// A: the host air's code is compiled in (frames with air run these).
+template <bool L, bool F, bool A>
 __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_extend(const __grid_constant__ TraceParams P,
                                                                             const __grid_constant__ WaveParams W,
                                                                             uint32_t t) {
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
     if (blockIdx.x * kThreads >= n) return;
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
-    NoGrad nograd;
+    Forward<A> nograd;
     float4 *st = W.state[t & 1u];
     float4 *H = W.hits;
     uint32_t round = 0;
@@ -98,6 +99,14 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
             } else {
                 slot = load_ray_part(st, W.pool, i, p);
             }
+            // A continuation leaving the host air may be attenuated in
+            // extend: it needs its throughput.
+            const bool was_in_air = A && !fresh && p.in_air;
+            if (was_in_air) {
+                const float4 c = st[2 * W.pool + i];
+                p.throughput = xyz4(c);
+                p.previous_pdf = c.w;
+            }
             if (valid) {
                 Extension e;
                 const bool alive = extend(S, K, p, nograd, e);
@@ -108,9 +117,8 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                         store_path(st, W.pool, i, p, slot);
                     } else {
                         st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
-                        st[6 * W.pool + i] = make_float4(
-                            __uint_as_float(p.iterations | (p.point_gained ? 0x80000000u : 0u)),
-                            __uint_as_float(p.depth | (p.null_crossings << 16)), __uint_as_float(slot), 0.0f);
+                        st[6 * W.pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot), 0.0f);
+                        if (was_in_air) st[2 * W.pool + i] = pack3(p.throughput, p.previous_pdf);
                     }
                     if (ring) H[1 * W.pool + i] = pack3(e.ring.p, e.ring.t);
                     else H[0 * W.pool + i] = pack3(e.hit.n, e.hit.t);
@@ -122,8 +130,12 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                     // surface_vertex's miss). A new path's radiance is still
                     // zero.
                     if (!fresh) load_radiance_part(st, W.pool, i, p);
-                    if (alive && P.sky_on) {
-                        if (!fresh) p.throughput = xyz4(st[2 * W.pool + i]);
+                    if (alive && (P.sky_on || (A && p.sky_on_escape))) {
+                        if (!fresh && !was_in_air) p.throughput = xyz4(st[2 * W.pool + i]);
+                        // A sky-lit local surface's continuation sees the
+                        // surface sky cache (pathtrace.wgsl:1497-1499).
+                        if (A && p.sky_on_escape)
+                            p.radiance = p.radiance + p.throughput * surface_sky_lookup(S, p.ray.d);
                         sky_miss(S, p);
                     }
                     W.results[slot] = finish_path(p);
@@ -141,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
 }
 
 // Ring (R == true) or surface stage over its queue.
-template <bool L, bool F, bool R>
+template <bool L, bool F, bool R, bool A>
 __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
                                                                            const __grid_constant__ WaveParams W,
                                                                            uint32_t t) {
@@ -152,7 +164,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
     if (blockIdx.x * kThreads >= n) return;
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
-    StageGrad nograd;
+    Stage<A> nograd;
     const float4 *st = W.state[t & 1u];
     float4 *out = W.state[(t + 1u) & 1u];
     const float4 *H = W.hits;
@@ -248,22 +260,22 @@ struct StageSet {
     const void *extend, *ring, *surface;
 };
 
-template <bool L, bool F>
+template <bool L, bool F, bool A>
 StageSet stage_set() {
-    return StageSet{(const void *)wave_extend<L, F>, (const void *)wave_shade<L, F, true>,
-                    (const void *)wave_shade<L, F, false>};
+    return StageSet{(const void *)wave_extend<L, F, A>, (const void *)wave_shade<L, F, true, A>,
+                    (const void *)wave_shade<L, F, false, A>};
 }
 
-template <bool L, bool F>
+template <bool L, bool F, bool A>
 cudaError_t run_iteration(const TraceParams &p, const WaveParams &w, uint32_t t, const int (&grid)[3], size_t smem,
                           cudaStream_t stream, StageMarks *m) {
     cudaError_t e;
     if ((e = mark(m, kStageExtend, stream)) != cudaSuccess) return e;
-    wave_extend<L, F><<<grid[0], kThreads, smem, stream>>>(p, w, t);
+    wave_extend<L, F, A><<<grid[0], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageRing, stream)) != cudaSuccess) return e;
-    wave_shade<L, F, true><<<grid[1], kThreads, smem, stream>>>(p, w, t);
+    wave_shade<L, F, true, A><<<grid[1], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageSurface, stream)) != cudaSuccess) return e;
-    wave_shade<L, F, false><<<grid[2], kThreads, smem, stream>>>(p, w, t);
+    wave_shade<L, F, false, A><<<grid[2], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageGap, stream)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -287,8 +299,18 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
     if (marks) marks->used = 0;
     if (z == 0 || pixels == 0) return cudaSuccess;
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const StageSet set = land ? (p.fp64_sites ? stage_set<true, true>() : stage_set<true, false>())
-                              : (p.fp64_sites ? stage_set<false, true>() : stage_set<false, false>());
+    const int variant = (p.air_on ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    StageSet set;
+    switch (variant) {
+        case 0: set = stage_set<false, false, false>(); break;
+        case 1: set = stage_set<false, true, false>(); break;
+        case 2: set = stage_set<true, false, false>(); break;
+        case 3: set = stage_set<true, true, false>(); break;
+        case 4: set = stage_set<false, false, true>(); break;
+        case 5: set = stage_set<false, true, true>(); break;
+        case 6: set = stage_set<true, false, true>(); break;
+        default: set = stage_set<true, true, true>(); break;
+    }
     const size_t smem = trace_smem_bytes(p);
     const void *fns[3] = {set.extend, set.ring, set.surface};
     int grid[3];
@@ -327,10 +349,16 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
         for (uint64_t t = 0;; ++t) {
             if (t >= bound) return cudaErrorLaunchTimeout;
             const uint32_t it = (uint32_t)t;
-            e = land ? (p.fp64_sites ? run_iteration<true, true>(p, w, it, grid, smem, stream, marks)
-                                     : run_iteration<true, false>(p, w, it, grid, smem, stream, marks))
-                     : (p.fp64_sites ? run_iteration<false, true>(p, w, it, grid, smem, stream, marks)
-                                     : run_iteration<false, false>(p, w, it, grid, smem, stream, marks));
+            switch (variant) {
+                case 0: e = run_iteration<false, false, false>(p, w, it, grid, smem, stream, marks); break;
+                case 1: e = run_iteration<false, true, false>(p, w, it, grid, smem, stream, marks); break;
+                case 2: e = run_iteration<true, false, false>(p, w, it, grid, smem, stream, marks); break;
+                case 3: e = run_iteration<true, true, false>(p, w, it, grid, smem, stream, marks); break;
+                case 4: e = run_iteration<false, false, true>(p, w, it, grid, smem, stream, marks); break;
+                case 5: e = run_iteration<false, true, true>(p, w, it, grid, smem, stream, marks); break;
+                case 6: e = run_iteration<true, false, true>(p, w, it, grid, smem, stream, marks); break;
+                default: e = run_iteration<true, true, true>(p, w, it, grid, smem, stream, marks); break;
+            }
             if (e != cudaSuccess) return e;
             run->iterations += 1;
             run->kernels += 3;

@@ -239,3 +239,24 @@ def render_options(wl: Workload, spp: int = 64, noise_seed: int = 0) -> abi.Opti
     o.milky_way = 0.0
     o.noise_seed = noise_seed & 0xFFFFFFFF
     return o
+
+
+def earthlike_air() -> dict:
+    """`Atmosphere::earthlike` (src/sim.rs:295-306): sea-level Rayleigh
+    5.8, 13.5, 33.1 and Mie 21 per million metres, 8.5 km scale height,
+    80 km thick, Mie asymmetry 0.76; lengths in AU."""
+    return dict(scale_height=8500.0 / AU_M, thickness=80000.0 / AU_M,
+                rayleigh=[5.8e-6 * AU_M, 13.5e-6 * AU_M, 33.1e-6 * AU_M], mie=21.0e-6 * AU_M, mie_g=0.76)
+
+
+def with_air(frame: Frame, host_index: int, air: dict | None = None) -> Frame:
+    """Give body `host_index` of a packed frame its air, as `build_frame`
+    does (src/main.rs:941-962): the centre and radius of the host's packed
+    sphere, the coefficients, and atmo_params.w = host index + 1."""
+    a = air or earthlike_air()
+    host = frame.bodies[host_index]
+    g = frame.globals
+    g.atmo_center[:] = [host.center[0], host.center[1], host.center[2], host.radius]
+    g.atmo_rayleigh[:] = [*a["rayleigh"], a["mie"]]
+    g.atmo_params[:] = [a["mie_g"], a["scale_height"], a["thickness"], float(host_index + 1)]
+    return frame

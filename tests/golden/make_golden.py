@@ -1,6 +1,6 @@
 """Generate the golden fixtures under tests/golden/ with the CPU oracle.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [image names]
 
 The oracle is itself pinned against the reference's known-answer tests
 (tests/test_oracle_known_answers.py); these fixtures freeze its outputs on
@@ -26,7 +26,7 @@ import known_answers as ka  # noqa: E402
 from stargaze_b200 import abi  # noqa: E402
 from stargaze_b200.pathtracer import rays_array  # noqa: E402
 from stargaze_b200.scene import body, frame  # noqa: E402
-from stargaze_b200.workloads import rings_1080p, spheres_256, terrain_1080p  # noqa: E402
+from stargaze_b200.workloads import rings_1080p, spheres_256, terrain_1080p, with_air  # noqa: E402
 
 N_RAYS = 2048
 
@@ -129,6 +129,7 @@ IMAGES = {
     "spheres_64": (spheres_256, 64, 64, 16, 2),
     "rings_96x54": (rings_1080p, 96, 54, 16, 2),
     "terrain_96x54": (None, 96, 54, 16, 2),
+    "terrain_air_96x54": (None, 96, 54, 16, 2),
 }
 
 
@@ -136,6 +137,8 @@ def image_workload(name):
     factory, w, h, spp, batches = IMAGES[name]
     if factory is None:
         wl, land = terrain_small(width=w, height=h)
+        if "air" in name:
+            with_air(wl.frame, 1)
         return wl, land
     return factory(width=w, height=h), None
 
@@ -150,9 +153,9 @@ def image_fixture(name):
     return t.read_pixels()
 
 
-def image_fixtures():
+def image_fixtures(names=None):
     out = {}
-    for name in IMAGES:
+    for name in names or IMAGES:
         img = image_fixture(name)
         np.savez_compressed(HERE / f"image_{name}.npz", image=img)
         out[name] = float(img[:, :3].mean())
@@ -160,5 +163,9 @@ def image_fixtures():
 
 
 if __name__ == "__main__":
-    print(ray_fixtures())
-    print(image_fixtures())
+    # With image names as arguments, only those image fixtures are rebuilt.
+    if len(sys.argv) > 1:
+        print(image_fixtures(sys.argv[1:]))
+    else:
+        print(ray_fixtures())
+        print(image_fixtures())

@@ -484,3 +484,171 @@ def heightfield_oracle(make, heights: np.ndarray, data: np.ndarray, cells: int, 
                 assert np.all(np.isfinite(n)) and abs(np.linalg.norm(n) - 1.0) < 1e-4 and n[1] > 0.0, (radius, k, n)
             results.append((radius, k, actual, expected))
     return results
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:842-994 — gpu_atmosphere
+# ---------------------------------------------------------------------------
+AU_KM = 149_597_870.7
+
+
+def earthlike() -> dict:
+    """`Atmosphere::earthlike` (src/sim.rs:295-306), coefficients per AU."""
+    au_m = AU_KM * 1000.0
+    return dict(scale_height=8500.0 / au_m, thickness=80000.0 / au_m,
+                rayleigh=[5.8e-6 * au_m, 13.5e-6 * au_m, 33.1e-6 * au_m], mie=21.0e-6 * au_m, mie_g=0.76)
+
+
+def dense() -> dict:
+    """`Atmosphere::dense` (src/sim.rs:287-292): three times the scattering."""
+    a = earthlike()
+    a["rayleigh"] = [b * 3.0 for b in a["rayleigh"]]
+    a["mie"] *= 3.0
+    return a
+
+
+def set_air(f, a: dict, center, radius: float, host: float = 1.0) -> None:
+    f.globals.atmo_center[:] = [center[0], center[1], center[2], radius]
+    f.globals.atmo_rayleigh[:] = [*a["rayleigh"], a["mie"]]
+    f.globals.atmo_params[:] = [a["mie_g"], a["scale_height"], a["thickness"], host]
+
+
+def catalogue_star(bright: float = 1.0) -> dict:
+    return dict(dir=[0.0, 0.0, -1.0], color=[1.0, 1.0, 1.0], bright=bright, angular_radius=0.01)
+
+
+def atmosphere(make) -> dict:
+    from stargaze_b200 import sky
+
+    opts = test_options(samples_per_frame=64, max_bounces=1, exposure=1.0)
+    background = catalogue_star()
+    tracer = make((1, 1), opts)
+    tracer.upload_catalogue(*sky.ray_catalogue([background]))
+    f = frame()
+    a = earthlike()
+    radius = np.float32(6371.0 / AU_KM)
+    # The camera looks straight up, two metres above the host surface.
+    center = [0.0, 0.0, float(np.float32(radius + np.float32(0.002 / AU_KM)))]
+    f.bodies = [body(center, float(radius), [0.0] * 3, False)]
+    set_air(f, a, center, float(radius))
+    attenuated = sample(tracer, f, 1)[0]
+    star = sky.radiance(background)
+    # Eight midpoint cells integrate an exponential profile to exactly
+    # x / (2 sinh(x / 2)) times the continuous column, x one cell's
+    # thickness in scale heights.
+    h, top = a["scale_height"], a["thickness"]
+    column = h * (math.exp(-0.002 / AU_KM / h) - math.exp(-top / h))
+    x = (top - 0.002 / AU_KM) / (8.0 * h)
+    midpoint = column * x / (2.0 * math.sinh(x * 0.5))
+    for c in range(3):
+        expected = float(np.float32(math.exp(-(a["rayleigh"][c] + a["mie"]) * midpoint))) * star[c]
+        assert abs(attenuated[c] - expected) < 0.001 * expected, (c, attenuated[c], expected)
+    f.globals.atmo_params[3] = 0.0
+    unattenuated = sample(tracer, f, 1)[0]
+    for c in range(3):
+        assert abs(unattenuated[c] - star[c]) <= 1e-5 * star[c], (unattenuated, star)
+    assert unattenuated[3] == 0.0
+    f.globals.atmo_params[3] = 1.0
+
+    # No catalogue: any light in this zenith ray comes from scattering.
+    tracer = make((1, 1), opts)
+    f.bodies.append(body([1.0, 0.0, -1.0], 0.005, [100_000.0] * 3, True))
+    day = sample(tracer, f, 4)[0]
+    assert np.all(np.isfinite(day[:3])) and np.all(day[:3] > 0.01), day
+    assert day[2] > day[0], day
+    f.bodies.append(body([0.5, 0.0, -0.5], 0.05, [0.0] * 3, False))
+    eclipsed = sample(tracer, f, 4)[0]
+    assert np.array_equal(eclipsed, np.zeros(4, np.float32)), eclipsed
+    f.bodies.pop()
+    f.bodies[1].center[:] = [1.0, 0.0, 0.03]
+    twilight = sample(tracer, f, 4)[0]
+    assert twilight[0] > 0.0001, twilight
+    f.bodies[1].center[:] = [0.0, 0.0, 1.0]
+    assert np.array_equal(sample(tracer, f, 1)[0], np.zeros(4, np.float32))
+
+    # Dense haze hides the catalogue by day, keeps it by night and while an
+    # eclipse shadows the air.
+    d = dense()
+    f.globals.atmo_rayleigh[:] = [*d["rayleigh"], d["mie"]]
+    bright = catalogue_star(1.62)
+    with_stars = make((1, 1), opts)
+    with_stars.upload_catalogue(*sky.ray_catalogue([bright]))
+    night = sample(with_stars, f, 4)[0]
+    star = sky.radiance(bright)
+    assert night[0] > 0.3 * star[0], night
+    f.bodies[1] = body([1.0, 0.0, -1.0], 0.005, [44_444.0] * 3, True)
+    day_sky = sample(tracer, f, 4)[0]
+    day_stars = sample(with_stars, f, 4)[0]
+    for c in range(3):
+        assert abs(day_stars[c] - day_sky[c]) < 0.03 * day_sky[c], (day_stars, day_sky)
+    f.bodies.append(body([0.5, 0.0, -0.5], 0.05, [0.0] * 3, False))
+    eclipse = sample(with_stars, f, 4)[0]
+    for c in range(3):
+        assert abs(eclipse[c] - night[c]) < 0.01 * night[c] + 1e-9, (eclipse, night)
+    return dict(attenuated=attenuated, day=day, twilight=twilight, night=night, day_sky=day_sky,
+                day_stars=day_stars, eclipse=eclipse)
+
+
+# ---------------------------------------------------------------------------
+# src/pathtracer_tests.rs:996-1104 — gpu_reflected_atmosphere
+# ---------------------------------------------------------------------------
+def reflected_atmosphere(make) -> dict:
+    """The glow is the difference of two renders. The reference takes them
+    from one tracer (independent noise sequences); the daylight case then
+    compares the day sky's noise, about 2e-4 of it at 2048 samples (the Mie
+    lobe varies by +-2.5 % across the sun's disc), with 2 % of the glow. Here
+    both renders use the same sequence (common random numbers): planetshine
+    draws from its own stream, so the difference is the glow alone."""
+    opts = test_options(samples_per_frame=64, max_bounces=1)
+    f = frame()
+    a = earthlike()
+    radius = np.float32(6371.0 / AU_KM)
+    center = [0.0, 0.0, float(np.float32(radius + np.float32(0.002 / AU_KM)))]
+    set_air(f, a, center, float(radius))
+    # A large moon just outside the zenith ray; the sun is below the host's
+    # horizon but lights the moon without a lunar eclipse.
+    f.bodies = [body(center, float(radius), [0.0] * 3, False),
+                body([0.0004, 0.0, -0.002], 0.00015, [0.8] * 3, False),
+                body([0.3, 0.0, 1.0], 0.005, [100_000.0] * 3, True)]
+
+    def glow():
+        color = list(f.bodies[1].color)
+        f.bodies[1].color[:] = [0.0] * 3
+        background = sample(make((1, 1), opts), f, 32)[0]
+        f.bodies[1].color[:] = color
+        lit = sample(make((1, 1), opts), f, 32)[0]
+        return np.array([lit[c] - background[c] for c in range(3)], np.float64)
+
+    full = glow()
+    assert np.all(np.isfinite(full)) and np.all(full > 1e-4), full
+    f.bodies[1].color[:] = [0.4, 0.2, 0.1]
+    tinted = glow()
+    for c in range(3):
+        expected = full[c] * [0.5, 0.25, 0.125][c]
+        assert abs(tinted[c] - expected) < expected * 0.02, (tinted, full)
+    f.bodies[1].color[:] = [0.8] * 3
+    f.bodies[1].radius *= 0.5
+    small = glow()
+    assert full[0] * 0.15 < small[0] < full[0] * 0.35, (small, full)
+    f.bodies[1].radius *= 2.0
+    f.bodies[2].center[:] = [1.0, 0.0, 0.0]
+    quarter = glow()
+    f.bodies[2].center[:] = [-0.3, 0.0, -1.0]
+    new = glow()
+    assert full[0] * 0.1 < quarter[0] < full[0] * 0.6, (quarter, full)
+    assert abs(new[0]) < full[0] * 0.02, (new, full)
+    f.bodies[2].center[:] = [0.3, 0.0, 1.0]
+    # Starlight blocked on its way to the moon.
+    f.bodies.append(body([0.1502, 0.0, 0.499], 0.01, [0.0] * 3, False))
+    eclipsed = glow()
+    assert np.all(np.abs(eclipsed) < 1e-6), eclipsed
+    f.bodies.pop()
+    # Moonlight blocked on its way to the air.
+    f.bodies.append(body([0.0002, 0.0, -0.001], 0.00012, [0.0] * 3, False))
+    hidden = glow()
+    assert np.all(np.abs(hidden) < 1e-6), hidden
+    f.bodies.pop()
+    f.globals.atmo_params[3] = 0.0
+    airless = glow()
+    assert np.all(np.abs(airless) < 1e-6), airless
+    return dict(full=full, tinted=tinted, small=small, quarter=quarter, new=new)

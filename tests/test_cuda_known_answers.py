@@ -6,6 +6,7 @@ import pytest
 
 import known_answers as ka
 from stargaze_b200 import PathTracer, abi
+from stargaze_b200._lib import StargazeError
 
 pytestmark = pytest.mark.gpu
 
@@ -87,3 +88,44 @@ def test_shadow_queries_match_closest_hits(stars):
                 t = np.float32(t * p[2])
         ref[k] = t
     assert np.array_equal(vis, ref)
+
+
+def test_atmosphere():
+    r = ka.atmosphere(make)
+    assert r["day"][2] > r["day"][0]
+
+
+@pytest.mark.parametrize("integrator", ["megakernel", "wavefront"])
+def test_reflected_atmosphere(integrator):
+    def make_with(dimensions, options):
+        t = PathTracer(dimensions, options)
+        t.set_integrator(integrator)
+        return t
+
+    r = ka.reflected_atmosphere(make_with)
+    assert r["small"][0] < r["full"][0]
+
+
+def test_atmosphere_matches_oracle_pixel_for_pixel():
+    """The zenith-sky scenario's renders, CUDA against the oracle: the same
+    random sequences through the camera air, planetshine and the fresh
+    frame's four-stratum light samples."""
+    from oracle.binding import OracleTracer
+
+    outs = []
+    for cls in (PathTracer, OracleTracer):
+        outs.append(ka.atmosphere(lambda d, o, cls=cls: cls(d, o)))
+    cuda, cpu = outs
+    for key in cpu:
+        ref = np.asarray(cpu[key], np.float64)
+        got = np.asarray(cuda[key], np.float64)
+        assert np.all(np.abs(got - ref) <= 2e-5 * np.abs(ref) + 1e-12), (key, got, ref)
+
+
+def test_air_frames_are_not_differentiated():
+    f = ka.frame()
+    ka.set_air(f, ka.earthlike(), [0.0, 0.0, 1e-4], 4e-5)
+    t = PathTracer((2, 2), ka.test_options())
+    t.encode(f)
+    with pytest.raises(StargazeError, match="host air"):
+        t.backward(f, t.tape(), np.ones((4, 4), np.float32))

@@ -116,3 +116,21 @@ def test_rng_matches_wgsl(seed):
         b, ostate = oracle_random(ostate)
         assert a == b and state == ostate
         assert 0.0 <= a < 1.0
+
+
+def test_atmosphere():
+    r = ka.atmosphere(make)
+    assert r["day"][2] > r["day"][0]
+
+
+def test_reflected_atmosphere():
+    r = ka.reflected_atmosphere(make)
+    assert r["small"][0] < r["full"][0]
+
+
+def test_air_frames_are_not_differentiated():
+    f = ka.frame()
+    ka.set_air(f, ka.earthlike(), [0.0, 0.0, 1e-4], 4e-5)
+    tracer = make((2, 2), ka.test_options())
+    with pytest.raises(Exception):
+        tracer.tangent(f, 0, 1)
