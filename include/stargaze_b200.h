@@ -341,6 +341,15 @@ SG_API int sg_ring_energy(sg_context *ctx, float albedo, float tau, float mu,
  * accumulation on the next encode. */
 SG_API int sg_set_fp64_sites(sg_context *ctx, int enable);
 
+/* The guided ground sampler: `guided` of PathTracer::new_with_guided_ground
+ * (src/pathtracer.rs:305-312; the sampler is src/guided_ground.rs:14-79).
+ * In frames with host air, a camera ray's local surface picks a reflecting
+ * body (sample_reflector) and draws half of its continuations toward it,
+ * weighting next-event and continuation by the full mixture density. Off by
+ * default (the reference's plain constructor); the reference's app turns it
+ * on. Changing it resets the accumulation on the next encode. */
+SG_API int sg_set_guided_ground(sg_context *ctx, int enable);
+
 /* Extension (no reference counterpart; the reference has one WGSL compute
  * pass, pathtrace.wgsl:1645-1675): which CUDA integrator sg_encode runs.
  *   SG_INTEGRATOR_MEGAKERNEL  one thread per pixel walks every path of the

@@ -38,6 +38,7 @@ class Tables(C.Structure):
         ("catalogue_n", C.c_uint32),
         ("sky_cells", C.c_void_p),
         ("milky_way", C.c_void_p),
+        ("guided_ground", C.c_uint32),
     ]
 
 
@@ -131,6 +132,7 @@ class TableSet:
         self.catalogue: np.ndarray | None = None
         self.sky_cells: np.ndarray | None = None
         self.milky: np.ndarray | None = None
+        self.guided_ground = False
 
     def upload(self, slot: int, tau) -> None:
         self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
@@ -196,6 +198,7 @@ class TableSet:
             t.sky_cells = self.sky_cells.ctypes.data
         if self.milky is not None:
             t.milky_way = self.milky.ctypes.data
+        t.guided_ground = 1 if self.guided_ground else 0
         return t
 
 
@@ -304,6 +307,13 @@ class OracleTracer:
 
     def upload_milky_way(self, texels) -> None:
         self.tables.upload_milky_way(texels)
+
+    def set_guided_ground(self, enable: bool) -> None:
+        """The guided ground sampler (src/guided_ground.rs:14-79); like a
+        new tracer, a change restarts the accumulation."""
+        if bool(enable) != self.tables.guided_ground:
+            self.tables.guided_ground = bool(enable)
+            self.tables.version += 1
 
     def encode(self, frame: Frame, stream=None, rows=None) -> None:
         if len(frame.bodies) > abi.BODY_CAPACITY:

@@ -1452,6 +1452,22 @@ static v3 reflected_radiance(const scene *S, ray_t ray, uint32_t index, uint32_t
     return radiance;
 }
 
+/* ground_reflector_pdf: src/guided_ground.rs:21-37 */
+static float ground_reflector_pdf(const scene *S, ray_t ray) {
+    uint32_t host = (uint32_t)S->s->g.atmo_params[3] - 1u;
+    float total = 0.0f, density = 0.0f;
+    for (uint32_t b = 0; b < S->s->counts[0]; b++) {
+        if (b == host || b_emissive(S, b) > 0.5f) continue;
+        float width = cone_width(S, ray, b);
+        v3 c = b_color(S, b);
+        float weight = width * maxf_(c.x, maxf_(c.y, c.z));
+        if (weight <= 0.0f) continue;
+        total += weight;
+        if (sphere_hit(S, ray, b).index != MISS) density += weight / (TAU_F * width);
+    }
+    return density / maxf_(total, 1.0e-30f);
+}
+
 /* brightest_risen_light: pathtrace.wgsl:1078-1089 */
 static float brightest_risen_light(const scene *S, v3 origin) {
     ray_t ray = {origin, V(0.0f, 0.0f, -1.0f), MISS};
@@ -1929,6 +1945,11 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
             outgoing.dir = normal;
             outgoing.anchor = hit.index;
         }
+        /* The guided ground sampler (src/guided_ground.rs:38-48). */
+        reflector_t ground_reflector = {MISS, 0.0f};
+        if (S->t && S->t->guided_ground && local && depth == 0u && st->g.atmo_params[3] > 0.5f)
+            ground_reflector = sample_reflector(S, camera_origin(S, outgoing), rng);
+        int guided = ground_reflector.index != MISS;
         v3 direct_light = V(0, 0, 0), ddirect_light = V(0, 0, 0);
         int last_vertex = depth + 1u == st->counts[3];
         uint32_t count = light_count(S);
@@ -1942,7 +1963,9 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
             float visibility = light_visibility(S, outgoing, i);
             if (visibility > 0.0f) {
                 float bsdf_pdf = cosine / PI_F;
-                float weight = power_weight(sample.pdf, bsdf_pdf);
+                float path_pdf = bsdf_pdf;
+                if (guided) path_pdf = 0.5f * (bsdf_pdf + ground_reflector_pdf(S, outgoing));
+                float weight = power_weight(sample.pdf, path_pdf);
                 if (last_vertex) weight = 1.0f;
                 v3 color = b_color(S, i);
                 if (air_on(S)) color = vmulv(color, air_transmittance(S, outgoing, sample.dir));
@@ -1992,10 +2015,20 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
         float cosine = sqrtf(1.0f - u);
         outgoing.dir = basis_direction(normal, sqrtf(u) * cosf(phi), sqrtf(u) * sinf(phi), cosine);
         previous_pdf = cosine / PI_F;
+        /* src/guided_ground.rs:59-76 */
+        float path_weight = 1.0f;
+        if (guided) {
+            if (rnd(S, rng) < 0.5f) outgoing.dir = sample_light(S, outgoing, ground_reflector.index, rng).dir;
+            float sampled_cosine = maxf_(vdot(normal, outgoing.dir), 0.0f);
+            if (sampled_cosine == 0.0f) break;
+            float brdf_pdf = sampled_cosine / PI_F;
+            previous_pdf = 0.5f * (brdf_pdf + ground_reflector_pdf(S, outgoing));
+            path_weight = brdf_pdf / previous_pdf;
+        }
         if (D) dthroughput = vadd(vmulv(dthroughput, albedo), vmulv(throughput, dalbedo));
         if (D && captured) dthroughput_full = vadd(vmulv(dthroughput_full, albedo), vmulv(throughput, dalbedo));
         dlog_previous_pdf = 0.0f;
-        throughput = vmulv(throughput, albedo);
+        throughput = vmulv(throughput, vmul(albedo, path_weight));
         if (depth >= 2u) {
             float survival = clampf_(maxf_(throughput.x, maxf_(throughput.y, throughput.z)), 0.05f, 0.95f);
             int survived = rnd(S, rng) < survival;

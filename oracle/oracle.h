@@ -51,6 +51,8 @@ typedef struct oracle_tables {
     uint32_t catalogue_n;
     const uint32_t *sky_cells;
     const uint32_t *milky_way;
+    /* The guided ground sampler (src/guided_ground.rs:14-79) when nonzero. */
+    uint32_t guided_ground;
 } oracle_tables;
 
 /* Floats of the reference terrain layout for `cells` cells per side

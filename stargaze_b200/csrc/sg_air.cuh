@@ -254,6 +254,29 @@ __device__ __forceinline__ float3 reflected_radiance(const Scene &S, Counter<C, 
     return radiance;
 }
 
+// ground_reflector_pdf (src/guided_ground.rs:21-37): the reflector half of
+// the guided mixture's density along `ray` — every candidate's cone density
+// where the ray hits it, weighted by its selection probability.
+template <bool C, bool L, bool F>
+static __device__ __noinline__ float ground_reflector_pdf(Scene S, Counter<C, L, F> K, Ray ray) {
+    const uint32_t host = (uint32_t)S.s->g.atmo_params[3] - 1u;
+    float total = 0.0f, density = 0.0f;
+    const uint32_t n = S.s->counts[0];
+#pragma unroll 1
+    for (uint32_t b = 0; b < n; ++b) {
+        const float4 material = bf(S, b, kMaterial);
+        if (b == host || material.w > 0.5f) continue;
+        const float radius = b_radius(S, b);
+        const float width = cone_width_oc(relative_center(S, ray, b), radius);
+        const float weight = width * fmaxf(material.x, fmaxf(material.y, material.z));
+        if (weight <= 0.0f) continue;
+        total += weight;
+        float delta;
+        if (sphere_distance(S, K, ray, b, radius, delta) < 1.0e30f) density += weight / (kTau * width);
+    }
+    return density / fmaxf(total, 1.0e-30f);
+}
+
 // brightest_risen_light (pathtrace.wgsl:1078-1089).
 __device__ __forceinline__ float brightest_risen_light(const Scene &S, float3 origin) {
     const Ray ray{origin, f3(0.0f, 0.0f, -1.0f), kMiss};

@@ -79,6 +79,7 @@ struct sg_context {
     uint32_t map_width = 0, map_height = 0;
     float map_extent = 0.0f;
     bool fp64_sites = false;                // ring plane, host sphere, 5 mm offset in FP64
+    bool guided_ground = false;             // the guided ground sampler (air frames)
     // Wavefront integrator (sg_set_integrator), buffers allocated on first use.
     int integrator = SG_INTEGRATOR_WAVEFRONT;
     uint32_t wave_pool_request = 0;         // 0: the default pool
@@ -210,6 +211,7 @@ std::vector<uint8_t> history_key(const sg_context *ctx, const sg_frame *frame) {
     append(key, ctx->options.milky_way);
     append(key, ctx->table_version);
     append(key, ctx->fp64_sites);
+    append(key, ctx->guided_ground);
     return key;
 }
 
@@ -405,6 +407,7 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.backdrop = ctx->backdrop;
     p.air_on = s.g.atmo_params[3] >= 0.5f ? 1u : 0u;
     p.sky_light = ctx->sky_light;
+    p.guided_ground = ctx->guided_ground ? 1u : 0u;
     return p;
 }
 
@@ -1279,6 +1282,12 @@ int sg_get_stage_times(const sg_context *ctx, float *ms) {
 int sg_set_fp64_sites(sg_context *ctx, int enable) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     ctx->fp64_sites = enable != 0;
+    return SG_OK;
+}
+
+int sg_set_guided_ground(sg_context *ctx, int enable) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    ctx->guided_ground = enable != 0;
     return SG_OK;
 }
 

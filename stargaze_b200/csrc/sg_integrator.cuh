@@ -389,6 +389,17 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
             // Celestial surfaces keep a body-relative origin.
             outgoing = Ray{normal * (radius * (1.0f + 2.0e-6f)), normal, bi};
         }
+        // The guided ground sampler (src/guided_ground.rs:38-48): a camera
+        // ray's local surface under air picks a reflector (main random
+        // stream) to propose half of its continuations toward.
+        [[maybe_unused]] Reflector ground_reflector{kMiss, 0.0f};
+        bool guided = false;
+        if constexpr (G::air && L) {
+            if (S.p->guided_ground && local && depth == 0u && s->g.atmo_params[3] > 0.5f) {
+                ground_reflector = sample_reflector(S, K, camera_origin(S, outgoing), rng);
+                guided = ground_reflector.index != kMiss;
+            }
+        }
         const bool last_vertex = depth + 1u == max_vertices;
         // The adjoint needs the albedo (and its parameter) before the light
         // loop; the forward evaluates it after, as the WGSL does.
@@ -423,7 +434,13 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
             }
             if (visibility > 0.0f) {
                 const float bsdf_pdf = cosine / kPi;
-                const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, bsdf_pdf);
+                // MIS against the full continuation density (the guided
+                // mixture's where it applies; src/guided_ground.rs:50-57).
+                float path_pdf = bsdf_pdf;
+                if constexpr (G::air && L) {
+                    if (guided) path_pdf = 0.5f * (bsdf_pdf + ground_reflector_pdf(S, K, outgoing));
+                }
+                const float weight = last_vertex ? 1.0f : power_weight(sample.pdf, path_pdf);
                 float3 color = xyz(light_material);
                 if constexpr (G::air) {
                     if (S.p->air_on) color = color * air_transmittance(S, outgoing, sample.d);
@@ -473,7 +490,24 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
         const float su = sqrtf(u);
         outgoing.d = basis_direction(normal, su * cp, su * sp, cosine);
         previous_pdf = cosine / kPi;
-        throughput = throughput * albedo;
+        float path_weight = 1.0f;
+        if constexpr (G::air && L) {
+            // src/guided_ground.rs:59-76: half the continuations toward the
+            // reflector, weighted by cosine density over the mixture's.
+            if (guided) {
+                if (rnd(K, rng) < 0.5f) {
+                    const LightSample toward = sample_light(S, K, outgoing, ground_reflector.index, rng);
+                    rng = toward.rng;
+                    outgoing.d = toward.d;
+                }
+                const float sampled_cosine = fmaxf(dot(normal, outgoing.d), 0.0f);
+                if (sampled_cosine == 0.0f) return true;
+                const float brdf_pdf = sampled_cosine / kPi;
+                previous_pdf = 0.5f * (brdf_pdf + ground_reflector_pdf(S, K, outgoing));
+                path_weight = brdf_pdf / previous_pdf;
+            }
+        }
+        throughput = throughput * (albedo * path_weight);
         if constexpr (G::adjoint) {
             factor(grad, albedo_e);
             grad.prev_param = kNoParam;

@@ -51,6 +51,9 @@ struct TraceParams {
     // texels (terrain.wgsl:286-302), built when an accumulation starts.
     uint32_t air_on;
     const float4 *sky_light;
+    // The guided ground sampler (src/guided_ground.rs:14-79): depth-0 local
+    // surfaces under air also propose directions toward a reflecting body.
+    uint32_t guided_ground;
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,

@@ -114,6 +114,11 @@ class PathTracer:
         FP64 (extension; off: the reference's f32 arithmetic)."""
         check(self._lib.sg_set_fp64_sites(self._ctx, int(bool(enable))), self._ctx)
 
+    def set_guided_ground(self, enable: bool) -> None:
+        """The guided ground sampler of `PathTracer::new_with_guided_ground`
+        (the reference app's default; off here as in `PathTracer::new`)."""
+        check(self._lib.sg_set_guided_ground(self._ctx, int(bool(enable))), self._ctx)
+
     def set_integrator(self, integrator: str, pool_paths: int = 0) -> None:
         """"wavefront" (default; stage kernels over a pool of `pool_paths`
         paths in device memory, 0 = default pool) or "megakernel" (one

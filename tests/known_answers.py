@@ -652,3 +652,48 @@ def reflected_atmosphere(make) -> dict:
     airless = glow()
     assert np.all(np.abs(airless) < 1e-6), airless
     return dict(full=full, tinted=tinted, small=small, quarter=quarter, new=new)
+
+
+# ---------------------------------------------------------------------------
+# The guided ground sampler (src/guided_ground.rs:14-79)
+# ---------------------------------------------------------------------------
+def moonlit_ground_frame(size: int = 4):
+    """`local_frame` at night under earthlike air: the star set 17 degrees
+    below the horizon, a large sunlit moon (0.1 rad across, albedo 0.5) high
+    in the south. The ground sees the moon only through continuations (the
+    moon is not a light), the case the guided sampler aims at."""
+    f = local_frame(6_371_000.0)
+    f.globals.viewport[:] = [float(size), float(size), 1.0, 1.0]
+    f.globals.cam_forward[3] = 0.05
+    host = f.bodies[0]
+    set_air(f, earthlike(), list(host.center), host.radius, host=1.0)
+    up = np.array(f.globals.ground_up[:3], np.float64)
+    north = np.array(f.globals.ground_north[:3], np.float64)
+    sun_dir = -0.3 * up + north
+    sun_dir /= np.linalg.norm(sun_dir)
+    f.bodies[1] = body(list(sun_dir * 1.0), 0.00465, [40_000.0] * 3, True)
+    moon_dir = 0.8 * up - 0.6 * north
+    moon_dir /= np.linalg.norm(moon_dir)
+    d = 3.0e-4
+    f.bodies.append(body(list(moon_dir * d), d * 0.05, [0.5] * 3, False))
+    return f
+
+
+def guided_ground_is_unbiased(make, batches: int = 24) -> dict:
+    """Plain and guided estimates of the moonlit ground agree; the guided
+    one has the lower variance. Batch means give the standard errors."""
+    f = moonlit_ground_frame()
+    out = {}
+    for guided in (False, True):
+        means = []
+        for k in range(batches):
+            t = make((4, 4), test_options(samples_per_frame=64, max_bounces=3, noise_seed=1000 * k + 7))
+            t.set_guided_ground(guided)
+            means.append(float(sample(t, f, 1)[:, :3].mean()))
+        m = np.array(means)
+        out[guided] = (m.mean(), m.std(ddof=1) / np.sqrt(len(m)))
+    (mp, sp), (mg, sg) = out[False], out[True]
+    assert mg > 0.0 and mp > 0.0, out
+    assert abs(mg - mp) < 4.0 * np.hypot(sp, sg), out
+    assert sg < sp, out
+    return dict(plain=out[False], guided=out[True])

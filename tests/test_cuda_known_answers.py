@@ -129,3 +129,36 @@ def test_air_frames_are_not_differentiated():
     t.encode(f)
     with pytest.raises(StargazeError, match="host air"):
         t.backward(f, t.tape(), np.ones((4, 4), np.float32))
+
+
+@pytest.mark.parametrize("integrator", ["megakernel", "wavefront"])
+def test_guided_ground_is_unbiased(integrator):
+    def make_with(dimensions, options):
+        t = PathTracer(dimensions, options)
+        t.set_integrator(integrator)
+        return t
+
+    ka.guided_ground_is_unbiased(make_with)
+
+
+@pytest.mark.parametrize("guided", [False, True])
+@pytest.mark.parametrize("integrator", ["megakernel", "wavefront"])
+def test_moonlit_ground_matches_oracle(integrator, guided):
+    """The guided ground sampler and the air's extinction of next-event and
+    continuations, CUDA against the oracle on the same random sequences."""
+    from oracle.binding import OracleTracer
+
+    f = ka.moonlit_ground_frame(size=8)
+    imgs = []
+    for cls in (PathTracer, OracleTracer):
+        t = cls((8, 8), ka.test_options(samples_per_frame=64, max_bounces=3))
+        if cls is PathTracer:
+            t.set_integrator(integrator)
+        t.set_guided_ground(guided)
+        imgs.append(ka.sample(t, f, 2))
+    img, ref = imgs
+    assert np.isfinite(img).all() and ref[:, :3].mean() > 0.0
+    err = np.sqrt(((img[:, :3] - ref[:, :3]) ** 2).sum() / (ref[:, :3] ** 2).sum())
+    assert err < 2e-3, err
+    close = np.abs(img[:, :3] - ref[:, :3]) <= 1e-4 * np.maximum(np.abs(ref[:, :3]), 1e-3 * ref[:, :3].max())
+    assert close.all(axis=1).mean() >= 0.99

@@ -134,3 +134,8 @@ def test_air_frames_are_not_differentiated():
     tracer = make((2, 2), ka.test_options())
     with pytest.raises(Exception):
         tracer.tangent(f, 0, 1)
+
+
+def test_guided_ground_is_unbiased():
+    r = ka.guided_ground_is_unbiased(make)
+    assert r["guided"][1] < r["plain"][1]
