@@ -550,7 +550,7 @@ static float point_gain(const scene *S, float extent, float distance) {
 }
 
 /* ---------------------------------------------------------------- */
-/* Surface albedo, style 0 (pathtrace.wgsl:338-389, :897-925)        */
+/* Surface albedo (pathtrace.wgsl:338-389, :897-925)                 */
 /* ---------------------------------------------------------------- */
 static float hash31(v3 p) {
     v3 q = V(fractf(p.x * 0.1031f), fractf(p.y * 0.1030f), fractf(p.z * 0.0973f));
@@ -568,11 +568,439 @@ static float vnoise(v3 p) {
     float d = mixf(hash31(vadd(i, V(0, 1, 1))), hash31(vadd(i, V(1, 1, 1))), u.x);
     return mixf(mixf(a, b, u.y), mixf(c, d, u.y), u.z);
 }
+/* ---------------------------------------------------------------- */
+/* Procedural surface styles 1-6 (pathtrace.wgsl:357-895)            */
+/* ---------------------------------------------------------------- */
+static inline v3 vsplat(float s) { return V(s, s, s); }
+static inline v3 vadds(v3 a, float s) { return V(a.x + s, a.y + s, a.z + s); }
+static inline v3 vsubs(v3 a, float s) { return V(a.x - s, a.y - s, a.z - s); }
+static inline v3 vmix(v3 a, v3 b, float t) { return V(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
+static inline v3 vfloor(v3 a) { return V(floorf(a.x), floorf(a.y), floorf(a.z)); }
+static inline float stepf(float edge, float x) { return x >= edge ? 1.0f : 0.0f; }
+
+/* fbm: pathtrace.wgsl:357-373 (the octave rotation is a column matrix). */
+static float fbm(v3 p, uint32_t octaves) {
+    float amplitude = 0.5f, sum = 0.0f, norm = 0.0f;
+    for (uint32_t octave = 0; octave < octaves; octave++) {
+        sum += amplitude * vnoise(p);
+        norm += amplitude;
+        v3 r = V((0.0f * p.x + -1.6f * p.y) + -1.2f * p.z, (1.6f * p.x + 0.72f * p.y) + -0.96f * p.z,
+                 (1.2f * p.x + -0.96f * p.y) + 1.28f * p.z);
+        p = vadd(r, V(17.3f, 5.1f, 11.7f));
+        amplitude *= 0.5f;
+    }
+    return sum / norm;
+}
+/* seed_offset: pathtrace.wgsl:384-389 */
+static v3 seed_offset(float seed) {
+    return vmul(V(hash31(V(seed, 1.0f, 7.0f)), hash31(V(3.0f, seed, 5.0f)), hash31(V(9.0f, 2.0f, seed))), 512.0f);
+}
+static inline v3 body_field(const sg_sphere *b, const float *f) { (void)b; return V(f[0], f[1], f[2]); }
+
+/* gas_giant_albedo: pathtrace.wgsl:394-472 */
+static v3 gas_giant_albedo(const sg_sphere *body, v3 local) {
+    v3 off = seed_offset(body->axis_y[3]);
+    v3 zone = body_field(body, body->color), belt = body_field(body, body->surface_color);
+    float turbulence = body->surface_color[3];
+    float bands = body->surface_params[0];
+    uint32_t storms = (uint32_t)(body->surface_params[1] + 0.5f);
+    v3 q = local;
+    float masks[3] = {0, 0, 0}, rims[3] = {0, 0, 0};
+    for (uint32_t k = 0; k < storms && k < 3u; k++) {
+        float fk = (float)k;
+        float lat = (hash31(vadd(off, V(7.1f * fk, 1.3f, 2.9f))) - 0.5f) * 1.1f;
+        float lon = hash31(vadd(off, V(3.7f, 5.3f * fk, 8.1f))) * TAU_F;
+        float size = (k == 0u ? 0.11f : 0.05f) * (0.8f + 0.4f * hash31(vadd(off, V(fk, 9.0f, 4.0f))));
+        v3 centre = V(cosf(lat) * cosf(lon), cosf(lat) * sinf(lon), sinf(lat));
+        if (vdot(q, centre) <= 0.0f) continue;
+        v3 east = V(-sinf(lon), cosf(lon), 0.0f);
+        v3 north = vcross(centre, east);
+        float dx = vdot(vsub(q, centre), east) / (2.0f * size);
+        float dy = vdot(vsub(q, centre), north) / size;
+        float e = sqrtf(dx * dx + dy * dy);
+        float influence = 1.0f - smoothstepf(0.0f, 2.4f, e);
+        float angle = (lat < 0.0f ? 3.2f : -3.2f) * influence * influence;
+        float c = cosf(angle), s = sinf(angle);
+        float rx = c * dx - s * dy;
+        float ry = s * dx + c * dy;
+        q = vnormalize(vadd(vadd(q, vmul(east, (rx - dx) * 2.0f * size)), vmul(north, (ry - dy) * size)));
+        float ragged = e + 0.25f * (fbm(vadd(vmul(q, 18.0f), off), 3) - 0.5f);
+        masks[k] = 1.0f - smoothstepf(0.7f, 1.0f, ragged);
+        rims[k] = smoothstepf(0.75f, 1.0f, ragged) * (1.0f - smoothstepf(1.0f, 1.35f, ragged));
+    }
+    v3 p = vadd(V(q.x * 2.2f, q.y * 2.2f, q.z * 9.0f), off);
+    float warp1 = fbm(p, 5) - 0.5f;
+    float warp2 = fbm(vadds(vadd(vmul(p, 2.1f), V(5.2f, 1.3f, 7.7f)), 4.0f * warp1), 5) - 0.5f;
+    float lat = q.z + 0.07f * sinf(3.0f * PI_F * q.z + off.z) + 0.04f * sinf(5.0f * PI_F * q.z + off.y);
+    float shear = 0.35f + 0.65f * fabsf(cosf(PI_F * bands * lat + off.x));
+    float lon = atan2f(q.y, q.x);
+    float ripple = sinf(lon * (9.0f + floorf(bands)) + 6.0f * warp1 + off.y) * 0.5f +
+                   sinf(lon * 23.0f + 9.0f * warp2 + off.z) * 0.25f;
+    float mu = lat + turbulence * shear * (0.16f * warp1 + 0.10f * warp2 + 0.025f * ripple);
+    float wave = 0.5f + 0.5f * sinf(PI_F * bands * mu + off.x);
+    float irregular = fbm(V(mu * bands * 1.7f, off.y, off.z), 3);
+    float profile = 0.5f * wave + 0.5f * irregular;
+    float tone = fbm(V(mu * bands * 0.9f, off.z, off.x), 2);
+    float fine = fbm(vadds(vadd(V(q.x * 7.0f, q.y * 7.0f, q.z * 70.0f), off), 3.0f * warp2), 4);
+    float eddies = fbm(vadd(vmul(p, 5.0f), vmul(V(warp1, warp2, warp1), 6.0f)), 4);
+    v3 color = vmix(belt, zone, smoothstepf(0.3f, 0.75f, profile));
+    color = vmix(color, vmulv(color, vadds(vmul(color, 0.5f), 0.55f)), smoothstepf(0.35f, 0.75f, tone) * 0.8f);
+    color = vmul(color, (0.78f + 0.44f * fine) * (0.9f + 0.2f * eddies));
+    float polar = smoothstepf(0.55f, 0.92f, fabsf(local.z));
+    color = vmix(color, vmul(vmix(zone, belt, 0.55f), 0.8f + 0.2f * fine), polar * 0.8f);
+    for (uint32_t k = 0; k < storms && k < 3u; k++) {
+        v3 tint = k == 0u ? vmul(vmulv(belt, belt), 1.5f) : vmul(zone, 1.15f);
+        float core = 1.0f - 0.25f * (1.0f - smoothstepf(0.0f, 0.6f, masks[k] - rims[k]));
+        color = vmix(color, vmul(vmul(tint, 0.7f + 0.6f * fine), core), masks[k] * 0.92f);
+        color = vmix(color, vmul(zone, 1.1f), rims[k] * 0.45f);
+    }
+    return color;
+}
+
+/* surface_gaussian, hash33, ridge, maria, cell_centre: pathtrace.wgsl:477-516 */
+static inline float surface_gaussian(float distance) { return expf(-(distance * distance)); }
+static v3 hash33(v3 p) {
+    return V(hash31(p), hash31(vadd(p, V(19.1f, 7.3f, 3.7f))), hash31(vadd(p, V(5.9f, 31.7f, 11.3f))));
+}
+static inline float ridge(float n, float width) { return 1.0f - smoothstepf(0.0f, width, fabsf(n - 0.5f)); }
+static float maria(v3 q, v3 off) {
+    float warp = fbm(vadd(vmul(q, 2.0f), off), 4) - 0.5f;
+    return smoothstepf(0.5f, 0.56f, fbm(vadds(vadd(vmul(q, 1.2f), off), 1.5f * warp), 5));
+}
+static int cell_centre(v3 cell, v3 key, float scale, v3 off, v3 *centre_out) {
+    for (uint32_t t = 0; t < 3u; t++) {
+        v3 centre = vnormalize(vsub(vadd(cell, hash33(vadds(key, (float)t * 17.0f))), off));
+        v3 f = vfloor(vadd(vmul(centre, scale), off));
+        if (f.x == cell.x && f.y == cell.y && f.z == cell.z) {
+            *centre_out = centre;
+            return 1;
+        }
+    }
+    return 0;
+}
+static inline v3 corner(v3 base, uint32_t i) {
+    return vadd(base, V((float)(i & 1u), (float)((i >> 1u) & 1u), (float)((i >> 2u) & 1u)));
+}
+
+/* crater_layer: pathtrace.wgsl:527-633. state = (floor darkness, relief). */
+static void crater_layer(v3 q, float scale, float density, v3 off, v3 body_off, float flood, float contrast,
+                         float rays, float state[2]) {
+    v3 p = vadd(vmul(q, scale), off);
+    v3 base = vfloor(vsubs(p, 0.5f));
+    uint32_t slots[6];
+    float ages[6];
+    v3 centres[6];
+    uint32_t count = 0;
+    for (uint32_t i = 0; i < 16u; i++) {
+        v3 grid = corner(base, i);
+        v3 a = vsub(grid, p), b = vsubs(vsub(p, grid), 1.0f);
+        v3 gap = V(maxf_(maxf_(a.x, b.x), 0.0f), maxf_(maxf_(a.y, b.y), 0.0f), maxf_(maxf_(a.z, b.z), 0.0f));
+        if (vdot(gap, gap) > 0.2343f) continue;
+        v3 key = vadds(grid, (float)(i >> 3u) * 1000.0f);
+        if (hash31(vadd(key, V(71.3f, 3.1f, 9.7f))) > density) continue;
+        v3 found;
+        if (!cell_centre(grid, key, scale, off, &found)) continue;
+        float size = hash31(vadd(key, V(3.1f, 8.3f, 1.7f)));
+        float radius = (0.06f + 0.16f * size * size) / scale;
+        if (vlength(vsub(q, found)) > 2.2f * radius) continue;
+        float age = hash31(vadd(key, V(29.0f, 61.0f, 7.0f)));
+        if (flood > 0.0f && age < 0.7f && maria(found, body_off) > 0.5f) continue;
+        if (count == 6u) {
+            if (age <= ages[0]) continue;
+            for (uint32_t m = 0; m < 5u; m++) {
+                ages[m] = ages[m + 1];
+                slots[m] = slots[m + 1];
+                centres[m] = centres[m + 1];
+            }
+            count = 5u;
+        }
+        uint32_t j = count;
+        while (j > 0u && ages[j - 1] > age) {
+            ages[j] = ages[j - 1];
+            slots[j] = slots[j - 1];
+            centres[j] = centres[j - 1];
+            j--;
+        }
+        ages[j] = age;
+        slots[j] = i;
+        centres[j] = found;
+        count++;
+    }
+    float floor_shade = 1.0f, relief = state[1];
+    for (uint32_t k = 0; k < count; k++) {
+        uint32_t i = slots[k];
+        v3 cell = vadds(corner(base, i), (float)(i >> 3u) * 1000.0f);
+        v3 centre = centres[k];
+        float size = hash31(vadd(cell, V(3.1f, 8.3f, 1.7f)));
+        float radius = (0.06f + 0.16f * size * size) / scale;
+        v3 offset = vsub(q, centre);
+        float d = vlength(offset) / radius;
+        v3 east = vcross(V(0.0f, 0.0f, 1.0f), centre);
+        east = vdivs(east, maxf_(vlength(east), 1.0e-4f));
+        v3 north = vcross(centre, east);
+        float angle = atan2f(vdot(offset, north), vdot(offset, east));
+        v3 phase = vmul(hash33(vadd(cell, V(41.0f, 5.0f, 23.0f))), TAU_F);
+        float wobble = 0.025f * (sinf(3.0f * angle + phase.x) + sinf(5.0f * angle + phase.y) +
+                                 0.6f * sinf(8.0f * angle + phase.z));
+        float r = d + wobble;
+        floor_shade = minf_(floor_shade, 1.0f - 0.18f * contrast * (1.0f - smoothstepf(0.55f, 0.9f, r)));
+        float rim = 0.22f * contrast * surface_gaussian((r - 1.0f) / 0.13f);
+        float footprint = 1.0f - smoothstepf(1.1f, 1.3f, r);
+        relief = mixf(relief, rim, footprint);
+        float blanket = (1.0f - smoothstepf(1.0f, 1.9f, r)) * (1.0f - footprint);
+        relief = mixf(relief, 0.0f, blanket * 0.3f) + 0.1f * contrast * blanket;
+        float fresh = hash31(vadd(cell, V(13.0f, 2.0f, 5.0f)));
+        if (rays > 0.0f && fresh > 0.82f) {
+            float streaks = powf(vnoise(V(cosf(angle) * 9.0f, sinf(angle) * 9.0f, fresh * 40.0f)), 3.0f);
+            relief += contrast * (rays * 0.9f * streaks * (1.0f - smoothstepf(1.0f, 2.2f, d)) * stepf(0.9f, d) +
+                                  rays * 0.25f * (1.0f - smoothstepf(0.0f, 1.0f, d)));
+        }
+    }
+    state[0] *= floor_shade;
+    state[1] = relief;
+}
+
+/* craters: pathtrace.wgsl:636-647 */
+static float craters(v3 q, float density, v3 off, float flood, float contrast, float rays) {
+    if (density <= 0.0f) return 1.0f;
+    float state[2] = {1.0f, 0.0f};
+    crater_layer(q, 1.5f, density, off, off, flood, contrast, rays, state);
+    crater_layer(q, 3.5f, density, vadds(off, 101.0f), off, flood, contrast, rays * 0.8f, state);
+    crater_layer(q, 8.0f, density, vadds(off, 203.0f), off, flood, contrast * 0.85f, rays * 0.5f, state);
+    crater_layer(q, 18.0f, density, vadds(off, 307.0f), off, 0.0f, contrast * 0.7f, 0.0f, state);
+    crater_layer(q, 40.0f, density, vadds(off, 401.0f), off, 0.0f, contrast * 0.55f, 0.0f, state);
+    return state[0] * (1.0f + state[1]);
+}
+
+/* polar_caps: pathtrace.wgsl:650-656 */
+static float polar_caps(v3 q, float extent, v3 off) {
+    if (extent <= 0.0f) return 0.0f;
+    float edge = 1.0f - extent + 0.12f * (fbm(vadd(vmul(q, 5.0f), off), 5) - 0.5f) +
+                 0.05f * (fbm(vadd(vmul(q, 18.0f), off), 3) - 0.5f);
+    return smoothstepf(edge - 0.015f, edge + 0.015f, fabsf(q.z));
+}
+
+/* cratered_albedo: pathtrace.wgsl:660-669 */
+static v3 cratered_albedo(const sg_sphere *body, v3 q) {
+    v3 off = seed_offset(body->axis_y[3]);
+    float mare = maria(q, off);
+    float grain = fbm(vadd(vmul(q, 45.0f), off), 3);
+    v3 color = vmix(body_field(body, body->color), body_field(body, body->surface_color), mare);
+    color = vmul(color, 0.9f + 0.2f * grain);
+    return vmul(color, craters(q, body->surface_color[3], off, 1.0f, 1.0f, 1.0f));
+}
+
+/* rocky_albedo: pathtrace.wgsl:673-687 */
+static v3 rocky_albedo(const sg_sphere *body, v3 q) {
+    v3 off = seed_offset(body->axis_y[3]);
+    v3 base = vadd(vmul(q, 1.8f), off);
+    v3 warp = vsubs(V(fbm(base, 4), fbm(vadds(base, 7.0f), 4), 0.0f), 0.5f);
+    float dark = smoothstepf(0.5f, 0.64f, fbm(vadd(vadd(vmul(q, 2.2f), off), V(2.0f * warp.x, 2.0f * warp.y, warp.x)), 6));
+    float tone = fbm(vadds(vadd(vmul(q, 5.0f), off), 3.0f), 4);
+    v3 color = vmix(body_field(body, body->color), body_field(body, body->surface_color), dark * 0.85f);
+    color = vmul(color, 0.85f + 0.3f * tone);
+    float streak = fbm(vadds(vadd(V(q.x * 4.0f, q.y * 4.0f, q.z * 18.0f), off), 9.0f), 3);
+    color = vmul(color, 0.95f + 0.1f * streak);
+    color = vmul(color, craters(q, body->surface_color[3], off, 0.0f, 0.45f, 0.0f));
+    float ice = polar_caps(q, body->surface_params[0], off);
+    return vmix(color, V(0.92f, 0.92f, 0.94f), ice);
+}
+
+/* ice_plates: pathtrace.wgsl:691-708 */
+static v3 ice_plates(v3 p) {
+    v3 base = vfloor(p);
+    float nearest = 10.0f, second = 10.0f, tone = 0.0f;
+    for (int i = 0; i < 27; i++) {
+        v3 cell = vadd(base, V((float)(i % 3 - 1), (float)((i / 3) % 3 - 1), (float)(i / 9 - 1)));
+        v3 delta = vsub(vadd(vadds(cell, 0.2f), vmul(hash33(cell), 0.6f)), p);
+        float d = vdot(delta, delta);
+        if (d < nearest) {
+            second = nearest;
+            nearest = d;
+            tone = hash31(vadds(cell, 57.0f));
+        } else {
+            second = minf_(second, d);
+        }
+    }
+    return V(sqrtf(nearest), sqrtf(second) - sqrtf(nearest), tone);
+}
+
+/* icy_albedo: pathtrace.wgsl:714-766 */
+static v3 icy_albedo(const sg_sphere *body, v3 q) {
+    v3 off = seed_offset(body->axis_y[3]);
+    v3 ice = body_field(body, body->color);
+    v3 rust = vmulv(body_field(body, body->surface_color), V(0.72f, 0.62f, 0.56f));
+    v3 b = vadd(vmul(q, 3.1f), off);
+    v3 warp = vsubs(V(fbm(vadds(b, 11.0f), 3), fbm(vadds(b, 23.0f), 3), fbm(vadds(b, 37.0f), 3)), 0.5f);
+    float terrain = fbm(vadd(vadd(vmul(q, 4.2f), off), warp), 5);
+    float rubble = fbm(vadd(vadd(vmul(q, 85.0f), off), vmul(warp, 7.0f)), 4);
+    float chaos = smoothstepf(0.42f, 0.65f, terrain + 0.14f * (rubble - 0.5f));
+    v3 plates = ice_plates(vadd(vadd(vmul(q, 72.0f), off), vmul(warp, 4.0f)));
+    float seams = 1.0f - smoothstepf(0.015f, 0.07f, plates.y);
+    float dust = chaos * (0.2f + 0.46f * rubble + 0.18f * plates.z);
+    v3 color = vmix(ice, rust, dust);
+    color = vmix(color, vmul(rust, 0.8f), seams * chaos * 0.35f);
+    float ridged_plain = ridge(fbm(vadds(vadd(vmul(q, 34.0f), off), 83.0f), 3), 0.025f);
+    color = vmix(color, rust, ridged_plain * (0.1f + 0.14f * chaos));
+    color = vmul(color, 0.87f + 0.22f * fbm(vadd(vmul(q, 180.0f), off), 3));
+    v3 warped = vadd(q, vmul(warp, 0.1f));
+    float roughness = 0.0015f * (rubble - 0.5f);
+    float shoulder = 0.0f, fissure = 0.0f, fresh_ridge = 0.0f;
+    for (uint32_t i = 0; i < 64u; i++) {
+        v3 h = hash33(vadd(off, V((float)i * 3.7f, 1.0f, 2.0f)));
+        v3 family = hash33(vadd(off, V((float)(i / 8u) * 17.3f, 21.0f, 7.0f)));
+        v3 n = vnormalize(vadd(vsubs(vmul(family, 2.0f), 1.0f), vmul(vsubs(vmul(h, 2.0f), 1.0f), 0.28f)));
+        float shift = (hash31(vadd(off, V((float)i, 9.0f, 4.0f))) - 0.5f) * 1.4f;
+        float width = (i < 10u ? 0.0015f + 0.0022f * h.z : 0.0005f + 0.0011f * h.z) *
+                      (0.65f + 0.8f * vnoise(vadd(vmul(q, 17.0f), vmul(h, 29.0f))));
+        float bend = 0.03f * (vnoise(vadd(vmul(q, 6.0f), vmul(family, 31.0f))) - 0.5f) +
+                     0.008f * (vnoise(vadd(vmul(q, 24.0f), vmul(family, 37.0f))) - 0.5f);
+        float dist = fabsf(vdot(warped, n) - shift + roughness + bend);
+        float along = smoothstepf(0.28f, 0.62f, vnoise(vadd(vmul(q, 3.5f), vmul(h, 50.0f))));
+        shoulder = maxf_(shoulder, (1.0f - smoothstepf(width, width * 4.0f, dist)) * along);
+        float double_ridge = fabsf(dist - width * 0.85f);
+        float single = 1.0f - smoothstepf(width * 0.25f, width, dist);
+        float paired = 1.0f - smoothstepf(width * 0.15f, width * 0.55f, double_ridge);
+        fissure = maxf_(fissure, (i < 10u ? paired : single) * along);
+        fresh_ridge = maxf_(fresh_ridge,
+                            (1.0f - smoothstepf(width * 0.15f, width * 0.35f, fabsf(dist - width * 1.8f))) * along);
+    }
+    color = vmix(color, rust, shoulder * 0.17f);
+    color = vmix(color, vmul(rust, 0.7f), fissure * 0.8f);
+    color = vmix(color, ice, fresh_ridge * 0.13f);
+    return vmul(color, craters(q, body->surface_color[3] * 0.2f, off, 0.0f, 0.3f, 0.4f));
+}
+
+/* volcanic_albedo: pathtrace.wgsl:770-850 */
+static v3 volcanic_albedo(const sg_sphere *body, v3 q) {
+    v3 off = seed_offset(body->axis_y[3]);
+    v3 sulphur = body_field(body, body->color), deposit = body_field(body, body->surface_color);
+    v3 b = vadd(vmul(q, 4.7f), off);
+    v3 warp = vsubs(V(fbm(b, 3), fbm(vadds(b, 19.0f), 3), fbm(vadds(b, 41.0f), 3)), 0.5f);
+    float terrain = fbm(vadd(vadd(vmul(q, 10.0f), off), vmul(warp, 2.0f)), 6);
+    float weathered = smoothstepf(0.38f, 0.65f, fbm(vadds(vadd(vmul(q, 3.7f), off), 11.0f), 5));
+    float fine = fbm(vadd(vadd(vmul(q, 90.0f), off), vmul(warp, 3.0f)), 4);
+    v3 crust = vmix(vmulv(sulphur, V(0.43f, 0.51f, 0.6f)), deposit, 0.12f);
+    v3 color = vmul(sulphur, 0.7f + 0.5f * terrain);
+    color = vmix(color, crust, weathered * (0.45f + 0.5f * terrain));
+    float frost = smoothstepf(0.38f, 0.74f, fbm(vadd(vadds(vadd(vmul(q, 6.0f), off), 29.0f), warp), 5) + 0.2f * (fine - 0.5f));
+    v3 frost_color = vmix(sulphur, V(0.72f, 0.7f, 0.62f), 0.8f);
+    color = vmix(color, frost_color, frost * 0.7f);
+    float flow_edges = ridge(fbm(vadd(vadd(vmul(q, 35.0f), off), vmul(warp, 2.0f)), 4), 0.025f);
+    color = vmix(color, crust, flow_edges * weathered * 0.4f);
+    color = vmul(color, (0.82f + 0.32f * fine) * (0.94f + 0.13f * fbm(vadd(vmul(q, 210.0f), off), 3)));
+    float dark = 0.0f, ash = 0.0f, red = 0.0f, white = 0.0f;
+    float density = body->surface_color[3];
+    float scale = 5.5f;
+    v3 p = vadds(vadd(vmul(q, scale), off), 300.0f);
+    v3 base = vfloor(p);
+    for (int i = 0; i < 27; i++) {
+        v3 cell = vadd(base, V((float)(i % 3 - 1), (float)((i / 3) % 3 - 1), (float)(i / 9 - 1)));
+        if (hash31(vadd(cell, V(4.0f, 41.0f, 9.0f))) > 0.6f * density) continue;
+        v3 centre;
+        if (!cell_centre(cell, cell, scale, vadds(off, 300.0f), &centre)) continue;
+        float size = hash31(vadd(cell, V(8.0f, 1.0f, 3.0f)));
+        float radius = (0.025f + 0.11f * size * size * size) / scale;
+        v3 offset = vsub(q, centre);
+        float reach = vlength(offset) * scale;
+        if (reach > 0.95f) continue;
+        float cutoff = 1.0f - smoothstepf(0.75f, 0.95f, reach);
+        v3 tangent = vcross(centre, V(0.37f, 0.83f, 0.41f));
+        v3 east = vdivs(tangent, maxf_(vlength(tangent), 1.0e-5f));
+        v3 north = vcross(centre, east);
+        float angle = TAU_F * hash31(vadds(cell, 91.0f));
+        float ux = vdot(offset, east) / radius, uy = vdot(offset, north) / radius;
+        float ca = cosf(angle), sa = sinf(angle);
+        float uvx = ux * ca - uy * sa, uvy = ux * sa + uy * ca;
+        float ragged = fbm(vadd(V(uvx * 2.7f, uvy * 2.7f, 0.0f), vmul(cell, 7.0f)), 3) - 0.5f;
+        float sx = uvx * (1.0f / (0.65f + 0.9f * size)), sy = uvy * 1.0f;
+        float d = sqrtf(sx * sx + sy * sy) + 0.42f * ragged;
+        float pit = 1.0f - smoothstepf(0.68f, 0.86f, d);
+        float age = hash31(vadds(cell, 31.0f));
+        float fx = uvx - (0.2f + 2.3f * age), fy = uvy - 0.35f * sinf(uvx * 1.3f + angle);
+        float gx = fx * (0.75f - 0.48f * age), gy = fy * (0.85f + 0.35f * size);
+        float flow_shape = sqrtf(gx * gx + gy * gy) + 0.65f * ragged +
+                           0.35f * (fbm(vadd(V(uvx * 1.8f, uvy * 1.8f, 0.0f), vmul(cell, 3.0f)), 4) - 0.5f);
+        float flow = (1.0f - smoothstepf(0.72f, 0.9f, flow_shape)) * smoothstepf(0.35f, 0.85f, age) * 0.85f;
+        dark = maxf_(dark, maxf_(pit, flow) * cutoff);
+        float plume = hash31(vadd(cell, V(2.0f, 6.0f, 17.0f)));
+        float hx = (uvx - 0.5f) * 0.16f, hy = (uvy - 0.3f) * 0.23f;
+        float halo = expf(-(hx * hx + hy * hy)) * cutoff;
+        ash = maxf_(ash, halo * (0.25f + 0.35f * age));
+        white = maxf_(white, halo * stepf(0.45f, plume) * (1.0f - stepf(0.83f, plume)));
+        float apron = surface_gaussian((sqrtf(uvx * uvx + uvy * uvy) + ragged - 3.5f) / 1.6f) *
+                      (0.25f + 0.75f * smoothstepf(-1.5f, 2.0f, uvy));
+        red = maxf_(red, apron * stepf(0.83f, plume) * cutoff);
+    }
+    color = vmix(color, vmul(crust, 0.7f), ash * 0.45f);
+    color = vmix(color, frost_color, white * 0.4f);
+    color = vmix(color, vmulv(deposit, V(0.85f, 0.7f, 0.65f)), red * 0.6f);
+    return vmix(color, V(0.035f, 0.032f, 0.026f), dark * 0.96f);
+}
+
+/* terran_albedo: pathtrace.wgsl:854-895 */
+static v3 terran_albedo(const sg_sphere *body, v3 q) {
+    v3 off = seed_offset(body->axis_y[3]);
+    v3 land_base = body_field(body, body->color), ocean = body_field(body, body->surface_color);
+    v3 b = vadd(vmul(q, 1.5f), off);
+    v3 warp = vsubs(V(fbm(b, 4), fbm(vadds(b, 13.0f), 4), fbm(vadds(b, 29.0f), 4)), 0.5f);
+    float height = fbm(vadd(vadd(vmul(q, 1.1f), off), vmul(warp, 0.9f)), 7);
+    float sea = 0.5f + (body->surface_params[1] - 0.5f) * 0.3f;
+    float coast = smoothstepf(sea, sea + 0.004f, height);
+    float shallow = 1.0f - smoothstepf(sea - 0.04f, sea, height);
+    v3 water = vmix(vadd(vmul(ocean, 1.8f), V(0.0f, 0.04f, 0.05f)), ocean, shallow);
+    float moisture = fbm(vadds(vadd(vmul(q, 3.0f), off), 41.0f), 5) + 0.25f * (fabsf(q.z) - 0.35f);
+    v3 green = vmulv(land_base, V(0.45f, 0.62f, 0.38f));
+    v3 land = vmix(land_base, green, smoothstepf(0.45f, 0.6f, moisture));
+    float altitude = smoothstepf(sea + 0.08f, sea + 0.2f, height);
+    land = vmix(land, V(0.42f, 0.38f, 0.34f), altitude * 0.6f);
+    land = vmix(land, V(0.9f, 0.9f, 0.92f), smoothstepf(sea + 0.19f, sea + 0.24f, height));
+    land = vmul(land, 0.88f + 0.24f * fbm(vadd(vmul(q, 25.0f), off), 3));
+    v3 color = vmix(water, land, coast);
+    float ice = polar_caps(q, body->surface_params[0], off);
+    color = vmix(color, V(0.9f, 0.92f, 0.95f), ice);
+    float cover = body->surface_params[2];
+    if (cover > 0.0f) {
+        v3 c1 = vadd(vmul(q, 1.6f), off);
+        v3 w1 = vsubs(V(fbm(vadds(c1, 77.0f), 4), fbm(vadds(c1, 91.0f), 4), 0.5f), 0.5f);
+        v3 c2 = vadd(vadd(vmul(q, 4.0f), off), vmul(w1, 3.0f));
+        v3 w2 = vsubs(V(fbm(c2, 4), fbm(vadd(vadds(vadd(vmul(q, 4.0f), off), 17.0f), vmul(w1, 3.0f)), 4), 0.5f), 0.5f);
+        v3 cq = vadd(vadd(vadd(V(q.x * 2.5f, q.y * 2.5f, q.z * 7.0f), off), vmul(w1, 2.5f)), vmul(w2, 1.2f));
+        float cloud = fbm(cq, 7);
+        float lat = fabsf(q.z);
+        float belts = 0.06f * (surface_gaussian(lat / 0.12f) + surface_gaussian((lat - 0.72f) / 0.15f)) -
+                      0.04f * surface_gaussian((lat - 0.42f) / 0.1f);
+        float threshold = 0.62f - 0.22f * cover - belts;
+        float mask = smoothstepf(threshold - 0.04f, threshold + 0.14f, cloud);
+        color = vmix(color, V(0.93f, 0.94f, 0.96f), mask * 0.95f);
+    }
+    return color;
+}
+
+/* surface_albedo, styles 1-6 (pathtrace.wgsl:897-910): clamped to [0, 1]. */
+static v3 style_albedo(const sg_sphere *body, uint32_t style, v3 local) {
+    v3 c;
+    switch (style) {
+        case 1u: c = gas_giant_albedo(body, local); break;
+        case 2u: c = cratered_albedo(body, local); break;
+        case 3u: c = rocky_albedo(body, local); break;
+        case 4u: c = icy_albedo(body, local); break;
+        case 5u: c = volcanic_albedo(body, local); break;
+        default: c = terran_albedo(body, local); break;
+    }
+    return V(clampf_(c.x, 0.0f, 1.0f), clampf_(c.y, 0.0f, 1.0f), clampf_(c.z, 0.0f, 1.0f));
+}
+
 static v3 surface_albedo_m(const scene *S, uint32_t index, v3 normal, float *mottle_out) {
     const sg_sphere *body = &S->b[index];
     v3 x = V(body->axis_x[0], body->axis_x[1], body->axis_x[2]);
     v3 y = V(body->axis_y[0], body->axis_y[1], body->axis_y[2]);
     v3 local = V(vdot(normal, x), vdot(normal, y), vdot(normal, vcross(x, y)));
+    uint32_t style = (uint32_t)(body->axis_x[3] + 0.5f);
+    if (style > 0u) {
+        if (mottle_out) *mottle_out = 1.0f;
+        return style_albedo(body, style, local);
+    }
     float mottle = 1.0f;
     if (body->center_low[3] > 0.0f) {
         float seed = body->axis_y[3];

@@ -697,3 +697,107 @@ def guided_ground_is_unbiased(make, batches: int = 24) -> dict:
     assert abs(mg - mp) < 4.0 * np.hypot(sp, sg), out
     assert sg < sp, out
     return dict(plain=out[False], guided=out[True])
+
+
+# ---------------------------------------------------------------------------
+# src/planetshine_tests.rs:53-104 — gpu_textured_planets_light_night_air
+# ---------------------------------------------------------------------------
+STYLES = ["gas_giant", "cratered", "rocky", "icy", "volcanic", "terran"]
+
+
+def default_surface(style: str, albedo) -> dict:
+    """`config::default_surface` (src/config.rs:191-290): a style's
+    defaults for a body of `albedo` (secondary colour, bands, turbulence,
+    storms, craters, ice caps, ocean, clouds)."""
+    a = np.asarray(albedo, np.float32)
+    peak = np.float32(max(1.0e-6, float(a.max())))
+
+    def deeper(scale, power):
+        return [float(np.float32(scale) * c * np.float32(np.power(np.float32(c / peak), np.float32(power)))) for c in a]
+
+    secondary = {
+        "gas_giant": lambda: deeper(0.8, 1.6), "cratered": lambda: deeper(0.55, 0.6),
+        "rocky": lambda: deeper(0.6, 1.0), "icy": lambda: [a[0] * 0.75, a[1] * 0.5, a[2] * 0.35],
+        "volcanic": lambda: [a[0] * 0.85, a[1] * 0.45, a[2] * 0.2], "terran": lambda: [0.03, 0.09, 0.2],
+    }[style]()
+    craters, ice_caps = {"gas_giant": (0.0, 0.0), "cratered": (0.8, 0.0), "rocky": (0.5, 0.06), "icy": (0.15, 0.0),
+                         "volcanic": (0.5, 0.0), "terran": (0.0, 0.1)}[style]
+    return dict(code=float(STYLES.index(style) + 1), secondary=[float(c) for c in secondary], bands=7.0,
+                turbulence=0.5, storms=1, craters=craters, ice_caps=ice_caps, ocean=0.65, clouds=0.4)
+
+
+def texture(sphere, style: str) -> None:
+    """`texture` (src/planetshine_tests.rs:30-51): a style's defaults on a
+    body, pattern seed 17, body axes along x and y."""
+    s = default_surface(style, list(sphere.color))
+    gas = style == "gas_giant"
+    sphere.axis_x[:] = [1.0, 0.0, 0.0, s["code"]]
+    sphere.axis_y[:] = [0.0, 1.0, 0.0, 17.0]
+    sphere.surface_color[:] = [*s["secondary"], s["turbulence"] if gas else s["craters"]]
+    sphere.surface_params[:] = ([s["bands"], float(s["storms"]), 0.0, 0.0] if gas
+                                else [s["ice_caps"], s["ocean"], s["clouds"], 0.0])
+
+
+def moonlit_scene():
+    """`moonlit_scene` (src/planetshine_tests.rs:4-28)."""
+    f = frame()
+    radius = np.float32(6371.0 / AU_KM)
+    center = [0.0, 0.0, float(np.float32(radius + np.float32(0.002 / AU_KM)))]
+    set_air(f, earthlike(), center, float(radius))
+    f.bodies = [body(center, float(radius), [0.0] * 3, False),
+                body([0.0004, 0.0, -0.002], 0.00015, [0.8, 0.6, 0.4], False),
+                body([0.3, 0.0, 1.0], 0.005, [100_000.0] * 3, True)]
+    return f
+
+
+def textured_planets_light_night_air(make, styles=STYLES) -> dict:
+    """Every textured style lights the night air with the right phase and no
+    glow from its unlit face. The glow is lit minus an untextured black moon;
+    both renders use the same sequence (common random numbers), as in
+    `reflected_atmosphere`."""
+    opts = test_options(samples_per_frame=32, max_bounces=1)
+    out = {}
+    for style in styles:
+        scene = moonlit_scene()
+        texture(scene.bodies[1], style)
+
+        def glow(scene):
+            lit = sample(make((1, 1), opts), scene, 32)[0]
+            black = moonlit_scene()
+            black.bodies[1] = type(scene.bodies[1]).from_buffer_copy(scene.bodies[1])
+            black.bodies[1].color[:] = [0.0] * 3
+            black.bodies[1].axis_x[3] = 0.0
+            black.bodies[2] = type(scene.bodies[2]).from_buffer_copy(scene.bodies[2])
+            background = sample(make((1, 1), opts), black, 32)[0]
+            return np.array([lit[c] - background[c] for c in range(3)], np.float64)
+
+        full = glow(scene)
+        scene.bodies[2].center[:] = [1.0, 0.0, 0.0]
+        quarter = glow(scene)
+        scene.bodies[2].center[:] = [-0.3, 0.0, -1.0]
+        new = glow(scene)
+        assert np.all(np.isfinite(full)) and np.all(full > 1e-4), (style, full)
+        assert full[0] * 0.03 < quarter[0] < full[0] * 0.8, (style, quarter, full)
+        assert np.all(np.abs(new) < full * 0.03), (style, new, full)
+        out[style] = dict(full=full, quarter=quarter, new=new)
+    return out
+
+
+def styles_scene(width: int = 96, height: int = 32):
+    """Six textured planets in a row (one per style, their defaults, pattern
+    seed 17), a star above and behind the camera, tan(half field) 0.17."""
+    f = frame()
+    f.globals.viewport[:] = [float(width), float(height), 1.0, width / height]
+    f.globals.cam_forward[3] = 0.17
+    colours = [[0.85, 0.7, 0.5], [0.5, 0.5, 0.48], [0.75, 0.45, 0.3], [0.9, 0.88, 0.85], [0.9, 0.8, 0.35],
+               [0.55, 0.5, 0.35]]
+    f.bodies = []
+    for k, style in enumerate(STYLES):
+        b = body([(k - 2.5) * 2.1, 0.0, -12.0], 0.95, colours[k], False)
+        texture(b, style)
+        # Tilt each body's axes so its pole leans toward the camera.
+        b.axis_x[:3] = [1.0, 0.0, 0.0]
+        b.axis_y[:3] = [0.0, 0.6, 0.8]
+        f.bodies.append(b)
+    f.bodies.append(body([4.0, 30.0, 20.0], 1.5, [400.0] * 3, True))
+    return f

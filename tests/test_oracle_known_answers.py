@@ -139,3 +139,8 @@ def test_air_frames_are_not_differentiated():
 def test_guided_ground_is_unbiased():
     r = ka.guided_ground_is_unbiased(make)
     assert r["guided"][1] < r["plain"][1]
+
+
+def test_textured_planets_light_night_air():
+    r = ka.textured_planets_light_night_air(make)
+    assert set(r) == set(ka.STYLES)
