@@ -571,6 +571,15 @@ static float vnoise(v3 p) {
 /* ---------------------------------------------------------------- */
 /* Procedural surface styles 1-6 (pathtrace.wgsl:357-895)            */
 /* ---------------------------------------------------------------- */
+/* Transcendentals are evaluated in double and rounded to f32 (the   */
+/* CUDA path does the same): the hash lattice amplifies any last-bit  */
+/* difference of a noise coordinate, so both sides must agree bit for */
+/* bit, and a correctly rounded value is the one both can produce.    */
+static inline float sin_d(float x) { return (float)sin((double)x); }
+static inline float cos_d(float x) { return (float)cos((double)x); }
+static inline float atan2_d(float y, float x) { return (float)atan2((double)y, (double)x); }
+static inline float exp_d(float x) { return (float)exp((double)x); }
+static inline float pow_d(float x, float y) { return (float)pow((double)x, (double)y); }
 static inline v3 vsplat(float s) { return V(s, s, s); }
 static inline v3 vadds(v3 a, float s) { return V(a.x + s, a.y + s, a.z + s); }
 static inline v3 vsubs(v3 a, float s) { return V(a.x - s, a.y - s, a.z - s); }
@@ -611,16 +620,16 @@ static v3 gas_giant_albedo(const sg_sphere *body, v3 local) {
         float lat = (hash31(vadd(off, V(7.1f * fk, 1.3f, 2.9f))) - 0.5f) * 1.1f;
         float lon = hash31(vadd(off, V(3.7f, 5.3f * fk, 8.1f))) * TAU_F;
         float size = (k == 0u ? 0.11f : 0.05f) * (0.8f + 0.4f * hash31(vadd(off, V(fk, 9.0f, 4.0f))));
-        v3 centre = V(cosf(lat) * cosf(lon), cosf(lat) * sinf(lon), sinf(lat));
+        v3 centre = V(cos_d(lat) * cos_d(lon), cos_d(lat) * sin_d(lon), sin_d(lat));
         if (vdot(q, centre) <= 0.0f) continue;
-        v3 east = V(-sinf(lon), cosf(lon), 0.0f);
+        v3 east = V(-sin_d(lon), cos_d(lon), 0.0f);
         v3 north = vcross(centre, east);
         float dx = vdot(vsub(q, centre), east) / (2.0f * size);
         float dy = vdot(vsub(q, centre), north) / size;
         float e = sqrtf(dx * dx + dy * dy);
         float influence = 1.0f - smoothstepf(0.0f, 2.4f, e);
         float angle = (lat < 0.0f ? 3.2f : -3.2f) * influence * influence;
-        float c = cosf(angle), s = sinf(angle);
+        float c = cos_d(angle), s = sin_d(angle);
         float rx = c * dx - s * dy;
         float ry = s * dx + c * dy;
         q = vnormalize(vadd(vadd(q, vmul(east, (rx - dx) * 2.0f * size)), vmul(north, (ry - dy) * size)));
@@ -631,13 +640,13 @@ static v3 gas_giant_albedo(const sg_sphere *body, v3 local) {
     v3 p = vadd(V(q.x * 2.2f, q.y * 2.2f, q.z * 9.0f), off);
     float warp1 = fbm(p, 5) - 0.5f;
     float warp2 = fbm(vadds(vadd(vmul(p, 2.1f), V(5.2f, 1.3f, 7.7f)), 4.0f * warp1), 5) - 0.5f;
-    float lat = q.z + 0.07f * sinf(3.0f * PI_F * q.z + off.z) + 0.04f * sinf(5.0f * PI_F * q.z + off.y);
-    float shear = 0.35f + 0.65f * fabsf(cosf(PI_F * bands * lat + off.x));
-    float lon = atan2f(q.y, q.x);
-    float ripple = sinf(lon * (9.0f + floorf(bands)) + 6.0f * warp1 + off.y) * 0.5f +
-                   sinf(lon * 23.0f + 9.0f * warp2 + off.z) * 0.25f;
+    float lat = q.z + 0.07f * sin_d(3.0f * PI_F * q.z + off.z) + 0.04f * sin_d(5.0f * PI_F * q.z + off.y);
+    float shear = 0.35f + 0.65f * fabsf(cos_d(PI_F * bands * lat + off.x));
+    float lon = atan2_d(q.y, q.x);
+    float ripple = sin_d(lon * (9.0f + floorf(bands)) + 6.0f * warp1 + off.y) * 0.5f +
+                   sin_d(lon * 23.0f + 9.0f * warp2 + off.z) * 0.25f;
     float mu = lat + turbulence * shear * (0.16f * warp1 + 0.10f * warp2 + 0.025f * ripple);
-    float wave = 0.5f + 0.5f * sinf(PI_F * bands * mu + off.x);
+    float wave = 0.5f + 0.5f * sin_d(PI_F * bands * mu + off.x);
     float irregular = fbm(V(mu * bands * 1.7f, off.y, off.z), 3);
     float profile = 0.5f * wave + 0.5f * irregular;
     float tone = fbm(V(mu * bands * 0.9f, off.z, off.x), 2);
@@ -658,7 +667,7 @@ static v3 gas_giant_albedo(const sg_sphere *body, v3 local) {
 }
 
 /* surface_gaussian, hash33, ridge, maria, cell_centre: pathtrace.wgsl:477-516 */
-static inline float surface_gaussian(float distance) { return expf(-(distance * distance)); }
+static inline float surface_gaussian(float distance) { return exp_d(-(distance * distance)); }
 static v3 hash33(v3 p) {
     return V(hash31(p), hash31(vadd(p, V(19.1f, 7.3f, 3.7f))), hash31(vadd(p, V(5.9f, 31.7f, 11.3f))));
 }
@@ -738,10 +747,10 @@ static void crater_layer(v3 q, float scale, float density, v3 off, v3 body_off, 
         v3 east = vcross(V(0.0f, 0.0f, 1.0f), centre);
         east = vdivs(east, maxf_(vlength(east), 1.0e-4f));
         v3 north = vcross(centre, east);
-        float angle = atan2f(vdot(offset, north), vdot(offset, east));
+        float angle = atan2_d(vdot(offset, north), vdot(offset, east));
         v3 phase = vmul(hash33(vadd(cell, V(41.0f, 5.0f, 23.0f))), TAU_F);
-        float wobble = 0.025f * (sinf(3.0f * angle + phase.x) + sinf(5.0f * angle + phase.y) +
-                                 0.6f * sinf(8.0f * angle + phase.z));
+        float wobble = 0.025f * (sin_d(3.0f * angle + phase.x) + sin_d(5.0f * angle + phase.y) +
+                                 0.6f * sin_d(8.0f * angle + phase.z));
         float r = d + wobble;
         floor_shade = minf_(floor_shade, 1.0f - 0.18f * contrast * (1.0f - smoothstepf(0.55f, 0.9f, r)));
         float rim = 0.22f * contrast * surface_gaussian((r - 1.0f) / 0.13f);
@@ -751,7 +760,7 @@ static void crater_layer(v3 q, float scale, float density, v3 off, v3 body_off, 
         relief = mixf(relief, 0.0f, blanket * 0.3f) + 0.1f * contrast * blanket;
         float fresh = hash31(vadd(cell, V(13.0f, 2.0f, 5.0f)));
         if (rays > 0.0f && fresh > 0.82f) {
-            float streaks = powf(vnoise(V(cosf(angle) * 9.0f, sinf(angle) * 9.0f, fresh * 40.0f)), 3.0f);
+            float streaks = pow_d(vnoise(V(cos_d(angle) * 9.0f, sin_d(angle) * 9.0f, fresh * 40.0f)), 3.0f);
             relief += contrast * (rays * 0.9f * streaks * (1.0f - smoothstepf(1.0f, 2.2f, d)) * stepf(0.9f, d) +
                                   rays * 0.25f * (1.0f - smoothstepf(0.0f, 1.0f, d)));
         }
@@ -910,14 +919,14 @@ static v3 volcanic_albedo(const sg_sphere *body, v3 q) {
         v3 north = vcross(centre, east);
         float angle = TAU_F * hash31(vadds(cell, 91.0f));
         float ux = vdot(offset, east) / radius, uy = vdot(offset, north) / radius;
-        float ca = cosf(angle), sa = sinf(angle);
+        float ca = cos_d(angle), sa = sin_d(angle);
         float uvx = ux * ca - uy * sa, uvy = ux * sa + uy * ca;
         float ragged = fbm(vadd(V(uvx * 2.7f, uvy * 2.7f, 0.0f), vmul(cell, 7.0f)), 3) - 0.5f;
         float sx = uvx * (1.0f / (0.65f + 0.9f * size)), sy = uvy * 1.0f;
         float d = sqrtf(sx * sx + sy * sy) + 0.42f * ragged;
         float pit = 1.0f - smoothstepf(0.68f, 0.86f, d);
         float age = hash31(vadds(cell, 31.0f));
-        float fx = uvx - (0.2f + 2.3f * age), fy = uvy - 0.35f * sinf(uvx * 1.3f + angle);
+        float fx = uvx - (0.2f + 2.3f * age), fy = uvy - 0.35f * sin_d(uvx * 1.3f + angle);
         float gx = fx * (0.75f - 0.48f * age), gy = fy * (0.85f + 0.35f * size);
         float flow_shape = sqrtf(gx * gx + gy * gy) + 0.65f * ragged +
                            0.35f * (fbm(vadd(V(uvx * 1.8f, uvy * 1.8f, 0.0f), vmul(cell, 3.0f)), 4) - 0.5f);
@@ -925,7 +934,7 @@ static v3 volcanic_albedo(const sg_sphere *body, v3 q) {
         dark = maxf_(dark, maxf_(pit, flow) * cutoff);
         float plume = hash31(vadd(cell, V(2.0f, 6.0f, 17.0f)));
         float hx = (uvx - 0.5f) * 0.16f, hy = (uvy - 0.3f) * 0.23f;
-        float halo = expf(-(hx * hx + hy * hy)) * cutoff;
+        float halo = exp_d(-(hx * hx + hy * hy)) * cutoff;
         ash = maxf_(ash, halo * (0.25f + 0.35f * age));
         white = maxf_(white, halo * stepf(0.45f, plume) * (1.0f - stepf(0.83f, plume)));
         float apron = surface_gaussian((sqrtf(uvx * uvx + uvy * uvy) + ragged - 3.5f) / 1.6f) *
@@ -996,7 +1005,7 @@ static v3 surface_albedo_m(const scene *S, uint32_t index, v3 normal, float *mot
     v3 x = V(body->axis_x[0], body->axis_x[1], body->axis_x[2]);
     v3 y = V(body->axis_y[0], body->axis_y[1], body->axis_y[2]);
     v3 local = V(vdot(normal, x), vdot(normal, y), vdot(normal, vcross(x, y)));
-    uint32_t style = (uint32_t)(body->axis_x[3] + 0.5f);
+    uint32_t style = body->axis_x[3] >= 0.5f ? (uint32_t)(body->axis_x[3] + 0.5f) : 0u;
     if (style > 0u) {
         if (mottle_out) *mottle_out = 1.0f;
         return style_albedo(body, style, local);
@@ -2690,8 +2699,11 @@ int oracle_tangent(const sg_settings *settings, const sg_sphere *bodies, const o
                    int threads) {
     int status = check_frame(settings);
     if (status != SG_OK) return status;
-    /* The adjoint does not differentiate the host air. */
+    /* The adjoint does not differentiate the host air or the procedural
+     * surface styles. */
     if (settings->g.atmo_params[3] >= 0.5f) return SG_ERR_INVALID;
+    for (uint32_t i = 0; i < settings->counts[0]; i++)
+        if (bodies[i].axis_x[3] >= 0.5f) return SG_ERR_INVALID;
     uint32_t width = (uint32_t)settings->g.viewport[0];
     uint32_t height = (uint32_t)settings->g.viewport[1];
     if (y1 > height) y1 = height;

@@ -17,7 +17,7 @@ INCLUDE = PACKAGE_DIR.parent / "include"
 LIBRARY = PACKAGE_DIR / "libstargaze_b200.so"
 
 SOURCES = ["sg_kernels.cu", "sg_wavefront.cu", "sg_wave_adjoint.cu", "sg_display.cu", "sg_host.cpp", "sg_noalloc.cu"]
-HEADERS = ["sg_adjoint.cuh", "sg_device.cuh", "sg_integrator.cuh", "sg_air.cuh", "sg_internal.h", "sg_landscape.cuh", "sg_wave_common.cuh"]
+HEADERS = ["sg_adjoint.cuh", "sg_device.cuh", "sg_surface.cuh", "sg_integrator.cuh", "sg_air.cuh", "sg_internal.h", "sg_landscape.cuh", "sg_wave_common.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

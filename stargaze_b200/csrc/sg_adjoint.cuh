@@ -101,9 +101,11 @@ struct GradSink {
     }
 };
 
-// The forward integrator: no hooks. A: the host air's code is compiled in.
-// Frames with air (atmo_params.w >= 0.5) run the A instantiations; the
-// others run kernels that carry none of its code or register pressure.
+// The forward integrator: no hooks. A: the host air's code and the
+// procedural surface styles are compiled in. Frames with air
+// (atmo_params.w >= 0.5) or a styled body (axis_x.w >= 0.5) run the A
+// instantiations; the others run kernels that carry none of that code or
+// its register pressure.
 template <bool A>
 struct Forward {
     static constexpr bool adjoint = false;

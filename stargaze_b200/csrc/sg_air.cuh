@@ -233,7 +233,7 @@ __device__ __forceinline__ float3 reflected_radiance(const Scene &S, Counter<C, 
     const float radius = b_radius(S, index);
     if (sphere_distance(S, K, ray, index, radius, delta) >= 1.0e30f) return f3(0.0f, 0.0f, 0.0f);
     const float3 normal = sphere_normal(S, ray, index, delta);
-    const float3 albedo = surface_albedo(S, index, normal);
+    const float3 albedo = surface_albedo<true>(S, index, normal);
     Ray outgoing{normal * (radius * (1.0f + 2.0e-6f)), normal, index};
     float3 radiance = f3(0.0f, 0.0f, 0.0f);
     const uint32_t n_lights = light_count(S.s);

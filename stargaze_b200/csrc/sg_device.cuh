@@ -53,8 +53,10 @@ enum BodyField : int {
     kRingPlane = 3,   // pole, inner
     kRingParams = 4,  // outer, tau, banded, table slot + 1
     kRingColor = 5,
-    kAxisX = 6,
-    kAxisY = 7,
+    kAxisX = 6,          // xyz body X axis, w surface style
+    kAxisY = 7,          // xyz body Y axis, w pattern seed
+    kSurfaceColor = 8,   // secondary colour, w turbulence or crater density
+    kSurfaceParams = 9,  // bands, storms or ice caps, ocean, clouds
 };
 
 // ---------------------------------------------------------------------------
@@ -822,12 +824,6 @@ static __device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float 
     return mixf(1.0f, 0.68f + 0.64f * noise, strength);
 }
 
-__device__ __forceinline__ float3 surface_albedo(const Scene &S, uint32_t i, float3 normal) {
-    const float4 material = bf(S, i, kMaterial);
-    const float strength = bf(S, i, kLow).w;
-    const float m = strength > 0.0f ? mottle(xyz(bf(S, i, kAxisX)), bf(S, i, kAxisY), strength, normal) : 1.0f;
-    return f3(clampf(material.x * m, 0.0f, 1.0f), clampf(material.y * m, 0.0f, 1.0f),
-              clampf(material.z * m, 0.0f, 1.0f));
-}
-
 }  // namespace sg
+
+#include "sg_surface.cuh"

@@ -840,6 +840,8 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
         status = upload_bodies(ctx, frame, stream);
         if (status != SG_OK) return status;
         sg::TraceParams p = make_params(ctx, s);
+        for (uint32_t k = 0; k < frame->n_bodies; ++k)
+            if (frame->bodies[k].axis_x[3] >= 0.5f) p.styled = 1u;
         // A backdrop left by an earlier sky (the history has reset since).
         if (!p.sky_on && ctx->backdrop_written) {
             SG_CUDA(ctx, cudaMemsetAsync(ctx->backdrop, 0, (size_t)ctx->width * ctx->height * sizeof(float4), stream));
@@ -1326,6 +1328,9 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate the sky backdrop; remove the catalogue and panorama");
     if (frame->globals->atmo_params[3] >= 0.5f)
         return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate the host air (atmo_params.w >= 0.5)");
+    for (uint32_t i = 0; i < frame->n_bodies; ++i)
+        if (frame->bodies[i].axis_x[3] >= 0.5f)
+            return fail(ctx, SG_ERR_STATE, "the adjoint does not differentiate procedural surface styles (axis_x.w >= 0.5)");
     if (key_hash(history_key(ctx, frame)) != tape->history_hash)
         return fail(ctx, SG_ERR_STATE, "frame, options or tables differ from the ones the tape was recorded with");
     grads->dropped = 0;

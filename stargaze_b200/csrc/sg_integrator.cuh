@@ -407,9 +407,9 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
         [[maybe_unused]] GradEntry albedo_e = no_entry();
         if constexpr (G::adjoint) {
             if constexpr (L) {
-                albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+                albedo_g = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo<G::air>(S, bi, normal);
             } else {
-                albedo_g = surface_albedo(S, bi, normal);
+                albedo_g = surface_albedo<G::air>(S, bi, normal);
             }
             albedo_e = albedo_entry<L>(S, grad.inv, ray, hit.t, bi, albedo_g);
         }
@@ -455,9 +455,9 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
         }
         float3 albedo;
         if constexpr (L) {
-            albedo = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo(S, bi, normal);
+            albedo = local ? landscape_albedo(S, ray, hit.t, bi, hit.n) : surface_albedo<G::air>(S, bi, normal);
         } else {
-            albedo = surface_albedo(S, bi, normal);
+            albedo = surface_albedo<G::air>(S, bi, normal);
         }
         radiance = radiance + throughput * albedo * direct_light;
         if (!local && has_ring(S, bi)) {

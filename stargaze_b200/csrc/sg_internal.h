@@ -54,6 +54,8 @@ struct TraceParams {
     // The guided ground sampler (src/guided_ground.rs:14-79): depth-0 local
     // surfaces under air also propose directions toward a reflecting body.
     uint32_t guided_ground;
+    // A body of the frame has a procedural surface style (axis_x.w >= 0.5).
+    uint32_t styled;
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,

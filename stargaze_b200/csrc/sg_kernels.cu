@@ -446,10 +446,12 @@ cudaError_t launch_trace(const TraceParams &p, bool count_events, cudaStream_t s
     const dim3 grid((p.width + kTile - 1) / kTile, (p.height + kTile - 1) / kTile);
     // The landscape instantiation only for frames that enable it: the
     // celestial one carries neither its registers nor its code.
-    // Frames with host air run the instantiations that carry its code; the
-    // event-counting ones always do (it is gated at run time there).
+    // Frames with host air or styled bodies run the instantiations that
+    // carry that code; the event-counting ones always do (gated at run time
+    // there).
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const int which = (count_events ? 8 : 0) | (p.air_on ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    const int which =
+        (count_events ? 8 : 0) | (p.air_on || p.styled ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
     switch (which) {
         case 0: return launch_variant(trace_kernel<false, false, false, false>, grid, smem, stream, p);
         case 1: return launch_variant(trace_kernel<false, false, true, false>, grid, smem, stream, p);

@@ -47,7 +47,8 @@ namespace {
 // ---------------------------------------------------------------------------
 // Stages
 // ---------------------------------------------------------------------------
-// A: the host air's code is compiled in (frames with air run these).
+// A: the host air's code and the surface styles are compiled in (frames
+// with air or styled bodies run these).
 template <bool L, bool F, bool A>
 __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_extend(const __grid_constant__ TraceParams P,
                                                                             const __grid_constant__ WaveParams W,
@@ -299,7 +300,7 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
     if (marks) marks->used = 0;
     if (z == 0 || pixels == 0) return cudaSuccess;
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const int variant = (p.air_on ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    const int variant = (p.air_on || p.styled ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
     StageSet set;
     switch (variant) {
         case 0: set = stage_set<false, false, false>(); break;

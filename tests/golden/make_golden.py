@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import sys
 from pathlib import Path
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -130,11 +131,15 @@ IMAGES = {
     "rings_96x54": (rings_1080p, 96, 54, 16, 2),
     "terrain_96x54": (None, 96, 54, 16, 2),
     "terrain_air_96x54": (None, 96, 54, 16, 2),
+    "styles_96x32": (None, 96, 32, 16, 2),
 }
 
 
 def image_workload(name):
     factory, w, h, spp, batches = IMAGES[name]
+    if name.startswith("styles"):
+        # The six procedural surface styles side by side (no landscape).
+        return SimpleNamespace(frame=ka.styles_scene(w, h), ring_tables={}, max_bounces=2), None
     if factory is None:
         wl, land = terrain_small(width=w, height=h)
         if "air" in name:

@@ -162,3 +162,22 @@ def test_moonlit_ground_matches_oracle(integrator, guided):
     assert err < 2e-3, err
     close = np.abs(img[:, :3] - ref[:, :3]) <= 1e-4 * np.maximum(np.abs(ref[:, :3]), 1e-3 * ref[:, :3].max())
     assert close.all(axis=1).mean() >= 0.99
+
+
+@pytest.mark.parametrize("integrator", ["megakernel", "wavefront"])
+def test_textured_planets_light_night_air(integrator):
+    def make_with(dimensions, options):
+        t = PathTracer(dimensions, options)
+        t.set_integrator(integrator)
+        return t
+
+    r = ka.textured_planets_light_night_air(make_with)
+    assert set(r) == set(ka.STYLES)
+
+
+def test_styled_frames_are_not_differentiated():
+    f = ka.styles_scene(8, 4)
+    t = PathTracer((8, 4), ka.test_options())
+    t.encode(f)
+    with pytest.raises(StargazeError, match="surface styles"):
+        t.backward(f, t.tape(), np.ones((32, 4), np.float32))
