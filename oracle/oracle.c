@@ -1299,6 +1299,15 @@ static void t_interval(const float *T, uint32_t cells, v3 o, v3 inv, uint32_t in
 
 static int is_terrain_alpine(const scene *S) { return ground_theme(S) == 3u; }
 
+/* terrain_shading: terrain.wgsl:142-150 (alpine: steep triangles shade with
+ * their flat face). */
+static v3 terrain_shading(const scene *S, v3 smooth_normal, v3 a, v3 b, v3 c) {
+    if (!is_terrain_alpine(S)) return smooth_normal;
+    v3 face = vnormalize(vcross(vsub(b, a), vsub(c, a)));
+    if (face.y < 0.0f) face = vneg(face);
+    return vnormalize(vmix(smooth_normal, face, smoothstepf(0.25f, 0.5f, 1.0f - face.y)));
+}
+
 /* terrain_query: terrain.wgsl:152-234 (stack widened to 40 slots so 4096
  * cells, eleven internal levels, fit: 3 * 11 + 1 = 34 entries). */
 static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d, float initial_limit, int occlusion,
@@ -1317,7 +1326,6 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
     stack_node[0] = 0u;
     stack_t[0] = maxf_(re, 0.0f);
     uint32_t count = 1;
-    (void)is_terrain_alpine;
     while (count > 0u) {
         count--;
         if (stack_t[count] >= limit) continue;
@@ -1337,7 +1345,7 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
                         v3 n = vnormalize(vadd(vadd(vmul(t_normal(T, cells, x, z), 1.0f - first.x - first.y),
                                                     vmul(t_normal(T, cells, x, z + 1u), first.x)),
                                                vmul(t_normal(T, cells, x + 1u, z), first.y)));
-                        *normal = n;
+                        *normal = terrain_shading(S, n, a, c, b);
                         result = first.z;
                         limit = first.z;
                     }
@@ -1346,7 +1354,7 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
                         v3 n = vnormalize(vadd(vadd(vmul(t_normal(T, cells, x + 1u, z + 1u), 1.0f - second.x - second.y),
                                                     vmul(t_normal(T, cells, x + 1u, z), second.x)),
                                                vmul(t_normal(T, cells, x, z + 1u), second.y)));
-                        *normal = n;
+                        *normal = terrain_shading(S, n, e, b, c);
                         result = second.z;
                         limit = second.z;
                     }
@@ -1604,6 +1612,267 @@ static float map_albedo(const scene *S, v3 p) { return S->t->albedo_map[map_texe
 
 /* landscape_albedo: ground.wgsl:597-632 (themes 0-2; vegetation kinds are
  * rejected), with the albedo-map extension for the ground itself. */
+/* ---------------------------------------------------------------- */
+/* Landscape themes 3 (alpine) and 5 (dunes): ground.wgsl:320-596,   */
+/* terrain.wgsl:142-150. Strict f32 with correctly rounded            */
+/* transcendentals, like the surface styles.                          */
+/* ---------------------------------------------------------------- */
+#define ICE_FLOW 4.4f
+#define DUNE_WIND 0.61f
+#define DUNE_PAN_LEVEL 2.0f
+typedef struct { float x, y; } v2;
+static inline v2 V2(float x, float y) { v2 r = {x, y}; return r; }
+static inline float v2dot(v2 a, v2 b) { return a.x * b.x + a.y * b.y; }
+static inline float v2len(v2 a) { return sqrtf(a.x * a.x + a.y * a.y); }
+
+static inline float terrain_scale(const scene *S) { return clampf_(S->s->g.ground_up[3] / 200000.0f, 0.0001f, 1.0f); }
+static inline float footprint_at(const scene *S, float distance) {
+    return distance * 2.0f * S->s->g.cam_forward[3] / maxf_(S->s->g.viewport[1], 1.0f);
+}
+/* The surface-frame point in terrain units above the curved datum. */
+static inline v3 terrain_local(const scene *S, v3 p) {
+    float c = t_curvature(p.x, p.z, S->s->g.ground_up[3]);
+    return vdivs(V(p.x, p.y - c, p.z), terrain_scale(S));
+}
+
+/* lookout_hill: ground.wgsl:322-325 */
+static float lookout_hill(float r) {
+    float u = minf_(v2len(V2(r, 30.0f)) / 700.0f, 1.0f);
+    return 180.0f * (1.0f - u) * (1.0f - u);
+}
+
+/* dune_cracks: ground.wgsl:490-503 (the gap between the two nearest
+ * jittered cells). */
+static float dune_cracks(v2 p) {
+    v2 g = V2(floorf(p.x), floorf(p.y));
+    v2 f = V2(p.x - g.x, p.y - g.y);
+    float d1 = 8.0f, d2 = 8.0f;
+    for (int j = -1; j <= 1; j++) {
+        for (int i = -1; i <= 1; i++) {
+            v2 o = V2((float)i, (float)j);
+            v3 h = hash33(V(g.x + o.x, g.y + o.y, 3.0f));
+            float d = v2len(V2(o.x + 0.15f + 0.7f * h.x - f.x, o.y + 0.15f + 0.7f * h.y - f.y));
+            if (d < d1) {
+                d2 = d1;
+                d1 = d;
+            } else if (d < d2) {
+                d2 = d;
+            }
+        }
+    }
+    return d2 - d1;
+}
+
+/* ice_crevasse: ground.wgsl:333-360; (coverage, depth from the lip). */
+static v2 ice_crevasse(v2 q, float footprint) {
+    float r = v2len(q);
+    float tension = smoothstepf(650.0f, 900.0f, r) * (1.0f - smoothstepf(1800.0f, 2600.0f, r));
+    float strain = maxf_(smoothstepf(0.47f, 0.58f, fbm(V(q.x / 2600.0f + 4.0f, 2.0f, q.y / 2600.0f), 2)), tension) *
+                   smoothstepf(600.0f, 750.0f, r);
+    if (strain <= 0.0f) return V2(0.0f, 0.0f);
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    float along = v2dot(q, flow) + 280.0f * (vnoise(V(q.x / 1500.0f, q.y / 1500.0f, 1.0f)) - 0.5f);
+    float across = v2dot(q, V2(flow.y, -flow.x)) + 120.0f * (vnoise(V(q.x / 900.0f, q.y / 900.0f, 5.0f)) - 0.5f);
+    float spacing = 60.0f;
+    float row = floorf(along / spacing);
+    uint32_t key = hash_u32(((uint32_t)(int32_t)row * 0x8da6b343u) ^ 0xc3e5u);
+    float length_m = 120.0f + 300.0f * (float)(key & 255u) / 255.0f;
+    float s = across / length_m + (float)((key >> 8u) & 255u) / 255.0f;
+    float segment = floorf(s);
+    float lens = pow_d(maxf_(sin_d(PI_F * (s - segment)), 0.0f), 0.7f);
+    uint32_t open = hash_u32(key ^ (uint32_t)(int32_t)segment);
+    if ((open & 255u) < 70u) return V2(0.0f, 0.0f);
+    float centre = 0.5f + 0.3f * ((float)((open >> 8u) & 255u) / 255.0f - 0.5f);
+    float half_width = 0.5f * (2.0f + 14.0f * (float)((open >> 16u) & 255u) / 255.0f) * lens * strain;
+    float d = fabsf(along / spacing - row - centre) * spacing + 0.8f * (vnoise(V(q.x * 0.15f, q.y * 0.15f, 9.0f)) - 0.5f);
+    float aa = maxf_(footprint, 1.0e-3f);
+    float coverage = clampf_((half_width - d) / aa + 0.5f, 0.0f, 1.0f) * minf_(1.0f, 2.0f * half_width / aa);
+    return V2(coverage, 1.0f - clampf_(d / maxf_(half_width, 1.0e-3f), 0.0f, 1.0f));
+}
+
+/* alpine_floor: ground.wgsl:365-427 */
+static v3 alpine_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float scale = terrain_scale(S);
+    v3 q = terrain_local(S, p);
+    float hill = lookout_hill(v2len(V2(q.x, q.z)));
+    q.y = q.y - hill;
+    float footprint = footprint_at(S, distance) / scale;
+    float detail = 1.0f - smoothstepf(0.025f, 0.2f, footprint);
+    float slope = 1.0f - maxf_(normal.y, 0.0f);
+    float broad = vnoise(vadd(vmul(q, 0.004f), V(11.0f, 4.0f, 1.0f)));
+    float middle = vnoise(vmul(q, 0.2f));
+    float grain = vnoise(vmul(q, 4.0f));
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    float along = v2dot(V2(q.x, q.z), flow);
+    float across = v2dot(V2(q.x, q.z), V2(flow.y, -flow.x));
+    float crust = smoothstepf(0.45f, 0.6f, fbm(V(along * 0.004f, 2.0f, across * 0.012f), 3));
+    v3 snow = vmix(V(0.86f, 0.88f, 0.91f), V(0.76f, 0.8f, 0.86f), crust);
+    snow = vmul(snow, 0.97f + 0.05f * middle);
+    float bare = smoothstepf(0.47f, 0.53f, fbm(vadd(vmul(q, 0.0016f), V(3.0f, 0.0f, 8.0f)), 4) + 0.1f * (broad - 0.5f));
+    v3 ice = vmix(V(0.36f, 0.55f, 0.7f), V(0.52f, 0.67f, 0.78f), middle);
+    float fracture_width = 0.03f + footprint / 4.0f;
+    float fractures = (1.0f - smoothstepf(0.0f, fracture_width, dune_cracks(V2(q.x / 4.0f + 9.0f, q.z / 4.0f + 9.0f)))) *
+                      0.03f / fracture_width;
+    ice = vmix(ice, V(0.82f, 0.86f, 0.9f), minf_(fractures, 1.0f) * 0.7f);
+    ice = vmul(ice, 1.0f + (grain - 0.5f) * 0.12f * detail);
+    v3 glacier = vmix(snow, ice, bare);
+    v3 debris = vmix(V(0.12f, 0.115f, 0.11f), V(0.26f, 0.24f, 0.22f), grain);
+    float dirty = smoothstepf(6.0f, 30.0f, q.y) * (1.0f - smoothstepf(30.0f, 70.0f, q.y));
+    glacier = vmix(glacier, vmix(debris, glacier, 0.45f), dirty * smoothstepf(0.4f, 0.7f, broad) * 0.8f);
+    float wall = smoothstepf(0.35f, 0.6f, slope) * (1.0f - smoothstepf(20.0f, 45.0f, q.y));
+    float depth = smoothstepf(4.0f, -4.0f, q.y);
+    v3 blue = vmix(V(0.32f, 0.55f, 0.72f), V(0.1f, 0.25f, 0.42f), depth);
+    glacier = vmix(glacier, vmul(blue, 0.9f + 0.2f * middle), wall);
+    v2 crack = ice_crevasse(V2(q.x, q.z), footprint);
+    float fade = 1.0f - smoothstepf(10.0f, 25.0f, q.y);
+    crack = V2(crack.x * fade, crack.y * fade);
+    float lip = (1.0f - smoothstepf(0.0f, 0.12f, crack.y)) * crack.x;
+    v3 inside = vmix(V(0.3f, 0.55f, 0.74f), V(0.02f, 0.06f, 0.12f), smoothstepf(0.1f, 0.8f, crack.y));
+    glacier = vmix(glacier, inside, crack.x);
+    glacier = vmix(glacier, V(0.9f, 0.92f, 0.95f), lip * 0.5f);
+    float mountain = maxf_(smoothstepf(25.0f, 70.0f, q.y + 30.0f * (broad - 0.5f)), smoothstepf(4.0f, 15.0f, hill));
+    float joints = 1.0f - smoothstepf(0.0f, 0.06f + footprint / 3.0f,
+                                      dune_cracks(V2((q.x + q.y * 0.5f) / 3.0f, q.z / 3.0f)));
+    v3 granite = vmix(V(0.09f, 0.085f, 0.08f), V(0.24f, 0.215f, 0.19f), broad);
+    granite = vmul(granite, 0.85f + 0.3f * middle - 0.35f * joints * (1.0f - smoothstepf(0.1f, 1.0f, footprint)));
+    float lichen = smoothstepf(0.68f, 0.78f, vnoise(vmul(q, 0.9f))) * (1.0f - smoothstepf(0.6f, 0.9f, slope));
+    granite = vmix(granite, V(0.3f, 0.17f, 0.06f), lichen * 0.5f * detail);
+    float cover = 1.0f - smoothstepf(0.17f, 0.33f, slope + (broad - 0.5f) * 0.18f + (middle - 0.5f) * 0.08f);
+    float scoured = smoothstepf(0.52f, 0.62f, fbm(vadd(vmul(q, 0.012f), V(2.0f, 0.0f, 6.0f)), 4)) *
+                    smoothstepf(25.0f, 90.0f, hill) * (1.0f - smoothstepf(150.0f, 172.0f, hill));
+    float cover_hill = cover * (1.0f - scoured);
+    v3 peak = vmix(granite, snow, cover_hill);
+    v3 color = vmix(glacier, peak, mountain);
+    return vmul(color, 1.0f + (grain - 0.5f) * 0.08f * detail);
+}
+
+/* alpine_shading_normal: ground.wgsl:430-459 (telescope-space normal in
+ * and out, surface-frame point). */
+static v3 alpine_shading_normal(const scene *S, v3 p, float distance, v3 normal) {
+    float footprint = footprint_at(S, distance);
+    v3 n = to_ground(S, normal);
+    float snowy = 1.0f - smoothstepf(0.3f, 0.5f, 1.0f - n.y);
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    v2 side = V2(flow.y, -flow.x);
+    v2 gradient = V2(0.0f, 0.0f);
+    float scale = 1.2f, strength = 0.2f;
+    for (uint32_t octave = 0; octave < 3u; octave++) {
+        float fade = 1.0f - smoothstepf(0.08f * scale, 0.25f * scale, footprint);
+        if (fade > 0.0f) {
+            float a = v2dot(V2(p.x, p.z), flow) / (6.0f * scale);
+            float c = v2dot(V2(p.x, p.z), side) / scale;
+            float e = 0.08f;
+            float o = (float)octave * 13.0f;
+            float da = vnoise(V(a + e, o, c)) - vnoise(V(a - e, o, c));
+            float dc = vnoise(V(a, o, c + e)) - vnoise(V(a, o, c - e));
+            float ridge_ = 1.0f + 1.5f * (1.0f - fabsf(vnoise(V(a, o, c)) * 2.0f - 1.0f));
+            float k = strength * fade * ridge_ * scale;
+            float gx = (flow.x * da / (6.0f * scale) + side.x * dc / scale) / (2.0f * e) * k;
+            float gz = (flow.y * da / (6.0f * scale) + side.y * dc / scale) / (2.0f * e) * k;
+            gradient = V2(gradient.x + gx, gradient.y + gz);
+        }
+        scale *= 6.0f;
+        strength *= 0.6f;
+    }
+    gradient = V2(gradient.x * snowy, gradient.y * snowy);
+    return vnormalize(vadd(normal, from_ground(S, V(-gradient.x, 0.0f, -gradient.y))));
+}
+
+/* dune_pan: ground.wgsl:483-486 */
+static v3 dune_pan(uint32_t i) {
+    return i == 0u ? V(842.6f, 707.1f, 560.0f) : V(4346.7f, 1164.7f, 900.0f);
+}
+
+/* dune_floor: ground.wgsl:509-568 */
+static v3 dune_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float scale = terrain_scale(S);
+    v3 q = terrain_local(S, p);
+    float footprint = footprint_at(S, distance) / scale;
+    float detail = 1.0f - smoothstepf(0.02f, 0.15f, footprint);
+    float slope = 1.0f - maxf_(normal.y, 0.0f);
+    float broad = vnoise(vadd(vmul(q, 0.0015f), V(1.0f, 7.0f, 3.0f)));
+    float middle = vnoise(vmul(q, 0.05f));
+    float rise = smoothstepf(6.0f, 160.0f, q.y + 40.0f * (broad - 0.5f));
+    v3 plinth = vmix(V(0.3f, 0.095f, 0.038f), V(0.36f, 0.12f, 0.045f), broad);
+    v3 upper = vmix(V(0.42f, 0.155f, 0.06f), V(0.47f, 0.19f, 0.072f), broad);
+    v3 sand = vmul(vmix(plinth, upper, rise), 0.94f + 0.08f * middle);
+    float flat = v2len(V2(normal.x, normal.z));
+    if (flat > 1.0e-3f) {
+        v2 down = V2(-normal.x / flat, -normal.z / flat);
+        float across = v2dot(V2(q.x, q.z), V2(-down.y, down.x));
+        float along = v2dot(V2(q.x, q.z), down);
+        float tongues = fbm(V(across * 0.18f, along * 0.012f, 5.0f), 3);
+        float slip = smoothstepf(0.32f, 0.45f, slope);
+        sand = vmix(sand, vmul(vmulv(sand, V(1.06f, 1.12f, 1.16f)), 0.86f + 0.28f * tongues), slip);
+    }
+    float lag = smoothstepf(0.6f, 0.76f, fbm(vadd(vmulv(q, V(0.013f, 0.0f, 0.004f)), V(9.0f, 0.0f, 2.0f)), 4)) *
+                (1.0f - smoothstepf(0.04f, 0.16f, slope)) * (1.0f - smoothstepf(10.0f, 45.0f, q.y));
+    sand = vmix(sand, V(0.13f, 0.065f, 0.05f), lag * 0.55f);
+    float corridor = (1.0f - smoothstepf(5.0f, 16.0f, q.y + 6.0f * (broad - 0.5f))) *
+                     (1.0f - smoothstepf(0.03f, 0.1f, slope));
+    v3 gravel = vmix(V(0.39f, 0.21f, 0.115f), V(0.45f, 0.28f, 0.16f), vnoise(vmul(q, 0.3f)));
+    float pebbles = smoothstepf(0.72f, 0.8f, vnoise(vmul(q, 7.0f))) * detail;
+    sand = vmix(sand, vmul(gravel, 1.0f - 0.45f * pebbles), corridor * 0.6f);
+    float pan = 0.0f;
+    for (uint32_t i = 0; i < 2u; i++) {
+        v3 c = dune_pan(i);
+        pan = maxf_(pan, 1.0f - smoothstepf(c.z * 1.2f, c.z * 1.35f + 140.0f, v2len(V2(q.x - c.x, q.z - c.y))));
+    }
+    pan *= 1.0f - smoothstepf(DUNE_PAN_LEVEL + 0.25f, DUNE_PAN_LEVEL + 1.5f, q.y);
+    if (pan > 0.0f) {
+        float tone = fbm(vadd(vmul(q, 0.012f), V(4.0f, 0.0f, 1.0f)), 4);
+        v3 clay = vmix(V(0.4f, 0.35f, 0.29f), V(0.6f, 0.56f, 0.49f), smoothstepf(0.3f, 0.7f, tone));
+        clay = vmul(clay, 0.82f + 0.18f * smoothstepf(0.35f, 1.0f, pan));
+        float fine_width = 0.04f + footprint / 0.9f;
+        float cracks = (1.0f - smoothstepf(0.0f, fine_width, dune_cracks(V2(q.x / 0.9f, q.z / 0.9f)))) * 0.04f / fine_width;
+        float wide_width = 0.03f + footprint / 6.0f;
+        float large = (1.0f - smoothstepf(0.0f, wide_width, dune_cracks(V2(q.x / 6.0f + 17.0f, q.z / 6.0f + 17.0f)))) *
+                      0.03f / wide_width;
+        clay = vmul(clay, 1.0f - 0.6f * minf_(cracks, 1.0f) - 0.45f * minf_(large, 1.0f));
+        clay = vmul(clay, 0.92f + 0.16f * vnoise(vmul(q, 2.3f)) * (1.0f - smoothstepf(0.04f, 0.25f, footprint)));
+        sand = vmix(sand, clay, pan);
+    }
+    return vmul(sand, 1.0f + (vnoise(vmul(q, 9.0f)) - 0.5f) * 0.12f * detail);
+}
+
+/* dune_ripples: ground.wgsl:571-582; the surface-frame (x, z) gradient. */
+static v2 dune_ripples(v3 p, float wavelength, float warp, float amplitude) {
+    v2 wind = V2(sin_d(DUNE_WIND), cos_d(DUNE_WIND));
+    v2 side = V2(wind.y, -wind.x);
+    float bend = warp * (vnoise(V(p.x / (9.0f * wavelength), p.z / (9.0f * wavelength), 1.0f)) +
+                         0.35f * vnoise(V(p.x / (2.5f * wavelength), p.z / (2.5f * wavelength), 7.0f)));
+    float phase = v2dot(V2(p.x, p.z), wind) / wavelength + bend +
+                  0.4f * sin_d(v2dot(V2(p.x, p.z), side) / (3.0f * wavelength));
+    float theta = TAU_F * phase;
+    float slope = cos_d(theta + 0.65f * sin_d(theta)) * (1.0f + 0.65f * cos_d(theta));
+    float patches = smoothstepf(0.25f, 0.6f, vnoise(V(p.x / (14.0f * wavelength), p.z / (14.0f * wavelength), 3.0f)));
+    float k = slope * amplitude * TAU_F / wavelength * patches;
+    return V2(wind.x * k, wind.y * k);
+}
+
+/* dune_shading_normal: ground.wgsl:583-595 */
+static v3 dune_shading_normal(const scene *S, v3 p, float distance, v3 normal) {
+    float footprint = footprint_at(S, distance);
+    v3 n = to_ground(S, normal);
+    float gentle = 1.0f - smoothstepf(0.22f, 0.38f, 1.0f - n.y);
+    v3 q = terrain_local(S, p);
+    float dry = smoothstepf(DUNE_PAN_LEVEL + 0.4f, DUNE_PAN_LEVEL + 1.5f, q.y);
+    v2 gradient = V2(0.0f, 0.0f);
+    float fine = 1.0f - smoothstepf(0.03f, 0.07f, footprint);
+    if (fine > 0.0f) {
+        v2 r = dune_ripples(p, 0.12f, 2.5f, 0.006f);
+        gradient = V2(gradient.x + r.x * fine, gradient.y + r.y * fine);
+    }
+    float coarse = (1.0f - smoothstepf(0.15f, 0.4f, footprint)) * (1.0f - smoothstepf(9.0f, 16.0f, q.y));
+    if (coarse > 0.0f) {
+        v2 r = dune_ripples(vadds(p, 31.0f), 0.8f, 2.0f, 0.03f);
+        gradient = V2(gradient.x + r.x * coarse, gradient.y + r.y * coarse);
+    }
+    float k = gentle * dry;
+    gradient = V2(gradient.x * k, gradient.y * k);
+    return vnormalize(vadd(normal, from_ground(S, V(-gradient.x, 0.0f, -gradient.y))));
+}
+
 static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
     v3 p = landscape_point(S, ray, hit);
     float distance = hit.distance * METRES_PER_AU;
@@ -1613,6 +1882,8 @@ static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
         switch (ground_theme(S)) {
             case 1u: return desert_floor(S, p, distance, n);
             case 2u: return crater_floor(S, p, distance, n);
+            case 3u: return alpine_floor(S, p, distance, n);
+            case 5u: return dune_floor(S, p, distance, n);
             default: return forest_floor(S, p, distance, n);
         }
     }
@@ -1643,6 +1914,8 @@ static v3 landscape_shading_normal(const scene *S, ray_t ray, hit_t hit) {
     if (hit.index != LOCAL_BASE && hit.index != TERRAIN_ID) return hit.normal;
     v3 p = landscape_point(S, ray, hit);
     float distance = hit.distance * METRES_PER_AU;
+    if (ground_theme(S) == 5u) return dune_shading_normal(S, p, distance, hit.normal);
+    if (ground_theme(S) == 3u) return alpine_shading_normal(S, p, distance, hit.normal);
     float strength = 0.11f * (1.0f - smoothstepf(8.0f, 65.0f, distance));
     float dx = vnoise(vmul(vadd(p, V(0.025f, 0.0f, 0.0f)), 6.0f)) - vnoise(vmul(vsub(p, V(0.025f, 0.0f, 0.0f)), 6.0f));
     float dz = vnoise(vmul(vadd(p, V(0.0f, 0.0f, 0.025f)), 6.0f)) - vnoise(vmul(vsub(p, V(0.0f, 0.0f, 0.025f)), 6.0f));
@@ -2527,13 +2800,14 @@ static v3 camera_direction(const scene *S, uint32_t x, uint32_t y, uint32_t *rng
     return vnormalize(V(ndc_x * tangent * S->s->g.viewport[3], ndc_y * tangent, -1.0f));
 }
 
-/* Frames the restatement covers: landscape themes 0-2;
+/* Frames the restatement covers: landscape themes 0-3 and 5;
  * no vegetation primitives; terrain only with a terrain table. */
 static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
     if (!s) return SG_ERR_INVALID;
     if (s->counts[0] > SG_BODY_CAPACITY) return SG_ERR_CAPACITY;
     if (s->g.ground_north[3] != 0.0f) {
-        if ((s->g.ground_counts[2] & 255u) > 2u) return SG_ERR_INVALID;
+        uint32_t theme = s->g.ground_counts[2] & 255u;
+        if (theme == 4u || theme > 5u) return SG_ERR_INVALID;
         if (s->g.ground_counts[1] != 0u && (!t || !t->terrain)) return SG_ERR_INVALID;
         if (s->g.ground_counts[0] > 0u && (!t || !t->ground || t->n_ground < s->g.ground_counts[0])) return SG_ERR_INVALID;
         for (uint32_t i = 0; t && t->ground && i < s->g.ground_counts[0]; i++)

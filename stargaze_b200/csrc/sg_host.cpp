@@ -252,8 +252,9 @@ int validate_frame(sg_context *ctx, const sg_frame *frame) {
     if (host != 0.0f) {
         if (host != std::floor(host) || host < 1.0f || host > (float)frame->n_bodies)
             return fail(ctx, SG_ERR_INVALID, "ground_north.w must be 0 or a body index + 1");
-        if ((frame->globals->ground_counts[2] & 255u) > 2u)
-            return fail(ctx, SG_ERR_INVALID, "landscape themes 3-5 (alpine, basalt, dunes) are not implemented");
+        const uint32_t theme = frame->globals->ground_counts[2] & 255u;
+        if (theme == 4u || theme > 5u)
+            return fail(ctx, SG_ERR_INVALID, "landscape theme 4 (basalt) and themes above 5 are not implemented");
         if (frame->globals->ground_counts[1] != 0u && !ctx->terrain)
             return fail(ctx, SG_ERR_STATE, "terrain is enabled but no terrain was uploaded");
         if (!(frame->globals->ground_up[3] > 0.0f))

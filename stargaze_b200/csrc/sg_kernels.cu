@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(kThreads) terrain_probe_kernel(const __grid_co
     if (P.terrain) {
         const float3 o = f3(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]);
         const float3 d = f3(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
-        result = terrain_query(P.terrain, P.terrain_cells, P.s.g.ground_up[3], o, d, 1.0e29f, false);
+        result = terrain_query(P.terrain, P.terrain_cells, P.s.g.ground_up[3], (P.s.g.ground_counts[2] & 255u) == 3u,
+                               o, d, 1.0e29f, false);
     }
     out[4 * k + 0] = result.x;
     out[4 * k + 1] = result.y;

@@ -242,7 +242,8 @@ __device__ __forceinline__ float2 t_interval(const float *T, uint32_t cells, flo
 
 // terrain_query (terrain.wgsl:152-234): near-to-far min/max quadtree.
 // Returns (normal, distance); distance 1e30 on a miss.
-static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cells, float radius, float3 o, float3 d,
+static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cells, float radius, bool alpine, float3 o,
+                                                    float3 d,
                                              float initial_limit, bool occlusion) {
     float4 result = make_float4(0.0f, 0.0f, 0.0f, 1.0e30f);
     float limit = initial_limit;
@@ -275,17 +276,19 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
                     const float3 second = t_triangle(o, d, e, b, c);
                     if (first.z < limit) {
                         if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, first.z);
-                        const float3 n = normalize(t_normal(T, cells, x, z) * (1.0f - first.x - first.y) +
-                                                   t_normal(T, cells, x, z + 1u) * first.x +
-                                                   t_normal(T, cells, x + 1u, z) * first.y);
+                        float3 n = normalize(t_normal(T, cells, x, z) * (1.0f - first.x - first.y) +
+                                             t_normal(T, cells, x, z + 1u) * first.x +
+                                             t_normal(T, cells, x + 1u, z) * first.y);
+                        if (alpine) n = style::alpine_face_shading(n, a, c, b);
                         result = make_float4(n.x, n.y, n.z, first.z);
                         limit = first.z;
                     }
                     if (second.z < limit) {
                         if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, second.z);
-                        const float3 n = normalize(t_normal(T, cells, x + 1u, z + 1u) * (1.0f - second.x - second.y) +
-                                                   t_normal(T, cells, x + 1u, z) * second.x +
-                                                   t_normal(T, cells, x, z + 1u) * second.y);
+                        float3 n = normalize(t_normal(T, cells, x + 1u, z + 1u) * (1.0f - second.x - second.y) +
+                                             t_normal(T, cells, x + 1u, z) * second.x +
+                                             t_normal(T, cells, x, z + 1u) * second.y);
+                        if (alpine) n = style::alpine_face_shading(n, e, b, c);
                         result = make_float4(n.x, n.y, n.z, second.z);
                         limit = second.z;
                     }
@@ -413,7 +416,8 @@ static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K,
     }
     if (s->g.ground_counts[1] != 0u && S.p->terrain) {
         const float tl = __fmul_rn(fminf(closest.t, 1.0e18f), kMetresPerAu);
-        const float4 terrain = terrain_query(S.p->terrain, S.p->terrain_cells, radius, o, d, tl, occlusion);
+        const float4 terrain = terrain_query(S.p->terrain, S.p->terrain_cells, radius,
+                                             (S.s->g.ground_counts[2] & 255u) == 3u, o, d, tl, occlusion);
         if (terrain.w < tl && terrain.w < 1.0e29f) {
             closest = LandHit{__fdiv_rn(terrain.w, kMetresPerAu), kTerrainId, 0.0f, from_ground(S, xyz(terrain))};
             if (occlusion) return closest;
@@ -554,6 +558,286 @@ static __device__ __noinline__ float3 crater_floor(float3 p, float footprint, fl
     return f3(tone, tone * 0.97f, tone * 0.93f);
 }
 
+namespace style {
+
+// Landscape themes 3 (alpine) and 5 (dunes), in the strict arithmetic of
+// the surface styles (sg_surface.cuh): their floors hash surface-frame
+// coordinates, so each operation rounds exactly as the CPU restatement's.
+struct v2 {
+    sf x, y;
+};
+__device__ __forceinline__ v2 V2(sf x, sf y) { return v2{x, y}; }
+__device__ __forceinline__ sf v2dot(v2 a, v2 b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ sf v2len(v2 a) { return sqrtf(a.x * a.x + a.y * a.y); }
+__device__ __forceinline__ sv to_ground_s(const Scene &S, sv v) {
+    const float3 g = to_ground(S, to_f3(v));
+    return V(g.x, g.y, g.z);
+}
+__device__ __forceinline__ sv from_ground_s(const Scene &S, sv v) {
+    const float3 g = from_ground(S, to_f3(v));
+    return V(g.x, g.y, g.z);
+}
+__device__ __forceinline__ sf terrain_scale(const Scene &S) {
+    return clampf_(sf(S.s->g.ground_up[3]) / sf(200000.0f), 0.0001f, 1.0f);
+}
+__device__ __forceinline__ sf footprint_at(const Scene &S, sf distance) {
+    return distance * 2.0f * S.s->g.cam_forward[3] / maxf_(S.s->g.viewport[1], 1.0f);
+}
+// The surface-frame point in terrain units above the curved datum.
+__device__ __forceinline__ sv terrain_local(const Scene &S, sv p) {
+    const sf c = sf(t_curvature(p.x.v, p.z.v, S.s->g.ground_up[3]));
+    return vdivs(V(p.x, p.y - c, p.z), terrain_scale(S));
+}
+
+/* ---------------------------------------------------------------- */
+/* Landscape themes 3 (alpine) and 5 (dunes): ground.wgsl:320-596,   */
+/* terrain.wgsl:142-150. Strict f32 with correctly rounded            */
+/* transcendentals, like the surface styles.                          */
+/* ---------------------------------------------------------------- */
+constexpr float ICE_FLOW = 4.4f;
+constexpr float DUNE_WIND = 0.61f;
+constexpr float DUNE_PAN_LEVEL = 2.0f;
+
+/* lookout_hill: ground.wgsl:322-325 */
+static __device__ __noinline__ sf lookout_hill(sf r) {
+    sf u = minf_(v2len(V2(r, 30.0f)) / 700.0f, 1.0f);
+    return 180.0f * (1.0f - u) * (1.0f - u);
+}
+
+/* dune_cracks: ground.wgsl:490-503 (the gap between the two nearest
+ * jittered cells). */
+static __device__ __noinline__ sf dune_cracks(v2 p) {
+    v2 g = V2(floorf(p.x), floorf(p.y));
+    v2 f = V2(p.x - g.x, p.y - g.y);
+    sf d1 = 8.0f, d2 = 8.0f;
+    for (int j = -1; j <= 1; j++) {
+        for (int i = -1; i <= 1; i++) {
+            v2 o = V2((float)i, (float)j);
+            sv h = hash33(V(g.x + o.x, g.y + o.y, 3.0f));
+            sf d = v2len(V2(o.x + 0.15f + 0.7f * h.x - f.x, o.y + 0.15f + 0.7f * h.y - f.y));
+            if (d < d1) {
+                d2 = d1;
+                d1 = d;
+            } else if (d < d2) {
+                d2 = d;
+            }
+        }
+    }
+    return d2 - d1;
+}
+
+/* ice_crevasse: ground.wgsl:333-360; (coverage, depth from the lip). */
+static __device__ __noinline__ v2 ice_crevasse(v2 q, sf footprint) {
+    sf r = v2len(q);
+    sf tension = smoothstepf(650.0f, 900.0f, r) * (1.0f - smoothstepf(1800.0f, 2600.0f, r));
+    sf strain = maxf_(smoothstepf(0.47f, 0.58f, fbm(V(q.x / 2600.0f + 4.0f, 2.0f, q.y / 2600.0f), 2)), tension) *
+                   smoothstepf(600.0f, 750.0f, r);
+    if (strain <= 0.0f) return V2(0.0f, 0.0f);
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    sf along = v2dot(q, flow) + 280.0f * (vnoise(V(q.x / 1500.0f, q.y / 1500.0f, 1.0f)) - 0.5f);
+    sf across = v2dot(q, V2(flow.y, -flow.x)) + 120.0f * (vnoise(V(q.x / 900.0f, q.y / 900.0f, 5.0f)) - 0.5f);
+    sf spacing = 60.0f;
+    sf row = floorf(along / spacing);
+    uint32_t key = hash_u32(((uint32_t)(int32_t)row.v * 0x8da6b343u) ^ 0xc3e5u);
+    sf length_m = 120.0f + 300.0f * (float)(key & 255u) / 255.0f;
+    sf s = across / length_m + (float)((key >> 8u) & 255u) / 255.0f;
+    sf segment = floorf(s);
+    sf lens = pow_d(maxf_(sin_d(PI_F * (s - segment)), 0.0f), 0.7f);
+    uint32_t open = hash_u32(key ^ (uint32_t)(int32_t)segment.v);
+    if ((open & 255u) < 70u) return V2(0.0f, 0.0f);
+    sf centre = 0.5f + 0.3f * ((float)((open >> 8u) & 255u) / 255.0f - 0.5f);
+    sf half_width = 0.5f * (2.0f + 14.0f * (float)((open >> 16u) & 255u) / 255.0f) * lens * strain;
+    sf d = fabsf(along / spacing - row - centre) * spacing + 0.8f * (vnoise(V(q.x * 0.15f, q.y * 0.15f, 9.0f)) - 0.5f);
+    sf aa = maxf_(footprint, 1.0e-3f);
+    sf coverage = clampf_((half_width - d) / aa + 0.5f, 0.0f, 1.0f) * minf_(1.0f, 2.0f * half_width / aa);
+    return V2(coverage, 1.0f - clampf_(d / maxf_(half_width, 1.0e-3f), 0.0f, 1.0f));
+}
+
+/* alpine_floor: ground.wgsl:365-427 */
+static __device__ __noinline__ sv alpine_floor(const Scene &S, sv p, sf distance, sv normal) {
+    sf scale = terrain_scale(S);
+    sv q = terrain_local(S, p);
+    sf hill = lookout_hill(v2len(V2(q.x, q.z)));
+    q.y = q.y - hill;
+    sf footprint = footprint_at(S, distance) / scale;
+    sf detail = 1.0f - smoothstepf(0.025f, 0.2f, footprint);
+    sf slope = 1.0f - maxf_(normal.y, 0.0f);
+    sf broad = vnoise(vadd(vmul(q, 0.004f), V(11.0f, 4.0f, 1.0f)));
+    sf middle = vnoise(vmul(q, 0.2f));
+    sf grain = vnoise(vmul(q, 4.0f));
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    sf along = v2dot(V2(q.x, q.z), flow);
+    sf across = v2dot(V2(q.x, q.z), V2(flow.y, -flow.x));
+    sf crust = smoothstepf(0.45f, 0.6f, fbm(V(along * 0.004f, 2.0f, across * 0.012f), 3));
+    sv snow = vmix(V(0.86f, 0.88f, 0.91f), V(0.76f, 0.8f, 0.86f), crust);
+    snow = vmul(snow, 0.97f + 0.05f * middle);
+    sf bare = smoothstepf(0.47f, 0.53f, fbm(vadd(vmul(q, 0.0016f), V(3.0f, 0.0f, 8.0f)), 4) + 0.1f * (broad - 0.5f));
+    sv ice = vmix(V(0.36f, 0.55f, 0.7f), V(0.52f, 0.67f, 0.78f), middle);
+    sf fracture_width = 0.03f + footprint / 4.0f;
+    sf fractures = (1.0f - smoothstepf(0.0f, fracture_width, dune_cracks(V2(q.x / 4.0f + 9.0f, q.z / 4.0f + 9.0f)))) *
+                      0.03f / fracture_width;
+    ice = vmix(ice, V(0.82f, 0.86f, 0.9f), minf_(fractures, 1.0f) * 0.7f);
+    ice = vmul(ice, 1.0f + (grain - 0.5f) * 0.12f * detail);
+    sv glacier = vmix(snow, ice, bare);
+    sv debris = vmix(V(0.12f, 0.115f, 0.11f), V(0.26f, 0.24f, 0.22f), grain);
+    sf dirty = smoothstepf(6.0f, 30.0f, q.y) * (1.0f - smoothstepf(30.0f, 70.0f, q.y));
+    glacier = vmix(glacier, vmix(debris, glacier, 0.45f), dirty * smoothstepf(0.4f, 0.7f, broad) * 0.8f);
+    sf wall = smoothstepf(0.35f, 0.6f, slope) * (1.0f - smoothstepf(20.0f, 45.0f, q.y));
+    sf depth = smoothstepf(4.0f, -4.0f, q.y);
+    sv blue = vmix(V(0.32f, 0.55f, 0.72f), V(0.1f, 0.25f, 0.42f), depth);
+    glacier = vmix(glacier, vmul(blue, 0.9f + 0.2f * middle), wall);
+    v2 crack = ice_crevasse(V2(q.x, q.z), footprint);
+    sf fade = 1.0f - smoothstepf(10.0f, 25.0f, q.y);
+    crack = V2(crack.x * fade, crack.y * fade);
+    sf lip = (1.0f - smoothstepf(0.0f, 0.12f, crack.y)) * crack.x;
+    sv inside = vmix(V(0.3f, 0.55f, 0.74f), V(0.02f, 0.06f, 0.12f), smoothstepf(0.1f, 0.8f, crack.y));
+    glacier = vmix(glacier, inside, crack.x);
+    glacier = vmix(glacier, V(0.9f, 0.92f, 0.95f), lip * 0.5f);
+    sf mountain = maxf_(smoothstepf(25.0f, 70.0f, q.y + 30.0f * (broad - 0.5f)), smoothstepf(4.0f, 15.0f, hill));
+    sf joints = 1.0f - smoothstepf(0.0f, 0.06f + footprint / 3.0f,
+                                      dune_cracks(V2((q.x + q.y * 0.5f) / 3.0f, q.z / 3.0f)));
+    sv granite = vmix(V(0.09f, 0.085f, 0.08f), V(0.24f, 0.215f, 0.19f), broad);
+    granite = vmul(granite, 0.85f + 0.3f * middle - 0.35f * joints * (1.0f - smoothstepf(0.1f, 1.0f, footprint)));
+    sf lichen = smoothstepf(0.68f, 0.78f, vnoise(vmul(q, 0.9f))) * (1.0f - smoothstepf(0.6f, 0.9f, slope));
+    granite = vmix(granite, V(0.3f, 0.17f, 0.06f), lichen * 0.5f * detail);
+    sf cover = 1.0f - smoothstepf(0.17f, 0.33f, slope + (broad - 0.5f) * 0.18f + (middle - 0.5f) * 0.08f);
+    sf scoured = smoothstepf(0.52f, 0.62f, fbm(vadd(vmul(q, 0.012f), V(2.0f, 0.0f, 6.0f)), 4)) *
+                    smoothstepf(25.0f, 90.0f, hill) * (1.0f - smoothstepf(150.0f, 172.0f, hill));
+    sf cover_hill = cover * (1.0f - scoured);
+    sv peak = vmix(granite, snow, cover_hill);
+    sv color = vmix(glacier, peak, mountain);
+    return vmul(color, 1.0f + (grain - 0.5f) * 0.08f * detail);
+}
+
+/* alpine_shading_normal: ground.wgsl:430-459 (telescope-space normal in
+ * and out, surface-frame point). */
+static __device__ __noinline__ sv alpine_shading_normal(const Scene &S, sv p, sf distance, sv normal) {
+    sf footprint = footprint_at(S, distance);
+    sv n = to_ground_s(S, normal);
+    sf snowy = 1.0f - smoothstepf(0.3f, 0.5f, 1.0f - n.y);
+    v2 flow = V2(sin_d(ICE_FLOW), cos_d(ICE_FLOW));
+    v2 side = V2(flow.y, -flow.x);
+    v2 gradient = V2(0.0f, 0.0f);
+    sf scale = 1.2f, strength = 0.2f;
+    for (uint32_t octave = 0; octave < 3u; octave++) {
+        sf fade = 1.0f - smoothstepf(0.08f * scale, 0.25f * scale, footprint);
+        if (fade > 0.0f) {
+            sf a = v2dot(V2(p.x, p.z), flow) / (6.0f * scale);
+            sf c = v2dot(V2(p.x, p.z), side) / scale;
+            sf e = 0.08f;
+            sf o = (float)octave * 13.0f;
+            sf da = vnoise(V(a + e, o, c)) - vnoise(V(a - e, o, c));
+            sf dc = vnoise(V(a, o, c + e)) - vnoise(V(a, o, c - e));
+            sf ridge_ = 1.0f + 1.5f * (1.0f - fabsf(vnoise(V(a, o, c)) * 2.0f - 1.0f));
+            sf k = strength * fade * ridge_ * scale;
+            sf gx = (flow.x * da / (6.0f * scale) + side.x * dc / scale) / (2.0f * e) * k;
+            sf gz = (flow.y * da / (6.0f * scale) + side.y * dc / scale) / (2.0f * e) * k;
+            gradient = V2(gradient.x + gx, gradient.y + gz);
+        }
+        scale *= 6.0f;
+        strength *= 0.6f;
+    }
+    gradient = V2(gradient.x * snowy, gradient.y * snowy);
+    return vnormalize(vadd(normal, from_ground_s(S, V(-gradient.x, 0.0f, -gradient.y))));
+}
+
+/* dune_pan: ground.wgsl:483-486 */
+static __device__ __noinline__ sv dune_pan(uint32_t i) {
+    return i == 0u ? V(842.6f, 707.1f, 560.0f) : V(4346.7f, 1164.7f, 900.0f);
+}
+
+/* dune_floor: ground.wgsl:509-568 */
+static __device__ __noinline__ sv dune_floor(const Scene &S, sv p, sf distance, sv normal) {
+    sf scale = terrain_scale(S);
+    sv q = terrain_local(S, p);
+    sf footprint = footprint_at(S, distance) / scale;
+    sf detail = 1.0f - smoothstepf(0.02f, 0.15f, footprint);
+    sf slope = 1.0f - maxf_(normal.y, 0.0f);
+    sf broad = vnoise(vadd(vmul(q, 0.0015f), V(1.0f, 7.0f, 3.0f)));
+    sf middle = vnoise(vmul(q, 0.05f));
+    sf rise = smoothstepf(6.0f, 160.0f, q.y + 40.0f * (broad - 0.5f));
+    sv plinth = vmix(V(0.3f, 0.095f, 0.038f), V(0.36f, 0.12f, 0.045f), broad);
+    sv upper = vmix(V(0.42f, 0.155f, 0.06f), V(0.47f, 0.19f, 0.072f), broad);
+    sv sand = vmul(vmix(plinth, upper, rise), 0.94f + 0.08f * middle);
+    sf flat = v2len(V2(normal.x, normal.z));
+    if (flat > 1.0e-3f) {
+        v2 down = V2(-normal.x / flat, -normal.z / flat);
+        sf across = v2dot(V2(q.x, q.z), V2(-down.y, down.x));
+        sf along = v2dot(V2(q.x, q.z), down);
+        sf tongues = fbm(V(across * 0.18f, along * 0.012f, 5.0f), 3);
+        sf slip = smoothstepf(0.32f, 0.45f, slope);
+        sand = vmix(sand, vmul(vmulv(sand, V(1.06f, 1.12f, 1.16f)), 0.86f + 0.28f * tongues), slip);
+    }
+    sf lag = smoothstepf(0.6f, 0.76f, fbm(vadd(vmulv(q, V(0.013f, 0.0f, 0.004f)), V(9.0f, 0.0f, 2.0f)), 4)) *
+                (1.0f - smoothstepf(0.04f, 0.16f, slope)) * (1.0f - smoothstepf(10.0f, 45.0f, q.y));
+    sand = vmix(sand, V(0.13f, 0.065f, 0.05f), lag * 0.55f);
+    sf corridor = (1.0f - smoothstepf(5.0f, 16.0f, q.y + 6.0f * (broad - 0.5f))) *
+                     (1.0f - smoothstepf(0.03f, 0.1f, slope));
+    sv gravel = vmix(V(0.39f, 0.21f, 0.115f), V(0.45f, 0.28f, 0.16f), vnoise(vmul(q, 0.3f)));
+    sf pebbles = smoothstepf(0.72f, 0.8f, vnoise(vmul(q, 7.0f))) * detail;
+    sand = vmix(sand, vmul(gravel, 1.0f - 0.45f * pebbles), corridor * 0.6f);
+    sf pan = 0.0f;
+    for (uint32_t i = 0; i < 2u; i++) {
+        sv c = dune_pan(i);
+        pan = maxf_(pan, 1.0f - smoothstepf(c.z * 1.2f, c.z * 1.35f + 140.0f, v2len(V2(q.x - c.x, q.z - c.y))));
+    }
+    pan *= 1.0f - smoothstepf(DUNE_PAN_LEVEL + 0.25f, DUNE_PAN_LEVEL + 1.5f, q.y);
+    if (pan > 0.0f) {
+        sf tone = fbm(vadd(vmul(q, 0.012f), V(4.0f, 0.0f, 1.0f)), 4);
+        sv clay = vmix(V(0.4f, 0.35f, 0.29f), V(0.6f, 0.56f, 0.49f), smoothstepf(0.3f, 0.7f, tone));
+        clay = vmul(clay, 0.82f + 0.18f * smoothstepf(0.35f, 1.0f, pan));
+        sf fine_width = 0.04f + footprint / 0.9f;
+        sf cracks = (1.0f - smoothstepf(0.0f, fine_width, dune_cracks(V2(q.x / 0.9f, q.z / 0.9f)))) * 0.04f / fine_width;
+        sf wide_width = 0.03f + footprint / 6.0f;
+        sf large = (1.0f - smoothstepf(0.0f, wide_width, dune_cracks(V2(q.x / 6.0f + 17.0f, q.z / 6.0f + 17.0f)))) *
+                      0.03f / wide_width;
+        clay = vmul(clay, 1.0f - 0.6f * minf_(cracks, 1.0f) - 0.45f * minf_(large, 1.0f));
+        clay = vmul(clay, 0.92f + 0.16f * vnoise(vmul(q, 2.3f)) * (1.0f - smoothstepf(0.04f, 0.25f, footprint)));
+        sand = vmix(sand, clay, pan);
+    }
+    return vmul(sand, 1.0f + (vnoise(vmul(q, 9.0f)) - 0.5f) * 0.12f * detail);
+}
+
+/* dune_ripples: ground.wgsl:571-582; the surface-frame (x, z) gradient. */
+static __device__ __noinline__ v2 dune_ripples(sv p, sf wavelength, sf warp, sf amplitude) {
+    v2 wind = V2(sin_d(DUNE_WIND), cos_d(DUNE_WIND));
+    v2 side = V2(wind.y, -wind.x);
+    sf bend = warp * (vnoise(V(p.x / (9.0f * wavelength), p.z / (9.0f * wavelength), 1.0f)) +
+                         0.35f * vnoise(V(p.x / (2.5f * wavelength), p.z / (2.5f * wavelength), 7.0f)));
+    sf phase = v2dot(V2(p.x, p.z), wind) / wavelength + bend +
+                  0.4f * sin_d(v2dot(V2(p.x, p.z), side) / (3.0f * wavelength));
+    sf theta = TAU_F * phase;
+    sf slope = cos_d(theta + 0.65f * sin_d(theta)) * (1.0f + 0.65f * cos_d(theta));
+    sf patches = smoothstepf(0.25f, 0.6f, vnoise(V(p.x / (14.0f * wavelength), p.z / (14.0f * wavelength), 3.0f)));
+    sf k = slope * amplitude * TAU_F / wavelength * patches;
+    return V2(wind.x * k, wind.y * k);
+}
+
+/* dune_shading_normal: ground.wgsl:583-595 */
+static __device__ __noinline__ sv dune_shading_normal(const Scene &S, sv p, sf distance, sv normal) {
+    sf footprint = footprint_at(S, distance);
+    sv n = to_ground_s(S, normal);
+    sf gentle = 1.0f - smoothstepf(0.22f, 0.38f, 1.0f - n.y);
+    sv q = terrain_local(S, p);
+    sf dry = smoothstepf(DUNE_PAN_LEVEL + 0.4f, DUNE_PAN_LEVEL + 1.5f, q.y);
+    v2 gradient = V2(0.0f, 0.0f);
+    sf fine = 1.0f - smoothstepf(0.03f, 0.07f, footprint);
+    if (fine > 0.0f) {
+        v2 r = dune_ripples(p, 0.12f, 2.5f, 0.006f);
+        gradient = V2(gradient.x + r.x * fine, gradient.y + r.y * fine);
+    }
+    sf coarse = (1.0f - smoothstepf(0.15f, 0.4f, footprint)) * (1.0f - smoothstepf(9.0f, 16.0f, q.y));
+    if (coarse > 0.0f) {
+        v2 r = dune_ripples(vadds(p, 31.0f), 0.8f, 2.0f, 0.03f);
+        gradient = V2(gradient.x + r.x * coarse, gradient.y + r.y * coarse);
+    }
+    sf k = gentle * dry;
+    gradient = V2(gradient.x * k, gradient.y * k);
+    return vnormalize(vadd(normal, from_ground_s(S, V(-gradient.x, 0.0f, -gradient.y))));
+}
+
+}  // namespace style
+
 // Albedo-map extension: index of the nearest texel at surface-frame (x, z).
 __device__ __forceinline__ uint32_t map_texel(const TraceParams *P, float3 p) {
     const float u = (p.x / P->map_extent + 1.0f) * 0.5f * (float)P->map_width;
@@ -564,7 +848,7 @@ __device__ __forceinline__ uint32_t map_texel(const TraceParams *P, float3 p) {
     return (uint32_t)j * P->map_width + (uint32_t)i;
 }
 
-// landscape_albedo (ground.wgsl:597-632), themes 0-2, plus the map.
+// landscape_albedo (ground.wgsl:597-632), themes 0-3 and 5, plus the map.
 static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
@@ -578,6 +862,11 @@ static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t
         const uint32_t theme = S.s->g.ground_counts[2] & 255u;
         if (theme == 1u) return desert_floor(p, footprint, n);
         if (theme == 2u) return crater_floor(p, footprint, n);
+        if (theme == 3u || theme == 5u) {
+            const style::sv sp = style::V(p.x, p.y, p.z), sn = style::V(n.x, n.y, n.z);
+            return style::to_f3(theme == 3u ? style::alpine_floor(S, sp, distance, sn)
+                                            : style::dune_floor(S, sp, distance, sn));
+        }
         return forest_floor(p, footprint, n);
     }
     const float4 albedo = S.p->props[3u * (index - kLocalBase - 1u) + 2u];
@@ -594,11 +883,17 @@ static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t
     return mix3(stone, f3(0.11f, 0.145f, 0.037f), lichen * 0.65f);
 }
 
-// landscape_shading_normal (ground.wgsl:633-648), themes 0-2.
+// landscape_shading_normal (ground.wgsl:633-648), themes 0-3 and 5.
 static __device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     if (index != kLocalBase && index != kTerrainId) return normal;
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
+    const uint32_t theme = S.s->g.ground_counts[2] & 255u;
+    if (theme == 3u || theme == 5u) {
+        const style::sv sp = style::V(p.x, p.y, p.z), sn = style::V(normal.x, normal.y, normal.z);
+        return style::to_f3(theme == 5u ? style::dune_shading_normal(S, sp, distance, sn)
+                                        : style::alpine_shading_normal(S, sp, distance, sn));
+    }
     const float strength = 0.11f * (1.0f - smoothstepf(8.0f, 65.0f, distance));
     const float dx = vnoise((p + f3(0.025f, 0.0f, 0.0f)) * 6.0f) - vnoise((p - f3(0.025f, 0.0f, 0.0f)) * 6.0f);
     const float dz = vnoise((p + f3(0.0f, 0.0f, 0.025f)) * 6.0f) - vnoise((p - f3(0.0f, 0.0f, 0.025f)) * 6.0f);

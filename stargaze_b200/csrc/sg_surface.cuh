@@ -504,6 +504,16 @@ static __device__ __noinline__ sv style_albedo(const float4 *body, uint32_t styl
 }
 
 
+// terrain_shading (terrain.wgsl:142-150): on alpine ground a steep
+// triangle shades with its own flat face.
+__device__ __forceinline__ float3 alpine_face_shading(float3 smooth_normal, float3 a, float3 b, float3 c) {
+    const sv pa = V(a.x, a.y, a.z), pb = V(b.x, b.y, b.z), pc = V(c.x, c.y, c.z);
+    sv face = vnormalize(vcross(vsub(pb, pa), vsub(pc, pa)));
+    if (face.y < sf(0.0f)) face = V(-face.x, -face.y, -face.z);
+    const sv n = V(smooth_normal.x, smooth_normal.y, smooth_normal.z);
+    return to_f3(vnormalize(vmix(n, face, smoothstepf(0.25f, 0.5f, sf(1.0f) - face.y))));
+}
+
 }  // namespace style
 
 // surface_albedo's styled branch (pathtrace.wgsl:897-910): the body's ten

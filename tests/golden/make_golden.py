@@ -132,7 +132,12 @@ IMAGES = {
     "terrain_96x54": (None, 96, 54, 16, 2),
     "terrain_air_96x54": (None, 96, 54, 16, 2),
     "styles_96x32": (None, 96, 32, 16, 2),
+    "terrain_alpine_96x54": (None, 96, 54, 16, 2),
+    "terrain_dunes_96x54": (None, 96, 54, 16, 2),
 }
+
+# Landscape themes of the terrain images (ground_counts.z low byte).
+THEMES = {"alpine": 3, "dunes": 5}
 
 
 def image_workload(name):
@@ -144,6 +149,10 @@ def image_workload(name):
         wl, land = terrain_small(width=w, height=h)
         if "air" in name:
             with_air(wl.frame, 1)
+        for theme, code in THEMES.items():
+            if theme in name:
+                g = wl.frame.globals
+                g.ground_counts[2] = (g.ground_counts[2] & ~255) | code
         return wl, land
     return factory(width=w, height=h), None
 

@@ -32,7 +32,10 @@ def test_heightfield_compact_layout_4096():
     ka.heightfield_oracle(make, heights, T.pack_terrain(heights, cells), cells, rays=rays)
 
 
-def test_terrain_probe_matches_oracle_bit_exact():
+@pytest.mark.parametrize("theme", [0, 3], ids=["forest", "alpine"])
+def test_terrain_probe_matches_oracle_bit_exact(theme):
+    """Distances bit-exact; normals within 2e-6 (alpine ground mixes the
+    smooth normal with the triangle's flat face, terrain.wgsl:142-150)."""
     from oracle.binding import OracleTracer
 
     cells = 256
@@ -46,7 +49,9 @@ def test_terrain_probe_matches_oracle_bit_exact():
     results = []
     for tracer in (PathTracer((1, 1), ka.test_options()), OracleTracer((1, 1), ka.test_options())):
         tracer.upload_terrain(data, cells)
-        results.append(tracer.terrain_probe(ka.terrain_frame(6_371_000.0), o.astype(np.float32), d.astype(np.float32)))
+        f = ka.terrain_frame(6_371_000.0)
+        f.globals.ground_counts[2] = (f.globals.ground_counts[2] & ~255) | theme
+        results.append(tracer.terrain_probe(f, o.astype(np.float32), d.astype(np.float32)))
     cuda, cpu = results
     assert np.array_equal(cuda[:, 3], cpu[:, 3])  # distances bit-exact (and misses)
     hit = cpu[:, 3] < 1e29
