@@ -255,8 +255,11 @@ SG_API int sg_upload_ring_profile(sg_context *ctx, uint32_t slot, const float *t
  * `terrain::Terrain::data` vector (src/terrain.rs:781-838) for a grid of
  * `cells` cells per side (power of two, 2..SG_TERRAIN_MAX_CELLS):
  * (cells+1)^2 heights, then (cells <= 1024 only) x and z derivatives, then
- * (min, max) per quadtree node in breadth-first order; `n_floats` must be
- * exactly that length. The device appends the geometry cache of
+ * (min, max) per quadtree node in breadth-first order; `n_floats` is that
+ * length, or that length plus the basalt elevation atlas
+ * (`volcano::detail()`, src/volcano.rs:36-96), which the reference writes
+ * at DETAIL_OFFSET, right after the geometry cache, and which basalt ground
+ * (theme 4) shades from. The device appends the geometry cache of
  * cache_terrain_geometry (terrain.wgsl:242-285) on the next encode and
  * whenever the host radius (ground_up.w) changes. Frames with
  * ground_counts.y != 0 need an uploaded terrain. Uploading bumps the

@@ -28,6 +28,7 @@ class Tables(C.Structure):
         ("ring_bins", C.c_uint32 * abi.RING_TABLE_SLOTS),
         ("terrain", C.c_void_p),
         ("terrain_cells", C.c_uint32),
+        ("terrain_detail_floats", C.c_uint32),
         ("ground", C.c_void_p),
         ("n_ground", C.c_uint32),
         ("albedo_map", C.c_void_p),
@@ -125,6 +126,7 @@ class TableSet:
         self.version = 0
         self.terrain: np.ndarray | None = None
         self.terrain_cells = 0
+        self.terrain_detail = 0
         self.terrain_radius: float | None = None
         self.albedo: np.ndarray | None = None
         self.map_extent = 0.0
@@ -138,13 +140,19 @@ class TableSet:
         self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
         self.version += 1
 
-    def upload_terrain(self, data, cells: int) -> None:
+    def upload_terrain(self, data, cells: int, detail=None) -> None:
+        """The reference terrain layout; `detail`, the measured elevation
+        atlas of basalt ground, follows the vertex cache (volcano.rs)."""
         lib = load()
-        full = np.zeros(lib.oracle_terrain_floats(cells), dtype=np.float32)
+        n = lib.oracle_terrain_floats(cells)
+        extra = np.zeros(0, np.float32) if detail is None else np.asarray(detail, dtype=np.float32).ravel()
+        full = np.zeros(n + extra.size, dtype=np.float32)
         data = np.asarray(data, dtype=np.float32)
         full[: data.size] = data
+        full[n:] = extra
         self.terrain = full
         self.terrain_cells = cells
+        self.terrain_detail = int(extra.size)
         self.terrain_radius = None
         self.version += 1
 
@@ -183,6 +191,7 @@ class TableSet:
         if self.terrain is not None:
             t.terrain = self.terrain.ctypes.data
             t.terrain_cells = self.terrain_cells
+            t.terrain_detail_floats = self.terrain_detail
         if frame is not None and frame.ground:
             self._ground = (abi.Primitive * len(frame.ground))(*frame.ground)
             t.ground = C.cast(self._ground, C.c_void_p)
@@ -287,8 +296,8 @@ class OracleTracer:
     def upload_ring_profile(self, slot: int, tau) -> None:
         self.tables.upload(slot, tau)
 
-    def upload_terrain(self, data, cells: int) -> None:
-        self.tables.upload_terrain(data, cells)
+    def upload_terrain(self, data, cells: int, detail=None) -> None:
+        self.tables.upload_terrain(data, cells, detail)
 
     def upload_albedo_map(self, albedo, extent_m: float) -> None:
         self.tables.upload_albedo_map(albedo, extent_m)

@@ -1873,6 +1873,136 @@ static v3 dune_shading_normal(const scene *S, v3 p, float distance, v3 normal) {
     return vnormalize(vadd(normal, from_ground(S, V(-gradient.x, 0.0f, -gradient.y))));
 }
 
+/* ---------------------------------------------------------------- */
+/* Theme 4 (basalt): basalt_floor (ground.wgsl:463-477) and the      */
+/* shading normals from the measured elevation atlas that follows the */
+/* terrain's vertex cache (volcano.wgsl). Reads past the uploaded     */
+/* atlas return 0 (the reference's buffer always holds one).          */
+/* ---------------------------------------------------------------- */
+static inline uint32_t u32_sat(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967040.0f) return 0xffffffffu;
+    return (uint32_t)x;
+}
+static inline int32_t i32_sat(float x) {
+    if (!(x > -2147483520.0f)) return x != x ? 0 : (int32_t)0x80000000u;
+    if (x >= 2147483520.0f) return 0x7fffffff;
+    return (int32_t)x;
+}
+static inline float fract_(float x) { return x - floorf(x); }
+static inline float log2_d(float x) { return (float)log2((double)x); }
+static float volcano_data(const scene *S, uint32_t i) {
+    if (!S->t || !S->t->terrain || i >= S->t->terrain_detail_floats) return 0.0f;
+    return S->t->terrain[oracle_terrain_floats(t_cells(S)) + i];
+}
+typedef struct { float x, y, z, w; } v4;
+static v4 volcano_record(const scene *S, uint32_t i) {
+    v4 r = {volcano_data(S, i), volcano_data(S, i + 1u), volcano_data(S, i + 2u), volcano_data(S, i + 3u)};
+    return r;
+}
+static inline uint32_t clamp_index(int32_t v, uint32_t width) {
+    int32_t hi = (int32_t)width - 1;
+    return (uint32_t)(v < 0 ? 0 : (v > hi ? hi : v));
+}
+static float volcano_bilinear(const scene *S, uint32_t offset, uint32_t width, v2 uv) {
+    v2 pixel = V2(uv.x * (float)width - 0.5f, uv.y * (float)width - 0.5f);
+    int32_t lx = i32_sat(floorf(pixel.x)), ly = i32_sat(floorf(pixel.y));
+    uint32_t ax = clamp_index(lx, width), ay = clamp_index(ly, width);
+    uint32_t bx = clamp_index(lx == 0x7fffffff ? lx : lx + 1, width), by = clamp_index(ly == 0x7fffffff ? ly : ly + 1, width);
+    v2 f = V2(fract_(pixel.x), fract_(pixel.y));
+    return mixf(mixf(volcano_data(S, offset + ay * width + ax), volcano_data(S, offset + ay * width + bx), f.x),
+                mixf(volcano_data(S, offset + by * width + ax), volcano_data(S, offset + by * width + bx), f.x), f.y);
+}
+static float volcano_map(const scene *S, uint32_t map, v2 p, float footprint) {
+    v4 desc = volcano_record(S, map * 4u);
+    v2 local = V2(p.x, p.y - desc.w);
+    float reach = 0.5f * (desc.y - 1.0f) * desc.z;
+    if (fabsf(local.x) > reach || fabsf(local.y) > reach) return 0.0f;
+    v2 uv = V2((local.x / desc.z + 0.5f * desc.y) / desc.y, (local.y / desc.z + 0.5f * desc.y) / desc.y);
+    float lod = maxf_(log2_d(maxf_(footprint / desc.z, 1.0f)), 0.0f);
+    uint32_t offset = u32_sat(desc.x), width = u32_sat(desc.y);
+    uint32_t levels = u32_sat(lod);
+    for (uint32_t level = 0; level < levels && width > 1u; level++) {
+        offset += width * width;
+        width = (width + 1u) / 2u;
+    }
+    float a = volcano_bilinear(S, offset, width, uv);
+    if (width == 1u) return a;
+    float b = volcano_bilinear(S, offset + width * width, (width + 1u) / 2u, uv);
+    return mixf(a, b, fract_(lod));
+}
+static float volcano_fine_weight(const scene *S, v2 p) {
+    v4 desc = volcano_record(S, 4u);
+    v2 local = V2(p.x, p.y - desc.w);
+    float reach = 0.5f * (desc.y - 1.0f) * desc.z;
+    return 1.0f - smoothstepf(reach - 72.0f, reach, maxf_(fabsf(local.x), fabsf(local.y)));
+}
+static float volcano_height(const scene *S, uint32_t map, v2 p, float footprint) {
+    float coarse = volcano_map(S, map, p, footprint);
+    if (map != 0u) return coarse;
+    float weight = volcano_fine_weight(S, p);
+    if (weight <= 0.0f) return coarse;
+    return mixf(coarse, volcano_map(S, 1u, p, footprint), weight);
+}
+/* volcano_normal: volcano.wgsl:49-88 (surface-frame normals). */
+static v3 volcano_normal(const scene *S, v3 p, float distance, v3 fallback) {
+    float scale = terrain_scale(S);
+    v2 point = V2(p.x / scale, p.z / scale);
+    float footprint = footprint_at(S, distance) / scale;
+    float best = 1.0f;
+    uint32_t chosen = 0u;
+    v2 local = V2(0.0f, 0.0f);
+    v4 transform = {0.0f, 0.0f, 1.0f, 0.0f};
+    float site_scale = 1.0f;
+    for (uint32_t site = 0; site < 9u; site++) {
+        v4 frame = volcano_record(S, 16u + site * 8u);
+        v4 info = volcano_record(S, 20u + site * 8u);
+        v2 relative = V2((point.x - frame.x) / info.x, (point.y - frame.y) / info.x);
+        v2 q = V2(frame.z * relative.x - frame.w * relative.y, frame.w * relative.x + frame.z * relative.y);
+        float height = volcano_height(S, u32_sat(info.y), q, footprint / info.x) * info.x;
+        if (height > best) {
+            best = height;
+            chosen = u32_sat(info.y);
+            local = q;
+            transform = frame;
+            site_scale = info.x;
+        }
+    }
+    if (best <= 1.0f) return fallback;
+    float spacing = volcano_record(S, chosen * 4u).z;
+    if (chosen == 0u) spacing = mixf(spacing, 1.0f, volcano_fine_weight(S, local));
+    float delta = maxf_(spacing, footprint / site_scale * 0.5f);
+    float fp = footprint / site_scale;
+    float dx = (volcano_height(S, chosen, V2(local.x + delta, local.y), fp) -
+                volcano_height(S, chosen, V2(local.x - delta, local.y), fp)) / (2.0f * delta);
+    float dz = (volcano_height(S, chosen, V2(local.x, local.y + delta), fp) -
+                volcano_height(S, chosen, V2(local.x, local.y - delta), fp)) / (2.0f * delta);
+    v2 gradient = V2(transform.z * dx + transform.w * dz, -transform.w * dx + transform.z * dz);
+    float radius = S->s->g.ground_up[3];
+    float k = sqrtf(maxf_(radius * radius - (p.x * p.x + p.z * p.z), 1.0f));
+    v2 curvature = V2(p.x / k, p.z / k);
+    v3 n = vnormalize(V(-gradient.x + curvature.x, 1.0f, -gradient.y + curvature.y));
+    if (vdot(n, fallback) < 0.2f) return vnormalize(vmix(fallback, n, 0.7f));
+    return n;
+}
+
+/* basalt_floor: ground.wgsl:463-477 */
+static v3 basalt_floor(const scene *S, v3 p, float distance, v3 normal) {
+    float footprint = footprint_at(S, distance);
+    float broad = fbm(vadd(vmul(p, 0.006f), V(5.0f, 9.0f, 2.0f)), 4);
+    float weather = fbm(vadd(vmul(p, 0.017f), V(23.0f, 7.0f, 11.0f)), 3);
+    float middle = mixf(fbm(vmul(p, 0.08f), 3), 0.5f, smoothstepf(1.0f, 12.0f, footprint));
+    v3 ash = vmix(V(0.065f, 0.060f, 0.052f), V(0.14f, 0.12f, 0.095f), broad);
+    v3 rock = vmix(V(0.028f, 0.030f, 0.031f), V(0.07f, 0.064f, 0.054f), middle);
+    rock = vmix(rock, V(0.16f, 0.073f, 0.037f), smoothstepf(0.48f, 0.68f, weather) * 0.45f);
+    float slope = 1.0f - maxf_(normal.y, 0.0f);
+    float loose = 1.0f - smoothstepf(0.14f, 0.43f, slope + 0.12f * (weather - 0.5f));
+    v3 color = vmix(rock, ash, loose);
+    color = vmul(color, 0.86f + 0.28f * middle);
+    float grain = vnoise(vmul(p, 5.0f));
+    return vmul(color, 1.0f + (grain - 0.5f) * 0.28f * (1.0f - smoothstepf(0.025f, 0.2f, footprint)));
+}
+
 static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
     v3 p = landscape_point(S, ray, hit);
     float distance = hit.distance * METRES_PER_AU;
@@ -1883,6 +2013,7 @@ static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
             case 1u: return desert_floor(S, p, distance, n);
             case 2u: return crater_floor(S, p, distance, n);
             case 3u: return alpine_floor(S, p, distance, n);
+            case 4u: return basalt_floor(S, p, distance, n);
             case 5u: return dune_floor(S, p, distance, n);
             default: return forest_floor(S, p, distance, n);
         }
@@ -1914,6 +2045,8 @@ static v3 landscape_shading_normal(const scene *S, ray_t ray, hit_t hit) {
     if (hit.index != LOCAL_BASE && hit.index != TERRAIN_ID) return hit.normal;
     v3 p = landscape_point(S, ray, hit);
     float distance = hit.distance * METRES_PER_AU;
+    if (ground_theme(S) == 4u && hit.index == TERRAIN_ID)
+        return from_ground(S, volcano_normal(S, p, distance, to_ground(S, hit.normal)));
     if (ground_theme(S) == 5u) return dune_shading_normal(S, p, distance, hit.normal);
     if (ground_theme(S) == 3u) return alpine_shading_normal(S, p, distance, hit.normal);
     float strength = 0.11f * (1.0f - smoothstepf(8.0f, 65.0f, distance));
@@ -2800,14 +2933,14 @@ static v3 camera_direction(const scene *S, uint32_t x, uint32_t y, uint32_t *rng
     return vnormalize(V(ndc_x * tangent * S->s->g.viewport[3], ndc_y * tangent, -1.0f));
 }
 
-/* Frames the restatement covers: landscape themes 0-3 and 5;
+/* Frames the restatement covers: landscape themes 0-5;
  * no vegetation primitives; terrain only with a terrain table. */
 static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
     if (!s) return SG_ERR_INVALID;
     if (s->counts[0] > SG_BODY_CAPACITY) return SG_ERR_CAPACITY;
     if (s->g.ground_north[3] != 0.0f) {
         uint32_t theme = s->g.ground_counts[2] & 255u;
-        if (theme == 4u || theme > 5u) return SG_ERR_INVALID;
+        if (theme > 5u) return SG_ERR_INVALID;
         if (s->g.ground_counts[1] != 0u && (!t || !t->terrain)) return SG_ERR_INVALID;
         if (s->g.ground_counts[0] > 0u && (!t || !t->ground || t->n_ground < s->g.ground_counts[0])) return SG_ERR_INVALID;
         for (uint32_t i = 0; t && t->ground && i < s->g.ground_counts[0]; i++)

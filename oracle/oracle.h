@@ -35,6 +35,9 @@ typedef struct oracle_tables {
      * oracle_cache_terrain. */
     const float *terrain;
     uint32_t terrain_cells;
+    /* Floats of the measured elevation atlas that follows the vertex cache
+     * (basalt ground, volcano.wgsl); 0 without one. */
+    uint32_t terrain_detail_floats;
     /* Landscape primitives of the frame (ground.wgsl:3-12). */
     const sg_primitive *ground;
     uint32_t n_ground;

@@ -73,6 +73,7 @@ struct sg_context {
     std::vector<float4> trig_host;
     float *terrain = nullptr;       // full layout incl. the geometry cache
     uint32_t terrain_cells = 0;
+    uint32_t terrain_detail = 0;            // floats of the basalt elevation atlas
     bool terrain_cached = false;
     float terrain_radius = 0.0f;    // host radius the cache was built for
     float *albedo_map = nullptr;
@@ -252,9 +253,8 @@ int validate_frame(sg_context *ctx, const sg_frame *frame) {
     if (host != 0.0f) {
         if (host != std::floor(host) || host < 1.0f || host > (float)frame->n_bodies)
             return fail(ctx, SG_ERR_INVALID, "ground_north.w must be 0 or a body index + 1");
-        const uint32_t theme = frame->globals->ground_counts[2] & 255u;
-        if (theme == 4u || theme > 5u)
-            return fail(ctx, SG_ERR_INVALID, "landscape theme 4 (basalt) and themes above 5 are not implemented");
+        if ((frame->globals->ground_counts[2] & 255u) > 5u)
+            return fail(ctx, SG_ERR_INVALID, "landscape themes above 5 do not exist");
         if (frame->globals->ground_counts[1] != 0u && !ctx->terrain)
             return fail(ctx, SG_ERR_STATE, "terrain is enabled but no terrain was uploaded");
         if (!(frame->globals->ground_up[3] > 0.0f))
@@ -392,6 +392,7 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.events = nullptr;
     p.terrain = ctx->terrain;
     p.terrain_cells = ctx->terrain_cells;
+    p.terrain_detail_floats = ctx->terrain_detail;
     p.props = reinterpret_cast<const float4 *>(ctx->props);
     p.prop_trig = ctx->prop_trig;
     p.n_props = s.g.ground_counts[0];
@@ -527,16 +528,25 @@ int sg_upload_terrain(sg_context *ctx, const float *data, size_t n_floats, uint3
         return fail(ctx, SG_ERR_INVALID, "cells must be a power of two in 2..4096");
     if (!data) return fail(ctx, SG_ERR_INVALID, "data is NULL");
     const size_t source = sg::terrain_source_floats(cells);
-    if (n_floats != source) return fail(ctx, SG_ERR_INVALID, "terrain data length does not match the grid");
+    // An optional tail after the source layout is the basalt elevation atlas
+    // (src/volcano.rs), stored where volcano.wgsl reads it: after the cache.
+    if (n_floats < source || n_floats - source > (size_t)UINT32_MAX)
+        return fail(ctx, SG_ERR_INVALID, "terrain data length does not match the grid");
+    const size_t detail = n_floats - source;
+    const size_t full = sg::terrain_floats(cells);
     DeviceGuard guard(ctx->device);
     cudaDeviceSynchronize();
     cudaFree(ctx->terrain);
     ctx->terrain = nullptr;
     ctx->terrain_cells = 0;
+    ctx->terrain_detail = 0;
     ctx->terrain_cached = false;
-    SG_CUDA(ctx, cudaMalloc(&ctx->terrain, sg::terrain_floats(cells) * sizeof(float)));
+    SG_CUDA(ctx, cudaMalloc(&ctx->terrain, (full + detail) * sizeof(float)));
     SG_CUDA(ctx, cudaMemcpy(ctx->terrain, data, source * sizeof(float), cudaMemcpyHostToDevice));
+    if (detail)
+        SG_CUDA(ctx, cudaMemcpy(ctx->terrain + full, data + source, detail * sizeof(float), cudaMemcpyHostToDevice));
     ctx->terrain_cells = cells;
+    ctx->terrain_detail = (uint32_t)detail;
     ctx->table_version += 1;
     return SG_OK;
 }

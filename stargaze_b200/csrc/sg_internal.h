@@ -30,6 +30,7 @@ struct TraceParams {
     // (center, extent, albedo) each, optional scalar albedo map.
     const float *terrain;
     uint32_t terrain_cells;
+    uint32_t terrain_detail_floats;  // basalt elevation atlas after the vertex cache
     const float4 *props;
     const float4 *prop_trig;  // 2 float4 per prop: (sin, cos) of x, y; z
     uint32_t n_props;

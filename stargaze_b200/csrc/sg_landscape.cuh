@@ -836,6 +836,140 @@ static __device__ __noinline__ sv dune_shading_normal(const Scene &S, sv p, sf d
     return vnormalize(vadd(normal, from_ground_s(S, V(-gradient.x, 0.0f, -gradient.y))));
 }
 
+// Theme 4 (basalt): the measured elevation atlas follows the terrain's
+// vertex cache; reads past the uploaded atlas return 0.
+__device__ __forceinline__ uint32_t u32_sat(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967040.0f) return 0xffffffffu;
+    return (uint32_t)x;
+}
+__device__ __forceinline__ int32_t i32_sat(float x) {
+    if (!(x > -2147483520.0f)) return x != x ? 0 : (int32_t)0x80000000u;
+    if (x >= 2147483520.0f) return 0x7fffffff;
+    return (int32_t)x;
+}
+__device__ __forceinline__ sf fract_(sf x) { return x - floorf(x); }
+__device__ __forceinline__ sf log2_d(sf x) { return sf((float)::log2((double)x.v)); }
+__device__ __forceinline__ sf volcano_data(const Scene &S, uint32_t i) {
+    if (!S.p->terrain || i >= S.p->terrain_detail_floats) return sf(0.0f);
+    const uint32_t cells = S.p->terrain_cells;
+    return sf(S.p->terrain[(size_t)t_vertex_cache(cells) + (size_t)t_vertices(cells) * t_vertex_stride(cells) + i]);
+}
+struct v4 {
+    sf x, y, z, w;
+};
+__device__ __forceinline__ v4 volcano_record(const Scene &S, uint32_t i) {
+    return v4{volcano_data(S, i), volcano_data(S, i + 1u), volcano_data(S, i + 2u), volcano_data(S, i + 3u)};
+}
+/* ---------------------------------------------------------------- */
+/* Theme 4 (basalt): basalt_floor (ground.wgsl:463-477) and the      */
+/* shading normals from the measured elevation atlas that follows the */
+/* terrain's vertex cache (volcano.wgsl). Reads past the uploaded     */
+/* atlas return 0 (the reference's buffer always holds one).          */
+/* ---------------------------------------------------------------- */
+__device__ __forceinline__ uint32_t clamp_index(int32_t v, uint32_t width) {
+    int32_t hi = (int32_t)width - 1;
+    return (uint32_t)(v < 0 ? 0 : (v > hi ? hi : v));
+}
+static __device__ __noinline__ sf volcano_bilinear(const Scene &S, uint32_t offset, uint32_t width, v2 uv) {
+    v2 pixel = V2(uv.x * (float)width - 0.5f, uv.y * (float)width - 0.5f);
+    int32_t lx = i32_sat(floorf(pixel.x).v), ly = i32_sat(floorf(pixel.y).v);
+    uint32_t ax = clamp_index(lx, width), ay = clamp_index(ly, width);
+    uint32_t bx = clamp_index(lx == 0x7fffffff ? lx : lx + 1, width), by = clamp_index(ly == 0x7fffffff ? ly : ly + 1, width);
+    v2 f = V2(fract_(pixel.x), fract_(pixel.y));
+    return mixf(mixf(volcano_data(S, offset + ay * width + ax), volcano_data(S, offset + ay * width + bx), f.x),
+                mixf(volcano_data(S, offset + by * width + ax), volcano_data(S, offset + by * width + bx), f.x), f.y);
+}
+static __device__ __noinline__ sf volcano_map(const Scene &S, uint32_t map, v2 p, sf footprint) {
+    v4 desc = volcano_record(S, map * 4u);
+    v2 local = V2(p.x, p.y - desc.w);
+    sf reach = 0.5f * (desc.y - 1.0f) * desc.z;
+    if (fabsf(local.x) > reach || fabsf(local.y) > reach) return 0.0f;
+    v2 uv = V2((local.x / desc.z + 0.5f * desc.y) / desc.y, (local.y / desc.z + 0.5f * desc.y) / desc.y);
+    sf lod = maxf_(log2_d(maxf_(footprint / desc.z, 1.0f)), 0.0f);
+    uint32_t offset = u32_sat(desc.x.v), width = u32_sat(desc.y.v);
+    uint32_t levels = u32_sat(lod.v);
+    for (uint32_t level = 0; level < levels && width > 1u; level++) {
+        offset += width * width;
+        width = (width + 1u) / 2u;
+    }
+    sf a = volcano_bilinear(S, offset, width, uv);
+    if (width == 1u) return a;
+    sf b = volcano_bilinear(S, offset + width * width, (width + 1u) / 2u, uv);
+    return mixf(a, b, fract_(lod));
+}
+static __device__ __noinline__ sf volcano_fine_weight(const Scene &S, v2 p) {
+    v4 desc = volcano_record(S, 4u);
+    v2 local = V2(p.x, p.y - desc.w);
+    sf reach = 0.5f * (desc.y - 1.0f) * desc.z;
+    return 1.0f - smoothstepf(reach - 72.0f, reach, maxf_(fabsf(local.x), fabsf(local.y)));
+}
+static __device__ __noinline__ sf volcano_height(const Scene &S, uint32_t map, v2 p, sf footprint) {
+    sf coarse = volcano_map(S, map, p, footprint);
+    if (map != 0u) return coarse;
+    sf weight = volcano_fine_weight(S, p);
+    if (weight <= 0.0f) return coarse;
+    return mixf(coarse, volcano_map(S, 1u, p, footprint), weight);
+}
+/* volcano_normal: volcano.wgsl:49-88 (surface-frame normals). */
+static __device__ __noinline__ sv volcano_normal(const Scene &S, sv p, sf distance, sv fallback) {
+    sf scale = terrain_scale(S);
+    v2 point = V2(p.x / scale, p.z / scale);
+    sf footprint = footprint_at(S, distance) / scale;
+    sf best = 1.0f;
+    uint32_t chosen = 0u;
+    v2 local = V2(0.0f, 0.0f);
+    v4 transform = {0.0f, 0.0f, 1.0f, 0.0f};
+    sf site_scale = 1.0f;
+    for (uint32_t site = 0; site < 9u; site++) {
+        v4 frame = volcano_record(S, 16u + site * 8u);
+        v4 info = volcano_record(S, 20u + site * 8u);
+        v2 relative = V2((point.x - frame.x) / info.x, (point.y - frame.y) / info.x);
+        v2 q = V2(frame.z * relative.x - frame.w * relative.y, frame.w * relative.x + frame.z * relative.y);
+        sf height = volcano_height(S, u32_sat(info.y.v), q, footprint / info.x) * info.x;
+        if (height > best) {
+            best = height;
+            chosen = u32_sat(info.y.v);
+            local = q;
+            transform = frame;
+            site_scale = info.x;
+        }
+    }
+    if (best <= 1.0f) return fallback;
+    sf spacing = volcano_record(S, chosen * 4u).z;
+    if (chosen == 0u) spacing = mixf(spacing, 1.0f, volcano_fine_weight(S, local));
+    sf delta = maxf_(spacing, footprint / site_scale * 0.5f);
+    sf fp = footprint / site_scale;
+    sf dx = (volcano_height(S, chosen, V2(local.x + delta, local.y), fp) -
+                volcano_height(S, chosen, V2(local.x - delta, local.y), fp)) / (2.0f * delta);
+    sf dz = (volcano_height(S, chosen, V2(local.x, local.y + delta), fp) -
+                volcano_height(S, chosen, V2(local.x, local.y - delta), fp)) / (2.0f * delta);
+    v2 gradient = V2(transform.z * dx + transform.w * dz, -transform.w * dx + transform.z * dz);
+    sf radius = S.s->g.ground_up[3];
+    sf k = sqrtf(maxf_(radius * radius - (p.x * p.x + p.z * p.z), 1.0f));
+    v2 curvature = V2(p.x / k, p.z / k);
+    sv n = vnormalize(V(-gradient.x + curvature.x, 1.0f, -gradient.y + curvature.y));
+    if (vdot(n, fallback) < 0.2f) return vnormalize(vmix(fallback, n, 0.7f));
+    return n;
+}
+
+/* basalt_floor: ground.wgsl:463-477 */
+static __device__ __noinline__ sv basalt_floor(const Scene &S, sv p, sf distance, sv normal) {
+    sf footprint = footprint_at(S, distance);
+    sf broad = fbm(vadd(vmul(p, 0.006f), V(5.0f, 9.0f, 2.0f)), 4);
+    sf weather = fbm(vadd(vmul(p, 0.017f), V(23.0f, 7.0f, 11.0f)), 3);
+    sf middle = mixf(fbm(vmul(p, 0.08f), 3), 0.5f, smoothstepf(1.0f, 12.0f, footprint));
+    sv ash = vmix(V(0.065f, 0.060f, 0.052f), V(0.14f, 0.12f, 0.095f), broad);
+    sv rock = vmix(V(0.028f, 0.030f, 0.031f), V(0.07f, 0.064f, 0.054f), middle);
+    rock = vmix(rock, V(0.16f, 0.073f, 0.037f), smoothstepf(0.48f, 0.68f, weather) * 0.45f);
+    sf slope = 1.0f - maxf_(normal.y, 0.0f);
+    sf loose = 1.0f - smoothstepf(0.14f, 0.43f, slope + 0.12f * (weather - 0.5f));
+    sv color = vmix(rock, ash, loose);
+    color = vmul(color, 0.86f + 0.28f * middle);
+    sf grain = vnoise(vmul(p, 5.0f));
+    return vmul(color, 1.0f + (grain - 0.5f) * 0.28f * (1.0f - smoothstepf(0.025f, 0.2f, footprint)));
+}
+
 }  // namespace style
 
 // Albedo-map extension: index of the nearest texel at surface-frame (x, z).
@@ -848,7 +982,7 @@ __device__ __forceinline__ uint32_t map_texel(const TraceParams *P, float3 p) {
     return (uint32_t)j * P->map_width + (uint32_t)i;
 }
 
-// landscape_albedo (ground.wgsl:597-632), themes 0-3 and 5, plus the map.
+// landscape_albedo (ground.wgsl:597-632), themes 0-5, plus the map.
 static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
@@ -862,10 +996,11 @@ static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t
         const uint32_t theme = S.s->g.ground_counts[2] & 255u;
         if (theme == 1u) return desert_floor(p, footprint, n);
         if (theme == 2u) return crater_floor(p, footprint, n);
-        if (theme == 3u || theme == 5u) {
+        if (theme >= 3u && theme <= 5u) {
             const style::sv sp = style::V(p.x, p.y, p.z), sn = style::V(n.x, n.y, n.z);
-            return style::to_f3(theme == 3u ? style::alpine_floor(S, sp, distance, sn)
-                                            : style::dune_floor(S, sp, distance, sn));
+            if (theme == 3u) return style::to_f3(style::alpine_floor(S, sp, distance, sn));
+            if (theme == 4u) return style::to_f3(style::basalt_floor(S, sp, distance, sn));
+            return style::to_f3(style::dune_floor(S, sp, distance, sn));
         }
         return forest_floor(p, footprint, n);
     }
@@ -883,12 +1018,18 @@ static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t
     return mix3(stone, f3(0.11f, 0.145f, 0.037f), lichen * 0.65f);
 }
 
-// landscape_shading_normal (ground.wgsl:633-648), themes 0-3 and 5.
+// landscape_shading_normal (ground.wgsl:633-648), themes 0-5.
 static __device__ __noinline__ float3 landscape_shading_normal(Scene S, Ray ray, float t, uint32_t index, float3 normal) {
     if (index != kLocalBase && index != kTerrainId) return normal;
     const float3 p = landscape_point(S, ray, t);
     const float distance = t * kMetresPerAu;
     const uint32_t theme = S.s->g.ground_counts[2] & 255u;
+    if (theme == 4u && index == kTerrainId) {
+        // The survey's elevations supply the detail (volcano.wgsl).
+        const float3 g = to_ground(S, normal);
+        const style::sv n = style::volcano_normal(S, style::V(p.x, p.y, p.z), distance, style::V(g.x, g.y, g.z));
+        return from_ground(S, style::to_f3(n));
+    }
     if (theme == 3u || theme == 5u) {
         const style::sv sp = style::V(p.x, p.y, p.z), sn = style::V(normal.x, normal.y, normal.z);
         return style::to_f3(theme == 5u ? style::dune_shading_normal(S, sp, distance, sn)

@@ -160,9 +160,13 @@ class PathTracer:
         t = np.ascontiguousarray(tau, dtype=np.float32)
         check(self._lib.sg_upload_ring_profile(self._ctx, slot, _ptr(t), t.size), self._ctx)
 
-    def upload_terrain(self, data, cells: int) -> None:
-        """`Terrain::data` for a grid of `cells` cells (see terrain.py)."""
-        d = np.ascontiguousarray(data, dtype=np.float32)
+    def upload_terrain(self, data, cells: int, detail=None) -> None:
+        """`Terrain::data` for a grid of `cells` cells (see terrain.py), and
+        optionally the basalt elevation atlas (terrain.volcano_atlas)."""
+        d = np.asarray(data, dtype=np.float32).ravel()
+        if detail is not None:
+            d = np.concatenate([d, np.asarray(detail, dtype=np.float32).ravel()])
+        d = np.ascontiguousarray(d)
         check(self._lib.sg_upload_terrain(self._ctx, _ptr(d), d.size, cells), self._ctx)
 
     def upload_albedo_map(self, albedo, extent_m: float) -> None:

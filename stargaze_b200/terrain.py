@@ -225,3 +225,42 @@ def build_prop_bvh(props: list[abi.Primitive], leaf_size: int = 4) -> list[abi.P
     if props:
         emit(list(range(len(props))))
     return out
+
+
+def elevation_pyramid(level: np.ndarray) -> np.ndarray:
+    """An area-averaged mip pyramid of a square elevation grid, odd edges
+    repeating their last sample (src/volcano.rs:73-93), levels concatenated
+    down to 1 x 1."""
+    level = np.asarray(level, np.float32)
+    width = level.shape[0]
+    out = [level.ravel()]
+    while width > 1:
+        nxt = (width + 1) // 2
+        i = np.arange(nxt)
+        x0, x1 = 2 * i, np.minimum(2 * i + 1, width - 1)
+        level = (np.float32(0.25) * (level[x0][:, x0] + level[x0][:, x1] + level[x1][:, x0] + level[x1][:, x1])).astype(np.float32)
+        out.append(level.ravel())
+        width = nxt
+    return np.concatenate(out)
+
+
+def volcano_atlas(maps, sites) -> np.ndarray:
+    """The measured-elevation atlas of basalt ground in the layout
+    `volcano.wgsl` reads (src/volcano.rs:36-96): four map descriptors
+    (offset, width, spacing, north offset), nine site records (x, z, cos and
+    sin of the site's turn; scale, map, 0, 0) — the first the identity on map
+    0 — then each map's pyramid. `maps`: four (elevations (w, w), spacing,
+    north offset); `sites`: up to eight (x, z, turn radians, scale, map)."""
+    header = np.zeros(4 * 4 + 9 * 8, np.float32)
+    header[16:24] = [0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0, 0.0]
+    for i, (x, z, turn, scale, m) in enumerate(sites):
+        header[24 + 8 * i:32 + 8 * i] = [x, z, np.cos(turn), np.sin(turn), scale, float(m), 0.0, 0.0]
+    parts = [header]
+    offset = header.size
+    for k, (grid, spacing, north) in enumerate(maps):
+        grid = np.asarray(grid, np.float32)
+        header[4 * k:4 * k + 4] = [float(offset), float(grid.shape[0]), spacing, north]
+        pyramid = elevation_pyramid(grid)
+        parts.append(pyramid)
+        offset += pyramid.size
+    return np.concatenate(parts).astype(np.float32)

@@ -139,6 +139,7 @@ class LandscapeData:
     cells: int
     albedo_map: np.ndarray | None = None
     map_extent: float = 0.0
+    detail: np.ndarray | None = None  # basalt elevation atlas (terrain.volcano_atlas)
 
 
 def terrain_1080p(width: int = 1920, height: int = 1080, spp: int = 128, cells: int = 4096,
@@ -225,7 +226,10 @@ def upload_workload(tracer, wl: Workload) -> None:
     for slot, tau in wl.ring_tables.items():
         tracer.upload_ring_profile(slot, tau)
     if wl.landscape is not None:
-        tracer.upload_terrain(wl.landscape.terrain, wl.landscape.cells)
+        if wl.landscape.detail is not None:
+            tracer.upload_terrain(wl.landscape.terrain, wl.landscape.cells, wl.landscape.detail)
+        else:
+            tracer.upload_terrain(wl.landscape.terrain, wl.landscape.cells)
         if wl.landscape.albedo_map is not None:
             tracer.upload_albedo_map(wl.landscape.albedo_map, wl.landscape.map_extent)
 

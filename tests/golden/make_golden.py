@@ -93,7 +93,7 @@ def make_tracer(f, tables, dims=(1, 1), land=None, **opts):
     for slot, tau in tables.items():
         t.upload_ring_profile(slot, tau)
     if land is not None:
-        t.upload_terrain(land.terrain, land.cells)
+        t.upload_terrain(land.terrain, land.cells, getattr(land, "detail", None))
     return t
 
 
@@ -134,10 +134,33 @@ IMAGES = {
     "styles_96x32": (None, 96, 32, 16, 2),
     "terrain_alpine_96x54": (None, 96, 54, 16, 2),
     "terrain_dunes_96x54": (None, 96, 54, 16, 2),
+    "terrain_basalt_96x54": (None, 96, 54, 16, 2),
 }
 
 # Landscape themes of the terrain images (ground_counts.z low byte).
-THEMES = {"alpine": 3, "dunes": 5}
+THEMES = {"alpine": 3, "basalt": 4, "dunes": 5}
+
+
+def synthetic_volcano_atlas():
+    """A basalt elevation atlas of smooth synthetic elevations in the layout
+    of src/volcano.rs (the reference's maps are surveys): a 640 m cone on map
+    0 around the observer, a 2 m-spaced summit map 250 m north, two more
+    islands on maps 2 and 3 placed by site records."""
+    from stargaze_b200.terrain import volcano_atlas
+
+    def grid(width, spacing, peak, radius, ripple):
+        c = (np.arange(width) - (width - 1) / 2.0) * spacing
+        x, z = np.meshgrid(c, c)
+        r = np.hypot(x, z)
+        h = peak * np.exp(-(r / radius) ** 2) + ripple * (1.0 + np.sin(x / 37.0) * np.cos(z / 53.0))
+        return np.maximum(h, 0.0).astype(np.float32)
+
+    maps = [(grid(65, 20.0, 300.0, 350.0, 6.0), 20.0, 0.0),
+            (grid(33, 2.0, 40.0, 20.0, 1.5), 2.0, 250.0),
+            (grid(49, 25.0, 200.0, 300.0, 4.0), 25.0, 0.0),
+            (grid(49, 25.0, 150.0, 250.0, 3.0), 25.0, 0.0)]
+    sites = [(2500.0, 1800.0, 0.6, 1.2, 2), (-3000.0, 900.0, -0.4, 0.9, 3)]
+    return volcano_atlas(maps, sites)
 
 
 def image_workload(name):
@@ -153,6 +176,8 @@ def image_workload(name):
             if theme in name:
                 g = wl.frame.globals
                 g.ground_counts[2] = (g.ground_counts[2] & ~255) | code
+        if "basalt" in name:
+            land.detail = synthetic_volcano_atlas()
         return wl, land
     return factory(width=w, height=h), None
 

@@ -22,7 +22,7 @@ def cuda_tracer(tables, dims=(1, 1), land=None, **opts):
     for slot, tau in tables.items():
         t.upload_ring_profile(slot, tau)
     if land is not None:
-        t.upload_terrain(land.terrain, land.cells)
+        t.upload_terrain(land.terrain, land.cells, getattr(land, "detail", None))
     return t
 
 
