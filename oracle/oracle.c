@@ -1415,8 +1415,104 @@ static float landscape_top(const scene *S) {
     return top;
 }
 
-/* landscape_query: ground.wgsl:123-242 (vegetation kinds > 2.5 are not
- * restated; frames carrying them are rejected). */
+/* ---------------------------------------------------------------- */
+/* Vegetation primitives (kinds 3 conifer, 4 grass, 5 trunk):        */
+/* forest.wgsl:56-136, in the primitive's frame. (normal, distance), */
+/* distance 1e30 on a miss. Strict f32, correctly rounded            */
+/* transcendentals.                                                  */
+/* ---------------------------------------------------------------- */
+typedef struct { v3 n; float t; } veg_hit;
+static veg_hit trunk_hit(v3 p, v3 d, v3 e) {
+    v3 o = V(p.x / e.x, p.y / e.y, p.z / e.z);
+    v3 v = V(d.x / e.x, d.y / e.y, d.z / e.z);
+    veg_hit result = {V(0.0f, 0.0f, 0.0f), 1.0e30f};
+    float a = v.x * v.x + v.z * v.z;
+    float b = o.x * v.x + o.z * v.z;
+    float c = o.x * o.x + o.z * o.z - 1.0f;
+    float disc = b * b - a * c;
+    if (a > 1.0e-15f && disc >= 0.0f) {
+        for (uint32_t side = 0; side < 2u; side++) {
+            float t = (-b + (side == 1u ? sqrtf(disc) : -sqrtf(disc))) / a;
+            v3 q = vadd(o, vmul(v, t));
+            if (t > 0.001f && t < result.t && fabsf(q.y) <= 1.0f) {
+                result.n = vnormalize(V(q.x / e.x, 0.0f / e.y, q.z / e.z));
+                result.t = t;
+            }
+        }
+    }
+    if (fabsf(v.y) > 1.0e-15f) {
+        for (uint32_t side = 0; side < 2u; side++) {
+            float sign_y = side == 1u ? 1.0f : -1.0f;
+            float t = (sign_y - o.y) / v.y;
+            v3 q = vadd(o, vmul(v, t));
+            if (t > 0.001f && t < result.t && q.x * q.x + q.z * q.z <= 1.0f) {
+                result.n = V(0.0f, sign_y, 0.0f);
+                result.t = t;
+            }
+        }
+    }
+    return result;
+}
+static veg_hit conifer_hit(v3 p, v3 d, v3 e) {
+    veg_hit result = trunk_hit(vadd(p, V(0.0f, e.y * 0.08f, 0.0f)), d, V(e.x * 0.065f, e.y * 0.92f, e.z * 0.065f));
+    v3 o = V(p.x / e.x, p.y / e.y, p.z / e.z);
+    v3 v = V(d.x / e.x, d.y / e.y, d.z / e.z);
+    for (uint32_t tier = 0; tier < 6u; tier++) {
+        float t = (float)tier;
+        float base = -0.6f + t * 0.27f;
+        float height = minf_(0.66f - t * 0.045f, 1.0f - base);
+        float radius = 0.94f - t * 0.148f;
+        float ox = sin_d(t * 4.1f) * 0.022f, oz = cos_d(t * 3.7f) * 0.022f;
+        v3 q = vsub(o, V(ox, base + height, oz));
+        float k = radius / height;
+        float a = v.x * v.x + v.z * v.z - k * k * v.y * v.y;
+        float b = q.x * v.x + q.z * v.z - k * k * q.y * v.y;
+        float c = q.x * q.x + q.z * q.z - k * k * q.y * q.y;
+        float disc = b * b - a * c;
+        if (fabsf(a) < 1.0e-12f || disc < 0.0f) continue;
+        for (uint32_t side = 0; side < 2u; side++) {
+            float distance = (-b + (side == 1u ? sqrtf(disc) : -sqrtf(disc))) / a;
+            v3 h = vadd(q, vmul(v, distance));
+            if (distance <= 0.001f || distance >= result.t || h.y > 0.0f || h.y < -height) continue;
+            float angle = atan2_d(h.z, h.x);
+            float skirt = -h.y / height;
+            float branches = 0.5f + 0.5f * sin_d(angle * (9.0f + t) + t * 3.7f);
+            float needle = vnoise(vadds(vmulv(vadd(p, vmul(d, distance)), V(9.0f, 17.0f, 9.0f)), t * 7.0f));
+            if (skirt > 0.76f + 0.19f * branches || (skirt > 0.4f && needle < 0.26f)) continue;
+            result.n = vnormalize(V(h.x / e.x, -k * k * h.y / e.y, h.z / e.z));
+            result.t = distance;
+        }
+    }
+    return result;
+}
+static veg_hit grass_hit(v3 p, v3 d, v3 e) {
+    veg_hit result = {V(0.0f, 0.0f, 0.0f), 1.0e30f};
+    for (uint32_t blade = 0; blade < 9u; blade++) {
+        float i = (float)blade;
+        float angle = i * 2.39996f;
+        v3 side = V(cos_d(angle), 0.0f, sin_d(angle));
+        v3 base = vsub(vmul(vmul(side, e.x), 0.15f), V(0.0f, e.y, 0.0f));
+        v3 tip = vadd(vmul(vmul(side, e.x), 0.6f + 0.3f * sin_d(i * 3.0f)),
+                      V(0.0f, e.y * (0.5f + 0.5f * cos_d(i * 1.3f)), 0.0f));
+        v3 width = vmul(V(-side.z, 0.0f, side.x), 0.035f);
+        v3 hit = t_triangle(p, d, vsub(base, width), vadd(base, width), tip);
+        if (hit.z < result.t) {
+            v3 normal = vnormalize(vcross(width, vsub(tip, base)));
+            if (vdot(normal, d) > 0.0f) normal = vneg(normal);
+            result.n = normal;
+            result.t = hit.z;
+        }
+    }
+    return result;
+}
+/* The vegetation branch of landscape_query (ground.wgsl:197-202). */
+static veg_hit vegetation_hit(float kind, v3 p, v3 d, v3 e) {
+    if (kind < 3.5f) return conifer_hit(p, d, e);
+    if (kind < 4.5f) return grass_hit(p, d, e);
+    return trunk_hit(p, d, e);
+}
+
+/* landscape_query: ground.wgsl:123-242 */
 static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusion) {
     hit_t closest = {limit, MISS, {0, 0, 0}};
     if (S->s->g.ground_north[3] == 0.0f) return closest;
@@ -1483,7 +1579,12 @@ static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusi
         float distance = 1.0e30f;
         v3 n = V(0, 0, 0);
         if (kind > 2.5f) {
-            continue; /* vegetation: rejected by check_frame */
+            float bn, bf_;
+            box_interval(p, v, e, &bn, &bf_);
+            if (bn > bf_ || bf_ <= 0.001f || bn / METRES_PER_AU > closest.distance) continue;
+            veg_hit vegetation = vegetation_hit(kind, p, v, e);
+            distance = vegetation.t;
+            n = vegetation.n;
         } else if (kind > 1.5f) {
             float bn, bf_;
             box_interval(p, v, e, &bn, &bf_);
@@ -2025,6 +2126,16 @@ static v3 landscape_albedo(const scene *S, ray_t ray, hit_t hit) {
     float middle = vnoise(vmul(p, 1.7f));
     float fine = mixf(vnoise(vmul(p, 12.0f)), 0.5f, smoothstepf(18.0f, 110.0f, distance));
     if (kind > 4.5f) return vmul(tint, 0.65f + 0.6f * middle);
+    if (kind > 2.5f) {
+        /* Conifers: bark on the lower trunk (ground.wgsl:618-625). */
+        v3 q = rotate_north(vsub(p, V(object->center[0], object->center[1], object->center[2])), -object->extent[3]);
+        q = V(q.x / object->extent[0], q.y / object->extent[1], q.z / object->extent[2]);
+        if (kind > 3.5f || (q.y < -0.35f && sqrtf(q.x * q.x + q.z * q.z) < 0.09f)) {
+            float bark = vnoise(vmulv(p, V(25.0f, 1.5f, 25.0f)));
+            return vmul(V(0.13f, 0.073f, 0.032f), 0.5f + 0.85f * bark);
+        }
+        return vmul(tint, 0.7f + 0.55f * middle + 0.2f * fine);
+    }
     float strata = sinf(p.y * 8.0f + 2.5f * middle);
     float lichen = smoothstepf(0.52f, 0.76f, middle) * maxf_(n.y, 0.0f);
     v3 stone = vmul(tint, 0.7f + 0.45f * fine + 0.07f * strata);
@@ -2933,8 +3044,8 @@ static v3 camera_direction(const scene *S, uint32_t x, uint32_t y, uint32_t *rng
     return vnormalize(V(ndc_x * tangent * S->s->g.viewport[3], ndc_y * tangent, -1.0f));
 }
 
-/* Frames the restatement covers: landscape themes 0-5;
- * no vegetation primitives; terrain only with a terrain table. */
+/* Frames the restatement covers: landscape themes 0-5; terrain only with
+ * a terrain table. */
 static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
     if (!s) return SG_ERR_INVALID;
     if (s->counts[0] > SG_BODY_CAPACITY) return SG_ERR_CAPACITY;
@@ -2943,8 +3054,6 @@ static int check_frame_t(const sg_settings *s, const oracle_tables *t) {
         if (theme > 5u) return SG_ERR_INVALID;
         if (s->g.ground_counts[1] != 0u && (!t || !t->terrain)) return SG_ERR_INVALID;
         if (s->g.ground_counts[0] > 0u && (!t || !t->ground || t->n_ground < s->g.ground_counts[0])) return SG_ERR_INVALID;
-        for (uint32_t i = 0; t && t->ground && i < s->g.ground_counts[0]; i++)
-            if (t->ground[i].center[3] > 2.5f) return SG_ERR_INVALID;
     }
     return SG_OK;
 }

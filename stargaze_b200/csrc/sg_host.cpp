@@ -261,8 +261,6 @@ int validate_frame(sg_context *ctx, const sg_frame *frame) {
             return fail(ctx, SG_ERR_INVALID, "ground_up.w (host radius in metres) must be positive");
         for (uint32_t i = 0; i < frame->n_ground; ++i) {
             const float kind = frame->ground[i].center[3];
-            if (kind > 2.5f)
-                return fail(ctx, SG_ERR_INVALID, "vegetation primitives (kind > 2.5) are not implemented");
             if (kind < 0.0f && (kind != std::floor(kind) || (double)i - (double)kind >= (double)frame->n_ground + 1.0))
                 return fail(ctx, SG_ERR_INVALID, "a group marker skips past the end of the primitive list");
         }

@@ -367,6 +367,17 @@ static __device__ __noinline__ LandHit host_sphere_fp64(Scene S, Ray ray, float 
 
 // landscape_query (ground.wgsl:123-242). Vegetation kinds (> 2.5) are
 // rejected on the host and never reach the device.
+// A rock (kinds 2, 2.25) or vegetation (3 conifer, 4 grass, 5 trunk;
+// forest.wgsl:56-136): one out-of-line call site in the primitive loop.
+static __device__ __noinline__ float4 solid_hit(float kind, float3 p, float3 v, float3 e) {
+    if (kind > 2.5f) {
+        const style::veg_hit g =
+            style::vegetation_hit(kind, style::V(p.x, p.y, p.z), style::V(v.x, v.y, v.z), style::V(e.x, e.y, e.z));
+        return make_float4(g.n.x.v, g.n.y.v, g.n.z.v, g.t.v);
+    }
+    return rock_hit(p, v, e);
+}
+
 template <bool C, bool L, bool F>
 static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion) {
     LandHit closest{limit, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
@@ -450,11 +461,12 @@ static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K,
         float distance = 1.0e30f;
         float3 n = f3(0.0f, 0.0f, 0.0f);
         if (kind > 1.5f) {
+            // Rocks and vegetation, inside their bounding boxes.
             const float2 bounds = box_interval(p, v, e);
             if (bounds.x > bounds.y || bounds.y <= 0.001f || __fdiv_rn(bounds.x, kMetresPerAu) > closest.t) continue;
-            const float4 rock = rock_hit(p, v, e);
-            distance = rock.w;
-            n = xyz(rock);
+            const float4 solid = solid_hit(kind, p, v, e);
+            distance = solid.w;
+            n = xyz(solid);
         } else if (kind > 0.5f) {
             const float3 sp = div3_rn(p, e), sd = div3_rn(v, e);
             const float aa = dot_rn(sd, sd), bb = dot_rn(sp, sd), cc = __fsub_rn(dot_rn(sp, sp), 1.0f);
@@ -1011,6 +1023,18 @@ static __device__ __noinline__ float3 landscape_albedo(Scene S, Ray ray, float t
     const float middle = vnoise(p * 1.7f);
     const float fine = mixf(vnoise(p * 12.0f), 0.5f, smoothstepf(18.0f, 110.0f, distance));
     if (kind > 4.5f) return tint * (0.65f + 0.6f * middle);
+    if (kind > 2.5f) {
+        // Conifers: bark on the lower trunk (ground.wgsl:618-625).
+        const uint32_t k = index - kLocalBase - 1u;
+        const float4 oc = S.p->props[3u * k], oe = S.p->props[3u * k + 1u];
+        const float4 t1 = S.p->prop_trig[2u * k + 1u];
+        const float3 q = div3_rn(rotate_north(sub_rn(p, xyz(oc)), -t1.x, t1.y), xyz(oe));
+        if (kind > 3.5f || (q.y < -0.35f && __fsqrt_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.z, q.z))) < 0.09f)) {
+            const float bark = vnoise(f3(__fmul_rn(p.x, 25.0f), __fmul_rn(p.y, 1.5f), __fmul_rn(p.z, 25.0f)));
+            return f3(0.13f, 0.073f, 0.032f) * (0.5f + 0.85f * bark);
+        }
+        return tint * (0.7f + 0.55f * middle + 0.2f * fine);
+    }
     const float strata = sinf(p.y * 8.0f + 2.5f * middle);
     const float lichen = smoothstepf(0.52f, 0.76f, middle) * fmaxf(n.y, 0.0f);
     const float3 stone = tint * (0.7f + 0.45f * fine + 0.07f * strata);

@@ -514,6 +514,123 @@ __device__ __forceinline__ float3 alpine_face_shading(float3 smooth_normal, floa
     return to_f3(vnormalize(vmix(n, face, smoothstepf(0.25f, 0.5f, sf(1.0f) - face.y))));
 }
 
+/* ---------------------------------------------------------------- */
+/* Vegetation primitives (kinds 3 conifer, 4 grass, 5 trunk):        */
+/* forest.wgsl:56-136, in the primitive's frame. (normal, distance), */
+/* distance 1e30 on a miss. Strict f32, correctly rounded            */
+/* transcendentals.                                                  */
+/* ---------------------------------------------------------------- */
+struct veg_hit {
+    sv n;
+    sf t;
+};
+// terrain_triangle (terrain.wgsl:102-116) in this arithmetic: (u, v, t).
+__device__ __forceinline__ sv tri_hit(sv o, sv d, sv a, sv b, sv c) {
+    const sv ab = vsub(b, a), ac = vsub(c, a);
+    const sv p = vcross(d, ac);
+    const sf determinant = vdot(ab, p);
+    if (fabsf(determinant) < sf(1.0e-12f)) return V(0.0f, 0.0f, 1.0e30f);
+    const sf inverse = sf(1.0f) / determinant;
+    const sv relative = vsub(o, a);
+    const sf u = vdot(relative, p) * inverse;
+    const sv q = vcross(relative, ab);
+    const sf v = vdot(d, q) * inverse;
+    const sf distance = vdot(ac, q) * inverse;
+    if (u < sf(-1.0e-6f) || v < sf(-1.0e-6f) || u + v > sf(1.000001f) || distance <= sf(0.001f))
+        return V(0.0f, 0.0f, 1.0e30f);
+    return V(u, v, distance);
+}
+__device__ __forceinline__ sv vneg(sv a) { return V(-a.x, -a.y, -a.z); }
+static __device__ __noinline__ veg_hit trunk_hit(sv p, sv d, sv e) {
+    sv o = V(p.x / e.x, p.y / e.y, p.z / e.z);
+    sv v = V(d.x / e.x, d.y / e.y, d.z / e.z);
+    veg_hit result{V(0.0f, 0.0f, 0.0f), sf(1.0e30f)};
+    sf a = v.x * v.x + v.z * v.z;
+    sf b = o.x * v.x + o.z * v.z;
+    sf c = o.x * o.x + o.z * o.z - 1.0f;
+    sf disc = b * b - a * c;
+    if (a > 1.0e-15f && disc >= 0.0f) {
+        for (uint32_t side = 0; side < 2u; side++) {
+            sf t = (-b + (side == 1u ? sqrtf(disc) : -sqrtf(disc))) / a;
+            sv q = vadd(o, vmul(v, t));
+            if (t > 0.001f && t < result.t && fabsf(q.y) <= 1.0f) {
+                result.n = vnormalize(V(q.x / e.x, 0.0f / e.y, q.z / e.z));
+                result.t = t;
+            }
+        }
+    }
+    if (fabsf(v.y) > 1.0e-15f) {
+        for (uint32_t side = 0; side < 2u; side++) {
+            sf sign_y = side == 1u ? 1.0f : -1.0f;
+            sf t = (sign_y - o.y) / v.y;
+            sv q = vadd(o, vmul(v, t));
+            if (t > 0.001f && t < result.t && q.x * q.x + q.z * q.z <= 1.0f) {
+                result.n = V(0.0f, sign_y, 0.0f);
+                result.t = t;
+            }
+        }
+    }
+    return result;
+}
+static __device__ __noinline__ veg_hit conifer_hit(sv p, sv d, sv e) {
+    veg_hit result = trunk_hit(vadd(p, V(0.0f, e.y * 0.08f, 0.0f)), d, V(e.x * 0.065f, e.y * 0.92f, e.z * 0.065f));
+    sv o = V(p.x / e.x, p.y / e.y, p.z / e.z);
+    sv v = V(d.x / e.x, d.y / e.y, d.z / e.z);
+    for (uint32_t tier = 0; tier < 6u; tier++) {
+        sf t = (float)tier;
+        sf base = -0.6f + t * 0.27f;
+        sf height = minf_(0.66f - t * 0.045f, 1.0f - base);
+        sf radius = 0.94f - t * 0.148f;
+        sf ox = sin_d(t * 4.1f) * 0.022f, oz = cos_d(t * 3.7f) * 0.022f;
+        sv q = vsub(o, V(ox, base + height, oz));
+        sf k = radius / height;
+        sf a = v.x * v.x + v.z * v.z - k * k * v.y * v.y;
+        sf b = q.x * v.x + q.z * v.z - k * k * q.y * v.y;
+        sf c = q.x * q.x + q.z * q.z - k * k * q.y * q.y;
+        sf disc = b * b - a * c;
+        if (fabsf(a) < 1.0e-12f || disc < 0.0f) continue;
+        for (uint32_t side = 0; side < 2u; side++) {
+            sf distance = (-b + (side == 1u ? sqrtf(disc) : -sqrtf(disc))) / a;
+            sv h = vadd(q, vmul(v, distance));
+            if (distance <= 0.001f || distance >= result.t || h.y > 0.0f || h.y < -height) continue;
+            sf angle = atan2_d(h.z, h.x);
+            sf skirt = -h.y / height;
+            sf branches = 0.5f + 0.5f * sin_d(angle * (9.0f + t) + t * 3.7f);
+            sf needle = vnoise(vadds(vmulv(vadd(p, vmul(d, distance)), V(9.0f, 17.0f, 9.0f)), t * 7.0f));
+            if (skirt > 0.76f + 0.19f * branches || (skirt > 0.4f && needle < 0.26f)) continue;
+            result.n = vnormalize(V(h.x / e.x, -k * k * h.y / e.y, h.z / e.z));
+            result.t = distance;
+        }
+    }
+    return result;
+}
+static __device__ __noinline__ veg_hit grass_hit(sv p, sv d, sv e) {
+    veg_hit result{V(0.0f, 0.0f, 0.0f), sf(1.0e30f)};
+    for (uint32_t blade = 0; blade < 9u; blade++) {
+        sf i = (float)blade;
+        sf angle = i * 2.39996f;
+        sv side = V(cos_d(angle), 0.0f, sin_d(angle));
+        sv base = vsub(vmul(vmul(side, e.x), 0.15f), V(0.0f, e.y, 0.0f));
+        sv tip = vadd(vmul(vmul(side, e.x), 0.6f + 0.3f * sin_d(i * 3.0f)),
+                      V(0.0f, e.y * (0.5f + 0.5f * cos_d(i * 1.3f)), 0.0f));
+        sv width = vmul(V(-side.z, 0.0f, side.x), 0.035f);
+        sv hit = tri_hit(p, d, vsub(base, width), vadd(base, width), tip);
+        if (hit.z < result.t) {
+            sv normal = vnormalize(vcross(width, vsub(tip, base)));
+            if (vdot(normal, d) > 0.0f) normal = vneg(normal);
+            result.n = normal;
+            result.t = hit.z;
+        }
+    }
+    return result;
+}
+/* The vegetation branch of landscape_query (ground.wgsl:197-202). */
+static __device__ __noinline__ veg_hit vegetation_hit(sf kind, sv p, sv d, sv e) {
+    if (kind < 3.5f) return conifer_hit(p, d, e);
+    if (kind < 4.5f) return grass_hit(p, d, e);
+    return trunk_hit(p, d, e);
+}
+
 }  // namespace style
 
 // surface_albedo's styled branch (pathtrace.wgsl:897-910): the body's ten

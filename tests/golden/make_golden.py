@@ -49,22 +49,37 @@ def terrain_small(width=96, height=54):
     return terrain_1080p(width=width, height=height, cells=256, rocks=200, foliage=500, prop_range=(10.0, 200.0))
 
 
+def vegetate(frame):
+    """Turn the terrain fixture's foliage ellipsoids into vegetation
+    primitives in turn (3 conifer, 4 grass, 5 trunk, 1 ellipsoid); each stays
+    inside its box, so the prop BVH's bounds still hold."""
+    kinds = [3.0, 4.0, 5.0, 1.0]
+    k = 0
+    for prim in frame.ground:
+        if prim.center[3] == 1.0:
+            prim.center[3] = kinds[k % 4]
+            k += 1
+    return frame
+
+
 def scenes():
     s = spheres_256()
     r = rings_1080p()
     t, _land = terrain_small()
+    v, _land = terrain_small()
     return {
         "transport": transport_scene(),
         "spheres_256": (s.frame, s.ring_tables),
         "rings_1080p": (r.frame, r.ring_tables),
         "shadow_ring": (ka.shadow_ring_scene(), {}),
         "terrain": (t.frame, {}),
+        "vegetation": (vegetate(v.frame), {}),
     }
 
 
 def landscape_of(name):
     """Terrain data a ray scene needs (None for scenes without terrain)."""
-    return terrain_small()[1] if name == "terrain" else None
+    return terrain_small()[1] if name in ("terrain", "vegetation") else None
 
 
 def visibility_rays(f, rays, seed):
@@ -135,6 +150,7 @@ IMAGES = {
     "terrain_alpine_96x54": (None, 96, 54, 16, 2),
     "terrain_dunes_96x54": (None, 96, 54, 16, 2),
     "terrain_basalt_96x54": (None, 96, 54, 16, 2),
+    "terrain_vegetation_96x54": (None, 96, 54, 16, 2),
 }
 
 # Landscape themes of the terrain images (ground_counts.z low byte).
@@ -178,6 +194,8 @@ def image_workload(name):
                 g.ground_counts[2] = (g.ground_counts[2] & ~255) | code
         if "basalt" in name:
             land.detail = synthetic_volcano_atlas()
+        if "vegetation" in name:
+            vegetate(wl.frame)
         return wl, land
     return factory(width=w, height=h), None
 
