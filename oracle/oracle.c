@@ -7,12 +7,16 @@
  * WGSL source; the file must be compiled with -ffp-contract=off and without
  * -ffast-math so that f32 + - * / sqrt round exactly as written.
  *
- * Scope: the airless integrator of pathtrace.wgsl (sample loop, spheres,
- * rings, stellar NEE with MIS, ringshine, point discs, Russian roulette,
- * running-mean accumulation) and rings.wgsl. The host atmosphere, catalogue
- * stars, Milky Way map, procedural surface styles 1-6 and the local
- * landscape are not restated: they are inert for the frames this oracle
- * accepts (atmo_params.w == 0, ground_north.w == 0).
+ * Scope: the integrator of pathtrace.wgsl (sample loop, spheres, rings,
+ * stellar NEE with MIS, ringshine, point discs, Russian roulette,
+ * running-mean accumulation) and rings.wgsl; the host atmosphere with its
+ * camera-air pass and surface sky cache; the catalogue and Milky Way
+ * backdrop; procedural surface styles 1-6; the local landscape of
+ * ground.wgsl, terrain.wgsl, volcano.wgsl and forest.wgsl (themes 0-5,
+ * props, vegetation); the guided ground sampler (src/guided_ground.rs).
+ * Where the WGSL hashes coordinates derived from transcendental functions
+ * (surface styles, themes 3-5, vegetation), those functions are evaluated
+ * in double and rounded to f32, as the CUDA path does.
  */
 #include "oracle.h"
 

@@ -9,12 +9,15 @@
  * Parity pin: the reference is Rust + WGSL executed by wgpu, which cannot be
  * built or run here (no Rust toolchain, no graphics stack). The restatement
  * is pinned against the reference's own analytic known-answer tests
- * (src/pathtracer_tests.rs, src/ring_tests.rs, src/ground_tests.rs), which
- * the test suite re-runs against this library.
+ * (src/pathtracer_tests.rs, src/ring_tests.rs, src/ground_tests.rs,
+ * src/planetshine_tests.rs), which the test suite re-runs against this
+ * library. Landscape themes 3-5 and vegetation have no such tests outside
+ * the reference's YAML scenes: their restatement is pinned by reading.
  *
  * Arithmetic is IEEE f32 compiled with -ffp-contract=off, so + - * / sqrt
  * follow the WGSL expression order exactly; transcendental functions come
- * from the C library.
+ * from the C library (in double, rounded to f32, where the WGSL hashes
+ * coordinates derived from them).
  */
 #ifndef STARGAZE_ORACLE_H
 #define STARGAZE_ORACLE_H
