@@ -90,8 +90,6 @@ extern "C" int sg_closest_hit_noalloc(int device, const sg_frame *frame, const s
     if (!frame || !frame->globals) return fail(SG_ERR_INVALID, "frame or frame->globals is NULL");
     if (frame->n_bodies > SG_BODY_CAPACITY) return fail(SG_ERR_CAPACITY, "too many scene bodies");
     if (frame->n_bodies && !frame->bodies) return fail(SG_ERR_INVALID, "frame->bodies is NULL");
-    if (frame->globals->atmo_params[3] >= 0.5f)
-        return fail(SG_ERR_INVALID, "the host atmosphere (atmo_params.w >= 0.5) is not implemented");
     if (frame->globals->ground_north[3] != 0.0f)
         return fail(SG_ERR_INVALID,
                     "frames with a local landscape need a context (terrain and primitives): use sg_closest_hit");
