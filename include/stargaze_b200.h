@@ -500,7 +500,11 @@ SG_API int sg_get_tape(const sg_context *ctx, sg_tape *tape);
  * wavefront integrator (the default) the replay runs in the same stages as
  * the forward, over a pool of up to 16 Mi paths (pool_paths of
  * sg_set_integrator when set) holding about 1.1 KB of device memory each,
- * allocated on first use; with the megakernel, one thread per pixel. */
+ * allocated on first use; with the megakernel, one thread per pixel.
+ * SG_ERR_STATE for frames whose radiance this adjoint does not
+ * differentiate: a sky backdrop (catalogue or panorama bound), host air
+ * (atmo_params.w >= 0.5) or a body with a procedural surface style
+ * (axis_x.w >= 0.5). */
 SG_API int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape,
                        const float *dl_dimage, int on_device, sg_gradients *grads,
                        void *stream);
