@@ -144,3 +144,31 @@ def test_guided_ground_is_unbiased():
 def test_textured_planets_light_night_air():
     r = ka.textured_planets_light_night_air(make)
     assert set(r) == set(ka.STYLES)
+
+
+def test_guided_ground_is_inert_without_air_or_reflectors():
+    """The guided sampler only acts at depth-0 local surfaces under air with
+    a reflecting body (src/guided_ground.rs:38-48): elsewhere it draws no
+    random numbers, so the images are identical."""
+    base = ka.moonlit_ground_frame()
+    cases = []
+    airless = base.copy()
+    airless.globals.atmo_params[3] = 0.0
+    cases.append(airless)
+    no_reflector = base.copy()
+    no_reflector.bodies[2].color[:] = [0.0, 0.0, 0.0]
+    cases.append(no_reflector)
+    for f in cases:
+        imgs = []
+        for guided in (False, True):
+            t = make((4, 4), ka.test_options(samples_per_frame=64, max_bounces=3))
+            t.set_guided_ground(guided)
+            imgs.append(ka.sample(t, f, 1))
+        assert np.array_equal(imgs[0], imgs[1])
+    # With air and a lit moon it does change the estimate's samples.
+    imgs = []
+    for guided in (False, True):
+        t = make((4, 4), ka.test_options(samples_per_frame=64, max_bounces=3))
+        t.set_guided_ground(guided)
+        imgs.append(ka.sample(t, base, 1))
+    assert not np.array_equal(imgs[0], imgs[1])
