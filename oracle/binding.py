@@ -93,6 +93,8 @@ def load() -> C.CDLL:
     lib.oracle_cache_terrain.restype = C.c_int
     lib.oracle_terrain_query.argtypes = [S, C.POINTER(Tables), P, P, C.c_float, C.c_int, P]
     lib.oracle_terrain_query.restype = C.c_int
+    lib.oracle_sky_cache.argtypes = [S, P, C.POINTER(Tables), P]
+    lib.oracle_sky_cache.restype = C.c_int
     lib.oracle_tangent.argtypes = [S, P, C.POINTER(Tables), C.POINTER(Direction), P, P, C.c_uint32, C.c_uint32,
                                    C.c_int]
     lib.oracle_tangent.restype = C.c_int
@@ -368,6 +370,15 @@ class OracleTracer:
         out = np.zeros(4, dtype=np.float32)
         _check(self.lib.oracle_terrain_query(C.byref(s), C.byref(t), _ptr(o), _ptr(d), limit, int(occlusion),
                                              _ptr(out)), "oracle_terrain_query")
+        return out
+
+    def sky_cache(self, frame: Frame) -> np.ndarray:
+        """The surface sky cache of `frame` (terrain.wgsl:286-302): (8, 16, 4)
+        texels by elevation row and azimuth."""
+        s, bodies, t = self._probe_args(frame)
+        out = np.zeros((8, 16, 4), dtype=np.float32)
+        _check(self.lib.oracle_sky_cache(C.byref(s), C.cast(bodies, C.c_void_p), C.byref(t), _ptr(out)),
+               "oracle_sky_cache")
         return out
 
     def closest_hit(self, frame: Frame, rays: np.ndarray) -> np.ndarray:

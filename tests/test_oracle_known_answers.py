@@ -172,3 +172,36 @@ def test_guided_ground_is_inert_without_air_or_reflectors():
         t.set_guided_ground(guided)
         imgs.append(ka.sample(t, base, 1))
     assert not np.array_equal(imgs[0], imgs[1])
+
+
+def test_surface_sky_cache_holds_air_light_over_terrain_only():
+    """cache_surface_sky (terrain.wgsl:286-302): air light in 16 x 8
+    directions of the local sky when both the host air and the terrain are
+    on, zero otherwise; a daylit sky is bluer toward the zenith than the
+    horizon is reddened."""
+    cells = 64
+    from stargaze_b200 import terrain as T
+
+    heights = T.fbm_heights(cells, seed=2)
+    data = T.pack_terrain(heights, cells)
+    f = ka.terrain_frame(6_371_000.0)
+    host = f.bodies[0]
+    ka.set_air(f, ka.earthlike(), list(host.center), host.radius, host=1.0)
+    # A sun high in the south (the local frame's up and north).
+    up = np.array(f.globals.ground_up[:3], np.float64)
+    north = np.array(f.globals.ground_north[:3], np.float64)
+    sun = 0.8 * up - 0.6 * north
+    f.bodies[1] = ka.body(list(sun / np.linalg.norm(sun)), 0.00465, [40_000.0] * 3, True)
+    t = make((1, 1), ka.test_options())
+    t.upload_terrain(data, cells)
+    lit = t.sky_cache(f)
+    assert np.isfinite(lit).all() and (lit[..., :3] > 0.0).all()
+    assert (lit[..., 3] == 0.0).all()
+    zenith = lit[7].mean(axis=0)
+    assert zenith[2] > zenith[0], zenith
+    no_terrain = f.copy()
+    no_terrain.globals.ground_counts[1] = 0
+    assert (t.sky_cache(no_terrain) == 0.0).all()
+    no_air = f.copy()
+    no_air.globals.atmo_params[3] = 0.0
+    assert (t.sky_cache(no_air) == 0.0).all()
