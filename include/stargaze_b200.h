@@ -353,6 +353,16 @@ SG_API int sg_set_fp64_sites(sg_context *ctx, int enable);
  * on. Changing it resets the accumulation on the next encode. */
 SG_API int sg_set_guided_ground(sg_context *ctx, int enable);
 
+/* Ringshine: the next-event estimation of a ringed planet's own sunlit
+ * rings onto its surface (ringshine, pathtrace.wgsl:1248-1296, called from
+ * trace at :1567-1571, with the MIS of continuations that reach the rings at
+ * :1424-1430). On by default, as in the reference. Off reproduces the
+ * integrator as it stood before ringshine was added, the one the
+ * reference's published benchmark images were rendered with
+ * (benchmarks/optimizations/rx7600xt-2026-10-04/, benchmarks/m4pro-2026-10-15/).
+ * Changing it resets the accumulation on the next encode. */
+SG_API int sg_set_ringshine(sg_context *ctx, int enable);
+
 /* Extension (no reference counterpart; the reference has one WGSL compute
  * pass, pathtrace.wgsl:1645-1675): which CUDA integrator sg_encode runs.
  *   SG_INTEGRATOR_MEGAKERNEL  one thread per pixel walks every path of the

@@ -40,6 +40,7 @@ class Tables(C.Structure):
         ("sky_cells", C.c_void_p),
         ("milky_way", C.c_void_p),
         ("guided_ground", C.c_uint32),
+        ("ringshine_off", C.c_uint32),
     ]
 
 
@@ -137,6 +138,7 @@ class TableSet:
         self.sky_cells: np.ndarray | None = None
         self.milky: np.ndarray | None = None
         self.guided_ground = False
+        self.ringshine = True
 
     def upload(self, slot: int, tau) -> None:
         self.tables[slot] = np.ascontiguousarray(tau, dtype=np.float32)
@@ -210,6 +212,7 @@ class TableSet:
         if self.milky is not None:
             t.milky_way = self.milky.ctypes.data
         t.guided_ground = 1 if self.guided_ground else 0
+        t.ringshine_off = 0 if self.ringshine else 1
         return t
 
 
@@ -324,6 +327,13 @@ class OracleTracer:
         new tracer, a change restarts the accumulation."""
         if bool(enable) != self.tables.guided_ground:
             self.tables.guided_ground = bool(enable)
+            self.tables.version += 1
+
+    def set_ringshine(self, enable: bool) -> None:
+        """Ringshine next-event estimation (pathtrace.wgsl:1248-1296), on by
+        default; a change restarts the accumulation."""
+        if bool(enable) != self.tables.ringshine:
+            self.tables.ringshine = bool(enable)
             self.tables.version += 1
 
     def encode(self, frame: Frame, stream=None, rows=None) -> None:

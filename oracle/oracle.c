@@ -2948,7 +2948,7 @@ static void trace(const scene *S, ray_t initial, uint32_t *rng, float out[7], co
                                   vadd(vmulv(vadd(vmulv(dthroughput_full, albedo), vmulv(throughput, dalbedo)), direct_light),
                                        vmulv(vmulv(throughput, albedo), ddirect_light)));
         shine_body = MISS;
-        if (!local) {
+        if (!local && !(S->t && S->t->ringshine_off)) {
             v3 dshine = V(0, 0, 0);
             v3 shine = ringshine(S, hit.index, outgoing.offset, normal, last_vertex, rng, D, D ? &dshine : NULL);
             radiance = vadd(radiance, vmulv(vmulv(throughput, albedo), shine));

@@ -59,6 +59,11 @@ typedef struct oracle_tables {
     const uint32_t *milky_way;
     /* The guided ground sampler (src/guided_ground.rs:14-79) when nonzero. */
     uint32_t guided_ground;
+    /* Nonzero leaves out ringshine (pathtrace.wgsl:1248-1296): no annulus
+     * sample, no light samples from it and no MIS of continuations that hit
+     * the rings. This is the integrator the reference's published benchmark
+     * images were rendered with (their manifests predate ringshine). */
+    uint32_t ringshine_off;
 } oracle_tables;
 
 /* Floats of the reference terrain layout for `cells` cells per side

@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PACKAGE_DIR = Path(__file__).resolve().parent
@@ -53,27 +54,35 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= built for p in _inputs())
 
 
-def build_library(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the kernels and the C-ABI host runtime into LIBRARY."""
-    if not force and up_to_date():
-        return LIBRARY
-    tmp = LIBRARY.with_suffix(".so.tmp")
-    cmd = [
-        nvcc_path(),
-        *ARCH_FLAGS,
-        *NVCC_FLAGS,
-        "-shared",
-        "-o",
-        str(tmp),
-        *[str(CSRC / s) for s in SOURCES],
-    ]
+def _compile(source: str, objdir: Path) -> tuple[Path, str]:
+    obj = objdir / (Path(source).stem + ".o")
+    cmd = [nvcc_path(), *ARCH_FLAGS, *NVCC_FLAGS, "-c", "-o", str(obj), str(CSRC / source)]
     proc = subprocess.run(cmd, cwd=str(CSRC), capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{' '.join(cmd)}\n{proc.stdout}\n{proc.stderr}")
+    return obj, proc.stdout + proc.stderr
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the kernels and the C-ABI host runtime into LIBRARY: one nvcc
+    per translation unit, run concurrently, then one shared-library link."""
+    if not force and up_to_date():
+        return LIBRARY
+    objdir = PACKAGE_DIR / "_build"
+    objdir.mkdir(exist_ok=True)
+    workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        results = list(pool.map(lambda s: _compile(s, objdir), SOURCES))
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    cmd = [nvcc_path(), *ARCH_FLAGS, "-shared", "-o", str(tmp), *[str(obj) for obj, _ in results]]
+    proc = subprocess.run(cmd, cwd=str(CSRC), capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc link failed ({proc.returncode}):\n{' '.join(cmd)}\n{proc.stdout}\n{proc.stderr}")
+    report = "".join(log for _, log in results) + proc.stdout + proc.stderr
     if verbose:
-        print(proc.stdout + proc.stderr)
+        print(report)
     os.replace(tmp, LIBRARY)
-    (PACKAGE_DIR / "ptxas_report.txt").write_text(proc.stdout + proc.stderr)
+    (PACKAGE_DIR / "ptxas_report.txt").write_text(report)
     return LIBRARY
 
 

@@ -47,6 +47,7 @@ _SIGNATURES = {
     "sg_closest_hit_noalloc": (C.c_int, [C.c_int, C.POINTER(abi.FrameView), _P, C.c_uint32, _P, _P]),
     "sg_set_fp64_sites": (C.c_int, [_P, C.c_int]),
     "sg_set_guided_ground": (C.c_int, [_P, C.c_int]),
+    "sg_set_ringshine": (C.c_int, [_P, C.c_int]),
     "sg_set_integrator": (C.c_int, [_P, C.c_int, C.c_uint32]),
     "sg_get_integrator": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "sg_set_stage_timing": (C.c_int, [_P, C.c_int]),

@@ -81,6 +81,7 @@ struct sg_context {
     float map_extent = 0.0f;
     bool fp64_sites = false;                // ring plane, host sphere, 5 mm offset in FP64
     bool guided_ground = false;             // the guided ground sampler (air frames)
+    bool ringshine = true;                  // ringshine NEE at ringed bodies' surfaces
     // Wavefront integrator (sg_set_integrator), buffers allocated on first use.
     int integrator = SG_INTEGRATOR_WAVEFRONT;
     uint32_t wave_pool_request = 0;         // 0: the default pool
@@ -213,6 +214,7 @@ std::vector<uint8_t> history_key(const sg_context *ctx, const sg_frame *frame) {
     append(key, ctx->table_version);
     append(key, ctx->fp64_sites);
     append(key, ctx->guided_ground);
+    append(key, ctx->ringshine);
     return key;
 }
 
@@ -408,6 +410,7 @@ sg::TraceParams make_params(sg_context *ctx, const sg_settings &s) {
     p.air_on = s.g.atmo_params[3] >= 0.5f ? 1u : 0u;
     p.sky_light = ctx->sky_light;
     p.guided_ground = ctx->guided_ground ? 1u : 0u;
+    p.ringshine = ctx->ringshine ? 1u : 0u;
     return p;
 }
 
@@ -1299,6 +1302,12 @@ int sg_set_fp64_sites(sg_context *ctx, int enable) {
 int sg_set_guided_ground(sg_context *ctx, int enable) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     ctx->guided_ground = enable != 0;
+    return SG_OK;
+}
+
+int sg_set_ringshine(sg_context *ctx, int enable) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    ctx->ringshine = enable != 0;
     return SG_OK;
 }
 

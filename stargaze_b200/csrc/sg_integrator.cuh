@@ -460,7 +460,8 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
             albedo = surface_albedo<G::air>(S, bi, normal);
         }
         radiance = radiance + throughput * albedo * direct_light;
-        if (!local && has_ring(S, bi)) {
+        const bool shines = !local && S.p->ringshine && has_ring(S, bi);
+        if (shines) {
             Shine shine;
             if constexpr (G::adjoint)
                 shine = ringshine_grad(S, K, bi, outgoing.o, normal, last_vertex, rng, grad, throughput * albedo,
@@ -481,7 +482,7 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
                 radiance = radiance + throughput * albedo * sky.radiance;
             }
         }
-        shine_body = local ? kMiss : bi;
+        shine_body = (local || !S.p->ringshine) ? kMiss : bi;
         if (last_vertex) return true;
         const float u = rnd(K, rng);
         float sp, cp;

@@ -57,6 +57,9 @@ struct TraceParams {
     uint32_t guided_ground;
     // A body of the frame has a procedural surface style (axis_x.w >= 0.5).
     uint32_t styled;
+    // Ringshine next-event estimation (pathtrace.wgsl:1248-1296) at ringed
+    // bodies' surfaces; 0 leaves it out (sg_set_ringshine).
+    uint32_t ringshine;
 };
 
 // Geometry cache of the heightfield (cache_terrain_geometry,

@@ -119,6 +119,13 @@ class PathTracer:
         (the reference app's default; off here as in `PathTracer::new`)."""
         check(self._lib.sg_set_guided_ground(self._ctx, int(bool(enable))), self._ctx)
 
+    def set_ringshine(self, enable: bool) -> None:
+        """Ringshine next-event estimation (pathtrace.wgsl:1248-1296), on by
+        default as in the reference; off gives the integrator the
+        reference's published benchmark images were rendered with. A change
+        restarts the accumulation."""
+        check(self._lib.sg_set_ringshine(self._ctx, int(bool(enable))), self._ctx)
+
     def set_integrator(self, integrator: str, pool_paths: int = 0) -> None:
         """"wavefront" (default; stage kernels over a pool of `pool_paths`
         paths in device memory, 0 = default pool) or "megakernel" (one
