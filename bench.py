@@ -58,11 +58,24 @@ OPS_PER_EVENT = {
     "ring_events": 120,    # optics, transmission, slab BSDF, MIS, null/scatter
     "surface_events": 110, # normal, outgoing, albedo, cosine bounce, roulette
     "rng_draws": 10,       # LCG step + permutation + float conversion
+    # Local landscape (sg_landscape.cuh): an interior quadtree node decodes
+    # its Morton index (30) and slab-tests its four children (4 x 25 for
+    # t_interval, 4 x 4 for the validity test, 10 for sort and push); a
+    # terrain triangle is one Moller-Trumbore test (58) plus its share of the
+    # cell's four vertex fetches (12); a group-marker box is one 3-slab
+    # interval (27) plus the skip test (7); a primitive test is the
+    # translation and rotation into its frame (18) plus the shape test,
+    # weighted 5:2 ellipsoids (45) to rocks (150) as in the terrain scene.
+    "terrain_nodes": 156,
+    "terrain_triangles": 70,
+    "prop_boxes": 34,
+    "prop_tests": 93,
 }
 EVENT_ORDER = ["vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples", "shadow_rays",
-               "ring_events", "surface_events", "rng_draws"]
-# DRAM traffic of one trace launch on this workload from an ncu capture
-# (profiles/trace_kernel_rings_1080p.md); None until measured.
+               "ring_events", "surface_events", "rng_draws", "terrain_nodes", "terrain_triangles", "prop_boxes",
+               "prop_tests"]
+# DRAM traffic of one dispatch on this workload from an ncu capture of its
+# stage kernels; None until measured.
 TRAFFIC_BYTES_PER_LAUNCH = None
 L2_FLUSH_BYTES = 256 << 20
 
@@ -250,7 +263,7 @@ def cpu_baseline(wl, seconds: float, threads: int = 0) -> dict:
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     return {"value": samples / elapsed / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{samples} samples ({wl.width}x{wl.height} frame, 8-sample dispatches, row bands) "
-                      f"in {elapsed:.1f} s"}
+                      f"in {elapsed:.1f} s", "build": oracle_build_flags()}
 
 
 # Replicas: rank r renders noise keys from RANK_KEY_STRIDE * r on, so ranks
@@ -284,31 +297,54 @@ def relative_rmse(x: np.ndarray, reference: np.ndarray) -> float:
     return float(np.sqrt((d * d).sum() / (reference[:, :3].astype(np.float64) ** 2).sum()))
 
 
+CONVERGED_SPP = 4096
+CONVERGED_NOISE_SEED = 0x40000000  # keys disjoint from every timed render's
+
+
+def _to_1pct(err: float, spp: int, ref_spp: int, width: int, height: int, msamples_per_s: float) -> dict:
+    """Samples per pixel (and time at `msamples_per_s`) for 1 % relative
+    RMSE from the 1/sqrt(spp) law, after removing the reference image's own
+    noise: with independent keys err^2 = e^2 (1 + spp / ref_spp)."""
+    own = err / np.sqrt(1.0 + spp / ref_spp)
+    spp_1pct = spp * (own / 0.01) ** 2
+    return {"relative_rmse": err, "spp_to_1pct": spp_1pct,
+            "ms_to_1pct": spp_1pct * width * height / (msamples_per_s * 1e6) * 1e3}
+
+
 def convergence(wl, image: np.ndarray, spp: int, msamples_per_s: float, device: int, stream) -> dict:
-    """Relative RMSE of a `spp`-sample image against a 4096-sample image of
-    the same workload with disjoint noise keys, and the samples per pixel
-    (and time at `msamples_per_s`) for 1 % relative RMSE, from the
-    1 / sqrt(spp) law."""
+    """Relative RMSE (scripts/benchmark.py:219-232) of the `spp`-sample
+    image against the oracle's 4096-sample image of the workload (rendered
+    once on the host by oracle/render_converged.py, disjoint noise keys) and
+    against this integrator's own 4096-sample image, with the spp and time
+    each implies for 1 %."""
     from stargaze_b200 import PathTracer
     from stargaze_b200.workloads import render_options, upload_workload
 
-    ref_spp = 4096
-    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH, noise_seed=0x40000000), device=device)
+    out = {"spp": spp, "reference_spp": CONVERGED_SPP}
+    cached = ROOT / "oracle" / "_cache" / f"{wl.name}_{CONVERGED_SPP}spp.npy"
+    if cached.exists():
+        oracle_image = np.load(cached)
+        out["vs_oracle"] = _to_1pct(relative_rmse(image, oracle_image), spp, CONVERGED_SPP, wl.width, wl.height,
+                                    msamples_per_s)
+        out["reference"] = f"oracle at {CONVERGED_SPP} spp ({cached.name})"
+    else:
+        out["reference"] = f"oracle image missing: run oracle/render_converged.py --workload {wl.name}"
+    t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH, noise_seed=CONVERGED_NOISE_SEED),
+                   device=device)
     upload_workload(t, wl)
     frame = wl.frame.copy()
     frame.scene_time = -12345.0
-    for _ in range(ref_spp // BATCH):
+    for _ in range(CONVERGED_SPP // BATCH):
         t.encode(frame, stream)
-    reference = t.read_pixels(stream)
+    own_image = t.read_pixels(stream)
     t.close()
-    err = relative_rmse(image, reference)
-    # The reference's own noise adds err_ref^2 = err^2 * spp / ref_spp.
-    own = err * np.sqrt(max(1.0 - spp / ref_spp, 1e-6))
-    spp_1pct = spp * (own / 0.01) ** 2
-    return {"relative_rmse": err, "spp": spp, "reference_spp": ref_spp,
-            "spp_to_1pct": spp_1pct,
-            "ms_to_1pct": spp_1pct * wl.width * wl.height / (msamples_per_s * 1e6) * 1e3,
-            "reference": "this integrator at 4096 spp, disjoint noise (parity with the oracle is tested at small sizes)"}
+    out["vs_self"] = _to_1pct(relative_rmse(image, own_image), spp, CONVERGED_SPP, wl.width, wl.height,
+                              msamples_per_s)
+    if cached.exists():
+        # Both references are converged estimates of the same image: their
+        # distance bounds any bias between the CUDA path and the oracle.
+        out["oracle_vs_self_relative_rmse"] = relative_rmse(own_image, oracle_image)
+    return out
 
 
 def timed_forward(t, wl, frame, stream) -> float:
@@ -373,6 +409,115 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
             "ratio": b / f, "forward_plus_adjoint_over_forward": (f + b) / f,
             "parameters": params, "dropped_entries": int(g.dropped),
             "note": "forward: wavefront; backward: staged adjoint (per-pixel adjoint kernel beside it)"}
+
+
+def count_ops(lib, wl, opts, frame, device: int, stream, batches: int):
+    """Events of one step through the counting variant of the integrator
+    (same image and noise keys), and the FP32/INT operations per dispatch
+    they imply under OPS_PER_EVENT."""
+    import ctypes as C
+
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import upload_workload
+
+    counter = PathTracer((wl.width, wl.height), opts, device=device)
+    upload_workload(counter, wl)
+    totals = np.zeros(len(EVENT_ORDER), np.uint64)
+    ev = (C.c_uint64 * len(EVENT_ORDER))()
+    for _ in range(batches):
+        view = frame.view()
+        status = lib.sg_encode_counted(counter.handle, C.byref(view), C.c_void_p(stream.cuda_stream), ev)
+        assert status == 0, status
+        totals += np.array(list(ev), np.uint64)
+    counter.close()
+    ops = float(sum(int(totals[k]) * OPS_PER_EVENT[n] for k, n in enumerate(EVENT_ORDER))) / batches
+    return totals, ops
+
+
+def config_entry(lib, wl, device: int, stream, peak: float, reps: int = 2) -> dict:
+    """Another configuration's step (its spp from a fresh accumulation,
+    64-sample dispatches, wavefront integrator) with its own roofline."""
+    import torch
+
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    opts = render_options(wl, spp=BATCH)
+    batches = (wl.spp + BATCH - 1) // BATCH
+    t = PathTracer((wl.width, wl.height), opts, device=device)
+    upload_workload(t, wl)
+    times, dispatch_ms = [], []
+    for r in range(reps + 1):
+        frame = wl.frame.copy()
+        frame.scene_time = float(-900 - r)
+        t.prepare_frame(frame)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(batches + 1)]
+        marks[0].record(stream)
+        for b in range(batches):
+            t.encode(frame, stream)
+            marks[b + 1].record(stream)
+        stream.synchronize()
+        if r > 0:
+            times.append(marks[0].elapsed_time(marks[-1]))
+            dispatch_ms += [marks[b].elapsed_time(marks[b + 1]) for b in range(batches)]
+    t.close()
+    totals, ops = count_ops(lib, wl, opts, wl.frame.copy(), device, stream, batches)
+    ms = statistics.median(times)
+    achieved = ops / (statistics.mean(dispatch_ms) * 1e-3)
+    return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+            "max_bounces": wl.max_bounces, "ms_per_step": ms,
+            "msamples_per_s": wl.width * wl.height * wl.spp / (ms * 1e3),
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "ops_per_launch": ops,
+                         "events_per_launch": {n: int(totals[k]) // batches for k, n in enumerate(EVENT_ORDER)}}}
+
+
+def checkpoint_comparison(wl, device: int, stream, every: int = 2, reps: int = 2) -> dict:
+    """The adjoint with vertex checkpoints every `every` bounces against path
+    replay on the same scene and spp: forward and backward times (CUDA
+    events, median of `reps`) and the device memory the checkpoints hold."""
+    import torch
+
+    from stargaze_b200 import PathTracer
+    from stargaze_b200.workloads import render_options, upload_workload
+
+    dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
+    out = {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp, "every": every}
+    for mode in ("replay", "checkpoints"):
+        t = PathTracer((wl.width, wl.height), render_options(wl, spp=BATCH), device=device)
+        upload_workload(t, wl)
+        if mode == "checkpoints":
+            t.set_checkpoints(every, wl.spp)
+        fwd, bwd, stats = [], [], None
+        for r in range(reps + 1):
+            frame = wl.frame.copy()
+            frame.scene_time = float(-500 - r)
+            f = timed_forward(t, wl, frame, stream)
+            if mode == "checkpoints":
+                stats = t.checkpoint_stats()
+            tape = t.tape()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            t.backward(frame, tape, dl, stream)
+            b.record(stream)
+            stream.synchronize()
+            if r > 0:
+                fwd.append(f)
+                bwd.append(a.elapsed_time(b))
+        t.close()
+        entry = {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd)}
+        entry["forward_plus_adjoint_ms"] = entry["forward_ms"] + entry["backward_ms"]
+        if stats is not None:
+            entry["device_bytes"] = stats["device_bytes"]
+            entry["records"] = stats["records"]
+            entry["records_dropped"] = stats["dropped"]
+        else:
+            entry["device_bytes"] = 0
+        out[mode] = entry
+    out["note"] = ("replay: the staged adjoint replays every sample from its noise key; checkpoints: the "
+                   "forward stores path state every `every` bounces and each sample's radiance, the "
+                   "backward replays segments between checkpoints (device_bytes: what they hold)")
+    return out
 
 
 def integrator_comparison(wl, device: int, stream, reps: int = 3) -> dict:
@@ -486,7 +631,22 @@ def air_terrain(device: int, stream, reps: int = 1) -> dict:
     return out
 
 
+def oracle_build_flags() -> str:
+    """The compile line of the oracle library (oracle/Makefile)."""
+    try:
+        text = (ROOT / "oracle" / "Makefile").read_text()
+        flags = next(line.split("=", 1)[1].strip() for line in text.splitlines() if line.startswith("CFLAGS"))
+        return f"gcc {flags}"
+    except (OSError, StopIteration):
+        return "unknown"
+
+
 def run_reference(args):
+    """The reference integrator's CPU restatement (the oracle) on every host
+    core. Each step is one bounded sample of the workload: row bands of the
+    frame in 8-sample dispatches for `per_step` seconds. `ms_per_step` is
+    that measured wall time; the full 256-spp frame it extrapolates to is
+    reported apart."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
@@ -496,18 +656,24 @@ def run_reference(args):
     per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(args.steps + args.warmup, 1)))
     for _ in range(args.warmup):
         cpu_baseline(wl, min(per_step, 2.0))
-    values = [cpu_baseline(wl, per_step) for _ in range(args.steps)]
+    values, walls = [], []
+    for _ in range(args.steps):
+        start = time.perf_counter()
+        values.append(cpu_baseline(wl, per_step))
+        walls.append((time.perf_counter() - start) * 1e3)
     value = statistics.median(v["value"] for v in values)
     base = values[0]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * wl.width * wl.height * args.spp / (value * 1e6),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": args.spp,
-                   "max_bounces": wl.max_bounces, "cpu_sample": base["sample"]},
+                   "max_bounces": wl.max_bounces,
+                   "step": f"a bounded sample of the workload, about {per_step:.1f} s of row bands",
+                   "cpu_sample": base["sample"],
+                   "full_frame_ms_extrapolated": 1e3 * wl.width * wl.height * args.spp / (value * 1e6)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": base["kind"],
-                         "sample": base["sample"]},
+                         "sample": base["sample"], "build": oracle_build_flags()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -555,17 +721,7 @@ def run_ours(args):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     # Algorithmic work of one launch (counting kernel, outside timing).
-    counter = PathTracer((wl.width, wl.height), opts, device=local)
-    upload_workload(counter, wl)
-    totals = np.zeros(len(EVENT_ORDER), np.uint64)
-    ev = (C.c_uint64 * len(EVENT_ORDER))()
-    for _ in range(batches):
-        view = frame.view()
-        status = lib.sg_encode_counted(counter.handle, C.byref(view), C.c_void_p(stream.cuda_stream), ev)
-        assert status == 0, status
-        totals += np.array(list(ev), np.uint64)
-    counter.close()
-    ops_per_launch = float(sum(int(totals[k]) * OPS_PER_EVENT[n] for k, n in enumerate(EVENT_ORDER))) / batches
+    totals, ops_per_launch = count_ops(lib, wl, opts, frame, local, stream, batches)
     peak = C.c_double()
     assert lib.sg_measure_fp32_peak(local, C.byref(peak)) == 0
 
@@ -632,17 +788,22 @@ def run_ours(args):
             from stargaze_b200 import workloads as W
 
             image = tracer.read_pixels(stream)
+            extras["fp64_sites"] = fp64_sites(wl, local, stream)
+            extras["integrators"] = integrator_comparison(wl, local, stream)
+            extras["air"] = air_terrain(local, stream)
+            extras["configs"] = {"spheres_256": config_entry(lib, W.spheres_256(), local, stream, peak.value),
+                                 "terrain_1080p": config_entry(lib, W.WORKLOADS["terrain_1080p"](), local, stream,
+                                                               peak.value)}
             extras["convergence"] = convergence(wl, image, args.spp, value, local, stream)
-            ring = adjoint_ratio(W.rings_1080p(512, 512, 64), local, stream)
             land_wl, land = W.terrain_1080p(1920, 1080, 256)
             land.albedo_map = np.random.default_rng(1).uniform(0.05, 0.6, (1024, 1024)).astype(np.float32)
             land.map_extent = 2000.0
             terrain = adjoint_ratio(land_wl, local, stream, reps=2)
-            extras["adjoint"] = {"ratio": ring["ratio"], "ring_512": ring, "terrain_1080p": terrain,
+            checkpoints = checkpoint_comparison(land_wl, local, stream)
+            ring = adjoint_ratio(W.rings_1080p(512, 512, 64), local, stream)
+            extras["adjoint"] = {"terrain_1080p": terrain, "checkpoints_terrain_1080p": checkpoints,
+                                 "ring_512": ring, "ratio": ring["ratio"],
                                  "note": "ratio = adjoint time / forward time at equal spp (ring scene)"}
-            extras["fp64_sites"] = fp64_sites(wl, local, stream)
-            extras["integrators"] = integrator_comparison(wl, local, stream)
-            extras["air"] = air_terrain(local, stream)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

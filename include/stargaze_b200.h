@@ -310,7 +310,9 @@ SG_API int sg_terrain_probe(sg_context *ctx, const sg_frame *frame,
  * time: a host application that gives the whole device to its own
  * allocator or memory pool, where a library cudaMalloc fails or splits the
  * pool, and latency-bound callers, for which cudaMalloc synchronises the
- * device. The results equal sg_closest_hit's. Unlike it, this call needs no
+ * device. The results equal sg_closest_hit's with FP64 sites off (this
+ * entry point has no context, so it always runs the reference's f32
+ * arithmetic). Unlike it, this call needs no
  * context and stages the frame's bodies, the rays and the hits in one
  * fixed device array of SG_NOALLOC_SCRATCH_BYTES that every GPU loading the
  * library holds until the process exits.
@@ -319,7 +321,9 @@ SG_API int sg_terrain_probe(sg_context *ctx, const sg_frame *frame,
  *   - frames with a local landscape (ground_north.w != 0) need a context
  *     and fail with SG_ERR_INVALID: use sg_closest_hit;
  *   - the first call on a device looks up the array's device address; make
- *     it before any stream capture;
+ *     it before any stream capture. The address is kept for the life of the
+ *     process: after cudaDeviceReset on that device, reload the library
+ *     before calling this again;
  *   - every call on a device shares the array, so calls whose work
  *     overlaps on the GPU (other host threads, other streams) race;
  *   - errors are reported by sg_last_error(NULL).
@@ -362,6 +366,30 @@ SG_API int sg_set_guided_ground(sg_context *ctx, int enable);
  * (benchmarks/optimizations/rx7600xt-2026-10-04/, benchmarks/m4pro-2026-10-15/).
  * Changing it resets the accumulation on the next encode. */
 SG_API int sg_set_ringshine(sg_context *ctx, int enable);
+
+/* Extension (no reference counterpart; the reference renders forward only):
+ * vertex checkpoints for sg_backward, the alternative to replaying every
+ * path from its noise key. With `every` > 0, each wavefront sg_encode of an
+ * accumulation stores a path's whole state (SG_CHECKPOINT_BYTES) whenever a
+ * scatter brings its depth to a multiple of `every`, and every sample's
+ * radiance (16 B per sample and pixel, for the first `max_samples` samples
+ * of the accumulation). sg_backward then replays each sample only up to its
+ * first checkpoint and every later segment from its record, in parallel,
+ * with the path's total known, so nothing is deferred or replayed twice.
+ * Samples whose ring-indirect cap binds, or whose records did not fit
+ * `record_bytes` (0: half the free device memory at the first encode), are
+ * replayed from their noise key as without checkpoints. Frames with host
+ * air, procedural styles or a sky backdrop, the megakernel integrator and
+ * sg_encode_counted store none (their samples replay). `every` = 0 (the
+ * default) turns checkpointing off and frees the buffers; a change resets
+ * the accumulation on the next encode. */
+#define SG_CHECKPOINT_BYTES 128u
+SG_API int sg_set_checkpoints(sg_context *ctx, uint32_t every, uint32_t max_samples, uint64_t record_bytes);
+
+/* Device memory the checkpoints of the current accumulation hold (totals
+ * plus stored records), the records stored, and the records that did not
+ * fit the budget. Any pointer may be NULL. Synchronises the device. */
+SG_API int sg_get_checkpoint_stats(sg_context *ctx, uint64_t *device_bytes, uint64_t *records, uint64_t *dropped);
 
 /* Extension (no reference counterpart; the reference has one WGSL compute
  * pass, pathtrace.wgsl:1645-1675): which CUDA integrator sg_encode runs.
@@ -534,9 +562,11 @@ SG_API int sg_launch_count(const sg_context *ctx, uint64_t *launches);
 /* sg_encode through the event-counting variant of the integrator kernel:
  * same image and history effect, plus per-dispatch event totals in
  * `events[SG_EVENT_COUNT]` (vertices, sphere tests, sphere hits, ring tests,
- * light samples, shadow rays, ring events, surface events, RNG draws).
+ * light samples, shadow rays, ring events, surface events, RNG draws,
+ * terrain quadtree nodes expanded, terrain triangle tests, landscape
+ * group-marker box tests, landscape primitive tests).
  * Synchronises `stream`. Used to model the algorithmic work of a launch. */
-#define SG_EVENT_COUNT 9
+#define SG_EVENT_COUNT 13
 SG_API int sg_encode_counted(sg_context *ctx, const sg_frame *frame,
                              void *stream, uint64_t *events);
 

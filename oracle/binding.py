@@ -56,7 +56,8 @@ class Direction(C.Structure):
 class Events(C.Structure):
     _fields_ = [(name, C.c_uint64) for name in (
         "samples", "vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples",
-        "shadow_rays", "ring_events", "surface_events", "rng_draws")]
+        "shadow_rays", "ring_events", "surface_events", "rng_draws", "terrain_nodes", "terrain_triangles",
+        "prop_boxes", "prop_tests")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

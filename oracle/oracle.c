@@ -1338,6 +1338,8 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
         if (node[3] == 2u) {
             for (uint32_t z = node[2]; z < node[2] + 2u; z++) {
                 for (uint32_t x = node[1]; x < node[1] + 2u; x++) {
+                    EV(terrain_triangles);
+                    EV(terrain_triangles);
                     v3 a = t_vertex(T, cells, scale, x, z);
                     v3 b = t_vertex(T, cells, scale, x + 1u, z);
                     v3 c = t_vertex(T, cells, scale, x, z + 1u);
@@ -1365,6 +1367,7 @@ static float t_query(const scene *S, const float *T, uint32_t cells, v3 o, v3 d,
                 }
             }
         } else {
+            EV(terrain_nodes);
             uint32_t children[4];
             float distances[4];
             uint32_t half_size = node[3] / 2u;
@@ -1565,11 +1568,13 @@ static hit_t landscape_query(const scene *S, ray_t ray, float limit, int occlusi
         v3 e = V(object->extent[0], object->extent[1], object->extent[2]);
         float kind = object->center[3];
         if (kind < 0.0f) {
+            EV(prop_boxes);
             float bn, bf_;
             box_interval(vsub(o, center), d, e, &bn, &bf_);
             if (bn > bf_ || bf_ <= 0.001f || bn / METRES_PER_AU > closest.distance) i += (uint32_t)(-kind);
             continue;
         }
+        EV(prop_tests);
         v3 p = vsub(o, center), v = d;
         v3 angles = V(0, 0, 0);
         if (kind == 2.25f) {

@@ -91,6 +91,10 @@ typedef struct oracle_events {
     uint64_t ring_events;    /* ring scattering / null vertices         */
     uint64_t surface_events; /* surface shading vertices                */
     uint64_t rng_draws;      /* random() calls                          */
+    uint64_t terrain_nodes;  /* quadtree interior nodes expanded        */
+    uint64_t terrain_triangles; /* terrain_triangle calls               */
+    uint64_t prop_boxes;     /* group-marker bounding-box tests         */
+    uint64_t prop_tests;     /* landscape primitive tests               */
 } oracle_events;
 
 /* One dispatch of the WGSL `main` entry point (pathtrace.wgsl:1645-1675)

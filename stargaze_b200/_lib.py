@@ -48,6 +48,8 @@ _SIGNATURES = {
     "sg_set_fp64_sites": (C.c_int, [_P, C.c_int]),
     "sg_set_guided_ground": (C.c_int, [_P, C.c_int]),
     "sg_set_ringshine": (C.c_int, [_P, C.c_int]),
+    "sg_set_checkpoints": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint64]),
+    "sg_get_checkpoint_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "sg_set_integrator": (C.c_int, [_P, C.c_int, C.c_uint32]),
     "sg_get_integrator": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "sg_set_stage_timing": (C.c_int, [_P, C.c_int]),

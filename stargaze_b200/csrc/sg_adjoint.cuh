@@ -152,6 +152,10 @@ struct Prb {
     static constexpr bool sky = false;  // sg_backward rejects frames with a sky
     static constexpr bool air = false;  // ... and frames with host air
     bool pass2;
+    // A segment of a checkpointed path (sg_set_checkpoints): the path's total
+    // is known from the forward, so one replay scatters everything at once
+    // (contributions at full weight, factors with the radiance after them).
+    bool known_total;
     // Pass 1's summary.
     float cap;
     float3 base;            // radiance at the cap vertex's scatter
@@ -234,7 +238,8 @@ static __device__ SG_ADJ_HOOK void contribute(Prb &G, float3 value, bool cap_ter
     const bool post = G.post();
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     const float3 full = cap_term ? G.w_cap : (post ? G.w_post : G.w_pre);
-    const float3 local = !G.pass2 ? full : (cap_term ? G.w_cap : (post ? G.w_post - G.w_pre : zero));
+    const float3 local =
+        (!G.pass2 || G.known_total) ? full : (cap_term ? G.w_cap : (post ? G.w_post - G.w_pre : zero));
     const float3 w = mul3(local, value);
     const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : zero;
     if (w.x != 0.0f || w.y != 0.0f || w.z != 0.0f || wp.x != 0.0f || wp.y != 0.0f || wp.z != 0.0f) {
@@ -589,6 +594,7 @@ static __device__ SG_ADJ_HOOK void record_roulette(Prb &G, uint32_t iteration, f
 __device__ __forceinline__ void pass1_setup(Prb &G, float3 w) {
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = false;
+    G.known_total = false;
     G.capture_iter = 0;
     G.n_rr = 0;
     G.binding = false;
@@ -637,6 +643,7 @@ static __device__ SG_ADJ_HOOK void pass2_setup(Prb &G, float3 total, float3 w) {
     const float3 lum = f3(0.2126f, 0.7152f, 0.0722f);
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = true;
+    G.known_total = false;
     G.w_pre = w;
     G.w_post = w;
     G.w_pdf = zero;
@@ -675,6 +682,34 @@ static __device__ SG_ADJ_HOOK void pass2_setup(Prb &G, float3 total, float3 w) {
         G.n_rr = 0;
     }
     G.a_total = mul3(w, G.base) + mul3(G.w_post, indirect) + mul3(G.w_cap, G.cap_light);
+}
+
+// A segment of a checkpointed path whose ring-indirect cap does not bind:
+// the path's radiance `total` (from the forward) and the radiance it had
+// gathered at the segment's start `so_far` give every weight, so the
+// segment replays once, from its checkpoint, with nothing deferred.
+__device__ __forceinline__ void segment_setup(Prb &G, float3 w, float3 total, float3 so_far) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    G.pass2 = true;
+    G.known_total = true;
+    G.capture_iter = 0;
+    G.n_rr = 0;
+    G.binding = false;
+    G.iteration = 0;
+    G.w_pre = w;
+    G.w_post = w;
+    G.w_pdf = zero;
+    G.w_cap = zero;
+    G.score = 0.0f;
+    G.a = mul3(w, so_far);
+    G.b = zero;
+    G.a_total = mul3(w, total);
+    G.b_total = zero;
+    G.prev_param = kNoParam;
+    G.prev_dlog_pdf = 0.0f;
+    G.n_local = 0;
+    G.n_fac = 0;
+    G.deferral_full = false;
 }
 
 }  // namespace sg

@@ -124,7 +124,7 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
 // Event counters for the algorithmic-work model.
 struct Events {
     uint32_t vertices, sphere_tests, sphere_hits, ring_tests, light_samples, shadow_rays,
-        ring_events, surface_events, rng_draws;
+        ring_events, surface_events, rng_draws, terrain_nodes, terrain_triangles, prop_boxes, prop_tests;
 };
 
 // Counting is compiled out of the production variant (C == false); L turns
@@ -817,11 +817,11 @@ static __device__ __noinline__ float mottle(float3 axis_x, float4 axis_y, float 
     float3 p = add_rn(mul_rn(local, 2.4f), off);
     float amplitude = 0.5f, noise = 0.0f;
     for (int octave = 0; octave < 5; ++octave) {
-        noise += amplitude * vnoise(p);
-        p = p * 2.07f;
+        noise = __fadd_rn(noise, __fmul_rn(amplitude, vnoise(p)));
+        p = mul_rn(p, 2.07f);
         amplitude *= 0.5f;
     }
-    return mixf(1.0f, 0.68f + 0.64f * noise, strength);
+    return mix_rn(1.0f, __fadd_rn(0.68f, __fmul_rn(0.64f, noise)), strength);
 }
 
 }  // namespace sg

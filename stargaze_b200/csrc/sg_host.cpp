@@ -120,6 +120,17 @@ struct sg_context {
     float4 *dl_dimage = nullptr;            // staging of a host d loss / d image
     size_t dl_pixels = 0;
     unsigned long long *dropped = nullptr;  // one counter
+    // Vertex checkpoints (sg_set_checkpoints): settings, then the buffers of
+    // the current accumulation.
+    uint32_t ck_every = 0;
+    uint32_t ck_samples = 0;                // accumulation samples covered
+    uint64_t ck_record_bytes = 0;           // record budget (0: automatic)
+    float4 *ck_records = nullptr;
+    uint32_t ck_capacity = 0;
+    float4 *ck_totals = nullptr;
+    size_t ck_totals_size = 0;
+    uint32_t *ck_count = nullptr;
+    bool ck_valid = false;                  // every sample so far went through the checkpointing forward
 };
 
 namespace {
@@ -215,6 +226,7 @@ std::vector<uint8_t> history_key(const sg_context *ctx, const sg_frame *frame) {
     append(key, ctx->fp64_sites);
     append(key, ctx->guided_ground);
     append(key, ctx->ringshine);
+    append(key, ctx->ck_every);
     return key;
 }
 
@@ -509,6 +521,9 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->wave_state);
     cudaFree(ctx->wave_results);
     cudaFree(ctx->adjoint_slots);
+    cudaFree(ctx->ck_records);
+    cudaFree(ctx->ck_totals);
+    cudaFree(ctx->ck_count);
     cudaFree(ctx->exposure);
     cudaFree(ctx->histogram);
     cudaFree(ctx->catalogue);
@@ -834,6 +849,38 @@ static int meter_exposure(sg_context *ctx, cudaStream_t stream) {
     return SG_OK;
 }
 
+// The checkpoint buffers of an accumulation: totals for ck_samples samples
+// of every pixel and the record budget (by default half the device memory
+// left after the totals). A fresh accumulation clears the record count.
+static int ensure_checkpoints(sg_context *ctx, cudaStream_t stream) {
+    const size_t pixels = (size_t)ctx->width * ctx->height;
+    const size_t totals = pixels * ctx->ck_samples * sizeof(float4);
+    if (ctx->ck_totals_size < totals) {
+        cudaStreamSynchronize(stream);
+        cudaFree(ctx->ck_totals);
+        ctx->ck_totals = nullptr;
+        ctx->ck_totals_size = 0;
+        SG_CUDA(ctx, cudaMalloc(&ctx->ck_totals, totals));
+        ctx->ck_totals_size = totals;
+    }
+    if (!ctx->ck_count) SG_CUDA(ctx, cudaMalloc(&ctx->ck_count, sizeof(uint32_t)));
+    if (!ctx->ck_records) {
+        const size_t record = sg::kCheckpointVec4 * sizeof(float4);
+        size_t budget = ctx->ck_record_bytes;
+        if (budget == 0) {
+            size_t free_bytes = 0, total_bytes = 0;
+            SG_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
+            budget = free_bytes / 2;
+        }
+        const size_t capacity = std::min<size_t>(budget / record, 0xffffffffu);
+        if (capacity == 0) return fail(ctx, SG_ERR_OOM, "no device memory left for vertex checkpoints");
+        SG_CUDA(ctx, cudaMalloc(&ctx->ck_records, capacity * record));
+        ctx->ck_capacity = (uint32_t)capacity;
+    }
+    if (ctx->history.samples == 0u) SG_CUDA(ctx, cudaMemsetAsync(ctx->ck_count, 0, sizeof(uint32_t), stream));
+    return SG_OK;
+}
+
 static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr, uint64_t *events) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     int status = validate_frame(ctx, frame);
@@ -877,10 +924,26 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
             SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
             p.events = ctx->events;
         }
+        const bool checkpointing = ctx->ck_every > 0u && !events && ctx->integrator == SG_INTEGRATOR_WAVEFRONT &&
+                                   !p.air_on && !p.styled && !p.sky_on;
+        if (ctx->history.samples == 0u) ctx->ck_valid = checkpointing;
+        if (!checkpointing) ctx->ck_valid = false;
         if (!events && ctx->integrator == SG_INTEGRATOR_WAVEFRONT) {
             sg::WaveParams w{};
             status = ensure_wave(ctx, count, w);
             if (status != SG_OK) return status;
+            if (ctx->ck_valid) {
+                status = ensure_checkpoints(ctx, stream);
+                if (status != SG_OK) return status;
+                w.ck.records = ctx->ck_records;
+                w.ck.count = ctx->ck_count;
+                w.ck.capacity = ctx->ck_capacity;
+                w.ck.totals = ctx->ck_totals;
+                w.ck.samples = ctx->ck_samples;
+                w.ck.sample_base = ctx->history.samples;
+                w.ck.every = ctx->ck_every;
+                w.ck.max_depth = ctx->options.max_bounces;
+            }
             sg::WaveRun run;
             sg::StageMarks *marks = ctx->stage_timing ? &ctx->stage_marks : nullptr;
             cudaError_t e = sg::launch_wavefront(p, w, ctx->wave_pinned, ctx->wave_ready, stream, &run, marks);
@@ -1305,6 +1368,41 @@ int sg_set_guided_ground(sg_context *ctx, int enable) {
     return SG_OK;
 }
 
+int sg_set_checkpoints(sg_context *ctx, uint32_t every, uint32_t max_samples, uint64_t record_bytes) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    if (every > 64u) return fail(ctx, SG_ERR_INVALID, "every must be in 0..64");
+    if (every > 0u && (max_samples == 0u || max_samples > SG_MAX_SAMPLES))
+        return fail(ctx, SG_ERR_INVALID, "max_samples must be in 1..SG_MAX_SAMPLES");
+    DeviceGuard guard(ctx->device);
+    cudaDeviceSynchronize();
+    cudaFree(ctx->ck_records);
+    cudaFree(ctx->ck_totals);
+    ctx->ck_records = nullptr;
+    ctx->ck_totals = nullptr;
+    ctx->ck_totals_size = 0;
+    ctx->ck_capacity = 0;
+    ctx->ck_every = every;
+    ctx->ck_samples = every > 0u ? max_samples : 0u;
+    ctx->ck_record_bytes = record_bytes;
+    ctx->ck_valid = false;
+    return SG_OK;
+}
+
+int sg_get_checkpoint_stats(sg_context *ctx, uint64_t *device_bytes, uint64_t *records, uint64_t *dropped) {
+    if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
+    uint32_t claimed = 0;
+    if (ctx->ck_count) {
+        DeviceGuard guard(ctx->device);
+        SG_CUDA(ctx, cudaMemcpy(&claimed, ctx->ck_count, sizeof(claimed), cudaMemcpyDeviceToHost));
+    }
+    const uint64_t stored = std::min<uint64_t>(claimed, ctx->ck_capacity);
+    if (device_bytes)
+        *device_bytes = ctx->ck_totals_size + stored * sg::kCheckpointVec4 * sizeof(float4) + (ctx->ck_count ? 4u : 0u);
+    if (records) *records = stored;
+    if (dropped) *dropped = claimed - stored;
+    return SG_OK;
+}
+
 int sg_set_ringshine(sg_context *ctx, int enable) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     ctx->ringshine = enable != 0;
@@ -1397,7 +1495,26 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         if (ctx->ring_bins[k]) tau_used = k * SG_RING_TABLE_MAX_BINS + ctx->ring_bins[k];
     a.tau_window = tau_used <= 8192u ? tau_used : 0u;
     a.color_window = 6u * frame->n_bodies;
-    const bool staged = ctx->integrator == SG_INTEGRATOR_WAVEFRONT;
+    a.ck = sg::Checkpoints{};
+    // With vertex checkpoints of this accumulation, the per-pixel replay
+    // takes each sample only up to its first checkpoint and the segment
+    // kernel replays the rest from the stored records.
+    const bool checkpointed = ctx->ck_every > 0u && ctx->ck_valid && ctx->ck_records;
+    uint32_t records = 0;
+    if (checkpointed) {
+        uint32_t claimed = 0;
+        SG_CUDA(ctx, cudaMemcpyAsync(&claimed, ctx->ck_count, sizeof(claimed), cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(ctx, cudaStreamSynchronize(stream));
+        records = std::min(claimed, ctx->ck_capacity);
+        a.ck.records = ctx->ck_records;
+        a.ck.count = ctx->ck_count;
+        a.ck.capacity = ctx->ck_capacity;
+        a.ck.totals = ctx->ck_totals;
+        a.ck.samples = ctx->ck_samples;
+        a.ck.every = ctx->ck_every;
+        a.ck.max_depth = ctx->options.max_bounces;
+    }
+    const bool staged = ctx->integrator == SG_INTEGRATOR_WAVEFRONT && !checkpointed;
     sg::WaveParams w{};
     sg::AdjointWave x{};
     if (staged) {
@@ -1409,10 +1526,13 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         cudaError_t e = sg::reset_adjoint_slots(x, w.pool, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint slot reset");
     }
+    uint32_t accumulated = 0;  // accumulation index of the launch's first sample
     for (uint32_t k = 0; k < tape->n_ranges; ++k) {
         for (uint32_t done = 0; done < tape->count[k]; done += SG_MAX_BATCH_SAMPLES) {
             s.sampling[0] = tape->first[k] + done;
             s.counts[2] = std::min<uint32_t>(SG_MAX_BATCH_SAMPLES, tape->count[k] - done);
+            a.ck.sample_base = accumulated;
+            accumulated += s.counts[2];
             const sg::TraceParams p = make_params(ctx, s);
             if (staged) {
                 sg::WaveRun run;
@@ -1428,6 +1548,12 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
                 ctx->launches += 1;
             }
         }
+    }
+    if (checkpointed && records > 0) {
+        const sg::TraceParams p = make_params(ctx, s);
+        cudaError_t e = sg::launch_checkpoint_segments(p, a, records, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "checkpoint segments");
+        ctx->launches += 1;
     }
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (grads->ring_tau)

@@ -41,6 +41,10 @@ struct Path {
     bool in_air;
     bool sky_on_escape;
     uint32_t sample;  // the sample's index in its dispatch (its counts.y offset)
+    // Checkpoints the forward stored for this sample (sg_set_checkpoints):
+    // bit 0 some were stored, bit 1 one did not fit (the sample then replays
+    // from its seed).
+    uint32_t ckpt;
 };
 
 // camera_direction (pathtrace.wgsl:1619-1626).
@@ -78,6 +82,7 @@ __device__ __forceinline__ void start_path(Path &p, const sg_settings *s, Counte
     p.in_air = false;
     p.sky_on_escape = false;
     p.sample = smp;
+    p.ckpt = 0;
 }
 
 // The ring-indirect cap after the loop (pathtrace.wgsl:1609-1615); W holds

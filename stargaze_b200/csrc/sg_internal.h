@@ -70,7 +70,7 @@ cudaError_t launch_terrain_cache(float *terrain, uint32_t cells, float radius_m,
 size_t terrain_floats(uint32_t cells);
 size_t terrain_source_floats(uint32_t cells);
 
-constexpr int kEventCount = 9;
+constexpr int kEventCount = SG_EVENT_COUNT;
 
 // Shared-memory bytes a launch with these parameters needs.
 size_t trace_smem_bytes(const TraceParams &p);
@@ -107,6 +107,28 @@ constexpr uint32_t kWaveCounterSets = 8;
 constexpr uint32_t kWavePlanes = 7;
 constexpr uint32_t kWaveHitPlanes = 3;
 
+// Vertex checkpoints (sg_set_checkpoints): the forward stores a path's
+// whole state each time a scatter brings its depth to a multiple of
+// `every` (up to max_depth), and every sample's radiance before the ring
+// cap with its checkpoint bits. The backward then replays each segment
+// between checkpoints on its own instead of every path from its seed.
+//   record r: kWavePlanes float4 of path state (the pool's planes), then
+//             (pixel, sample, depth, 0) — `sample` indexes the accumulation;
+//   totals[sample * pixels + pixel] = (radiance, bits): bit 0 the sample has
+//             records, bit 1 it must be replayed from its seed (a record did
+//             not fit, or its ring-indirect cap binds).
+constexpr uint32_t kCheckpointVec4 = 8;
+struct Checkpoints {
+    float4 *records;          // capacity * kCheckpointVec4 float4
+    uint32_t *count;          // records claimed (may exceed capacity)
+    uint32_t capacity;
+    float4 *totals;           // samples * pixels entries
+    uint32_t samples;         // accumulation samples `totals` covers
+    uint32_t sample_base;     // accumulation index of the dispatch's first sample
+    uint32_t every;
+    uint32_t max_depth;
+};
+
 struct WaveParams {
     float4 *state[2];         // kWavePlanes planes of `pool` float4 each
     float4 *hits;             // kWaveHitPlanes planes of `pool` float4
@@ -121,6 +143,7 @@ struct WaveParams {
     uint32_t tiles_x, tiles_y;
     uint32_t chunk_first;     // first sample of the chunk within the dispatch
     uint32_t chunk_samples;   // samples of the chunk
+    Checkpoints ck;           // vertex checkpoints of the forward (off: ck.records null)
 };
 
 // Bytes of the per-context wavefront buffers for `pool` path slots and
@@ -207,7 +230,16 @@ struct AdjointParams {
     uint32_t tau_window;              // shared-memory window over [0, tau_window)
     uint32_t color_window;            // ... and over [kGradColor, + color_window)
     unsigned long long *overflow;     // derivative entries dropped (full lists)
+    // Vertex checkpoints of the forward (ck.totals null: replay every sample
+    // from its seed). ck.sample_base: accumulation index of the launch's
+    // first sample.
+    Checkpoints ck;
 };
+
+// The segments between the forward's vertex checkpoints: one thread per
+// stored record, `records` of them (sg_set_checkpoints).
+cudaError_t launch_checkpoint_segments(const TraceParams &p, const AdjointParams &a, uint32_t records,
+                                       cudaStream_t stream);
 
 // Dynamic shared memory of an adjoint launch.
 size_t adjoint_smem_bytes(const TraceParams &p, const AdjointParams &a);

@@ -5,16 +5,19 @@
 // Kahan-compensated per-pixel sum. CTAs cover 16x16 pixel tiles and each
 // warp an 8x4 sub-tile, so neighbouring lanes trace neighbouring pixels and
 // take the same branches as long as possible.
-#include "sg_integrator.cuh"
+#include <algorithm>
+
+#include "sg_wave_common.cuh"
 
 namespace sg {
 
 namespace {
 
 __device__ __forceinline__ void flush_events(const Events &ev, unsigned long long *events) {
-    const uint32_t v[kEventCount] = {ev.vertices,    ev.sphere_tests,  ev.sphere_hits,
-                                     ev.ring_tests,  ev.light_samples, ev.shadow_rays,
-                                     ev.ring_events, ev.surface_events, ev.rng_draws};
+    const uint32_t v[kEventCount] = {ev.vertices,      ev.sphere_tests,      ev.sphere_hits, ev.ring_tests,
+                                     ev.light_samples, ev.shadow_rays,       ev.ring_events, ev.surface_events,
+                                     ev.rng_draws,     ev.terrain_nodes,     ev.terrain_triangles,
+                                     ev.prop_boxes,    ev.prop_tests};
 #pragma unroll
     for (int k = 0; k < kEventCount; ++k) {
         unsigned long long x = v[k];
@@ -104,21 +107,38 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // warp's lanes that run the same samples; they meet after each pass so that
 // a warp replays one pass at a time (lanes left to drift between the two
 // passes would run two copies of the integrator apart).
+// Replays a checkpointed path from `path` until a scatter brings its depth
+// to `end_depth`, where the next segment's record starts, or it ends.
+template <bool L, bool F>
+__device__ __forceinline__ void replay_segment(const Scene &S, Counter<false, L, F> K, Prb &G, Path &path,
+                                               uint32_t end_depth) {
+    while (!step(S, K, path, G)) {
+        if (path.depth >= end_depth) break;
+    }
+}
+
 template <bool L, bool F>
 __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L, F> K, Prb &G, float3 w, uint32_t pixel,
-                                               uint32_t x, uint32_t y, uint32_t smp, unsigned lanes) {
+                                               uint32_t x, uint32_t y, uint32_t smp, unsigned lanes,
+                                               uint32_t segment_end) {
     bool again = true;
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
         if (again) {
             Path path;
             start_path(path, S.s, K, pixel, x, y, smp);
-            while (!step(S, K, path, G)) {
-            }
-            if (pass == 0) {
-                again = G.deferral_full || cap_binds(G, path.radiance);
-                if (again) pass2_setup(G, path.radiance, w);
-                else flush_deferred(G);
+            if (segment_end) {
+                // A checkpointed sample: its first segment, once.
+                replay_segment(S, K, G, path, segment_end);
+                again = false;
+            } else {
+                while (!step(S, K, path, G)) {
+                }
+                if (pass == 0) {
+                    again = G.deferral_full || cap_binds(G, path.radiance);
+                    if (again) pass2_setup(G, path.radiance, w);
+                    else flush_deferred(G);
+                }
             }
         }
         __syncwarp(lanes);
@@ -172,13 +192,93 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     const unsigned lanes = __ballot_sync(0xffffffffu, busy);
     if (busy) {
         const uint32_t z = P.s.counts[2];
+        const uint32_t pixels = P.width * P.height;
 #pragma unroll 1
         for (uint32_t smp = 0; smp < z; ++smp) {
-            pass1_setup(G, w);
-            adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes);
+            // With the forward's checkpoints, a sample that has them (and no
+            // binding cap) replays only up to its first one; the segment
+            // kernel replays the rest.
+            uint32_t segment_end = 0;
+            if (A.ck.totals && A.ck.sample_base + smp < A.ck.samples) {
+                const float4 t = A.ck.totals[(size_t)(A.ck.sample_base + smp) * pixels + pixel];
+                if ((__float_as_uint(t.w) & 3u) == 1u) {
+                    segment_setup(G, w, f3(t.x, t.y, t.z), f3(0.0f, 0.0f, 0.0f));
+                    segment_end = A.ck.every;
+                }
+            }
+            if (!segment_end) pass1_setup(G, w);
+            adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes, segment_end);
         }
     }
     // Per-thread colour sums: reduce over the warp, then into the window.
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) {
+        float v = own[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0u && v != 0.0f) {
+            if (k < A.color_window) atomicAdd(window + A.tau_window + k, v);
+            else atomicAdd(A.grad + kGradColor + k, v);
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) {
+        const float v = window[k];
+        if (v != 0.0f) atomicAdd(A.grad + (k < A.tau_window ? k : kGradColor + (k - A.tau_window)), v);
+    }
+    unsigned long long dropped = G.dropped;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dropped += __shfl_down_sync(0xffffffffu, dropped, o);
+    if (lane == 0u && dropped != 0ull && A.overflow) atomicAdd(A.overflow, dropped);
+}
+
+// The segments between vertex checkpoints: one thread per record of the
+// forward (Checkpoints), replaying from the stored state with the weights of
+// the path's known total until the next checkpoint depth or the path's end.
+// Gradient sinks as in adjoint_kernel.
+template <bool L, bool F>
+__global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
+    segment_kernel(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A, uint32_t records) {
+    extern __shared__ float4 smem[];
+    const uint32_t n_bodies = P.s.counts[0];
+    float4 *inv = smem + trace_smem_floats(P) / 4u;
+    float *window = reinterpret_cast<float *>(inv + 2u * n_bodies);
+    const uint32_t window_n = A.tau_window + A.color_window;
+    for (uint32_t k = threadIdx.x; k < window_n; k += blockDim.x) window[k] = 0.0f;
+    for (uint32_t k = threadIdx.x; k < n_bodies; k += blockDim.x) {
+        const float4 m = P.bodies[k * kBodyVec4 + kMaterial], r = P.bodies[k * kBodyVec4 + kRingColor];
+        inv[2u * k] = make_float4(inv_or_zero(m.x), inv_or_zero(m.y), inv_or_zero(m.z), 0.0f);
+        inv[2u * k + 1u] = make_float4(inv_or_zero(r.x), inv_or_zero(r.y), inv_or_zero(r.z), 0.0f);
+    }
+    const Scene S = stage_scene(P, smem);  // synchronises the block
+    const Counter<false, L, F> K{nullptr};
+    const uint32_t lane = threadIdx.x & 31u;
+    float own[6u * kColorSlots];
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
+    const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
+    PrbLists lists;
+    Prb G;
+    G.lists = &lists;
+    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.inv = inv;
+    G.dropped = 0;
+    const uint32_t pixels = P.width * P.height;
+#pragma unroll 1
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < records; r += gridDim.x * blockDim.x) {
+        Path path;
+        const uint3 key = load_checkpoint(A.ck, r, path);  // (pixel, sample, depth)
+        path.backdrop = f3(0.0f, 0.0f, 0.0f);
+        path.sample = 0u;
+        const float4 t = A.ck.totals[(size_t)key.y * pixels + key.x];
+        if (__float_as_uint(t.w) & 2u) continue;  // replayed from its seed
+        const float4 d = A.dl_dimage[key.x];
+        const float3 w = f3(d.x, d.y, d.z) * A.inv_samples;
+        if (w.x == 0.0f && w.y == 0.0f && w.z == 0.0f) continue;
+        segment_setup(G, w, f3(t.x, t.y, t.z), path.radiance);
+        const uint32_t next = key.z + A.ck.every;
+        replay_segment(S, K, G, path, next <= A.ck.max_depth ? next : 0xffffffffu);
+    }
 #pragma unroll
     for (uint32_t k = 0; k < 6u * kColorSlots; ++k) {
         float v = own[k];
@@ -276,8 +376,8 @@ __global__ void __launch_bounds__(kThreads) terrain_probe_kernel(const __grid_co
     if (P.terrain) {
         const float3 o = f3(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]);
         const float3 d = f3(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
-        result = terrain_query(P.terrain, P.terrain_cells, P.s.g.ground_up[3], (P.s.g.ground_counts[2] & 255u) == 3u,
-                               o, d, 1.0e29f, false);
+        result = terrain_query<false>(P.terrain, P.terrain_cells, P.s.g.ground_up[3],
+                                      (P.s.g.ground_counts[2] & 255u) == 3u, o, d, 1.0e29f, false, nullptr);
     }
     out[4 * k + 0] = result.x;
     out[4 * k + 1] = result.y;
@@ -490,6 +590,32 @@ cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStr
         case 2: return launch_variant(adjoint_kernel<true, false>, grid, smem, stream, p, a);
         default: return launch_variant(adjoint_kernel<true, true>, grid, smem, stream, p, a);
     }
+}
+
+cudaError_t launch_checkpoint_segments(const TraceParams &p, const AdjointParams &a, uint32_t records,
+                                       cudaStream_t stream) {
+    if (records == 0) return cudaSuccess;
+    const size_t smem = adjoint_smem_bytes(p, a);
+    const bool land = p.s.g.ground_north[3] != 0.0f;
+    const void *fn;
+    switch ((land ? 2 : 0) | (p.fp64_sites ? 1 : 0)) {
+        case 0: fn = (const void *)segment_kernel<false, false>; break;
+        case 1: fn = (const void *)segment_kernel<false, true>; break;
+        case 2: fn = (const void *)segment_kernel<true, false>; break;
+        default: fn = (const void *)segment_kernel<true, true>; break;
+    }
+    int grid = 0;
+    cudaError_t e = set_smem(fn, smem);
+    if (e == cudaSuccess) e = persistent_grid(fn, smem, &grid);
+    if (e != cudaSuccess) return e;
+    grid = (int)std::min<uint32_t>((uint32_t)grid, (records + kThreads - 1) / kThreads);
+    switch ((land ? 2 : 0) | (p.fp64_sites ? 1 : 0)) {
+        case 0: segment_kernel<false, false><<<grid, kThreads, smem, stream>>>(p, a, records); break;
+        case 1: segment_kernel<false, true><<<grid, kThreads, smem, stream>>>(p, a, records); break;
+        case 2: segment_kernel<true, false><<<grid, kThreads, smem, stream>>>(p, a, records); break;
+        default: segment_kernel<true, true><<<grid, kThreads, smem, stream>>>(p, a, records); break;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_closest_hit(const TraceParams &p, const sg_ray *rays, sg_hit *hits, uint32_t n,

@@ -242,9 +242,10 @@ __device__ __forceinline__ float2 t_interval(const float *T, uint32_t cells, flo
 
 // terrain_query (terrain.wgsl:152-234): near-to-far min/max quadtree.
 // Returns (normal, distance); distance 1e30 on a miss.
+// With C, `ev` counts the interior nodes expanded and the triangles tested.
+template <bool C>
 static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cells, float radius, bool alpine, float3 o,
-                                                    float3 d,
-                                             float initial_limit, bool occlusion) {
+                                                    float3 d, float initial_limit, bool occlusion, Events *ev) {
     float4 result = make_float4(0.0f, 0.0f, 0.0f, 1.0e30f);
     float limit = initial_limit;
     const float scale = t_scale_r(radius);
@@ -268,6 +269,7 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
             for (uint32_t z = node.y; z < node.y + 2u; ++z) {
 #pragma unroll 1
                 for (uint32_t x = node.x; x < node.x + 2u; ++x) {
+                    if constexpr (C) ev->terrain_triangles += 2u;
                     const float3 a = t_vertex(T, cells, scale, x, z);
                     const float3 b = t_vertex(T, cells, scale, x + 1u, z);
                     const float3 c = t_vertex(T, cells, scale, x, z + 1u);
@@ -295,6 +297,7 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
                 }
             }
         } else {
+            if constexpr (C) ev->terrain_nodes += 1u;
             uint32_t children[4];
             float distances[4];
 #pragma unroll
@@ -427,8 +430,8 @@ static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K,
     }
     if (s->g.ground_counts[1] != 0u && S.p->terrain) {
         const float tl = __fmul_rn(fminf(closest.t, 1.0e18f), kMetresPerAu);
-        const float4 terrain = terrain_query(S.p->terrain, S.p->terrain_cells, radius,
-                                             (S.s->g.ground_counts[2] & 255u) == 3u, o, d, tl, occlusion);
+        const float4 terrain = terrain_query<C>(S.p->terrain, S.p->terrain_cells, radius,
+                                                (S.s->g.ground_counts[2] & 255u) == 3u, o, d, tl, occlusion, K.ev);
         if (terrain.w < tl && terrain.w < 1.0e29f) {
             closest = LandHit{__fdiv_rn(terrain.w, kMetresPerAu), kTerrainId, 0.0f, from_ground(S, xyz(terrain))};
             if (occlusion) return closest;
@@ -444,11 +447,13 @@ static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K,
         const float kind = oc.w;
         if (kind < 0.0f) {
             // Group marker: skip the subtree when its bounds are missed.
+            K.add(&Events::prop_boxes);
             const float2 bounds = box_interval(sub_rn(o, center), d, e);
             if (bounds.x > bounds.y || bounds.y <= 0.001f || __fdiv_rn(bounds.x, kMetresPerAu) > closest.t)
                 i += (uint32_t)(-kind);
             continue;
         }
+        K.add(&Events::prop_tests);
         float3 p = sub_rn(o, center), v = d;
         const float4 t0 = S.p->prop_trig[2u * i], t1 = S.p->prop_trig[2u * i + 1u];
         if (kind == 2.25f) {

@@ -70,6 +70,7 @@ __device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, fl
     const uint32_t flags = __float_as_uint(s2.w);
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = (flags & kFlagPass2) != 0u;
+    G.known_total = false;
     G.a = xyz4(s0);
     G.cap = s0.w;
     G.base = xyz4(s1);

@@ -30,7 +30,8 @@ namespace {
 //   1  ray.d, rng                   5  previous_vertex.o, previous_vertex.anchor
 //   2  throughput, previous_pdf     6  iterations | point_gained << 31,
 //   3  radiance, ring_cap              depth | null_crossings << 16 | in_air << 30
-//                                      | sky_on_escape << 31, result slot
+//                                      | sky_on_escape << 31, result slot,
+//                                      checkpoint bits
 // The previous vertex is only ever used for its position (relative_center),
 // so its direction is not stored.
 __device__ __forceinline__ float4 pack3(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
@@ -53,7 +54,7 @@ __device__ __forceinline__ void store_path(float4 *st, uint32_t pool, uint32_t i
     st[3 * pool + i] = pack3(p.radiance, p.ring_cap);
     st[4 * pool + i] = pack3u(p.ring_base, p.shine_body);
     st[5 * pool + i] = pack3u(p.previous_vertex.o, p.previous_vertex.anchor);
-    st[6 * pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot), 0.0f);
+    st[6 * pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot), __uint_as_float(p.ckpt));
 }
 
 // Planes 0, 1 and 6: what extend reads. Returns the result slot.
@@ -69,6 +70,7 @@ __device__ __forceinline__ uint32_t load_ray_part(const float4 *st, uint32_t poo
     p.in_air = (dn & 0x40000000u) != 0u;
     p.sky_on_escape = (dn & 0x80000000u) != 0u;
     p.backdrop = f3(0.0f, 0.0f, 0.0f);  // set only where a path escapes, which ends it
+    p.ckpt = __float_as_uint(g.w);
     return __float_as_uint(g.z);
 }
 
@@ -88,6 +90,46 @@ __device__ __forceinline__ void load_shade_part(const float4 *st, uint32_t pool,
     p.throughput = xyz4(c);
     p.previous_pdf = c.w;
     p.previous_vertex = Ray{xyz4(e), f3(0.0f, 0.0f, 0.0f), __float_as_uint(e.w)};
+}
+
+// ---------------------------------------------------------------------------
+// Vertex checkpoints (Checkpoints in sg_internal.h)
+// ---------------------------------------------------------------------------
+// The ring-indirect cap clamps this finished path (as finish_path does).
+__device__ __forceinline__ bool cap_clamps(const Path &p) {
+    return p.ring_cap < 1.0e29f && luminance(p.radiance - p.ring_base) > p.ring_cap;
+}
+
+// Accumulation index of the chunk sample behind result slot `slot`.
+__device__ __forceinline__ uint32_t checkpoint_sample(const Checkpoints &ck, uint32_t chunk_first, uint32_t pixels,
+                                                      uint32_t slot) {
+    return ck.sample_base + chunk_first + slot / pixels;
+}
+
+// A path's end: its radiance before the cap and its checkpoint bits.
+__device__ __forceinline__ void checkpoint_total(const Checkpoints &ck, uint32_t chunk_first, uint32_t pixels,
+                                                 uint32_t slot, const Path &p) {
+    const uint32_t sample = checkpoint_sample(ck, chunk_first, pixels, slot);
+    if (sample >= ck.samples) return;
+    ck.totals[(size_t)sample * pixels + slot % pixels] = pack3u(p.radiance, p.ckpt | (cap_clamps(p) ? 2u : 0u));
+}
+
+// Record `r`: the path's state as the pool stores it, then its key.
+__device__ __forceinline__ void store_checkpoint(const Checkpoints &ck, uint32_t r, const Path &p, uint32_t pixel,
+                                                 uint32_t sample) {
+    float4 *rec = ck.records + (size_t)r * kCheckpointVec4;
+    store_path(rec, 1u, 0u, p, 0u);
+    rec[kWavePlanes] = make_float4(__uint_as_float(pixel), __uint_as_float(sample), __uint_as_float(p.depth), 0.0f);
+}
+
+// Loads record `r` into a path; returns its key (pixel, sample, depth).
+__device__ __forceinline__ uint3 load_checkpoint(const Checkpoints &ck, uint32_t r, Path &p) {
+    const float4 *rec = ck.records + (size_t)r * kCheckpointVec4;
+    load_ray_part(rec, 1u, 0u, p);
+    load_radiance_part(rec, 1u, 0u, p);
+    load_shade_part(rec, 1u, 0u, p);
+    const float4 key = rec[kWavePlanes];
+    return make_uint3(__float_as_uint(key.x), __float_as_uint(key.y), __float_as_uint(key.z));
 }
 
 // ---------------------------------------------------------------------------

@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                         store_path(st, W.pool, i, p, slot);
                     } else {
                         st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
-                        st[6 * W.pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot), 0.0f);
+                        st[6 * W.pool + i] = make_float4(iteration_word(p), depth_word(p), __uint_as_float(slot),
+                                                         __uint_as_float(p.ckpt));
                         if (was_in_air) st[2 * W.pool + i] = pack3(p.throughput, p.previous_pdf);
                     }
                     if (ring) H[1 * W.pool + i] = pack3(e.ring.p, e.ring.t);
@@ -141,6 +142,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                     }
                     W.results[slot] = finish_path(p);
                     if (W.sky_results) W.sky_results[slot] = pack3(p.backdrop, 0.0f);
+                    if (W.ck.records) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
                 }
             }
         }
@@ -153,13 +155,15 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
     }
 }
 
-// Ring (R == true) or surface stage over its queue.
-template <bool L, bool F, bool R, bool A>
+// Ring (R == true) or surface stage over its queue. CK: the forward stores
+// vertex checkpoints (W.ck).
+template <bool L, bool F, bool R, bool A, bool CK = false>
 __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
                                                                            const __grid_constant__ WaveParams W,
                                                                            uint32_t t) {
     extern __shared__ float4 smem[];
-    __shared__ Append<1> sm[2];
+    constexpr int kQueues = CK ? 2 : 1;
+    __shared__ Append<kQueues> sm[2];
     WaveCounters *c = counters(W, t);
     const uint32_t n = R ? c->ring : c->surface;
     if (blockIdx.x * kThreads >= n) return;
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
     uint32_t round = 0;
     for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
         const uint32_t j = base + threadIdx.x;
-        bool keep = false;
+        bool keep = false, record = false;
         Path p;
         uint32_t slot = 0;
         if (j < n) {
@@ -181,6 +185,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
             slot = load_ray_part(st, W.pool, i, p);
             load_radiance_part(st, W.pool, i, p);
             load_shade_part(st, W.pool, i, p);
+            const uint32_t depth_before = p.depth;
             const float4 h2 = H[2 * W.pool + i];
             bool ended;
             if constexpr (R) {
@@ -196,13 +201,36 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
             if (ended) {
                 W.results[slot] = finish_path(p);
                 if (W.sky_results) W.sky_results[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if constexpr (CK) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
+            }
+            if constexpr (CK) {
+                // A scatter brought the depth to a checkpoint depth.
+                record = keep && p.depth != depth_before && p.depth % W.ck.every == 0u && p.depth <= W.ck.max_depth &&
+                         checkpoint_sample(W.ck, W.chunk_first, P.width * P.height, slot) < W.ck.samples;
             }
         }
-        const bool flags[1] = {keep};
-        uint32_t *const ctr[1] = {&counters(W, t + 1u)->cont};
-        uint32_t q[1];
-        block_append<1>(sm[round & 1u], flags, ctr, q);
-        if (keep) store_path(out, W.pool, q[0], p, slot);
+        if constexpr (CK) {
+            const bool flags[2] = {keep, record};
+            uint32_t *const ctr[2] = {&counters(W, t + 1u)->cont, W.ck.count};
+            uint32_t q[2];
+            block_append<2>(sm[round & 1u], flags, ctr, q);
+            if (record) {
+                if (q[1] < W.ck.capacity) {
+                    p.ckpt |= 1u;
+                    const uint32_t pixels = P.width * P.height;
+                    store_checkpoint(W.ck, q[1], p, slot % pixels, checkpoint_sample(W.ck, W.chunk_first, pixels, slot));
+                } else {
+                    p.ckpt |= 2u;
+                }
+            }
+            if (keep) store_path(out, W.pool, q[0], p, slot);
+        } else {
+            const bool flags[1] = {keep};
+            uint32_t *const ctr[1] = {&counters(W, t + 1u)->cont};
+            uint32_t q[1];
+            block_append<1>(sm[round & 1u], flags, ctr, q);
+            if (keep) store_path(out, W.pool, q[0], p, slot);
+        }
     }
 }
 
@@ -261,22 +289,22 @@ struct StageSet {
     const void *extend, *ring, *surface;
 };
 
-template <bool L, bool F, bool A>
+template <bool L, bool F, bool A, bool CK = false>
 StageSet stage_set() {
-    return StageSet{(const void *)wave_extend<L, F, A>, (const void *)wave_shade<L, F, true, A>,
-                    (const void *)wave_shade<L, F, false, A>};
+    return StageSet{(const void *)wave_extend<L, F, A>, (const void *)wave_shade<L, F, true, A, CK>,
+                    (const void *)wave_shade<L, F, false, A, CK>};
 }
 
-template <bool L, bool F, bool A>
+template <bool L, bool F, bool A, bool CK = false>
 cudaError_t run_iteration(const TraceParams &p, const WaveParams &w, uint32_t t, const int (&grid)[3], size_t smem,
                           cudaStream_t stream, StageMarks *m) {
     cudaError_t e;
     if ((e = mark(m, kStageExtend, stream)) != cudaSuccess) return e;
     wave_extend<L, F, A><<<grid[0], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageRing, stream)) != cudaSuccess) return e;
-    wave_shade<L, F, true, A><<<grid[1], kThreads, smem, stream>>>(p, w, t);
+    wave_shade<L, F, true, A, CK><<<grid[1], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageSurface, stream)) != cudaSuccess) return e;
-    wave_shade<L, F, false, A><<<grid[2], kThreads, smem, stream>>>(p, w, t);
+    wave_shade<L, F, false, A, CK><<<grid[2], kThreads, smem, stream>>>(p, w, t);
     if ((e = mark(m, kStageGap, stream)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -300,7 +328,11 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
     if (marks) marks->used = 0;
     if (z == 0 || pixels == 0) return cudaSuccess;
     const bool land = p.s.g.ground_north[3] != 0.0f;
-    const int variant = (p.air_on || p.styled ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
+    // Checkpoints are stored for the frames the adjoint differentiates
+    // (no air, no styles): variants 8-11.
+    const bool ck = w.ck.records != nullptr;
+    if (ck && (p.air_on || p.styled)) return cudaErrorInvalidValue;
+    const int variant = (ck ? 8 : 0) | (p.air_on || p.styled ? 4 : 0) | (land ? 2 : 0) | (p.fp64_sites ? 1 : 0);
     StageSet set;
     switch (variant) {
         case 0: set = stage_set<false, false, false>(); break;
@@ -310,7 +342,11 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
         case 4: set = stage_set<false, false, true>(); break;
         case 5: set = stage_set<false, true, true>(); break;
         case 6: set = stage_set<true, false, true>(); break;
-        default: set = stage_set<true, true, true>(); break;
+        case 7: set = stage_set<true, true, true>(); break;
+        case 8: set = stage_set<false, false, false, true>(); break;
+        case 9: set = stage_set<false, true, false, true>(); break;
+        case 10: set = stage_set<true, false, false, true>(); break;
+        default: set = stage_set<true, true, false, true>(); break;
     }
     const size_t smem = trace_smem_bytes(p);
     const void *fns[3] = {set.extend, set.ring, set.surface};
@@ -358,7 +394,11 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
                 case 4: e = run_iteration<false, false, true>(p, w, it, grid, smem, stream, marks); break;
                 case 5: e = run_iteration<false, true, true>(p, w, it, grid, smem, stream, marks); break;
                 case 6: e = run_iteration<true, false, true>(p, w, it, grid, smem, stream, marks); break;
-                default: e = run_iteration<true, true, true>(p, w, it, grid, smem, stream, marks); break;
+                case 7: e = run_iteration<true, true, true>(p, w, it, grid, smem, stream, marks); break;
+                case 8: e = run_iteration<false, false, false, true>(p, w, it, grid, smem, stream, marks); break;
+                case 9: e = run_iteration<false, true, false, true>(p, w, it, grid, smem, stream, marks); break;
+                case 10: e = run_iteration<true, false, false, true>(p, w, it, grid, smem, stream, marks); break;
+                default: e = run_iteration<true, true, false, true>(p, w, it, grid, smem, stream, marks); break;
             }
             if (e != cudaSuccess) return e;
             run->iterations += 1;

@@ -126,6 +126,21 @@ class PathTracer:
         restarts the accumulation."""
         check(self._lib.sg_set_ringshine(self._ctx, int(bool(enable))), self._ctx)
 
+    def set_checkpoints(self, every: int, max_samples: int = 0, record_bytes: int = 0) -> None:
+        """Vertex checkpoints for backward() (extension): with `every` > 0
+        the forward stores each path's state every `every` bounces and the
+        radiance of the accumulation's first `max_samples` samples, and the
+        adjoint replays segments between checkpoints instead of whole paths
+        from their seeds. 0 turns it off."""
+        check(self._lib.sg_set_checkpoints(self._ctx, int(every), int(max_samples), int(record_bytes)), self._ctx)
+
+    def checkpoint_stats(self) -> dict:
+        """Device bytes the checkpoints hold, records stored and records
+        that did not fit."""
+        b, r, d = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(self._lib.sg_get_checkpoint_stats(self._ctx, C.byref(b), C.byref(r), C.byref(d)), self._ctx)
+        return {"device_bytes": b.value, "records": r.value, "dropped": d.value}
+
     def set_integrator(self, integrator: str, pool_paths: int = 0) -> None:
         """"wavefront" (default; stage kernels over a pool of `pool_paths`
         paths in device memory, 0 = default pool) or "megakernel" (one

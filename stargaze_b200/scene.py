@@ -148,7 +148,11 @@ class Body:
     luminosity_w: float = 0.0
     emission: tuple[float, float, float] = (1.0, 1.0, 1.0)
     ring: Ring | None = None
-    mottle: float = 0.0
+    # Strength of the value-noise mottle of style-0 albedo (center_low.w,
+    # pathtrace.wgsl:912-923): build_frame sets 1 on every body that is not a
+    # star (src/main.rs:907); the reference's test and benchmark fixtures
+    # use 0 (src/render_benchmark.rs:272-288).
+    mottle: float = 1.0
 
     @property
     def star(self) -> bool:

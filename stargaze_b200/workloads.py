@@ -87,11 +87,26 @@ def ring_tau_profile(bins: int = 512, seed: int = 0, gaps: int = 12) -> np.ndarr
     return np.clip(tau, 0.0, 2.0).astype(np.float32)
 
 
+# The benchmark scenes have Lambertian bodies of constant albedo: mottle 0,
+# as the reference's own test and benchmark fixtures set it
+# (src/render_benchmark.rs:272-288); with_mottle() turns it on as the app's
+# build_frame does.
+
+
+def with_mottle(frame, strength: float = 1.0):
+    """center_low.w = `strength` on every body that is not a star
+    (src/main.rs:907): the style-0 albedo's value-noise mottle."""
+    for b in frame.bodies:
+        if b.emissive < 0.5:
+            b.center_low[3] = strength
+    return frame
+
+
 def spheres_256(width: int = 256, height: int = 256, spp: int = 64) -> Workload:
     star = Body(np.array([1.5e11, 0.0, 0.0]), 7.0e8, luminosity_w=3.8e26)
-    host = Body(np.zeros(3), 6.4e6, albedo=(0.3, 0.3, 0.3))
+    host = Body(np.zeros(3), 6.4e6, albedo=(0.3, 0.3, 0.3), mottle=0.0)
     moon_dir = np.array([math.cos(math.radians(100.0)), math.sin(math.radians(100.0)), 0.0])
-    moon = Body(3.84e8 * moon_dir, 1.74e6, albedo=(0.12, 0.12, 0.12))
+    moon = Body(3.84e8 * moon_dir, 1.74e6, albedo=(0.12, 0.12, 0.12), mottle=0.0)
     bodies = [star, host, moon]
     view = aim(host, math.radians(35.0), math.radians(30.0), 2.0, moon.position_m)
     frame = pack_frame(bodies, view, width, height, math.radians(60.0), host_index=1, height_m=2.0)
@@ -112,10 +127,10 @@ def rings_1080p(width: int = 1920, height: int = 1080, spp: int = 256, max_bounc
     side /= np.linalg.norm(side)
     off = math.radians(8.0)
     moon_dir = math.cos(off) * to_star + math.sin(off) * side
-    moon = Body(planet_pos + 2.0e8 * moon_dir, 1.5e6, albedo=(0.12, 0.12, 0.12))
+    moon = Body(planet_pos + 2.0e8 * moon_dir, 1.5e6, albedo=(0.12, 0.12, 0.12), mottle=0.0)
     pole = np.array([0.3, 0.2, 0.93])
     ring = Ring(7.4e7, 1.37e8, (0.5, 0.5, 0.5), optical_depth=1.0, table_slot=0, pole=pole / np.linalg.norm(pole))
-    planet = Body(planet_pos, 5.8e7, albedo=(0.5, 0.5, 0.5), ring=ring)
+    planet = Body(planet_pos, 5.8e7, albedo=(0.5, 0.5, 0.5), ring=ring, mottle=0.0)
     bodies = [star_a, star_b, planet, moon]
     # Camera zenith: rotate the moon-to-planet direction 60 degrees towards
     # the ring pole so the planet stands 30 degrees above the horizon.
@@ -161,7 +176,7 @@ def terrain_1080p(width: int = 1920, height: int = 1080, spp: int = 128, cells: 
     terrain = T.pack_terrain(heights, cells)
 
     R = 6.4e6
-    host = Body(np.zeros(3), R, albedo=(0.3, 0.3, 0.3))
+    host = Body(np.zeros(3), R, albedo=(0.3, 0.3, 0.3), mottle=0.0)
     lat, lon = math.radians(35.0), math.radians(30.0)
     base = aim(host, lat, lon, observer_m, np.array([1.0e9, 0.0, 0.0]))
     # Star: azimuth 140 degrees (south-east), 20 degrees above the horizon.

@@ -27,7 +27,7 @@ import known_answers as ka  # noqa: E402
 from stargaze_b200 import abi  # noqa: E402
 from stargaze_b200.pathtracer import rays_array  # noqa: E402
 from stargaze_b200.scene import body, frame  # noqa: E402
-from stargaze_b200.workloads import rings_1080p, spheres_256, terrain_1080p, with_air  # noqa: E402
+from stargaze_b200.workloads import rings_1080p, spheres_256, terrain_1080p, with_air, with_mottle  # noqa: E402
 
 N_RAYS = 2048
 
@@ -151,6 +151,7 @@ IMAGES = {
     "terrain_dunes_96x54": (None, 96, 54, 16, 2),
     "terrain_basalt_96x54": (None, 96, 54, 16, 2),
     "terrain_vegetation_96x54": (None, 96, 54, 16, 2),
+    "mottled_96x54": (rings_1080p, 96, 54, 16, 2),
 }
 
 # Landscape themes of the terrain images (ground_counts.z low byte).
@@ -197,7 +198,11 @@ def image_workload(name):
         if "vegetation" in name:
             vegetate(wl.frame)
         return wl, land
-    return factory(width=w, height=h), None
+    wl = factory(width=w, height=h)
+    if name.startswith("mottled"):
+        # The ring workload with the app's mottle on every non-star body.
+        with_mottle(wl.frame)
+    return wl, None
 
 
 def image_fixture(name):

@@ -9,7 +9,7 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 RAY_SCENES = ["transport", "spheres_256", "rings_1080p", "shadow_ring", "terrain", "vegetation"]
 IMAGE_NAMES = ["spheres_64", "rings_96x54", "terrain_96x54", "terrain_air_96x54", "styles_96x32",
                "terrain_alpine_96x54", "terrain_dunes_96x54", "terrain_basalt_96x54",
-               "terrain_vegetation_96x54"]
+               "terrain_vegetation_96x54", "mottled_96x54"]
 
 
 def load_rays(name: str) -> dict:

@@ -57,6 +57,25 @@ def test_noalloc_closest_hit_equals_sg_closest_hit(scene):
         assert (hits["index"] != abi.MISS).any()
 
 
+def test_noalloc_closest_hit_allocates_no_device_memory():
+    """After a first call (which loads the kernel and looks up the array's
+    address), a call at the largest size leaves the device's free memory
+    unchanged."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    wl = W.rings_1080p(width=64, height=64)
+    status, _ = noalloc_closest_hit(lib, wl.frame, seeded_rays(wl.frame, 64, 5))
+    assert status == abi.SG_OK, lib.sg_last_error(None)
+    rays = seeded_rays(wl.frame, abi.NOALLOC_MAX_RAYS, 6)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(0)
+    status, hits = noalloc_closest_hit(lib, wl.frame, rays)
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert status == abi.SG_OK, lib.sg_last_error(None)
+    assert (hits["index"] != abi.MISS).any()
+    assert free_after == free_before
+
+
 def test_noalloc_closest_hit_rejects_what_it_cannot_stage():
     lib = _lib.load()
     wl = W.spheres_256(width=64, height=64)
