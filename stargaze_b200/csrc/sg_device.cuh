@@ -232,16 +232,26 @@ struct LandHit {
 template <bool C, bool L, bool F>
 static __device__ SG_HELPER LandHit landscape_query(Scene S, Counter<C, L, F> K, Ray ray, float limit, bool occlusion);
 
+// Bodies and rings a ray is tested against: a camera ray takes its tile's
+// cull masks (TraceParams::camera_cull), every other ray all of them. A
+// cleared bit is a test that would miss, so skipping it changes nothing.
+struct Cull {
+    uint32_t bodies, rings;
+    __device__ __forceinline__ bool body(uint32_t i) const { return i >= 32u || ((bodies >> i) & 1u); }
+    __device__ __forceinline__ bool ring(uint32_t i) const { return i >= 32u || ((rings >> i) & 1u); }
+};
+constexpr Cull kTestAll{0xffffffffu, 0xffffffffu};
+
 // closest_hit (pathtrace.wgsl:173-185): every body except the landscape
 // host, then the landscape.
 template <bool C, bool L, bool F>
-__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C, L, F> K, const Ray &r) {
+__device__ __forceinline__ Hit closest_hit(const Scene &S, Counter<C, L, F> K, const Ray &r, Cull cull = kTestAll) {
     Hit best{1.0e30f, kMiss, 0.0f, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
     const float host = S.s->g.ground_north[3];
 #pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
-        if (host == (float)(i + 1u)) continue;
+        if (host == (float)(i + 1u) || !cull.body(i)) continue;
         float delta;
         const float t = sphere_distance(S, K, r, i, b_radius(S, i), delta);
         if (t < best.t) best = Hit{t, i, delta, f3(0.0f, 0.0f, 0.0f)};
@@ -395,11 +405,13 @@ __device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L, F> K, 
 
 // closest_ring (rings.wgsl:36-45).
 template <bool C, bool L, bool F>
-__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C, L, F> K, const Ray &r, float limit) {
+__device__ __forceinline__ RingHit closest_ring(const Scene &S, Counter<C, L, F> K, const Ray &r, float limit,
+                                                Cull cull = kTestAll) {
     RingHit best{limit, kMiss, f3(0.0f, 0.0f, 0.0f)};
     const uint32_t n = S.s->counts[0];
 #pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
+        if (!cull.ring(i)) continue;
         const RingHit h = ring_hit(S, K, r, i);
         if (h.index != kMiss && h.t < best.t) best = h;
     }
@@ -749,7 +761,8 @@ struct DiscHit {
 // point_disc_hit (pathtrace.wgsl:1308-1333): depth-0 camera rays see an
 // unresolved body as a disc of at least a bright star's size.
 template <bool C, bool L, bool F>
-static __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, Ray r, Hit closest, uint32_t rng) {
+static __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, Ray r, Hit closest, uint32_t rng,
+                                                   Cull cull = kTestAll) {
     const sg_settings *s = S.s;
     DiscHit out{closest, 1.0f, rng};
     float total = 0.0f;
@@ -759,7 +772,7 @@ static __device__ SG_HELPER DiscHit point_disc_hit(Scene S, Counter<C, L, F> K, 
     const uint32_t n = s->counts[0];
 #pragma unroll 1
     for (uint32_t i = 0; i < n; ++i) {
-        if (i == host || s->g.ground_north[3] == (float)(i + 1u)) continue;
+        if (i == host || s->g.ground_north[3] == (float)(i + 1u) || !cull.body(i)) continue;
         const float radius = b_radius(S, i);
         const float drawn = __fmul_rn(angle, length_rn(relative_center(S, r, i)));
         if (radius <= 0.0f || drawn <= radius) continue;

@@ -131,6 +131,8 @@ struct sg_context {
     size_t ck_totals_size = 0;
     uint32_t *ck_count = nullptr;
     bool ck_valid = false;                  // every sample so far went through the checkpointing forward
+    uint2 *camera_cull = nullptr;           // per-tile cull masks of camera rays
+    size_t camera_cull_tiles = 0;
 };
 
 namespace {
@@ -524,6 +526,7 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->ck_records);
     cudaFree(ctx->ck_totals);
     cudaFree(ctx->ck_count);
+    cudaFree(ctx->camera_cull);
     cudaFree(ctx->exposure);
     cudaFree(ctx->histogram);
     cudaFree(ctx->catalogue);
@@ -923,6 +926,21 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
         if (events) {
             SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
             p.events = ctx->events;
+        } else if (frame->n_bodies <= 32u) {
+            // Camera rays test only the bodies and rings their tile can see.
+            const size_t tiles = (size_t)((ctx->width + 15u) / 16u) * ((ctx->height + 15u) / 16u);
+            if (ctx->camera_cull_tiles < tiles) {
+                cudaStreamSynchronize(stream);
+                cudaFree(ctx->camera_cull);
+                ctx->camera_cull = nullptr;
+                ctx->camera_cull_tiles = 0;
+                SG_CUDA(ctx, cudaMalloc(&ctx->camera_cull, tiles * sizeof(uint2)));
+                ctx->camera_cull_tiles = tiles;
+            }
+            cudaError_t e = sg::launch_camera_cull(p, ctx->camera_cull, stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "camera cull masks");
+            ctx->launches += 1;
+            p.camera_cull = ctx->camera_cull;
         }
         const bool checkpointing = ctx->ck_every > 0u && !events && ctx->integrator == SG_INTEGRATOR_WAVEFRONT &&
                                    !p.air_on && !p.styled && !p.sky_on;

@@ -165,8 +165,11 @@ struct Extension {
 // the iteration bound, the closest hit, the depth-0 point-disc test and the
 // closest ring crossing before the hit. Returns false when the path has
 // ended at the bound.
+// `cull`: the tile's masks for a camera ray (its first extend), else
+// kTestAll.
 template <bool C, bool L, bool F, class G>
-__device__ __forceinline__ bool extend(const Scene &S, Counter<C, L, F> K, Path &p, G &grad, Extension &e) {
+__device__ __forceinline__ bool extend(const Scene &S, Counter<C, L, F> K, Path &p, G &grad, Extension &e,
+                                       Cull cull = kTestAll) {
     const sg_settings *s = S.s;
     const uint32_t max_vertices = s->counts[3];
     const uint32_t n_bodies = s->counts[0];
@@ -175,15 +178,15 @@ __device__ __forceinline__ bool extend(const Scene &S, Counter<C, L, F> K, Path 
     if (++p.iterations > max_vertices * (n_bodies + 2u) + 1u) return false;
     if constexpr (G::adjoint) grad.iteration = p.iterations;
     K.add(&Events::vertices);
-    e.hit = closest_hit(S, K, p.ray);
+    e.hit = closest_hit(S, K, p.ray, cull);
     e.disc_scale = 1.0f;
     if (p.depth == 0u && p.null_crossings == 0u && s->background[3] > 0.0f) {
-        const DiscHit disc = point_disc_hit(S, K, p.ray, e.hit, p.rng);
+        const DiscHit disc = point_disc_hit(S, K, p.ray, e.hit, p.rng, cull);
         e.hit = disc.hit;
         e.disc_scale = disc.scale;
         p.rng = disc.rng;
     }
-    e.ring = closest_ring(S, K, p.ray, e.hit.t);
+    e.ring = closest_ring(S, K, p.ray, e.hit.t, cull);
     if constexpr (G::air) {
         if (S.p->air_on) air_extend(S, K, p, e.hit, e.ring);
     }
@@ -546,11 +549,21 @@ __device__ __forceinline__ bool surface_vertex(const Scene &S, Counter<C, L, F> 
 // whose second scatters derivatives. Hooks never change the path's own
 // arithmetic or random draws, so every replay takes the same decisions.
 template <bool C, bool L, bool F, class G>
-__device__ __forceinline__ bool step(const Scene &S, Counter<C, L, F> K, Path &p, G &grad) {
+__device__ __forceinline__ bool step(const Scene &S, Counter<C, L, F> K, Path &p, G &grad, Cull cull = kTestAll) {
     Extension e;
-    if (!extend(S, K, p, grad, e)) return true;
+    if (!extend(S, K, p, grad, e, cull)) return true;
     if (e.ring.index != kMiss) return ring_vertex(S, K, p, e.ring, grad);
     return surface_vertex(S, K, p, e.hit, e.disc_scale, grad);
+}
+
+// The cull masks of the camera rays of 16x16 tile `tile` (kTestAll when the
+// frame has none, or for the counting kernel, whose events must be the
+// reference algorithm's).
+template <bool C>
+__device__ __forceinline__ Cull camera_cull(const TraceParams &P, uint32_t tile) {
+    if (C || !P.camera_cull) return kTestAll;
+    const uint2 m = P.camera_cull[tile];
+    return Cull{m.x, m.y};
 }
 
 // Stage the body table (and small ring tables) into shared memory.

@@ -60,7 +60,16 @@ struct TraceParams {
     // Ringshine next-event estimation (pathtrace.wgsl:1248-1296) at ringed
     // bodies' surfaces; 0 leaves it out (sg_set_ringshine).
     uint32_t ringshine;
+    // Per 16x16 pixel tile of the viewport: the bodies (x) and rings (y) a
+    // camera ray of the tile can meet, by a conservative cone test
+    // (launch_camera_cull). Camera rays skip the others' intersection
+    // tests, which would miss. Null: test every body.
+    const uint2 *camera_cull;
 };
+
+// The camera-ray cull masks of every 16x16 tile into `out` (tiles_x *
+// tiles_y entries) for frames of at most 32 bodies.
+cudaError_t launch_camera_cull(const TraceParams &p, uint2 *out, cudaStream_t stream);
 
 // Geometry cache of the heightfield (cache_terrain_geometry,
 // terrain.wgsl:242-285) for host radius `radius_m`, in place.

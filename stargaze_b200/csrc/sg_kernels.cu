@@ -56,9 +56,13 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
         float3 sky = f3(0.0f, 0.0f, 0.0f);
         Path path;
         Forward<A> nograd;
+        const Cull cull = camera_cull<C>(P, blockIdx.y * gridDim.x + blockIdx.x);
         for (uint32_t smp = 0; smp < z; ++smp) {
             start_path(path, &P.s, K, pixel, x, y, smp);
-            while (!step(S, K, path, nograd)) {
+            // The camera ray takes the tile's cull masks, later rays none.
+            if (!step(S, K, path, nograd, cull)) {
+                while (!step(S, K, path, nograd)) {
+                }
             }
             const float4 r = finish_path(path);
             total.x += r.x;
@@ -590,6 +594,75 @@ cudaError_t launch_adjoint(const TraceParams &p, const AdjointParams &a, cudaStr
         case 2: return launch_variant(adjoint_kernel<true, false>, grid, smem, stream, p, a);
         default: return launch_variant(adjoint_kernel<true, true>, grid, smem, stream, p, a);
     }
+}
+
+// Whether a sphere of radius `rho` at `c` (telescope space, camera at the
+// origin) can meet a ray inside the cone of half-angle `alpha` about the
+// unit direction `axis`: the directions that hit an external sphere form
+// the cone of half-angle asin(rho / |c|) about c. Radius and angles carry
+// margins (1e-3 relative, 1e-3 rad) far above the f32 error of the exact
+// intersection tests, so a false here is a certain miss there.
+__device__ __forceinline__ bool cone_meets_sphere(double3 axis, double alpha, double3 c, double rho) {
+    const double dist = sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+    const double r = rho * (1.0 + 1.0e-3);
+    if (!(dist > r)) return true;  // the camera is inside or at the sphere (or the input is not finite)
+    const double cosb = fmin(fmax((axis.x * c.x + axis.y * c.y + axis.z * c.z) / dist, -1.0), 1.0);
+    return acos(cosb) <= alpha + asin(r / dist) + 1.0e-3;
+}
+
+__device__ __forceinline__ double3 unit_direction(double ndc_x, double ndc_y, double tangent, double aspect) {
+    const double x = ndc_x * tangent * aspect, y = ndc_y * tangent;
+    const double inv = 1.0 / sqrt(x * x + y * y + 1.0);
+    return make_double3(x * inv, y * inv, -inv);
+}
+
+// One CTA per 16x16 tile, one thread per body: the bodies (their point
+// discs included) and the rings a camera ray of the tile may meet. A camera
+// ray of pixel (x, y) has ndc in [2x/W - 1, 2(x+1)/W - 1] x [1 - 2(y+1)/H,
+// 1 - 2y/H] (camera_direction, pathtrace.wgsl:1619-1626); the tile's rays
+// lie in the cone about its centre ray through its farthest corner.
+__global__ void __launch_bounds__(32) camera_cull_kernel(const __grid_constant__ TraceParams P, uint2 *out,
+                                                         uint32_t tiles_x) {
+    const uint32_t tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
+    const uint32_t i = threadIdx.x;
+    const uint32_t n = P.s.counts[0];
+    bool body = false, ring = false;
+    if (i < n) {
+        const double w = P.s.g.viewport[0], h = P.s.g.viewport[1];
+        const double tangent = P.s.g.cam_forward[3], aspect = P.s.g.viewport[3];
+        const double x0 = 2.0 * (tx * kTile) / w - 1.0, x1 = 2.0 * fmin((double)(tx * kTile + kTile), w) / w - 1.0;
+        const double y0 = 1.0 - 2.0 * fmin((double)(ty * kTile + kTile), h) / h, y1 = 1.0 - 2.0 * (ty * kTile) / h;
+        const double3 axis = unit_direction(0.5 * (x0 + x1), 0.5 * (y0 + y1), tangent, aspect);
+        double alpha = 0.0;
+        const double cx[2] = {x0, x1}, cy[2] = {y0, y1};
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                const double3 d = unit_direction(cx[a], cy[b], tangent, aspect);
+                const double c = fmin(fmax(d.x * axis.x + d.y * axis.y + d.z * axis.z, -1.0), 1.0);
+                alpha = fmax(alpha, acos(c));
+            }
+        const float4 hi = P.bodies[i * kBodyVec4 + kCenter], lo = P.bodies[i * kBodyVec4 + kLow];
+        const double3 c = make_double3((double)hi.x + lo.x, (double)hi.y + lo.y, (double)hi.z + lo.z);
+        const double dist = sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+        // point_disc_hit draws an unresolved body as a disc of at least
+        // `angle` radians (pathtrace.wgsl:1308-1333).
+        const double pixel = 2.0 * tangent / fmax(h, 1.0);
+        const double angle = fmin(fmax((double)kPointDiscRadius, 0.7 * pixel), (double)kStarDotPixels * pixel);
+        const double radius = hi.w;
+        body = cone_meets_sphere(axis, alpha, c, fmax(radius, angle * dist));
+        const float4 plane = P.bodies[i * kBodyVec4 + kRingPlane], params = P.bodies[i * kBodyVec4 + kRingParams];
+        // The annulus lies inside the sphere of its outer radius.
+        if (params.x > plane.w && params.y > 0.0f) ring = cone_meets_sphere(axis, alpha, c, (double)params.x * radius);
+    }
+    const uint32_t bodies = __ballot_sync(0xffffffffu, body), rings = __ballot_sync(0xffffffffu, ring);
+    if (i == 0) out[blockIdx.x] = make_uint2(bodies, rings);
+}
+
+cudaError_t launch_camera_cull(const TraceParams &p, uint2 *out, cudaStream_t stream) {
+    const uint32_t tiles_x = (p.width + kTile - 1) / kTile, tiles_y = (p.height + kTile - 1) / kTile;
+    if (p.s.counts[0] > 32u || tiles_x * tiles_y == 0) return cudaErrorInvalidValue;
+    camera_cull_kernel<<<tiles_x * tiles_y, 32, 0, stream>>>(p, out, tiles_x);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_checkpoint_segments(const TraceParams &p, const AdjointParams &a, uint32_t records,

@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
             uint32_t slot = 0;
             const bool fresh = i >= kept;
             bool valid = true;
+            Cull cull = kTestAll;
             if (fresh) {
                 // Sample k of the chunk, numbered sample-major over the
                 // padded tile grid; padding pixels are skipped.
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                     const uint32_t pixel = y * P.width + x;
                     start_path(p, &P.s, K, pixel, x, y, W.chunk_first + smp);
                     slot = smp * P.width * P.height + pixel;
+                    cull = camera_cull<false>(P, tile);
                 }
             } else {
                 slot = load_ray_part(st, W.pool, i, p);
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
             }
             if (valid) {
                 Extension e;
-                const bool alive = extend(S, K, p, nograd, e);
+                const bool alive = extend(S, K, p, nograd, e, cull);
                 ring = alive && e.ring.index != kMiss;
                 surface = alive && !ring && e.hit.index != kMiss;
                 if (ring || surface) {
