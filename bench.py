@@ -148,7 +148,26 @@ def profile_wavefront_terrain_640x360():
     print(t.integrator(), flush=True)
 
 
+def profile_dispatch_rings_1080p():
+    """The bench's own dispatch: ring workload at 1920x1080 with the default
+    16 Mi-path pool, two 64-sample dispatches (the first allocates the pool
+    and loads the kernels)."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl = W.rings_1080p()
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.prepare_frame(frame)
+        t.encode(frame)
+    t.read_pixels()
+    print(t.integrator(), flush=True)
+
+
 PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512,
+                 "dispatch_rings_1080p": profile_dispatch_rings_1080p,
                  "wavefront_rings_1080p": profile_wavefront_rings_1080p,
                  "wavefront_terrain_640x360": profile_wavefront_terrain_640x360}
 
@@ -800,6 +819,10 @@ def run_ours(args):
             land.map_extent = 2000.0
             terrain = adjoint_ratio(land_wl, local, stream, reps=2)
             checkpoints = checkpoint_comparison(land_wl, local, stream)
+            from stargaze_b200 import inverse
+
+            extras["ring_inverse_512"] = {"adam": inverse.ring_inverse(device=local),
+                                          "central_differences": inverse.central_difference_check(device=local)}
             ring = adjoint_ratio(W.rings_1080p(512, 512, 64), local, stream)
             extras["adjoint"] = {"terrain_1080p": terrain, "checkpoints_terrain_1080p": checkpoints,
                                  "ring_512": ring, "ratio": ring["ratio"],

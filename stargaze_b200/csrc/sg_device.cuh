@@ -183,15 +183,19 @@ __device__ __forceinline__ float sphere_distance(const Scene &S, Counter<C, L, F
                                                  float radius, float &delta) {
     K.add(&Events::sphere_tests);
     const float3 oc = relative_center(S, r, i);
-    const float a = dot_rn(r.d, r.d);
     const float b = dot_rn(oc, r.d);
+    const float c = __fsub_rn(dot_rn(oc, oc), __fmul_rn(radius, radius));
+    // An origin outside the sphere with the centre behind it: both roots
+    // are negative whatever h is (q = b - root < 0, so q / a < 0 and
+    // c / q < 0), so the exact test below would miss. Signs are exact.
+    if (b < 0.0f && c > 0.0f) return 1.0e30f;
+    const float a = dot_rn(r.d, r.d);
     const float3 pc = cross_rn(oc, r.d);
     const float h = __fsub_rn(__fmul_rn(__fmul_rn(a, radius), radius), dot_rn(pc, pc));
     if (h < 0.0f) return 1.0e30f;
     const float root = __fsqrt_rn(h);
     const float q = __fadd_rn(b, b >= 0.0f ? root : -root);
     if (q == 0.0f) return 1.0e30f;
-    const float c = __fsub_rn(dot_rn(oc, oc), __fmul_rn(radius, radius));
     // The far root is divided out only when the near one is behind the
     // origin; the values are those of the WGSL's c/q and q/a.
     float distance = b < 0.0f ? __fdiv_rn(q, a) : __fdiv_rn(c, q);
@@ -393,6 +397,16 @@ __device__ __forceinline__ RingHit ring_hit(const Scene &S, Counter<C, L, F> K, 
     if (fabsf(denom) < 1.0e-7f) return miss;
     const float3 oc = relative_center(S, r, i);
     const float a = dot_rn(r.d, r.d);
+    // The ray's line passes farther from the centre than the annulus
+    // reaches (|oc x d|^2 / a > (outer R)^2, with a 1e-3 margin far above
+    // the rounding of either side): every point of the ray, the plane
+    // crossing included, lies outside the annulus, so the exact test below
+    // would miss.
+    {
+        const float3 pc = cross(oc, r.d);
+        const float reach = params.x * b_radius(S, i);
+        if (dot(pc, pc) > a * reach * reach * 1.001f) return miss;
+    }
     const float3 perpendicular = div_rn(cross_rn(r.d, cross_rn(r.d, oc)), a);
     const float along = __fdiv_rn(-dot_rn(perpendicular, n), denom);
     const float distance = __fadd_rn(__fdiv_rn(dot_rn(oc, r.d), a), along);

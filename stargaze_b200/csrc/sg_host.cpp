@@ -884,6 +884,26 @@ static int ensure_checkpoints(sg_context *ctx, cudaStream_t stream) {
     return SG_OK;
 }
 
+// Camera rays of frames with at most 32 bodies test only the bodies and
+// rings their 16x16 tile can see: the tile masks, into p.camera_cull.
+static int camera_cull(sg_context *ctx, const sg_frame *frame, sg::TraceParams &p, cudaStream_t stream) {
+    if (frame->n_bodies > 32u || frame->n_bodies == 0u) return SG_OK;
+    const size_t tiles = (size_t)((ctx->width + 15u) / 16u) * ((ctx->height + 15u) / 16u);
+    if (ctx->camera_cull_tiles < tiles) {
+        cudaStreamSynchronize(stream);
+        cudaFree(ctx->camera_cull);
+        ctx->camera_cull = nullptr;
+        ctx->camera_cull_tiles = 0;
+        SG_CUDA(ctx, cudaMalloc(&ctx->camera_cull, tiles * sizeof(uint2)));
+        ctx->camera_cull_tiles = tiles;
+    }
+    cudaError_t e = sg::launch_camera_cull(p, ctx->camera_cull, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "camera cull masks");
+    ctx->launches += 1;
+    p.camera_cull = ctx->camera_cull;
+    return SG_OK;
+}
+
 static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr, uint64_t *events) {
     if (!ctx) return fail(nullptr, SG_ERR_INVALID, "ctx is NULL");
     int status = validate_frame(ctx, frame);
@@ -926,21 +946,9 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
         if (events) {
             SG_CUDA(ctx, cudaMemsetAsync(ctx->events, 0, sg::kEventCount * sizeof(unsigned long long), stream));
             p.events = ctx->events;
-        } else if (frame->n_bodies <= 32u) {
-            // Camera rays test only the bodies and rings their tile can see.
-            const size_t tiles = (size_t)((ctx->width + 15u) / 16u) * ((ctx->height + 15u) / 16u);
-            if (ctx->camera_cull_tiles < tiles) {
-                cudaStreamSynchronize(stream);
-                cudaFree(ctx->camera_cull);
-                ctx->camera_cull = nullptr;
-                ctx->camera_cull_tiles = 0;
-                SG_CUDA(ctx, cudaMalloc(&ctx->camera_cull, tiles * sizeof(uint2)));
-                ctx->camera_cull_tiles = tiles;
-            }
-            cudaError_t e = sg::launch_camera_cull(p, ctx->camera_cull, stream);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "camera cull masks");
-            ctx->launches += 1;
-            p.camera_cull = ctx->camera_cull;
+        } else {
+            status = camera_cull(ctx, frame, p, stream);
+            if (status != SG_OK) return status;
         }
         const bool checkpointing = ctx->ck_every > 0u && !events && ctx->integrator == SG_INTEGRATOR_WAVEFRONT &&
                                    !p.air_on && !p.styled && !p.sky_on;
@@ -1551,7 +1559,9 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
             s.counts[2] = std::min<uint32_t>(SG_MAX_BATCH_SAMPLES, tape->count[k] - done);
             a.ck.sample_base = accumulated;
             accumulated += s.counts[2];
-            const sg::TraceParams p = make_params(ctx, s);
+            sg::TraceParams p = make_params(ctx, s);
+            status = camera_cull(ctx, frame, p, stream);
+            if (status != SG_OK) return status;
             if (staged) {
                 sg::WaveRun run;
                 cudaError_t e =

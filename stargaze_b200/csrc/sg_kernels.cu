@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(kThreads, SG_TRACE_MIN_BLOCKS) trace_kernel(co
 // to `end_depth`, where the next segment's record starts, or it ends.
 template <bool L, bool F>
 __device__ __forceinline__ void replay_segment(const Scene &S, Counter<false, L, F> K, Prb &G, Path &path,
-                                               uint32_t end_depth) {
+                                               uint32_t end_depth, Cull first = kTestAll) {
+    if (step(S, K, path, G, first) || path.depth >= end_depth) return;
     while (!step(S, K, path, G)) {
         if (path.depth >= end_depth) break;
     }
@@ -124,7 +125,7 @@ __device__ __forceinline__ void replay_segment(const Scene &S, Counter<false, L,
 template <bool L, bool F>
 __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L, F> K, Prb &G, float3 w, uint32_t pixel,
                                                uint32_t x, uint32_t y, uint32_t smp, unsigned lanes,
-                                               uint32_t segment_end) {
+                                               uint32_t segment_end, Cull cull) {
     bool again = true;
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
@@ -133,10 +134,13 @@ __device__ __forceinline__ void adjoint_sample(const Scene &S, Counter<false, L,
             start_path(path, S.s, K, pixel, x, y, smp);
             if (segment_end) {
                 // A checkpointed sample: its first segment, once.
-                replay_segment(S, K, G, path, segment_end);
+                replay_segment(S, K, G, path, segment_end, cull);
                 again = false;
             } else {
-                while (!step(S, K, path, G)) {
+                // The camera ray takes the tile's cull masks.
+                if (!step(S, K, path, G, cull)) {
+                    while (!step(S, K, path, G)) {
+                    }
                 }
                 if (pass == 0) {
                     again = G.deferral_full || cap_binds(G, path.radiance);
@@ -194,6 +198,7 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     }
     const bool busy = w.x != 0.0f || w.y != 0.0f || w.z != 0.0f;
     const unsigned lanes = __ballot_sync(0xffffffffu, busy);
+    const Cull cull = camera_cull<false>(P, blockIdx.y * gridDim.x + blockIdx.x);
     if (busy) {
         const uint32_t z = P.s.counts[2];
         const uint32_t pixels = P.width * P.height;
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
                 }
             }
             if (!segment_end) pass1_setup(G, w);
-            adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes, segment_end);
+            adjoint_sample(S, K, G, w, pixel, x, y, smp, lanes, segment_end, cull);
         }
     }
     // Per-thread colour sums: reduce over the warp, then into the window.

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
         uint32_t pixel = 0, slot = 0, smp = 0;
         float3 w = f3(0.0f, 0.0f, 0.0f);
         const bool fresh = i >= kept;
+        Cull cull = kTestAll;
         if (i < n) {
             bool valid = true;
             if (fresh) {
@@ -299,7 +300,10 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
                     // Pixels the loss does not weigh are not replayed.
                     valid = w.x != 0.0f || w.y != 0.0f || w.z != 0.0f;
                 }
-                if (valid) start_path(p, &P.s, K, pixel, x, y, smp);
+                if (valid) {
+                    start_path(p, &P.s, K, pixel, x, y, smp);
+                    cull = camera_cull<false>(P, tile);
+                }
             } else {
                 load_ray_part(st, W.pool, i, p);
                 const float4 g = st[6 * W.pool + i];
@@ -308,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
             }
             if (valid) {
                 NoGrad nograd;  // extend's only hook sets the iteration
-                const bool alive = extend(S, K, p, nograd, e);
+                const bool alive = extend(S, K, p, nograd, e, cull);
                 ring = alive && e.ring.index != kMiss;
                 surface = alive && !ring && e.hit.index != kMiss;
                 take_slot = fresh && (ring || surface);

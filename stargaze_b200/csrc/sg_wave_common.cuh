@@ -22,6 +22,10 @@ namespace {
 #ifndef SG_WAVE_SHADE_MIN_BLOCKS
 #define SG_WAVE_SHADE_MIN_BLOCKS SG_WAVE_MIN_BLOCKS
 #endif
+// Paths a thread of the extend stage takes per queue append.
+#ifndef SG_WAVE_EXTEND_ITEMS
+#define SG_WAVE_EXTEND_ITEMS 1
+#endif
 
 // ---------------------------------------------------------------------------
 // Path state planes
@@ -174,6 +178,53 @@ __device__ __forceinline__ void block_append(Append<Q, B> &sm, const bool (&flag
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < Q; ++q) slot[q] = sm.base[q] + sm.warp_counts[q][warp] + __popc(ballot[q] & below);
+}
+
+// The same for K items per thread: bit k of flags[q] marks the thread's
+// item k for queue q. Slots follow item order first, then thread order, so
+// a round's queue entries keep the order of its input (k * B + thread).
+// One barrier pair per K items: warps whose items took longer wait once
+// per round instead of once per item.
+template <int Q, int K, int B = kThreads>
+struct AppendK {
+    uint32_t warp_counts[Q][K][B / 32];
+    uint32_t base[Q];
+};
+
+template <int Q, int K, int B = kThreads>
+__device__ __forceinline__ void block_append_k(AppendK<Q, K, B> &sm, const uint32_t (&flags)[Q],
+                                               uint32_t *const (&counter)[Q], uint32_t (&slot)[Q][K]) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t ballot[Q][K];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            ballot[q][k] = __ballot_sync(0xffffffffu, (flags[q] >> k) & 1u);
+            if (lane == 0) sm.warp_counts[q][k][warp] = __popc(ballot[q][k]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < Q) {
+        const int q = threadIdx.x;
+        uint32_t total = 0;
+        for (int k = 0; k < K; ++k) {
+            for (uint32_t w = 0; w < (uint32_t)B / 32u; ++w) {
+                const uint32_t c = sm.warp_counts[q][k][w];
+                sm.warp_counts[q][k][w] = total;  // exclusive prefix in (item, warp) order
+                total += c;
+            }
+        }
+        sm.base[q] = total ? atomicAdd(counter[q], total) : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            slot[q][k] = sm.base[q] + sm.warp_counts[q][k][warp] + __popc(ballot[q][k] & below);
+    }
 }
 
 __device__ __forceinline__ WaveCounters *counters(const WaveParams &W, uint32_t t) {

@@ -54,7 +54,8 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                                                                             const __grid_constant__ WaveParams W,
                                                                             uint32_t t) {
     extern __shared__ float4 smem[];
-    __shared__ Append<2> sm[2];
+    constexpr uint32_t kItems = SG_WAVE_EXTEND_ITEMS;
+    __shared__ AppendK<2, kItems> sm[2];
     WaveCounters *c = counters(W, t);
     // Paths the previous iteration kept occupy [0, kept); new samples of the
     // chunk fill the pool up to n.
@@ -66,15 +67,20 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
         counters(W, t + 1u)->next = next + take;
         *counters(W, t + 2u) = WaveCounters{};
     }
-    if (blockIdx.x * kThreads >= n) return;
+    if (blockIdx.x * kThreads * kItems >= n) return;
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
     Forward<A> nograd;
     float4 *st = W.state[t & 1u];
     float4 *H = W.hits;
     uint32_t round = 0;
-    for (uint32_t base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads, ++round) {
-        const uint32_t i = base + threadIdx.x;
+    // Each round a thread extends kItems paths (i = base + k * kThreads +
+    // threadIdx.x), then the CTA appends them to the queues at once.
+    for (uint32_t base = blockIdx.x * kThreads * kItems; base < n; base += gridDim.x * kThreads * kItems, ++round) {
+      uint32_t ring_bits = 0, surface_bits = 0;
+#pragma unroll 1
+      for (uint32_t item = 0; item < kItems; ++item) {
+        const uint32_t i = base + item * kThreads + threadIdx.x;
         bool ring = false, surface = false;
         if (i < n) {
             Path p;
@@ -148,12 +154,19 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                 }
             }
         }
-        const bool flags[2] = {ring, surface};
-        uint32_t *const ctr[2] = {&c->ring, &c->surface};
-        uint32_t q[2];
-        block_append<2>(sm[round & 1u], flags, ctr, q);
-        if (ring) W.ring_queue[q[0]] = i;
-        if (surface) W.surface_queue[q[1]] = i;
+        ring_bits |= (ring ? 1u : 0u) << item;
+        surface_bits |= (surface ? 1u : 0u) << item;
+      }
+      const uint32_t flags[2] = {ring_bits, surface_bits};
+      uint32_t *const ctr[2] = {&c->ring, &c->surface};
+      uint32_t q[2][kItems];
+      block_append_k<2, kItems>(sm[round & 1u], flags, ctr, q);
+#pragma unroll
+      for (uint32_t item = 0; item < kItems; ++item) {
+        const uint32_t i = base + item * kThreads + threadIdx.x;
+        if ((ring_bits >> item) & 1u) W.ring_queue[q[0][item]] = i;
+        if ((surface_bits >> item) & 1u) W.surface_queue[q[1][item]] = i;
+      }
     }
 }
 
