@@ -74,9 +74,13 @@ OPS_PER_EVENT = {
 EVENT_ORDER = ["vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_samples", "shadow_rays",
                "ring_events", "surface_events", "rng_draws", "terrain_nodes", "terrain_triangles", "prop_boxes",
                "prop_tests"]
-# DRAM traffic of one dispatch on this workload from an ncu capture of its
-# stage kernels; None until measured.
-TRAFFIC_BYTES_PER_LAUNCH = None
+# DRAM traffic of one 64-sample dispatch of the ring workload: an ncu
+# capture of one steady-state iteration of the three stage kernels (4 Mi-path
+# pool: 664 MB for 4.19 M path extensions) scaled to the dispatch's 183 M
+# path extensions (1.38 per sample, counting kernel). Issue-slot fraction of
+# the same capture, weighted by the stages' share of the step.
+TRAFFIC_BYTES_PER_LAUNCH = 664.2e6 * (1.38 * 1920 * 1080 * 64) / 4.194e6
+ISSUE_SLOT_FRACTION = 0.59
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -187,6 +191,14 @@ def parse_args():
     p.add_argument("--profile-case", choices=sorted(PROFILE_CASES),
                    help="run one small case for an ncu capture (profiles/) and exit")
     return p.parse_args()
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool's B200s (GB/s), if known."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def dist_env():
@@ -796,6 +808,14 @@ def run_ours(args):
     e2e_value = job_msamples_per_s(world, samples_per_step, args.steps, e2e_total)
     mean_launch_s = statistics.mean(launch_ms) * 1e-3
     achieved = ops_per_launch / mean_launch_s
+    # Queue and result traffic by construction (wavefront): an extension
+    # reads 3 and writes 4 float4 (planes 0, 1, 6; planes 1, 6 and two hit
+    # planes), a shade vertex reads 7 planes and 2 hit planes and writes 7
+    # planes, every sample writes and the resolve reads one float4.
+    ev = {n: int(totals[k]) / batches for k, n in enumerate(EVENT_ORDER)}
+    queue_bytes = (ev["vertices"] * 7 + (ev["ring_events"] + ev["surface_events"]) * 16) * 16 + \
+        wl.width * wl.height * BATCH * 32
+    hbm_peak_gbs = measured_hbm_gbs()
     result = None
     if rank == 0:
         base = None
@@ -837,7 +857,13 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}, disjoint noise sequences",
                        "integrator": args.integrator},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                         "frac": achieved / peak.value, "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                         "frac": achieved / peak.value,
+                         "traffic": TRAFFIC_BYTES_PER_LAUNCH if wl.name == "rings_1080p" else None,
+                         "traffic_note": "scaled from a one-iteration capture by path extensions",
+                         "algorithmic_bytes_per_launch": queue_bytes,
+                         "queue_hbm_frac": queue_bytes / (statistics.mean(launch_ms) * 1e-3) / (hbm_peak_gbs * 1e9)
+                         if hbm_peak_gbs else None,
+                         "issue_slot_fraction": ISSUE_SLOT_FRACTION if wl.name == "rings_1080p" else None,
                          "kernel": ("wavefront dispatch (extend, ring and surface stages, resolve)"
                                     if args.integrator == "wavefront" else "trace_kernel (megakernel)"),
                          "ops_per_launch": ops_per_launch,

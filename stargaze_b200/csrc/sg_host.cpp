@@ -1522,9 +1522,9 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
     a.tau_window = tau_used <= 8192u ? tau_used : 0u;
     a.color_window = 6u * frame->n_bodies;
     a.ck = sg::Checkpoints{};
-    // With vertex checkpoints of this accumulation, the per-pixel replay
-    // takes each sample only up to its first checkpoint and the segment
-    // kernel replays the rest from the stored records.
+    // With vertex checkpoints of this accumulation, the replay (staged or
+    // per-pixel) takes each sample, its radiance known, only up to its first
+    // checkpoint, and the segment kernel replays the rest from the records.
     const bool checkpointed = ctx->ck_every > 0u && ctx->ck_valid && ctx->ck_records;
     uint32_t records = 0;
     if (checkpointed) {
@@ -1540,7 +1540,7 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
         a.ck.every = ctx->ck_every;
         a.ck.max_depth = ctx->options.max_bounces;
     }
-    const bool staged = ctx->integrator == SG_INTEGRATOR_WAVEFRONT && !checkpointed;
+    const bool staged = ctx->integrator == SG_INTEGRATOR_WAVEFRONT;
     sg::WaveParams w{};
     sg::AdjointWave x{};
     if (staged) {

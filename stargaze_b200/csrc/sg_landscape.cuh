@@ -263,8 +263,11 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
         count -= 1u;
         if (stack_t[count] >= limit) continue;
         const uint32_t index = stack_node[count];
-        const uint3 node = t_node(index, cells);
-        if (node.z == 2u) {
+        // The node's size from its heap level; its cell coordinates (the
+        // Morton decode of t_node) only where a leaf needs them.
+        const uint32_t size = cells >> ((31u - __clz(3u * index + 1u)) / 2u);
+        if (size == 2u) {
+            const uint3 node = t_node(index, cells);
 #pragma unroll 1
             for (uint32_t z = node.y; z < node.y + 2u; ++z) {
 #pragma unroll 1
@@ -308,17 +311,22 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
                     (bounds.x <= bounds.y && bounds.y > 0.001f && bounds.x < limit) ? fmaxf(bounds.x, 0.0f) : 1.0e30f;
             }
             // Far first on the stack: the nearest child is popped first.
+            // The reference's insertion sort, as a fixed sequence of
+            // compare-exchanges that swap only on a strictly nearer left
+            // element: once an element stops, the ones before it are no
+            // nearer, so the extra exchanges never fire and the order
+            // (ties included) is the insertion sort's.
 #pragma unroll
             for (uint32_t i = 1; i < 4u; ++i) {
 #pragma unroll
                 for (uint32_t j = i; j > 0u; --j) {
-                    if (distances[j - 1u] >= distances[j]) break;
-                    const float dd = distances[j - 1u];
-                    const uint32_t cc = children[j - 1u];
-                    distances[j - 1u] = distances[j];
-                    children[j - 1u] = children[j];
-                    distances[j] = dd;
-                    children[j] = cc;
+                    const bool swap = distances[j - 1u] < distances[j];
+                    const float dl = distances[j - 1u], dr = distances[j];
+                    const uint32_t cl = children[j - 1u], cr = children[j];
+                    distances[j - 1u] = swap ? dr : dl;
+                    distances[j] = swap ? dl : dr;
+                    children[j - 1u] = swap ? cr : cl;
+                    children[j] = swap ? cl : cr;
                 }
             }
 #pragma unroll

@@ -63,6 +63,12 @@ constexpr uint32_t kFlagDeferralFull = 1u << 16;
 constexpr uint32_t kFlagCapDirect = 1u << 17;
 constexpr uint32_t kFlagBinding = 1u << 18;
 constexpr uint32_t kFlagPass2 = 1u << 19;
+// The forward stored the sample's radiance (sg_set_checkpoints): one
+// replay scatters everything at once (segment_setup); with kFlagStops the
+// replay ends where the first vertex checkpoint starts (the segment kernel
+// replays the rest).
+constexpr uint32_t kFlagKnownTotal = 1u << 20;
+constexpr uint32_t kFlagStops = 1u << 21;
 
 __device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, float3 w, Prb &G, uint32_t &smp) {
     const float4 *q = X.side + (size_t)slot * kAdjointSideVec4;
@@ -70,7 +76,7 @@ __device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, fl
     const uint32_t flags = __float_as_uint(s2.w);
     const float3 zero = f3(0.0f, 0.0f, 0.0f);
     G.pass2 = (flags & kFlagPass2) != 0u;
-    G.known_total = false;
+    G.known_total = (flags & kFlagKnownTotal) != 0u;
     G.a = xyz4(s0);
     G.cap = s0.w;
     G.base = xyz4(s1);
@@ -106,11 +112,12 @@ __device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, fl
     G.dropped = 0;
 }
 
-__device__ __forceinline__ void store_prb(const AdjointWave &X, uint32_t slot, const Prb &G, uint32_t smp) {
+__device__ __forceinline__ void store_prb(const AdjointWave &X, uint32_t slot, const Prb &G, uint32_t smp,
+                                          uint32_t extra = 0u) {
     float4 *q = X.side + (size_t)slot * kAdjointSideVec4;
     const uint32_t flags = (G.n_fac & 0xffu) | ((G.n_rr & 0xffu) << 8) | (G.deferral_full ? kFlagDeferralFull : 0u) |
                            (G.cap_direct ? kFlagCapDirect : 0u) | (G.binding ? kFlagBinding : 0u) |
-                           (G.pass2 ? kFlagPass2 : 0u);
+                           (G.pass2 ? kFlagPass2 : 0u) | (G.known_total ? kFlagKnownTotal : 0u) | extra;
     q[0] = pack3(G.a, G.cap);
     q[1] = pack3u(G.base, G.capture_iter);
     q[2] = pack3u(G.cap_light, flags);
@@ -338,7 +345,21 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
             slot = X.free_ring[q[4] % W.pool];
             Prb G;
             fresh_prb(G, w);
-            store_prb(X, slot, G, smp);
+            // With the forward's radiance of this sample (and no binding
+            // cap, no overflowing record), one replay with every weight
+            // known; it stops at the first checkpoint when the sample has
+            // records.
+            uint32_t extra = 0u;
+            const uint32_t sample = A.ck.sample_base + smp;
+            if (A.ck.totals && sample < A.ck.samples) {
+                const float4 tot = A.ck.totals[(size_t)sample * P.width * P.height + pixel];
+                const uint32_t bits = __float_as_uint(tot.w);
+                if (!(bits & 2u)) {
+                    segment_setup(G, w, f3(tot.x, tot.y, tot.z), f3(0.0f, 0.0f, 0.0f));
+                    if (bits & 1u) extra = kFlagStops;
+                }
+            }
+            store_prb(X, slot, G, smp, extra);
             store_adjoint_path(st, W.pool, i, p, pixel, slot);
         } else if (ring || surface) {
             st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
@@ -414,6 +435,11 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
                 ended = surface_vertex(S, K, p, hit, h2.w, G);
             }
             keep = !ended || end_replay(P, K, G, p, pixel, smp, w);
+            // A checkpointed sample's replay ends where its first record
+            // starts (the same scatter that stored it in the forward).
+            if (keep && !ended && G.known_total && p.depth >= A.ck.every &&
+                (__float_as_uint(X.side[(size_t)slot * kAdjointSideVec4 + 2].w) & kFlagStops))
+                keep = false;
             give = !keep;
             dropped += G.dropped;
         }
@@ -422,7 +448,9 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
         uint32_t q[2];
         block_append<2, kShadeThreads>(sm[round & 1u], flags, ctr, q);
         if (keep) {
-            store_prb(X, slot, G, smp);
+            const uint32_t stops =
+                G.known_total ? (__float_as_uint(X.side[(size_t)slot * kAdjointSideVec4 + 2].w) & kFlagStops) : 0u;
+            store_prb(X, slot, G, smp, stops);
             store_adjoint_path(out, W.pool, q[0], p, pixel, slot);
         }
         if (give) X.free_ring[q[1] % W.pool] = slot;

@@ -22,9 +22,10 @@ namespace {
 #ifndef SG_WAVE_SHADE_MIN_BLOCKS
 #define SG_WAVE_SHADE_MIN_BLOCKS SG_WAVE_MIN_BLOCKS
 #endif
-// Paths a thread of the extend stage takes per queue append.
+// Paths a thread of the extend stage takes per queue append (celestial
+// frames).
 #ifndef SG_WAVE_EXTEND_ITEMS
-#define SG_WAVE_EXTEND_ITEMS 1
+#define SG_WAVE_EXTEND_ITEMS 4
 #endif
 
 // ---------------------------------------------------------------------------

@@ -54,7 +54,11 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                                                                             const __grid_constant__ WaveParams W,
                                                                             uint32_t t) {
     extern __shared__ float4 smem[];
-    constexpr uint32_t kItems = SG_WAVE_EXTEND_ITEMS;
+    // Celestial frames take several paths per append (their work per path
+    // is even); landscape frames one, so that a CTA's last round is small
+    // when traversal costs differ (measured: rings 59.5 -> 56.5 ms per step
+    // with four, terrain 455 -> 531 ms).
+    constexpr uint32_t kItems = L ? 1u : SG_WAVE_EXTEND_ITEMS;
     __shared__ AppendK<2, kItems> sm[2];
     WaveCounters *c = counters(W, t);
     // Paths the previous iteration kept occupy [0, kept); new samples of the

@@ -60,13 +60,16 @@ def test_checkpointed_adjoint_equals_replay_on_the_terrain_scene(every):
     assert_same_gradient(ckpt.body_color, replay.body_color, "body_color")
 
 
-def test_checkpointed_adjoint_equals_replay_on_the_ring_scene():
+@pytest.mark.parametrize("every", [2, 64])
+def test_checkpointed_adjoint_equals_replay_on_the_ring_scene(every):
     """Ring scatters, null crossings and the ring-indirect cap (its binding
-    samples replay from the seed)."""
+    samples replay from the seed). every = 64, beyond the bounce limit,
+    stores the radiance alone: whole paths replay once with known weights."""
     wl = W.rings_1080p(96, 64, 8)
     _, replay, _ = forward_backward(wl, 8, 22)
-    _, ckpt, stats = forward_backward(wl, 8, 22, every=2)
-    assert stats["records"] > 0
+    _, ckpt, stats = forward_backward(wl, 8, 22, every=every)
+    assert (stats["records"] > 0) == (every < wl.max_bounces)
+    assert stats["device_bytes"] >= 96 * 64 * 8 * 16
     assert_same_gradient(ckpt.ring_tau[0, :512], replay.ring_tau[0, :512], "ring_tau")
     assert_same_gradient(ckpt.ring_albedo, replay.ring_albedo, "ring_albedo")
     assert_same_gradient(ckpt.body_color, replay.body_color, "body_color")
