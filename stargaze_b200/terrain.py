@@ -160,12 +160,14 @@ def height_at(heights: np.ndarray, cells: int, x: float, z: float, radius_m: flo
     scale = terrain_scale(radius_m)
     c = coordinates(cells, scale).astype(np.float64)
     width = cells + 1
-    h = np.asarray(heights, dtype=np.float64).reshape(width, width)
+    h = np.asarray(heights).reshape(width, width)  # the four corners are widened to f64 below
     ix = int(np.clip(np.searchsorted(c, x) - 1, 0, cells - 1))
     iz = int(np.clip(np.searchsorted(c, z) - 1, 0, cells - 1))
     u = float(np.clip((x - c[ix]) / (c[ix + 1] - c[ix]), 0.0, 1.0))
     v = float(np.clip((z - c[iz]) / (c[iz + 1] - c[iz]), 0.0, 1.0))
-    y = (h[iz, ix] * (1 - u) + h[iz, ix + 1] * u) * (1 - v) + (h[iz + 1, ix] * (1 - u) + h[iz + 1, ix + 1] * u) * v
+    h00, h01 = float(h[iz, ix]), float(h[iz, ix + 1])
+    h10, h11 = float(h[iz + 1, ix]), float(h[iz + 1, ix + 1])
+    y = (h00 * (1 - u) + h01 * u) * (1 - v) + (h10 * (1 - u) + h11 * u) * v
     r = radius_m
     d2 = x * x + z * z
     return y * scale - d2 / (r + math.sqrt(max(r * r - d2, 0.0)))
