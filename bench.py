@@ -115,6 +115,24 @@ def profile_adjoint_ring_512():
         t.backward(frame, t.tape(), dl)
 
 
+def profile_adjoint_ring_512_small():
+    """As adjoint_ring_512 with a 2 Mi-path pool (about 2.5 GB of path state
+    and adjoint slots on the device, small enough for multi-pass captures)."""
+    from stargaze_b200 import PathTracer, workloads as W
+
+    wl = W.rings_1080p(512, 512, 64)
+    t = PathTracer((wl.width, wl.height), W.render_options(wl, 64))
+    W.upload_workload(t, wl)
+    t.set_integrator("wavefront", 1 << 21)
+    dl = np.random.default_rng(0).uniform(0.0, 1.0, (wl.width * wl.height, 4)).astype(np.float32)
+    for r in range(2):
+        frame = wl.frame.copy()
+        frame.scene_time = float(r)
+        t.prepare_frame(frame)
+        t.encode(frame)
+        t.backward(frame, t.tape(), dl)
+
+
 def profile_wavefront_rings_1080p():
     """Ring workload at 1920x1080 through the wavefront integrator with a
     4 Mi-path pool (3.4 GB on the device, small enough for multi-pass
@@ -171,6 +189,7 @@ def profile_dispatch_rings_1080p():
 
 
 PROFILE_CASES = {"terrain_640x360": profile_terrain_640x360, "adjoint_ring_512": profile_adjoint_ring_512,
+                 "adjoint_ring_512_small": profile_adjoint_ring_512_small,
                  "dispatch_rings_1080p": profile_dispatch_rings_1080p,
                  "wavefront_rings_1080p": profile_wavefront_rings_1080p,
                  "wavefront_terrain_640x360": profile_wavefront_terrain_640x360}

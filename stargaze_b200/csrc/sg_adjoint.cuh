@@ -77,12 +77,19 @@ struct GradEntry {
 };
 
 __device__ __forceinline__ GradEntry no_entry() { return GradEntry{kNoParam, make_float3(0.0f, 0.0f, 0.0f)}; }
+__device__ __forceinline__ float4 pack_entry(const GradEntry &e) {
+    return make_float4(__uint_as_float(e.param), e.dlog.x, e.dlog.y, e.dlog.z);
+}
+__device__ __forceinline__ GradEntry unpack_entry(float4 v) {
+    return GradEntry{__float_as_uint(v.x), make_float3(v.y, v.z, v.w)};
+}
 
 // Where gradients land: the colours of the first kColorSlots bodies in
 // per-thread sums (every lane of a warp hits the same few of them; the
 // kernel reduces them once at its end), shared-memory windows over the
 // ring tables in use and the other body colours, global memory for the
-// rest.
+// rest. Sum k of a thread is own[k * own_stride]: a local array (stride 1)
+// or the thread's column of a shared-memory block (stride: CTA size).
 struct GradSink {
     float *own;         // per-thread sums over [kGradColor, kGradColor + own_n)
     uint32_t own_n;
@@ -91,10 +98,11 @@ struct GradSink {
     float *color;
     uint32_t color_n;
     float *global;
+    uint32_t own_stride;
     __device__ __forceinline__ void add(uint32_t param, float value) const {
         if (value == 0.0f) return;
         const uint32_t c = param - kGradColor;
-        if (c < own_n) own[c] += value;
+        if (c < own_n) own[c * own_stride] += value;
         else if (param < tau_n) atomicAdd(tau + param, value);
         else if (c < color_n) atomicAdd(color + c, value);
         else atomicAdd(global + param, value);
@@ -174,7 +182,11 @@ struct Prb {
     uint32_t prev_param;      // tau parameter of the last ring scatter
     float prev_dlog_pdf;      // ... and d log of its scatter pdf
     uint32_t n_rr;
-    GradEntry local[kMaxLocal];
+    // The factors of the pending contribution: entry k at
+    // local[k * local_stride] (a local array, stride 1, or the thread's
+    // column of a shared-memory block), packed as float4.
+    float4 *local;
+    uint32_t local_stride;
     uint32_t n_local, dropped;
     // Pass 1's deferred throughput factors (count), and where the lists live.
     uint32_t n_fac;
@@ -185,7 +197,7 @@ struct Prb {
     __device__ __forceinline__ bool after_capture() const { return capture_iter != 0u && iteration >= capture_iter; }
     __device__ __forceinline__ void local_factor(GradEntry e) {
         if (e.param == kNoParam) return;
-        if (n_local < (uint32_t)kMaxLocal) local[n_local++] = e;
+        if (n_local < (uint32_t)kMaxLocal) local[(n_local++) * local_stride] = pack_entry(e);
         else dropped += 1u;
     }
 };
@@ -244,7 +256,7 @@ static __device__ SG_ADJ_HOOK void contribute(Prb &G, float3 value, bool cap_ter
     const float3 wp = (!cap_term && post) ? mul3(G.w_pdf, value) : zero;
     if (w.x != 0.0f || w.y != 0.0f || w.z != 0.0f || wp.x != 0.0f || wp.y != 0.0f || wp.z != 0.0f) {
 #pragma unroll 1
-        for (uint32_t k = 0; k < G.n_local; ++k) scatter_entry(G.sink, G.local[k], w, wp);
+        for (uint32_t k = 0; k < G.n_local; ++k) scatter_entry(G.sink, unpack_entry(G.local[k * G.local_stride]), w, wp);
     }
     G.n_local = 0;
     G.a = G.a + mul3(full, value);

@@ -817,7 +817,8 @@ static int ensure_adjoint(sg_context *ctx, uint32_t samples, sg::WaveParams &w, 
     }
     char *base = static_cast<char *>(ctx->adjoint_slots);
     x.side = reinterpret_cast<float4 *>(base);
-    x.lists = base + (size_t)pool * sg::kAdjointSideVec4 * sizeof(float4);
+    x.queued = reinterpret_cast<uint4 *>(base + (size_t)pool * sg::kAdjointSideVec4 * sizeof(float4));
+    x.lists = base + (size_t)pool * (sg::kAdjointSideVec4 * sizeof(float4) + 2u * sizeof(uint4));
     x.free_ring = reinterpret_cast<uint32_t *>(base + sg::adjoint_slot_bytes(pool) - (size_t)pool * sizeof(uint32_t) -
                                                4 * sizeof(uint32_t));
     x.free_ends = x.free_ring + pool;

@@ -267,6 +267,8 @@ constexpr uint32_t kAdjointSideVec4 = 10;  // float4 words of one slot's state
 
 struct AdjointWave {
     float4 *side;         // kAdjointSideVec4 float4 per slot
+    uint4 *queued;        // 2 * pool: per ring-queue entry, then per surface-queue entry,
+                          // (slot, pixel, sample, 1 if the sample starts in this iteration)
     void *lists;          // one PrbLists per slot
     uint32_t *free_ring;  // `pool` slot ids
     uint32_t *free_ends;  // [0] next allocation, [1] next free position (monotonic)

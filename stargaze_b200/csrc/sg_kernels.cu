@@ -184,9 +184,12 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
     const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
     PrbLists lists;
+    float4 local[kMaxLocal];
     Prb G;
     G.lists = &lists;
-    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.local = local;
+    G.local_stride = 1u;
+    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad, 1u};
     G.inv = inv;
     G.dropped = 0;
     const bool inside = x < P.width && y < P.height;
@@ -267,9 +270,12 @@ __global__ void __launch_bounds__(kThreads, SG_ADJOINT_MIN_BLOCKS)
     for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
     const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
     PrbLists lists;
+    float4 local[kMaxLocal];
     Prb G;
     G.lists = &lists;
-    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad};
+    G.local = local;
+    G.local_stride = 1u;
+    G.sink = GradSink{own, own_n, window, A.tau_window, window + A.tau_window, A.color_window, A.grad, 1u};
     G.inv = inv;
     G.dropped = 0;
     const uint32_t pixels = P.width * P.height;

@@ -70,7 +70,8 @@ constexpr uint32_t kFlagPass2 = 1u << 19;
 constexpr uint32_t kFlagKnownTotal = 1u << 20;
 constexpr uint32_t kFlagStops = 1u << 21;
 
-__device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, float3 w, Prb &G, uint32_t &smp) {
+// Returns the slot's flags word.
+__device__ __forceinline__ uint32_t load_prb(const AdjointWave &X, uint32_t slot, float3 w, Prb &G, uint32_t &smp) {
     const float4 *q = X.side + (size_t)slot * kAdjointSideVec4;
     const float4 s0 = q[0], s1 = q[1], s2 = q[2], s3 = q[3];
     const uint32_t flags = __float_as_uint(s2.w);
@@ -108,8 +109,11 @@ __device__ __forceinline__ void load_prb(const AdjointWave &X, uint32_t slot, fl
         G.b_total = zero;
     }
     G.lists = reinterpret_cast<PrbLists *>(X.lists) + slot;
+    G.local = nullptr;  // the shade stages point it at their shared-memory lists
+    G.local_stride = 0u;
     G.n_local = 0;
     G.dropped = 0;
+    return flags;
 }
 
 __device__ __forceinline__ void store_prb(const AdjointWave &X, uint32_t slot, const Prb &G, uint32_t smp,
@@ -142,6 +146,29 @@ __device__ __forceinline__ void fresh_prb(Prb &G, float3 w) {
     G.dropped = 0;
 }
 
+// The adjoint state of a sample that starts in this iteration, as its slot
+// would hold it: pass 1 from the start, or — with the forward's radiance of
+// the sample (sg_set_checkpoints) and no binding cap or overflowing record
+// — one replay with every weight known (segment_setup), which ends at the
+// first checkpoint when the sample has records (returns kFlagStops then).
+__device__ __forceinline__ uint32_t fresh_sample(const TraceParams &P, const AdjointParams &A, const AdjointWave &X,
+                                                 uint32_t slot, uint32_t pixel, uint32_t smp, float3 w, Prb &G) {
+    const float3 zero = f3(0.0f, 0.0f, 0.0f);
+    fresh_prb(G, w);
+    G.a_total = zero;
+    G.b_total = zero;
+    G.lists = reinterpret_cast<PrbLists *>(X.lists) + slot;
+    G.local = nullptr;
+    G.local_stride = 0u;
+    const uint32_t sample = A.ck.sample_base + smp;
+    if (!A.ck.totals || sample >= A.ck.samples) return 0u;
+    const float4 tot = A.ck.totals[(size_t)sample * P.width * P.height + pixel];
+    const uint32_t bits = __float_as_uint(tot.w);
+    if (bits & 2u) return 0u;
+    segment_setup(G, w, f3(tot.x, tot.y, tot.z), zero);
+    return (bits & 1u) ? kFlagStops : 0u;
+}
+
 // The pixel weight of the loss: d loss / d pixel over the samples behind it.
 __device__ __forceinline__ float3 pixel_weight(const AdjointParams &A, uint32_t pixel) {
     const float4 d = A.dl_dimage[pixel];
@@ -149,11 +176,17 @@ __device__ __forceinline__ float3 pixel_weight(const AdjointParams &A, uint32_t 
 }
 
 // Per-block gradient sinks: shared-memory windows over the ring tables and
-// the body colours, per-thread sums for the first bodies' colours.
+// the body colours, and per-thread sums for the first bodies' colours in
+// shared memory too (column threadIdx.x of a 6 kColorSlots x CTA-size
+// block after the windows). In local memory those sums are read and
+// written at every colour derivative, and at two 256-thread CTAs per SM
+// the stages' local memory does not stay in L1.
 struct BlockSink {
     float4 *inv;
     float *window;
     uint32_t window_n;
+    float *own;     // this thread's column
+    float4 *local;  // this thread's column of the pending-factor lists (shade stages)
 };
 
 __device__ __forceinline__ BlockSink open_sink(const TraceParams &P, const AdjointParams &A, float4 *smem) {
@@ -162,6 +195,11 @@ __device__ __forceinline__ BlockSink open_sink(const TraceParams &P, const Adjoi
     b.inv = smem + trace_smem_floats(P) / 4u;
     b.window = reinterpret_cast<float *>(b.inv + 2u * n_bodies);
     b.window_n = A.tau_window + A.color_window;
+    b.own = b.window + b.window_n + threadIdx.x;
+    b.local = reinterpret_cast<float4 *>(b.window + ((b.window_n + 3u) & ~3u) + 6u * kColorSlots * blockDim.x) +
+              threadIdx.x;
+#pragma unroll
+    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) b.own[k * blockDim.x] = 0.0f;
     for (uint32_t k = threadIdx.x; k < b.window_n; k += blockDim.x) b.window[k] = 0.0f;
     for (uint32_t k = threadIdx.x; k < n_bodies; k += blockDim.x) {
         const float4 m = P.bodies[k * kBodyVec4 + kMaterial], r = P.bodies[k * kBodyVec4 + kRingColor];
@@ -172,12 +210,11 @@ __device__ __forceinline__ BlockSink open_sink(const TraceParams &P, const Adjoi
 }
 
 // Reduce the per-thread sums over the warp, then flush the windows.
-__device__ __forceinline__ void close_sink(const AdjointParams &A, const BlockSink &b, const float *own,
-                                           unsigned long long dropped) {
+__device__ __forceinline__ void close_sink(const AdjointParams &A, const BlockSink &b, unsigned long long dropped) {
     const uint32_t lane = threadIdx.x & 31u;
 #pragma unroll
     for (uint32_t k = 0; k < 6u * kColorSlots; ++k) {
-        float v = own[k];
+        float v = b.own[k * blockDim.x];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0u && v != 0.0f) {
@@ -270,12 +307,10 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
     const BlockSink bs = open_sink(P, A, smem);
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
-    float own[6u * kColorSlots];
-#pragma unroll
-    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
     const uint32_t n_bodies = P.s.counts[0];
     const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
-    const GradSink sink{own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad};
+    const GradSink sink{bs.own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad,
+                        blockDim.x};
     unsigned long long dropped = 0;
     float4 *st = W.state[t & 1u];
     float4 *out = W.state[(t + 1u) & 1u];
@@ -342,24 +377,8 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
         uint32_t q[5];
         block_append<5>(sm[round & 1u], flags, ctr, q);
         if (take_slot) {
+            // The slot's state is set up by the shade stage (fresh_sample).
             slot = X.free_ring[q[4] % W.pool];
-            Prb G;
-            fresh_prb(G, w);
-            // With the forward's radiance of this sample (and no binding
-            // cap, no overflowing record), one replay with every weight
-            // known; it stops at the first checkpoint when the sample has
-            // records.
-            uint32_t extra = 0u;
-            const uint32_t sample = A.ck.sample_base + smp;
-            if (A.ck.totals && sample < A.ck.samples) {
-                const float4 tot = A.ck.totals[(size_t)sample * P.width * P.height + pixel];
-                const uint32_t bits = __float_as_uint(tot.w);
-                if (!(bits & 2u)) {
-                    segment_setup(G, w, f3(tot.x, tot.y, tot.z), f3(0.0f, 0.0f, 0.0f));
-                    if (bits & 1u) extra = kFlagStops;
-                }
-            }
-            store_prb(X, slot, G, smp, extra);
             store_adjoint_path(st, W.pool, i, p, pixel, slot);
         } else if (ring || surface) {
             st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
@@ -370,13 +389,15 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
             else H[0 * W.pool + i] = pack3(e.hit.n, e.hit.t);
             H[2 * W.pool + i] = make_float4(__uint_as_float(e.hit.index), __uint_as_float(e.ring.index), e.hit.delta,
                                             e.disc_scale);
+            const uint32_t at = ring ? q[0] : W.pool + q[1];
             if (ring) W.ring_queue[q[0]] = i;
             else W.surface_queue[q[1]] = i;
+            X.queued[at] = make_uint4(slot, pixel, smp, take_slot ? 1u : 0u);
         }
         if (restart) store_adjoint_path(out, W.pool, q[2], p, pixel, slot);
         if (give) X.free_ring[q[3] % W.pool] = slot;
     }
-    close_sink(A, bs, own, dropped);
+    close_sink(A, bs, dropped);
 }
 
 // Ring (R == true) or surface stage of the replay over its queue.
@@ -392,12 +413,10 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     const BlockSink bs = open_sink(P, A, smem);
     const Scene S = stage_scene(P, smem);
     const Counter<false, L, F> K{nullptr};
-    float own[6u * kColorSlots];
-#pragma unroll
-    for (uint32_t k = 0; k < 6u * kColorSlots; ++k) own[k] = 0.0f;
     const uint32_t n_bodies = P.s.counts[0];
     const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
-    const GradSink sink{own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad};
+    const GradSink sink{bs.own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad,
+                        blockDim.x};
     unsigned long long dropped = 0;
     const float4 *st = W.state[t & 1u];
     float4 *out = W.state[(t + 1u) & 1u];
@@ -410,18 +429,29 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
         Path p;
         Prb G;
         uint32_t pixel = 0, slot = 0, smp = 0;
+        uint32_t stops = 0u;
         if (j < n) {
+            // The path and its slot, pixel and sample come from the queue
+            // entry, so that the slot state, the pixel weight and the path
+            // state are read at once.
             const uint32_t i = queue[j];
+            const uint4 entry = X.queued[(R ? 0u : W.pool) + j];
+            slot = entry.x;
+            pixel = entry.y;
             load_ray_part(st, W.pool, i, p);
             load_radiance_part(st, W.pool, i, p);
             load_shade_part(st, W.pool, i, p);
-            const float4 g = st[6 * W.pool + i];
-            pixel = __float_as_uint(g.z);
-            slot = __float_as_uint(g.w);
             const float3 w = pixel_weight(A, pixel);
-            load_prb(X, slot, w, G, smp);
+            if (entry.w) {
+                smp = entry.z;
+                stops = fresh_sample(P, A, X, slot, pixel, smp, w, G);
+            } else {
+                stops = load_prb(X, slot, w, G, smp) & kFlagStops;
+            }
             G.sink = sink;
             G.inv = bs.inv;
+            G.local = bs.local;
+            G.local_stride = blockDim.x;
             G.iteration = p.iterations;
             const float4 h2 = H[2 * W.pool + i];
             bool ended;
@@ -437,9 +467,7 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
             keep = !ended || end_replay(P, K, G, p, pixel, smp, w);
             // A checkpointed sample's replay ends where its first record
             // starts (the same scatter that stored it in the forward).
-            if (keep && !ended && G.known_total && p.depth >= A.ck.every &&
-                (__float_as_uint(X.side[(size_t)slot * kAdjointSideVec4 + 2].w) & kFlagStops))
-                keep = false;
+            if (keep && !ended && G.known_total && p.depth >= A.ck.every && stops) keep = false;
             give = !keep;
             dropped += G.dropped;
         }
@@ -448,14 +476,12 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
         uint32_t q[2];
         block_append<2, kShadeThreads>(sm[round & 1u], flags, ctr, q);
         if (keep) {
-            const uint32_t stops =
-                G.known_total ? (__float_as_uint(X.side[(size_t)slot * kAdjointSideVec4 + 2].w) & kFlagStops) : 0u;
-            store_prb(X, slot, G, smp, stops);
+            store_prb(X, slot, G, smp, G.known_total ? stops : 0u);
             store_adjoint_path(out, W.pool, q[0], p, pixel, slot);
         }
         if (give) X.free_ring[q[1] % W.pool] = slot;
     }
-    close_sink(A, bs, own, dropped);
+    close_sink(A, bs, dropped);
 }
 
 __global__ void adj_reset_slots(uint32_t *ring, uint32_t *ends, uint32_t pool) {
@@ -469,19 +495,19 @@ __global__ void adj_reset_slots(uint32_t *ring, uint32_t *ends, uint32_t pool) {
 
 template <bool L, bool F>
 cudaError_t run_adjoint_iteration(const TraceParams &p, const AdjointParams &a, const WaveParams &w,
-                                  const AdjointWave &x, uint32_t t, const int (&grid)[3], size_t smem,
+                                  const AdjointWave &x, uint32_t t, const int (&grid)[3], const size_t (&smem)[2],
                                   cudaStream_t stream) {
-    adj_extend<L, F><<<grid[0], kThreads, smem, stream>>>(p, a, w, x, t);
-    adj_shade<L, F, true><<<grid[1], kShadeThreads, smem, stream>>>(p, a, w, x, t);
-    adj_shade<L, F, false><<<grid[2], kShadeThreads, smem, stream>>>(p, a, w, x, t);
+    adj_extend<L, F><<<grid[0], kThreads, smem[0], stream>>>(p, a, w, x, t);
+    adj_shade<L, F, true><<<grid[1], kShadeThreads, smem[1], stream>>>(p, a, w, x, t);
+    adj_shade<L, F, false><<<grid[2], kShadeThreads, smem[1], stream>>>(p, a, w, x, t);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 size_t adjoint_slot_bytes(uint32_t pool) {
-    return (size_t)pool * (kAdjointSideVec4 * sizeof(float4) + sizeof(PrbLists)) + (size_t)pool * sizeof(uint32_t) +
-           4 * sizeof(uint32_t);
+    return (size_t)pool * (kAdjointSideVec4 * sizeof(float4) + 2u * sizeof(uint4) + sizeof(PrbLists)) +
+           (size_t)pool * sizeof(uint32_t) + 4 * sizeof(uint32_t);
 }
 
 cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t pool, cudaStream_t stream) {
@@ -506,14 +532,20 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
         fns[1] = p.fp64_sites ? (const void *)adj_shade<false, true, true> : (const void *)adj_shade<false, false, true>;
         fns[2] = p.fp64_sites ? (const void *)adj_shade<false, true, false> : (const void *)adj_shade<false, false, false>;
     }
-    const size_t smem = adjoint_smem_bytes(p, a);
+    // After the adjoint's shared memory: the per-thread colour sums, and in
+    // the shade stages the pending-factor lists (16-byte aligned).
+    const size_t smem[2] = {
+        adjoint_smem_bytes(p, a) + (size_t)6u * kColorSlots * kThreads * sizeof(float),
+        adjoint_smem_bytes(p, a) + 16u + (size_t)6u * kColorSlots * kShadeThreads * sizeof(float) +
+            (size_t)kMaxLocal * kShadeThreads * sizeof(float4)};
     int grid[3];
     for (int k = 0; k < 3; ++k) {
-        if (smem > 48u * 1024u) {
-            cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const size_t bytes = smem[k == 0 ? 0 : 1];
+        if (bytes > 48u * 1024u) {
+            cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
             if (e != cudaSuccess) return e;
         }
-        cudaError_t e = persistent_grid(fns[k], smem, &grid[k], k == 0 ? kThreads : kShadeThreads);
+        cudaError_t e = persistent_grid(fns[k], bytes, &grid[k], k == 0 ? kThreads : kShadeThreads);
         if (e != cudaSuccess) return e;
     }
     w.tiles_x = (p.width + kTile - 1) / kTile;

@@ -57,7 +57,12 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
     // Celestial frames take several paths per append (their work per path
     // is even); landscape frames one, so that a CTA's last round is small
     // when traversal costs differ (measured: rings 59.5 -> 56.5 ms per step
-    // with four, terrain 455 -> 531 ms).
+    // with four, terrain 455 -> 531 ms). Landscape frames keep the append
+    // barrier although their quadtree walks differ in length: writing a
+    // per-path kind instead and building the queues in a kernel of their
+    // own let the warps of a CTA drift apart, and the terrain step went
+    // from 450 to 513 ms (the barrier keeps neighbouring pixels' walks
+    // through the same quadtree nodes at the same time, in L1).
     constexpr uint32_t kItems = L ? 1u : SG_WAVE_EXTEND_ITEMS;
     __shared__ AppendK<2, kItems> sm[2];
     WaveCounters *c = counters(W, t);
