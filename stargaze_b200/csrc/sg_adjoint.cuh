@@ -132,25 +132,32 @@ struct Stage {
 };
 
 // A Russian-roulette decision after the cap vertex (pathtrace.wgsl:
-// 1484-1490, :1600-1604).
+// 1484-1490, :1600-1604); its record (PrbLists::rr) also holds the radiance
+// gathered since the cap vertex, before it.
 struct Roulette {
     uint32_t iteration;
     uint32_t bits;  // max channel (0-2) | 4 survived | 8 survival clamped
     float s;        // survival probability
-    float3 before;  // radiance gathered since the cap vertex, before it
 };
 
 // The lists a path's adjoint appends to: Russian-roulette events after the
 // cap vertex (with pass 2's coefficient of each) and pass 1's deferred
 // throughput factors with the running sum at each. The per-pixel adjoint
 // keeps them in the thread's local memory, the staged adjoint in a device
-// slot that stays with the path across stages.
+// slot that stays with the path across stages. Each entry is one 32-byte
+// record (one DRAM sector in device memory, written whole):
+//   fac[k]: (param, dlog.xyz), (running sum at the factor, 0)
+//   rr[r]:  (iteration, bits, s, pass 2's coefficient), (before.xyz, 0)
 struct PrbLists {
-    Roulette rr[kMaxRoulette];
-    float rr_coef[kMaxRoulette];
-    GradEntry fac[kMaxDeferred];
-    float3 fac_at[kMaxDeferred];
+    float4 fac[kMaxDeferred][2];
+    float4 rr[kMaxRoulette][2];
 };
+
+__device__ __forceinline__ Roulette roulette_at(const PrbLists *l, uint32_t r, float &coef) {
+    const float4 a = l->rr[r][0];
+    coef = a.w;
+    return Roulette{__float_as_uint(a.x), __float_as_uint(a.y), a.z};
+}
 
 // The adjoint's state. Both passes run the same integrator code (one
 // instantiation, so a warp's instruction footprint is that of one replay);
@@ -271,8 +278,8 @@ static __device__ SG_ADJ_HOOK void factor(Prb &G, GradEntry e) {
     if (!G.pass2) {
         // Pass 1: defer until the path's end.
         if (G.n_fac < (uint32_t)kMaxDeferred) {
-            G.lists->fac[G.n_fac] = e;
-            G.lists->fac_at[G.n_fac] = G.a;
+            G.lists->fac[G.n_fac][0] = pack_entry(e);
+            G.lists->fac[G.n_fac][1] = make_float4(G.a.x, G.a.y, G.a.z, 0.0f);
             G.n_fac += 1u;
         } else {
             G.deferral_full = true;
@@ -291,10 +298,10 @@ static __device__ SG_ADJ_HOOK void factor(Prb &G, GradEntry e) {
         int prev = -1;
 #pragma unroll 1
         for (uint32_t r = 0; r < G.n_rr; ++r) {
-            const Roulette ev = G.lists->rr[r];
+            float c;
+            const Roulette ev = roulette_at(G.lists, r, c);
             if (ev.iteration < G.iteration || (ev.bits & 8u)) continue;
             const uint32_t m = ev.bits & 3u;
-            const float c = G.lists->rr_coef[r];
             if (vec) {
                 const float dm = c * channel(e.dlog, m);
                 add = f3(add.x + (m == 0u ? dm : 0.0f), add.y + (m == 1u ? dm : 0.0f), add.z + (m == 2u ? dm : 0.0f));
@@ -599,7 +606,11 @@ static __device__ SG_ADJ_HOOK void record_roulette(Prb &G, uint32_t iteration, f
     const float mx = fmaxf(t.x, fmaxf(t.y, t.z));
     const uint32_t m = t.x >= mx ? 0u : (t.y >= mx ? 1u : 2u);
     const bool clamped = !(mx > 0.05f && mx < 0.95f);
-    G.lists->rr[G.n_rr++] = Roulette{iteration, m | (survived ? 4u : 0u) | (clamped ? 8u : 0u), s, radiance - G.base};
+    const float3 before = radiance - G.base;
+    const uint32_t bits = m | (survived ? 4u : 0u) | (clamped ? 8u : 0u);
+    G.lists->rr[G.n_rr][0] = make_float4(__uint_as_float(iteration), __uint_as_float(bits), s, 0.0f);
+    G.lists->rr[G.n_rr][1] = make_float4(before.x, before.y, before.z, 0.0f);
+    G.n_rr += 1u;
 }
 
 // Start of pass 1 for a pixel weight w.
@@ -636,8 +647,8 @@ __device__ __forceinline__ bool cap_binds(const Prb &G, float3 total) {
 static __device__ SG_ADJ_HOOK void flush_deferred(Prb &G) {
 #pragma unroll 1
     for (uint32_t k = 0; k < G.n_fac; ++k) {
-        const GradEntry e = G.lists->fac[k];
-        const float3 rem = G.a - G.lists->fac_at[k];
+        const GradEntry e = unpack_entry(G.lists->fac[k][0]);
+        const float3 rem = G.a - xyz(G.lists->fac[k][1]);
         if (e.param & kVectorBit) {
             const uint32_t base = e.param & ~kVectorBit;
             G.sink.add(base + 0u, rem.x * e.dlog.x);
@@ -685,10 +696,11 @@ static __device__ SG_ADJ_HOOK void pass2_setup(Prb &G, float3 total, float3 w) {
         G.score = (s - 1.0f) * dot(w, indirect);
         G.b_total = mul3(G.w_pdf, indirect);
         for (uint32_t r = 0; r < G.n_rr && r < (uint32_t)kMaxRoulette; ++r) {
-            const Roulette ev = G.lists->rr[r];
-            const bool survived = (ev.bits & 4u) != 0u;
-            G.lists->rr_coef[r] = survived ? G.score - dot(G.w_pdf, indirect - ev.before)
-                                    : -G.score * ev.s / (1.0f - ev.s);
+            const float4 head = G.lists->rr[r][0];
+            const float3 before = xyz(G.lists->rr[r][1]);
+            const bool survived = (__float_as_uint(head.y) & 4u) != 0u;
+            const float sr = head.z;
+            G.lists->rr[r][0].w = survived ? G.score - dot(G.w_pdf, indirect - before) : -G.score * sr / (1.0f - sr);
         }
     } else {
         G.n_rr = 0;
