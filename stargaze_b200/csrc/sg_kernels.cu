@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(256) terrain_cache_kernel(float *T, uint32_t c
 
 }  // namespace
 
-size_t terrain_source_floats(uint32_t cells) { return (size_t)t_cache(cells); }
+size_t terrain_source_floats(uint32_t cells) { return (size_t)t_source(cells); }
 size_t terrain_floats(uint32_t cells) {
     return (size_t)t_vertex_cache(cells) + (size_t)t_vertices(cells) * t_vertex_stride(cells);
 }

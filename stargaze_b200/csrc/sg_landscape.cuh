@@ -163,7 +163,16 @@ __host__ __device__ __forceinline__ uint32_t t_nodes(uint32_t cells) {
 __host__ __device__ __forceinline__ uint32_t t_bounds(uint32_t cells) {
     return (t_compact(cells) ? 1u : 3u) * t_vertices(cells);
 }
-__host__ __device__ __forceinline__ uint32_t t_cache(uint32_t cells) { return t_bounds(cells) + 2u * t_nodes(cells); }
+// The uploaded source: vertex bounds (heights, or heights and gradients)
+// and each node's height range.
+__host__ __device__ __forceinline__ uint32_t t_source(uint32_t cells) { return t_bounds(cells) + 2u * t_nodes(cells); }
+// The node boxes (6 floats each) start 2 floats past a 16-byte boundary, so
+// the four children of any node (indices 4k+1 .. 4k+4, 96 contiguous
+// bytes) start on one: a node expansion reads them as six float4.
+__host__ __device__ __forceinline__ uint32_t t_cache(uint32_t cells) {
+    const uint32_t s = t_source(cells);
+    return s + ((2u - (s & 3u)) & 3u);
+}
 __host__ __device__ __forceinline__ uint32_t t_vertex_cache(uint32_t cells) { return t_cache(cells) + 6u * t_nodes(cells); }
 
 __device__ __forceinline__ float t_scale_r(float r) { return clampf(__fdiv_rn(r, 200000.0f), 0.0001f, 1.0f); }
@@ -225,10 +234,8 @@ __device__ __forceinline__ float3 t_triangle(float3 o, float3 d, float3 a, float
     return f3(u, v, distance);
 }
 
-// terrain_interval (terrain.wgsl:118-130).
-__device__ __forceinline__ float2 t_interval(const float *T, uint32_t cells, float3 o, float3 inv, uint32_t index) {
-    const float *c = T + t_cache(cells) + (size_t)index * 6u;
-    const float3 lo = f3(c[0], c[1], c[2]), hi = f3(c[3], c[4], c[5]);
+// terrain_interval (terrain.wgsl:118-130) of the box [lo, hi].
+__device__ __forceinline__ float2 t_interval(float3 lo, float3 hi, float3 o, float3 inv) {
     const bool px = fabsf(inv.x) >= 1.0e29f, py = fabsf(inv.y) >= 1.0e29f, pz = fabsf(inv.z) >= 1.0e29f;
     if ((px && (o.x < lo.x || o.x > hi.x)) || (py && (o.y < lo.y || o.y > hi.y)) || (pz && (o.z < lo.z || o.z > hi.z)))
         return make_float2(1.0e30f, -1.0e30f);
@@ -252,7 +259,8 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
     const float3 inv = f3(__fdiv_rn(d.x >= 0.0f ? 1.0f : -1.0f, fmaxf(fabsf(d.x), 1.0e-30f)),
                           __fdiv_rn(d.y >= 0.0f ? 1.0f : -1.0f, fmaxf(fabsf(d.y), 1.0e-30f)),
                           __fdiv_rn(d.z >= 0.0f ? 1.0f : -1.0f, fmaxf(fabsf(d.z), 1.0e-30f)));
-    const float2 root = t_interval(T, cells, o, inv, 0u);
+    const float *rc = T + t_cache(cells);
+    const float2 root = t_interval(f3(rc[0], rc[1], rc[2]), f3(rc[3], rc[4], rc[5]), o, inv);
     if (root.x > root.y || root.y <= 0.001f || root.x >= limit) return result;
     uint32_t stack_node[kTerrainStack];
     float stack_t[kTerrainStack];
@@ -303,10 +311,14 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
             if constexpr (C) ev->terrain_nodes += 1u;
             uint32_t children[4];
             float distances[4];
+            const float4 *box = reinterpret_cast<const float4 *>(T + t_cache(cells) + (size_t)(index * 4u + 1u) * 6u);
+            const float4 q0 = box[0], q1 = box[1], q2 = box[2], q3 = box[3], q4 = box[4], q5 = box[5];
+            const float3 lo[4] = {f3(q0.x, q0.y, q0.z), f3(q1.z, q1.w, q2.x), f3(q3.x, q3.y, q3.z), f3(q4.z, q4.w, q5.x)};
+            const float3 hi[4] = {f3(q0.w, q1.x, q1.y), f3(q2.y, q2.z, q2.w), f3(q3.w, q4.x, q4.y), f3(q5.y, q5.z, q5.w)};
 #pragma unroll
             for (uint32_t child = 0; child < 4u; ++child) {
                 children[child] = index * 4u + child + 1u;
-                const float2 bounds = t_interval(T, cells, o, inv, children[child]);
+                const float2 bounds = t_interval(lo[child], hi[child], o, inv);
                 distances[child] =
                     (bounds.x <= bounds.y && bounds.y > 0.001f && bounds.x < limit) ? fmaxf(bounds.x, 0.0f) : 1.0e30f;
             }
