@@ -270,44 +270,46 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
     while (count > 0u) {
         count -= 1u;
         if (stack_t[count] >= limit) continue;
-        const uint32_t index = stack_node[count];
-        // The node's size from its heap level; its cell coordinates (the
-        // Morton decode of t_node) only where a leaf needs them.
-        const uint32_t size = cells >> ((31u - __clz(3u * index + 1u)) / 2u);
-        if (size == 2u) {
-            const uint3 node = t_node(index, cells);
+        uint32_t index = stack_node[count];
+        for (;;) {
+            // The node's size from its heap level; its cell coordinates (the
+            // Morton decode of t_node) only where a leaf needs them.
+            const uint32_t size = cells >> ((31u - __clz(3u * index + 1u)) / 2u);
+            if (size == 2u) {
+                const uint3 node = t_node(index, cells);
 #pragma unroll 1
-            for (uint32_t z = node.y; z < node.y + 2u; ++z) {
+                for (uint32_t z = node.y; z < node.y + 2u; ++z) {
 #pragma unroll 1
-                for (uint32_t x = node.x; x < node.x + 2u; ++x) {
-                    if constexpr (C) ev->terrain_triangles += 2u;
-                    const float3 a = t_vertex(T, cells, scale, x, z);
-                    const float3 b = t_vertex(T, cells, scale, x + 1u, z);
-                    const float3 c = t_vertex(T, cells, scale, x, z + 1u);
-                    const float3 e = t_vertex(T, cells, scale, x + 1u, z + 1u);
-                    const float3 first = t_triangle(o, d, a, c, b);
-                    const float3 second = t_triangle(o, d, e, b, c);
-                    if (first.z < limit) {
-                        if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, first.z);
-                        float3 n = normalize(t_normal(T, cells, x, z) * (1.0f - first.x - first.y) +
-                                             t_normal(T, cells, x, z + 1u) * first.x +
-                                             t_normal(T, cells, x + 1u, z) * first.y);
-                        if (alpine) n = style::alpine_face_shading(n, a, c, b);
-                        result = make_float4(n.x, n.y, n.z, first.z);
-                        limit = first.z;
-                    }
-                    if (second.z < limit) {
-                        if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, second.z);
-                        float3 n = normalize(t_normal(T, cells, x + 1u, z + 1u) * (1.0f - second.x - second.y) +
-                                             t_normal(T, cells, x + 1u, z) * second.x +
-                                             t_normal(T, cells, x, z + 1u) * second.y);
-                        if (alpine) n = style::alpine_face_shading(n, e, b, c);
-                        result = make_float4(n.x, n.y, n.z, second.z);
-                        limit = second.z;
+                    for (uint32_t x = node.x; x < node.x + 2u; ++x) {
+                        if constexpr (C) ev->terrain_triangles += 2u;
+                        const float3 a = t_vertex(T, cells, scale, x, z);
+                        const float3 b = t_vertex(T, cells, scale, x + 1u, z);
+                        const float3 c = t_vertex(T, cells, scale, x, z + 1u);
+                        const float3 e = t_vertex(T, cells, scale, x + 1u, z + 1u);
+                        const float3 first = t_triangle(o, d, a, c, b);
+                        const float3 second = t_triangle(o, d, e, b, c);
+                        if (first.z < limit) {
+                            if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, first.z);
+                            float3 n = normalize(t_normal(T, cells, x, z) * (1.0f - first.x - first.y) +
+                                                 t_normal(T, cells, x, z + 1u) * first.x +
+                                                 t_normal(T, cells, x + 1u, z) * first.y);
+                            if (alpine) n = style::alpine_face_shading(n, a, c, b);
+                            result = make_float4(n.x, n.y, n.z, first.z);
+                            limit = first.z;
+                        }
+                        if (second.z < limit) {
+                            if (occlusion) return make_float4(0.0f, 0.0f, 0.0f, second.z);
+                            float3 n = normalize(t_normal(T, cells, x + 1u, z + 1u) * (1.0f - second.x - second.y) +
+                                                 t_normal(T, cells, x + 1u, z) * second.x +
+                                                 t_normal(T, cells, x, z + 1u) * second.y);
+                            if (alpine) n = style::alpine_face_shading(n, e, b, c);
+                            result = make_float4(n.x, n.y, n.z, second.z);
+                            limit = second.z;
+                        }
                     }
                 }
+                break;
             }
-        } else {
             if constexpr (C) ev->terrain_nodes += 1u;
             uint32_t children[4];
             float distances[4];
@@ -322,7 +324,7 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
                 distances[child] =
                     (bounds.x <= bounds.y && bounds.y > 0.001f && bounds.x < limit) ? fmaxf(bounds.x, 0.0f) : 1.0e30f;
             }
-            // Far first on the stack: the nearest child is popped first.
+            // Far first on the stack; the nearest child is visited next.
             // The reference's insertion sort, as a fixed sequence of
             // compare-exchanges that swap only on a strictly nearer left
             // element: once an element stops, the ones before it are no
@@ -342,13 +344,17 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
                 }
             }
 #pragma unroll
-            for (uint32_t i = 0; i < 4u; ++i) {
+            for (uint32_t i = 0; i < 3u; ++i) {
                 if (distances[i] < limit && count < (uint32_t)kTerrainStack) {
                     stack_node[count] = children[i];
                     stack_t[count] = distances[i];
                     count += 1u;
                 }
             }
+            // The nearest child would be pushed last and popped at once
+            // with the same limit: descend into it directly.
+            if (!(distances[3] < limit && count < (uint32_t)kTerrainStack)) break;
+            index = children[3];
         }
     }
     return result;
