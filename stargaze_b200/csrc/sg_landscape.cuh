@@ -176,8 +176,11 @@ __host__ __device__ __forceinline__ uint32_t t_cache(uint32_t cells) {
 __host__ __device__ __forceinline__ uint32_t t_vertex_cache(uint32_t cells) { return t_cache(cells) + 6u * t_nodes(cells); }
 
 __device__ __forceinline__ float t_scale_r(float r) { return clampf(__fdiv_rn(r, 200000.0f), 0.0001f, 1.0f); }
+// 2 i / cells: cells is a power of two, so the IEEE quotient is the exact
+// product with 2^-log2(cells).
 __device__ __forceinline__ float t_coordinate(uint32_t i, uint32_t cells, float scale) {
-    const float u = __fsub_rn(__fdiv_rn(__fmul_rn(2.0f, (float)i), (float)cells), 1.0f);
+    const float inv_cells = __uint_as_float((127u - (31u - __clz(cells))) << 23);
+    const float u = __fsub_rn(__fmul_rn(__fmul_rn(2.0f, (float)i), inv_cells), 1.0f);
     return __fmul_rn(__fmul_rn(__fmul_rn(u, fabsf(u)), 16000.0f), scale);
 }
 __device__ __forceinline__ float t_curvature(float px, float pz, float r) {
@@ -199,6 +202,10 @@ __device__ __forceinline__ uint3 t_node(uint32_t index, uint32_t cells) {
     return make_uint3(compact_bits(morton) * size, compact_bits(morton >> 1) * size, size);
 }
 
+// The cached (curved) height of a vertex of a compact grid.
+__device__ __forceinline__ float t_height(const float *T, uint32_t cells, uint32_t x, uint32_t z) {
+    return T[t_vertex_cache(cells) + (size_t)(z * t_width(cells) + x) * t_vertex_stride(cells)];
+}
 __device__ __forceinline__ float3 t_vertex(const float *T, uint32_t cells, float scale, uint32_t x, uint32_t z) {
     const float *v = T + t_vertex_cache(cells) + (size_t)(z * t_width(cells) + x) * t_vertex_stride(cells);
     if (t_compact(cells)) return f3(t_coordinate(x, cells, scale), v[0], t_coordinate(z, cells, scale));
@@ -277,15 +284,37 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
             const uint32_t size = cells >> ((31u - __clz(3u * index + 1u)) / 2u);
             if (size == 2u) {
                 const uint3 node = t_node(index, cells);
+                // On compact grids a vertex's x and z come from its indices:
+                // the leaf's three columns and rows once, not per triangle.
+                const bool compact = t_compact(cells);
+                float cx[3] = {0.0f, 0.0f, 0.0f}, cz[3] = {0.0f, 0.0f, 0.0f};
+                if (compact) {
+#pragma unroll
+                    for (uint32_t k = 0; k < 3u; ++k) {
+                        cx[k] = t_coordinate(node.x + k, cells, scale);
+                        cz[k] = t_coordinate(node.y + k, cells, scale);
+                    }
+                }
 #pragma unroll 1
                 for (uint32_t z = node.y; z < node.y + 2u; ++z) {
 #pragma unroll 1
                     for (uint32_t x = node.x; x < node.x + 2u; ++x) {
                         if constexpr (C) ev->terrain_triangles += 2u;
-                        const float3 a = t_vertex(T, cells, scale, x, z);
-                        const float3 b = t_vertex(T, cells, scale, x + 1u, z);
-                        const float3 c = t_vertex(T, cells, scale, x, z + 1u);
-                        const float3 e = t_vertex(T, cells, scale, x + 1u, z + 1u);
+                        float3 a, b, c, e;
+                        if (compact) {
+                            const bool x1 = x != node.x, z1 = z != node.y;
+                            const float x0c = x1 ? cx[1] : cx[0], x1c = x1 ? cx[2] : cx[1];
+                            const float z0c = z1 ? cz[1] : cz[0], z1c = z1 ? cz[2] : cz[1];
+                            a = f3(x0c, t_height(T, cells, x, z), z0c);
+                            b = f3(x1c, t_height(T, cells, x + 1u, z), z0c);
+                            c = f3(x0c, t_height(T, cells, x, z + 1u), z1c);
+                            e = f3(x1c, t_height(T, cells, x + 1u, z + 1u), z1c);
+                        } else {
+                            a = t_vertex(T, cells, scale, x, z);
+                            b = t_vertex(T, cells, scale, x + 1u, z);
+                            c = t_vertex(T, cells, scale, x, z + 1u);
+                            e = t_vertex(T, cells, scale, x + 1u, z + 1u);
+                        }
                         const float3 first = t_triangle(o, d, a, c, b);
                         const float3 second = t_triangle(o, d, e, b, c);
                         if (first.z < limit) {
