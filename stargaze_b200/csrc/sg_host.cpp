@@ -92,8 +92,7 @@ struct sg_context {
     void *adjoint_slots = nullptr;          // staged adjoint: slot state, lists, free ring
     size_t adjoint_slots_size = 0;
     size_t wave_results_size = 0;
-    sg::WaveCounters *wave_pinned = nullptr;
-    cudaEvent_t wave_ready = nullptr;
+    sg::WaveProgress wave_progress;         // the stage loops' progress ring (mapped host memory)
     uint32_t wave_iterations = 0;           // stage iterations of the last dispatch
     // Sky backdrop: catalogue (2 float4 per star), cell table, panorama.
     float4 *catalogue = nullptr;
@@ -534,8 +533,9 @@ int sg_destroy(sg_context *ctx) {
     cudaFree(ctx->milky_way);
     cudaFree(ctx->sky_samples);
     cudaFree(ctx->sky_light);
-    if (ctx->wave_pinned) cudaFreeHost(ctx->wave_pinned);
-    if (ctx->wave_ready) cudaEventDestroy(ctx->wave_ready);
+    if (ctx->wave_progress.host) cudaFreeHost(ctx->wave_progress.host);
+    for (cudaEvent_t e : ctx->wave_progress.done)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->stage_marks.events) cudaEventDestroy(e);
     delete ctx;
     return SG_OK;
@@ -751,8 +751,14 @@ static int ensure_wave_state(sg_context *ctx, uint32_t pool, sg::WaveParams &w) 
         SG_CUDA(ctx, cudaMalloc(&ctx->wave_state, state_bytes));
         ctx->wave_state_size = state_bytes;
     }
-    if (!ctx->wave_pinned) SG_CUDA(ctx, cudaMallocHost(&ctx->wave_pinned, sizeof(sg::WaveCounters)));
-    if (!ctx->wave_ready) SG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->wave_ready, cudaEventDisableTiming));
+    sg::WaveProgress &pr = ctx->wave_progress;
+    if (!pr.host) {
+        SG_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void **>(&pr.host), sg::kProgressSlots * sizeof(uint2),
+                                   cudaHostAllocMapped));
+        SG_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void **>(&pr.device), pr.host, 0));
+    }
+    for (cudaEvent_t &e : pr.done)
+        if (!e) SG_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     float4 *base = ctx->wave_state;
     w.state[0] = base;
     w.state[1] = base + (size_t)sg::kWavePlanes * pool;
@@ -760,6 +766,7 @@ static int ensure_wave_state(sg_context *ctx, uint32_t pool, sg::WaveParams &w) 
     w.ring_queue = reinterpret_cast<uint32_t *>(w.hits + (size_t)sg::kWaveHitPlanes * pool);
     w.surface_queue = w.ring_queue + pool;
     w.counters = reinterpret_cast<sg::WaveCounters *>(w.surface_queue + pool);
+    w.progress = pr.device;
     w.pool = pool;
     w.tiles_x = w.tiles_y = 0;
     w.chunk_first = 0;
@@ -973,7 +980,7 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
             }
             sg::WaveRun run;
             sg::StageMarks *marks = ctx->stage_timing ? &ctx->stage_marks : nullptr;
-            cudaError_t e = sg::launch_wavefront(p, w, ctx->wave_pinned, ctx->wave_ready, stream, &run, marks);
+            cudaError_t e = sg::launch_wavefront(p, w, ctx->wave_progress, stream, &run, marks);
             ctx->wave_iterations = run.iterations;
             ctx->launches += run.kernels;
             if (e == cudaErrorLaunchTimeout)
@@ -1565,8 +1572,7 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
             if (status != SG_OK) return status;
             if (staged) {
                 sg::WaveRun run;
-                cudaError_t e =
-                    sg::launch_adjoint_wavefront(p, a, w, x, ctx->wave_pinned, ctx->wave_ready, stream, &run);
+                cudaError_t e = sg::launch_adjoint_wavefront(p, a, w, x, ctx->wave_progress, stream, &run);
                 ctx->launches += run.kernels;
                 if (e == cudaErrorLaunchTimeout)
                     return fail(ctx, SG_ERR_TIMEOUT, "staged adjoint did not drain within its iteration bound");

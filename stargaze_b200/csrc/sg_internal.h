@@ -112,6 +112,18 @@ struct WaveCounters {
 };
 // Iteration t uses counter sets t and t + 1 (mod this) and clears t + 2.
 constexpr uint32_t kWaveCounterSets = 8;
+
+// How far the GPU has got through a stage loop: at its start, extend of
+// iteration t writes (paths kept, next sample) to slot t % kProgressSlots of
+// a ring in mapped host memory, and the host records done[t % ...] after
+// the iteration. The host enqueues iterations ahead of the one it inspects,
+// so the GPU does not wait for it between iterations.
+constexpr uint32_t kProgressSlots = 8;
+struct WaveProgress {
+    uint2 *host = nullptr;    // mapped pinned memory, kProgressSlots slots
+    uint2 *device = nullptr;  // its device address
+    cudaEvent_t done[kProgressSlots] = {};
+};
 // Float4 planes of one path's state, and of one extend result.
 constexpr uint32_t kWavePlanes = 7;
 constexpr uint32_t kWaveHitPlanes = 3;
@@ -144,6 +156,7 @@ struct WaveParams {
     uint32_t *ring_queue;     // `pool` path indices
     uint32_t *surface_queue;  // `pool` path indices
     WaveCounters *counters;   // kWaveCounterSets sets
+    uint2 *progress;          // WaveProgress::device
     float4 *results;          // chunk_samples planes of width * height radiance samples
     float4 *totals;           // per-pixel running sums between chunks
     float4 *sky_results;      // as results, the backdrop of each sample (null: no sky)
@@ -176,12 +189,12 @@ struct WaveRun {
 };
 
 // Runs the dispatch described by `p` (counts.z samples) in chunks of at
-// most w.chunk_samples samples. Between groups of iterations it copies the
-// live counters into `pinned` (host memory) and waits on `ready` to decide
-// whether the chunk has drained, so it returns once the GPU has finished
-// all but the final resolve. With `marks`, events bracket every stage.
-cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *pinned, cudaEvent_t ready,
-                             cudaStream_t stream, WaveRun *run, StageMarks *marks);
+// most w.chunk_samples samples. It reads the GPU's progress (`progress`,
+// w.progress its device ring) a few iterations behind the last one it
+// enqueued to decide whether the chunk has drained, so it returns once the
+// GPU has nearly finished. With `marks`, events bracket every stage.
+cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveProgress &progress, cudaStream_t stream,
+                             WaveRun *run, StageMarks *marks);
 cudaError_t launch_closest_hit(const TraceParams &p, const sg_ray *rays, sg_hit *hits, uint32_t n,
                                cudaStream_t stream);
 cudaError_t launch_light_visibility(const TraceParams &p, const sg_ray *rays, const uint32_t *lights,
@@ -270,20 +283,20 @@ struct AdjointWave {
     uint4 *queued;        // 2 * pool: per ring-queue entry, then per surface-queue entry,
                           // (slot, pixel, sample, 1 if the sample starts in this iteration)
     void *lists;          // one PrbLists per slot
-    uint32_t *free_ring;  // `pool` slot ids
-    uint32_t *free_ends;  // [0] next allocation, [1] next free position (monotonic)
+    uint32_t *free_ring;  // `pool` slot ids: give-back k writes position k % pool
+    uint32_t *free_ends;  // [0] allocations, [1] give-backs so far (monotonic)
 };
 
 // Bytes of the adjoint slots for `pool` paths.
 size_t adjoint_slot_bytes(uint32_t pool);
 
-// Puts every slot of `x` on the free ring; once per backward call.
+// Makes every slot of `x` free (both counters to zero: allocation j < pool
+// takes slot j); once per backward call.
 cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t pool, cudaStream_t stream);
 
 // The samples of `p` (as launch_adjoint) through the stages; returns once
 // they have drained (host checks as launch_wavefront).
 cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &a, WaveParams w,
-                                     const AdjointWave &x, WaveCounters *pinned, cudaEvent_t ready,
-                                     cudaStream_t stream, WaveRun *run);
+                                     const AdjointWave &x, WaveProgress &progress, cudaStream_t stream, WaveRun *run);
 
 }  // namespace sg

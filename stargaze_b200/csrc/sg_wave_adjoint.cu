@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters(W, t + 1u)->next = next + take;
         *counters(W, t + 2u) = WaveCounters{};
+        W.progress[t % kProgressSlots] = make_uint2(kept, next);
     }
     if (blockIdx.x * kThreads >= n) return;
     const BlockSink bs = open_sink(P, A, smem);
@@ -378,7 +379,10 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_ADJ_EXTEND_MIN_BLOCKS)
         block_append<5>(sm[round & 1u], flags, ctr, q);
         if (take_slot) {
             // The slot's state is set up by the shade stage (fresh_sample).
-            slot = X.free_ring[q[4] % W.pool];
+            // Allocation j takes slot j while j < pool, then the slot that
+            // give-back j - pool wrote (in an earlier launch: a launch's
+            // fresh paths fit in the slots free at its start).
+            slot = q[4] < W.pool ? q[4] : X.free_ring[q[4] % W.pool];
             store_adjoint_path(st, W.pool, i, p, pixel, slot);
         } else if (ring || surface) {
             st[1 * W.pool + i] = pack3u(p.ray.d, p.rng);
@@ -484,15 +488,6 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     close_sink(A, bs, dropped);
 }
 
-__global__ void adj_reset_slots(uint32_t *ring, uint32_t *ends, uint32_t pool) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < pool) ring[k] = k;
-    if (k == 0) {
-        ends[0] = 0u;
-        ends[1] = pool;
-    }
-}
-
 template <bool L, bool F>
 cudaError_t run_adjoint_iteration(const TraceParams &p, const AdjointParams &a, const WaveParams &w,
                                   const AdjointWave &x, uint32_t t, const int (&grid)[3], const size_t (&smem)[2],
@@ -510,14 +505,12 @@ size_t adjoint_slot_bytes(uint32_t pool) {
            (size_t)pool * sizeof(uint32_t) + 4 * sizeof(uint32_t);
 }
 
-cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t pool, cudaStream_t stream) {
-    adj_reset_slots<<<(pool + 255u) / 256u, 256, 0, stream>>>(x.free_ring, x.free_ends, pool);
-    return cudaGetLastError();
+cudaError_t reset_adjoint_slots(const AdjointWave &x, uint32_t, cudaStream_t stream) {
+    return cudaMemsetAsync(x.free_ends, 0, 2 * sizeof(uint32_t), stream);
 }
 
 cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &a, WaveParams w,
-                                     const AdjointWave &x, WaveCounters *pinned, cudaEvent_t ready,
-                                     cudaStream_t stream, WaveRun *run) {
+                                     const AdjointWave &x, WaveProgress &progress, cudaStream_t stream, WaveRun *run) {
     *run = WaveRun{};
     const uint32_t z = p.s.counts[2];
     if (z == 0 || p.width == 0 || p.height == 0) return cudaSuccess;
@@ -559,8 +552,6 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
     const uint64_t bound = ((uint64_t)samples + 1u) * cap;
     cudaError_t e = cudaMemsetAsync(w.counters, 0, kWaveCounterSets * sizeof(WaveCounters), stream);
     if (e != cudaSuccess) return e;
-    constexpr uint64_t kTailCheck = 2;
-    uint64_t check_at = (samples + (uint64_t)w.pool - 1u) / w.pool;
     for (uint64_t t = 0;; ++t) {
         if (t >= bound) return cudaErrorLaunchTimeout;
         const uint32_t it = (uint32_t)t;
@@ -569,16 +560,13 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
                  : (p.fp64_sites ? run_adjoint_iteration<false, true>(p, a, w, x, it, grid, smem, stream)
                                  : run_adjoint_iteration<false, false>(p, a, w, x, it, grid, smem, stream));
         if (e != cudaSuccess) return e;
+        if ((e = iteration_done(progress, t, stream)) != cudaSuccess) return e;
         run->iterations += 1;
         run->kernels += 3;
-        if (t + 1 < check_at) continue;
-        const WaveCounters *dev = w.counters + ((t + 1) % kWaveCounterSets);
-        if ((e = cudaMemcpyAsync(pinned, dev, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-            (e = cudaEventRecord(ready, stream)) != cudaSuccess || (e = cudaEventSynchronize(ready)) != cudaSuccess)
-            return e;
-        if (pinned->cont == 0 && pinned->next >= samples) break;
-        const uint64_t left = pinned->next >= samples ? 0u : samples - pinned->next;
-        check_at = t + 1 + (left ? (left + w.pool - 1u) / w.pool : kTailCheck);
+        if (t < kLookahead) continue;
+        bool empty = false;
+        if ((e = drained(progress, t - kLookahead, samples, &empty)) != cudaSuccess) return e;
+        if (empty) break;
     }
     return cudaSuccess;
 }

@@ -249,6 +249,25 @@ inline cudaError_t persistent_grid(const void *fn, size_t smem, int *grid, int t
     return cudaSuccess;
 }
 
+// Iterations the host enqueues beyond the one whose start it inspects.
+constexpr uint64_t kLookahead = 2;
+
+// Records the end of iteration t.
+inline cudaError_t iteration_done(WaveProgress &pr, uint64_t t, cudaStream_t stream) {
+    return cudaEventRecord(pr.done[t % kProgressSlots], stream);
+}
+
+// Whether iteration s started with no path kept and no sample left (of
+// `samples`): then it and every later iteration had nothing to do.
+inline cudaError_t drained(const WaveProgress &pr, uint64_t s, uint32_t samples, bool *empty) {
+    cudaError_t e = cudaEventSynchronize(pr.done[s % kProgressSlots]);
+    if (e != cudaSuccess) return e;
+    const volatile uint2 *h = pr.host + s % kProgressSlots;
+    const uint32_t kept = h->x, next = h->y;
+    *empty = kept == 0u && next >= samples;
+    return cudaSuccess;
+}
+
 inline cudaError_t mark(StageMarks *m, int stage, cudaStream_t stream) {
     if (!m) return cudaSuccess;
     if (m->used == m->events.size()) {

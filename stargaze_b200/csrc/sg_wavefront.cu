@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters(W, t + 1u)->next = next + take;
         *counters(W, t + 2u) = WaveCounters{};
+        W.progress[t % kProgressSlots] = make_uint2(kept, next);
     }
     if (blockIdx.x * kThreads * kItems >= n) return;
     const Scene S = stage_scene(P, smem);
@@ -344,8 +345,8 @@ size_t wave_result_bytes(uint32_t pixels, uint32_t chunk_samples) {
     return (size_t)pixels * sizeof(float4) * ((size_t)chunk_samples + 1u);
 }
 
-cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *pinned, cudaEvent_t ready,
-                             cudaStream_t stream, WaveRun *run, StageMarks *marks) {
+cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveProgress &progress, cudaStream_t stream,
+                             WaveRun *run, StageMarks *marks) {
     const uint32_t z = p.s.counts[2];
     const uint32_t pixels = p.width * p.height;
     *run = WaveRun{};
@@ -391,8 +392,7 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
     // A path ends within max_vertices * (bodies + 2) + 1 iterations, and an
     // iteration that takes no new sample has a full pool of paths that all
     // advance, so a chunk drains within (samples + 1) * (that + 1)
-    // iterations: a host-side guard, the loop below never waits on the GPU
-    // for longer than one group of iterations.
+    // iterations: a host-side guard.
     const uint64_t cap = (uint64_t)p.s.counts[3] * (p.s.counts[0] + 2u) + 2u;
     for (uint32_t first = 0; first < z; first += chunk) {
         w.chunk_first = first;
@@ -401,12 +401,9 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
         const uint64_t bound = ((uint64_t)samples + 1u) * cap;
         cudaError_t e = cudaMemsetAsync(w.counters, 0, kWaveCounterSets * sizeof(WaveCounters), stream);
         if (e != cudaSuccess) return e;
-        // Every iteration takes at most `pool` new samples, so the chunk
-        // cannot drain before all samples could have been taken; after a
-        // check the same bound gives the next one, and once every sample is
-        // out the check runs every kTailCheck iterations.
-        constexpr uint64_t kTailCheck = 2;
-        uint64_t check_at = (samples + (uint64_t)w.pool - 1u) / w.pool;
+        // The host reads the start of iteration t - kLookahead while the
+        // GPU runs the later ones; once one started empty the chunk has
+        // drained (the iterations after it are empty launches).
         for (uint64_t t = 0;; ++t) {
             if (t >= bound) return cudaErrorLaunchTimeout;
             const uint32_t it = (uint32_t)t;
@@ -425,17 +422,13 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveCounters *p
                 default: e = run_iteration<true, true, false, true>(p, w, it, grid, smem, stream, marks); break;
             }
             if (e != cudaSuccess) return e;
+            if ((e = iteration_done(progress, t, stream)) != cudaSuccess) return e;
             run->iterations += 1;
             run->kernels += 3;
-            if (t + 1 < check_at) continue;
-            const WaveCounters *dev = w.counters + ((t + 1) % kWaveCounterSets);
-            if ((e = cudaMemcpyAsync(pinned, dev, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream)) !=
-                    cudaSuccess ||
-                (e = cudaEventRecord(ready, stream)) != cudaSuccess || (e = cudaEventSynchronize(ready)) != cudaSuccess)
-                return e;
-            if (pinned->cont == 0 && pinned->next >= samples) break;
-            const uint64_t left = pinned->next >= samples ? 0u : samples - pinned->next;
-            check_at = t + 1 + (left ? (left + w.pool - 1u) / w.pool : kTailCheck);
+            if (t < kLookahead) continue;
+            bool empty = false;
+            if ((e = drained(progress, t - kLookahead, samples, &empty)) != cudaSuccess) return e;
+            if (empty) break;
         }
         const bool first_chunk = first == 0, last_chunk = first + w.chunk_samples >= z;
         if ((e = mark(marks, kStageResolve, stream)) != cudaSuccess) return e;
