@@ -479,9 +479,10 @@ SG_API int sg_set_exposure_controls(sg_context *ctx, int automatic, float bias);
 /* Extension (measurement): with timing on, every wavefront stage launch is
  * bracketed by CUDA events and sg_encode waits for the dispatch to finish;
  * sg_get_stage_times then gives the milliseconds of the last timed
- * dispatch spent in ms[0] extend, ms[1] ring, ms[2] surface, ms[3] resolve
- * and ms[4] between stages (launch gaps and host checks). */
-#define SG_STAGE_COUNT 5
+ * dispatch spent in ms[0] extend, ms[1] ring, ms[2] surface, ms[3] resolve,
+ * ms[4] between stages (launch gaps and host checks) and ms[5] finishing
+ * the last few paths of each sample chunk in one launch. */
+#define SG_STAGE_COUNT 6
 SG_API int sg_set_stage_timing(sg_context *ctx, int enable);
 SG_API int sg_get_stage_times(const sg_context *ctx, float *ms);
 

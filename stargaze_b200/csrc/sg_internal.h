@@ -175,7 +175,7 @@ size_t wave_result_bytes(uint32_t pixels, uint32_t chunk_samples);
 
 // Optional per-stage timing of a wavefront dispatch: an event is recorded
 // at every stage boundary; stage[k] names what runs from mark k to k + 1.
-enum WaveStage : int { kStageExtend = 0, kStageRing, kStageSurface, kStageResolve, kStageGap, kStageCount };
+enum WaveStage : int { kStageExtend = 0, kStageRing, kStageSurface, kStageResolve, kStageGap, kStageFinish, kStageCount };
 struct StageMarks {
     std::vector<cudaEvent_t> events;  // owned; grown on demand, reused
     std::vector<int> stage;

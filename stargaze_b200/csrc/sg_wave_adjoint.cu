@@ -50,6 +50,12 @@ namespace {
 #define SG_WAVE_ADJ_SHADE_THREADS 256
 #endif
 constexpr int kShadeThreads = SG_WAVE_ADJ_SHADE_THREADS;
+// Live paths at or below which, once every sample is out, the rest of the
+// replay runs in adj_finish (about one resident wave of its threads).
+#ifndef SG_ADJ_FINISH_PATHS
+#define SG_ADJ_FINISH_PATHS (1u << 18)
+#endif
+constexpr uint32_t kFinishPaths = SG_ADJ_FINISH_PATHS;
 
 // Slot state (float4 words):
 //   0  a.xyz, cap                         5  w_pdf.xyz        (pass 2)
@@ -488,6 +494,61 @@ __global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
     close_sink(A, bs, dropped);
 }
 
+// The tail of the replay: once every sample is out and few paths are left
+// (mostly second replays of samples whose cap binds, a fraction of a
+// percent), stage iterations cost their launches and load chains for a
+// handful of paths each. Here every path live at the start of iteration t
+// runs to its end in its own thread — the remaining vertices, and the
+// second replay if its first ends on a binding cap — through the same
+// per-path functions and hooks; no queues, no barriers.
+template <bool L, bool F>
+__global__ void __launch_bounds__(kShadeThreads, SG_WAVE_ADJ_SHADE_MIN_BLOCKS)
+    adj_finish(const __grid_constant__ TraceParams P, const __grid_constant__ AdjointParams A,
+               const __grid_constant__ WaveParams W, const __grid_constant__ AdjointWave X, uint32_t t) {
+    extern __shared__ float4 smem[];
+    const uint32_t n = counters(W, t)->cont;
+    if (blockIdx.x * kShadeThreads >= n) return;
+    const BlockSink bs = open_sink(P, A, smem);
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    const uint32_t n_bodies = P.s.counts[0];
+    const uint32_t own_n = 6u * (n_bodies < kColorSlots ? n_bodies : kColorSlots);
+    const GradSink sink{bs.own, own_n, bs.window, A.tau_window, bs.window + A.tau_window, A.color_window, A.grad,
+                        blockDim.x};
+    unsigned long long dropped = 0;
+    const float4 *st = W.state[t & 1u];
+#pragma unroll 1
+    for (uint32_t i = blockIdx.x * kShadeThreads + threadIdx.x; i < n; i += gridDim.x * kShadeThreads) {
+        Path p;
+        load_ray_part(st, W.pool, i, p);
+        load_radiance_part(st, W.pool, i, p);
+        load_shade_part(st, W.pool, i, p);
+        const float4 g = st[6 * W.pool + i];
+        const uint32_t pixel = __float_as_uint(g.z), slot = __float_as_uint(g.w);
+        const float3 w = pixel_weight(A, pixel);
+        Prb G;
+        uint32_t smp;
+        const uint32_t stops = load_prb(X, slot, w, G, smp) & kFlagStops;
+        G.sink = sink;
+        G.inv = bs.inv;
+        G.local = bs.local;
+        G.local_stride = blockDim.x;
+#pragma unroll 1
+        for (;;) {
+            const bool ended = step(S, K, p, G);
+            if (!ended) {
+                // A checkpointed sample's replay ends where its first record
+                // starts (the segment kernel replays the rest).
+                if (G.known_total && stops && p.depth >= A.ck.every) break;
+                continue;
+            }
+            if (!end_replay(P, K, G, p, pixel, smp, w)) break;
+        }
+        dropped += G.dropped;
+    }
+    close_sink(A, bs, dropped);
+}
+
 template <bool L, bool F>
 cudaError_t run_adjoint_iteration(const TraceParams &p, const AdjointParams &a, const WaveParams &w,
                                   const AdjointWave &x, uint32_t t, const int (&grid)[3], const size_t (&smem)[2],
@@ -550,6 +611,15 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
     // iteration bound; see launch_wavefront for the host-side guard.
     const uint64_t cap = 2ull * ((uint64_t)p.s.counts[3] * (p.s.counts[0] + 2u) + 2u);
     const uint64_t bound = ((uint64_t)samples + 1u) * cap;
+    const void *finish = land ? (p.fp64_sites ? (const void *)adj_finish<true, true> : (const void *)adj_finish<true, false>)
+                              : (p.fp64_sites ? (const void *)adj_finish<false, true>
+                                              : (const void *)adj_finish<false, false>);
+    int finish_grid = 0;
+    if (smem[1] > 48u * 1024u) {
+        cudaError_t e = cudaFuncSetAttribute(finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem[1]);
+        if (e != cudaSuccess) return e;
+    }
+    if (cudaError_t e = persistent_grid(finish, smem[1], &finish_grid, kShadeThreads); e != cudaSuccess) return e;
     cudaError_t e = cudaMemsetAsync(w.counters, 0, kWaveCounterSets * sizeof(WaveCounters), stream);
     if (e != cudaSuccess) return e;
     for (uint64_t t = 0;; ++t) {
@@ -564,9 +634,27 @@ cudaError_t launch_adjoint_wavefront(const TraceParams &p, const AdjointParams &
         run->iterations += 1;
         run->kernels += 3;
         if (t < kLookahead) continue;
-        bool empty = false;
-        if ((e = drained(progress, t - kLookahead, samples, &empty)) != cudaSuccess) return e;
-        if (empty) break;
+        WaveStart start;
+        if ((e = started(progress, t - kLookahead, &start)) != cudaSuccess) return e;
+        if (start.kept == 0u && start.next >= samples) break;
+        // Every sample is out and few paths are left: no later iteration
+        // holds more than iteration t - kLookahead did; finish them at once.
+        if (start.next >= samples && start.kept <= kFinishPaths) {
+            const uint32_t blocks = std::min<uint32_t>(finish_grid, (start.kept + kShadeThreads - 1) / kShadeThreads);
+            const uint32_t next_t = it + 1u;
+            if (blocks > 0u) {
+                if (land) {
+                    if (p.fp64_sites) adj_finish<true, true><<<blocks, kShadeThreads, smem[1], stream>>>(p, a, w, x, next_t);
+                    else adj_finish<true, false><<<blocks, kShadeThreads, smem[1], stream>>>(p, a, w, x, next_t);
+                } else {
+                    if (p.fp64_sites) adj_finish<false, true><<<blocks, kShadeThreads, smem[1], stream>>>(p, a, w, x, next_t);
+                    else adj_finish<false, false><<<blocks, kShadeThreads, smem[1], stream>>>(p, a, w, x, next_t);
+                }
+                if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                run->kernels += 1;
+            }
+            break;
+        }
     }
     return cudaSuccess;
 }

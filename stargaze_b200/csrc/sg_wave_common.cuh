@@ -257,15 +257,26 @@ inline cudaError_t iteration_done(WaveProgress &pr, uint64_t t, cudaStream_t str
     return cudaEventRecord(pr.done[t % kProgressSlots], stream);
 }
 
-// Whether iteration s started with no path kept and no sample left (of
-// `samples`): then it and every later iteration had nothing to do.
-inline cudaError_t drained(const WaveProgress &pr, uint64_t s, uint32_t samples, bool *empty) {
+// What iteration s started from: the paths kept and the next sample.
+struct WaveStart {
+    uint32_t kept, next;
+};
+inline cudaError_t started(const WaveProgress &pr, uint64_t s, WaveStart *out) {
     cudaError_t e = cudaEventSynchronize(pr.done[s % kProgressSlots]);
     if (e != cudaSuccess) return e;
     const volatile uint2 *h = pr.host + s % kProgressSlots;
-    const uint32_t kept = h->x, next = h->y;
-    *empty = kept == 0u && next >= samples;
+    out->kept = h->x;
+    out->next = h->y;
     return cudaSuccess;
+}
+
+// Whether iteration s started with no path kept and no sample left (of
+// `samples`): then it and every later iteration had nothing to do.
+inline cudaError_t drained(const WaveProgress &pr, uint64_t s, uint32_t samples, bool *empty) {
+    WaveStart start;
+    cudaError_t e = started(pr, s, &start);
+    if (e == cudaSuccess) *empty = start.kept == 0u && start.next >= samples;
+    return e;
 }
 
 inline cudaError_t mark(StageMarks *m, int stage, cudaStream_t stream) {

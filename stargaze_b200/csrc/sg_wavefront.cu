@@ -259,6 +259,36 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade
     }
 }
 
+// The tail of a chunk: once every sample is out and few paths are left,
+// stage iterations cost their launches and load chains for a handful of
+// paths each. Here every path live at the start of iteration t runs to its
+// end in its own thread through the same per-path functions (step(), as
+// the megakernel), and writes its result as the stages would.
+template <bool L, bool F, bool A>
+__global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_finish(const __grid_constant__ TraceParams P,
+                                                                            const __grid_constant__ WaveParams W,
+                                                                            uint32_t t) {
+    extern __shared__ float4 smem[];
+    const uint32_t n = counters(W, t)->cont;
+    if (blockIdx.x * kThreads >= n) return;
+    const Scene S = stage_scene(P, smem);
+    const Counter<false, L, F> K{nullptr};
+    Forward<A> nograd;
+    const float4 *st = W.state[t & 1u];
+#pragma unroll 1
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        Path p;
+        const uint32_t slot = load_ray_part(st, W.pool, i, p);
+        load_radiance_part(st, W.pool, i, p);
+        load_shade_part(st, W.pool, i, p);
+        p.backdrop = f3(0.0f, 0.0f, 0.0f);
+        while (!step(S, K, p, nograd)) {
+        }
+        W.results[slot] = finish_path(p);
+        if (W.sky_results) W.sky_results[slot] = pack3(p.backdrop, 0.0f);
+    }
+}
+
 // Per pixel: the chunk's samples summed in sample order onto the running
 // total, and on the last chunk the megakernel's compensated fold.
 __global__ void __launch_bounds__(kThreads) wave_resolve(const __grid_constant__ TraceParams P,
@@ -312,16 +342,32 @@ __global__ void __launch_bounds__(kThreads) wave_resolve(const __grid_constant__
 // ---------------------------------------------------------------------------
 struct StageSet {
     const void *extend, *ring, *surface;
+    const void *finish;  // null where vertex checkpoints are stored (their records need the stages' appends)
 };
 
 template <bool L, bool F, bool A, bool CK = false>
 StageSet stage_set() {
     return StageSet{(const void *)wave_extend<L, F, A>, (const void *)wave_shade<L, F, true, A, CK>,
-                    (const void *)wave_shade<L, F, false, A, CK>};
+                    (const void *)wave_shade<L, F, false, A, CK>,
+                    CK ? nullptr : (const void *)wave_finish<L, F, A>};
 }
 
+template <bool L, bool F, bool A>
+cudaError_t run_finish(const TraceParams &p, const WaveParams &w, uint32_t t, uint32_t blocks, size_t smem,
+                       cudaStream_t stream) {
+    wave_finish<L, F, A><<<blocks, kThreads, smem, stream>>>(p, w, t);
+    return cudaGetLastError();
+}
+
+// Live paths at or below which, once every sample of the chunk is out, the
+// rest of the chunk runs in wave_finish (about one resident wave).
+#ifndef SG_WAVE_FINISH_PATHS
+#define SG_WAVE_FINISH_PATHS (1u << 18)
+#endif
+constexpr uint32_t kFinishPaths = SG_WAVE_FINISH_PATHS;
+
 template <bool L, bool F, bool A, bool CK = false>
-cudaError_t run_iteration(const TraceParams &p, const WaveParams &w, uint32_t t, const int (&grid)[3], size_t smem,
+cudaError_t run_iteration(const TraceParams &p, const WaveParams &w, uint32_t t, const int (&grid)[4], size_t smem,
                           cudaStream_t stream, StageMarks *m) {
     cudaError_t e;
     if ((e = mark(m, kStageExtend, stream)) != cudaSuccess) return e;
@@ -374,9 +420,10 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveProgress &p
         default: set = stage_set<true, true, false, true>(); break;
     }
     const size_t smem = trace_smem_bytes(p);
-    const void *fns[3] = {set.extend, set.ring, set.surface};
-    int grid[3];
-    for (int k = 0; k < 3; ++k) {
+    const void *fns[4] = {set.extend, set.ring, set.surface, set.finish};
+    int grid[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) {
+        if (!fns[k]) continue;
         const size_t bytes = smem;
         if (bytes > 48u * 1024u) {
             cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -426,9 +473,31 @@ cudaError_t launch_wavefront(const TraceParams &p, WaveParams w, WaveProgress &p
             run->iterations += 1;
             run->kernels += 3;
             if (t < kLookahead) continue;
-            bool empty = false;
-            if ((e = drained(progress, t - kLookahead, samples, &empty)) != cudaSuccess) return e;
-            if (empty) break;
+            WaveStart start;
+            if ((e = started(progress, t - kLookahead, &start)) != cudaSuccess) return e;
+            if (start.kept == 0u && start.next >= samples) break;
+            // Every sample is out and few paths are left: no later iteration
+            // holds more than iteration t - kLookahead did; finish them at once.
+            if (set.finish && start.next >= samples && start.kept <= kFinishPaths) {
+                const uint32_t blocks = std::min<uint32_t>(grid[3], (start.kept + kThreads - 1) / kThreads);
+                if (blocks > 0u) {
+                    if ((e = mark(marks, kStageFinish, stream)) != cudaSuccess) return e;
+                    switch (variant) {
+                        case 0: e = run_finish<false, false, false>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 1: e = run_finish<false, true, false>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 2: e = run_finish<true, false, false>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 3: e = run_finish<true, true, false>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 4: e = run_finish<false, false, true>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 5: e = run_finish<false, true, true>(p, w, it + 1u, blocks, smem, stream); break;
+                        case 6: e = run_finish<true, false, true>(p, w, it + 1u, blocks, smem, stream); break;
+                        default: e = run_finish<true, true, true>(p, w, it + 1u, blocks, smem, stream); break;
+                    }
+                    if (e != cudaSuccess) return e;
+                    if ((e = mark(marks, kStageGap, stream)) != cudaSuccess) return e;
+                    run->kernels += 1;
+                }
+                break;
+            }
         }
         const bool first_chunk = first == 0, last_chunk = first + w.chunk_samples >= z;
         if ((e = mark(marks, kStageResolve, stream)) != cudaSuccess) return e;

@@ -159,7 +159,7 @@ class PathTracer:
         name = "wavefront" if kind.value == abi.INTEGRATOR_WAVEFRONT else "megakernel"
         return {"integrator": name, "pool_paths": pool.value, "iterations": iterations.value}
 
-    STAGES = ("extend", "ring", "surface", "resolve", "gaps")
+    STAGES = ("extend", "ring", "surface", "resolve", "gaps", "finish")
 
     def set_stage_timing(self, enable: bool) -> None:
         """Bracket every wavefront stage with CUDA events (measurement)."""
