@@ -449,14 +449,37 @@ def adjoint_ratio(wl, device: int, stream, reps: int = 3) -> dict:
             mega.append(m)
             bwd.append(e[0].elapsed_time(e[1]))
             per_pixel.append(e[2].elapsed_time(e[3]))
+    # With the forward storing each sample's radiance (sg_set_checkpoints
+    # with every beyond the bounce limit: totals only, 16 B per sample),
+    # samples whose ring-indirect cap does not bind replay once with every
+    # weight known.
+    t.set_integrator("wavefront")
+    t.set_checkpoints(wl.max_bounces + 1, wl.spp)
+    fwd_totals, bwd_totals = [], []
+    for r in range(reps + 1):
+        frame = wl.frame.copy()
+        frame.scene_time = float(-200 - r)
+        ft = timed_forward(t, wl, frame, stream)
+        tape = t.tape()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e[0].record(stream)
+        t.backward(frame, tape, dl, stream)
+        e[1].record(stream)
+        stream.synchronize()
+        if r > 0:
+            fwd_totals.append(ft)
+            bwd_totals.append(e[0].elapsed_time(e[1]))
     t.close()
     f, m, b = statistics.median(fwd), statistics.median(mega), statistics.median(bwd)
+    ft, bt = statistics.median(fwd_totals), statistics.median(bwd_totals)
     params = int(sum(v.size for v in wl.ring_tables.values())) + 6 * len(wl.frame.bodies)
     if wl.landscape is not None and wl.landscape.albedo_map is not None:
         params += int(wl.landscape.albedo_map.size)
     return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp, "forward_ms": f,
             "forward_megakernel_ms": m, "backward_ms": b, "backward_per_pixel_ms": statistics.median(per_pixel),
             "ratio": b / f, "forward_plus_adjoint_over_forward": (f + b) / f,
+            "with_radiance_totals": {"forward_ms": ft, "backward_ms": bt,
+                                     "forward_plus_adjoint_over_plain_forward": (ft + bt) / f},
             "parameters": params, "dropped_entries": int(g.dropped),
             "note": "forward: wavefront; backward: staged adjoint (per-pixel adjoint kernel beside it)"}
 
