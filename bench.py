@@ -921,6 +921,25 @@ def run_ours(args):
             "cpu_baseline": base,
             **extras,
         }
+        if extras:
+            # The configs' headline figures once more, last, where a reader of
+            # the line's end finds them.
+            ring, terrain = extras["adjoint"]["ring_512"], extras["adjoint"]["terrain_1080p"]
+            result["summary"] = {
+                "C1_msamples_per_s": extras["configs"]["spheres_256"]["msamples_per_s"],
+                "C2_msamples_per_s": value, "C2_e2e_msamples_per_s": e2e_value,
+                "C2_spp_to_1pct_vs_oracle": extras["convergence"]["vs_oracle"]["spp_to_1pct"]
+                if extras["convergence"].get("vs_oracle") else None,
+                "C3_msamples_per_s": extras["configs"]["terrain_1080p"]["msamples_per_s"],
+                "C4_forward_plus_adjoint_over_forward": ring["forward_plus_adjoint_over_forward"],
+                "C5_forward_plus_adjoint_over_forward": terrain["forward_plus_adjoint_over_forward"],
+                "C5_checkpoints_vs_replay_ms": [extras["adjoint"]["checkpoints_terrain_1080p"]["checkpoints"]
+                                                ["forward_plus_adjoint_ms"],
+                                                extras["adjoint"]["checkpoints_terrain_1080p"]["replay"]
+                                                ["forward_plus_adjoint_ms"]],
+                "roofline_frac": result["roofline"]["frac"],
+                "cpu_baseline_msamples_per_s": base["value"] if base else None,
+            }
         print(json.dumps(result), flush=True)
     tracer.close()
     if dist:
