@@ -181,9 +181,11 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
 }
 
 // Ring (R == true) or surface stage over its queue. CK: the forward stores
-// vertex checkpoints (W.ck).
+// vertex checkpoints (W.ck). The ring stage runs at 3 CTAs per SM (85
+// registers, fewer spills: 13.07 → 12.81 ms per 1080p ring step; 2 CTAs
+// measured 13.57), the surface stage at 4 (3 measured slower).
 template <bool L, bool F, bool R, bool A, bool CK = false>
-__global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
+__global__ void __launch_bounds__(kThreads, R ? 3 : SG_WAVE_SHADE_MIN_BLOCKS) wave_shade(const __grid_constant__ TraceParams P,
                                                                            const __grid_constant__ WaveParams W,
                                                                            uint32_t t) {
     extern __shared__ float4 smem[];
