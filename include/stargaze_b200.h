@@ -376,8 +376,9 @@ SG_API int sg_set_ringshine(sg_context *ctx, int enable);
  * of the accumulation). sg_backward then replays each sample only up to its
  * first checkpoint and every later segment from its record, in parallel,
  * with the path's total known, so nothing is deferred or replayed twice.
- * An `every` of at least the bounce limit stores the radiance alone: the
- * backward then replays whole paths, once each, with every weight known.
+ * An `every` of at least the bounce limit stores the radiance alone (no
+ * record buffer is allocated): the backward then replays whole paths, once
+ * each, with every weight known.
  * Samples whose ring-indirect cap binds, or whose records did not fit
  * `record_bytes` (0: half the free device memory at the first encode), are
  * replayed from their noise key as without checkpoints. Frames with host

@@ -740,6 +740,12 @@ static uint32_t wave_pool_for(const sg_context *ctx, uint32_t samples, uint32_t 
     return (uint32_t)std::min<uint64_t>(want, (work + 255u) & ~(uint64_t)255u);
 }
 
+// Whether the forward stores vertex records: some depth a scatter can reach
+// (below the bounce limit) is a multiple of `every`.
+static bool checkpoint_records(const sg_context *ctx) {
+    return ctx->ck_every > 0u && ctx->ck_every < ctx->options.max_bounces;
+}
+
 // Path state planes, extend results, queues and counters for `pool` paths
 // (the buffer grows only; forward and backward share it).
 static int ensure_wave_state(sg_context *ctx, uint32_t pool, sg::WaveParams &w) {
@@ -875,7 +881,9 @@ static int ensure_checkpoints(sg_context *ctx, cudaStream_t stream) {
         ctx->ck_totals_size = totals;
     }
     if (!ctx->ck_count) SG_CUDA(ctx, cudaMalloc(&ctx->ck_count, sizeof(uint32_t)));
-    if (!ctx->ck_records) {
+    // Records only where a scatter can bring a path to a checkpoint depth;
+    // `every` beyond the bounce limit stores the radiance alone.
+    if (!ctx->ck_records && checkpoint_records(ctx)) {
         const size_t record = sg::kCheckpointVec4 * sizeof(float4);
         size_t budget = ctx->ck_record_bytes;
         if (budget == 0) {
@@ -969,7 +977,7 @@ static int encode_impl(sg_context *ctx, const sg_frame *frame, void *stream_ptr,
             if (ctx->ck_valid) {
                 status = ensure_checkpoints(ctx, stream);
                 if (status != SG_OK) return status;
-                w.ck.records = ctx->ck_records;
+                w.ck.records = checkpoint_records(ctx) ? ctx->ck_records : nullptr;
                 w.ck.count = ctx->ck_count;
                 w.ck.capacity = ctx->ck_capacity;
                 w.ck.totals = ctx->ck_totals;
@@ -1533,13 +1541,15 @@ int sg_backward(sg_context *ctx, const sg_frame *frame, const sg_tape *tape, con
     // With vertex checkpoints of this accumulation, the replay (staged or
     // per-pixel) takes each sample, its radiance known, only up to its first
     // checkpoint, and the segment kernel replays the rest from the records.
-    const bool checkpointed = ctx->ck_every > 0u && ctx->ck_valid && ctx->ck_records;
+    const bool checkpointed = ctx->ck_every > 0u && ctx->ck_valid && ctx->ck_totals;
     uint32_t records = 0;
     if (checkpointed) {
-        uint32_t claimed = 0;
-        SG_CUDA(ctx, cudaMemcpyAsync(&claimed, ctx->ck_count, sizeof(claimed), cudaMemcpyDeviceToHost, stream));
-        SG_CUDA(ctx, cudaStreamSynchronize(stream));
-        records = std::min(claimed, ctx->ck_capacity);
+        if (ctx->ck_records) {
+            uint32_t claimed = 0;
+            SG_CUDA(ctx, cudaMemcpyAsync(&claimed, ctx->ck_count, sizeof(claimed), cudaMemcpyDeviceToHost, stream));
+            SG_CUDA(ctx, cudaStreamSynchronize(stream));
+            records = std::min(claimed, ctx->ck_capacity);
+        }
         a.ck.records = ctx->ck_records;
         a.ck.count = ctx->ck_count;
         a.ck.capacity = ctx->ck_capacity;

@@ -23,9 +23,10 @@ namespace {
 #define SG_WAVE_SHADE_MIN_BLOCKS SG_WAVE_MIN_BLOCKS
 #endif
 // Paths a thread of the extend stage takes per queue append (celestial
-// frames).
+// frames). Measured on the 1080p ring step: 1 59.5 ms, 4 55.9, 6 55.1,
+// 8 55.5.
 #ifndef SG_WAVE_EXTEND_ITEMS
-#define SG_WAVE_EXTEND_ITEMS 4
+#define SG_WAVE_EXTEND_ITEMS 6
 #endif
 
 // ---------------------------------------------------------------------------

@@ -55,9 +55,9 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                                                                             uint32_t t) {
     extern __shared__ float4 smem[];
     // Celestial frames take several paths per append (their work per path
-    // is even); landscape frames one, so that a CTA's last round is small
-    // when traversal costs differ (measured: rings 59.5 -> 56.5 ms per step
-    // with four, terrain 455 -> 531 ms). Landscape frames keep the append
+    // is even; SG_WAVE_EXTEND_ITEMS); landscape frames one, so that a CTA's
+    // last round is small when traversal costs differ (measured with four:
+    // rings 59.5 -> 56.5 ms per step, terrain 455 -> 531 ms). Landscape frames keep the append
     // barrier although their quadtree walks differ in length: writing a
     // per-path kind instead and building the queues in a kernel of their
     // own let the warps of a CTA drift apart, and the terrain step went
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_EXTEND_MIN_BLOCKS) wave_exte
                     }
                     W.results[slot] = finish_path(p);
                     if (W.sky_results) W.sky_results[slot] = pack3(p.backdrop, 0.0f);
-                    if (W.ck.records) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
+                    if (W.ck.totals) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
                 }
             }
         }
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kThreads, R ? 3 : SG_WAVE_SHADE_MIN_BLOCKS) wa
             if (ended) {
                 W.results[slot] = finish_path(p);
                 if (W.sky_results) W.sky_results[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if constexpr (CK) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
+                if (W.ck.totals) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
             }
             if constexpr (CK) {
                 // A scatter brought the depth to a checkpoint depth.
@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(kThreads, SG_WAVE_SHADE_MIN_BLOCKS) wave_finis
         }
         W.results[slot] = finish_path(p);
         if (W.sky_results) W.sky_results[slot] = pack3(p.backdrop, 0.0f);
+        if (W.ck.totals) checkpoint_total(W.ck, W.chunk_first, P.width * P.height, slot, p);
     }
 }
 
