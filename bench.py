@@ -76,11 +76,11 @@ EVENT_ORDER = ["vertices", "sphere_tests", "sphere_hits", "ring_tests", "light_s
                "prop_tests"]
 # DRAM traffic of one 64-sample dispatch of the ring workload: an ncu
 # capture of one steady-state iteration of the three stage kernels (4 Mi-path
-# pool: 664 MB for 4.19 M path extensions) scaled to the dispatch's 183 M
+# pool: 655 MB for 4.19 M path extensions) scaled to the dispatch's 183 M
 # path extensions (1.38 per sample, counting kernel). Issue-slot fraction of
 # the same capture, weighted by the stages' share of the step.
-TRAFFIC_BYTES_PER_LAUNCH = 664.2e6 * (1.38 * 1920 * 1080 * 64) / 4.194e6
-ISSUE_SLOT_FRACTION = 0.59
+TRAFFIC_BYTES_PER_LAUNCH = 654.6e6 * (1.38 * 1920 * 1080 * 64) / 4.194e6
+ISSUE_SLOT_FRACTION = 0.60
 L2_FLUSH_BYTES = 256 << 20
 
 
