@@ -16,12 +16,16 @@ memory and the 33 MB accumulation read back to the host every step.
 `--impl reference` times the CPU restatement of the reference integrator
 (the oracle; the reference's own Rust/WGSL cannot run here) on the host.
 
-After the timed region (one GPU only) two further figures of the metric are
-measured: `convergence`, the relative RMSE of the 256-spp image against a
-4096-spp image of disjoint noise and the samples (and time) it takes to reach
-1 %; and `adjoint`, the path-replay adjoint's time against the forward's at
-equal spp on the ring scene (512x512, 64 spp) and on the terrain scene
-(1920x1080, 256 spp, 1024^2 albedo map).
+After the timed region (one GPU only) further figures of the metric are
+measured: `convergence`, the relative RMSE of the 256-spp image against the
+oracle's 4096-spp image of the workload (oracle/render_converged.py, when
+its cache is present) and against this integrator's own 4096-spp image, and
+the samples (and time) each implies for 1 %; `adjoint`, the path-replay
+adjoint's time against the forward's at equal spp on the ring scene
+(512x512, 64 spp) and on the terrain scene (1920x1080, 256 spp, 1024^2
+albedo map), and vertex checkpoints against replay on the latter; the C1
+and C3 configurations with their own rooflines; the ring inverse problem.
+The line ends with a summary of those figures.
 """
 from __future__ import annotations
 
