@@ -398,6 +398,15 @@ def convergence(wl, image: np.ndarray, spp: int, msamples_per_s: float, device: 
         # Both references are converged estimates of the same image: their
         # distance bounds any bias between the CUDA path and the oracle.
         out["oracle_vs_self_relative_rmse"] = relative_rmse(own_image, oracle_image)
+    # The oracle's f64 build at the same noise keys (the same paths, f64
+    # arithmetic): the f32 image's distance from it, and the 1 % figures.
+    cached_f64 = cached.with_name(f"{wl.name}_{CONVERGED_SPP}spp_f64.npy")
+    if cached_f64.exists():
+        oracle_f64 = np.load(cached_f64)
+        out["vs_oracle_f64"] = _to_1pct(relative_rmse(image, oracle_f64), spp, CONVERGED_SPP, wl.width, wl.height,
+                                        msamples_per_s)
+        if cached.exists():
+            out["oracle_f32_vs_f64_relative_rmse"] = relative_rmse(oracle_image, oracle_f64)
     return out
 
 

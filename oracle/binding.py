@@ -20,6 +20,9 @@ from stargaze_b200.scene import Frame
 
 ORACLE_DIR = Path(__file__).resolve().parent
 LIBRARY = ORACLE_DIR / "liboracle.so"
+# The same restatement with its arithmetic in f64 (-DORACLE_F64): converged
+# reference images free of f32 rounding. The interface is the f32 one.
+LIBRARY_F64 = ORACLE_DIR / "liboracle_f64.so"
 
 
 class Tables(C.Structure):
@@ -63,7 +66,7 @@ class Events(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
-_lib = None
+_libs: dict = {}
 
 
 def build() -> Path:
@@ -71,13 +74,13 @@ def build() -> Path:
     return LIBRARY
 
 
-def load() -> C.CDLL:
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not LIBRARY.exists():
+def load(f64: bool = False) -> C.CDLL:
+    if f64 in _libs:
+        return _libs[f64]
+    path = LIBRARY_F64 if f64 else LIBRARY
+    if not path.exists():
         build()
-    lib = C.CDLL(str(LIBRARY))
+    lib = C.CDLL(str(path))
     P = C.c_void_p
     S = C.POINTER(abi.Settings)
     lib.oracle_dispatch.argtypes = [S, P, C.POINTER(Tables), P, P, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(Events)]
@@ -107,7 +110,7 @@ def load() -> C.CDLL:
     for name in ("oracle_dispatch", "oracle_trace_sample", "oracle_closest_hit", "oracle_light_visibility",
                  "oracle_reference_visibility", "oracle_ring_probe", "oracle_sample_light"):
         getattr(lib, name).restype = C.c_int
-    _lib = lib
+    _libs[f64] = lib
     return lib
 
 
@@ -228,8 +231,8 @@ def frame_bytes(frame: Frame) -> bytes:
 class OracleTracer:
     """CPU restatement of the `PathTracer` host contract on the oracle."""
 
-    def __init__(self, dimensions, options: abi.Options | None = None, threads: int = 0):
-        self.lib = load()
+    def __init__(self, dimensions, options: abi.Options | None = None, threads: int = 0, f64: bool = False):
+        self.lib = load(f64)
         self.width, self.height = int(dimensions[0]), int(dimensions[1])
         self.opts = abi.Options.from_buffer_copy(options if options is not None else abi.default_options())
         self.threads = threads
