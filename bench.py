@@ -943,6 +943,8 @@ def run_ours(args):
                 "C2_msamples_per_s": value, "C2_e2e_msamples_per_s": e2e_value,
                 "C2_spp_to_1pct_vs_oracle": extras["convergence"]["vs_oracle"]["spp_to_1pct"]
                 if extras["convergence"].get("vs_oracle") else None,
+                "C2_spp_to_1pct_vs_oracle_f64": extras["convergence"]["vs_oracle_f64"]["spp_to_1pct"]
+                if extras["convergence"].get("vs_oracle_f64") else None,
                 "C3_msamples_per_s": extras["configs"]["terrain_1080p"]["msamples_per_s"],
                 "C4_forward_plus_adjoint_over_forward": ring["forward_plus_adjoint_over_forward"],
                 "C5_forward_plus_adjoint_over_forward": terrain["forward_plus_adjoint_over_forward"],
