@@ -269,15 +269,16 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
     const float *rc = T + t_cache(cells);
     const float2 root = t_interval(f3(rc[0], rc[1], rc[2]), f3(rc[3], rc[4], rc[5]), o, inv);
     if (root.x > root.y || root.y <= 0.001f || root.x >= limit) return result;
-    uint32_t stack_node[kTerrainStack];
-    float stack_t[kTerrainStack];
-    stack_node[0] = 0u;
-    stack_t[0] = fmaxf(root.x, 0.0f);
+    // Entries (node, entry distance bits): one 8-byte local access per push
+    // and per pop.
+    uint2 stack[kTerrainStack];
+    stack[0] = make_uint2(0u, __float_as_uint(fmaxf(root.x, 0.0f)));
     uint32_t count = 1u;
     while (count > 0u) {
         count -= 1u;
-        if (stack_t[count] >= limit) continue;
-        uint32_t index = stack_node[count];
+        const uint2 top = stack[count];
+        if (__uint_as_float(top.y) >= limit) continue;
+        uint32_t index = top.x;
         for (;;) {
             // The node's size from its heap level; its cell coordinates (the
             // Morton decode of t_node) only where a leaf needs them.
@@ -375,8 +376,7 @@ static __device__ __noinline__ float4 terrain_query(const float *T, uint32_t cel
 #pragma unroll
             for (uint32_t i = 0; i < 3u; ++i) {
                 if (distances[i] < limit && count < (uint32_t)kTerrainStack) {
-                    stack_node[count] = children[i];
-                    stack_t[count] = distances[i];
+                    stack[count] = make_uint2(children[i], __float_as_uint(distances[i]));
                     count += 1u;
                 }
             }
